@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""Throughput of the dealiased MHD nonlinear bundle on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload mhd_bundle|cross_28k|jvp_700k] [--form auto|fp64|split2|split3]
+
+One step = one pass of the nonlinear term over one batch of synthetic
+coefficients.  The default workload is the full MHD bundle: 1.4M Gauss
+points (200,000 P2 triangles x 7), m_max = 64 modes padded to 96,
+inputs u, w, b, j, gradT (6 slots each), outputs u x w, u x b, j x b
+(6 slots) and u . gradT (2 slots), coefficients N(0,1)*exp(-0.1 n).
+
+Metric: Gauss-point*modes per second, whole job.  ``value`` is timed with
+CUDA events on device-resident inputs (22 GB of inputs, far larger than the
+126 MB L2, so no flush is needed); ``e2e`` is the same metric through the
+library's host-array entry point (sfnl_bundle_mhd_host) with pinned host
+buffers, the copies inside the timed region.  Multi-GPU (torchrun) is weak
+scaling: every rank runs the full workload on its own points, no collective
+on the data path; the job time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "nonlinear-term Gauss-pt·modes/s: split-prec vs FP64 on 1 B200 at ≤1e-7 rel err"
+UNIT = "Gauss-pt*modes/s"
+
+# name: points, modes, pad, decay, input fields (6-slot), output slots, description
+WORKLOADS = {
+    "mhd_bundle": dict(np=1_400_000, m=64, pad=96, alpha=0.1,
+                       desc="MHD bundle u x w, u x b, j x b, u.gradT; 1.4M Gauss pts (200k P2 triangles x 7), "
+                            "m_max=64 padded to 96"),
+    "cross_28k": dict(np=28_000, m=16, pad=24, alpha=0.3,
+                      desc="cross product u x w; 28k Gauss pts (4000 P2 triangles x 7), m_max=16 padded to 24"),
+}
+IN_SLOTS = {"mhd_bundle": 30, "cross_28k": 12}
+OUT_SLOTS = {"mhd_bundle": 20, "cross_28k": 6}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["hbm_gbs"], p.get("bf16_tflops"), "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def synthetic_device(npts, nslot, m, alpha, seed, device):
+    """Fortran-layout (np, nslot, m) CUDA tensor, N(0,1)*exp(-alpha*n), sine of mode 0 = 0."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    t = torch.randn((m, nslot, npts), generator=g, device=device, dtype=torch.float64)
+    t *= torch.exp(-alpha * torch.arange(m, device=device, dtype=torch.float64))[:, None, None]
+    t[0, 1::2, :] = 0.0
+    return t.permute(2, 1, 0)
+
+
+def run_reference(args, world, rank):
+    """CPU baseline: the oracle's pocketfft port of the reference path on host cores."""
+    if rank != 0:
+        return
+    import numpy as np
+
+    from oracle import ref_fft as R
+
+    wl = WORKLOADS[args.workload]
+    m, pad, alpha = wl["m"], wl["pad"], wl["alpha"]
+    sample = args.cpu_sample or (2000 if args.workload == "mhd_bundle" else 28_000)
+    cores = os.cpu_count() or 1
+    if args.workload == "mhd_bundle":
+        f = [R.synthetic_field(sample, 6, m, alpha, 1000 + i) for i in range(5)]
+        eng = lambda op, x, y: R.fft_par(op, x, y, pad, workers=cores)  # noqa: E731
+        step = lambda: R.mhd_bundle(*f, pad, engine=eng)  # noqa: E731
+    else:
+        V1 = R.synthetic_field(sample, 6, m, alpha, 1001)
+        V2 = R.synthetic_field(sample, 6, m, alpha, 1002)
+        step = lambda: R.fft_par("cross", V1, V2, pad, workers=cores)  # noqa: E731
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / args.steps
+    value = sample * m / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "np": wl["np"], "m_max": m, "m_max_pad": pad, "alpha": alpha,
+                   "sample_points_per_step": sample, "desc": wl["desc"]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{sample} of {wl['np']} points per step, all {m} modes; pocketfft (scipy.fft, "
+                                   f"{cores} workers) restatement of fft_parallel.F90, no MPI_ALLTOALL cost"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mhd_bundle", choices=sorted(WORKLOADS))
+    ap.add_argument("--form", default="auto", choices=["auto", "fp64", "grid", "split2", "split3"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-sample", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = _dist_env()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import sfemans_b200 as sf
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    wl = WORKLOADS[args.workload]
+    npts, m, pad, alpha = wl["np"], wl["m"], wl["pad"], wl["alpha"]
+    seed = 1000 + 97 * rank
+    nin = 5 if args.workload == "mhd_bundle" else 2
+    ins = [synthetic_device(npts, 6, m, alpha, seed + i, dev) for i in range(nin)]
+    if args.workload == "mhd_bundle":
+        outs = tuple(sf.fortran_empty(npts, 6, m, device=dev) for _ in range(3)) + (sf.fortran_empty(npts, 2, m, device=dev),)
+    else:
+        outs = (sf.fortran_empty(npts, 6, m, device=dev),)
+
+    # pick the form
+    forms = {"fp64": dict(algo=sf.ALGO_AUTO), "grid": dict(algo=sf.ALGO_GRID), "split2": dict(split=sf.SPLIT_BF16X2),
+             "split3": dict(split=sf.SPLIT_BF16X3)}
+    form = args.form
+    if form == "auto":
+        form = "split3"
+        try:
+            _call(sf, args.workload, ins, outs, pad, forms[form])
+        except sf.SfnlError:
+            form = "fp64"
+    kw = forms[form]
+    stream = torch.cuda.current_stream()
+
+    def step():
+        _call(sf, args.workload, ins, outs, pad, kw)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    for i in range(args.steps):
+        step()
+        ev[i + 1].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    per = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
+    ms = sum(per) / len(per)
+    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    units = npts * m
+    value = world * units / (ms / 1e3)
+    algo_bytes = 8.0 * m * (IN_SLOTS[args.workload] + OUT_SLOTS[args.workload]) * npts
+    hbm, _, peak_kind = _peaks()
+    achieved = algo_bytes / (ms / 1e3) / 1e9
+
+    # e2e through the host-array entry point (pinned host buffers, copies timed)
+    e2e = None
+    if args.workload == "mhd_bundle" and args.e2e_steps > 0:
+        e2e = _e2e_bundle(sf, torch, ins, npts, m, pad, form, args.e2e_steps, world, dist)
+
+    # accuracy of this form and the CPU baseline, rank 0, single GPU only
+    cpu = None
+    acc = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu, acc = _cpu_baseline(args, ins, outs, npts, m, pad)
+
+    traffic = _traffic(args.workload, form)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if form in ("fp64", "grid") else "bf16-sliced f64 (fp32 accumulate, fp64 recombine)",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "form": form, "np": npts, "m_max": m, "m_max_pad": pad,
+                   "alpha": alpha, "l2": "inputs larger than L2 (no flush needed)", "desc": wl["desc"],
+                   "parallelism": f"point-sharded replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": traffic, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": algo_bytes},
+        "clocks": clk,
+        "gpu_launches": args.steps * 1,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "accuracy": acc,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _call(sf, workload, ins, outs, pad, kw):
+    if workload == "mhd_bundle":
+        sf.bundle_mhd(*ins, m_max_pad=pad, outs=outs, **kw)
+    else:
+        sf.product(sf.OP_CROSS, ins[0], ins[1], out=outs[0], m_max_pad=pad, **kw)
+
+
+def _e2e_bundle(sf, torch, ins, npts, m, pad, form, steps, world, dist):
+    import ctypes
+
+    need = 8 * npts * m * 50
+    try:
+        with open("/proc/meminfo") as f:
+            avail = int([l for l in f if l.startswith("MemAvailable")][0].split()[1]) * 1024
+    except Exception:
+        avail = 0
+    if avail < 2 * need:
+        return {"value": None, "unit": UNIT, "skipped": f"host memory {avail / 1e9:.0f} GB < 2x {need / 1e9:.0f} GB"}
+    h_in = [torch.empty(x.shape[::-1], dtype=torch.float64, pin_memory=True) for x in ins]
+    for h, x in zip(h_in, ins):
+        h.copy_(x.permute(2, 1, 0))
+    h_out = [torch.empty((m, 6, npts), dtype=torch.float64, pin_memory=True) for _ in range(3)]
+    h_out.append(torch.empty((m, 2, npts), dtype=torch.float64, pin_memory=True))
+    P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    fm = 0 if form in ("fp64", "grid") else int(form[-1])
+    torch.cuda.synchronize()
+    rc = sf.lib().sfnl_bundle_mhd_host(*[P(t) for t in h_in + h_out], npts, m, pad, fm)  # warm-up, sizes workspace
+    if rc != 0:
+        return {"value": None, "unit": UNIT, "skipped": sf.last_error()}
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sf.lib().sfnl_bundle_mhd_host(*[P(t) for t in h_in + h_out], npts, m, pad, fm)
+    dt = (time.perf_counter() - t0) / steps
+    t_split = (ctypes.c_double * 3)()
+    sf.lib().sfnl_last_host_timing(ctypes.cast(t_split, ctypes.c_void_p))
+    dt_t = torch.tensor([dt], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(dt_t, op=dist.ReduceOp.MAX)
+    dt = float(dt_t.item())
+    sf.finalize()
+    return {"value": world * npts * m / dt, "unit": UNIT, "h2d_bytes_per_step": 8 * npts * m * 30,
+            "d2h_bytes_per_step": 8 * npts * m * 20, "ms_per_step": dt * 1e3,
+            "last_step_split_s": {"h2d": t_split[0], "kernels": t_split[1], "d2h": t_split[2]},
+            "api": "sfnl_bundle_mhd_host (host arrays, pinned)"}
+
+
+def _cpu_baseline(args, ins, outs, npts, m, pad):
+    """Oracle port timed on the host cores over a bounded sample; also the checker of this run's output."""
+    import numpy as np
+
+    import sfemans_b200 as sf
+    from oracle import ref_fft as R
+
+    sample = args.cpu_sample or (2000 if args.workload == "mhd_bundle" else 28_000)
+    sample = min(sample, npts)
+    cores = os.cpu_count() or 1
+    h = [np.asfortranarray(sf.to_host(x[:sample])) for x in ins]
+    eng = lambda op, x, y: R.fft_par(op, x, y, pad, workers=cores)  # noqa: E731
+    if args.workload == "mhd_bundle":
+        run = lambda: R.mhd_bundle(*h, pad, engine=eng)  # noqa: E731
+    else:
+        run = lambda: (R.fft_par("cross", h[0], h[1], pad, workers=cores),)  # noqa: E731
+    run()
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        ref = run()
+        reps += 1
+        if time.perf_counter() - t0 > 10.0 or reps >= 50:
+            break
+    dt = (time.perf_counter() - t0) / reps
+    names = ["uxw", "uxb", "jxb", "ugradt"] if args.workload == "mhd_bundle" else ["uxw"]
+    acc = {n: R.rel_l2(sf.to_host(o[:sample]), r) for n, o, r in zip(names, outs, ref)}
+    cpu = {"value": sample * m / dt, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"{sample} of {npts} points x {m} modes, {reps} reps; pocketfft (scipy.fft) restatement of "
+                     "fft_parallel.F90 with all modes on one process (no MPI_ALLTOALL)"}
+    return cpu, {"rel_l2_vs_cpu_port": acc, "sample_points": sample}
+
+
+def _traffic(workload, form):
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            t = json.load(f)
+        return t.get(f"{workload}:{form}")
+    except Exception:
+        return None
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,181 @@
+/*
+ * sfemans_nl.h -- C-ABI of the B200 pseudo-spectral nonlinear-term library.
+ *
+ * Replaces the dealiased products of SFEMaNS's MODULE fft_parallele
+ * (SOURCES/POST_PROCESSING/fft_parallel.F90, PUBLIC list :8-17):
+ *   FFT_PAR_CROSS_PROD_DCL  :147-328   V_out = V1 x V2
+ *   FFT_PAR_DOT_PROD_DCL    :330-500   c_out = V1 . V2
+ *   FFT_PAR_PROD_DCL        :502-665   c_out = c1 * c2
+ *
+ * Array layout: every coefficient array is the Fortran array V(np, nslot, m)
+ * in column-major order, point index fastest: element (p, s, n) is at
+ * V[p + np*(s + nslot*n)].  Slot 2k (0-based) holds the cosine coefficient
+ * and slot 2k+1 the sine coefficient of component k (r, theta, z for
+ * 3-vectors).  Input sine-of-mode-0 entries are ignored; output ones are 0.
+ * Batched arrays append a last dimension: V(np, nslot, m, k_batch).
+ *
+ * Semantics: out = T[ (S a) op (S b) ] where S evaluates the Fourier series
+ * f(theta) = a_0 + sum_{n<m} a_n cos(n theta) + b_n sin(n theta) on a grid of
+ * N equispaced angles and T is the DFT analysis truncated to n < m
+ * (a_0 = (1/N) sum f, a_n = (2/N) sum f cos, b_n = (2/N) sum f sin).
+ * With m_max_pad >= ceil((3m-1)/2), which every SFEMaNS caller uses
+ * (m_max_pad = 3*m_max/2, subroutine_ns_with_velocity.F90:626), the result
+ * is the exact truncated product and does not depend on N.
+ *
+ * Return value of every entry point: SFNL_OK (0) or a negative SFNL_ERR_*
+ * code; sfnl_last_error() gives a one-line message for the calling thread.
+ * The reference prints 'BUG in FFT_PAR_...' and STOPs (fft_parallel.F90:188-191);
+ * the Fortran shim (sfemans_b200/fortran/fft_parallele_gpu.F90) turns a
+ * non-zero status into the same STOP.
+ *
+ * Threading: entry points are thread-safe; work is enqueued on the stream
+ * passed in (NULL = the legacy default stream) and the device-pointer entry
+ * points return without synchronising.  The *_host entry points take host
+ * arrays, copy them in and out, and return after the result is on the host.
+ */
+#ifndef SFEMANS_NL_H
+#define SFEMANS_NL_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void *sfnl_stream_t; /* a cudaStream_t */
+
+enum {
+  SFNL_OK = 0,
+  SFNL_ERR_ARG = -1,         /* null pointer, np < 0, m < 1, k_batch < 1, odd nb_field ... */
+  SFNL_ERR_SHAPE = -2,       /* nb_field/nslot not what the product needs, np > nb_procs*bloc_size */
+  SFNL_ERR_ALIAS = -3,       /* m_max_pad < m_max, or (fast/split forms) grid too short to dealias */
+  SFNL_ERR_UNSUPPORTED = -4, /* size beyond this build's limits, nb_procs != 1 on one GPU */
+  SFNL_ERR_CUDA = -5,        /* a CUDA runtime call or kernel launch failed */
+  SFNL_ERR_NONFINITE = -6,   /* (check mode) a NaN/Inf was found in the output */
+  SFNL_ERR_ALLOC = -7        /* device or pinned host allocation failed */
+};
+
+/* Algorithm of the all-FP64 forms. */
+enum {
+  SFNL_ALGO_AUTO = 0, /* FAST when the grid dealiases, GRID otherwise */
+  SFNL_ALGO_GRID = 1, /* dense DFT on the caller's grid N (reproduces aliasing of short pads) */
+  SFNL_ALGO_FAST = 2  /* factored transforms on an internal alias-free grid */
+};
+
+/* Split-precision forms (tensor cores, FP32 accumulation, FP64 recombination). */
+enum {
+  SFNL_SPLIT_BF16X2 = 2, /* 2 bf16 slices, 3 slice products ("hi/lo") */
+  SFNL_SPLIT_BF16X3 = 3  /* 3 bf16 slices, 6 slice products */
+};
+
+/* ---------------------------------------------------------------------------
+ * FP64 forms, device pointers.
+ *   np        number of points (Gauss points or nodes), >= 0
+ *   m_max     number of Fourier modes held per point (all modes: one GPU)
+ *   m_max_pad zero-padding length; the grid has N = 2*m_max_pad-1 angles
+ *             (fft_parallel.F90:183); must be >= m_max
+ * ------------------------------------------------------------------------- */
+
+/* FFT_PAR_CROSS_PROD_DCL (fft_parallel.F90:147-328): v1, v2, out are (np, 6, m_max). */
+int sfnl_cross_f64(const double *v1, const double *v2, double *out, int64_t np, int m_max, int m_max_pad,
+                   sfnl_stream_t stream);
+/* FFT_PAR_DOT_PROD_DCL (fft_parallel.F90:330-500): v1, v2 (np, 6, m_max) -> out (np, 2, m_max). */
+int sfnl_dot_f64(const double *v1, const double *v2, double *out, int64_t np, int m_max, int m_max_pad,
+                 sfnl_stream_t stream);
+/* FFT_PAR_PROD_DCL (fft_parallel.F90:502-665): c1, c2, out are (np, 2, m_max). */
+int sfnl_prod_f64(const double *c1, const double *c2, double *out, int64_t np, int m_max, int m_max_pad,
+                  sfnl_stream_t stream);
+
+/* Same three products with an explicit algorithm and grid length.
+ * op: 0 cross, 1 dot, 2 prod.  n_theta = 0 selects N = 2*m_max_pad-1. */
+int sfnl_product_f64(int op, const double *a, const double *b, double *out, int64_t np, int m_max,
+                     int m_max_pad, int n_theta, int algo, sfnl_stream_t stream);
+
+/* The MHD nonlinear bundle in one launch, each term with the semantics of
+ * the reference routine that computes it today:
+ *   uxw   = u x w     (FFT_PAR_CROSS_PROD_DCL, subroutine_ns_with_velocity.F90:627 passes (RotV, W))
+ *   uxb   = u x b     (update_maxwell_with_B.F90:555)
+ *   jxb   = j x b     (subroutine_ns_with_velocity.F90:719, J = curl H)
+ *   ugradt= u . gradt (FFT_PAR_DOT_PROD_DCL, subroutine_temperature_with_T.F90:341)
+ * u, w, b, j, gradt, uxw, uxb, jxb: (np, 6, m_max); ugradt: (np, 2, m_max). */
+int sfnl_bundle_mhd_f64(const double *u, const double *w, const double *b, const double *j, const double *gradt,
+                        double *uxw, double *uxb, double *jxb, double *ugradt, int64_t np, int m_max,
+                        int m_max_pad, int algo, sfnl_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Linearised cross product N(u, w) = u x w about a base state (u, w).
+ * New capability: the reference's LightKrylov operator binds rmatvec to the
+ * forward map (LIGHTKRYLOV_OBJECTS/exponential_propagator.F90:61-62).
+ *   JVP  tan (np, 12, m, k): slots 0-5 = du, 6-11 = dw;  out (np, 6, m, k) = du x w + u x dw
+ *   VJP  cot (np, 6, m, k) -> out (np, 12, m, k) = J^T cot, the transpose for the
+ *        plain Euclidean inner product of the coefficient arrays, so that
+ *        <J v, c> = <v, J^T c> exactly in exact arithmetic.
+ * u, w: (np, 6, m) shared by all k_batch tangents.
+ * ------------------------------------------------------------------------- */
+int sfnl_cross_jvp_f64(const double *u, const double *w, const double *tan, double *out, int64_t np, int m_max,
+                       int m_max_pad, int k_batch, sfnl_stream_t stream);
+int sfnl_cross_vjp_f64(const double *u, const double *w, const double *cot, double *out, int64_t np, int m_max,
+                       int m_max_pad, int k_batch, sfnl_stream_t stream);
+
+/* Linearised pair (u x w, u x b) about (u, w, b), sharing u:
+ *   JVP  tan (np, 18, m, k) = (du, dw, db) -> out (np, 12, m, k) = (du x w + u x dw, du x b + u x db)
+ *   VJP  cot (np, 12, m, k) -> out (np, 18, m, k). */
+int sfnl_mhd_jvp_f64(const double *u, const double *w, const double *b, const double *tan, double *out, int64_t np,
+                     int m_max, int m_max_pad, int k_batch, sfnl_stream_t stream);
+int sfnl_mhd_vjp_f64(const double *u, const double *w, const double *b, const double *cot, double *out, int64_t np,
+                     int m_max, int m_max_pad, int k_batch, sfnl_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Split-precision forms: operands split into bf16 slices with a per-point
+ * power-of-two scale, DFT contractions on the tcgen05 tensor cores with FP32
+ * accumulation in TMEM, FP64 recombination, pointwise product and final
+ * truncation.  split = SFNL_SPLIT_BF16X2 or SFNL_SPLIT_BF16X3.
+ * ------------------------------------------------------------------------- */
+int sfnl_product_split(int op, const double *a, const double *b, double *out, int64_t np, int m_max, int m_max_pad,
+                       int split, sfnl_stream_t stream);
+int sfnl_bundle_mhd_split(const double *u, const double *w, const double *b, const double *j, const double *gradt,
+                          double *uxw, double *uxb, double *jxb, double *ugradt, int64_t np, int m_max,
+                          int m_max_pad, int split, sfnl_stream_t stream);
+int sfnl_mhd_jvp_split(const double *u, const double *w, const double *b, const double *tan, double *out,
+                       int64_t np, int m_max, int m_max_pad, int k_batch, int split, sfnl_stream_t stream);
+int sfnl_mhd_vjp_split(const double *u, const double *w, const double *b, const double *cot, double *out,
+                       int64_t np, int m_max, int m_max_pad, int k_batch, int split, sfnl_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Reference-signature entry points on HOST arrays, for the ISO_C_BINDING
+ * shim.  Arguments are those of fft_parallel.F90:147 / :330 / :502:
+ *   np, nb_field, m_max_c = SIZE(V1_in,1..3); nb_procs, bloc_size, m_max_pad as
+ *   passed by the caller; temps (may be NULL) = the optional REAL(8) temps(3):
+ *   zeroed, then temps[1] += seconds spent on the GPU (copies included).
+ * One GPU holds all modes, so nb_procs must be 1 (SFNL_ERR_UNSUPPORTED
+ * otherwise); bloc_size is checked (np <= nb_procs*bloc_size, the reference's
+ * buffer bound) and otherwise unused: there are no dummy points.
+ * ------------------------------------------------------------------------- */
+int sfnl_fft_par_cross_prod_dcl(const double *V1_in, const double *V2_in, double *V_out, int np, int nb_field,
+                                int m_max_c, int nb_procs, int bloc_size, int m_max_pad, double *temps);
+int sfnl_fft_par_dot_prod_dcl(const double *V1_in, const double *V2_in, double *c_out, int np, int nb_field,
+                              int m_max_c, int nb_procs, int bloc_size, int m_max_pad, double *temps);
+int sfnl_fft_par_prod_dcl(const double *c1_in, const double *c2_in, double *c_out, int np, int m_max_c,
+                          int nb_procs, int bloc_size, int m_max_pad, double *temps);
+
+/* Host-array variants of the device entry points (copy in, compute, copy out). */
+int sfnl_product_f64_host(int op, const double *a, const double *b, double *out, int64_t np, int m_max,
+                          int m_max_pad, int algo);
+int sfnl_bundle_mhd_host(const double *u, const double *w, const double *b, const double *j, const double *gradt,
+                         double *uxw, double *uxb, double *jxb, double *ugradt, int64_t np, int m_max,
+                         int m_max_pad, int form /* 0 = FP64, 2/3 = split */);
+
+/* ---------------------------------------------------------------------------
+ * Library state.
+ * ------------------------------------------------------------------------- */
+const char *sfnl_last_error(void); /* message of the last failing call on this thread */
+const char *sfnl_version(void);
+int sfnl_set_check_finite(int on); /* 1: scan outputs for NaN/Inf after each call (synchronises) */
+int sfnl_finalize(void);           /* release cached device tables and pinned staging buffers */
+/* Seconds spent in the last *_host call of this thread: [copy in, kernels, copy out]. */
+int sfnl_last_host_timing(double *seconds3);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SFEMANS_NL_H */

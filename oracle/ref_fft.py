@@ -1,0 +1,306 @@
+"""CPU oracle, Python side.  TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module: it is the checker for the CUDA path, never part of it.
+
+Three independent CPU formulations of the dealiased products of
+SOURCES/POST_PROCESSING/fft_parallel.F90 (FFT_PAR_CROSS_PROD_DCL :147-328,
+FFT_PAR_DOT_PROD_DCL :330-500, FFT_PAR_PROD_DCL :502-665):
+
+* ``c_oracle``   -- ctypes binding of oracle/sfnl_oracle.c, the step-by-step
+  long-double restatement of the reference (pack, emulated MPI_ALLTOALL,
+  c2r, product, r2c, 1/N, 2*CONJG, truncation, unpack).
+* ``fft_par``    -- the same algorithm with a library FFT (scipy.fft, i.e.
+  pocketfft, multithreaded) in place of FFTW: the FFTW-class CPU path that
+  bench.py times as the CPU baseline.
+* ``spectral_product`` -- the exact truncated product computed directly in
+  coefficient space (discrete convolution of the two Fourier series in long
+  double): no grid, no aliasing, no transform.
+
+Arrays follow the reference's Fortran layout: numpy arrays of shape
+(np, nslot, m) in Fortran (column-major) order, slot 2k holds the cosine and
+slot 2k+1 the sine coefficient of component k (0-based), mode n along the
+last axis.  The sine of mode 0 is ignored on input and 0 on output.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+OP_CROSS, OP_DOT, OP_PROD = 0, 1, 2
+_OPS = {"cross": OP_CROSS, "dot": OP_DOT, "prod": OP_PROD}
+
+
+# ----------------------------------------------------------------------------
+# synthetic inputs (SplitMix64 -> Box-Muller), shared by tests and bench
+# ----------------------------------------------------------------------------
+_M64 = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def _splitmix64(seed: int, count: int) -> np.ndarray:
+    """``count`` consecutive SplitMix64 outputs for state ``seed``."""
+    with np.errstate(over="ignore"):
+        idx = np.arange(1, count + 1, dtype=np.uint64)
+        z = np.uint64(seed) + idx * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return z
+
+
+def synthetic_field(npts: int, nslot: int, m: int, alpha: float, seed: int) -> np.ndarray:
+    """Fortran-ordered (npts, nslot, m) array: x[p,s,n] = z*exp(-alpha*n).
+
+    z ~ N(0,1) from SplitMix64 + Box-Muller in Fortran memory order; the sine
+    slot of mode 0 is set to 0 (the reference ignores it, fft_parallel.F90:241).
+    """
+    total = npts * nslot * m
+    pairs = (total + 1) // 2
+    bits = _splitmix64(seed, 2 * pairs)
+    u = ((bits >> np.uint64(11)).astype(np.float64) + 1.0) * (1.0 / 9007199254740992.0)
+    u1, u2 = u[0::2], u[1::2]
+    rad = np.sqrt(-2.0 * np.log(u1))
+    z = np.empty(2 * pairs)
+    z[0::2] = rad * np.cos(2.0 * np.pi * u2)
+    z[1::2] = rad * np.sin(2.0 * np.pi * u2)
+    x = z[:total].reshape((npts, nslot, m), order="F")
+    x = x * np.exp(-alpha * np.arange(m))[None, None, :]
+    x[:, 1::2, 0] = 0.0
+    return np.asfortranarray(x)
+
+
+# ----------------------------------------------------------------------------
+# C oracle (long double restatement of the reference)
+# ----------------------------------------------------------------------------
+def _lib():
+    global _LIB
+    if _LIB is None:
+        so = os.path.join(HERE, "_build", "libsfnl_oracle.so")
+        if not os.path.exists(so):
+            subprocess.check_call(["make", "-s", "-C", HERE])
+        lib = ctypes.CDLL(so)
+        P = ctypes.POINTER(ctypes.c_double)
+        for name in ("orc_fft_par_dcl",):
+            f = getattr(lib, name)
+            f.restype = ctypes.c_int
+            f.argtypes = [ctypes.c_int, P, P, P] + [ctypes.c_int] * 6
+        f = lib.orc_fft_par_dcl_n
+        f.restype = ctypes.c_int
+        f.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                      ctypes.POINTER(ctypes.c_double)] + [ctypes.c_int] * 7
+        _LIB = lib
+    return _LIB
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def c_oracle(op: str, V1, V2, m_max_pad: int, nb_procs: int = 1, bloc_size: int | None = None,
+             n_theta: int | None = None):
+    """Long-double restatement of FFT_PAR_*_DCL on global arrays.
+
+    ``V1``/``V2`` hold all m_max = m_max_c*nb_procs modes; rank r of the
+    emulated Fourier communicator owns modes [r*m_max_c, (r+1)*m_max_c).
+    ``bloc_size`` defaults to the callers' choice np/nb_procs+1
+    (subroutine_ns_with_velocity.F90:625).  Returns V_out (np, 6|2, m_max).
+    Raises ValueError with the oracle's status for inputs the reference rejects.
+    """
+    opc = _OPS[op]
+    V1 = np.asfortranarray(V1, dtype=np.float64)
+    V2 = np.asfortranarray(V2, dtype=np.float64)
+    npts, nf, m = V1.shape
+    if m % nb_procs:
+        raise ValueError("m_max must be a multiple of nb_procs")
+    if bloc_size is None:
+        bloc_size = npts // nb_procs + 1
+    nout = 6 if opc == OP_CROSS else 2
+    out = np.zeros((npts, nout, m), order="F")
+    N = 2 * m_max_pad - 1 if n_theta is None else n_theta
+    rc = _lib().orc_fft_par_dcl_n(opc, _ptr(V1), _ptr(V2), _ptr(out), npts, nf, m // nb_procs, nb_procs,
+                                  bloc_size, m_max_pad, N)
+    if rc != 0:
+        raise ValueError(f"oracle rejected arguments (status {rc})")
+    return out
+
+
+# ----------------------------------------------------------------------------
+# pocketfft restatement (FFTW-class CPU path; the timed CPU baseline)
+# ----------------------------------------------------------------------------
+def _to_complex(V, nfield):
+    """cu = 0.5*(a - i b), cu_0 = a_0 (fft_parallel.F90:234-241); V (np, 2*nfield, m)."""
+    a = V[:, 0::2, :]
+    b = V[:, 1::2, :]
+    cu = 0.5 * (a - 1j * b)
+    cu[:, :, 0] = a[:, :, 0]
+    return cu
+
+
+def _pointwise(op, ru):
+    if op == OP_CROSS:
+        r1, r2, r3, r4, r5, r6 = (ru[:, k, :] for k in range(6))
+        return np.stack([r2 * r6 - r3 * r5, r3 * r4 - r1 * r6, r1 * r5 - r2 * r4], axis=1)
+    if op == OP_DOT:
+        return (ru[:, 0] * ru[:, 3] + ru[:, 1] * ru[:, 4] + ru[:, 2] * ru[:, 5])[:, None, :]
+    return (ru[:, 0] * ru[:, 1])[:, None, :]
+
+
+def fft_par(op: str, V1, V2, m_max_pad: int, n_theta: int | None = None, workers: int = 1):
+    """pocketfft version of FFT_PAR_*_DCL for one rank holding all modes.
+
+    Same steps as the reference: half-complex pack with zero padding to
+    m_max_pad, c2r of length N = 2*m_max_pad-1 (unnormalised: N*irfft),
+    pointwise product, r2c, 1/N, 2*CONJG, truncation to m_max.
+    """
+    import scipy.fft as sfft
+
+    opc = _OPS[op]
+    npts, nf, m = V1.shape
+    N = 2 * m_max_pad - 1 if n_theta is None else n_theta
+    nh = N // 2 + 1
+    nin = nf // 2
+    cu = np.zeros((npts, 2 * nin, nh), dtype=np.complex128)
+    cu[:, :nin, :m] = _to_complex(V1, nin)
+    cu[:, nin:, :m] = _to_complex(V2, nin)
+    ru = sfft.irfft(cu, n=N, axis=2, norm="forward", workers=workers)  # unnormalised c2r
+    prod_ru = _pointwise(opc, ru)
+    pc = sfft.rfft(prod_ru, n=N, axis=2, norm="forward", workers=workers)  # includes 1/N
+    pc = pc[:, :, :m]
+    out = np.empty((npts, 2 * pc.shape[1], m), order="F")
+    out[:, 0::2, :] = 2.0 * pc.real
+    out[:, 1::2, :] = -2.0 * pc.imag
+    out[:, 0::2, 0] = pc[:, :, 0].real
+    out[:, 1::2, 0] = pc[:, :, 0].imag
+    return out
+
+
+# ----------------------------------------------------------------------------
+# exact spectral convolution (no grid)
+# ----------------------------------------------------------------------------
+def _full_spectrum(a, b):
+    """Complex coefficients F_n, n = -(m-1)..m-1, of f = sum a_n cos + b_n sin."""
+    m = a.shape[-1]
+    F = np.zeros(a.shape[:-1] + (2 * m - 1,), dtype=np.clongdouble)
+    c = 0.5 * (a.astype(np.longdouble) - 1j * b.astype(np.longdouble))
+    F[..., m - 1] = a[..., 0].astype(np.longdouble)
+    F[..., m:] = c[..., 1:]
+    F[..., : m - 1] = np.conj(c[..., 1:][..., ::-1])
+    return F
+
+
+def _scalar_product_coeffs(a1, b1, a2, b2):
+    """cos/sin coefficients (modes < m) of (f1*f2), exact convolution in long double."""
+    m = a1.shape[-1]
+    F1 = _full_spectrum(a1, b1)
+    F2 = _full_spectrum(a2, b2)
+    H = np.zeros(a1.shape[:-1] + (m,), dtype=np.clongdouble)
+    # H_k = sum_n F1_n F2_{k-n}, k = 0..m-1, n over -(m-1)..m-1
+    for k in range(m):
+        for n in range(-(m - 1), m):
+            q = k - n
+            if -(m - 1) <= q <= m - 1:
+                H[..., k] += F1[..., n + m - 1] * F2[..., q + m - 1]
+    a = 2.0 * H.real
+    b = -2.0 * H.imag
+    a[..., 0] = H[..., 0].real
+    b[..., 0] = 0.0
+    return a, b
+
+
+def spectral_product(op: str, V1, V2):
+    """Exact dealiased truncated product, no transform: (np, 6|2, m) float64."""
+    opc = _OPS[op]
+    npts, nf, m = V1.shape
+
+    def sp(f1, k1, f2, k2):
+        return _scalar_product_coeffs(f1[:, 2 * k1, :], f1[:, 2 * k1 + 1, :], f2[:, 2 * k2, :], f2[:, 2 * k2 + 1, :])
+
+    if opc == OP_CROSS:
+        comps = []
+        for (i, j) in ((1, 2), (2, 0), (0, 1)):  # out_r = v1_t v2_z - v1_z v2_t, ...
+            a1, b1 = sp(V1, i, V2, j)
+            a2, b2 = sp(V1, j, V2, i)
+            comps.append((a1 - a2, b1 - b2))
+    elif opc == OP_DOT:
+        a = b = 0
+        for k in range(3):
+            ak, bk = sp(V1, k, V2, k)
+            a, b = a + ak, b + bk
+        comps = [(a, b)]
+    else:
+        comps = [sp(V1, 0, V2, 0)]
+    out = np.empty((npts, 2 * len(comps), m), order="F")
+    for c, (a, b) in enumerate(comps):
+        out[:, 2 * c, :] = a.astype(np.float64)
+        out[:, 2 * c + 1, :] = b.astype(np.float64)
+    return out
+
+
+# ----------------------------------------------------------------------------
+# compositions used by the bundle / linearised forms
+# ----------------------------------------------------------------------------
+def mhd_bundle(u, w, b, j, gradT, m_max_pad, engine=None):
+    """(u x w, u x b, j x b, u . gradT) through the reference routines."""
+    f = engine or (lambda op, x, y: c_oracle(op, x, y, m_max_pad))
+    return f("cross", u, w), f("cross", u, b), f("cross", j, b), f("dot", u, gradT)
+
+
+def cross_jvp(u, w, du, dw, m_max_pad, engine=None):
+    """d(u x w) = du x w + u x dw (the cross product is bilinear, so exact)."""
+    f = engine or (lambda op, x, y: c_oracle(op, x, y, m_max_pad))
+    return f("cross", du, w) + f("cross", u, dw)
+
+
+def _grid(m, N):
+    th = 2.0 * np.pi * np.arange(N) / N
+    n = np.arange(m)
+    return np.cos(np.outer(n, th)), np.sin(np.outer(n, th))
+
+
+def cross_vjp(u, w, cot, N=None):
+    """Transpose of v=(du,dw) -> du x w + u x dw on the coefficient arrays.
+
+    J^T c = ( S^T[W x (S D c)],  S^T[(S D c) x U] ) with S the synthesis on an
+    alias-free grid, D = diag(1/N, 2/N, ...) the analysis scaling and
+    U = S u, W = S w.  Returns (np, 12, m).
+    """
+    npts, _, m = u.shape
+    if N is None:
+        N = 3 * m
+    C, S = _grid(m, N)
+
+    def synth(V, scale):
+        a = V[:, 0::2, :] * scale[None, None, :]
+        b = V[:, 1::2, :] * scale[None, None, :]
+        b = b.copy()
+        b[:, :, 0] = 0.0
+        return np.einsum("pkn,nj->pkj", a, C) + np.einsum("pkn,nj->pkj", b, S)
+
+    def synthT(G):
+        out = np.empty((npts, 2 * G.shape[1], m), order="F")
+        out[:, 0::2, :] = np.einsum("pkj,nj->pkn", G, C)
+        out[:, 1::2, :] = np.einsum("pkj,nj->pkn", G, S)
+        out[:, 1::2, 0] = 0.0
+        return out
+
+    one = np.ones(m)
+    dsc = np.full(m, 2.0 / N)
+    dsc[0] = 1.0 / N
+    U, W = synth(u, one), synth(w, one)
+    Cg = synth(cot, dsc)
+    gu = np.cross(W, Cg, axis=1)      # W x (S D c)
+    gw = np.cross(Cg, U, axis=1)      # (S D c) x U
+    return np.concatenate([synthT(gu), synthT(gw)], axis=1)
+
+
+def rel_l2(x, ref):
+    x = np.asarray(x, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    den = np.linalg.norm(ref)
+    return float(np.linalg.norm(x - ref) / (den if den > 0 else 1.0))

@@ -1,0 +1,24 @@
+/* sfnl_oracle.h -- CPU oracle (test infrastructure only; see sfnl_oracle.c). */
+#ifndef SFNL_ORACLE_H
+#define SFNL_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_CROSS = 0, ORC_DOT = 1, ORC_PROD = 2 };
+
+/* Restatement of FFT_PAR_{CROSS_PROD,DOT_PROD,PROD}_DCL (fft_parallel.F90:147-665).
+ * V1, V2: global arrays (np, nb_field, m_max_c*nb_procs), Fortran order; rank r
+ * owns modes [r*m_max_c, (r+1)*m_max_c).  Vout: (np, 6 | 2, m_max_c*nb_procs).
+ * Returns 0, or <0 for arguments the reference rejects or cannot handle. */
+int orc_fft_par_dcl(int op, const double *V1, const double *V2, double *Vout, int np, int nb_field,
+                    int m_max_c, int nb_procs, int bloc_size, int m_max_pad);
+/* Same with an explicit grid length N (the reference uses N = 2*m_max_pad-1). */
+int orc_fft_par_dcl_n(int op, const double *V1, const double *V2, double *Vout, int np, int nb_field,
+                      int m_max_c, int nb_procs, int bloc_size, int m_max_pad, int N);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,549 @@
+// sfnl_capi.cu -- the extern "C" boundary (include/sfemans_nl.h).
+//
+// Validates arguments the way the reference does (fft_parallel.F90:184-191:
+// nb_field even, m_max_c > 0; the buffers of :163-171 bound np by
+// nb_procs*bloc_size and the padded modes by m_max_pad), describes each call
+// as a program over scalar fields (sfnl_ops.cuh) and dispatches it to one of
+// the kernel families:
+//   GRID  sfnl_grid.cu   dense FP64 DFT on the caller's grid (any N)
+//   FAST  sfnl_fast.cu   FP64 factored transforms on an internal alias-free grid
+//   SPLIT sfnl_split.cu  bf16-sliced tcgen05 contractions, FP64 recombination
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/sfemans_nl.h"
+#include "sfnl_internal.h"
+#include "sfnl_ops.cuh"
+
+namespace sfnl {
+
+namespace {
+thread_local std::string g_err = "no error";
+thread_local double g_host_timing[3] = {0, 0, 0};
+int g_check_finite = 0;
+
+struct DevState {
+  int sms = 0;
+  int *d_flag = nullptr;
+  char *work = nullptr;
+  size_t work_bytes = 0;
+  std::mutex mu;
+};
+constexpr int kMaxDev = 64;
+DevState g_dev[kMaxDev];
+std::mutex g_dev_mu;
+
+DevState *dev_state() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDev) return nullptr;
+  return &g_dev[d];
+}
+}  // namespace
+
+int set_error(int code, const char *msg) {
+  g_err = msg;
+  return code;
+}
+
+int check_launch(const char *what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    return SFNL_ERR_CUDA;
+  }
+  return SFNL_OK;
+}
+
+int num_sms() {
+  DevState *s = dev_state();
+  if (!s) return 148;
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  if (s->sms == 0) {
+    int d = 0, v = 0;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d);
+    s->sms = v > 0 ? v : 148;
+  }
+  return s->sms;
+}
+
+namespace {
+
+__global__ void finite_scan(const double *p, int64_t n, int *flag) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (!isfinite(p[i])) {
+      *flag = 1;
+      return;
+    }
+}
+
+int scan_outputs(const ProgArgs &a, cudaStream_t st) {
+  DevState *s = dev_state();
+  if (!s) return set_error(SFNL_ERR_CUDA, "no current device");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (!s->d_flag && cudaMalloc(&s->d_flag, sizeof(int)) != cudaSuccess)
+    return set_error(SFNL_ERR_ALLOC, "cudaMalloc of the finite-check flag failed");
+  if (cudaMemsetAsync(s->d_flag, 0, sizeof(int), st) != cudaSuccess) return set_error(SFNL_ERR_CUDA, "memset failed");
+  const int no = op_nout(a.op);
+  for (int o = 0; o < no; ++o) {
+    // Each output field is a strided set of (cos,sin) rows; scan the span it covers.
+    for (int b = 0; b < a.batch; ++b)
+      for (int n = 0; n < a.m; ++n) {
+        const double *row = a.out[o] + (int64_t)b * a.out_bs[o] + (int64_t)n * a.out_ldm[o];
+        finite_scan<<<32, 256, 0, st>>>(row, 2 * a.np, s->d_flag);
+      }
+  }
+  int h = 0;
+  if (cudaMemcpyAsync(&h, s->d_flag, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return set_error(SFNL_ERR_CUDA, "finite check failed");
+  return h ? set_error(SFNL_ERR_NONFINITE, "non-finite value in the output") : SFNL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// argument checks shared by all forms
+// ---------------------------------------------------------------------------
+int check_common(int64_t np, int m, int pad, int n_theta, int k_batch, int *N_out) {
+  if (np < 0) return set_error(SFNL_ERR_ARG, "np < 0");
+  if (m < 1) return set_error(SFNL_ERR_ARG, "m_max < 1 (the reference stops on m_max_c==0)");
+  if (k_batch < 1 || k_batch > 65535) return set_error(SFNL_ERR_ARG, "k_batch outside [1, 65535]");
+  if (pad < m) return set_error(SFNL_ERR_ALIAS, "m_max_pad < m_max: the padded spectrum cannot hold the modes");
+  if (m > 4096 || pad > (1 << 20)) return set_error(SFNL_ERR_UNSUPPORTED, "m_max or m_max_pad beyond this build's limits");
+  const int N = n_theta > 0 ? n_theta : 2 * pad - 1;
+  if (m > N / 2 + 1) return set_error(SFNL_ERR_ALIAS, "grid shorter than 2*m_max-1 angles");
+  *N_out = N;
+  return SFNL_OK;
+}
+
+bool dealiased(int m, int N) { return N >= 3 * m - 2; }
+
+// Field of a Fortran array V(np, nslot, m[, k]): component k -> slots 2k, 2k+1.
+void set_in(ProgArgs &a, int f, const double *base, int64_t np, int nslot, int comp, int m, bool batched) {
+  a.in[f] = base + (int64_t)2 * comp * np;
+  a.in_ldm[f] = np * nslot;
+  a.in_bs[f] = batched ? np * nslot * (int64_t)m : 0;
+}
+void set_out(ProgArgs &a, int o, double *base, int64_t np, int nslot, int comp, int m, bool batched) {
+  a.out[o] = base + (int64_t)2 * comp * np;
+  a.out_ldm[o] = np * nslot;
+  a.out_bs[o] = batched ? np * nslot * (int64_t)m : 0;
+}
+
+ProgArgs make_args(int op, int64_t np, int m, int N, int batch) {
+  ProgArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.op = op;
+  a.np = np;
+  a.m = m;
+  a.N = N;
+  a.batch = batch;
+  return a;
+}
+
+int run_fp64(ProgArgs a, int algo, int N_caller, cudaStream_t st) {
+  const bool alias_free = dealiased(a.m, N_caller);
+  if (algo == SFNL_ALGO_AUTO) algo = (alias_free && fast_supported(a.op, a.m, fast_grid_length(a.m))) ? SFNL_ALGO_FAST : SFNL_ALGO_GRID;
+  int rc;
+  if (algo == SFNL_ALGO_GRID) {
+    a.N = N_caller;
+    rc = launch_grid(a, st);
+  } else if (algo == SFNL_ALGO_FAST) {
+    if (!alias_free) return set_error(SFNL_ERR_ALIAS, "FAST form needs a dealiasing pad (2*m_max_pad-1 >= 3*m_max-2)");
+    a.N = fast_grid_length(a.m);
+    if (!fast_supported(a.op, a.m, a.N)) return set_error(SFNL_ERR_UNSUPPORTED, "FAST form not built for this size");
+    rc = launch_fast(a, st);
+  } else {
+    return set_error(SFNL_ERR_ARG, "unknown algo");
+  }
+  if (rc == SFNL_OK && g_check_finite) rc = scan_outputs(a, st);
+  return rc;
+}
+
+int run_split(ProgArgs a, int split, int N_caller, cudaStream_t st) {
+  if (split != SFNL_SPLIT_BF16X2 && split != SFNL_SPLIT_BF16X3) return set_error(SFNL_ERR_ARG, "split must be 2 or 3");
+  if (!dealiased(a.m, N_caller)) return set_error(SFNL_ERR_ALIAS, "split forms need a dealiasing pad (2*m_max_pad-1 >= 3*m_max-2)");
+  if (!split_supported(a.op, a.m)) return set_error(SFNL_ERR_UNSUPPORTED, "split form not built for this program/size");
+  int rc = launch_split(a, split, st);
+  if (rc == SFNL_OK && g_check_finite) rc = scan_outputs(a, st);
+  return rc;
+}
+
+// Products of fft_parallel.F90: op 0 cross (6 slots), 1 dot (6 -> 2), 2 prod (2 -> 2).
+int build_product(int op, const double *x, const double *y, double *out, int64_t np, int m, int N, ProgArgs *pa) {
+  if (op < 0 || op > 2) return set_error(SFNL_ERR_ARG, "op must be 0 (cross), 1 (dot) or 2 (prod)");
+  if (np > 0 && (!x || !y || !out)) return set_error(SFNL_ERR_ARG, "null array");
+  ProgArgs a = make_args(op, np, m, N, 1);
+  if (op == OP_PROD) {
+    set_in(a, 0, x, np, 2, 0, m, false);
+    set_in(a, 1, y, np, 2, 0, m, false);
+    set_out(a, 0, out, np, 2, 0, m, false);
+  } else {
+    for (int k = 0; k < 3; ++k) {
+      set_in(a, k, x, np, 6, k, m, false);
+      set_in(a, 3 + k, y, np, 6, k, m, false);
+    }
+    if (op == OP_CROSS)
+      for (int k = 0; k < 3; ++k) set_out(a, k, out, np, 6, k, m, false);
+    else
+      set_out(a, 0, out, np, 2, 0, m, false);
+  }
+  *pa = a;
+  return SFNL_OK;
+}
+
+int build_bundle(const double *u, const double *w, const double *b, const double *j, const double *gt, double *uxw,
+                 double *uxb, double *jxb, double *ugt, int64_t np, int m, int N, ProgArgs *pa) {
+  if (np > 0 && (!u || !w || !b || !j || !gt || !uxw || !uxb || !jxb || !ugt)) return set_error(SFNL_ERR_ARG, "null array");
+  ProgArgs a = make_args(OP_BUNDLE, np, m, N, 1);
+  const double *ins[5] = {u, w, b, j, gt};
+  for (int v = 0; v < 5; ++v)
+    for (int k = 0; k < 3; ++k) set_in(a, 3 * v + k, ins[v], np, 6, k, m, false);
+  double *outs[3] = {uxw, uxb, jxb};
+  for (int v = 0; v < 3; ++v)
+    for (int k = 0; k < 3; ++k) set_out(a, 3 * v + k, outs[v], np, 6, k, m, false);
+  set_out(a, 9, ugt, np, 2, 0, m, false);
+  *pa = a;
+  return SFNL_OK;
+}
+
+// Linearised programs.  kind: 0 cross JVP, 1 cross VJP, 2 mhd JVP, 3 mhd VJP.
+int build_linear(int kind, const double *u, const double *w, const double *b, const double *x, double *out, int64_t np,
+                 int m, int N, int kb, ProgArgs *pa) {
+  if (np > 0 && (!u || !w || !x || !out || (kind >= 2 && !b))) return set_error(SFNL_ERR_ARG, "null array");
+  static const int ops[4] = {OP_CROSS_JVP, OP_CROSS_VJP, OP_MHD_JVP, OP_MHD_VJP};
+  ProgArgs a = make_args(ops[kind], np, m, N, kb);
+  const int nbase = kind >= 2 ? 3 : 2;
+  const double *base[3] = {u, w, b};
+  for (int v = 0; v < nbase; ++v)
+    for (int k = 0; k < 3; ++k) set_in(a, 3 * v + k, base[v], np, 6, k, m, false);
+  // batched input x: JVP tangents (6*nbase slots) or VJP cotangents (6*(nbase-1) slots)
+  const int nx = (kind == 0) ? 12 : (kind == 1) ? 6 : (kind == 2) ? 18 : 12;
+  const int ny = (kind == 0) ? 6 : (kind == 1) ? 12 : (kind == 2) ? 12 : 18;
+  for (int k = 0; k < nx / 2; ++k) set_in(a, 3 * nbase + k, x, np, nx, k, m, true);
+  for (int k = 0; k < ny / 2; ++k) set_out(a, k, out, np, ny, k, m, true);
+  *pa = a;
+  return SFNL_OK;
+}
+
+cudaStream_t as_stream(sfnl_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ---------------------------------------------------------------------------
+// host-array plumbing: grow-only device workspace per device
+// ---------------------------------------------------------------------------
+struct HostBuf {
+  const void *src;  // host input (copied in) or nullptr
+  void *dst;        // host output (copied out) or nullptr
+  size_t bytes;
+  double *dev;
+};
+
+int with_device_buffers(std::vector<HostBuf> &bufs, int (*run)(std::vector<HostBuf> &, void *, cudaStream_t),
+                        void *ctx, double *temps) {
+  using clk = std::chrono::steady_clock;
+  DevState *s = dev_state();
+  if (!s) return set_error(SFNL_ERR_CUDA, "no current CUDA device");
+  std::lock_guard<std::mutex> lk(s->mu);
+  size_t total = 0;
+  for (auto &b : bufs) total += (b.bytes + 255) & ~size_t(255);
+  if (total > s->work_bytes) {
+    if (s->work) cudaFree(s->work);
+    s->work = nullptr;
+    s->work_bytes = 0;
+    if (cudaMalloc(&s->work, total) != cudaSuccess) {
+      cudaGetLastError();
+      return set_error(SFNL_ERR_ALLOC, "cudaMalloc of the host-call workspace failed");
+    }
+    s->work_bytes = total;
+  }
+  size_t off = 0;
+  for (auto &b : bufs) {
+    b.dev = reinterpret_cast<double *>(s->work + off);
+    off += (b.bytes + 255) & ~size_t(255);
+  }
+  cudaStream_t st = cudaStreamPerThread;
+  auto t0 = clk::now();
+  for (auto &b : bufs)
+    if (b.src && b.bytes && cudaMemcpyAsync(b.dev, b.src, b.bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return set_error(SFNL_ERR_CUDA, "host-to-device copy failed");
+  if (cudaStreamSynchronize(st) != cudaSuccess) return set_error(SFNL_ERR_CUDA, "host-to-device copy failed");
+  auto t1 = clk::now();
+  int rc = run(bufs, ctx, st);
+  if (rc != SFNL_OK) return rc;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return set_error(SFNL_ERR_CUDA, "kernel execution failed");
+  auto t2 = clk::now();
+  for (auto &b : bufs)
+    if (b.dst && b.bytes && cudaMemcpyAsync(b.dst, b.dev, b.bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      return set_error(SFNL_ERR_CUDA, "device-to-host copy failed");
+  if (cudaStreamSynchronize(st) != cudaSuccess) return set_error(SFNL_ERR_CUDA, "device-to-host copy failed");
+  auto t3 = clk::now();
+  g_host_timing[0] = std::chrono::duration<double>(t1 - t0).count();
+  g_host_timing[1] = std::chrono::duration<double>(t2 - t1).count();
+  g_host_timing[2] = std::chrono::duration<double>(t3 - t2).count();
+  if (temps) {
+    temps[0] = g_host_timing[0] + g_host_timing[2];  // data movement (the reference's comm slot)
+    temps[1] = g_host_timing[1];                     // transforms + product
+    temps[2] = 0.0;                                  // no repacking
+  }
+  return SFNL_OK;
+}
+
+struct ProdCtx {
+  int op, m, pad, n_theta, algo;
+  int64_t np;
+};
+
+int run_prod_dev(std::vector<HostBuf> &b, void *vctx, cudaStream_t st) {
+  auto *c = static_cast<ProdCtx *>(vctx);
+  ProgArgs a;
+  int N = 0;
+  int rc = check_common(c->np, c->m, c->pad, c->n_theta, 1, &N);
+  if (rc) return rc;
+  rc = build_product(c->op, b[0].dev, b[1].dev, b[2].dev, c->np, c->m, N, &a);
+  if (rc) return rc;
+  return run_fp64(a, c->algo, N, st);
+}
+
+int host_product(int op, const double *x, const double *y, double *out, int64_t np, int m, int pad, int n_theta,
+                 int algo, double *temps) {
+  if (temps) temps[0] = temps[1] = temps[2] = 0.0;
+  int N = 0;
+  int rc = check_common(np, m, pad, n_theta, 1, &N);
+  if (rc) return rc;
+  if (op < 0 || op > 2) return set_error(SFNL_ERR_ARG, "op must be 0, 1 or 2");
+  if (np == 0) return SFNL_OK;
+  if (!x || !y || !out) return set_error(SFNL_ERR_ARG, "null array");
+  const int nsl_in = op == OP_PROD ? 2 : 6, nsl_out = op == OP_CROSS ? 6 : 2;
+  const size_t bin = sizeof(double) * (size_t)np * nsl_in * m, bout = sizeof(double) * (size_t)np * nsl_out * m;
+  std::vector<HostBuf> bufs = {{x, nullptr, bin, nullptr}, {y, nullptr, bin, nullptr}, {nullptr, out, bout, nullptr}};
+  ProdCtx c{op, m, pad, n_theta, algo, np};
+  return with_device_buffers(bufs, run_prod_dev, &c, temps);
+}
+
+int check_fortran_args(int np, int nb_field, int m_max_c, int nb_procs, int bloc_size, bool need6) {
+  if (np < 0 || m_max_c <= 0 || (nb_field % 2) != 0)
+    return set_error(SFNL_ERR_ARG, "BUG in FFT_PAR_*: MOD(nb_field,2)/=0 .OR. m_max_c==0");
+  if (need6 && nb_field != 6) return set_error(SFNL_ERR_SHAPE, "the cross/dot products need nb_field == 6");
+  if (nb_procs != 1) return set_error(SFNL_ERR_UNSUPPORTED, "one GPU holds all modes: nb_procs must be 1");
+  if (bloc_size < 1 || (int64_t)np > (int64_t)nb_procs * bloc_size)
+    return set_error(SFNL_ERR_SHAPE, "np > nb_procs*bloc_size");
+  return SFNL_OK;
+}
+
+struct BundleCtx {
+  int64_t np;
+  int m, pad, algo, form;
+};
+
+int run_bundle_dev(std::vector<HostBuf> &b, void *vctx, cudaStream_t st);
+
+}  // namespace
+}  // namespace sfnl
+
+using namespace sfnl;
+
+extern "C" {
+
+const char *sfnl_last_error(void) { return g_err.c_str(); }
+const char *sfnl_version(void) { return "sfemans_nl 0.1 (sm_100a)"; }
+int sfnl_set_check_finite(int on) {
+  g_check_finite = on ? 1 : 0;
+  return SFNL_OK;
+}
+int sfnl_last_host_timing(double *s3) {
+  if (!s3) return set_error(SFNL_ERR_ARG, "null pointer");
+  for (int i = 0; i < 3; ++i) s3[i] = g_host_timing[i];
+  return SFNL_OK;
+}
+
+int sfnl_finalize(void) {
+  for (int d = 0; d < kMaxDev; ++d) {
+    DevState &s = g_dev[d];
+    std::lock_guard<std::mutex> lk(s.mu);
+    if (!s.work && !s.d_flag) continue;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(d);
+    if (s.work) cudaFree(s.work);
+    if (s.d_flag) cudaFree(s.d_flag);
+    s.work = nullptr;
+    s.d_flag = nullptr;
+    s.work_bytes = 0;
+    cudaSetDevice(prev);
+  }
+  return SFNL_OK;
+}
+
+int sfnl_product_f64(int op, const double *a, const double *b, double *out, int64_t np, int m_max, int m_max_pad,
+                     int n_theta, int algo, sfnl_stream_t stream) {
+  int N = 0;
+  int rc = check_common(np, m_max, m_max_pad, n_theta, 1, &N);
+  if (rc) return rc;
+  ProgArgs pa;
+  rc = build_product(op, a, b, out, np, m_max, N, &pa);
+  if (rc) return rc;
+  if (np == 0) return SFNL_OK;
+  return run_fp64(pa, algo, N, as_stream(stream));
+}
+
+int sfnl_cross_f64(const double *v1, const double *v2, double *out, int64_t np, int m_max, int m_max_pad,
+                   sfnl_stream_t stream) {
+  return sfnl_product_f64(OP_CROSS, v1, v2, out, np, m_max, m_max_pad, 0, SFNL_ALGO_AUTO, stream);
+}
+int sfnl_dot_f64(const double *v1, const double *v2, double *out, int64_t np, int m_max, int m_max_pad,
+                 sfnl_stream_t stream) {
+  return sfnl_product_f64(OP_DOT, v1, v2, out, np, m_max, m_max_pad, 0, SFNL_ALGO_AUTO, stream);
+}
+int sfnl_prod_f64(const double *c1, const double *c2, double *out, int64_t np, int m_max, int m_max_pad,
+                  sfnl_stream_t stream) {
+  return sfnl_product_f64(OP_PROD, c1, c2, out, np, m_max, m_max_pad, 0, SFNL_ALGO_AUTO, stream);
+}
+
+int sfnl_bundle_mhd_f64(const double *u, const double *w, const double *b, const double *j, const double *gradt,
+                        double *uxw, double *uxb, double *jxb, double *ugradt, int64_t np, int m_max, int m_max_pad,
+                        int algo, sfnl_stream_t stream) {
+  int N = 0;
+  int rc = check_common(np, m_max, m_max_pad, 0, 1, &N);
+  if (rc) return rc;
+  ProgArgs pa;
+  rc = build_bundle(u, w, b, j, gradt, uxw, uxb, jxb, ugradt, np, m_max, N, &pa);
+  if (rc) return rc;
+  if (np == 0) return SFNL_OK;
+  return run_fp64(pa, algo, N, as_stream(stream));
+}
+
+static int linear_f64(int kind, const double *u, const double *w, const double *b, const double *x, double *out,
+                      int64_t np, int m, int pad, int kb, sfnl_stream_t stream) {
+  int N = 0;
+  int rc = check_common(np, m, pad, 0, kb, &N);
+  if (rc) return rc;
+  ProgArgs pa;
+  rc = build_linear(kind, u, w, b, x, out, np, m, N, kb, &pa);
+  if (rc) return rc;
+  if (np == 0) return SFNL_OK;
+  return run_fp64(pa, SFNL_ALGO_AUTO, N, as_stream(stream));
+}
+
+int sfnl_cross_jvp_f64(const double *u, const double *w, const double *tan, double *out, int64_t np, int m_max,
+                       int m_max_pad, int k_batch, sfnl_stream_t stream) {
+  return linear_f64(0, u, w, nullptr, tan, out, np, m_max, m_max_pad, k_batch, stream);
+}
+int sfnl_cross_vjp_f64(const double *u, const double *w, const double *cot, double *out, int64_t np, int m_max,
+                       int m_max_pad, int k_batch, sfnl_stream_t stream) {
+  return linear_f64(1, u, w, nullptr, cot, out, np, m_max, m_max_pad, k_batch, stream);
+}
+int sfnl_mhd_jvp_f64(const double *u, const double *w, const double *b, const double *tan, double *out, int64_t np,
+                     int m_max, int m_max_pad, int k_batch, sfnl_stream_t stream) {
+  return linear_f64(2, u, w, b, tan, out, np, m_max, m_max_pad, k_batch, stream);
+}
+int sfnl_mhd_vjp_f64(const double *u, const double *w, const double *b, const double *cot, double *out, int64_t np,
+                     int m_max, int m_max_pad, int k_batch, sfnl_stream_t stream) {
+  return linear_f64(3, u, w, b, cot, out, np, m_max, m_max_pad, k_batch, stream);
+}
+
+int sfnl_product_split(int op, const double *a, const double *b, double *out, int64_t np, int m_max, int m_max_pad,
+                       int split, sfnl_stream_t stream) {
+  int N = 0;
+  int rc = check_common(np, m_max, m_max_pad, 0, 1, &N);
+  if (rc) return rc;
+  ProgArgs pa;
+  rc = build_product(op, a, b, out, np, m_max, N, &pa);
+  if (rc) return rc;
+  if (np == 0) return SFNL_OK;
+  return run_split(pa, split, N, as_stream(stream));
+}
+
+int sfnl_bundle_mhd_split(const double *u, const double *w, const double *b, const double *j, const double *gradt,
+                          double *uxw, double *uxb, double *jxb, double *ugradt, int64_t np, int m_max, int m_max_pad,
+                          int split, sfnl_stream_t stream) {
+  int N = 0;
+  int rc = check_common(np, m_max, m_max_pad, 0, 1, &N);
+  if (rc) return rc;
+  ProgArgs pa;
+  rc = build_bundle(u, w, b, j, gradt, uxw, uxb, jxb, ugradt, np, m_max, N, &pa);
+  if (rc) return rc;
+  if (np == 0) return SFNL_OK;
+  return run_split(pa, split, N, as_stream(stream));
+}
+
+static int linear_split(int kind, const double *u, const double *w, const double *b, const double *x, double *out,
+                        int64_t np, int m, int pad, int kb, int split, sfnl_stream_t stream) {
+  int N = 0;
+  int rc = check_common(np, m, pad, 0, kb, &N);
+  if (rc) return rc;
+  ProgArgs pa;
+  rc = build_linear(kind, u, w, b, x, out, np, m, N, kb, &pa);
+  if (rc) return rc;
+  if (np == 0) return SFNL_OK;
+  return run_split(pa, split, N, as_stream(stream));
+}
+
+int sfnl_mhd_jvp_split(const double *u, const double *w, const double *b, const double *tan, double *out, int64_t np,
+                       int m_max, int m_max_pad, int k_batch, int split, sfnl_stream_t stream) {
+  return linear_split(2, u, w, b, tan, out, np, m_max, m_max_pad, k_batch, split, stream);
+}
+int sfnl_mhd_vjp_split(const double *u, const double *w, const double *b, const double *cot, double *out, int64_t np,
+                       int m_max, int m_max_pad, int k_batch, int split, sfnl_stream_t stream) {
+  return linear_split(3, u, w, b, cot, out, np, m_max, m_max_pad, k_batch, split, stream);
+}
+
+int sfnl_fft_par_cross_prod_dcl(const double *V1_in, const double *V2_in, double *V_out, int np, int nb_field,
+                                int m_max_c, int nb_procs, int bloc_size, int m_max_pad, double *temps) {
+  int rc = check_fortran_args(np, nb_field, m_max_c, nb_procs, bloc_size, true);
+  if (rc) return rc;
+  return host_product(OP_CROSS, V1_in, V2_in, V_out, np, m_max_c * nb_procs, m_max_pad, 0, SFNL_ALGO_AUTO, temps);
+}
+int sfnl_fft_par_dot_prod_dcl(const double *V1_in, const double *V2_in, double *c_out, int np, int nb_field,
+                              int m_max_c, int nb_procs, int bloc_size, int m_max_pad, double *temps) {
+  int rc = check_fortran_args(np, nb_field, m_max_c, nb_procs, bloc_size, true);
+  if (rc) return rc;
+  return host_product(OP_DOT, V1_in, V2_in, c_out, np, m_max_c * nb_procs, m_max_pad, 0, SFNL_ALGO_AUTO, temps);
+}
+int sfnl_fft_par_prod_dcl(const double *c1_in, const double *c2_in, double *c_out, int np, int m_max_c, int nb_procs,
+                          int bloc_size, int m_max_pad, double *temps) {
+  int rc = check_fortran_args(np, 2, m_max_c, nb_procs, bloc_size, false);
+  if (rc) return rc;
+  return host_product(OP_PROD, c1_in, c2_in, c_out, np, m_max_c * nb_procs, m_max_pad, 0, SFNL_ALGO_AUTO, temps);
+}
+
+int sfnl_product_f64_host(int op, const double *a, const double *b, double *out, int64_t np, int m_max, int m_max_pad,
+                          int algo) {
+  return host_product(op, a, b, out, np, m_max, m_max_pad, 0, algo, nullptr);
+}
+
+int sfnl_bundle_mhd_host(const double *u, const double *w, const double *b, const double *j, const double *gradt,
+                         double *uxw, double *uxb, double *jxb, double *ugradt, int64_t np, int m_max, int m_max_pad,
+                         int form) {
+  int N = 0;
+  int rc = check_common(np, m_max, m_max_pad, 0, 1, &N);
+  if (rc) return rc;
+  if (form != 0 && form != SFNL_SPLIT_BF16X2 && form != SFNL_SPLIT_BF16X3) return set_error(SFNL_ERR_ARG, "form must be 0, 2 or 3");
+  if (np == 0) return SFNL_OK;
+  if (!u || !w || !b || !j || !gradt || !uxw || !uxb || !jxb || !ugradt) return set_error(SFNL_ERR_ARG, "null array");
+  const size_t b6 = sizeof(double) * (size_t)np * 6 * m_max, b2 = sizeof(double) * (size_t)np * 2 * m_max;
+  std::vector<HostBuf> bufs = {{u, nullptr, b6, nullptr},    {w, nullptr, b6, nullptr},   {b, nullptr, b6, nullptr},
+                               {j, nullptr, b6, nullptr},    {gradt, nullptr, b6, nullptr}, {nullptr, uxw, b6, nullptr},
+                               {nullptr, uxb, b6, nullptr},  {nullptr, jxb, b6, nullptr}, {nullptr, ugradt, b2, nullptr}};
+  BundleCtx c{np, m_max, m_max_pad, SFNL_ALGO_AUTO, form};
+  return with_device_buffers(bufs, run_bundle_dev, &c, nullptr);
+}
+
+}  // extern "C"
+
+namespace sfnl {
+namespace {
+int run_bundle_dev(std::vector<HostBuf> &b, void *vctx, cudaStream_t st) {
+  auto *c = static_cast<BundleCtx *>(vctx);
+  if (c->form == 0)
+    return sfnl_bundle_mhd_f64(b[0].dev, b[1].dev, b[2].dev, b[3].dev, b[4].dev, b[5].dev, b[6].dev, b[7].dev,
+                               b[8].dev, c->np, c->m, c->pad, c->algo, st);
+  return sfnl_bundle_mhd_split(b[0].dev, b[1].dev, b[2].dev, b[3].dev, b[4].dev, b[5].dev, b[6].dev, b[7].dev,
+                               b[8].dev, c->np, c->m, c->pad, c->form, st);
+}
+}  // namespace
+}  // namespace sfnl

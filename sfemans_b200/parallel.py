@@ -1,0 +1,84 @@
+"""Multi-rank plumbing around the single-GPU kernels.
+
+Two decompositions, one process per GPU:
+
+* Point sharding (the default, :func:`shard_range`): every point of the
+  nonlinear term is independent (the transforms run along the azimuth of
+  each point), so G GPUs each take a contiguous range of points and no data
+  crosses NVLink.  bench.py runs this as weak scaling.
+
+* The reference's mode-distributed layout (:func:`fft_par_distributed`):
+  each rank owns m_max_c contiguous Fourier modes of every point
+  (initialization.F90:823-835) and FFT_PAR_*_DCL transposes mode <-> point
+  with two MPI_ALLTOALLs (fft_parallel.F90:217, :306).  Here the same two
+  exchanges are ``torch.distributed.all_to_all_single`` calls (NCCL over
+  NVLink on GPUs, gloo in the CPU tests), and the per-rank product on
+  bloc_size points with all modes is the single-GPU kernel.  Dummy points
+  beyond np are zero (the reference fills them with 1.d100, :211; they are
+  dropped on output either way).
+"""
+from __future__ import annotations
+
+
+def shard_range(npts: int, rank: int, world: int) -> tuple[int, int]:
+    """Contiguous [start, stop) of the points rank ``rank`` of ``world`` owns."""
+    if world < 1 or not (0 <= rank < world):
+        raise ValueError("bad rank/world")
+    base, rem = divmod(npts, world)
+    start = rank * base + min(rank, rem)
+    return start, start + base + (1 if rank < rem else 0)
+
+
+def _default_compute(kind, x, y, m_max_pad):
+    from . import OP_CROSS, OP_DOT, OP_PROD, product
+
+    op = {"cross": OP_CROSS, "dot": OP_DOT, "prod": OP_PROD}[kind]
+    return product(op, x, y, m_max_pad=m_max_pad)
+
+
+def fft_par_distributed(kind, group, x, y, out, nb_procs, bloc_size, m_max_pad, temps=None, compute=None):
+    """FFT_PAR_{CROSS_PROD,DOT_PROD,PROD}_DCL over a mode-distributed communicator.
+
+    x, y: this rank's (np, nslot, m_max_c) tensors (Fortran layout); out:
+    (np, 6|2, m_max_c).  ``compute(kind, xb, yb, m_max_pad)`` maps the
+    gathered (bloc_size, nslot, m_max) blocks to (bloc_size, nout, m_max);
+    it defaults to the CUDA kernels.
+    """
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    if world != nb_procs:
+        raise ValueError("nb_procs must equal the communicator size")
+    npts, nsl, mc = x.shape
+    np_tot = nb_procs * bloc_size
+    if npts > np_tot:
+        raise ValueError("np > nb_procs*bloc_size")
+    compute = compute or _default_compute
+    nout = out.shape[1]
+
+    def to_blocks(t, ns):
+        # (np, ns, mc) -> send buffer [dest q][mode i][slot s][point n], points padded to np_tot.
+        tp = torch.zeros((np_tot, ns, mc), dtype=t.dtype, device=t.device)
+        tp[:npts] = t
+        return tp.reshape(nb_procs, bloc_size, ns, mc).permute(0, 3, 2, 1).contiguous()
+
+    send = torch.cat([to_blocks(x, nsl), to_blocks(y, nsl)], dim=2)          # (P, mc, 2ns, bloc)
+    recv = torch.empty_like(send)
+    dist.all_to_all_single(recv.view(-1), send.view(-1), group=group)       # fft_parallel.F90:217
+    # recv[r] = source rank r's modes for my points -> (bloc, ns, m_max) Fortran layout with
+    # global mode r*mc + i (the shiftl bookkeeping of :223-231).
+    full = recv.permute(3, 2, 0, 1).reshape(bloc_size, 2 * nsl, nb_procs * mc)
+    xb = full[:, :nsl, :].contiguous().permute(2, 1, 0).contiguous().permute(2, 1, 0)
+    yb = full[:, nsl:, :].contiguous().permute(2, 1, 0).contiguous().permute(2, 1, 0)
+    pb = compute(kind, xb, yb, m_max_pad)                                     # (bloc, nout, m_max)
+    # send back modes [q*mc, (q+1)*mc) of my points to rank q (:306)
+    back = pb.reshape(bloc_size, nout, nb_procs, mc).permute(2, 3, 1, 0).contiguous()  # (P, mc, nout, bloc)
+    got = torch.empty_like(back)
+    dist.all_to_all_single(got.view(-1), back.view(-1), group=group)
+    # got[q] = my modes for rank q's points -> (np_tot, nout, mc), drop dummies (:311-324)
+    res = got.permute(0, 3, 2, 1).reshape(np_tot, nout, mc)[:npts]
+    out.copy_(res)
+    if temps is not None:
+        temps[:] = 0.0
+    return out

@@ -1,0 +1,54 @@
+"""Generate the golden fixtures under tests/golden/ from the CPU oracle.
+
+    python tests/golden/make_golden.py
+
+Each case stores the seeded inputs and the long-double oracle's output
+(oracle/sfnl_oracle.c, the step-by-step restatement of
+SOURCES/POST_PROCESSING/fft_parallel.F90:147-665).  Cases are small so that
+the fixtures stay a few hundred KB in total.  The exact spectral
+convolution (oracle/ref_fft.py) is checked against every case before it is
+written, so a fixture is only produced when two independent formulations
+agree to 1e-15.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import ref_fft as R  # noqa: E402
+
+# name, op, np, m, m_max_pad, nb_procs, alpha, seed
+CASES = [
+    ("cross_np37_m5", "cross", 37, 5, 7, 1, 0.3, 11),
+    ("dot_np37_m5", "dot", 37, 5, 7, 1, 0.3, 12),
+    ("prod_np37_m5", "prod", 37, 5, 7, 1, 0.3, 13),
+    ("cross_np64_m16", "cross", 64, 16, 24, 1, 0.3, 14),   # the 3/2-rule pad of the 28k-point case
+    ("cross_np29_m6_p3", "cross", 29, 6, 9, 3, 0.2, 15),   # 3 Fourier ranks, dummy points
+    ("dot_np29_m6_p2", "dot", 29, 6, 9, 2, 0.2, 16),
+    ("prod_np33_m7", "prod", 33, 7, 10, 1, 0.1, 17),       # m odd: N = 3m-2, the alias-free limit
+    ("cross_np1_m3", "cross", 1, 3, 4, 1, 0.5, 18),        # single point
+    ("cross_np40_m1", "cross", 40, 1, 1, 1, 0.0, 19),      # mode 0 only, N = 1
+    ("dot_np70_m32", "dot", 70, 32, 48, 1, 0.05, 20),      # slow decay
+]
+
+
+def make(case):
+    name, op, npts, m, pad, procs, alpha, seed = case
+    nsl = 2 if op == "prod" else 6
+    V1 = R.synthetic_field(npts, nsl, m, alpha, 1000 + seed)
+    V2 = R.synthetic_field(npts, nsl, m, alpha, 2000 + seed)
+    out = R.c_oracle(op, V1, V2, pad, nb_procs=procs)
+    ex = R.spectral_product(op, V1, V2)
+    err = R.rel_l2(out, ex)
+    assert err < 1e-15, (name, err)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), V1=V1, V2=V2, out=out,
+                        meta=np.array([npts, m, pad, procs], dtype=np.int64), op=np.array(op))
+    return name, err
+
+
+if __name__ == "__main__":
+    for c in CASES:
+        print(*make(c))

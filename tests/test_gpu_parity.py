@@ -1,0 +1,216 @@
+"""GPU parity of the all-FP64 forms against the CPU oracle.
+
+Bar (north star): rel-L2 <= 1e-12 per output array against the long-double
+restatement of fft_parallel.F90 (FP64_TOL below).  Every call goes through
+the C-ABI library (ctypes), on device tensors or on host arrays.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import sfemans_b200 as sf
+from oracle import ref_fft as R
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+ALGOS = [sf.ALGO_GRID, sf.ALGO_AUTO]
+
+
+def dev(a):
+    return sf.to_device(a)
+
+
+def host(t):
+    return sf.to_host(t)
+
+
+def _sync():
+    import torch
+
+    torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLD, "*.npz"))))
+@pytest.mark.parametrize("algo", ALGOS)
+def test_golden_fixtures(path, algo):
+    z = np.load(path)
+    npts, m, pad, procs = (int(v) for v in z["meta"])
+    op = {"cross": 0, "dot": 1, "prod": 2}[str(z["op"])]
+    out = sf.product(op, dev(z["V1"]), dev(z["V2"]), m_max_pad=pad, algo=algo)
+    _sync()
+    assert R.rel_l2(host(out), z["out"]) <= FP64_TOL
+
+
+CASES = [  # np, m, m_max_pad
+    (1, 1, 1), (5, 2, 3), (33, 5, 7), (257, 16, 24), (130, 13, 19), (1000, 32, 48), (77, 64, 96),
+]
+
+
+@pytest.mark.parametrize("op", [0, 1, 2])
+@pytest.mark.parametrize("npts,m,pad", CASES)
+@pytest.mark.parametrize("algo", ALGOS)
+def test_products_match_oracle(op, npts, m, pad, algo):
+    name = ("cross", "dot", "prod")[op]
+    nsl = 2 if op == 2 else 6
+    V1 = R.synthetic_field(npts, nsl, m, 0.2, 100 + m)
+    V2 = R.synthetic_field(npts, nsl, m, 0.2, 200 + m)
+    ref = R.c_oracle(name, V1, V2, pad)
+    out = sf.product(op, dev(V1), dev(V2), m_max_pad=pad, algo=algo)
+    _sync()
+    assert R.rel_l2(host(out), ref) <= FP64_TOL
+
+
+@pytest.mark.parametrize("npts,m,pad,n_theta", [(64, 16, 24, 48), (50, 7, 10, 22), (40, 8, 8, 0)])
+def test_grid_form_follows_the_grid(npts, m, pad, n_theta):
+    # GRID on an explicit grid, including the aliasing pad m_max_pad = m_max.
+    V1 = R.synthetic_field(npts, 6, m, 0.0, 1)
+    V2 = R.synthetic_field(npts, 6, m, 0.0, 2)
+    ref = R.c_oracle("cross", V1, V2, pad, n_theta=n_theta or None)
+    out = sf.product(0, dev(V1), dev(V2), m_max_pad=pad, n_theta=n_theta, algo=sf.ALGO_GRID)
+    _sync()
+    assert R.rel_l2(host(out), ref) <= FP64_TOL
+
+
+def test_fast_form_refuses_aliasing_pad():
+    V = dev(R.synthetic_field(10, 6, 8, 0.1, 1))
+    with pytest.raises(sf.SfnlError) as e:
+        sf.product(0, V, V, m_max_pad=8, algo=sf.ALGO_FAST)
+    assert e.value.code == -3
+
+
+@pytest.mark.parametrize("kind", ["cross", "dot", "prod"])
+def test_reference_signature_on_host_arrays(kind):
+    m, npts = 12, 301
+    nsl = 2 if kind == "prod" else 6
+    V1 = R.synthetic_field(npts, nsl, m, 0.3, 11)
+    V2 = R.synthetic_field(npts, nsl, m, 0.3, 12)
+    out = np.zeros((npts, 6 if kind == "cross" else 2, m), order="F")
+    temps = np.full(3, 7.0)
+    fn = {"cross": sf.FFT_PAR_CROSS_PROD_DCL, "dot": sf.FFT_PAR_DOT_PROD_DCL, "prod": sf.FFT_PAR_PROD_DCL}[kind]
+    bloc = npts + 1  # the callers' bloc_size = np/nb_procs+1
+    fn(None, V1, V2, out, 1, bloc, 3 * m // 2, temps)
+    assert R.rel_l2(out, R.c_oracle(kind, V1, V2, 3 * m // 2)) <= FP64_TOL
+    assert temps[1] > 0 and temps[2] == 0.0
+
+
+def test_reference_signature_on_device_tensors():
+    m, npts = 8, 100
+    V1 = R.synthetic_field(npts, 6, m, 0.3, 13)
+    V2 = R.synthetic_field(npts, 6, m, 0.3, 14)
+    out = sf.fortran_empty(npts, 6, m)
+    sf.FFT_PAR_CROSS_PROD_DCL(None, dev(V1), dev(V2), out, 1, npts + 1, 12)
+    _sync()
+    assert R.rel_l2(host(out), R.c_oracle("cross", V1, V2, 12)) <= FP64_TOL
+
+
+@pytest.mark.parametrize("npts,m", [(200, 8), (65, 21)])
+@pytest.mark.parametrize("algo", ALGOS)
+def test_mhd_bundle(npts, m, algo):
+    pad = 3 * m // 2
+    f = [R.synthetic_field(npts, 6, m, 0.1, 300 + i) for i in range(5)]
+    refs = R.mhd_bundle(*f, pad)
+    outs = sf.bundle_mhd(*[dev(x) for x in f], m_max_pad=pad, algo=algo)
+    _sync()
+    for o, r in zip(outs, refs):
+        assert R.rel_l2(host(o), r) <= FP64_TOL
+
+
+def test_host_bundle_entry_point():
+    import ctypes
+
+    npts, m = 90, 10
+    pad = 15
+    f = [R.synthetic_field(npts, 6, m, 0.1, 400 + i) for i in range(5)]
+    outs = [np.zeros((npts, 6, m), order="F") for _ in range(3)] + [np.zeros((npts, 2, m), order="F")]
+    P = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+    rc = sf.lib().sfnl_bundle_mhd_host(*[P(a) for a in f + outs], npts, m, pad, 0)
+    assert rc == 0, sf.last_error()
+    for o, r in zip(outs, R.mhd_bundle(*f, pad)):
+        assert R.rel_l2(o, r) <= FP64_TOL
+
+
+def _batched(npts, nslot, m, k, alpha, seed):
+    x = np.empty((npts, nslot, m, k), order="F")
+    for t in range(k):
+        x[:, :, :, t] = R.synthetic_field(npts, nslot, m, alpha, seed + t)
+    return x
+
+
+@pytest.mark.parametrize("npts,m,k", [(120, 8, 3), (33, 17, 1)])
+def test_cross_jvp_matches_linearisation(npts, m, k):
+    pad = 3 * m // 2
+    u = R.synthetic_field(npts, 6, m, 0.2, 1)
+    w = R.synthetic_field(npts, 6, m, 0.2, 2)
+    tan = _batched(npts, 12, m, k, 0.2, 10)
+    out = host(sf.cross_jvp(dev(u), dev(w), dev(tan), m_max_pad=pad))
+    for t in range(k):
+        du = np.asfortranarray(tan[:, :6, :, t])
+        dw = np.asfortranarray(tan[:, 6:, :, t])
+        assert R.rel_l2(out[:, :, :, t], R.cross_jvp(u, w, du, dw, pad)) <= FP64_TOL
+
+
+def test_cross_jvp_central_finite_differences():
+    # N(u + h du, w + h dw) - N(u - h du, w - h dw) = 2h J(du, dw) exactly for a
+    # bilinear N; the check bounds rounding at ~eps/h (h = 1e-6).
+    npts, m, h = 700, 32, 1e-6
+    pad = 48
+    u = R.synthetic_field(npts, 6, m, 0.2, 21)
+    w = R.synthetic_field(npts, 6, m, 0.2, 22)
+    du = R.synthetic_field(npts, 6, m, 0.2, 23)
+    dw = R.synthetic_field(npts, 6, m, 0.2, 24)
+    tan = np.asfortranarray(np.concatenate([du, dw], axis=1))
+    jv = host(sf.cross_jvp(dev(u), dev(w), dev(tan), m_max_pad=pad))[..., 0]
+    plus = host(sf.product(0, dev(u + h * du), dev(w + h * dw), m_max_pad=pad))
+    minus = host(sf.product(0, dev(u - h * du), dev(w - h * dw), m_max_pad=pad))
+    fd = (plus - minus) / (2 * h)
+    assert R.rel_l2(jv, fd) < 1e-8
+
+
+@pytest.mark.parametrize("npts,m,k", [(150, 8, 2), (40, 32, 1)])
+def test_cross_vjp_dot_product_identity(npts, m, k):
+    pad = 3 * m // 2
+    u = R.synthetic_field(npts, 6, m, 0.2, 31)
+    w = R.synthetic_field(npts, 6, m, 0.2, 32)
+    v = _batched(npts, 12, m, k, 0.2, 40)
+    c = _batched(npts, 6, m, k, 0.2, 50)
+    jv = host(sf.cross_jvp(dev(u), dev(w), dev(v), m_max_pad=pad))
+    jtc = host(sf.cross_vjp(dev(u), dev(w), dev(c), m_max_pad=pad))
+    for t in range(k):
+        lhs = np.dot(jv[..., t].ravel(), c[..., t].ravel())
+        rhs = np.dot(v[..., t].ravel(), jtc[..., t].ravel())
+        assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), np.linalg.norm(jv[..., t]) * np.linalg.norm(c[..., t]))
+        assert R.rel_l2(jtc[..., t], R.cross_vjp(u, w, np.asfortranarray(c[..., t]))) <= FP64_TOL
+
+
+def test_mhd_jvp_vjp():
+    npts, m, k = 90, 12, 2
+    pad = 18
+    u, w, b = (R.synthetic_field(npts, 6, m, 0.2, 60 + i) for i in range(3))
+    v = _batched(npts, 18, m, k, 0.2, 70)
+    c = _batched(npts, 12, m, k, 0.2, 80)
+    jv = host(sf.mhd_jvp(dev(u), dev(w), dev(b), dev(v), m_max_pad=pad))
+    jtc = host(sf.mhd_vjp(dev(u), dev(w), dev(b), dev(c), m_max_pad=pad))
+    for t in range(k):
+        du, dw, db = (np.asfortranarray(v[:, 6 * i:6 * i + 6, :, t]) for i in range(3))
+        assert R.rel_l2(jv[:, :6, :, t], R.cross_jvp(u, w, du, dw, pad)) <= FP64_TOL
+        assert R.rel_l2(jv[:, 6:, :, t], R.cross_jvp(u, b, du, db, pad)) <= FP64_TOL
+        lhs = np.dot(jv[..., t].ravel(), c[..., t].ravel())
+        rhs = np.dot(v[..., t].ravel(), jtc[..., t].ravel())
+        assert abs(lhs - rhs) <= 1e-12 * np.linalg.norm(jv[..., t]) * np.linalg.norm(c[..., t])
+
+
+def test_finite_check_mode():
+    V1 = R.synthetic_field(64, 6, 4, 0.1, 1)
+    V1[3, 2, 1] = np.nan
+    V2 = R.synthetic_field(64, 6, 4, 0.1, 2)
+    sf.set_check_finite(True)
+    try:
+        with pytest.raises(sf.SfnlError) as e:
+            sf.product(0, dev(V1), dev(V2), m_max_pad=6)
+        assert e.value.code == -6
+    finally:
+        sf.set_check_finite(False)

@@ -1,0 +1,144 @@
+"""The CPU oracle, pinned before it is trusted.
+
+The reference ships no array-level golden vectors for FFT_PAR_*_DCL; its
+only known answers that isolate the product arithmetic are the manufactured
+nonlinear sources of the regression tests (REGRESSION_SUITE/TEST1/
+LOCAL_SOURCES/condlim.F90:140-210: mode-1 fields whose product lands on
+modes 0 and 2 by the rule (a cos + b sin)(c cos + d sin) = (ac+bd)/2 +
+(ac-bd)/2 cos 2t + (ad+bc)/2 sin 2t).  The oracle is pinned by that
+identity, by two independent formulations (pocketfft and an exact spectral
+convolution with no grid), and by the committed fixtures.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from oracle import ref_fft as R
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _mode1_fields(npts, m, seed):
+    rng = np.random.default_rng(seed)
+    V = np.zeros((npts, 6, m), order="F")
+    V[:, :, 1] = rng.standard_normal((npts, 6))
+    return V
+
+
+@pytest.mark.parametrize("nb_procs", [1, 3])
+def test_mode1_product_identity(nb_procs):
+    # TEST1 runs m_max = 3 on 3 Fourier ranks (REGRESSION_TESTS/data); u and
+    # curl u are pure mode-1 fields.
+    m = 3
+    U = _mode1_fields(17, m, 1)
+    W = _mode1_fields(17, m, 2)
+    out = R.c_oracle("cross", U, W, 3 * m // 2, nb_procs=nb_procs)
+    c = lambda V, k: V[:, 2 * k, 1]  # noqa: E731
+    s = lambda V, k: V[:, 2 * k + 1, 1]  # noqa: E731
+
+    def prod_rule(f, k1, g, k2):
+        a, b, cc, d = c(f, k1), s(f, k1), c(g, k2), s(g, k2)
+        return (a * cc + b * d) / 2, (a * cc - b * d) / 2, (a * d + b * cc) / 2
+
+    for comp, (i, j) in enumerate(((1, 2), (2, 0), (0, 1))):
+        p = prod_rule(U, i, W, j)
+        q = prod_rule(W, i, U, j)  # the second term of the cross product, u_j w_i
+        mean, c2, s2 = (p[t] - q[t] for t in range(3))
+        np.testing.assert_allclose(out[:, 2 * comp, 0], mean, rtol=0, atol=1e-14)
+        np.testing.assert_allclose(out[:, 2 * comp, 2], c2, rtol=0, atol=1e-14)
+        np.testing.assert_allclose(out[:, 2 * comp + 1, 2], s2, rtol=0, atol=1e-14)
+        np.testing.assert_allclose(out[:, 2 * comp + 1, 0], 0.0, atol=0)
+        np.testing.assert_allclose(out[:, 2 * comp:2 * comp + 2, 1], 0.0, atol=1e-14)
+
+
+@pytest.mark.parametrize("op", ["cross", "dot", "prod"])
+@pytest.mark.parametrize("npts,m,pad", [(23, 4, 6), (9, 9, 13), (31, 16, 24)])
+def test_three_formulations_agree(op, npts, m, pad):
+    nsl = 2 if op == "prod" else 6
+    V1 = R.synthetic_field(npts, nsl, m, 0.2, 5)
+    V2 = R.synthetic_field(npts, nsl, m, 0.2, 6)
+    ref = R.c_oracle(op, V1, V2, pad)
+    assert R.rel_l2(R.spectral_product(op, V1, V2), ref) < 1e-15
+    assert R.rel_l2(R.fft_par(op, V1, V2, pad), ref) < 1e-14
+    # The even grid N = 2*m_max_pad also dealiases: same truncated product.
+    assert R.rel_l2(R.c_oracle(op, V1, V2, pad, n_theta=2 * pad), ref) < 1e-15
+
+
+def test_nb_procs_emulation_is_layout_only():
+    V1 = R.synthetic_field(29, 6, 6, 0.3, 7)
+    V2 = R.synthetic_field(29, 6, 6, 0.3, 8)
+    ref = R.c_oracle("cross", V1, V2, 9)
+    for P in (2, 3, 6):
+        np.testing.assert_array_equal(R.c_oracle("cross", V1, V2, 9, nb_procs=P), ref)
+    # bloc_size larger than needed only adds dummy points
+    np.testing.assert_array_equal(R.c_oracle("cross", V1, V2, 9, nb_procs=3, bloc_size=15), ref)
+
+
+def test_short_pad_aliases():
+    # m_max_pad = m_max: the grid is too short and the reference's result is aliased.
+    V1 = R.synthetic_field(13, 6, 8, 0.0, 9)
+    V2 = R.synthetic_field(13, 6, 8, 0.0, 10)
+    ali = R.c_oracle("cross", V1, V2, 8)
+    exact = R.spectral_product("cross", V1, V2)
+    assert R.rel_l2(ali, exact) > 1e-3
+    assert R.rel_l2(R.fft_par("cross", V1, V2, 8), ali) < 1e-14
+
+
+def test_oracle_rejects_what_the_reference_cannot_do():
+    V = R.synthetic_field(10, 6, 4, 0.1, 1)
+    with pytest.raises(ValueError):
+        R.c_oracle("cross", V, V, 3)                   # m_max_pad < m_max
+    with pytest.raises(ValueError):
+        R.c_oracle("cross", V, V, 6, nb_procs=2, bloc_size=4)  # np > nb_procs*bloc_size
+    W = R.synthetic_field(10, 4, 4, 0.1, 1)
+    with pytest.raises(ValueError):
+        R.c_oracle("cross", W, W, 6)                   # nb_field != 6
+
+
+def test_sine_of_mode_zero_is_ignored():
+    V1 = R.synthetic_field(11, 6, 5, 0.2, 3)
+    V2 = R.synthetic_field(11, 6, 5, 0.2, 4)
+    ref = R.c_oracle("cross", V1, V2, 7)
+    V1b = V1.copy(order="F")
+    V1b[:, 1::2, 0] = 123.0
+    np.testing.assert_array_equal(R.c_oracle("cross", V1b, V2, 7), ref)
+    assert np.all(ref[:, 1::2, 0] == 0.0) or np.abs(ref[:, 1::2, 0]).max() < 1e-15
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLD, "*.npz"))))
+def test_golden_fixtures_reproduce(path):
+    z = np.load(path)
+    npts, m, pad, procs = (int(v) for v in z["meta"])
+    op = str(z["op"])
+    out = R.c_oracle(op, z["V1"], z["V2"], pad, nb_procs=procs)
+    np.testing.assert_array_equal(out, z["out"])
+    assert R.rel_l2(R.spectral_product(op, z["V1"], z["V2"]), z["out"]) < 1e-15
+
+
+def test_synthetic_generator_shape_and_decay():
+    x = R.synthetic_field(1000, 6, 8, 0.3, 42)
+    assert x.flags.f_contiguous and x.shape == (1000, 6, 8)
+    assert np.all(x[:, 1::2, 0] == 0.0)
+    s = np.sqrt((x[:, 0::2, :] ** 2).mean(axis=(0, 1)))
+    np.testing.assert_allclose(s / s[0], np.exp(-0.3 * np.arange(8)), rtol=0.1)
+    np.testing.assert_array_equal(x, R.synthetic_field(1000, 6, 8, 0.3, 42))
+
+
+def test_vjp_restatement_is_the_transpose():
+    # Build J explicitly on a tiny case and compare J^T c with cross_vjp.
+    npts, m = 2, 3
+    u = R.synthetic_field(npts, 6, m, 0.0, 1)
+    w = R.synthetic_field(npts, 6, m, 0.0, 2)
+    cot = R.synthetic_field(npts, 6, m, 0.0, 3)
+    pad = 3 * m // 2
+    nin = npts * 12 * m
+    J = np.zeros((npts * 6 * m, nin))
+    for i in range(nin):
+        e = np.zeros(nin)
+        e[i] = 1.0
+        v = e.reshape((npts, 12, m), order="F")
+        J[:, i] = R.cross_jvp(u, w, np.asfortranarray(v[:, :6]), np.asfortranarray(v[:, 6:]), pad).reshape(-1, order="F")
+    jt = (J.T @ cot.reshape(-1, order="F")).reshape((npts, 12, m), order="F")
+    np.testing.assert_allclose(R.cross_vjp(u, w, cot), jt, rtol=0, atol=1e-13)
