@@ -1,8 +1,447 @@
-// sfnl_fast.cu -- FP64 factored transforms on an internal alias-free grid (placeholder).
+// sfnl_fast.cu -- all-FP64 products on an internal alias-free grid (SFNL_ALGO_FAST).
+//
+// When the caller's pad dealiases (2*m_max_pad-1 >= 3*m_max-2, which every
+// SFEMaNS caller satisfies with m_max_pad = 3*m_max/2), the reference's result
+// is the exact truncated product (fft_parallel.F90:147-665 with N = 2*m_pad-1)
+// and does not depend on the grid.  This form evaluates it on a grid chosen
+// for the hardware: N = 4Q angles theta_j = pi(2j+1)/N, Q a multiple of 8
+// with 4Q >= 3m-2.
+//
+// Transforms.  The two symmetry levels of a real Fourier series on that grid
+// are folded out exactly (the first two radix-2 stages of a real FFT, which
+// need no twiddles): with CE/CO the cosine sums over even/odd modes and SE/SO
+// the sine sums, evaluated at the Q angles of the first quadrant,
+//   f(t)      = CE+CO+SE+SO      f(pi-t)  = CE-CO-SE+SO
+//   f(pi+t)   = CE-CO+SE-SO      f(2pi-t) = CE+CO-SE-SO,
+// and the analysis folds the products g1..g4 at those four angles into
+//   PE = g1+g2+g3+g4 (even cos)  PO = g1-g2-g3+g4 (odd cos)
+//   QE = g1-g2+g3-g4 (even sin)  QO = g1+g2-g3-g4 (odd sin).
+// What remains are eight small dense contractions per field (K = m/2 modes x
+// Q angles each way), a quarter of the dense DFT, run on the FP64 tensor cores
+// (mma.sync m8n8k4 f64).  The product and both folds happen in registers on
+// the accumulator fragments: lane (g, q) of a warp holds point g and angles
+// 2q, 2q+1 of an 8-angle tile for every field and class, so the product needs
+// no data exchange, and the analysis takes each k-step's A fragment straight
+// from the element the same lane produced (the angle order inside a k-step is
+// chosen to make that true).
+//
+// Parallel decomposition: one CTA per 8-point tile; warp w owns quarter-angle
+// tiles t = w, w+NW, ... in the synthesis (the CTA's warps read the tile's
+// coefficients together, so L1 serves all but the first read), the folded
+// products go through shared memory in fragment order, then warp w owns output
+// mode tiles in the analysis.  Elementary programs are cross (6 -> 3), dot
+// (6 -> 1) and product (2 -> 1); the bundle and the linearised programs are
+// sequences of elementary launches on one stream (with accumulation).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
+
 #include "sfnl_internal.h"
 #include "sfnl_ops.cuh"
+
 namespace sfnl {
-int fast_grid_length(int m) { return 3 * m; }
-bool fast_supported(int, int, int) { return false; }
-int launch_fast(const ProgArgs &, cudaStream_t) { return set_error(SFNL_ERR_UNSUPPORTED, "FAST form not built"); }
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// geometry of the folded transforms
+// ---------------------------------------------------------------------------
+struct Geo {
+  int m, Q, N;   // modes, quarter angles, grid length
+  int NT;        // quarter-angle tiles of 8
+  int ke[4];     // modes per class (0 cos-even, 1 cos-odd, 2 sin-even, 3 sin-odd)
+  int KS[4];     // synthesis k-steps per class (modes padded to 4)
+  int NU[4];     // analysis output tiles per class (modes padded to 8)
+  int ks_off[4]; // prefix offsets
+  int nu_off[4];
+  int KS_tot, NU_tot;
+};
+
+Geo make_geo(int m) {
+  Geo g;
+  g.m = m;
+  int qmin = (3 * m - 2 + 3) / 4;
+  if (qmin < 1) qmin = 1;
+  g.Q = ((qmin + 7) / 8) * 8;
+  g.N = 4 * g.Q;
+  g.NT = g.Q / 8;
+  const int ev = (m + 1) / 2, od = m / 2;
+  const int cnt[4] = {ev, od, ev, od};
+  g.KS_tot = g.NU_tot = 0;
+  for (int c = 0; c < 4; ++c) {
+    g.ke[c] = cnt[c];
+    g.KS[c] = (cnt[c] + 3) / 4;
+    g.NU[c] = (cnt[c] + 7) / 8;
+    g.ks_off[c] = g.KS_tot;
+    g.nu_off[c] = g.NU_tot;
+    g.KS_tot += g.KS[c];
+    g.NU_tot += g.NU[c];
+  }
+  return g;
+}
+
+__host__ __device__ inline int class_mode(int c, int k) { return 2 * k + (c & 1); }
+
+// Device tables for one m: synthesis B fragments and two analysis variants.
+struct Tables {
+  double *syn = nullptr;   // [KS_tot][NT][32]
+  double *ana = nullptr;   // [2 variants][NU_tot][NT][2][32]
+};
+
+std::mutex g_tab_mu;
+std::map<std::pair<int, int>, Tables> g_tabs;  // (device, m) -> tables
+
+int get_tables(const Geo &g, Tables *out) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_tab_mu);
+  auto it = g_tabs.find({dev, g.m});
+  if (it != g_tabs.end()) {
+    *out = it->second;
+    return SFNL_OK;
+  }
+  const long double pi = acosl(-1.0L);
+  auto ang = [&](int j) { return pi * (long double)(2 * j + 1) / (long double)g.N; };
+  std::vector<double> syn((size_t)g.KS_tot * g.NT * 32, 0.0);
+  for (int c = 0; c < 4; ++c)
+    for (int s = 0; s < g.KS[c]; ++s)
+      for (int t = 0; t < g.NT; ++t)
+        for (int l = 0; l < 32; ++l) {
+          const int k = 4 * s + (l & 3), j = 8 * t + (l >> 2);
+          double v = 0.0;
+          if (k < g.ke[c]) {
+            const int n = class_mode(c, k);
+            const long double x = (long double)n * ang(j);
+            v = (double)(c < 2 ? cosl(x) : sinl(x));
+          }
+          syn[(((size_t)(g.ks_off[c] + s)) * g.NT + t) * 32 + l] = v;
+        }
+  std::vector<double> ana((size_t)2 * g.NU_tot * g.NT * 2 * 32, 0.0);
+  for (int var = 0; var < 2; ++var)
+    for (int c = 0; c < 4; ++c)
+      for (int u = 0; u < g.NU[c]; ++u)
+        for (int t = 0; t < g.NT; ++t)
+          for (int e = 0; e < 2; ++e)
+            for (int l = 0; l < 32; ++l) {
+              const int j = 8 * t + 2 * (l & 3) + e;  // angle of k-value (l & 3) in k-step (t, e)
+              const int kk = 8 * u + (l >> 2);         // output column inside the class
+              double v = 0.0;
+              if (kk < g.ke[c]) {
+                const int n = class_mode(c, kk);
+                const long double x = (long double)n * ang(j);
+                const long double w = var == 1 ? 1.0L : (n == 0 ? 1.0L : 2.0L) / (long double)g.N;
+                v = (double)(w * (c < 2 ? cosl(x) : sinl(x)));
+              }
+              ana[((((size_t)var * g.NU_tot + g.nu_off[c] + u) * g.NT + t) * 2 + e) * 32 + l] = v;
+            }
+  Tables T;
+  if (cudaMalloc(&T.syn, syn.size() * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&T.ana, ana.size() * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(SFNL_ERR_ALLOC, "cudaMalloc of the DFT tables failed");
+  }
+  if (cudaMemcpy(T.syn, syn.data(), syn.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(T.ana, ana.data(), ana.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    return set_error(SFNL_ERR_CUDA, "upload of the DFT tables failed");
+  g_tabs[{dev, g.m}] = T;
+  *out = T;
+  return SFNL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// kernel
+// ---------------------------------------------------------------------------
+enum { EK_CROSS = 0, EK_DOT = 1, EK_PROD = 2 };
+
+struct FastArgs {
+  const double *in[6];
+  double *out[3];
+  int64_t in_ldm[6], out_ldm[3], in_bs[6], out_bs[3];
+  int64_t np;
+  int m, N, NT;
+  int ks_off[4], KS[4], nu_off[4], NU[4], ke[4];
+  int NU_tot;
+  unsigned adj_in;  // bit f: input field f is a cotangent (synthesise with D)
+  int adj_out;      // 1: analyse without D (transpose of the synthesis)
+  int accumulate;   // 1: out += result
+  const double *syn, *ana;
+};
+
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+template <int EK>
+struct EKDef;
+template <>
+struct EKDef<EK_CROSS> {
+  static constexpr int NI = 6, NO = 3;
+  __device__ static void op(const double *x, double *y) { cross3(x, x + 3, y); }
+};
+template <>
+struct EKDef<EK_DOT> {
+  static constexpr int NI = 6, NO = 1;
+  __device__ static void op(const double *x, double *y) { y[0] = x[0] * x[3] + x[1] * x[4] + x[2] * x[5]; }
+};
+template <>
+struct EKDef<EK_PROD> {
+  static constexpr int NI = 2, NO = 1;
+  __device__ static void op(const double *x, double *y) { y[0] = x[0] * x[1]; }
+};
+
+template <int EK>
+__global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
+  constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO;
+  extern __shared__ double ps[];  // [NO][4][NT][2][32]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, NW = blockDim.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int64_t p = (int64_t)blockIdx.x * 8 + g;
+  const bool valid = p < a.np;
+  const int b = blockIdx.y;
+  const int NT = a.NT;
+  const double invN = 1.0 / a.N, twoN = 2.0 / a.N;
+
+  const double *src[NI];
+#pragma unroll
+  for (int f = 0; f < NI; ++f) src[f] = a.in[f] + (int64_t)b * a.in_bs[f] + (valid ? p : 0);
+
+  // ---- synthesis, fold, program, analysis pre-fold ----
+  for (int t = warp; t < NT; t += NW) {
+    double acc[NI][4][2];
+#pragma unroll
+    for (int f = 0; f < NI; ++f)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[f][c][0] = acc[f][c][1] = 0.0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const double *bt = a.syn + ((size_t)a.ks_off[c] * NT + t) * 32 + lane;
+      for (int s = 0; s < a.KS[c]; ++s) {
+        const int k = 4 * s + q;
+        const int n = class_mode(c, k);
+        const bool live = valid && k < a.ke[c] && !(c == 2 && n == 0);  // sine of mode 0 ignored
+        const int64_t off = (c >= 2 ? a.np : 0);
+        const double bv = __ldg(bt + (size_t)s * NT * 32);
+        double av[NI];
+#pragma unroll
+        for (int f = 0; f < NI; ++f) {
+          av[f] = live ? __ldg(src[f] + off + (int64_t)n * a.in_ldm[f]) : 0.0;
+          if (a.adj_in & (1u << f)) av[f] *= (n == 0 ? invN : twoN);
+        }
+#pragma unroll
+        for (int f = 0; f < NI; ++f) dmma(acc[f][c], av[f], bv);
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      double v[4][NI];
+#pragma unroll
+      for (int f = 0; f < NI; ++f) {
+        const double A = acc[f][0][e] + acc[f][1][e], B = acc[f][0][e] - acc[f][1][e];
+        const double C = acc[f][2][e] + acc[f][3][e], D = acc[f][3][e] - acc[f][2][e];
+        v[0][f] = A + C;  // theta
+        v[1][f] = B + D;  // pi - theta
+        v[2][f] = B - D;  // pi + theta
+        v[3][f] = A - C;  // 2 pi - theta
+      }
+      double gq[4][NO];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) EKDef<EK>::op(v[r], gq[r]);
+#pragma unroll
+      for (int o = 0; o < NO; ++o) {
+        const double s14 = gq[0][o] + gq[3][o], d14 = gq[0][o] - gq[3][o];
+        const double s23 = gq[1][o] + gq[2][o], d32 = gq[2][o] - gq[1][o];
+        double *dst = ps + ((size_t)((o * 4) * NT + t) * 2 + e) * 32 + lane;
+        const size_t cstride = (size_t)NT * 2 * 32;
+        dst[0] = s14 + s23;            // PE
+        dst[cstride] = s14 - s23;      // PO
+        dst[2 * cstride] = d14 + d32;  // QE
+        dst[3 * cstride] = d14 - d32;  // QO
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- analysis: output tiles (class c, tile u) ----
+  const double *anav = a.ana + (size_t)(a.adj_out ? 1 : 0) * a.NU_tot * NT * 2 * 32;
+  for (int cu = warp; cu < a.NU_tot; cu += NW) {
+    int c = 0;
+    while (c < 3 && cu >= a.nu_off[c + 1]) ++c;
+    const int u = cu - a.nu_off[c];
+    double y[NO][2];
+#pragma unroll
+    for (int o = 0; o < NO; ++o) y[o][0] = y[o][1] = 0.0;
+    const double *bt = anav + (size_t)cu * NT * 2 * 32 + lane;
+    for (int te = 0; te < 2 * NT; ++te) {
+      const double bv = __ldg(bt + (size_t)te * 32);
+#pragma unroll
+      for (int o = 0; o < NO; ++o) {
+        const double av = ps[((size_t)(o * 4 + c) * NT * 2 + te) * 32 + lane];
+        dmma(y[o], av, bv);
+      }
+    }
+    if (!valid) continue;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int kk = 8 * u + 2 * q + i;
+      if (kk >= a.ke[c]) continue;
+      const int n = class_mode(c, kk);
+#pragma unroll
+      for (int o = 0; o < NO; ++o) {
+        double *dst = a.out[o] + (int64_t)b * a.out_bs[o] + p + (int64_t)n * a.out_ldm[o] + (c >= 2 ? a.np : 0);
+        const double v = (c == 2 && n == 0) ? 0.0 : y[o][i];
+        if (a.accumulate)
+          *dst += v;
+        else
+          *dst = v;
+      }
+    }
+  }
+}
+
+template <int EK>
+int launch_ek(FastArgs &fa, int batch, cudaStream_t st) {
+  constexpr int NO = EKDef<EK>::NO;
+  const size_t smem = sizeof(double) * (size_t)NO * 4 * fa.NT * 2 * 32;
+  if (smem > 200 * 1024) return set_error(SFNL_ERR_UNSUPPORTED, "FAST form: m too large for shared memory");
+  int nw = fa.NT < 8 ? fa.NT : 8;
+  if (nw < 2) nw = 2;
+  auto kern = fast_kernel<EK>;
+  if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (fast form)");
+  const int64_t tiles = (fa.np + 7) / 8;
+  if (tiles > 0x7fffffff) return set_error(SFNL_ERR_UNSUPPORTED, "np too large");
+  dim3 grid((unsigned)tiles, (unsigned)batch);
+  kern<<<grid, nw * 32, smem, st>>>(fa);
+  return check_launch("fast form");
+}
+
+struct Elem {
+  int ek;
+  int in[6];      // field indices into ProgArgs.in
+  int out[3];     // indices into ProgArgs.out
+  unsigned adj;   // adjoint-input mask over the 6 (or 2) operands
+  int acc;
+};
+
+}  // namespace
+
+int fast_grid_length(int m) { return make_geo(m).N; }
+
+bool fast_supported(int op, int m, int N) {
+  (void)op;
+  if (m < 1 || m > 512) return false;
+  const Geo g = make_geo(m);
+  return g.N == N && (size_t)3 * 4 * g.NT * 2 * 32 * sizeof(double) <= 200 * 1024;
+}
+
+int launch_fast(const ProgArgs &a, cudaStream_t st) {
+  if (a.np == 0) return SFNL_OK;
+  const Geo g = make_geo(a.m);
+  if (g.N != a.N) return set_error(SFNL_ERR_ARG, "FAST form: unexpected grid length");
+  Tables T;
+  int rc = get_tables(g, &T);
+  if (rc) return rc;
+  std::vector<Elem> seq;
+  auto X = [](int a0, int a1, int a2, int b0, int b1, int b2) { return std::vector<int>{a0, a1, a2, b0, b1, b2}; };
+  auto add = [&](int ek, std::vector<int> in, std::vector<int> out, unsigned adj, int acc) {
+    Elem e{};
+    e.ek = ek;
+    for (size_t i = 0; i < in.size(); ++i) e.in[i] = in[i];
+    for (size_t i = 0; i < out.size(); ++i) e.out[i] = out[i];
+    e.adj = adj;
+    e.acc = acc;
+    seq.push_back(e);
+  };
+  const unsigned A1 = 0x38u, A0 = 0x07u;  // cotangent as second / first operand
+  switch (a.op) {
+    case OP_CROSS: add(EK_CROSS, X(0, 1, 2, 3, 4, 5), {0, 1, 2}, 0, 0); break;
+    case OP_DOT: add(EK_DOT, X(0, 1, 2, 3, 4, 5), {0}, 0, 0); break;
+    case OP_PROD: add(EK_PROD, {0, 1}, {0}, 0, 0); break;
+    case OP_BUNDLE:
+      add(EK_CROSS, X(0, 1, 2, 3, 4, 5), {0, 1, 2}, 0, 0);     // u x w
+      add(EK_CROSS, X(0, 1, 2, 6, 7, 8), {3, 4, 5}, 0, 0);     // u x b
+      add(EK_CROSS, X(9, 10, 11, 6, 7, 8), {6, 7, 8}, 0, 0);   // j x b
+      add(EK_DOT, X(0, 1, 2, 12, 13, 14), {9}, 0, 0);          // u . gradT
+      break;
+    case OP_CROSS_JVP:  // [u, w, du, dw]
+      add(EK_CROSS, X(6, 7, 8, 3, 4, 5), {0, 1, 2}, 0, 0);     // du x w
+      add(EK_CROSS, X(0, 1, 2, 9, 10, 11), {0, 1, 2}, 0, 1);   // + u x dw
+      break;
+    case OP_CROSS_VJP:  // [u, w, c]
+      add(EK_CROSS, X(3, 4, 5, 6, 7, 8), {0, 1, 2}, A1, 0);    // w x c
+      add(EK_CROSS, X(6, 7, 8, 0, 1, 2), {3, 4, 5}, A0, 0);    // c x u
+      break;
+    case OP_MHD_JVP:  // [u, w, b, du, dw, db]
+      add(EK_CROSS, X(9, 10, 11, 3, 4, 5), {0, 1, 2}, 0, 0);   // du x w
+      add(EK_CROSS, X(0, 1, 2, 12, 13, 14), {0, 1, 2}, 0, 1);  // + u x dw
+      add(EK_CROSS, X(9, 10, 11, 6, 7, 8), {3, 4, 5}, 0, 0);   // du x b
+      add(EK_CROSS, X(0, 1, 2, 15, 16, 17), {3, 4, 5}, 0, 1);  // + u x db
+      break;
+    case OP_MHD_VJP:  // [u, w, b, c1, c2]
+      add(EK_CROSS, X(3, 4, 5, 9, 10, 11), {0, 1, 2}, A1, 0);  // w x c1
+      add(EK_CROSS, X(6, 7, 8, 12, 13, 14), {0, 1, 2}, A1, 1); // + b x c2
+      add(EK_CROSS, X(9, 10, 11, 0, 1, 2), {3, 4, 5}, A0, 0);  // c1 x u
+      add(EK_CROSS, X(12, 13, 14, 0, 1, 2), {6, 7, 8}, A0, 0); // c2 x u
+      break;
+    default: return set_error(SFNL_ERR_ARG, "unknown program");
+  }
+  const bool adj_out = op_adjoint_out(a.op);
+  for (const Elem &e : seq) {
+    FastArgs fa;
+    std::memset(&fa, 0, sizeof(fa));
+    const int ni = e.ek == EK_PROD ? 2 : 6, no = e.ek == EK_CROSS ? 3 : 1;
+    for (int i = 0; i < ni; ++i) {
+      fa.in[i] = a.in[e.in[i]];
+      fa.in_ldm[i] = a.in_ldm[e.in[i]];
+      fa.in_bs[i] = a.in_bs[e.in[i]];
+    }
+    for (int o = 0; o < no; ++o) {
+      fa.out[o] = a.out[e.out[o]];
+      fa.out_ldm[o] = a.out_ldm[e.out[o]];
+      fa.out_bs[o] = a.out_bs[e.out[o]];
+    }
+    fa.np = a.np;
+    fa.m = g.m;
+    fa.N = g.N;
+    fa.NT = g.NT;
+    for (int c = 0; c < 4; ++c) {
+      fa.ks_off[c] = g.ks_off[c];
+      fa.KS[c] = g.KS[c];
+      fa.nu_off[c] = g.nu_off[c];
+      fa.NU[c] = g.NU[c];
+      fa.ke[c] = g.ke[c];
+    }
+    fa.NU_tot = g.NU_tot;
+    fa.adj_in = e.adj;
+    fa.adj_out = adj_out ? 1 : 0;
+    fa.accumulate = e.acc;
+    fa.syn = T.syn;
+    fa.ana = T.ana;
+    int r = e.ek == EK_CROSS ? launch_ek<EK_CROSS>(fa, a.batch, st)
+          : e.ek == EK_DOT   ? launch_ek<EK_DOT>(fa, a.batch, st)
+                             : launch_ek<EK_PROD>(fa, a.batch, st);
+    if (r) return r;
+  }
+  return SFNL_OK;
+}
+
+void fast_release_tables() {
+  std::lock_guard<std::mutex> lk(g_tab_mu);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  for (auto &kv : g_tabs) {
+    cudaSetDevice(kv.first.first);
+    cudaFree(kv.second.syn);
+    cudaFree(kv.second.ana);
+  }
+  g_tabs.clear();
+  cudaSetDevice(prev);
+}
+
 }  // namespace sfnl

@@ -23,6 +23,7 @@ int launch_grid(const ProgArgs &a, cudaStream_t st);   // sfnl_grid.cu
 int launch_fast(const ProgArgs &a, cudaStream_t st);   // sfnl_fast.cu
 bool fast_supported(int op, int m, int N_int);          // sfnl_fast.cu
 int fast_grid_length(int m);                            // sfnl_fast.cu
+void fast_release_tables();                             // sfnl_fast.cu
 int launch_split(const ProgArgs &a, int split, cudaStream_t st);  // sfnl_split.cu
 bool split_supported(int op, int m);                    // sfnl_split.cu
 
