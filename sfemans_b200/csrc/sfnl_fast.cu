@@ -155,8 +155,6 @@ int get_tables(const Geo &g, Tables *out) {
 // ---------------------------------------------------------------------------
 // kernel
 // ---------------------------------------------------------------------------
-enum { EK_CROSS = 0, EK_DOT = 1, EK_PROD = 2 };
-
 struct FastArgs {
   const double *in[6];
   double *out[3];
@@ -321,15 +319,56 @@ int launch_ek(FastArgs &fa, int batch, cudaStream_t st) {
   return check_launch("fast form");
 }
 
-struct Elem {
-  int ek;
-  int in[6];      // field indices into ProgArgs.in
-  int out[3];     // indices into ProgArgs.out
-  unsigned adj;   // adjoint-input mask over the 6 (or 2) operands
-  int acc;
-};
-
 }  // namespace
+
+int decompose_program(int op, std::vector<Elem> &seq) {
+  seq.clear();
+  auto add = [&](int ek, std::initializer_list<int> in, std::initializer_list<int> out, unsigned adj, int acc) {
+    Elem e{};
+    e.ek = ek;
+    int i = 0;
+    for (int v : in) e.in[i++] = v;
+    i = 0;
+    for (int v : out) e.out[i++] = v;
+    e.adj = adj;
+    e.acc = acc;
+    seq.push_back(e);
+  };
+  const unsigned A1 = 0x38u, A0 = 0x07u;  // cotangent as second / first operand
+  switch (op) {
+    case OP_CROSS: add(EK_CROSS, {0, 1, 2, 3, 4, 5}, {0, 1, 2}, 0, 0); break;
+    case OP_DOT: add(EK_DOT, {0, 1, 2, 3, 4, 5}, {0}, 0, 0); break;
+    case OP_PROD: add(EK_PROD, {0, 1}, {0}, 0, 0); break;
+    case OP_BUNDLE:
+      add(EK_CROSS, {0, 1, 2, 3, 4, 5}, {0, 1, 2}, 0, 0);     // u x w
+      add(EK_CROSS, {0, 1, 2, 6, 7, 8}, {3, 4, 5}, 0, 0);     // u x b
+      add(EK_CROSS, {9, 10, 11, 6, 7, 8}, {6, 7, 8}, 0, 0);   // j x b
+      add(EK_DOT, {0, 1, 2, 12, 13, 14}, {9}, 0, 0);          // u . gradT
+      break;
+    case OP_CROSS_JVP:  // [u, w, du, dw]
+      add(EK_CROSS, {6, 7, 8, 3, 4, 5}, {0, 1, 2}, 0, 0);     // du x w
+      add(EK_CROSS, {0, 1, 2, 9, 10, 11}, {0, 1, 2}, 0, 1);   // + u x dw
+      break;
+    case OP_CROSS_VJP:  // [u, w, c]
+      add(EK_CROSS, {3, 4, 5, 6, 7, 8}, {0, 1, 2}, A1, 0);    // w x c
+      add(EK_CROSS, {6, 7, 8, 0, 1, 2}, {3, 4, 5}, A0, 0);    // c x u
+      break;
+    case OP_MHD_JVP:  // [u, w, b, du, dw, db]
+      add(EK_CROSS, {9, 10, 11, 3, 4, 5}, {0, 1, 2}, 0, 0);   // du x w
+      add(EK_CROSS, {0, 1, 2, 12, 13, 14}, {0, 1, 2}, 0, 1);  // + u x dw
+      add(EK_CROSS, {9, 10, 11, 6, 7, 8}, {3, 4, 5}, 0, 0);   // du x b
+      add(EK_CROSS, {0, 1, 2, 15, 16, 17}, {3, 4, 5}, 0, 1);  // + u x db
+      break;
+    case OP_MHD_VJP:  // [u, w, b, c1, c2]
+      add(EK_CROSS, {3, 4, 5, 9, 10, 11}, {0, 1, 2}, A1, 0);  // w x c1
+      add(EK_CROSS, {6, 7, 8, 12, 13, 14}, {0, 1, 2}, A1, 1); // + b x c2
+      add(EK_CROSS, {9, 10, 11, 0, 1, 2}, {3, 4, 5}, A0, 0);  // c1 x u
+      add(EK_CROSS, {12, 13, 14, 0, 1, 2}, {6, 7, 8}, A0, 0); // c2 x u
+      break;
+    default: return set_error(SFNL_ERR_ARG, "unknown program");
+  }
+  return SFNL_OK;
+}
 
 int fast_grid_length(int m) { return make_geo(m).N; }
 
@@ -348,49 +387,8 @@ int launch_fast(const ProgArgs &a, cudaStream_t st) {
   int rc = get_tables(g, &T);
   if (rc) return rc;
   std::vector<Elem> seq;
-  auto X = [](int a0, int a1, int a2, int b0, int b1, int b2) { return std::vector<int>{a0, a1, a2, b0, b1, b2}; };
-  auto add = [&](int ek, std::vector<int> in, std::vector<int> out, unsigned adj, int acc) {
-    Elem e{};
-    e.ek = ek;
-    for (size_t i = 0; i < in.size(); ++i) e.in[i] = in[i];
-    for (size_t i = 0; i < out.size(); ++i) e.out[i] = out[i];
-    e.adj = adj;
-    e.acc = acc;
-    seq.push_back(e);
-  };
-  const unsigned A1 = 0x38u, A0 = 0x07u;  // cotangent as second / first operand
-  switch (a.op) {
-    case OP_CROSS: add(EK_CROSS, X(0, 1, 2, 3, 4, 5), {0, 1, 2}, 0, 0); break;
-    case OP_DOT: add(EK_DOT, X(0, 1, 2, 3, 4, 5), {0}, 0, 0); break;
-    case OP_PROD: add(EK_PROD, {0, 1}, {0}, 0, 0); break;
-    case OP_BUNDLE:
-      add(EK_CROSS, X(0, 1, 2, 3, 4, 5), {0, 1, 2}, 0, 0);     // u x w
-      add(EK_CROSS, X(0, 1, 2, 6, 7, 8), {3, 4, 5}, 0, 0);     // u x b
-      add(EK_CROSS, X(9, 10, 11, 6, 7, 8), {6, 7, 8}, 0, 0);   // j x b
-      add(EK_DOT, X(0, 1, 2, 12, 13, 14), {9}, 0, 0);          // u . gradT
-      break;
-    case OP_CROSS_JVP:  // [u, w, du, dw]
-      add(EK_CROSS, X(6, 7, 8, 3, 4, 5), {0, 1, 2}, 0, 0);     // du x w
-      add(EK_CROSS, X(0, 1, 2, 9, 10, 11), {0, 1, 2}, 0, 1);   // + u x dw
-      break;
-    case OP_CROSS_VJP:  // [u, w, c]
-      add(EK_CROSS, X(3, 4, 5, 6, 7, 8), {0, 1, 2}, A1, 0);    // w x c
-      add(EK_CROSS, X(6, 7, 8, 0, 1, 2), {3, 4, 5}, A0, 0);    // c x u
-      break;
-    case OP_MHD_JVP:  // [u, w, b, du, dw, db]
-      add(EK_CROSS, X(9, 10, 11, 3, 4, 5), {0, 1, 2}, 0, 0);   // du x w
-      add(EK_CROSS, X(0, 1, 2, 12, 13, 14), {0, 1, 2}, 0, 1);  // + u x dw
-      add(EK_CROSS, X(9, 10, 11, 6, 7, 8), {3, 4, 5}, 0, 0);   // du x b
-      add(EK_CROSS, X(0, 1, 2, 15, 16, 17), {3, 4, 5}, 0, 1);  // + u x db
-      break;
-    case OP_MHD_VJP:  // [u, w, b, c1, c2]
-      add(EK_CROSS, X(3, 4, 5, 9, 10, 11), {0, 1, 2}, A1, 0);  // w x c1
-      add(EK_CROSS, X(6, 7, 8, 12, 13, 14), {0, 1, 2}, A1, 1); // + b x c2
-      add(EK_CROSS, X(9, 10, 11, 0, 1, 2), {3, 4, 5}, A0, 0);  // c1 x u
-      add(EK_CROSS, X(12, 13, 14, 0, 1, 2), {6, 7, 8}, A0, 0); // c2 x u
-      break;
-    default: return set_error(SFNL_ERR_ARG, "unknown program");
-  }
+  rc = decompose_program(a.op, seq);
+  if (rc) return rc;
   const bool adj_out = op_adjoint_out(a.op);
   for (const Elem &e : seq) {
     FastArgs fa;

@@ -4,6 +4,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 #include "../../include/sfemans_nl.h"
 
@@ -25,6 +26,21 @@ bool fast_supported(int op, int m, int N_int);          // sfnl_fast.cu
 int fast_grid_length(int m);                            // sfnl_fast.cu
 void fast_release_tables();                             // sfnl_fast.cu
 int launch_split(const ProgArgs &a, int split, cudaStream_t st);  // sfnl_split.cu
+void split_release_tables();                            // sfnl_split.cu
+
+// Elementary programs: cross (6 -> 3), dot (6 -> 1), product (2 -> 1).  Every
+// program of sfnl_ops.cuh is a sequence of them on one stream (the bundle is
+// four, a linearised cross product two or four, accumulating where a term
+// adds to an earlier one).
+enum { EK_CROSS = 0, EK_DOT = 1, EK_PROD = 2 };
+struct Elem {
+  int ek;
+  int in[6];     // field indices into ProgArgs.in
+  int out[3];    // indices into ProgArgs.out
+  unsigned adj;  // bit f: operand f is a cotangent (synthesised with the analysis weights)
+  int acc;       // 1: add to the output instead of overwriting it
+};
+int decompose_program(int op, std::vector<Elem> &seq);   // sfnl_fast.cu
 bool split_supported(int op, int m);                    // sfnl_split.cu
 
 }  // namespace sfnl
