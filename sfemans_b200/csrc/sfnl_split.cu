@@ -315,16 +315,23 @@ __device__ __forceinline__ uint32_t bf16_bits(double v) {
   return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn((float)v));
 }
 
+// 2^e as a double (e clamped to the normal range).
+__device__ __forceinline__ double pow2(int e) {
+  e = e < -1022 ? -1022 : (e > 1023 ? 1023 : e);
+  return __longlong_as_double((long long)(e + 1023) << 52);
+}
+
 // Slices of x relative to the row bound 2^E (E from frexp of the row max).
+// Every step multiplies by an exact power of two, so h, mi, lo are exact.
 __device__ __forceinline__ void slice3(double x, int E, double &h, double &mi, double &lo) {
-  double unit = ldexp(1.0, E - kW);
-  h = rint(x / unit) * unit;
+  const double u0 = pow2(E - kW), i0 = pow2(kW - E);
+  const double u1 = pow2(E - 2 * kW - 1), i1 = pow2(2 * kW + 1 - E);
+  const double u2 = pow2(E - 3 * kW - 2), i2 = pow2(3 * kW + 2 - E);
+  h = rint(x * i0) * u0;
   double r = x - h;
-  unit = ldexp(unit, -(kW + 1));
-  mi = rint(r / unit) * unit;
+  mi = rint(r * i1) * u1;
   r -= mi;
-  unit = ldexp(unit, -(kW + 1));
-  lo = rint(r / unit) * unit;
+  lo = rint(r * i2) * u2;
 }
 
 __device__ __forceinline__ int row_exponent(double mx) {
@@ -487,7 +494,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
     phase ^= 1;
     tc_fence_after();
 
-    double *X = reinterpret_cast<double *>(sm + g.off_x);  // [p][f][quadrant][16]
+    double *X = reinterpret_cast<double *>(sm + g.off_x);  // [f][quadrant][16][p], point fastest
     double *sums = reinterpret_cast<double *>(sm + g.off_sum);  // [analysis column][row]
     // Adds the analysis of one chunk (TMEM, fp32) to the FP64 sums of the thread's row.
     auto add_chunk = [&](int chk) {
@@ -519,7 +526,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
               tmem_ld8(tmem + lane_base + (uint32_t)((c * 2 + ac) * g.Q + ch * 16 + h * 8), d[c][ac]);
           tmem_wait_ld();
           if (f < NI) {
-            double *xr = X + ((size_t)p * NI + f) * 64;
+            double *xr = X + (size_t)f * 64 * PTS + p;
 #pragma unroll
             for (int jj = 0; jj < 8; ++jj) {
               const double CE = (double)d[0][0][jj] + (double)d[0][1][jj];
@@ -528,10 +535,10 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
               const double SO = (double)d[3][0][jj] + (double)d[3][1][jj];
               const double A = CE + CO, B = CE - CO, C = SE + SO, D = SO - SE;
               const int j = h * 8 + jj;
-              xr[0 * 16 + j] = A + C;  // theta
-              xr[1 * 16 + j] = B + D;  // pi - theta
-              xr[2 * 16 + j] = B - D;  // pi + theta
-              xr[3 * 16 + j] = A - C;  // 2 pi - theta
+              xr[(0 * 16 + j) * PTS] = A + C;  // theta
+              xr[(1 * 16 + j) * PTS] = B + D;  // pi - theta
+              xr[(2 * 16 + j) * PTS] = B - D;  // pi + theta
+              xr[(3 * 16 + j) * PTS] = A - C;  // 2 pi - theta
             }
           }
         }
@@ -559,7 +566,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
           for (int r = 0; r < 4; ++r) {
             double xv[NI], yv[NO];
 #pragma unroll
-            for (int f = 0; f < NI; ++f) xv[f] = X[((size_t)p * NI + f) * 64 + r * 16 + j];
+            for (int f = 0; f < NI; ++f) xv[f] = X[((size_t)(f * 4 + r) * 16 + j) * PTS + p];
             SDef<EK>::op(xv, yv);
             gq[r] = yv[0];
 #pragma unroll
