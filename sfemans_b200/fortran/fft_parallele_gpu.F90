@@ -1,0 +1,147 @@
+!
+! fft_parallele_gpu -- drop-in for the dealiased products of MODULE fft_parallele
+! (SOURCES/POST_PROCESSING/fft_parallel.F90) backed by the B200 library
+! libsfemans_nl.so through ISO_C_BINDING.
+!
+! Same PUBLIC names, argument lists and argument meaning as
+!   FFT_PAR_CROSS_PROD_DCL  fft_parallel.F90:147
+!   FFT_PAR_DOT_PROD_DCL    fft_parallel.F90:330
+!   FFT_PAR_PROD_DCL        fft_parallel.F90:502
+! One GPU holds every Fourier mode, so the Fourier communicator must have
+! one rank (nb_procs == 1).  bloc_size is checked (np <= nb_procs*bloc_size)
+! and otherwise unused.  temps(3), when present, receives the data-movement
+! seconds in temps(1) and the kernel seconds in temps(2).  A non-zero status
+! from the library prints 'BUG in FFT_PAR_...' with the library's message and
+! STOPs, as the reference does (fft_parallel.F90:188-191).
+!
+MODULE fft_parallele_gpu
+#include "petsc/finclude/petsc.h"
+  USE petsc
+  USE ISO_C_BINDING
+  IMPLICIT NONE
+  PRIVATE
+  PUBLIC :: FFT_PAR_CROSS_PROD_DCL, FFT_PAR_DOT_PROD_DCL, FFT_PAR_PROD_DCL
+
+  INTERFACE
+     FUNCTION sfnl_fft_par_cross_prod_dcl(V1_in, V2_in, V_out, np, nb_field, m_max_c, nb_procs, &
+          bloc_size, m_max_pad, temps) RESULT(rc) BIND(C, NAME='sfnl_fft_par_cross_prod_dcl')
+       IMPORT :: C_INT, C_DOUBLE, C_PTR
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(IN)  :: V1_in, V2_in
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(OUT) :: V_out
+       INTEGER(C_INT), VALUE :: np, nb_field, m_max_c, nb_procs, bloc_size, m_max_pad
+       TYPE(C_PTR), VALUE    :: temps
+       INTEGER(C_INT)        :: rc
+     END FUNCTION sfnl_fft_par_cross_prod_dcl
+
+     FUNCTION sfnl_fft_par_dot_prod_dcl(V1_in, V2_in, c_out, np, nb_field, m_max_c, nb_procs, &
+          bloc_size, m_max_pad, temps) RESULT(rc) BIND(C, NAME='sfnl_fft_par_dot_prod_dcl')
+       IMPORT :: C_INT, C_DOUBLE, C_PTR
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(IN)  :: V1_in, V2_in
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(OUT) :: c_out
+       INTEGER(C_INT), VALUE :: np, nb_field, m_max_c, nb_procs, bloc_size, m_max_pad
+       TYPE(C_PTR), VALUE    :: temps
+       INTEGER(C_INT)        :: rc
+     END FUNCTION sfnl_fft_par_dot_prod_dcl
+
+     FUNCTION sfnl_fft_par_prod_dcl(c1_in, c2_in, c_out, np, m_max_c, nb_procs, &
+          bloc_size, m_max_pad, temps) RESULT(rc) BIND(C, NAME='sfnl_fft_par_prod_dcl')
+       IMPORT :: C_INT, C_DOUBLE, C_PTR
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(IN)  :: c1_in, c2_in
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(OUT) :: c_out
+       INTEGER(C_INT), VALUE :: np, m_max_c, nb_procs, bloc_size, m_max_pad
+       TYPE(C_PTR), VALUE    :: temps
+       INTEGER(C_INT)        :: rc
+     END FUNCTION sfnl_fft_par_prod_dcl
+
+     FUNCTION sfnl_last_error() RESULT(msg) BIND(C, NAME='sfnl_last_error')
+       IMPORT :: C_PTR
+       TYPE(C_PTR) :: msg
+     END FUNCTION sfnl_last_error
+  END INTERFACE
+
+CONTAINS
+
+  SUBROUTINE check_comm(communicator, nb_procs, what)
+    MPI_Comm,         INTENT(IN) :: communicator
+    INTEGER,          INTENT(IN) :: nb_procs
+    CHARACTER(LEN=*), INTENT(IN) :: what
+    INTEGER :: nproc, code
+    CALL MPI_COMM_SIZE(communicator, nproc, code)
+    IF (nproc /= nb_procs .OR. nb_procs /= 1) THEN
+       WRITE(*,*) ' BUG in ', what, ': the GPU path holds all Fourier modes on one rank (nb_procs must be 1)'
+       STOP
+    END IF
+  END SUBROUTINE check_comm
+
+  SUBROUTINE stop_on_error(rc, what)
+    INTEGER(C_INT),   INTENT(IN) :: rc
+    CHARACTER(LEN=*), INTENT(IN) :: what
+    CHARACTER(KIND=C_CHAR), DIMENSION(:), POINTER :: cmsg
+    CHARACTER(LEN=256) :: msg
+    INTEGER :: i
+    IF (rc == 0) RETURN
+    CALL C_F_POINTER(sfnl_last_error(), cmsg, [256])
+    msg = ' '
+    DO i = 1, 256
+       IF (cmsg(i) == C_NULL_CHAR) EXIT
+       msg(i:i) = cmsg(i)
+    END DO
+    WRITE(*,*) ' BUG in ', what, ' (status ', rc, '): ', TRIM(msg)
+    STOP
+  END SUBROUTINE stop_on_error
+
+  SUBROUTINE FFT_PAR_CROSS_PROD_DCL(communicator, V1_in, V2_in, V_out, nb_procs, bloc_size, m_max_pad, temps)
+    MPI_Comm :: communicator
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(IN)  :: V1_in, V2_in
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(OUT) :: V_out
+    INTEGER, INTENT(IN) :: nb_procs, bloc_size, m_max_pad
+    REAL(KIND=8), DIMENSION(:), OPTIONAL, INTENT(INOUT) :: temps
+    REAL(C_DOUBLE), DIMENSION(3), TARGET :: t3
+    INTEGER(C_INT) :: rc
+    CALL check_comm(communicator, nb_procs, 'FFT_PAR_CROSS_PROD_DCL')
+    rc = sfnl_fft_par_cross_prod_dcl(V1_in, V2_in, V_out, INT(SIZE(V1_in,1), C_INT), INT(SIZE(V1_in,2), C_INT), &
+         INT(SIZE(V1_in,3), C_INT), INT(nb_procs, C_INT), INT(bloc_size, C_INT), INT(m_max_pad, C_INT), C_LOC(t3))
+    CALL stop_on_error(rc, 'FFT_PAR_CROSS_PROD_DCL')
+    IF (PRESENT(temps)) THEN
+       temps = 0.d0
+       temps(1:MIN(3,SIZE(temps))) = t3(1:MIN(3,SIZE(temps)))
+    END IF
+  END SUBROUTINE FFT_PAR_CROSS_PROD_DCL
+
+  SUBROUTINE FFT_PAR_DOT_PROD_DCL(communicator, V1_in, V2_in, c_out, nb_procs, bloc_size, m_max_pad, temps)
+    MPI_Comm :: communicator
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(IN)  :: V1_in, V2_in
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(OUT) :: c_out
+    INTEGER, INTENT(IN) :: nb_procs, bloc_size, m_max_pad
+    REAL(KIND=8), DIMENSION(:), OPTIONAL, INTENT(INOUT) :: temps
+    REAL(C_DOUBLE), DIMENSION(3), TARGET :: t3
+    INTEGER(C_INT) :: rc
+    CALL check_comm(communicator, nb_procs, 'FFT_PAR_DOT_PROD_DCL')
+    rc = sfnl_fft_par_dot_prod_dcl(V1_in, V2_in, c_out, INT(SIZE(V1_in,1), C_INT), INT(SIZE(V1_in,2), C_INT), &
+         INT(SIZE(V1_in,3), C_INT), INT(nb_procs, C_INT), INT(bloc_size, C_INT), INT(m_max_pad, C_INT), C_LOC(t3))
+    CALL stop_on_error(rc, 'FFT_PAR_DOT_PROD_DCL')
+    IF (PRESENT(temps)) THEN
+       temps = 0.d0
+       temps(1:MIN(3,SIZE(temps))) = t3(1:MIN(3,SIZE(temps)))
+    END IF
+  END SUBROUTINE FFT_PAR_DOT_PROD_DCL
+
+  SUBROUTINE FFT_PAR_PROD_DCL(communicator, c1_in, c2_in, c_out, nb_procs, bloc_size, m_max_pad, temps)
+    MPI_Comm :: communicator
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(IN)  :: c1_in, c2_in
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(OUT) :: c_out
+    INTEGER, INTENT(IN) :: nb_procs, bloc_size, m_max_pad
+    REAL(KIND=8), DIMENSION(:), OPTIONAL, INTENT(INOUT) :: temps
+    REAL(C_DOUBLE), DIMENSION(3), TARGET :: t3
+    INTEGER(C_INT) :: rc
+    CALL check_comm(communicator, nb_procs, 'FFT_PAR_PROD_DCL')
+    rc = sfnl_fft_par_prod_dcl(c1_in, c2_in, c_out, INT(SIZE(c1_in,1), C_INT), INT(SIZE(c1_in,3), C_INT), &
+         INT(nb_procs, C_INT), INT(bloc_size, C_INT), INT(m_max_pad, C_INT), C_LOC(t3))
+    CALL stop_on_error(rc, 'FFT_PAR_PROD_DCL')
+    IF (PRESENT(temps)) THEN
+       temps = 0.d0
+       temps(1:MIN(3,SIZE(temps))) = t3(1:MIN(3,SIZE(temps)))
+    END IF
+  END SUBROUTINE FFT_PAR_PROD_DCL
+
+END MODULE fft_parallele_gpu

@@ -1,0 +1,76 @@
+"""Multi-rank host logic on CPU (gloo): point sharding and the reference's
+mode-distributed layout with its two all-to-all exchanges
+(fft_parallel.F90:217, :306).  The per-rank product on the gathered block
+is the CPU oracle here (no GPU in this process); on GPUs it is the CUDA
+kernel and the exchange runs over NCCL."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from oracle import ref_fft as R
+from sfemans_b200.parallel import fft_par_distributed, shard_range
+
+
+@pytest.mark.parametrize("npts,world", [(0, 1), (7, 3), (28000, 8), (1_400_000, 8), (5, 8)])
+def test_shard_range_partitions_points(npts, world):
+    spans = [shard_range(npts, r, world) for r in range(world)]
+    assert spans[0][0] == 0 and spans[-1][1] == npts
+    for (a, b), (c, d) in zip(spans, spans[1:]):
+        assert b == c and a <= b
+    sizes = [b - a for a, b in spans]
+    assert max(sizes) - min(sizes) <= 1
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _oracle_compute(kind, xb, yb, m_max_pad):
+    to_np = lambda t: np.asfortranarray(t.permute(2, 1, 0).contiguous().numpy().T)  # noqa: E731
+    out = R.c_oracle(kind, to_np(xb), to_np(yb), m_max_pad)
+    return torch.from_numpy(np.ascontiguousarray(out.T)).permute(2, 1, 0)
+
+
+def _worker(rank, world, port, kind, npts, m, pad, bloc, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        nsl = 2 if kind == "prod" else 6
+        V1 = R.synthetic_field(npts, nsl, m, 0.2, 41)
+        V2 = R.synthetic_field(npts, nsl, m, 0.2, 42)
+        mc = m // world
+        loc = lambda V: torch.from_numpy(np.ascontiguousarray(V[:, :, rank * mc:(rank + 1) * mc].T)).permute(2, 1, 0)  # noqa: E731
+        nout = 6 if kind == "cross" else 2
+        out = torch.zeros((mc, nout, npts), dtype=torch.float64).permute(2, 1, 0)
+        fft_par_distributed(kind, None, loc(V1), loc(V2), out, world, bloc, pad, compute=_oracle_compute)
+        ref = R.c_oracle(kind, V1, V2, pad)[:, :, rank * mc:(rank + 1) * mc]
+        q.put((rank, float(np.abs(out.numpy() - ref).max())))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("kind,world,npts,m", [("cross", 2, 23, 6), ("dot", 3, 31, 9), ("prod", 2, 40, 4)])
+def test_mode_distributed_layout_matches_single_rank(kind, world, npts, m):
+    pad = 3 * m // 2
+    bloc = npts // world + 1  # the callers' bloc_size (subroutine_ns_with_velocity.F90:625)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, kind, npts, m, pad, bloc, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    res = dict(q.get(timeout=5) for _ in range(world))
+    assert all(p.exitcode == 0 for p in procs)
+    for r in range(world):
+        assert res[r] < 1e-14, res
