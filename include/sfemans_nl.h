@@ -166,6 +166,24 @@ int sfnl_bundle_mhd_host(const double *u, const double *w, const double *b, cons
                          int m_max_pad, int form /* 0 = FP64, 2/3 = split */);
 
 /* ---------------------------------------------------------------------------
+ * No-allocation variant.  No counterpart in the reference.
+ * The FAST FP64 cross product (same arguments and result as sfnl_cross_f64 on
+ * a dealiasing pad) for callers that must not allocate device memory: codes
+ * whose GPU memory is owned by their own pool or by another framework, and
+ * callers that cannot afford cudaMalloc's implicit device synchronisation in
+ * their time loop.  Its DFT tables live in a fixed array inside the library
+ * (144 KiB of static device memory on every GPU that loads the library, held
+ * until the process exits), so m_max is limited to 64 (SFNL_ERR_UNSUPPORTED
+ * above).  The first call on a device, and any call whose m_max differs from
+ * the previous call's, looks up that array and rewrites it on `stream`; make
+ * that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (different streams) race on it when their
+ * m_max differs or while a rewrite is in flight.
+ * ------------------------------------------------------------------------- */
+int sfnl_cross_f64_noalloc(const double *v1, const double *v2, double *out, int64_t np, int m_max, int m_max_pad,
+                           sfnl_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Library state.
  * ------------------------------------------------------------------------- */
 const char *sfnl_last_error(void); /* message of the last failing call on this thread */

@@ -52,6 +52,7 @@ _SIGS = {
     "sfnl_dot_f64": [_P, _P, _P, _L, _I, _I, _P],
     "sfnl_prod_f64": [_P, _P, _P, _L, _I, _I, _P],
     "sfnl_product_f64": [_I, _P, _P, _P, _L, _I, _I, _I, _I, _P],
+    "sfnl_cross_f64_noalloc": [_P, _P, _P, _L, _I, _I, _P],
     "sfnl_bundle_mhd_f64": [_P] * 9 + [_L, _I, _I, _I, _P],
     "sfnl_cross_jvp_f64": [_P, _P, _P, _P, _L, _I, _I, _I, _P],
     "sfnl_cross_vjp_f64": [_P, _P, _P, _P, _L, _I, _I, _I, _P],

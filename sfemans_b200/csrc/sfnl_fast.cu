@@ -429,6 +429,70 @@ int launch_fast(const ProgArgs &a, cudaStream_t st) {
   return SFNL_OK;
 }
 
+// ---------------------------------------------------------------------------
+// sfnl_cross_f64_noalloc: the FAST cross product for callers that cannot
+// allocate device memory.  Its DFT tables live in the static device array
+// below (one copy per device that loads the library, kept until exit) and are
+// written on the device by build_tables_kernel, so the entry point calls no
+// cudaMalloc, cudaFree or other allocating routine.
+// ---------------------------------------------------------------------------
+constexpr int kNoAllocMaxM = 64;
+constexpr int kNoAllocDoubles = 18432;  // synthesis + both analysis variants at m = 64 (144 KiB)
+static __device__ __align__(256) double g_noalloc_tab[kNoAllocDoubles];
+
+namespace {
+std::mutex g_na_mu;
+double *g_na_ptr[64];  // device address of g_noalloc_tab, per device (set up on first use)
+int g_na_m[64];        // m_max whose tables the array holds, per device (0: none)
+
+// Writes the folded-transform tables of make_geo(m) (same entries as get_tables,
+// angles reduced exactly as n(2j+1) mod 2N before sincospi).
+__global__ void build_tables_kernel(double *syn, double *ana, FastArgs g) {
+  int ks_tot = 0;
+  for (int c = 0; c < 4; ++c) ks_tot += g.KS[c];
+  const int64_t n_syn = (int64_t)ks_tot * g.NT * 32, n_ana = (int64_t)2 * g.NU_tot * g.NT * 64;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n_syn + n_ana;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    int c = 0, k, j, n, var = 0;
+    bool live;
+    if (idx < n_syn) {
+      const int l = (int)(idx % 32), r = (int)(idx / 32), t = r % g.NT, ks = r / g.NT;
+      while (c < 3 && ks >= g.ks_off[c + 1]) ++c;
+      k = 4 * (ks - g.ks_off[c]) + (l & 3);
+      j = 8 * t + (l >> 2);
+      live = k < g.ke[c];
+    } else {
+      int64_t r = idx - n_syn;
+      const int l = (int)(r % 32);
+      r /= 32;
+      const int e = (int)(r % 2);
+      r /= 2;
+      const int t = (int)(r % g.NT);
+      r /= g.NT;
+      const int cu = (int)(r % g.NU_tot);
+      var = (int)(r / g.NU_tot);
+      while (c < 3 && cu >= g.nu_off[c + 1]) ++c;
+      j = 8 * t + 2 * (l & 3) + e;
+      k = 8 * (cu - g.nu_off[c]) + (l >> 2);
+      live = k < g.ke[c];
+    }
+    double v = 0.0;
+    if (live) {
+      n = 2 * k + (c & 1);
+      const long long rr = ((long long)n * (2 * j + 1)) % (2LL * g.N);
+      double sv, cv;
+      sincospi((double)rr / (double)g.N, &sv, &cv);
+      v = c < 2 ? cv : sv;
+      if (idx >= n_syn && var == 0) v *= (n == 0 ? 1.0 : 2.0) / (double)g.N;
+    }
+    if (idx < n_syn)
+      syn[idx] = v;
+    else
+      ana[idx - n_syn] = v;
+  }
+}
+}  // namespace
+
 void fast_release_tables() {
   std::lock_guard<std::mutex> lk(g_tab_mu);
   int prev = 0;
@@ -443,3 +507,63 @@ void fast_release_tables() {
 }
 
 }  // namespace sfnl
+
+extern "C" int sfnl_cross_f64_noalloc(const double *v1, const double *v2, double *out, int64_t np, int m_max,
+                                      int m_max_pad, sfnl_stream_t stream) {
+  using namespace sfnl;
+  if (np < 0 || m_max < 1) return set_error(SFNL_ERR_ARG, "sfnl_cross_f64_noalloc: np < 0 or m_max < 1");
+  if (m_max_pad < m_max) return set_error(SFNL_ERR_ALIAS, "sfnl_cross_f64_noalloc: m_max_pad < m_max");
+  if (2 * m_max_pad - 1 < 3 * m_max - 2)
+    return set_error(SFNL_ERR_ALIAS, "sfnl_cross_f64_noalloc: needs a dealiasing pad (2*m_max_pad-1 >= 3*m_max-2)");
+  if (m_max > kNoAllocMaxM)
+    return set_error(SFNL_ERR_UNSUPPORTED, "sfnl_cross_f64_noalloc: m_max > 64 does not fit its static table");
+  if (np == 0) return SFNL_OK;
+  if (!v1 || !v2 || !out) return set_error(SFNL_ERR_ARG, "sfnl_cross_f64_noalloc: null array");
+  const Geo g = make_geo(m_max);
+  const int n_syn = g.KS_tot * g.NT * 32, n_ana = 2 * g.NU_tot * g.NT * 64;
+  if (n_syn + n_ana > kNoAllocDoubles) return set_error(SFNL_ERR_UNSUPPORTED, "sfnl_cross_f64_noalloc: table overflow");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  FastArgs fa;
+  std::memset(&fa, 0, sizeof(fa));
+  for (int k = 0; k < 3; ++k) {
+    fa.in[k] = v1 + (int64_t)2 * k * np;
+    fa.in[3 + k] = v2 + (int64_t)2 * k * np;
+    fa.out[k] = out + (int64_t)2 * k * np;
+  }
+  for (int f = 0; f < 6; ++f) fa.in_ldm[f] = 6 * np;
+  for (int o = 0; o < 3; ++o) fa.out_ldm[o] = 6 * np;
+  fa.np = np;
+  fa.m = g.m;
+  fa.N = g.N;
+  fa.NT = g.NT;
+  for (int c = 0; c < 4; ++c) {
+    fa.ks_off[c] = g.ks_off[c];
+    fa.KS[c] = g.KS[c];
+    fa.nu_off[c] = g.nu_off[c];
+    fa.NU[c] = g.NU[c];
+    fa.ke[c] = g.ke[c];
+  }
+  fa.NU_tot = g.NU_tot;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    return set_error(SFNL_ERR_CUDA, "sfnl_cross_f64_noalloc: no current device");
+  {
+    std::lock_guard<std::mutex> lk(g_na_mu);
+    if (!g_na_ptr[dev]) {
+      void *p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_tab);
+      if (e != cudaSuccess || !p) return set_error(SFNL_ERR_CUDA, "sfnl_cross_f64_noalloc: cudaGetSymbolAddress failed");
+      g_na_ptr[dev] = static_cast<double *>(p);
+      g_na_m[dev] = 0;
+    }
+    fa.syn = g_na_ptr[dev];
+    fa.ana = g_na_ptr[dev] + n_syn;
+    if (g_na_m[dev] != m_max) {
+      build_tables_kernel<<<64, 256, 0, st>>>(g_na_ptr[dev], g_na_ptr[dev] + n_syn, fa);
+      const int rc = check_launch("sfnl_cross_f64_noalloc table set-up");
+      if (rc) return rc;
+      g_na_m[dev] = m_max;
+    }
+  }
+  return launch_ek<EK_CROSS>(fa, 1, st);
+}
