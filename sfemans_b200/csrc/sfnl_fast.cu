@@ -163,6 +163,7 @@ struct FastArgs {
   int m, N, NT;
   int ks_off[4], KS[4], nu_off[4], NU[4], ke[4];
   int NU_tot;
+  int KT;           // staged coefficient rows per field (4 * total synthesis k-steps)
   unsigned adj_in;  // bit f: input field f is a cotangent (synthesise with D)
   int adj_out;      // 1: analyse without D (transpose of the synthesis)
   int accumulate;   // 1: out += result
@@ -193,21 +194,42 @@ struct EKDef<EK_PROD> {
   __device__ static void op(const double *x, double *y) { y[0] = x[0] * x[1]; }
 };
 
+__device__ __forceinline__ void cp_async8(void *smem_dst, const void *gsrc) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
+               "l"(gsrc)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 template <int EK>
 __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
   constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO;
-  extern __shared__ double ps[];  // [NO][4][NT][2][32]
+  extern __shared__ double ps[];  // [NO][4][NT][2][32] folded products, then [NI][KT][8] staged coefficients
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, NW = blockDim.x >> 5;
   const int g = lane >> 2, q = lane & 3;
-  const int64_t p = (int64_t)blockIdx.x * 8 + g;
+  const int64_t p0 = (int64_t)blockIdx.x * 8, p = p0 + g;
   const bool valid = p < a.np;
   const int b = blockIdx.y;
-  const int NT = a.NT;
+  const int NT = a.NT, KT = a.KT;
   const double invN = 1.0 / a.N, twoN = 2.0 / a.N;
 
-  const double *src[NI];
-#pragma unroll
-  for (int f = 0; f < NI; ++f) src[f] = a.in[f] + (int64_t)b * a.in_bs[f] + (valid ? p : 0);
+  // ---- stage the tile's coefficients: row r of field f = (class c, k), 8 points each ----
+  double *xs = ps + (size_t)NO * 4 * NT * 2 * 32;
+  for (int idx = threadIdx.x; idx < NI * KT * 8; idx += blockDim.x) {
+    const int pp = idx & 7, fr = idx >> 3, r = fr % KT, f = fr / KT;
+    int c = 0;
+    while (c < 3 && r >= 4 * a.ks_off[c + 1]) ++c;
+    const int k = r - 4 * a.ks_off[c], n = class_mode(c, k);
+    const int64_t gp = p0 + pp;
+    if (gp < a.np && k < a.ke[c] && !(c == 2 && n == 0))  // the sine of mode 0 is ignored
+      cp_async8(xs + idx, a.in[f] + (int64_t)b * a.in_bs[f] + gp + (int64_t)n * a.in_ldm[f] + (c >= 2 ? a.np : 0));
+    else
+      xs[idx] = 0.0;
+  }
+  cp_async_wait_all();
+  __syncthreads();
 
   // ---- synthesis, fold, program, analysis pre-fold ----
   for (int t = warp; t < NT; t += NW) {
@@ -219,20 +241,21 @@ __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       const double *bt = a.syn + ((size_t)a.ks_off[c] * NT + t) * 32 + lane;
+      const double *xa = xs + (size_t)(4 * a.ks_off[c] + q) * 8 + g;
+      double bv = __ldg(bt);
+#pragma unroll 2
       for (int s = 0; s < a.KS[c]; ++s) {
-        const int k = 4 * s + q;
-        const int n = class_mode(c, k);
-        const bool live = valid && k < a.ke[c] && !(c == 2 && n == 0);  // sine of mode 0 ignored
-        const int64_t off = (c >= 2 ? a.np : 0);
-        const double bv = __ldg(bt + (size_t)s * NT * 32);
+        const double bn = (s + 1 < a.KS[c]) ? __ldg(bt + (size_t)(s + 1) * NT * 32) : 0.0;
+        const int n = class_mode(c, 4 * s + q);
         double av[NI];
 #pragma unroll
         for (int f = 0; f < NI; ++f) {
-          av[f] = live ? __ldg(src[f] + off + (int64_t)n * a.in_ldm[f]) : 0.0;
+          av[f] = xa[(size_t)f * KT * 8 + (size_t)s * 32];
           if (a.adj_in & (1u << f)) av[f] *= (n == 0 ? invN : twoN);
         }
 #pragma unroll
         for (int f = 0; f < NI; ++f) dmma(acc[f][c], av[f], bv);
+        bv = bn;
       }
     }
 #pragma unroll
@@ -275,13 +298,16 @@ __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
 #pragma unroll
     for (int o = 0; o < NO; ++o) y[o][0] = y[o][1] = 0.0;
     const double *bt = anav + (size_t)cu * NT * 2 * 32 + lane;
+    double bv = __ldg(bt);
+#pragma unroll 2
     for (int te = 0; te < 2 * NT; ++te) {
-      const double bv = __ldg(bt + (size_t)te * 32);
+      const double bn = (te + 1 < 2 * NT) ? __ldg(bt + (size_t)(te + 1) * 32) : 0.0;
 #pragma unroll
       for (int o = 0; o < NO; ++o) {
         const double av = ps[((size_t)(o * 4 + c) * NT * 2 + te) * 32 + lane];
         dmma(y[o], av, bv);
       }
+      bv = bn;
     }
     if (!valid) continue;
 #pragma unroll
@@ -304,8 +330,9 @@ __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
 
 template <int EK>
 int launch_ek(FastArgs &fa, int batch, cudaStream_t st) {
-  constexpr int NO = EKDef<EK>::NO;
-  const size_t smem = sizeof(double) * (size_t)NO * 4 * fa.NT * 2 * 32;
+  constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO;
+  fa.KT = 4 * (fa.KS[0] + fa.KS[1] + fa.KS[2] + fa.KS[3]);
+  const size_t smem = sizeof(double) * ((size_t)NO * 4 * fa.NT * 2 * 32 + (size_t)NI * fa.KT * 8);
   if (smem > 200 * 1024) return set_error(SFNL_ERR_UNSUPPORTED, "FAST form: m too large for shared memory");
   int nw = fa.NT < 8 ? fa.NT : 8;
   if (nw < 2) nw = 2;
@@ -376,7 +403,7 @@ bool fast_supported(int op, int m, int N) {
   (void)op;
   if (m < 1 || m > 512) return false;
   const Geo g = make_geo(m);
-  return g.N == N && (size_t)3 * 4 * g.NT * 2 * 32 * sizeof(double) <= 200 * 1024;
+  return g.N == N && sizeof(double) * ((size_t)3 * 4 * g.NT * 2 * 32 + (size_t)6 * 4 * g.KS_tot * 8) <= 200 * 1024;
 }
 
 int launch_fast(const ProgArgs &a, cudaStream_t st) {
