@@ -208,85 +208,125 @@ def main():
     else:
         outs = (sf.fortran_empty(npts, 6, m, device=dev),)
 
-    # pick the form
-    forms = {"fp64": dict(algo=sf.ALGO_AUTO), "grid": dict(algo=sf.ALGO_GRID), "split2": dict(split=sf.SPLIT_BF16X2),
-             "split3": dict(split=sf.SPLIT_BF16X3)}
-    form = args.form
-    if form == "auto":
-        form = "split3"
-        try:
-            _call(sf, args.workload, ins, outs, pad, forms[form])
-        except sf.SfnlError:
-            form = "fp64"
-    kw = forms[form]
+    forms = {"fp64": dict(algo=sf.ALGO_FAST), "split3": dict(split=sf.SPLIT_BF16X3),
+             "split2": dict(split=sf.SPLIT_BF16X2), "grid": dict(algo=sf.ALGO_GRID)}
+    launches = {"fp64": 4, "split3": 4, "split2": 4, "grid": 1} if args.workload == "mhd_bundle" else \
+        {"fp64": 1, "split3": 1, "split2": 1, "grid": 1}
+    order = ["fp64", "split3", "split2", "grid"] if args.form == "auto" else [args.form if args.form != "fp64" else "fp64"]
     stream = torch.cuda.current_stream()
 
-    def step():
-        _call(sf, args.workload, ins, outs, pad, kw)
+    # reference outputs on a bounded sample (rank 0, one GPU): the CPU port, also timed as the CPU baseline
+    cpu = None
+    ref = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu, ref, sample = _cpu_baseline(args, ins, npts, m, pad)
 
-    for _ in range(max(args.warmup, 3)):
-        step()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-    torch.cuda.synchronize()
-    ev[0].record(stream)
-    for i in range(args.steps):
-        step()
-        ev[i + 1].record(stream)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    clk = clocks.stop()
-    per = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
-    ms = sum(per) / len(per)
-    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms = float(ms_t.item())
-    units = npts * m
-    value = world * units / (ms / 1e3)
-    algo_bytes = 8.0 * m * (IN_SLOTS[args.workload] + OUT_SLOTS[args.workload]) * npts
+    results = {}
+    clk_all = None
+    for form in order:
+        kw = forms[form]
+        try:
+            _call(sf, args.workload, ins, outs, pad, kw)
+        except sf.SfnlError as e:
+            results[form] = {"unavailable": str(e)}
+            continue
+        steps = args.steps if form == order[0] or form == "fp64" else min(args.steps, 3)
+        ms, clk = _time_steps(lambda: _call(sf, args.workload, ins, outs, pad, kw), steps, args.warmup, stream, world,
+                              dist, local)
+        r = {"ms_per_step": ms, "value": world * npts * m / (ms / 1e3), "steps": steps, "gpu_launches_per_step": launches[form]}
+        if ref is not None:
+            names = ["uxw", "uxb", "jxb", "ugradt"] if args.workload == "mhd_bundle" else ["uxw"]
+            r["rel_l2_vs_cpu_port"] = {n: R_rel_l2(sf.to_host(o[:sample]), rr) for n, o, rr in zip(names, outs, ref)}
+        results[form] = r
+        if form == "fp64" or clk_all is None:
+            clk_all = clk
+
+    def ok(f):
+        r = results.get(f, {})
+        if "ms_per_step" not in r:
+            return False
+        if "rel_l2_vs_cpu_port" in r:
+            return max(r["rel_l2_vs_cpu_port"].values()) <= 1e-7
+        return f in ("fp64", "grid", "split3")  # bars enforced by the -m gpu tests
+    cands = [f for f in results if ok(f)]
+    best = min(cands, key=lambda f: results[f]["ms_per_step"])
+    ms = results[best]["ms_per_step"]
+    value = results[best]["value"]
+
+    # dominant kernel: the elementary cross product of the chosen form, timed per launch at full size
+    dom_ms = _time_steps(lambda: sf.product(sf.OP_CROSS, ins[0], ins[1], out=outs[0], m_max_pad=pad, **forms[best]),
+                         args.steps, args.warmup, stream, world, dist, local)[0] if best != "grid" or args.workload != "mhd_bundle" else ms
+    dom_bytes = 8.0 * m * ((12 + 6) if dom_ms != ms or args.workload != "mhd_bundle" else 50) * npts
     hbm, _, peak_kind = _peaks()
-    achieved = algo_bytes / (ms / 1e3) / 1e9
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
 
-    # e2e through the host-array entry point (pinned host buffers, copies timed)
     e2e = None
     if args.workload == "mhd_bundle" and args.e2e_steps > 0:
-        e2e = _e2e_bundle(sf, torch, ins, npts, m, pad, form, args.e2e_steps, world, dist)
+        e2e = _e2e_bundle(sf, torch, ins, npts, m, pad, best, args.e2e_steps, world, dist)
 
-    # accuracy of this form and the CPU baseline, rank 0, single GPU only
-    cpu = None
-    acc = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        cpu, acc = _cpu_baseline(args, ins, outs, npts, m, pad)
-
-    traffic = _traffic(args.workload, form)
+    kname = {"fp64": "fast_kernel<EK_CROSS>", "split3": "split_kernel<EK_CROSS>", "split2": "split_kernel<EK_CROSS>",
+             "grid": "grid_kernel<OP_BUNDLE>"}[best]
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if form in ("fp64", "grid") else "bf16-sliced f64 (fp32 accumulate, fp64 recombine)",
-        "data": "synthetic",
-        "config": {"workload": args.workload, "form": form, "np": npts, "m_max": m, "m_max_pad": pad,
-                   "alpha": alpha, "l2": "inputs larger than L2 (no flush needed)", "desc": wl["desc"],
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": results[best]["steps"],
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if best in ("fp64", "grid") else "f64 via bf16 slices (fp32 accumulate, fp64 recombine)",
+        "data": "synthetic N(0,1)*exp(-alpha*n) coefficients generated on the device",
+        "config": {"workload": args.workload, "form": best, "np": npts, "m_max": m, "m_max_pad": pad,
+                   "alpha": alpha, "desc": wl["desc"],
+                   "l2": "inputs larger than L2 (no flush needed)" if args.workload == "mhd_bundle"
+                   else "inputs smaller than L2: repeated steps re-read L2-resident data",
                    "parallelism": f"point-sharded replicas x{world}"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": traffic, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_launch": algo_bytes},
-        "clocks": clk,
-        "gpu_launches": args.steps * 1,
+        "forms": results,
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": _traffic(args.workload, best), "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": dom_ms},
+        "clocks": clk_all,
+        "gpu_launches": results[best]["steps"] * launches[best],
         "e2e": e2e,
         "cpu_baseline": cpu,
-        "accuracy": acc,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def R_rel_l2(x, ref):
+    import numpy as np
+
+    x = np.asarray(x, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    den = np.linalg.norm(ref)
+    return float(np.linalg.norm(x - ref) / (den if den > 0 else 1.0))
+
+
+def _time_steps(step, steps, warmup, stream, world, dist, local):
+    """CUDA-event timing of `steps` calls after `warmup` (>= 3), barrier + sync on both sides, max over ranks."""
+    import torch
+
+    for _ in range(max(warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    ev[0].record(stream)
+    for i in range(steps):
+        step()
+        ev[i + 1].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = sum(ev[i].elapsed_time(ev[i + 1]) for i in range(steps)) / steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, clk
 
 
 def _call(sf, workload, ins, outs, pad, kw):
@@ -337,8 +377,8 @@ def _e2e_bundle(sf, torch, ins, npts, m, pad, form, steps, world, dist):
             "api": "sfnl_bundle_mhd_host (host arrays, pinned)"}
 
 
-def _cpu_baseline(args, ins, outs, npts, m, pad):
-    """Oracle port timed on the host cores over a bounded sample; also the checker of this run's output."""
+def _cpu_baseline(args, ins, npts, m, pad):
+    """Oracle port timed on the host cores over a bounded sample; its output is also the checker of this run."""
     import numpy as np
 
     import sfemans_b200 as sf
@@ -361,12 +401,10 @@ def _cpu_baseline(args, ins, outs, npts, m, pad):
         if time.perf_counter() - t0 > 10.0 or reps >= 50:
             break
     dt = (time.perf_counter() - t0) / reps
-    names = ["uxw", "uxb", "jxb", "ugradt"] if args.workload == "mhd_bundle" else ["uxw"]
-    acc = {n: R.rel_l2(sf.to_host(o[:sample]), r) for n, o, r in zip(names, outs, ref)}
     cpu = {"value": sample * m / dt, "unit": UNIT, "cores": cores, "kind": "port",
            "sample": f"{sample} of {npts} points x {m} modes, {reps} reps; pocketfft (scipy.fft) restatement of "
                      "fft_parallel.F90 with all modes on one process (no MPI_ALLTOALL)"}
-    return cpu, {"rel_l2_vs_cpu_port": acc, "sample_points": sample}
+    return cpu, ref, sample
 
 
 def _traffic(workload, form):
