@@ -203,30 +203,70 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
-template <int EK>
+// Geometry of make_geo as constant expressions (the kernels specialise on m).
+__host__ __device__ constexpr int cg_qmin(int m) { return (3 * m - 2 + 3) / 4 < 1 ? 1 : (3 * m - 2 + 3) / 4; }
+__host__ __device__ constexpr int cg_NT(int m) { return (cg_qmin(m) + 7) / 8; }
+__host__ __device__ constexpr int cg_ke(int m, int c) { return (c & 1) ? m / 2 : (m + 1) / 2; }
+__host__ __device__ constexpr int cg_KS(int m, int c) { return (cg_ke(m, c) + 3) / 4; }
+__host__ __device__ constexpr int cg_NU(int m, int c) { return (cg_ke(m, c) + 7) / 8; }
+__host__ __device__ constexpr int cg_ksoff(int m, int c) { return c == 0 ? 0 : cg_ksoff(m, c - 1) + cg_KS(m, c - 1); }
+__host__ __device__ constexpr int cg_nuoff(int m, int c) { return c == 0 ? 0 : cg_nuoff(m, c - 1) + cg_NU(m, c - 1); }
+
+// Element c of a 4-array without dynamic indexing (keeps the arrays in registers).
+__device__ __forceinline__ int sel4(const int (&v)[4], int c) { return c == 0 ? v[0] : c == 1 ? v[1] : c == 2 ? v[2] : v[3]; }
+
+// EK: elementary program; M: modes when specialised (0: any m, geometry at run time);
+// ADJ: 0 plain, 1 first operand (fields 0-2) a cotangent, 2 second operand (fields 3-5) a cotangent.
+template <int EK, int M, int ADJ>
 __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
+  constexpr bool CT = M > 0;
   constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO;
-  extern __shared__ double ps[];  // [NO][4][NT][2][32] folded products, then [NI][KT][8] staged coefficients
+  extern __shared__ double ps[];  // [NO][4][NT][2][32] folded products, then the staged coefficients
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, NW = blockDim.x >> 5;
   const int g = lane >> 2, q = lane & 3;
   const int64_t p0 = (int64_t)blockIdx.x * 8, p = p0 + g;
   const bool valid = p < a.np;
   const int b = blockIdx.y;
-  const int NT = a.NT, KT = a.KT;
-  const double invN = 1.0 / a.N, twoN = 2.0 / a.N;
+  const int NT = CT ? cg_NT(M) : a.NT;
+  int KS[4], KOFF[4], KE[4], NU[4], NOFF[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    KS[c] = CT ? cg_KS(M, c) : a.KS[c];
+    KOFF[c] = CT ? cg_ksoff(M, c) : a.ks_off[c];
+    KE[c] = CT ? cg_ke(M, c) : a.ke[c];
+    NU[c] = CT ? cg_NU(M, c) : a.NU[c];
+    NOFF[c] = CT ? cg_nuoff(M, c) : a.nu_off[c];
+  }
+  const int KS_tot = KS[0] + KS[1] + KS[2] + KS[3], KT = 4 * KS_tot;
+  const int NU_tot = NU[0] + NU[1] + NU[2] + NU[3];
+  int ks_max = KS[0];
+#pragma unroll
+  for (int c = 1; c < 4; ++c) ks_max = KS[c] > ks_max ? KS[c] : ks_max;
+  const double invN = 1.0 / (4.0 * 8.0 * NT), twoN = 2.0 * invN;
 
-  // ---- stage the tile's coefficients: row r of field f = (class c, k), 8 points each ----
+  // ---- stage the tile's coefficients ----
+  // Global row r = 4*ks + q of field f (class c, mode index k = r - 4*KOFF[c]) holds 8 points;
+  // it lands at xs[((f*KS_tot + ks)*8 + point)*4 + q], so that lane (g, q) of a warp reads the
+  // A fragment of k-step ks as xs[(f*KS_tot + ks)*32 + lane]: 256 contiguous bytes.
   double *xs = ps + (size_t)NO * 4 * NT * 2 * 32;
-  for (int idx = threadIdx.x; idx < NI * KT * 8; idx += blockDim.x) {
-    const int pp = idx & 7, fr = idx >> 3, r = fr % KT, f = fr / KT;
-    int c = 0;
-    while (c < 3 && r >= 4 * a.ks_off[c + 1]) ++c;
-    const int k = r - 4 * a.ks_off[c], n = class_mode(c, k);
+  {
+    const int pp = threadIdx.x & 7, rstep = blockDim.x >> 3;
     const int64_t gp = p0 + pp;
-    if (gp < a.np && k < a.ke[c] && !(c == 2 && n == 0))  // the sine of mode 0 is ignored
-      cp_async8(xs + idx, a.in[f] + (int64_t)b * a.in_bs[f] + gp + (int64_t)n * a.in_ldm[f] + (c >= 2 ? a.np : 0));
-    else
-      xs[idx] = 0.0;
+    const bool pv = gp < a.np;
+#pragma unroll
+    for (int f = 0; f < NI; ++f) {
+      const double *base = a.in[f] + (int64_t)b * a.in_bs[f] + (pv ? gp : 0);
+      double *xf = xs + (size_t)f * KS_tot * 32 + pp * 4;
+      for (int r = threadIdx.x >> 3; r < KT; r += rstep) {
+        const int c = (r >= 4 * KOFF[1]) + (r >= 4 * KOFF[2]) + (r >= 4 * KOFF[3]);
+        const int k = r - 4 * sel4(KOFF, c), n = class_mode(c, k);
+        double *dst = xf + (size_t)(r >> 2) * 32 + (r & 3);
+        if (pv && k < sel4(KE, c) && !(c == 2 && n == 0))  // the sine of mode 0 is ignored
+          cp_async8(dst, base + (int64_t)n * a.in_ldm[f] + (c >= 2 ? a.np : 0));
+        else
+          *dst = 0.0;
+      }
+    }
   }
   cp_async_wait_all();
   __syncthreads();
@@ -238,24 +278,27 @@ __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
     for (int f = 0; f < NI; ++f)
 #pragma unroll
       for (int c = 0; c < 4; ++c) acc[f][c][0] = acc[f][c][1] = 0.0;
+    // k-steps outermost, the four classes inside: 4*NI independent accumulator chains per step
+    const double *syn_t = a.syn + (size_t)t * 32 + lane;
+    const double *xs_l = xs + lane;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const double *bt = a.syn + ((size_t)a.ks_off[c] * NT + t) * 32 + lane;
-      const double *xa = xs + (size_t)(4 * a.ks_off[c] + q) * 8 + g;
-      double bv = __ldg(bt);
-#pragma unroll 2
-      for (int s = 0; s < a.KS[c]; ++s) {
-        const double bn = (s + 1 < a.KS[c]) ? __ldg(bt + (size_t)(s + 1) * NT * 32) : 0.0;
-        const int n = class_mode(c, 4 * s + q);
+    for (int s = 0; s < ks_max; ++s) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        if (s >= KS[c]) continue;
+        const double bv = __ldg(syn_t + (size_t)(KOFF[c] + s) * NT * 32);
+        const double *xa = xs_l + (size_t)(KOFF[c] + s) * 32;
         double av[NI];
 #pragma unroll
-        for (int f = 0; f < NI; ++f) {
-          av[f] = xa[(size_t)f * KT * 8 + (size_t)s * 32];
-          if (a.adj_in & (1u << f)) av[f] *= (n == 0 ? invN : twoN);
+        for (int f = 0; f < NI; ++f) av[f] = xa[(size_t)f * KS_tot * 32];
+        if constexpr (ADJ != 0) {
+          const double wn = (s == 0 && q == 0 && (c & 1) == 0) ? invN : twoN;  // n == 0 only there
+#pragma unroll
+          for (int f = 0; f < NI; ++f)
+            if ((ADJ == 1 && f < 3) || (ADJ == 2 && f >= 3)) av[f] *= wn;
         }
 #pragma unroll
         for (int f = 0; f < NI; ++f) dmma(acc[f][c], av[f], bv);
-        bv = bn;
       }
     }
 #pragma unroll
@@ -289,36 +332,31 @@ __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
   __syncthreads();
 
   // ---- analysis: output tiles (class c, tile u) ----
-  const double *anav = a.ana + (size_t)(a.adj_out ? 1 : 0) * a.NU_tot * NT * 2 * 32;
-  for (int cu = warp; cu < a.NU_tot; cu += NW) {
-    int c = 0;
-    while (c < 3 && cu >= a.nu_off[c + 1]) ++c;
-    const int u = cu - a.nu_off[c];
+  const double *anav = a.ana + (size_t)(a.adj_out ? 1 : 0) * NU_tot * NT * 2 * 32 + lane;
+  for (int cu = warp; cu < NU_tot; cu += NW) {
+    const int c = (cu >= NOFF[1]) + (cu >= NOFF[2]) + (cu >= NOFF[3]);
+    const int u = cu - sel4(NOFF, c), kec = sel4(KE, c);
     double y[NO][2];
 #pragma unroll
     for (int o = 0; o < NO; ++o) y[o][0] = y[o][1] = 0.0;
-    const double *bt = anav + (size_t)cu * NT * 2 * 32 + lane;
-    double bv = __ldg(bt);
-#pragma unroll 2
-    for (int te = 0; te < 2 * NT; ++te) {
-      const double bn = (te + 1 < 2 * NT) ? __ldg(bt + (size_t)(te + 1) * 32) : 0.0;
+    const double *bt = anav + (size_t)cu * NT * 2 * 32;
+    const double *pa = ps + (size_t)c * NT * 2 * 32 + lane;
 #pragma unroll
-      for (int o = 0; o < NO; ++o) {
-        const double av = ps[((size_t)(o * 4 + c) * NT * 2 + te) * 32 + lane];
-        dmma(y[o], av, bv);
-      }
-      bv = bn;
+    for (int te = 0; te < 2 * NT; ++te) {
+      const double bv = __ldg(bt + (size_t)te * 32);
+#pragma unroll
+      for (int o = 0; o < NO; ++o) dmma(y[o], pa[((size_t)o * 4 * NT * 2 + te) * 32], bv);
     }
     if (!valid) continue;
 #pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const int kk = 8 * u + 2 * q + i;
-      if (kk >= a.ke[c]) continue;
+    for (int h = 0; h < 2; ++h) {
+      const int kk = 8 * u + 2 * q + h;
+      if (kk >= kec) continue;
       const int n = class_mode(c, kk);
 #pragma unroll
       for (int o = 0; o < NO; ++o) {
         double *dst = a.out[o] + (int64_t)b * a.out_bs[o] + p + (int64_t)n * a.out_ldm[o] + (c >= 2 ? a.np : 0);
-        const double v = (c == 2 && n == 0) ? 0.0 : y[o][i];
+        const double v = (c == 2 && n == 0) ? 0.0 : y[o][h];
         if (a.accumulate)
           *dst += v;
         else
@@ -328,15 +366,15 @@ __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
   }
 }
 
-template <int EK>
-int launch_ek(FastArgs &fa, int batch, cudaStream_t st) {
+template <int EK, int M, int ADJ>
+int launch_ek_m(FastArgs &fa, int batch, cudaStream_t st) {
   constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO;
   fa.KT = 4 * (fa.KS[0] + fa.KS[1] + fa.KS[2] + fa.KS[3]);
   const size_t smem = sizeof(double) * ((size_t)NO * 4 * fa.NT * 2 * 32 + (size_t)NI * fa.KT * 8);
   if (smem > 200 * 1024) return set_error(SFNL_ERR_UNSUPPORTED, "FAST form: m too large for shared memory");
   int nw = fa.NT < 8 ? fa.NT : 8;
   if (nw < 2) nw = 2;
-  auto kern = fast_kernel<EK>;
+  auto kern = fast_kernel<EK, M, ADJ>;
   if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (fast form)");
   const int64_t tiles = (fa.np + 7) / 8;
@@ -344,6 +382,28 @@ int launch_ek(FastArgs &fa, int batch, cudaStream_t st) {
   dim3 grid((unsigned)tiles, (unsigned)batch);
   kern<<<grid, nw * 32, smem, st>>>(fa);
   return check_launch("fast form");
+}
+
+template <int EK, int ADJ>
+int launch_ek_adj(FastArgs &fa, int batch, cudaStream_t st) {
+  switch (fa.m) {
+    case 16: return launch_ek_m<EK, 16, ADJ>(fa, batch, st);
+    case 32: return launch_ek_m<EK, 32, ADJ>(fa, batch, st);
+    case 64: return launch_ek_m<EK, 64, ADJ>(fa, batch, st);
+    default: return launch_ek_m<EK, 0, ADJ>(fa, batch, st);
+  }
+}
+
+template <int EK>
+int launch_ek(FastArgs &fa, int batch, cudaStream_t st) {
+  if constexpr (EK == EK_CROSS) {
+    if (fa.adj_in == 0x07u) return launch_ek_adj<EK, 1>(fa, batch, st);
+    if (fa.adj_in == 0x38u) return launch_ek_adj<EK, 2>(fa, batch, st);
+    if (fa.adj_in != 0u) return set_error(SFNL_ERR_ARG, "FAST form: unsupported cotangent operand");
+  } else {
+    if (fa.adj_in != 0u) return set_error(SFNL_ERR_ARG, "FAST form: unsupported cotangent operand");
+  }
+  return launch_ek_adj<EK, 0>(fa, batch, st);
 }
 
 }  // namespace
