@@ -25,20 +25,24 @@
 // corrections issued before hi x hi.  With 2 slices (3 products) the form
 // is the plain "bf16 hi/lo" split.
 //
-// Tile.  The 128 MMA rows are (field slot, point) pairs: 8 slots x 16 points
-// for cross/dot (6 fields), 4 slots x 32 points for the scalar product.  A
-// row's TMEM accumulators hold its field's four classes at all Q angles
-// (8Q fp32 columns, 384 at m=64).  After the synthesis each thread folds its
-// row to the 4Q physical angles in FP64 and the rows of one point meet in
-// shared memory, 16 quarter-angles at a time, where the pointwise program
-// runs; its folded products, sliced, are the A operand of the analysis,
-// whose 128 rows are (output, point) pairs and which accumulates over the
-// angle chunks in TMEM.
+// Tile.  One launch runs a whole program (the MHD bundle: 15 fields in, 10
+// out).  The 128 MMA rows are (field slot, point) pairs: 16 slots x 8 points
+// for programs with more than 8 input fields, 8 x 16 for the cross and dot
+// products, 4 x 32 for the scalar product.  A row's TMEM accumulators hold its
+// field's four classes at all Q angles (8Q fp32 columns, 384 at m=64).  After
+// the synthesis each row is folded to the 4Q physical angles in FP64 and the
+// rows of one point meet in shared memory, 16 quarter-angles at a time; each
+// output of the pointwise program is a sum of at most four signed products of
+// two fields (a constant term table per program), evaluated by one thread per
+// (output, point, half-chunk).  The folded products, sliced, are the A operand
+// of the analysis, whose rows are (output, point) pairs; each 16-angle chunk is
+// analysed into a fresh accumulator and added in FP64 to the output, which the
+// same thread updates chunk after chunk (the lines stay in L2).
 //
-// One CTA of 4 warps per SM (or two when they fit), persistent over tiles.
-// Thread 0 issues the MMAs; completion is signalled through an mbarrier
-// whose waits are bounded (a timeout sets a status word and abandons the
-// tile instead of spinning forever).
+// One CTA of 8 warps, persistent over tiles; two threads per row.  Thread 0
+// issues the MMAs; completion is signalled through an mbarrier whose waits
+// are bounded (a timeout sets a status word and abandons the tile instead of
+// spinning forever).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -57,7 +61,6 @@ namespace {
 
 constexpr int kW = 8;            // bits of the first slice (integers up to 2^8)
 constexpr int kKeMax = 32;       // modes per class held in registers (m <= 64)
-constexpr int kThreads = 128;
 
 __device__ int g_split_status;   // 0 ok; 1 an mbarrier wait timed out
 
@@ -65,13 +68,12 @@ __device__ int g_split_status;   // 0 ok; 1 an mbarrier wait timed out
 // geometry
 // ---------------------------------------------------------------------------
 struct SGeo {
-  int m, Q, N, NC;
+  int m, Q, N, NC, pts;
   int ke[4], Ks[4], No[4];      // modes per class, K padded to 16, output cols padded to 16
   int Ks_tot, No_tot;
   int tmem_cols, tmem_alloc;
   // shared-memory byte offsets (relative to the dynamic smem base)
-  int off_asyn[4][3], off_bsyn[4][3], off_bana[4][3], off_x, off_aana[4][3], off_sum, off_bar, smem_bytes;
-  int rs;  // analysis rows in use (outputs x points)
+  int off_asyn[4][3], off_bsyn[4][3], off_bana[4][3], off_x, off_aana[4][3], off_bar, smem_bytes;
   int ana_col[4];
 };
 
@@ -81,10 +83,11 @@ int pow2_at_least(int v) {
   return p;
 }
 
-bool make_sgeo(int m, int nslots, int nin, int nout, SGeo *out) {
+bool make_sgeo(int m, int pts, int nin, SGeo *out) {
   SGeo g;
   std::memset(&g, 0, sizeof(g));
   g.m = m;
+  g.pts = pts;
   const int qmin = (3 * m - 2 + 3) / 4;
   g.Q = ((qmin + 15) / 16) * 16;
   if (g.Q < 16) g.Q = 16;
@@ -110,23 +113,19 @@ bool make_sgeo(int m, int nslots, int nin, int nout, SGeo *out) {
     acc += g.No[c];
   }
   // Region 1: synthesis A operands, later overlaid by the exchange buffer and the analysis A operands.
-  const int pts = 128 / nslots;
   int asyn = 0;
   for (int c = 0; c < 4; ++c)
     for (int i = 0; i < 3; ++i) {
       g.off_asyn[c][i] = asyn;
       asyn += 128 * g.Ks[c] * 2;
     }
-  const int xbytes = pts * nin * 64 * 8;
+  const int xbytes = nin * 64 * pts * 8;
   int r1b = xbytes;
   for (int c = 0; c < 4; ++c)
     for (int i = 0; i < 3; ++i) {
       g.off_aana[c][i] = r1b;
       r1b += 128 * 16 * 2;
     }
-  g.rs = nout * pts;
-  g.off_sum = r1b;
-  r1b += g.rs * g.No_tot * 8;
   g.off_x = 0;
   int r1 = asyn > r1b ? asyn : r1b;
   r1 = (r1 + 127) & ~127;
@@ -340,44 +339,73 @@ __device__ __forceinline__ int row_exponent(double mx) {
   return e;
 }
 
+// ---------------------------------------------------------------------------
+// programs: each output is a sum of at most 4 signed products x[a]*x[b]
+// ---------------------------------------------------------------------------
+enum { PR_BUNDLE = 0, PR_CROSS, PR_DOT, PR_PROD, PR_CJVP, PR_CVJP, PR_MVJP, PR_COUNT };
+
+struct STerm {
+  signed char a, b, s;
+};
+#define T2(a0, b0, a1, b1) {{a0, b0, 1}, {a1, b1, -1}, {0, 0, 0}, {0, 0, 0}}
+#define T4(a0, b0, a1, b1, a2, b2, a3, b3) {{a0, b0, 1}, {a1, b1, -1}, {a2, b2, 1}, {a3, b3, -1}}
+__constant__ STerm c_terms[PR_COUNT][10][4] = {
+    // bundle [u 0-2, w 3-5, b 6-8, j 9-11, gradT 12-14] -> [u x w, u x b, j x b, u . gradT]
+    {T2(1, 5, 2, 4), T2(2, 3, 0, 5), T2(0, 4, 1, 3), T2(1, 8, 2, 7), T2(2, 6, 0, 8), T2(0, 7, 1, 6),
+     T2(10, 8, 11, 7), T2(11, 6, 9, 8), T2(9, 7, 10, 6), {{0, 12, 1}, {1, 13, 1}, {2, 14, 1}, {0, 0, 0}}},
+    // cross [v1 0-2, v2 3-5] -> v1 x v2
+    {T2(1, 5, 2, 4), T2(2, 3, 0, 5), T2(0, 4, 1, 3)},
+    // dot -> v1 . v2
+    {{{0, 3, 1}, {1, 4, 1}, {2, 5, 1}, {0, 0, 0}}},
+    // scalar product
+    {{{0, 1, 1}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}}},
+    // linearised cross [u 0-2, w 3-5, du 6-8, dw 9-11] -> du x w + u x dw
+    {T4(7, 5, 8, 4, 1, 11, 2, 10), T4(8, 3, 6, 5, 2, 9, 0, 11), T4(6, 4, 7, 3, 0, 10, 1, 9)},
+    // its transpose [u 0-2, w 3-5, c 6-8] -> [w x c, c x u]
+    {T2(4, 8, 5, 7), T2(5, 6, 3, 8), T2(3, 7, 4, 6), T2(7, 2, 8, 1), T2(8, 0, 6, 2), T2(6, 1, 7, 0)},
+    // transpose of (du x w + u x dw, du x b + u x db): [u, w, b, c1 9-11, c2 12-14] -> [w x c1 + b x c2, c1 x u, c2 x u]
+    {T4(4, 11, 5, 10, 7, 14, 8, 13), T4(5, 9, 3, 11, 8, 12, 6, 14), T4(3, 10, 4, 9, 6, 13, 7, 12),
+     T2(10, 2, 11, 1), T2(11, 0, 9, 2), T2(9, 1, 10, 0), T2(13, 2, 14, 1), T2(14, 0, 12, 2), T2(12, 1, 13, 0)},
+};
+#undef T2
+#undef T4
+
+__host__ __device__ constexpr int pr_nin(int pr) {
+  return pr == PR_BUNDLE ? 15 : pr == PR_CROSS ? 6 : pr == PR_DOT ? 6 : pr == PR_PROD ? 2 : pr == PR_CJVP ? 12
+       : pr == PR_CVJP ? 9 : 15;
+}
+__host__ __device__ constexpr int pr_nout(int pr) {
+  return pr == PR_BUNDLE ? 10 : pr == PR_CROSS ? 3 : pr == PR_DOT ? 1 : pr == PR_PROD ? 1 : pr == PR_CJVP ? 3
+       : pr == PR_CVJP ? 6 : 9;
+}
+__host__ __device__ constexpr int pr_slots(int pr) { return pr_nin(pr) > 8 ? 16 : pr_nin(pr) > 4 ? 8 : 4; }
+__host__ __device__ constexpr int pr_pts(int pr) { return 128 / pr_slots(pr); }
+// cotangent inputs (synthesised with the analysis weights) and transposed outputs (analysed without them)
+__host__ __device__ constexpr unsigned pr_adj_in(int pr) { return pr == PR_CVJP ? 0x1C0u : pr == PR_MVJP ? 0x7E00u : 0u; }
+__host__ __device__ constexpr bool pr_adj_out(int pr) { return pr == PR_CVJP || pr == PR_MVJP; }
+
 struct SplitArgs {
-  const double *in[6];
-  double *out[3];
-  int64_t in_ldm[6], out_ldm[3], in_bs[6], out_bs[3];
+  const double *in[16];
+  double *out[10];
+  int64_t in_ldm[16], out_ldm[10], in_bs[16], out_bs[10];
   int64_t np;
-  int batch;
-  unsigned adj_in;
-  int adj_out, accumulate, nsl;
+  int nsl;
   SGeo g;
   const void *bsyn, *bana;
   int bsyn_bytes, bana_bytes;
 };
 
-template <int EK>
-struct SDef;
-template <>
-struct SDef<EK_CROSS> {
-  static constexpr int NI = 6, NO = 3, SLOTS = 8;
-  __device__ static void op(const double *x, double *y) { cross3(x, x + 3, y); }
-};
-template <>
-struct SDef<EK_DOT> {
-  static constexpr int NI = 6, NO = 1, SLOTS = 8;
-  __device__ static void op(const double *x, double *y) { y[0] = x[0] * x[3] + x[1] * x[4] + x[2] * x[5]; }
-};
-template <>
-struct SDef<EK_PROD> {
-  static constexpr int NI = 2, NO = 1, SLOTS = 4;
-  __device__ static void op(const double *x, double *y) { y[0] = x[0] * x[1]; }
-};
+constexpr int kThreads = 256;
 
-template <int EK>
+template <int PR>
 __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
-  constexpr int NI = SDef<EK>::NI, NO = SDef<EK>::NO, SLOTS = SDef<EK>::SLOTS, PTS = 128 / SLOTS;
+  constexpr int NI = pr_nin(PR), NO = pr_nout(PR), PTS = pr_pts(PR);
+  constexpr unsigned ADJ = pr_adj_in(PR);
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ uint32_t s_tmem;
   const SGeo &g = a.g;
   const int t = threadIdx.x, warp = t >> 5;
+  const int row = t & 127, half = t >> 7;  // TMEM lane = row (warp w reads lanes 32*(w%4)..)
   const uint32_t mbar = smem_u32(sm + g.off_bar);
 
   // ---- setup: TMEM, mbarrier, DFT tables ----
@@ -390,12 +418,10 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
   {
     const uint4 *src = reinterpret_cast<const uint4 *>(a.bsyn);
     uint4 *dst = reinterpret_cast<uint4 *>(sm + g.off_bsyn[0][0]);
-    const int n16 = a.bsyn_bytes / 16;
-    for (int i = t; i < n16; i += kThreads) dst[i] = src[i];
+    for (int i = t; i < a.bsyn_bytes / 16; i += kThreads) dst[i] = src[i];
     const uint4 *src2 = reinterpret_cast<const uint4 *>(a.bana);
     uint4 *dst2 = reinterpret_cast<uint4 *>(sm + g.off_bana[0][0]);
-    const int n16b = a.bana_bytes / 16;
-    for (int i = t; i < n16b; i += kThreads) dst2[i] = src2[i];
+    for (int i = t; i < a.bana_bytes / 16; i += kThreads) dst2[i] = src2[i];
   }
   fence_async_smem();
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -403,25 +429,52 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s_tmem;
-  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+  const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
   uint32_t phase = 0;
   bool ok = true;
 
-  const int b = blockIdx.y;
   const int64_t ntiles = (a.np + PTS - 1) / PTS;
   const double invN = 1.0 / g.N, twoN = 2.0 / g.N;
   const int npairs = a.nsl == 3 ? 6 : 3;
+  double *X = reinterpret_cast<double *>(sm + g.off_x);  // [f][quadrant][16][PTS], point fastest
+
+  // Reads the analysis of one chunk and adds it (weighted) to the outputs: row = (o, p), half = class pair.
+  auto flush_chunk = [&](int64_t tile, int chk) {
+    const int o = row / PTS, p = row % PTS;
+    const int64_t gp = tile * PTS + p;
+    const bool live = row < NO * PTS && gp < a.np;
+#pragma unroll 1
+    for (int c = 2 * half; c < 2 * half + 2; ++c) {
+      for (int k0 = 0; k0 < g.No[c]; k0 += 8) {
+        float v[8];
+        tmem_ld8(tmem + lane_base + (uint32_t)(g.ana_col[c] + k0), v);
+        tmem_wait_ld();
+        if (!live) continue;
+        double *dst = a.out[o] + gp + (c >= 2 ? a.np : 0);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const int kk = k0 + e;
+          if (kk >= g.ke[c]) continue;
+          const int n = 2 * kk + (c & 1);
+          const double sc = pr_adj_out(PR) ? 1.0 : (n == 0 ? invN : twoN);
+          const double val = (c == 2 && n == 0) ? 0.0 : (double)v[e] * sc;
+          double *q = dst + (int64_t)n * a.out_ldm[o];
+          *q = (chk == 0 ? 0.0 : *q) + val;
+        }
+      }
+    }
+  };
 
   for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    // ---- 1. load + slice the input rows (row t = field slot f, point p) ----
+    // ---- 1. load + slice the input rows: row = field slot f, point p; half = class pair ----
     {
-      const int f = t / PTS, p = t % PTS;
+      const int f = row / PTS, p = row % PTS;
       const int64_t gp = tile * PTS + p;
       const bool valid = f < NI && gp < a.np;
-      const double *src = valid ? a.in[f] + (int64_t)b * a.in_bs[f] + gp : nullptr;
-      const double dsc = (f < NI && (a.adj_in >> f) & 1u) ? 1.0 : 0.0;  // 1: cotangent row
+      const double *src = valid ? a.in[f] + gp : nullptr;
+      const bool cot = f < NI && ((ADJ >> f) & 1u);
 #pragma unroll 1
-      for (int c = 0; c < 4; ++c) {
+      for (int c = 2 * half; c < 2 * half + 2; ++c) {
         double x[kKeMax];
         double mx = 0.0;
 #pragma unroll
@@ -430,7 +483,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
           const int n = 2 * k + (c & 1);
           if (valid && k < g.ke[c] && !(c == 2 && n == 0)) {
             double v = __ldg(src + (int64_t)n * a.in_ldm[f] + (c >= 2 ? a.np : 0));
-            if (dsc != 0.0) v *= (n == 0 ? invN : twoN);
+            if (cot) v *= (n == 0 ? invN : twoN);
             x[k] = v;
             mx = fmax(mx, fabs(v));
           }
@@ -455,7 +508,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
             w[1][q] = bf16_bits(s1[0]) | (bf16_bits(s1[1]) << 16);
             w[2][q] = bf16_bits(s2[0]) | (bf16_bits(s2[1]) << 16);
           }
-          const size_t off = (size_t)(t / 8) * (16 * K) + (size_t)kg * 128 + (size_t)(t % 8) * 16;
+          const size_t off = (size_t)(row / 8) * (16 * K) + (size_t)kg * 128 + (size_t)(row % 8) * 16;
 #pragma unroll
           for (int i = 0; i < 3; ++i)
             *reinterpret_cast<uint4 *>(sm + g.off_asyn[c][i] + off) = make_uint4(w[i][0], w[i][1], w[i][2], w[i][3]);
@@ -470,12 +523,12 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
     if (t == 0) {
       tc_fence_after();
       const uint32_t idesc = make_idesc(g.Q);
-      static const int pi_[6] = {0, 0, 1, 0, 1, 2}, pj_[6] = {0, 1, 0, 2, 1, 0};
       for (int c = 0; c < 4; ++c) {
         const uint32_t sbo = 16 * g.Ks[c];
         for (int s = 0; s < g.Ks[c] / 16; ++s)
           for (int pr = 0; pr < npairs; ++pr) {
-            const int i = pi_[pr], j = pj_[pr];
+            const int i = pr == 0 ? 0 : pr == 1 ? 0 : pr == 2 ? 1 : pr == 3 ? 0 : pr == 4 ? 1 : 2;
+            const int j = pr == 0 ? 0 : pr == 1 ? 1 : pr == 2 ? 0 : pr == 3 ? 2 : pr == 4 ? 1 : 0;
             const int accn = (i + j == 0) ? 0 : 1;
             const uint32_t dcol = tmem + (uint32_t)((c * 2 + accn) * g.Q);
             const uint64_t ad = make_sdesc(smem_u32(sm + g.off_asyn[c][i]) + 256 * s, 128, sbo);
@@ -494,58 +547,36 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
     phase ^= 1;
     tc_fence_after();
 
-    double *X = reinterpret_cast<double *>(sm + g.off_x);  // [f][quadrant][16][p], point fastest
-    double *sums = reinterpret_cast<double *>(sm + g.off_sum);  // [analysis column][row]
-    // Adds the analysis of one chunk (TMEM, fp32) to the FP64 sums of the thread's row.
-    auto add_chunk = [&](int chk) {
-#pragma unroll 1
-      for (int col = 0; col < g.No_tot; col += 8) {
-        float v[8];
-        tmem_ld8(tmem + lane_base + (uint32_t)(8 * g.Q + col), v);
-        tmem_wait_ld();
-        if (t < g.rs) {
-#pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            double *sp = sums + (size_t)(col + e) * g.rs + t;
-            *sp = (chk == 0 ? 0.0 : *sp) + (double)v[e];
-          }
-        }
-      }
-    };
     for (int ch = 0; ch < g.NC && ok; ++ch) {
-      // ---- 3a. read out, recombine in FP64, fold to the 4 quadrant angles ----
+      // ---- 3a. read out, recombine in FP64, fold to the 4 quadrant angles (half = 8 quarter-angles) ----
       {
-        const int f = t / PTS, p = t % PTS;
-#pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
-          float d[4][2][8];
+        const int f = row / PTS, p = row % PTS;
+        float d[4][2][8];
 #pragma unroll
-          for (int c = 0; c < 4; ++c)
+        for (int c = 0; c < 4; ++c)
 #pragma unroll
-            for (int ac = 0; ac < 2; ++ac)
-              tmem_ld8(tmem + lane_base + (uint32_t)((c * 2 + ac) * g.Q + ch * 16 + h * 8), d[c][ac]);
-          tmem_wait_ld();
-          if (f < NI) {
-            double *xr = X + (size_t)f * 64 * PTS + p;
+          for (int ac = 0; ac < 2; ++ac)
+            tmem_ld8(tmem + lane_base + (uint32_t)((c * 2 + ac) * g.Q + ch * 16 + half * 8), d[c][ac]);
+        tmem_wait_ld();
+        if (f < NI) {
+          double *xr = X + (size_t)f * 64 * PTS + (size_t)half * 8 * PTS + p;
 #pragma unroll
-            for (int jj = 0; jj < 8; ++jj) {
-              const double CE = (double)d[0][0][jj] + (double)d[0][1][jj];
-              const double CO = (double)d[1][0][jj] + (double)d[1][1][jj];
-              const double SE = (double)d[2][0][jj] + (double)d[2][1][jj];
-              const double SO = (double)d[3][0][jj] + (double)d[3][1][jj];
-              const double A = CE + CO, B = CE - CO, C = SE + SO, D = SO - SE;
-              const int j = h * 8 + jj;
-              xr[(0 * 16 + j) * PTS] = A + C;  // theta
-              xr[(1 * 16 + j) * PTS] = B + D;  // pi - theta
-              xr[(2 * 16 + j) * PTS] = B - D;  // pi + theta
-              xr[(3 * 16 + j) * PTS] = A - C;  // 2 pi - theta
-            }
+          for (int jj = 0; jj < 8; ++jj) {
+            const double CE = (double)d[0][0][jj] + (double)d[0][1][jj];
+            const double CO = (double)d[1][0][jj] + (double)d[1][1][jj];
+            const double SE = (double)d[2][0][jj] + (double)d[2][1][jj];
+            const double SO = (double)d[3][0][jj] + (double)d[3][1][jj];
+            const double A = CE + CO, B = CE - CO, C = SE + SO, D = SO - SE;
+            xr[(0 * 16 + jj) * PTS] = A + C;  // theta
+            xr[(1 * 16 + jj) * PTS] = B + D;  // pi - theta
+            xr[(2 * 16 + jj) * PTS] = B - D;  // pi + theta
+            xr[(3 * 16 + jj) * PTS] = A - C;  // 2 pi - theta
           }
         }
       }
       tc_fence_before();
       __syncthreads();
-      // The previous chunk's analysis must be complete: fold it into the FP64 sums.
+      // The previous chunk's analysis must be complete before its A operand is rewritten.
       if (ch > 0) {
         if (!mbar_wait(mbar, phase)) {
           ok = false;
@@ -553,48 +584,58 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
         }
         phase ^= 1;
         tc_fence_after();
-        add_chunk(ch - 1);
+        flush_chunk(tile, ch - 1);
       }
-      // ---- 3b. pointwise program, analysis pre-fold, slicing (row t = output o, point p) ----
-      if (t < NO * PTS) {
-        const int o = t / PTS, p = t % PTS;
-        double P[4][16];
+      // ---- 3b. program, analysis pre-fold, slicing: thread = (output o, point p, half of the chunk) ----
+      {
+        const int jh = t & 1, op = t >> 1, o = op / PTS, p = op % PTS;
+        const bool live = o < NO;
+        double P[4][8];
+        double mx[4] = {0.0, 0.0, 0.0, 0.0};
+        if (live) {
+          STerm tm[4];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          double gq[4];
+          for (int u = 0; u < 4; ++u) tm[u] = c_terms[PR][o][u];
 #pragma unroll
-          for (int r = 0; r < 4; ++r) {
-            double xv[NI], yv[NO];
+          for (int jj = 0; jj < 8; ++jj) {
+            const int j = jh * 8 + jj;
+            double gq[4];
 #pragma unroll
-            for (int f = 0; f < NI; ++f) xv[f] = X[((size_t)(f * 4 + r) * 16 + j) * PTS + p];
-            SDef<EK>::op(xv, yv);
-            gq[r] = yv[0];
+            for (int r = 0; r < 4; ++r) {
+              double acc = 0.0;
 #pragma unroll
-            for (int oo = 1; oo < NO; ++oo)
-              if (oo == o) gq[r] = yv[oo];
+              for (int u = 0; u < 4; ++u) {
+                if (tm[u].s == 0) continue;
+                const double xa = X[((size_t)tm[u].a * 64 + r * 16 + j) * PTS + p];
+                const double xb = X[((size_t)tm[u].b * 64 + r * 16 + j) * PTS + p];
+                acc = fma(tm[u].s > 0 ? xa : -xa, xb, acc);
+              }
+              gq[r] = acc;
+            }
+            const double s14 = gq[0] + gq[3], d14 = gq[0] - gq[3], s23 = gq[1] + gq[2], d32 = gq[2] - gq[1];
+            P[0][jj] = s14 + s23;
+            P[1][jj] = s14 - s23;
+            P[2][jj] = d14 + d32;
+            P[3][jj] = d14 - d32;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) mx[c] = fmax(mx[c], fabs(P[c][jj]));
           }
-          const double s14 = gq[0] + gq[3], d14 = gq[0] - gq[3], s23 = gq[1] + gq[2], d32 = gq[2] - gq[1];
-          P[0][j] = s14 + s23;
-          P[1][j] = s14 - s23;
-          P[2][j] = d14 + d32;
-          P[3][j] = d14 - d32;
         }
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          double mx = 0.0;
+        for (int c = 0; c < 4; ++c) mx[c] = fmax(mx[c], __shfl_xor_sync(0xffffffffu, mx[c], 1));
+        if (live) {
+          const int ro = o * PTS + p;
 #pragma unroll
-          for (int j = 0; j < 16; ++j) mx = fmax(mx, fabs(P[c][j]));
-          const int E = row_exponent(mx);
-#pragma unroll
-          for (int kg = 0; kg < 2; ++kg) {
+          for (int c = 0; c < 4; ++c) {
+            const int E = row_exponent(mx[c]);
             uint32_t w[3][4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
               double s0[2], s1[2], s2[2];
 #pragma unroll
               for (int e = 0; e < 2; ++e) {
-                if (mx > 0.0)
-                  slice3(P[c][kg * 8 + 2 * q + e], E, s0[e], s1[e], s2[e]);
+                if (mx[c] > 0.0)
+                  slice3(P[c][2 * q + e], E, s0[e], s1[e], s2[e]);
                 else
                   s0[e] = s1[e] = s2[e] = 0.0;
               }
@@ -602,7 +643,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
               w[1][q] = bf16_bits(s1[0]) | (bf16_bits(s1[1]) << 16);
               w[2][q] = bf16_bits(s2[0]) | (bf16_bits(s2[1]) << 16);
             }
-            const size_t off = (size_t)(t / 8) * 256 + (size_t)kg * 128 + (size_t)(t % 8) * 16;
+            const size_t off = (size_t)(ro / 8) * 256 + (size_t)jh * 128 + (size_t)(ro % 8) * 16;
 #pragma unroll
             for (int i = 0; i < 3; ++i)
               *reinterpret_cast<uint4 *>(sm + g.off_aana[c][i] + off) = make_uint4(w[i][0], w[i][1], w[i][2], w[i][3]);
@@ -612,27 +653,31 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
       fence_async_smem();
       tc_fence_before();
       __syncthreads();
-      // ---- 3c. analysis MMAs for this chunk (corrections first, then hi x hi) ----
+      // ---- 3c. analysis MMAs for this chunk, fresh accumulator (corrections first, then hi x hi) ----
       if (t == 0 && ok) {
         tc_fence_after();
-        static const int qi_[6] = {0, 1, 0, 1, 2, 0}, qj_[6] = {1, 0, 2, 1, 0, 0};
-        static const int ri_[3] = {0, 1, 0}, rj_[3] = {1, 0, 0};
         for (int c = 0; c < 4; ++c) {
           const uint32_t idesc = make_idesc(g.No[c]);
           const uint32_t dcol = tmem + (uint32_t)g.ana_col[c];
           for (int pr = 0; pr < npairs; ++pr) {
-            const int i = a.nsl == 3 ? qi_[pr] : ri_[pr], j = a.nsl == 3 ? qj_[pr] : rj_[pr];
+            int i, j;
+            if (a.nsl == 3) {
+              i = pr == 0 ? 0 : pr == 1 ? 1 : pr == 2 ? 0 : pr == 3 ? 1 : pr == 4 ? 2 : 0;
+              j = pr == 0 ? 1 : pr == 1 ? 0 : pr == 2 ? 2 : pr == 3 ? 1 : pr == 4 ? 0 : 0;
+            } else {
+              i = pr == 1 ? 1 : 0;
+              j = pr == 0 ? 1 : 0;
+            }
             const uint64_t ad = make_sdesc(smem_u32(sm + g.off_aana[c][i]), 128, 256);
             const uint64_t bd = make_sdesc(smem_u32(sm + g.off_bana[c][j]) + 256 * ch, 128, 16 * g.Q);
-            const uint32_t en = pr > 0 ? 1u : 0u;  // each chunk starts a fresh accumulator
-            umma_bf16(dcol, ad, bd, idesc, en);
+            umma_bf16(dcol, ad, bd, idesc, pr > 0 ? 1u : 0u);
           }
         }
         umma_commit(mbar);
       }
       __syncwarp();
     }
-    // ---- 4. last chunk into the sums, then the store: row t = (output o, point p) ----
+    // ---- 4. the last chunk into the outputs ----
     if (ok) {
       if (!mbar_wait(mbar, phase)) {
         ok = false;
@@ -641,28 +686,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
       phase ^= 1;
     }
     tc_fence_after();
-    if (ok) add_chunk(g.NC - 1);
-    __syncthreads();
-    if (ok) {
-      // rows t = o*PTS + p; a warp covers 32 consecutive rows -> consecutive points of one output
-      for (int idx = t; idx < g.rs * g.No_tot; idx += kThreads) {
-        const int row = idx % g.rs, col = idx / g.rs;
-        const int o = row / PTS, p = row % PTS;
-        int c = 0;
-        while (c < 3 && col >= g.ana_col[c + 1] - 8 * g.Q) ++c;
-        const int kk = col - (g.ana_col[c] - 8 * g.Q);
-        const int64_t gp = tile * PTS + p;
-        if (kk >= g.ke[c] || gp >= a.np) continue;
-        const int n = 2 * kk + (c & 1);
-        const double sc = a.adj_out ? 1.0 : (n == 0 ? invN : twoN);
-        const double val = (c == 2 && n == 0) ? 0.0 : sums[idx] * sc;
-        double *q = a.out[o] + (int64_t)b * a.out_bs[o] + gp + (int64_t)n * a.out_ldm[o] + (c >= 2 ? a.np : 0);
-        if (a.accumulate)
-          *q += val;
-        else
-          *q = val;
-      }
-    }
+    if (ok) flush_chunk(tile, g.NC - 1);
     tc_fence_before();
     __syncthreads();
   }
@@ -673,15 +697,14 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
   }
 }
 
-template <int EK>
-int launch_split_ek(SplitArgs &sa, cudaStream_t st) {
-  constexpr int SLOTS = SDef<EK>::SLOTS, PTS = 128 / SLOTS;
-  auto kern = split_kernel<EK>;
+template <int PR>
+int launch_split_pr(SplitArgs &sa, int batch, const ProgArgs &pa, const int *in_map, const int *out_map,
+                    cudaStream_t st) {
+  constexpr int NI = pr_nin(PR), NO = pr_nout(PR), PTS = pr_pts(PR);
+  auto kern = split_kernel<PR>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sa.g.smem_bytes) != cudaSuccess)
     return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (split form)");
   const int64_t ntiles = (sa.np + PTS - 1) / PTS;
-  // Keep the per-SM TMEM demand within its 512 columns: at most 512/alloc CTAs per SM,
-  // also bounded by shared memory.
   int per_sm_tmem = 512 / sa.g.tmem_alloc;
   int per_sm_smem = (int)((228 * 1024) / (sa.g.smem_bytes + 1024));
   int per_sm = per_sm_tmem < per_sm_smem ? per_sm_tmem : per_sm_smem;
@@ -689,9 +712,39 @@ int launch_split_ek(SplitArgs &sa, cudaStream_t st) {
   int64_t grid = (int64_t)num_sms() * per_sm;
   if (grid > ntiles) grid = ntiles;
   if (grid < 1) grid = 1;
-  dim3 gdim((unsigned)grid, (unsigned)sa.batch);
-  kern<<<gdim, kThreads, sa.g.smem_bytes, st>>>(sa);
-  return check_launch("split form");
+  for (int b = 0; b < batch; ++b) {
+    for (int i = 0; i < NI; ++i) {
+      sa.in[i] = pa.in[in_map[i]] + (int64_t)b * pa.in_bs[in_map[i]];
+      sa.in_ldm[i] = pa.in_ldm[in_map[i]];
+    }
+    for (int o = 0; o < NO; ++o) {
+      sa.out[o] = pa.out[out_map[o]] + (int64_t)b * pa.out_bs[out_map[o]];
+      sa.out_ldm[o] = pa.out_ldm[out_map[o]];
+    }
+    kern<<<(unsigned)grid, kThreads, sa.g.smem_bytes, st>>>(sa);
+    int rc = check_launch("split form");
+    if (rc) return rc;
+  }
+  return SFNL_OK;
+}
+
+template <int PR>
+int run_split_program(const ProgArgs &pa, int split, const int *in_map, const int *out_map, cudaStream_t st) {
+  SplitArgs sa;
+  std::memset(&sa, 0, sizeof(sa));
+  if (!make_sgeo(pa.m, pr_pts(PR), pr_nin(PR), &sa.g)) return set_error(SFNL_ERR_UNSUPPORTED, "split form: m too large");
+  STables T;
+  int rc = get_stables(sa.g, &T);
+  if (rc) return rc;
+  sa.np = pa.np;
+  sa.nsl = split;
+  sa.bsyn = T.bsyn;
+  sa.bana = T.bana;
+  sa.bsyn_bytes = (int)T.bsyn_bytes;
+  sa.bana_bytes = (int)T.bana_bytes;
+  if (sa.g.off_bsyn[0][0] + sa.bsyn_bytes != sa.g.off_bana[0][0] || sa.g.off_bana[0][0] + sa.bana_bytes > sa.g.off_bar)
+    return set_error(SFNL_ERR_UNSUPPORTED, "split form: table layout mismatch");
+  return launch_split_pr<PR>(sa, pa.batch, pa, in_map, out_map, st);
 }
 
 }  // namespace
@@ -700,52 +753,29 @@ bool split_supported(int op, int m) {
   (void)op;
   if (m < 1 || m > 64) return false;
   SGeo g;
-  return make_sgeo(m, 8, 6, 3, &g) && make_sgeo(m, 8, 6, 1, &g) && make_sgeo(m, 4, 2, 1, &g);
+  return make_sgeo(m, 8, 16, &g) && make_sgeo(m, 16, 8, &g) && make_sgeo(m, 32, 4, &g);
 }
 
 int launch_split(const ProgArgs &a, int split, cudaStream_t st) {
   if (a.np == 0) return SFNL_OK;
-  std::vector<Elem> seq;
-  int rc = decompose_program(a.op, seq);
-  if (rc) return rc;
-  const bool adj_out = op_adjoint_out(a.op);
-  for (const Elem &e : seq) {
-    const int nslots = e.ek == EK_PROD ? 4 : 8, nin = e.ek == EK_PROD ? 2 : 6, nout = e.ek == EK_CROSS ? 3 : 1;
-    SplitArgs sa;
-    std::memset(&sa, 0, sizeof(sa));
-    if (!make_sgeo(a.m, nslots, nin, nout, &sa.g)) return set_error(SFNL_ERR_UNSUPPORTED, "split form: m too large");
-    STables T;
-    rc = get_stables(sa.g, &T);
-    if (rc) return rc;
-    const int no = e.ek == EK_CROSS ? 3 : 1;
-    for (int i = 0; i < nin; ++i) {
-      sa.in[i] = a.in[e.in[i]];
-      sa.in_ldm[i] = a.in_ldm[e.in[i]];
-      sa.in_bs[i] = a.in_bs[e.in[i]];
+  static const int id[16] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15};
+  switch (a.op) {
+    case OP_BUNDLE: return run_split_program<PR_BUNDLE>(a, split, id, id, st);
+    case OP_CROSS: return run_split_program<PR_CROSS>(a, split, id, id, st);
+    case OP_DOT: return run_split_program<PR_DOT>(a, split, id, id, st);
+    case OP_PROD: return run_split_program<PR_PROD>(a, split, id, id, st);
+    case OP_CROSS_JVP: return run_split_program<PR_CJVP>(a, split, id, id, st);
+    case OP_CROSS_VJP: return run_split_program<PR_CVJP>(a, split, id, id, st);
+    case OP_MHD_VJP: return run_split_program<PR_MVJP>(a, split, id, id, st);
+    case OP_MHD_JVP: {  // [u, w, b, du, dw, db] -> two linearised cross products with disjoint outputs
+      static const int in1[12] = {0, 1, 2, 3, 4, 5, 9, 10, 11, 12, 13, 14}, out1[3] = {0, 1, 2};
+      static const int in2[12] = {0, 1, 2, 6, 7, 8, 9, 10, 11, 15, 16, 17}, out2[3] = {3, 4, 5};
+      int rc = run_split_program<PR_CJVP>(a, split, in1, out1, st);
+      if (rc) return rc;
+      return run_split_program<PR_CJVP>(a, split, in2, out2, st);
     }
-    for (int o = 0; o < no; ++o) {
-      sa.out[o] = a.out[e.out[o]];
-      sa.out_ldm[o] = a.out_ldm[e.out[o]];
-      sa.out_bs[o] = a.out_bs[e.out[o]];
-    }
-    sa.np = a.np;
-    sa.batch = a.batch;
-    sa.adj_in = e.adj;
-    sa.adj_out = adj_out ? 1 : 0;
-    sa.accumulate = e.acc;
-    sa.nsl = split;
-    sa.bsyn = T.bsyn;
-    sa.bana = T.bana;
-    sa.bsyn_bytes = (int)T.bsyn_bytes;
-    sa.bana_bytes = (int)T.bana_bytes;
-    if (sa.g.off_bsyn[0][0] + sa.bsyn_bytes != sa.g.off_bana[0][0] || sa.g.off_bana[0][0] + sa.bana_bytes > sa.g.off_bar)
-      return set_error(SFNL_ERR_UNSUPPORTED, "split form: table layout mismatch");
-    rc = e.ek == EK_CROSS ? launch_split_ek<EK_CROSS>(sa, st)
-       : e.ek == EK_DOT   ? launch_split_ek<EK_DOT>(sa, st)
-                          : launch_split_ek<EK_PROD>(sa, st);
-    if (rc) return rc;
   }
-  return SFNL_OK;
+  return set_error(SFNL_ERR_ARG, "unknown program");
 }
 
 int split_status_and_clear() {
