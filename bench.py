@@ -408,12 +408,16 @@ def _cpu_baseline(args, ins, npts, m, pad):
 
 
 def _traffic(workload, form):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary (profiles/traffic_per_launch.txt)."""
     try:
-        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            t = json.load(f)
-        return t.get(f"{workload}:{form}")
-    except Exception:
-        return None
+        with open(os.path.join(ROOT, "profiles", "traffic_per_launch.txt")) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 2 and parts[0] == f"{workload}:{form}":
+                    return float(parts[1])
+    except OSError:
+        pass
+    return None
 
 
 if __name__ == "__main__":

@@ -1,0 +1,62 @@
+"""Time one program of the library on synthetic data (the command the ncu captures use).
+
+    python -m sfemans_b200.profile_case --program bundle --form fast --np 100000 --m 64 --reps 1
+
+Programs: cross, dot, prod (the three reference routines) and bundle (u x w, u x b, j x b, u . gradT).
+Forms: fast (FP64, folded transforms), grid (FP64, caller's grid), split3 / split2 (bf16 slices on tcgen05).
+Inputs are N(0,1)*exp(-alpha*n) coefficients generated on the device; the padding is m_max_pad = 3*m/2.
+Prints the average milliseconds per call, timed with CUDA events after one untimed call.
+"""
+from __future__ import annotations
+
+import argparse
+
+
+def _field(torch, npts, nslot, m, alpha, seed):
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    t = torch.randn((m, nslot, npts), generator=g, device="cuda", dtype=torch.float64)
+    t *= torch.exp(-alpha * torch.arange(m, device="cuda", dtype=torch.float64))[:, None, None]
+    t[0, 1::2, :] = 0.0
+    return t.permute(2, 1, 0)
+
+
+def main(argv=None):
+    import torch
+
+    import sfemans_b200 as sf
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--program", default="cross", choices=["cross", "dot", "prod", "bundle"])
+    ap.add_argument("--form", default="fast", choices=["fast", "grid", "split3", "split2"])
+    ap.add_argument("--np", type=int, default=100_000)
+    ap.add_argument("--m", type=int, default=64)
+    ap.add_argument("--alpha", type=float, default=0.1)
+    ap.add_argument("--reps", type=int, default=3)
+    a = ap.parse_args(argv)
+    kw = {"fast": dict(algo=sf.ALGO_FAST), "grid": dict(algo=sf.ALGO_GRID), "split3": dict(split=sf.SPLIT_BF16X3),
+          "split2": dict(split=sf.SPLIT_BF16X2)}[a.form]
+    pad = 3 * a.m // 2 if a.m > 1 else 1
+    if a.program == "bundle":
+        ins = [_field(torch, a.np, 6, a.m, a.alpha, 10 + i) for i in range(5)]
+        outs = tuple(sf.fortran_empty(a.np, 6, a.m) for _ in range(3)) + (sf.fortran_empty(a.np, 2, a.m),)
+        call = lambda: sf.bundle_mhd(*ins, m_max_pad=pad, outs=outs, **kw)  # noqa: E731
+    else:
+        op = {"cross": sf.OP_CROSS, "dot": sf.OP_DOT, "prod": sf.OP_PROD}[a.program]
+        nsl = 2 if op == sf.OP_PROD else 6
+        x, y = _field(torch, a.np, nsl, a.m, a.alpha, 1), _field(torch, a.np, nsl, a.m, a.alpha, 2)
+        out = sf.fortran_empty(a.np, 6 if op == sf.OP_CROSS else 2, a.m)
+        call = lambda: sf.product(op, x, y, out=out, m_max_pad=pad, **kw)  # noqa: E731
+    call()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.reps):
+        call()
+    e1.record()
+    torch.cuda.synchronize()
+    print(f"{a.program} {a.form} np={a.np} m={a.m}: {e0.elapsed_time(e1) / a.reps:.4f} ms/call", flush=True)
+
+
+if __name__ == "__main__":
+    main()
