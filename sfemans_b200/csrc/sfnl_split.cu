@@ -310,33 +310,50 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-__device__ __forceinline__ uint32_t bf16_bits(double v) {
-  return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn((float)v));
-}
-
 // 2^e as a double (e clamped to the normal range).
 __device__ __forceinline__ double pow2(int e) {
   e = e < -1022 ? -1022 : (e > 1023 ? 1023 : e);
   return __longlong_as_double((long long)(e + 1023) << 52);
 }
 
-// Slices of x relative to the row bound 2^E (E from frexp of the row max).
-// Every step multiplies by an exact power of two, so h, mi, lo are exact.
-__device__ __forceinline__ void slice3(double x, int E, double &h, double &mi, double &lo) {
-  const double u0 = pow2(E - kW), i0 = pow2(kW - E);
-  const double u1 = pow2(E - 2 * kW - 1), i1 = pow2(2 * kW + 1 - E);
-  const double u2 = pow2(E - 3 * kW - 2), i2 = pow2(3 * kW + 2 - E);
-  h = rint(x * i0) * u0;
-  double r = x - h;
-  mi = rint(r * i1) * u1;
-  r -= mi;
-  lo = rint(r * i2) * u2;
-}
-
 __device__ __forceinline__ int row_exponent(double mx) {
   int e = 0;
   frexp(mx, &e);  // mx = f 2^e, f in [0.5, 1) -> mx < 2^e
   return e;
+}
+
+// 2^e as a float (e in the normal range).
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((e + 127) << 23); }
+
+// Per-row slicing factors for the bound 2^E: the first slice is cut in FP64, the remainder
+// (|r| <= 2^(E-9)) is rounded once to FP32 (error <= 2^(E-33), far below the last slice's
+// 2^(E-27)) and cut into the second and third slices in FP32; every step multiplies by an
+// exact power of two, so the slices are exact integers (<= 2^8) times powers of two.
+struct SliceScale {
+  double i0, u0;
+  float i1, u1, i2, u2;
+};
+__device__ __forceinline__ SliceScale slice_scale(int E) {
+  E = E < -100 ? -100 : (E > 100 ? 100 : E);  // keep the FP32 factors normal
+  SliceScale s;
+  s.i0 = pow2(kW - E);
+  s.u0 = pow2(E - kW);
+  s.i1 = pow2f(2 * kW + 1 - E);
+  s.u1 = pow2f(E - 2 * kW - 1);
+  s.i2 = pow2f(3 * kW + 2 - E);
+  s.u2 = pow2f(E - 3 * kW - 2);
+  return s;
+}
+__device__ __forceinline__ void slice3f(double x, const SliceScale &s, float &h, float &m, float &l) {
+  const double hd = rint(x * s.i0) * s.u0;
+  const float r = (float)(x - hd);
+  m = rintf(r * s.i1) * s.u1;
+  l = rintf((r - m) * s.i2) * s.u2;
+  h = (float)hd;
+}
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t *>(&v);
 }
 
 // ---------------------------------------------------------------------------
@@ -349,7 +366,7 @@ struct STerm {
 };
 #define T2(a0, b0, a1, b1) {{a0, b0, 1}, {a1, b1, -1}, {0, 0, 0}, {0, 0, 0}}
 #define T4(a0, b0, a1, b1, a2, b2, a3, b3) {{a0, b0, 1}, {a1, b1, -1}, {a2, b2, 1}, {a3, b3, -1}}
-__constant__ STerm c_terms[PR_COUNT][10][4] = {
+constexpr STerm kTerms[PR_COUNT][10][4] = {
     // bundle [u 0-2, w 3-5, b 6-8, j 9-11, gradT 12-14] -> [u x w, u x b, j x b, u . gradT]
     {T2(1, 5, 2, 4), T2(2, 3, 0, 5), T2(0, 4, 1, 3), T2(1, 8, 2, 7), T2(2, 6, 0, 8), T2(0, 7, 1, 6),
      T2(10, 8, 11, 7), T2(11, 6, 9, 8), T2(9, 7, 10, 6), {{0, 12, 1}, {1, 13, 1}, {2, 14, 1}, {0, 0, 0}}},
@@ -369,6 +386,7 @@ __constant__ STerm c_terms[PR_COUNT][10][4] = {
 };
 #undef T2
 #undef T4
+__constant__ STerm c_terms[PR_COUNT][10][4];  // filled from kTerms at first use (see upload_terms)
 
 __host__ __device__ constexpr int pr_nin(int pr) {
   return pr == PR_BUNDLE ? 15 : pr == PR_CROSS ? 6 : pr == PR_DOT ? 6 : pr == PR_PROD ? 2 : pr == PR_CJVP ? 12
@@ -397,16 +415,111 @@ struct SplitArgs {
 
 constexpr int kThreads = 256;
 
+// Compile-time geometry of make_sgeo for a given m (0: read it from the arguments).
+__host__ __device__ constexpr int sg_qmin(int m) { return (3 * m - 2 + 3) / 4; }
+__host__ __device__ constexpr int sg_Q(int m) { return ((sg_qmin(m) + 15) / 16) * 16 < 16 ? 16 : ((sg_qmin(m) + 15) / 16) * 16; }
+__host__ __device__ constexpr int sg_ke(int m, int c) { return (c & 1) ? m / 2 : (m + 1) / 2; }
+__host__ __device__ constexpr int sg_Ks(int m, int c) { return ((sg_ke(m, c) + 15) / 16) * 16 < 16 ? 16 : ((sg_ke(m, c) + 15) / 16) * 16; }
+__host__ __device__ constexpr int sg_anacol(int m, int c) { return c == 0 ? 8 * sg_Q(m) : sg_anacol(m, c - 1) + sg_Ks(m, c - 1); }
+
+// Product phase for one output O of program PR (warp-uniform): lane = point p + PTS*jg, each lane owns
+// J consecutive quarter-angles of the 16-angle chunk.  Evaluates the output at the 4 quadrant angles,
+// folds the products into the analysis classes, finds each class row's bound over the chunk (shuffles
+// across the lanes of the same point), slices and writes the analysis A operand row O*PTS + p.
+// Product phase for one output o (warp-uniform): lane = point p + PTS*jg, each lane owns J consecutive
+// quarter-angles of the 16-angle chunk.  The output's (at most 4) terms s*x[a]*x[b] are read once from
+// constant memory into registers as shared-memory offsets.  Evaluates the output at the 4 quadrant
+// angles, folds the products into the analysis classes, finds each class row's bound over the chunk
+// (shuffles across the lanes of the same point), slices and writes the analysis A operand row o*PTS + p.
 template <int PR>
+__device__ __forceinline__ void product_rows(int o, const double *X, unsigned char *sm, const SGeo &g, int lane) {
+  constexpr int PTS = pr_pts(PR), JG = 32 / PTS, J = 16 / JG;
+  const int p = lane % PTS, jg = lane / PTS;
+  const double *xa[4], *xb[4];
+  double sg[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const STerm tm = c_terms[PR][o][u];
+    xa[u] = X + (size_t)tm.a * 64 * PTS + (size_t)jg * J * PTS + p;
+    xb[u] = X + (size_t)tm.b * 64 * PTS + (size_t)jg * J * PTS + p;
+    sg[u] = (double)tm.s;  // 0 for an unused term
+  }
+  double P[4][J];
+  double mx[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int jj = 0; jj < J; ++jj) {
+    double gq[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int off = (r * 16 + jj) * PTS;
+      double acc = 0.0;
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (sg[u] != 0.0) acc = fma(sg[u] * xa[u][off], xb[u][off], acc);  // warp-uniform branch
+      gq[r] = acc;
+    }
+    const double s14 = gq[0] + gq[3], d14 = gq[0] - gq[3], s23 = gq[1] + gq[2], d32 = gq[2] - gq[1];
+    P[0][jj] = s14 + s23;
+    P[1][jj] = s14 - s23;
+    P[2][jj] = d14 + d32;
+    P[3][jj] = d14 - d32;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) mx[c] = fmax(mx[c], fabs(P[c][jj]));
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+#pragma unroll
+    for (int sh = PTS; sh < 32; sh <<= 1) mx[c] = fmax(mx[c], __shfl_xor_sync(0xffffffffu, mx[c], sh));
+  const int ro = o * PTS + p, k0 = jg * J;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const SliceScale sc = slice_scale(row_exponent(mx[c]));
+    uint32_t w[3][J / 2];
+#pragma unroll
+    for (int q = 0; q < J / 2; ++q) {
+      float h0, m0, l0, h1, m1, l1;
+      slice3f(P[c][2 * q], sc, h0, m0, l0);
+      slice3f(P[c][2 * q + 1], sc, h1, m1, l1);
+      w[0][q] = pack_bf16(h0, h1);
+      w[1][q] = pack_bf16(m0, m1);
+      w[2][q] = pack_bf16(l0, l1);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      unsigned char *rowp = sm + g.off_aana[c][i] + (size_t)(ro / 8) * 256 + (size_t)(ro % 8) * 16;
+#pragma unroll
+      for (int q0 = 0; q0 < J / 2; q0 += 4) {
+        const int k = k0 + 2 * q0;  // first of the (up to) 8 k-values of this store
+        unsigned char *dst = rowp + (size_t)(k / 8) * 128 + (size_t)(k % 8) * 2;
+        if constexpr (J / 2 >= 4)
+          *reinterpret_cast<uint4 *>(dst) = make_uint4(w[i][q0], w[i][q0 + 1], w[i][q0 + 2], w[i][q0 + 3]);
+        else
+          *reinterpret_cast<uint2 *>(dst) = make_uint2(w[i][0], w[i][1]);
+      }
+    }
+  }
+}
+
+template <int PR, int M>
 __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
   constexpr int NI = pr_nin(PR), NO = pr_nout(PR), PTS = pr_pts(PR);
   constexpr unsigned ADJ = pr_adj_in(PR);
+  constexpr bool CT = M > 0;
+  constexpr int KE_MAX = CT ? (M + 1) / 2 : kKeMax;
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ uint32_t s_tmem;
   const SGeo &g = a.g;
-  const int t = threadIdx.x, warp = t >> 5;
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int row = t & 127, half = t >> 7;  // TMEM lane = row (warp w reads lanes 32*(w%4)..)
   const uint32_t mbar = smem_u32(sm + g.off_bar);
+  const int Q = CT ? sg_Q(M) : g.Q, NC = Q / 16;
+  int KE[4], KS[4], ACOL[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    KE[c] = CT ? sg_ke(M, c) : g.ke[c];
+    KS[c] = CT ? sg_Ks(M, c) : g.Ks[c];
+    ACOL[c] = CT ? sg_anacol(M, c) : g.ana_col[c];
+  }
 
   // ---- setup: TMEM, mbarrier, DFT tables ----
   if (warp == 0) {
@@ -434,7 +547,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
   bool ok = true;
 
   const int64_t ntiles = (a.np + PTS - 1) / PTS;
-  const double invN = 1.0 / g.N, twoN = 2.0 / g.N;
+  const double invN = 1.0 / (4.0 * Q), twoN = 2.0 * invN;
   const int npairs = a.nsl == 3 ? 6 : 3;
   double *X = reinterpret_cast<double *>(sm + g.off_x);  // [f][quadrant][16][PTS], point fastest
 
@@ -443,25 +556,30 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
     const int o = row / PTS, p = row % PTS;
     const int64_t gp = tile * PTS + p;
     const bool live = row < NO * PTS && gp < a.np;
-#pragma unroll 1
-    for (int c = 2 * half; c < 2 * half + 2; ++c) {
-      for (int k0 = 0; k0 < g.No[c]; k0 += 8) {
+#pragma unroll
+    for (int cc = 0; cc < 2; ++cc) {
+      const int c = 2 * half + cc;  // classes 0,1 (cos) or 2,3 (sin)
+      const int kec = half ? KE[2 + cc] : KE[cc], ksc = half ? KS[2 + cc] : KS[cc];
+      const int acol = half ? ACOL[2 + cc] : ACOL[cc];
+      for (int k0 = 0; k0 < ksc; k0 += 8) {
         float v[8];
-        tmem_ld8(tmem + lane_base + (uint32_t)(g.ana_col[c] + k0), v);
+        tmem_ld8(tmem + lane_base + (uint32_t)(acol + k0), v);
         tmem_wait_ld();
         if (!live) continue;
-        double *dst = a.out[o] + gp + (c >= 2 ? a.np : 0);
+        double *dst = a.out[o] + gp + (half ? a.np : 0);
+        const int64_t ldm = a.out_ldm[o];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
           const int kk = k0 + e;
-          if (kk >= g.ke[c]) continue;
-          const int n = 2 * kk + (c & 1);
+          if (kk >= kec) break;
+          const int n = 2 * kk + cc;
           const double sc = pr_adj_out(PR) ? 1.0 : (n == 0 ? invN : twoN);
-          const double val = (c == 2 && n == 0) ? 0.0 : (double)v[e] * sc;
-          double *q = dst + (int64_t)n * a.out_ldm[o];
+          const double val = (half && n == 0) ? 0.0 : (double)v[e] * sc;
+          double *q = dst + (int64_t)n * ldm;
           *q = (chk == 0 ? 0.0 : *q) + val;
         }
       }
+      (void)c;
     }
   };
 
@@ -472,43 +590,43 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
       const int64_t gp = tile * PTS + p;
       const bool valid = f < NI && gp < a.np;
       const double *src = valid ? a.in[f] + gp : nullptr;
+      const int64_t ldm = valid ? a.in_ldm[f] : 0;
       const bool cot = f < NI && ((ADJ >> f) & 1u);
-#pragma unroll 1
-      for (int c = 2 * half; c < 2 * half + 2; ++c) {
-        double x[kKeMax];
+#pragma unroll
+      for (int cc = 0; cc < 2; ++cc) {
+        const int c = 2 * half + cc;
+        const int kec = half ? KE[2 + cc] : KE[cc], ksc = half ? KS[2 + cc] : KS[cc];
+        double x[KE_MAX];
         double mx = 0.0;
 #pragma unroll
-        for (int k = 0; k < kKeMax; ++k) {
-          x[k] = 0.0;
-          const int n = 2 * k + (c & 1);
-          if (valid && k < g.ke[c] && !(c == 2 && n == 0)) {
-            double v = __ldg(src + (int64_t)n * a.in_ldm[f] + (c >= 2 ? a.np : 0));
+        for (int k = 0; k < KE_MAX; ++k) {
+          const int n = 2 * k + cc;
+          double v = 0.0;
+          if (valid && k < kec && !(half && n == 0)) {
+            v = __ldg(src + (int64_t)n * ldm + (half ? a.np : 0));
             if (cot) v *= (n == 0 ? invN : twoN);
-            x[k] = v;
-            mx = fmax(mx, fabs(v));
           }
+          x[k] = v;
+          mx = fmax(mx, fabs(v));
         }
-        const int E = row_exponent(mx);
-        const int K = g.Ks[c];
+        const SliceScale sc = slice_scale(row_exponent(mx));
 #pragma unroll
-        for (int kg = 0; kg < kKeMax / 8; ++kg) {
-          if (kg * 8 >= K) break;
+        for (int kg = 0; kg < (KE_MAX + 7) / 8 + 1; ++kg) {
+          if (kg * 8 >= ksc) break;
           uint32_t w[3][4];
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
-            double s0[2], s1[2], s2[2];
+            float hv[2], mv[2], lv[2];
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
-              if (mx > 0.0)
-                slice3(x[kg * 8 + 2 * q + e], E, s0[e], s1[e], s2[e]);
-              else
-                s0[e] = s1[e] = s2[e] = 0.0;
+              const int k = kg * 8 + 2 * q + e;
+              slice3f(k < KE_MAX ? x[k < KE_MAX ? k : 0] : 0.0, sc, hv[e], mv[e], lv[e]);
             }
-            w[0][q] = bf16_bits(s0[0]) | (bf16_bits(s0[1]) << 16);
-            w[1][q] = bf16_bits(s1[0]) | (bf16_bits(s1[1]) << 16);
-            w[2][q] = bf16_bits(s2[0]) | (bf16_bits(s2[1]) << 16);
+            w[0][q] = pack_bf16(hv[0], hv[1]);
+            w[1][q] = pack_bf16(mv[0], mv[1]);
+            w[2][q] = pack_bf16(lv[0], lv[1]);
           }
-          const size_t off = (size_t)(row / 8) * (16 * K) + (size_t)kg * 128 + (size_t)(row % 8) * 16;
+          const size_t off = (size_t)(row / 8) * (16 * ksc) + (size_t)kg * 128 + (size_t)(row % 8) * 16;
 #pragma unroll
           for (int i = 0; i < 3; ++i)
             *reinterpret_cast<uint4 *>(sm + g.off_asyn[c][i] + off) = make_uint4(w[i][0], w[i][1], w[i][2], w[i][3]);
@@ -522,15 +640,15 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
     // ---- 2. synthesis MMAs: D0 (hi x hi) and D1 (corrections) per class ----
     if (t == 0) {
       tc_fence_after();
-      const uint32_t idesc = make_idesc(g.Q);
+      const uint32_t idesc = make_idesc(Q);
       for (int c = 0; c < 4; ++c) {
-        const uint32_t sbo = 16 * g.Ks[c];
-        for (int s = 0; s < g.Ks[c] / 16; ++s)
+        const uint32_t sbo = 16 * KS[c];
+        for (int s = 0; s < KS[c] / 16; ++s)
           for (int pr = 0; pr < npairs; ++pr) {
             const int i = pr == 0 ? 0 : pr == 1 ? 0 : pr == 2 ? 1 : pr == 3 ? 0 : pr == 4 ? 1 : 2;
             const int j = pr == 0 ? 0 : pr == 1 ? 1 : pr == 2 ? 0 : pr == 3 ? 2 : pr == 4 ? 1 : 0;
             const int accn = (i + j == 0) ? 0 : 1;
-            const uint32_t dcol = tmem + (uint32_t)((c * 2 + accn) * g.Q);
+            const uint32_t dcol = tmem + (uint32_t)((c * 2 + accn) * Q);
             const uint64_t ad = make_sdesc(smem_u32(sm + g.off_asyn[c][i]) + 256 * s, 128, sbo);
             const uint64_t bd = make_sdesc(smem_u32(sm + g.off_bsyn[c][j]) + 256 * s, 128, sbo);
             const uint32_t en = (s > 0 || (accn == 1 && pr > 1)) ? 1u : 0u;
@@ -547,7 +665,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
     phase ^= 1;
     tc_fence_after();
 
-    for (int ch = 0; ch < g.NC && ok; ++ch) {
+    for (int ch = 0; ch < NC && ok; ++ch) {
       // ---- 3a. read out, recombine in FP64, fold to the 4 quadrant angles (half = 8 quarter-angles) ----
       {
         const int f = row / PTS, p = row % PTS;
@@ -556,7 +674,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
         for (int c = 0; c < 4; ++c)
 #pragma unroll
           for (int ac = 0; ac < 2; ++ac)
-            tmem_ld8(tmem + lane_base + (uint32_t)((c * 2 + ac) * g.Q + ch * 16 + half * 8), d[c][ac]);
+            tmem_ld8(tmem + lane_base + (uint32_t)((c * 2 + ac) * Q + ch * 16 + half * 8), d[c][ac]);
         tmem_wait_ld();
         if (f < NI) {
           double *xr = X + (size_t)f * 64 * PTS + (size_t)half * 8 * PTS + p;
@@ -586,70 +704,8 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
         tc_fence_after();
         flush_chunk(tile, ch - 1);
       }
-      // ---- 3b. program, analysis pre-fold, slicing: thread = (output o, point p, half of the chunk) ----
-      {
-        const int jh = t & 1, op = t >> 1, o = op / PTS, p = op % PTS;
-        const bool live = o < NO;
-        double P[4][8];
-        double mx[4] = {0.0, 0.0, 0.0, 0.0};
-        if (live) {
-          STerm tm[4];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) tm[u] = c_terms[PR][o][u];
-#pragma unroll
-          for (int jj = 0; jj < 8; ++jj) {
-            const int j = jh * 8 + jj;
-            double gq[4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-              double acc = 0.0;
-#pragma unroll
-              for (int u = 0; u < 4; ++u) {
-                if (tm[u].s == 0) continue;
-                const double xa = X[((size_t)tm[u].a * 64 + r * 16 + j) * PTS + p];
-                const double xb = X[((size_t)tm[u].b * 64 + r * 16 + j) * PTS + p];
-                acc = fma(tm[u].s > 0 ? xa : -xa, xb, acc);
-              }
-              gq[r] = acc;
-            }
-            const double s14 = gq[0] + gq[3], d14 = gq[0] - gq[3], s23 = gq[1] + gq[2], d32 = gq[2] - gq[1];
-            P[0][jj] = s14 + s23;
-            P[1][jj] = s14 - s23;
-            P[2][jj] = d14 + d32;
-            P[3][jj] = d14 - d32;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) mx[c] = fmax(mx[c], fabs(P[c][jj]));
-          }
-        }
-#pragma unroll
-        for (int c = 0; c < 4; ++c) mx[c] = fmax(mx[c], __shfl_xor_sync(0xffffffffu, mx[c], 1));
-        if (live) {
-          const int ro = o * PTS + p;
-#pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            const int E = row_exponent(mx[c]);
-            uint32_t w[3][4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              double s0[2], s1[2], s2[2];
-#pragma unroll
-              for (int e = 0; e < 2; ++e) {
-                if (mx[c] > 0.0)
-                  slice3(P[c][2 * q + e], E, s0[e], s1[e], s2[e]);
-                else
-                  s0[e] = s1[e] = s2[e] = 0.0;
-              }
-              w[0][q] = bf16_bits(s0[0]) | (bf16_bits(s0[1]) << 16);
-              w[1][q] = bf16_bits(s1[0]) | (bf16_bits(s1[1]) << 16);
-              w[2][q] = bf16_bits(s2[0]) | (bf16_bits(s2[1]) << 16);
-            }
-            const size_t off = (size_t)(ro / 8) * 256 + (size_t)jh * 128 + (size_t)(ro % 8) * 16;
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-              *reinterpret_cast<uint4 *>(sm + g.off_aana[c][i] + off) = make_uint4(w[i][0], w[i][1], w[i][2], w[i][3]);
-          }
-        }
-      }
+      // ---- 3b. program, analysis pre-fold, slicing: one output per warp ----
+      for (int o = warp; o < NO; o += kThreads / 32) product_rows<PR>(o, X, sm, g, lane);
       fence_async_smem();
       tc_fence_before();
       __syncthreads();
@@ -657,8 +713,8 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
       if (t == 0 && ok) {
         tc_fence_after();
         for (int c = 0; c < 4; ++c) {
-          const uint32_t idesc = make_idesc(g.No[c]);
-          const uint32_t dcol = tmem + (uint32_t)g.ana_col[c];
+          const uint32_t idesc = make_idesc(KS[c]);
+          const uint32_t dcol = tmem + (uint32_t)ACOL[c];
           for (int pr = 0; pr < npairs; ++pr) {
             int i, j;
             if (a.nsl == 3) {
@@ -669,7 +725,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
               j = pr == 0 ? 1 : 0;
             }
             const uint64_t ad = make_sdesc(smem_u32(sm + g.off_aana[c][i]), 128, 256);
-            const uint64_t bd = make_sdesc(smem_u32(sm + g.off_bana[c][j]) + 256 * ch, 128, 16 * g.Q);
+            const uint64_t bd = make_sdesc(smem_u32(sm + g.off_bana[c][j]) + 256 * ch, 128, 16 * Q);
             umma_bf16(dcol, ad, bd, idesc, pr > 0 ? 1u : 0u);
           }
         }
@@ -686,7 +742,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
       phase ^= 1;
     }
     tc_fence_after();
-    if (ok) flush_chunk(tile, g.NC - 1);
+    if (ok) flush_chunk(tile, NC - 1);
     tc_fence_before();
     __syncthreads();
   }
@@ -697,11 +753,11 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
   }
 }
 
-template <int PR>
+template <int PR, int M>
 int launch_split_pr(SplitArgs &sa, int batch, const ProgArgs &pa, const int *in_map, const int *out_map,
                     cudaStream_t st) {
   constexpr int NI = pr_nin(PR), NO = pr_nout(PR), PTS = pr_pts(PR);
-  auto kern = split_kernel<PR>;
+  auto kern = split_kernel<PR, M>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sa.g.smem_bytes) != cudaSuccess)
     return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (split form)");
   const int64_t ntiles = (sa.np + PTS - 1) / PTS;
@@ -728,8 +784,24 @@ int launch_split_pr(SplitArgs &sa, int batch, const ProgArgs &pa, const int *in_
   return SFNL_OK;
 }
 
+// Copies the term table into constant memory once per device.
+int upload_terms() {
+  static std::mutex mu;
+  static bool done[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return set_error(SFNL_ERR_CUDA, "no current device");
+  std::lock_guard<std::mutex> lk(mu);
+  if (!done[dev]) {
+    if (cudaMemcpyToSymbol(c_terms, kTerms, sizeof(kTerms)) != cudaSuccess)
+      return set_error(SFNL_ERR_CUDA, "upload of the program term table failed");
+    done[dev] = true;
+  }
+  return SFNL_OK;
+}
+
 template <int PR>
 int run_split_program(const ProgArgs &pa, int split, const int *in_map, const int *out_map, cudaStream_t st) {
+  if (int rc = upload_terms()) return rc;
   SplitArgs sa;
   std::memset(&sa, 0, sizeof(sa));
   if (!make_sgeo(pa.m, pr_pts(PR), pr_nin(PR), &sa.g)) return set_error(SFNL_ERR_UNSUPPORTED, "split form: m too large");
@@ -744,7 +816,12 @@ int run_split_program(const ProgArgs &pa, int split, const int *in_map, const in
   sa.bana_bytes = (int)T.bana_bytes;
   if (sa.g.off_bsyn[0][0] + sa.bsyn_bytes != sa.g.off_bana[0][0] || sa.g.off_bana[0][0] + sa.bana_bytes > sa.g.off_bar)
     return set_error(SFNL_ERR_UNSUPPORTED, "split form: table layout mismatch");
-  return launch_split_pr<PR>(sa, pa.batch, pa, in_map, out_map, st);
+  switch (pa.m) {
+    case 16: return launch_split_pr<PR, 16>(sa, pa.batch, pa, in_map, out_map, st);
+    case 32: return launch_split_pr<PR, 32>(sa, pa.batch, pa, in_map, out_map, st);
+    case 64: return launch_split_pr<PR, 64>(sa, pa.batch, pa, in_map, out_map, st);
+    default: return launch_split_pr<PR, 0>(sa, pa.batch, pa, in_map, out_map, st);
+  }
 }
 
 }  // namespace
