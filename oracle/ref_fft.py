@@ -5,7 +5,8 @@ this module: it is the checker for the CUDA path, never part of it.
 
 Three independent CPU formulations of the dealiased products of
 SOURCES/POST_PROCESSING/fft_parallel.F90 (FFT_PAR_CROSS_PROD_DCL :147-328,
-FFT_PAR_DOT_PROD_DCL :330-500, FFT_PAR_PROD_DCL :502-665):
+FFT_PAR_DOT_PROD_DCL :330-500, FFT_PAR_PROD_DCL :502-665, FFT_PAR_DIV_DCL
+:667-830, FFT_SCALAR_VECT_DCL :1021-1220, FFT_TENSOR_DCL :1543-1796):
 
 * ``c_oracle``   -- ctypes binding of oracle/sfnl_oracle.c, the step-by-step
   long-double restatement of the reference (pack, emulated MPI_ALLTOALL,
@@ -33,8 +34,21 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
 
-OP_CROSS, OP_DOT, OP_PROD = 0, 1, 2
-_OPS = {"cross": OP_CROSS, "dot": OP_DOT, "prod": OP_PROD}
+OP_CROSS, OP_DOT, OP_PROD, OP_DIV, OP_SVECT, OP_SVDIV, OP_TENSOR, OP_TENSION = range(8)
+_OPS = {"cross": OP_CROSS, "dot": OP_DOT, "prod": OP_PROD, "div": OP_DIV, "svect": OP_SVECT, "svdiv": OP_SVDIV,
+        "tensor": OP_TENSOR, "tension": OP_TENSION}
+# input slots (V1, V2) and output slots each routine takes and returns
+_IN_SLOTS = {OP_CROSS: (6, 6), OP_DOT: (6, 6), OP_PROD: (2, 2), OP_DIV: (2, 2), OP_SVECT: (6, 2), OP_SVDIV: (6, 2),
+             OP_TENSOR: (6, 6), OP_TENSION: (6, 6)}
+_NOUT = {OP_CROSS: 3, OP_DOT: 1, OP_PROD: 1, OP_DIV: 1, OP_SVECT: 3, OP_SVDIV: 3, OP_TENSOR: 9, OP_TENSION: 9}
+
+
+def out_shape(op: str, npts: int, m: int):
+    """Shape of V_out: (np, 2*ncomp, m), or (3, np, 6, m) for the tensor routine (fft_parallel.F90:1552)."""
+    opc = _OPS[op]
+    if opc in (OP_TENSOR, OP_TENSION):
+        return (3, npts, 6, m)
+    return (npts, 2 * _NOUT[opc], m)
 
 
 # ----------------------------------------------------------------------------
@@ -94,6 +108,9 @@ def _lib():
         f.restype = ctypes.c_int
         f.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                       ctypes.POINTER(ctypes.c_double)] + [ctypes.c_int] * 7
+        f = lib.orc_apply_n
+        f.restype = ctypes.c_int
+        f.argtypes = [ctypes.c_int, P, ctypes.c_int, P, ctypes.c_int, P] + [ctypes.c_int] * 6
         _LIB = lib
     return _LIB
 
@@ -109,22 +126,23 @@ def c_oracle(op: str, V1, V2, m_max_pad: int, nb_procs: int = 1, bloc_size: int 
     ``V1``/``V2`` hold all m_max = m_max_c*nb_procs modes; rank r of the
     emulated Fourier communicator owns modes [r*m_max_c, (r+1)*m_max_c).
     ``bloc_size`` defaults to the callers' choice np/nb_procs+1
-    (subroutine_ns_with_velocity.F90:625).  Returns V_out (np, 6|2, m_max).
+    (subroutine_ns_with_velocity.F90:625).  Returns V_out (np, 2*ncomp, m_max),
+    or (3, np, 6, m_max) for "tensor" / "tension".
     Raises ValueError with the oracle's status for inputs the reference rejects.
     """
     opc = _OPS[op]
     V1 = np.asfortranarray(V1, dtype=np.float64)
     V2 = np.asfortranarray(V2, dtype=np.float64)
-    npts, nf, m = V1.shape
+    npts, nf1, m = V1.shape
+    nf2 = V2.shape[1]
     if m % nb_procs:
         raise ValueError("m_max must be a multiple of nb_procs")
     if bloc_size is None:
         bloc_size = npts // nb_procs + 1
-    nout = 6 if opc == OP_CROSS else 2
-    out = np.zeros((npts, nout, m), order="F")
+    out = np.zeros(out_shape(op, npts, m), order="F")
     N = 2 * m_max_pad - 1 if n_theta is None else n_theta
-    rc = _lib().orc_fft_par_dcl_n(opc, _ptr(V1), _ptr(V2), _ptr(out), npts, nf, m // nb_procs, nb_procs,
-                                  bloc_size, m_max_pad, N)
+    rc = _lib().orc_apply_n(opc, _ptr(V1), nf1, _ptr(V2), nf2, _ptr(out), npts, m // nb_procs, nb_procs,
+                            bloc_size, m_max_pad, N)
     if rc != 0:
         raise ValueError(f"oracle rejected arguments (status {rc})")
     return out
@@ -143,12 +161,25 @@ def _to_complex(V, nfield):
 
 
 def _pointwise(op, ru):
+    """Grid products, fft_parallel.F90:270-274, :449-451, :617, :786, :1150-1157, :1676-1706."""
     if op == OP_CROSS:
         r1, r2, r3, r4, r5, r6 = (ru[:, k, :] for k in range(6))
         return np.stack([r2 * r6 - r3 * r5, r3 * r4 - r1 * r6, r1 * r5 - r2 * r4], axis=1)
     if op == OP_DOT:
         return (ru[:, 0] * ru[:, 3] + ru[:, 1] * ru[:, 4] + ru[:, 2] * ru[:, 5])[:, None, :]
-    return (ru[:, 0] * ru[:, 1])[:, None, :]
+    if op == OP_PROD:
+        return (ru[:, 0] * ru[:, 1])[:, None, :]
+    if op == OP_DIV:
+        return (ru[:, 0] / ru[:, 1])[:, None, :]
+    if op == OP_SVECT:
+        return ru[:, 3:4] * ru[:, 0:3]
+    if op == OP_SVDIV:
+        return ru[:, 0:3] / ru[:, 3:4]
+    t = ru[:, 0:3, None, :] * ru[:, None, 3:6, :]  # t[:, k, l] = u_k v_l
+    if op == OP_TENSION:
+        nrm = np.sqrt(ru[:, 3] ** 2 + ru[:, 4] ** 2 + ru[:, 5] ** 2)[:, None, None, :]
+        t = t / (nrm + 1.0e-14) - np.eye(3)[None, :, :, None] * nrm
+    return t.reshape(ru.shape[0], 9, ru.shape[2])
 
 
 def fft_par(op: str, V1, V2, m_max_pad: int, n_theta: int | None = None, workers: int = 1):
@@ -161,13 +192,14 @@ def fft_par(op: str, V1, V2, m_max_pad: int, n_theta: int | None = None, workers
     import scipy.fft as sfft
 
     opc = _OPS[op]
-    npts, nf, m = V1.shape
+    npts, nf1, m = V1.shape
+    nf2 = V2.shape[1]
     N = 2 * m_max_pad - 1 if n_theta is None else n_theta
     nh = N // 2 + 1
-    nin = nf // 2
-    cu = np.zeros((npts, 2 * nin, nh), dtype=np.complex128)
-    cu[:, :nin, :m] = _to_complex(V1, nin)
-    cu[:, nin:, :m] = _to_complex(V2, nin)
+    n1, n2 = nf1 // 2, nf2 // 2
+    cu = np.zeros((npts, n1 + n2, nh), dtype=np.complex128)
+    cu[:, :n1, :m] = _to_complex(V1, n1)
+    cu[:, n1:, :m] = _to_complex(V2, n2)
     ru = sfft.irfft(cu, n=N, axis=2, norm="forward", workers=workers)  # unnormalised c2r
     prod_ru = _pointwise(opc, ru)
     pc = sfft.rfft(prod_ru, n=N, axis=2, norm="forward", workers=workers)  # includes 1/N
@@ -177,7 +209,18 @@ def fft_par(op: str, V1, V2, m_max_pad: int, n_theta: int | None = None, workers
     out[:, 1::2, :] = -2.0 * pc.imag
     out[:, 0::2, 0] = pc[:, :, 0].real
     out[:, 1::2, 0] = pc[:, :, 0].imag
+    if opc in (OP_TENSOR, OP_TENSION):
+        return tensor_layout(out)
     return out
+
+
+def tensor_layout(flat):
+    """(np, 18, m) with component o = 3k+l in slots 2o, 2o+1  ->  V_out(3, np, 6, m): V_out[k, :, 2l(+1), :]."""
+    npts, _, m = flat.shape
+    t = np.empty((3, npts, 6, m), order="F")
+    for k in range(3):
+        t[k] = flat[:, 6 * k:6 * k + 6, :]
+    return t
 
 
 # ----------------------------------------------------------------------------
@@ -233,12 +276,20 @@ def spectral_product(op: str, V1, V2):
             ak, bk = sp(V1, k, V2, k)
             a, b = a + ak, b + bk
         comps = [(a, b)]
-    else:
+    elif opc == OP_PROD:
         comps = [sp(V1, 0, V2, 0)]
+    elif opc == OP_SVECT:
+        comps = [sp(V1, k, V2, 0) for k in range(3)]
+    elif opc == OP_TENSOR:
+        comps = [sp(V1, k, V2, l) for k in range(3) for l in range(3)]
+    else:
+        raise ValueError(f"{op}: not a bilinear product (depends on the grid)")
     out = np.empty((npts, 2 * len(comps), m), order="F")
     for c, (a, b) in enumerate(comps):
         out[:, 2 * c, :] = a.astype(np.float64)
         out[:, 2 * c + 1, :] = b.astype(np.float64)
+    if opc == OP_TENSOR:
+        return tensor_layout(out)
     return out
 
 

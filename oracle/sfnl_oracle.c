@@ -12,6 +12,9 @@
  *   FFT_PAR_CROSS_PROD_DCL  fft_parallel.F90:147-328
  *   FFT_PAR_DOT_PROD_DCL    fft_parallel.F90:330-500
  *   FFT_PAR_PROD_DCL        fft_parallel.F90:502-665
+ *   FFT_PAR_DIV_DCL         fft_parallel.F90:667-830
+ *   FFT_SCALAR_VECT_DCL     fft_parallel.F90:1021-1220  (pb = 1 product, pb = 2 quotient)
+ *   FFT_TENSOR_DCL          fft_parallel.F90:1543-1796  (with and without opt_tension)
  *
  * including the nb_procs / bloc_size bookkeeping: each emulated rank owns
  * m_max_c contiguous Fourier modes, packs a mode-major dist_field with dummy
@@ -88,23 +91,43 @@ static void r2c_ld(int N, int ny, const ld *x, ld *yr, ld *yi, const ld *ct, con
   }
 }
 
-/* Pointwise products of fft_parallel.F90:270-274 (cross), :449-451 (dot), :617 (prod). */
-static void pointwise(int op, int N, const ld *ru, int nf, ld *prod) {
-  /* ru is (N, nf) column-major: ru[j + N*f]. prod is (N, nout). */
+/* Pointwise maps of fft_parallel.F90:270-274 (cross), :449-451 (dot), :617 (prod), :786 (div),
+ * :1150-1157 (scalar x vector, vector / scalar), :1676-1706 (tensor, tension). ru is (N, nf)
+ * column-major: ru[j + N*f]; prod is (N, nout). Tensor outputs are ordered o = 3*k + l. */
+static void pointwise(int op, int N, const ld *ru, ld *prod) {
   for (int j = 0; j < N; ++j) {
+    const ld *r = ru + j;
+#define RU(f) r[(size_t)N * (f)]
+#define PR(o) prod[j + (size_t)N * (o)]
     if (op == ORC_CROSS) {
-      const ld r1 = ru[j + N * 0], r2 = ru[j + N * 1], r3 = ru[j + N * 2];
-      const ld r4 = ru[j + N * 3], r5 = ru[j + N * 4], r6 = ru[j + N * 5];
-      prod[j + N * 0] = r2 * r6 - r3 * r5;
-      prod[j + N * 1] = r3 * r4 - r1 * r6;
-      prod[j + N * 2] = r1 * r5 - r2 * r4;
+      PR(0) = RU(1) * RU(5) - RU(2) * RU(4);
+      PR(1) = RU(2) * RU(3) - RU(0) * RU(5);
+      PR(2) = RU(0) * RU(4) - RU(1) * RU(3);
     } else if (op == ORC_DOT) {
-      prod[j] = ru[j + N * 0] * ru[j + N * 3] + ru[j + N * 1] * ru[j + N * 4] + ru[j + N * 2] * ru[j + N * 5];
-    } else {
-      prod[j] = ru[j + N * 0] * ru[j + N * 1];
+      PR(0) = RU(0) * RU(3) + RU(1) * RU(4) + RU(2) * RU(5);
+    } else if (op == ORC_PROD) {
+      PR(0) = RU(0) * RU(1);
+    } else if (op == ORC_DIV) {
+      PR(0) = RU(0) / RU(1);
+    } else if (op == ORC_SVECT) {
+      for (int k = 0; k < 3; ++k) PR(k) = RU(3) * RU(k);
+    } else if (op == ORC_SVDIV) {
+      for (int k = 0; k < 3; ++k) PR(k) = RU(k) / RU(3);
+    } else if (op == ORC_TENSOR) {
+      for (int k = 0; k < 3; ++k)
+        for (int l = 0; l < 3; ++l) PR(3 * k + l) = RU(k) * RU(3 + l);
+    } else { /* ORC_TENSION */
+      const ld nrm = sqrtl(RU(3) * RU(3) + RU(4) * RU(4) + RU(5) * RU(5));
+      for (int k = 0; k < 3; ++k)
+        for (int l = 0; l < 3; ++l) PR(3 * k + l) = RU(k) * RU(3 + l) / (nrm + 1.0e-14L) - (k == l ? nrm : 0.0L);
     }
+#undef RU
+#undef PR
   }
-  (void)nf;
+}
+
+static int op_nout(int op) {
+  return (op == ORC_CROSS || op == ORC_SVECT || op == ORC_SVDIV) ? 3 : (op == ORC_TENSOR || op == ORC_TENSION) ? 9 : 1;
 }
 
 int orc_fft_par_dcl(int op, const double *V1, const double *V2, double *Vout, int np, int nb_field,
@@ -115,11 +138,20 @@ int orc_fft_par_dcl(int op, const double *V1, const double *V2, double *Vout, in
 
 int orc_fft_par_dcl_n(int op, const double *V1, const double *V2, double *Vout, int np, int nb_field,
                       int m_max_c, int nb_procs, int bloc_size, int m_max_pad, int N) {
-  if (op != ORC_CROSS && op != ORC_DOT && op != ORC_PROD) return -1;
-  if (op == ORC_PROD) nb_field = 2; /* c_in is (np,2,m_max_c), fft_parallel.F90:510 */
-  /* fft_parallel.F90:188-191, :370-373, :560-563 */
-  if ((nb_field % 2) != 0 || m_max_c <= 0) return -1;
-  if (op != ORC_PROD && nb_field != 6) return -1; /* the product is only formed for nb_field==6 */
+  if (op != ORC_CROSS && op != ORC_DOT && op != ORC_PROD && op != ORC_DIV) return -1;
+  if (op == ORC_PROD || op == ORC_DIV) nb_field = 2; /* c_in is (np,2,m_max_c), fft_parallel.F90:510 */
+  return orc_apply_n(op, V1, nb_field, V2, nb_field, Vout, np, m_max_c, nb_procs, bloc_size, m_max_pad, N);
+}
+
+int orc_apply_n(int op, const double *V1, int nsl1, const double *V2, int nsl2, double *Vout, int np,
+                int m_max_c, int nb_procs, int bloc_size, int m_max_pad, int N) {
+  if (op < ORC_CROSS || op > ORC_TENSION) return -1;
+  /* fft_parallel.F90:188-191, :370-373, :560-563, :1068-1071, :1590-1593 */
+  if ((nsl1 % 2) != 0 || (nsl2 % 2) != 0 || m_max_c <= 0) return -1;
+  /* the product is only formed for these slot counts (:270, :449, :1130, :1676) */
+  if ((op == ORC_CROSS || op == ORC_DOT || op == ORC_TENSOR || op == ORC_TENSION) && (nsl1 != 6 || nsl2 != 6)) return -1;
+  if ((op == ORC_SVECT || op == ORC_SVDIV) && (nsl1 != 6 || nsl2 != 2)) return -1;
+  if ((op == ORC_PROD || op == ORC_DIV) && (nsl1 != 2 || nsl2 != 2)) return -1;
   if (nb_procs < 1 || bloc_size < 1 || np < 0) return -1;
   const int m_max = m_max_c * nb_procs;
   const int np_tot = nb_procs * bloc_size;
@@ -129,11 +161,11 @@ int orc_fft_par_dcl_n(int op, const double *V1, const double *V2, double *Vout, 
   const int nx = N / 2 + 1 < m_max_pad ? N / 2 + 1 : m_max_pad; /* half-complex entries used by c2r */
   if (m_max > N / 2 + 1) return -3;
 
-  const int nfc = (op == ORC_PROD) ? 2 : nb_field;      /* complex fields in cu (both inputs) */
-  const int nout = (op == ORC_CROSS) ? 3 : 1;           /* complex output fields */
-  const int nslot_out = 2 * nout;                       /* V_out second dimension */
-  const int nsl = (op == ORC_PROD) ? 2 : nb_field;      /* slots per input array */
-  const int dslots = 2 * nsl;                           /* dist_field second dimension */
+  const int nfc = (nsl1 + nsl2) / 2;                    /* complex fields in cu (both inputs) */
+  const int nout = op_nout(op);                         /* complex output fields */
+  const int tensor = (op == ORC_TENSOR || op == ORC_TENSION);
+  const int nslot_out = tensor ? 6 : 2 * nout;          /* V_out slots (tensor: V_out(3, np, 6, m)) */
+  const int dslots = nsl1 + nsl2;                       /* dist_field second dimension */
 
   ld *ct = NULL, *st = NULL;
   if (make_tables(N, &ct, &st)) return -4;
@@ -170,11 +202,10 @@ int orc_fft_par_dcl_n(int op, const double *V1, const double *V2, double *Vout, 
     for (size_t t = 0; t < dsz; ++t) dist[r][t] = 1.0e100;
     for (int i = 0; i < m_max_c; ++i) {
       const int g = r * m_max_c + i; /* global mode of local mode i (initialization.F90:823-835) */
-      for (int s = 0; s < nsl; ++s)
-        for (int p = 0; p < np; ++p) {
-          dist[r][IDX3(i, s, p, m_max_c, dslots)] = V1[IDX3(p, s, g, np, nsl)];
-          dist[r][IDX3(i, nsl + s, p, m_max_c, dslots)] = V2[IDX3(p, s, g, np, nsl)];
-        }
+      for (int p = 0; p < np; ++p) {
+        for (int s = 0; s < nsl1; ++s) dist[r][IDX3(i, s, p, m_max_c, dslots)] = V1[IDX3(p, s, g, np, nsl1)];
+        for (int s = 0; s < nsl2; ++s) dist[r][IDX3(i, nsl1 + s, p, m_max_c, dslots)] = V2[IDX3(p, s, g, np, nsl2)];
+      }
     }
   }
   /* (2) MPI_ALLTOALL: block q of rank r's send buffer lands in block r of rank q (:217). */
@@ -203,7 +234,7 @@ int orc_fft_par_dcl_n(int op, const double *V1, const double *V2, double *Vout, 
       }
       for (int nf = 0; nf < nfc; ++nf)
         c2r_ld(N, nx, cur + (size_t)m_max_pad * nf, cui + (size_t)m_max_pad * nf, ru + (size_t)N * nf, ct, st);
-      pointwise(op, N, ru, nfc, pru);
+      pointwise(op, N, ru, pru);
       const ld invN = 1.0L / (ld)N; /* (:288) */
       for (size_t t = 0; t < (size_t)m_max_pad * nout; ++t) pcr[t] = pci[t] = 0.0L;
       for (int o = 0; o < nout; ++o) {
@@ -241,8 +272,14 @@ int orc_fft_par_dcl_n(int op, const double *V1, const double *V2, double *Vout, 
           for (int o = 0; o < nout; ++o) {
             const size_t at = IDX3(o, n, shiftl + i, nout, bloc_size);
             const int g = r * m_max_c + i;
-            Vout[IDX3(n + shiftc, 2 * o, g, np, nslot_out)] = (double)dpr[r][at];
-            Vout[IDX3(n + shiftc, 2 * o + 1, g, np, nslot_out)] = (double)dpi[r][at];
+            if (tensor) { /* v_out(k, n+shiftc, 2l-1:2l, i) (:1786-1787) */
+              const int k = o / 3, l = o % 3;
+              Vout[k + 3 * IDX3(n + shiftc, 2 * l, g, np, 6)] = (double)dpr[r][at];
+              Vout[k + 3 * IDX3(n + shiftc, 2 * l + 1, g, np, 6)] = (double)dpi[r][at];
+            } else {
+              Vout[IDX3(n + shiftc, 2 * o, g, np, nslot_out)] = (double)dpr[r][at];
+              Vout[IDX3(n + shiftc, 2 * o + 1, g, np, nslot_out)] = (double)dpi[r][at];
+            }
           }
         }
       }

@@ -6,7 +6,7 @@
 extern "C" {
 #endif
 
-enum { ORC_CROSS = 0, ORC_DOT = 1, ORC_PROD = 2 };
+enum { ORC_CROSS = 0, ORC_DOT = 1, ORC_PROD = 2, ORC_DIV = 3, ORC_SVECT = 4, ORC_SVDIV = 5, ORC_TENSOR = 6, ORC_TENSION = 7 };
 
 /* Restatement of FFT_PAR_{CROSS_PROD,DOT_PROD,PROD}_DCL (fft_parallel.F90:147-665).
  * V1, V2: global arrays (np, nb_field, m_max_c*nb_procs), Fortran order; rank r
@@ -17,6 +17,11 @@ int orc_fft_par_dcl(int op, const double *V1, const double *V2, double *Vout, in
 /* Same with an explicit grid length N (the reference uses N = 2*m_max_pad-1). */
 int orc_fft_par_dcl_n(int op, const double *V1, const double *V2, double *Vout, int np, int nb_field,
                       int m_max_c, int nb_procs, int bloc_size, int m_max_pad, int N);
+
+/* Any of the routines on inputs with nsl1 / nsl2 slots (scalar x vector: 6 and 2). Tensor outputs are
+ * V_out(3, np, 6, m_max) (fft_parallel.F90:1552); the others V_out(np, 2*nout, m_max). */
+int orc_apply_n(int op, const double *V1, int nsl1, const double *V2, int nsl2, double *Vout, int np,
+                int m_max_c, int nb_procs, int bloc_size, int m_max_pad, int N);
 
 #ifdef __cplusplus
 }

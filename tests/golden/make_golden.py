@@ -4,11 +4,13 @@
 
 Each case stores the seeded inputs and the long-double oracle's output
 (oracle/sfnl_oracle.c, the step-by-step restatement of
-SOURCES/POST_PROCESSING/fft_parallel.F90:147-665).  Cases are small so that
-the fixtures stay a few hundred KB in total.  The exact spectral
-convolution (oracle/ref_fft.py) is checked against every case before it is
-written, so a fixture is only produced when two independent formulations
-agree to 1e-15.
+SOURCES/POST_PROCESSING/fft_parallel.F90:147-830, :1021-1220, :1543-1796).
+Cases are small so that the fixtures stay a few hundred KB in total.  The
+exact spectral convolution (oracle/ref_fft.py) is checked against every
+bilinear case before it is written, so a fixture is only produced when two
+independent formulations agree to 1e-15.  The quotients and the tension
+tensor depend on the grid; their cases are checked against the pocketfft
+restatement on the same grid (1e-13) instead.
 """
 import os
 import sys
@@ -32,18 +34,41 @@ CASES = [
     ("cross_np1_m3", "cross", 1, 3, 4, 1, 0.5, 18),        # single point
     ("cross_np40_m1", "cross", 40, 1, 1, 1, 0.0, 19),      # mode 0 only, N = 1
     ("dot_np70_m32", "dot", 70, 32, 48, 1, 0.05, 20),      # slow decay
+    ("svect_np37_m5", "svect", 37, 5, 7, 1, 0.3, 21),      # FFT_SCALAR_VECT_DCL pb = 1
+    ("svect_np31_m8_p2", "svect", 31, 8, 12, 2, 0.2, 22),
+    ("svdiv_np37_m5", "svdiv", 37, 5, 7, 1, 0.3, 23),      # FFT_SCALAR_VECT_DCL pb = 2
+    ("tensor_np37_m5", "tensor", 37, 5, 7, 1, 0.3, 24),    # FFT_TENSOR_DCL
+    ("tensor_np29_m6_p3", "tensor", 29, 6, 9, 3, 0.2, 25),
+    ("tension_np37_m5", "tension", 37, 5, 7, 1, 0.3, 26),  # FFT_TENSOR_DCL, opt_tension
+    ("div_np37_m5", "div", 37, 5, 7, 1, 0.3, 27),          # FFT_PAR_DIV_DCL
+    ("div_np33_m8_p2", "div", 33, 8, 12, 2, 0.2, 28),
 ]
+
+# (slots of V1, slots of V2) per routine
+SLOTS = {"cross": (6, 6), "dot": (6, 6), "prod": (2, 2), "div": (2, 2), "svect": (6, 2), "svdiv": (6, 2),
+         "tensor": (6, 6), "tension": (6, 6)}
+DENOMINATOR_OFFSET = 4.0  # added to the mode-0 cosine of a divisor so that it stays away from 0
+
+
+def inputs(op, npts, m, alpha, seed):
+    n1, n2 = SLOTS[op]
+    V1 = R.synthetic_field(npts, n1, m, alpha, 1000 + seed)
+    V2 = R.synthetic_field(npts, n2, m, alpha, 2000 + seed)
+    if op in ("div", "svdiv"):
+        V2[:, 0, 0] += DENOMINATOR_OFFSET
+    return V1, V2
 
 
 def make(case):
     name, op, npts, m, pad, procs, alpha, seed = case
-    nsl = 2 if op == "prod" else 6
-    V1 = R.synthetic_field(npts, nsl, m, alpha, 1000 + seed)
-    V2 = R.synthetic_field(npts, nsl, m, alpha, 2000 + seed)
+    V1, V2 = inputs(op, npts, m, alpha, seed)
     out = R.c_oracle(op, V1, V2, pad, nb_procs=procs)
-    ex = R.spectral_product(op, V1, V2)
-    err = R.rel_l2(out, ex)
-    assert err < 1e-15, (name, err)
+    if op in ("div", "svdiv", "tension"):
+        err = R.rel_l2(out, R.fft_par(op, V1, V2, pad))
+        assert err < 1e-13, (name, err)
+    else:
+        err = R.rel_l2(out, R.spectral_product(op, V1, V2))
+        assert err < 1e-15, (name, err)
     np.savez_compressed(os.path.join(HERE, name + ".npz"), V1=V1, V2=V2, out=out,
                         meta=np.array([npts, m, pad, procs], dtype=np.int64), op=np.array(op))
     return name, err
