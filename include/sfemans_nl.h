@@ -6,6 +6,11 @@
  *   FFT_PAR_CROSS_PROD_DCL  :147-328   V_out = V1 x V2
  *   FFT_PAR_DOT_PROD_DCL    :330-500   c_out = V1 . V2
  *   FFT_PAR_PROD_DCL        :502-665   c_out = c1 * c2
+ * and the same-pattern siblings with another pointwise map:
+ *   FFT_PAR_DIV_DCL         :667-830   c_out = c1 / c2
+ *   FFT_SCALAR_VECT_DCL     :1021-1220 V_out = s V (pb = 1) or V / s (pb = 2)
+ *   FFT_TENSOR_DCL          :1543-1796 V_out(k, :, 2l-1:2l, :) = V1_k V2_l, or with
+ *                                      opt_tension V1_k V2_l / (|V2| + 1e-14) - |V2| delta_kl
  *
  * Array layout: every coefficient array is the Fortran array V(np, nslot, m)
  * in column-major order, point index fastest: element (p, s, n) is at
@@ -62,6 +67,24 @@ enum {
   SFNL_ALGO_FAST = 2  /* factored transforms on an internal alias-free grid */
 };
 
+/* Products by op code (sfnl_product_f64, sfnl_product_split, sfnl_product_f64_host).
+ * Layouts: a, b as listed; out (np, nslot, m) except the tensor layout (3, np, 6, m)
+ * of fft_parallel.F90:1552, whose element (k, p, s, n) is at out[k + 3*(p + np*(s + 6*n))]. */
+enum {
+  SFNL_OP_CROSS = 0,       /* a, b (np, 6, m) -> (np, 6, m)   a x b         (:271-273) */
+  SFNL_OP_DOT = 1,         /* a, b (np, 6, m) -> (np, 2, m)   a . b         (:450) */
+  SFNL_OP_PROD = 2,        /* a, b (np, 2, m) -> (np, 2, m)   a b           (:617) */
+  SFNL_OP_DIV = 3,         /* a, b (np, 2, m) -> (np, 2, m)   a / b         (:786) */
+  SFNL_OP_SCALAR_VECT = 4, /* a (np, 6, m), b (np, 2, m) -> (np, 6, m)   b a  (:1150-1153, pb = 1) */
+  SFNL_OP_VECT_SCALAR = 5, /* a (np, 6, m), b (np, 2, m) -> (np, 6, m)   a / b (:1154-1157, pb = 2) */
+  SFNL_OP_TENSOR = 6,      /* a, b (np, 6, m) -> (3, np, 6, m)   a_k b_l    (:1676-1687) */
+  SFNL_OP_TENSION = 7      /* a, b (np, 6, m) -> (3, np, 6, m)   a_k b_l / (|b| + 1e-14) - |b| delta_kl (:1689-1703) */
+};
+/* The quotients (3, 5) and the tension tensor (7) are not products of two
+ * band-limited series: their result depends on the grid, so they run on the
+ * caller's grid N = 2*m_max_pad-1 (GRID form) only; FAST and split forms
+ * return SFNL_ERR_UNSUPPORTED for them. */
+
 /* Split-precision forms (tensor cores, FP32 accumulation, FP64 recombination). */
 enum {
   SFNL_SPLIT_BF16X2 = 2, /* 2 bf16 slices, 3 slice products ("hi/lo") */
@@ -86,10 +109,22 @@ int sfnl_dot_f64(const double *v1, const double *v2, double *out, int64_t np, in
 int sfnl_prod_f64(const double *c1, const double *c2, double *out, int64_t np, int m_max, int m_max_pad,
                   sfnl_stream_t stream);
 
-/* Same three products with an explicit algorithm and grid length.
- * op: 0 cross, 1 dot, 2 prod.  n_theta = 0 selects N = 2*m_max_pad-1. */
+/* Any product by op code (SFNL_OP_*) with an explicit algorithm and grid length.
+ * n_theta = 0 selects N = 2*m_max_pad-1. */
 int sfnl_product_f64(int op, const double *a, const double *b, double *out, int64_t np, int m_max,
                      int m_max_pad, int n_theta, int algo, sfnl_stream_t stream);
+
+/* FFT_PAR_DIV_DCL (fft_parallel.F90:667-830): c1, c2, out are (np, 2, m_max); out = T[S c1 / S c2]. */
+int sfnl_div_f64(const double *c1, const double *c2, double *out, int64_t np, int m_max, int m_max_pad,
+                 sfnl_stream_t stream);
+/* FFT_SCALAR_VECT_DCL (fft_parallel.F90:1021-1220): v, out (np, 6, m_max), s (np, 2, m_max);
+ * pb = 1: out = T[S s * S v]; pb = 2: out = T[S v / S s]; other pb: SFNL_ERR_ARG. */
+int sfnl_scalar_vect_f64(const double *v, const double *s, double *out, int64_t np, int m_max, int m_max_pad, int pb,
+                         sfnl_stream_t stream);
+/* FFT_TENSOR_DCL (fft_parallel.F90:1543-1796): v1, v2 (np, 6, m_max) -> out (3, np, 6, m_max);
+ * tension != 0 selects the opt_tension form. */
+int sfnl_tensor_f64(const double *v1, const double *v2, double *out, int64_t np, int m_max, int m_max_pad,
+                    int tension, sfnl_stream_t stream);
 
 /* The MHD nonlinear bundle in one launch, each term with the semantics of
  * the reference routine that computes it today:
@@ -157,6 +192,19 @@ int sfnl_fft_par_dot_prod_dcl(const double *V1_in, const double *V2_in, double *
                               int m_max_c, int nb_procs, int bloc_size, int m_max_pad, double *temps);
 int sfnl_fft_par_prod_dcl(const double *c1_in, const double *c2_in, double *c_out, int np, int m_max_c,
                           int nb_procs, int bloc_size, int m_max_pad, double *temps);
+/* fft_parallel.F90:667 (FFT_PAR_DIV_DCL): arguments as sfnl_fft_par_prod_dcl. */
+int sfnl_fft_par_div_dcl(const double *c1_in, const double *c2_in, double *c_out, int np, int m_max_c,
+                         int nb_procs, int bloc_size, int m_max_pad, double *temps);
+/* fft_parallel.F90:1021 (FFT_SCALAR_VECT_DCL): nb_field1 = SIZE(V1_in,2) must be 6 and
+ * nb_field2 = SIZE(V2_in,2) 2 (SFNL_ERR_SHAPE, the reference's error_petsc at :1163);
+ * pb outside {1, 2}: SFNL_ERR_ARG (:1160). */
+int sfnl_fft_scalar_vect_dcl(const double *V1_in, const double *V2_in, double *V_out, int pb, int np, int nb_field1,
+                             int nb_field2, int m_max_c, int nb_procs, int bloc_size, int m_max_pad, double *temps);
+/* fft_parallel.F90:1543 (FFT_TENSOR_DCL): V_out (3, np, 6, m_max_c).  opt_tension < 0: argument
+ * absent (plain tensor); > 0: present and .TRUE. (tension form); 0: present and .FALSE., which the
+ * reference rejects (error_petsc at :1705): SFNL_ERR_ARG.  nb_field != 6: SFNL_ERR_SHAPE. */
+int sfnl_fft_tensor_dcl(const double *V1_in, const double *V2_in, double *V_out, int np, int nb_field, int m_max_c,
+                        int nb_procs, int bloc_size, int m_max_pad, int opt_tension, double *temps);
 
 /* Host-array variants of the device entry points (copy in, compute, copy out). */
 int sfnl_product_f64_host(int op, const double *a, const double *b, double *out, int64_t np, int m_max,

@@ -2,12 +2,16 @@
 
 Python host layer over the C-ABI library ``_lib/libsfemans_nl.so``
 (include/sfemans_nl.h).  It mirrors the reference's MODULE fft_parallele
-(SOURCES/POST_PROCESSING/fft_parallel.F90, PUBLIC list :8-17) for the three
+(SOURCES/POST_PROCESSING/fft_parallel.F90, PUBLIC list :8-17) for the
 dealiased products, with the same names, argument order and meaning:
 
     FFT_PAR_CROSS_PROD_DCL(communicator, V1_in, V2_in, V_out, nb_procs, bloc_size, m_max_pad, temps=None)
     FFT_PAR_DOT_PROD_DCL  (communicator, V1_in, V2_in, c_out, nb_procs, bloc_size, m_max_pad, temps=None)
     FFT_PAR_PROD_DCL      (communicator, c1_in, c2_in, c_out, nb_procs, bloc_size, m_max_pad, temps=None)
+    FFT_PAR_DIV_DCL       (communicator, c1_in, c2_in, c_out, nb_procs, bloc_size, m_max_pad, temps=None)
+    FFT_SCALAR_VECT_DCL   (communicator, V1_in, V2_in, V_out, pb, nb_procs, bloc_size, m_max_pad, temps=None)
+    FFT_TENSOR_DCL        (communicator, V1_in, V2_in, V_out, nb_procs, bloc_size, m_max_pad, temps=None,
+                           opt_tension=None)
 
 Arrays are Fortran-ordered (np, nslot, m): numpy arrays in host memory
 (copied through the library's host entry points) or CUDA tensors with
@@ -26,8 +30,17 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libsfemans_nl.so")
 
-OP_CROSS, OP_DOT, OP_PROD = 0, 1, 2
+OP_CROSS, OP_DOT, OP_PROD, OP_DIV, OP_SCALAR_VECT, OP_VECT_SCALAR, OP_TENSOR, OP_TENSION = range(8)
 ALGO_AUTO, ALGO_GRID, ALGO_FAST = 0, 1, 2
+# routine name -> (op code, slots of the first input, of the second, of the output); the tensor
+# routines return V_out(3, np, 6, m) (fft_parallel.F90:1552)
+KINDS = {
+    "cross": (OP_CROSS, 6, 6, 6), "dot": (OP_DOT, 6, 6, 2), "prod": (OP_PROD, 2, 2, 2), "div": (OP_DIV, 2, 2, 2),
+    "svect": (OP_SCALAR_VECT, 6, 2, 6), "svdiv": (OP_VECT_SCALAR, 6, 2, 6), "tensor": (OP_TENSOR, 6, 6, 6),
+    "tension": (OP_TENSION, 6, 6, 6),
+}
+OP_KIND = {v[0]: k for k, v in KINDS.items()}
+TENSOR_OPS = (OP_TENSOR, OP_TENSION)
 SPLIT_BF16X2, SPLIT_BF16X3 = 2, 3
 
 ERRORS = {
@@ -66,6 +79,12 @@ _SIGS = {
     "sfnl_fft_par_dot_prod_dcl": [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P],
     "sfnl_fft_par_prod_dcl": [_P, _P, _P, _I, _I, _I, _I, _I, _P],
     "sfnl_product_f64_host": [_I, _P, _P, _P, _L, _I, _I, _I],
+    "sfnl_div_f64": [_P, _P, _P, _L, _I, _I, _P],
+    "sfnl_scalar_vect_f64": [_P, _P, _P, _L, _I, _I, _I, _P],
+    "sfnl_tensor_f64": [_P, _P, _P, _L, _I, _I, _I, _P],
+    "sfnl_fft_par_div_dcl": [_P, _P, _P, _I, _I, _I, _I, _I, _P],
+    "sfnl_fft_scalar_vect_dcl": [_P, _P, _P] + [_I] * 8 + [_P],
+    "sfnl_fft_tensor_dcl": [_P, _P, _P] + [_I] * 7 + [_P],
     "sfnl_bundle_mhd_host": [_P] * 9 + [_L, _I, _I, _I],
     "sfnl_set_check_finite": [_I],
     "sfnl_finalize": [],
@@ -112,6 +131,21 @@ def fortran_empty(npts: int, nslot: int, m: int, k: int | None = None, device="c
     if k is None:
         return torch.empty((m, nslot, npts), device=device, dtype=dtype).permute(2, 1, 0)
     return torch.empty((k, m, nslot, npts), device=device, dtype=dtype).permute(3, 2, 1, 0)
+
+
+def tensor_empty(npts: int, m: int, device="cuda", dtype=None):
+    """Uninitialised CUDA tensor of shape (3, np, 6, m) in Fortran order (FFT_TENSOR_DCL's V_out)."""
+    import torch
+
+    dtype = dtype or torch.float64
+    return torch.empty((m, 6, npts, 3), device=device, dtype=dtype).permute(3, 2, 1, 0)
+
+
+def out_empty(op: int, npts: int, m: int, device="cuda"):
+    """Output tensor of product ``op`` for np points and m modes."""
+    if op in TENSOR_OPS:
+        return tensor_empty(npts, m, device=device)
+    return fortran_empty(npts, KINDS[OP_KIND[op]][3], m, device=device)
 
 
 def to_device(a, device="cuda"):
@@ -161,12 +195,21 @@ def _stream(stream):
 # ----------------------------------------------------------------------------
 def product(op: int, a, b, out=None, m_max_pad: int | None = None, n_theta: int = 0, algo: int = ALGO_AUTO,
             split: int | None = None, stream=None):
-    """Dealiased product of two Fortran-layout CUDA tensors (op: 0 cross, 1 dot, 2 prod)."""
+    """Product ``op`` (OP_*) of two Fortran-layout CUDA tensors: cross, dot, prod, div, scalar x vector,
+    vector / scalar, tensor, tension tensor.  Shapes follow ``KINDS``."""
+    if op not in OP_KIND:
+        raise SfnlError(-1, f"op must be one of OP_* (0..7), got {op}")
+    _, nsl_a, nsl_b, nsl_o = KINDS[OP_KIND[op]]
     npts, nsl, m = a.shape
+    if nsl != nsl_a or tuple(b.shape) != (npts, nsl_b, m):
+        raise SfnlError(-2, f"{OP_KIND[op]}: inputs must be (np, {nsl_a}, m) and (np, {nsl_b}, m)")
     if m_max_pad is None:
         m_max_pad = 3 * m // 2
     if out is None:
-        out = fortran_empty(npts, 6 if op == OP_CROSS else 2, m, device=a.device)
+        out = out_empty(op, npts, m, device=a.device)
+    want = (3, npts, 6, m) if op in TENSOR_OPS else (npts, nsl_o, m)
+    if tuple(out.shape) != want:
+        raise SfnlError(-2, f"{OP_KIND[op]}: output must be {want}")
     if split is None:
         _check(lib().sfnl_product_f64(op, _dptr(a, "a"), _dptr(b, "b"), _dptr(out, "out"), npts, m, m_max_pad,
                                       n_theta, algo, _stream(stream)))
@@ -176,6 +219,25 @@ def product(op: int, a, b, out=None, m_max_pad: int | None = None, n_theta: int 
         _check(lib().sfnl_product_split(op, _dptr(a, "a"), _dptr(b, "b"), _dptr(out, "out"), npts, m, m_max_pad,
                                         split, _stream(stream)))
     return out
+
+
+def div(c1, c2, out=None, m_max_pad=None, stream=None):
+    """c1 / c2 on the caller's grid (FFT_PAR_DIV_DCL, fft_parallel.F90:667-830): (np, 2, m) -> (np, 2, m)."""
+    return product(OP_DIV, c1, c2, out=out, m_max_pad=m_max_pad, stream=stream)
+
+
+def scalar_vect(v, s, pb: int = 1, out=None, m_max_pad=None, split=None, stream=None):
+    """FFT_SCALAR_VECT_DCL (fft_parallel.F90:1021-1220): pb = 1 -> s v, pb = 2 -> v / s."""
+    if pb not in (1, 2):
+        raise SfnlError(-1, "error in problem type while calling FFT_SCALAR_VECT_DCL")
+    return product(OP_SCALAR_VECT if pb == 1 else OP_VECT_SCALAR, v, s, out=out, m_max_pad=m_max_pad, split=split,
+                   stream=stream)
+
+
+def tensor(v1, v2, tension: bool = False, out=None, m_max_pad=None, split=None, stream=None):
+    """FFT_TENSOR_DCL (fft_parallel.F90:1543-1796): (np, 6, m) x (np, 6, m) -> (3, np, 6, m)."""
+    return product(OP_TENSION if tension else OP_TENSOR, v1, v2, out=out, m_max_pad=m_max_pad, split=split,
+                   stream=stream)
 
 
 def bundle_mhd(u, w, b, j, gradt, m_max_pad: int | None = None, outs=None, algo: int = ALGO_AUTO,
@@ -255,7 +317,7 @@ def _fortran_call(kind, communicator, x, y, out, nb_procs, bloc_size, m_max_pad,
 
         return fft_par_distributed(kind, communicator, x, y, out, nb_procs, bloc_size, m_max_pad, temps)
     if hasattr(x, "is_cuda"):
-        op = {"cross": OP_CROSS, "dot": OP_DOT, "prod": OP_PROD}[kind]
+        op = KINDS[kind][0]
         if nb_procs != 1:
             raise SfnlError(-4, "one GPU holds all modes: nb_procs must be 1")
         if x.shape[0] > nb_procs * bloc_size:
@@ -270,15 +332,23 @@ def _fortran_call(kind, communicator, x, y, out, nb_procs, bloc_size, m_max_pad,
     t3 = np.zeros(3) if temps is None else temps
     npts, nf, mc = x.shape
     L = lib()
+    if out.shape != (out_shape := ((3, npts, 6, mc) if KINDS[kind][0] in TENSOR_OPS else (npts, KINDS[kind][3], mc))):
+        raise SfnlError(-2, f"V_out must be {out_shape}")
+    X, Y, O, T = _host_ptr(x), _host_ptr(y), _host_ptr(out), _host_ptr(t3)
     if kind == "cross":
-        rc = L.sfnl_fft_par_cross_prod_dcl(_host_ptr(x), _host_ptr(y), _host_ptr(out), npts, nf, mc, nb_procs,
-                                           bloc_size, m_max_pad, _host_ptr(t3))
+        rc = L.sfnl_fft_par_cross_prod_dcl(X, Y, O, npts, nf, mc, nb_procs, bloc_size, m_max_pad, T)
     elif kind == "dot":
-        rc = L.sfnl_fft_par_dot_prod_dcl(_host_ptr(x), _host_ptr(y), _host_ptr(out), npts, nf, mc, nb_procs,
-                                         bloc_size, m_max_pad, _host_ptr(t3))
+        rc = L.sfnl_fft_par_dot_prod_dcl(X, Y, O, npts, nf, mc, nb_procs, bloc_size, m_max_pad, T)
+    elif kind == "prod":
+        rc = L.sfnl_fft_par_prod_dcl(X, Y, O, npts, mc, nb_procs, bloc_size, m_max_pad, T)
+    elif kind == "div":
+        rc = L.sfnl_fft_par_div_dcl(X, Y, O, npts, mc, nb_procs, bloc_size, m_max_pad, T)
+    elif kind in ("svect", "svdiv"):
+        rc = L.sfnl_fft_scalar_vect_dcl(X, Y, O, 1 if kind == "svect" else 2, npts, nf, y.shape[1], mc, nb_procs,
+                                        bloc_size, m_max_pad, T)
     else:
-        rc = L.sfnl_fft_par_prod_dcl(_host_ptr(x), _host_ptr(y), _host_ptr(out), npts, mc, nb_procs, bloc_size,
-                                     m_max_pad, _host_ptr(t3))
+        rc = L.sfnl_fft_tensor_dcl(X, Y, O, npts, nf, mc, nb_procs, bloc_size, m_max_pad,
+                                   1 if kind == "tension" else -1, T)
     _check(rc)
     return out
 
@@ -296,3 +366,29 @@ def FFT_PAR_DOT_PROD_DCL(communicator, V1_in, V2_in, c_out, nb_procs, bloc_size,
 def FFT_PAR_PROD_DCL(communicator, c1_in, c2_in, c_out, nb_procs, bloc_size, m_max_pad, temps=None):
     """c_out = c1_in * c2_in, dealiased (fft_parallel.F90:502-665)."""
     return _fortran_call("prod", communicator, c1_in, c2_in, c_out, nb_procs, bloc_size, m_max_pad, temps)
+
+
+def FFT_PAR_DIV_DCL(communicator, c1_in, c2_in, c_out, nb_procs, bloc_size, m_max_pad, temps=None):
+    """c_out = c1_in / c2_in on the grid of 2*m_max_pad-1 angles (fft_parallel.F90:667-830)."""
+    return _fortran_call("div", communicator, c1_in, c2_in, c_out, nb_procs, bloc_size, m_max_pad, temps)
+
+
+def FFT_SCALAR_VECT_DCL(communicator, V1_in, V2_in, V_out, pb, nb_procs, bloc_size, m_max_pad, temps=None):
+    """V_out = V2_in * V1_in (pb = 1) or V1_in / V2_in (pb = 2); V1_in a vector (np, 6, m), V2_in a
+    scalar (np, 2, m) (fft_parallel.F90:1021-1220)."""
+    if V1_in.shape[1] != 6 or V2_in.shape[1] != 2:
+        raise SfnlError(-2, "error in dimension of INPUT variables while calling FFT_SCALAR_VECT_DCL")
+    if pb not in (1, 2):
+        raise SfnlError(-1, "error in problem type while calling FFT_SCALAR_VECT_DCL")
+    return _fortran_call("svect" if pb == 1 else "svdiv", communicator, V1_in, V2_in, V_out, nb_procs, bloc_size,
+                         m_max_pad, temps)
+
+
+def FFT_TENSOR_DCL(communicator, V1_in, V2_in, V_out, nb_procs, bloc_size, m_max_pad, temps=None, opt_tension=None):
+    """V_out(k, :, 2l-1:2l, :) = coefficients of V1_k V2_l, V_out of shape (3, np, 6, m); with
+    opt_tension=True the tension form (fft_parallel.F90:1543-1796).  opt_tension=False is rejected,
+    as the reference does (:1705)."""
+    if opt_tension is not None and not opt_tension:
+        raise SfnlError(-1, "BUG in FFT_TENSOR_DCL : opt_tension should be true if used")
+    return _fortran_call("tension" if opt_tension else "tensor", communicator, V1_in, V2_in, V_out, nb_procs,
+                         bloc_size, m_max_pad, temps)

@@ -92,11 +92,12 @@ int scan_outputs(const ProgArgs &a, cudaStream_t st) {
   if (cudaMemsetAsync(s->d_flag, 0, sizeof(int), st) != cudaSuccess) return set_error(SFNL_ERR_CUDA, "memset failed");
   const int no = op_nout(a.op);
   for (int o = 0; o < no; ++o) {
-    // Each output field is a strided set of (cos,sin) rows; scan the span it covers.
+    // Each output field is a strided set of (cos,sin) rows; scan the span each row covers
+    // (with a point stride of 3 the span also holds the other two tensor rows, all outputs).
     for (int b = 0; b < a.batch; ++b)
       for (int n = 0; n < a.m; ++n) {
         const double *row = a.out[o] + (int64_t)b * a.out_bs[o] + (int64_t)n * a.out_ldm[o];
-        finite_scan<<<32, 256, 0, st>>>(row, 2 * a.np, s->d_flag);
+        finite_scan<<<32, 256, 0, st>>>(row, (2 * a.np - 1) * a.out_ps + 1, s->d_flag);
       }
   }
   int h = 0;
@@ -143,17 +144,22 @@ ProgArgs make_args(int op, int64_t np, int m, int N, int batch) {
   a.m = m;
   a.N = N;
   a.batch = batch;
+  a.out_ps = 1;
   return a;
 }
 
 int run_fp64(ProgArgs a, int algo, int N_caller, cudaStream_t st) {
   const bool alias_free = dealiased(a.m, N_caller);
-  if (algo == SFNL_ALGO_AUTO) algo = (alias_free && fast_supported(a.op, a.m, fast_grid_length(a.m))) ? SFNL_ALGO_FAST : SFNL_ALGO_GRID;
+  if (algo == SFNL_ALGO_AUTO)
+    algo = (alias_free && op_bilinear(a.op) && fast_supported(a.op, a.m, fast_grid_length(a.m))) ? SFNL_ALGO_FAST
+                                                                                                 : SFNL_ALGO_GRID;
   int rc;
   if (algo == SFNL_ALGO_GRID) {
     a.N = N_caller;
     rc = launch_grid(a, st);
   } else if (algo == SFNL_ALGO_FAST) {
+    if (!op_bilinear(a.op))
+      return set_error(SFNL_ERR_UNSUPPORTED, "FAST form: quotients and the tension tensor depend on the grid (use GRID)");
     if (!alias_free) return set_error(SFNL_ERR_ALIAS, "FAST form needs a dealiasing pad (2*m_max_pad-1 >= 3*m_max-2)");
     a.N = fast_grid_length(a.m);
     if (!fast_supported(a.op, a.m, a.N)) return set_error(SFNL_ERR_UNSUPPORTED, "FAST form not built for this size");
@@ -167,6 +173,8 @@ int run_fp64(ProgArgs a, int algo, int N_caller, cudaStream_t st) {
 
 int run_split(ProgArgs a, int split, int N_caller, cudaStream_t st) {
   if (split != SFNL_SPLIT_BF16X2 && split != SFNL_SPLIT_BF16X3) return set_error(SFNL_ERR_ARG, "split must be 2 or 3");
+  if (!op_bilinear(a.op))
+    return set_error(SFNL_ERR_UNSUPPORTED, "split forms: quotients and the tension tensor depend on the grid (use GRID)");
   if (!dealiased(a.m, N_caller)) return set_error(SFNL_ERR_ALIAS, "split forms need a dealiasing pad (2*m_max_pad-1 >= 3*m_max-2)");
   if (!split_supported(a.op, a.m)) return set_error(SFNL_ERR_UNSUPPORTED, "split form not built for this program/size");
   int rc = launch_split(a, split, st);
@@ -174,24 +182,38 @@ int run_split(ProgArgs a, int split, int N_caller, cudaStream_t st) {
   return rc;
 }
 
-// Products of fft_parallel.F90: op 0 cross (6 slots), 1 dot (6 -> 2), 2 prod (2 -> 2).
+// The products of fft_parallel.F90 by library op code (SFNL_OP_*): internal program, slots of the
+// first and second input, and output slots (6 with tensor_out: the layout V(3, np, 6, m)).
+struct ProductKind {
+  int op, nsl_a, nsl_b, nsl_out;
+  bool tensor_out;
+};
+constexpr ProductKind kProducts[8] = {
+    {OP_CROSS, 6, 6, 6, false},  {OP_DOT, 6, 6, 2, false},   {OP_PROD, 2, 2, 2, false},
+    {OP_DIV, 2, 2, 2, false},    {OP_SVECT, 6, 2, 6, false}, {OP_SVDIV, 6, 2, 6, false},
+    {OP_TENSOR, 6, 6, 6, true},  {OP_TENSION, 6, 6, 6, true}};
+constexpr int kNumProducts = 8;
+
 int build_product(int op, const double *x, const double *y, double *out, int64_t np, int m, int N, ProgArgs *pa) {
-  if (op < 0 || op > 2) return set_error(SFNL_ERR_ARG, "op must be 0 (cross), 1 (dot) or 2 (prod)");
+  if (op < 0 || op >= kNumProducts) return set_error(SFNL_ERR_ARG, "op must be one of SFNL_OP_* (0..7)");
   if (np > 0 && (!x || !y || !out)) return set_error(SFNL_ERR_ARG, "null array");
-  ProgArgs a = make_args(op, np, m, N, 1);
-  if (op == OP_PROD) {
-    set_in(a, 0, x, np, 2, 0, m, false);
-    set_in(a, 1, y, np, 2, 0, m, false);
-    set_out(a, 0, out, np, 2, 0, m, false);
+  const ProductKind &pk = kProducts[op];
+  ProgArgs a = make_args(pk.op, np, m, N, 1);
+  const int na = pk.nsl_a / 2, nb = pk.nsl_b / 2;
+  for (int k = 0; k < na; ++k) set_in(a, k, x, np, pk.nsl_a, k, m, false);
+  for (int k = 0; k < nb; ++k) set_in(a, na + k, y, np, pk.nsl_b, k, m, false);
+  if (pk.tensor_out) {
+    // V_out(k, p, 2l-1:2l, n) holds the coefficients of u_k v_l (fft_parallel.F90:1786-1787).
+    for (int k = 0; k < 3; ++k)
+      for (int l = 0; l < 3; ++l) {
+        const int o = 3 * k + l;
+        a.out[o] = out + k + (int64_t)3 * 2 * l * np;
+        a.out_ldm[o] = (int64_t)3 * 6 * np;
+        a.out_bs[o] = 0;
+      }
+    a.out_ps = 3;
   } else {
-    for (int k = 0; k < 3; ++k) {
-      set_in(a, k, x, np, 6, k, m, false);
-      set_in(a, 3 + k, y, np, 6, k, m, false);
-    }
-    if (op == OP_CROSS)
-      for (int k = 0; k < 3; ++k) set_out(a, k, out, np, 6, k, m, false);
-    else
-      set_out(a, 0, out, np, 2, 0, m, false);
+    for (int o = 0; o < op_nout(pk.op); ++o) set_out(a, o, out, np, pk.nsl_out, o, m, false);
   }
   *pa = a;
   return SFNL_OK;
@@ -247,8 +269,9 @@ cudaStream_t as_stream(sfnl_stream_t s) { return reinterpret_cast<cudaStream_t>(
 struct HostBuf {
   const void *src;  // host input (copied in) or nullptr
   void *dst;        // host output (copied out) or nullptr
-  int nslot;        // second dimension of the Fortran array (np, nslot, m)
-  double *dev;      // device buffer of the current chunk, Fortran layout (np_chunk, nslot, m)
+  int nslot;        // slots of the Fortran array (np, nslot, m), or (ew, np, nslot, m)
+  double *dev;      // device buffer of the current chunk, same layout with np_chunk points
+  int ew = 1;       // leading extent (3 for the tensor layout V(3, np, 6, m))
 };
 
 constexpr int kPipe = 3;
@@ -272,7 +295,7 @@ int with_device_buffers(std::vector<HostBuf> &bufs, int64_t np, int m, ChunkRun 
     if (!ps.st[i] && cudaStreamCreateWithFlags(&ps.st[i], cudaStreamNonBlocking) != cudaSuccess)
       return set_error(SFNL_ERR_CUDA, "cudaStreamCreate failed");
   size_t per_point = 0;
-  for (auto &b : bufs) per_point += sizeof(double) * (size_t)b.nslot * m;
+  for (auto &b : bufs) per_point += sizeof(double) * (size_t)b.ew * b.nslot * m;
   int64_t cp = (int64_t)(kChunkBytes / (per_point ? per_point : 1));
   cp = (cp / 128) * 128;
   if (cp < 128) cp = 128;
@@ -280,7 +303,7 @@ int with_device_buffers(std::vector<HostBuf> &bufs, int64_t np, int m, ChunkRun 
   const int64_t nchunks = (np + cp - 1) / cp;
   const int slots = nchunks < kPipe ? (int)nchunks : kPipe;
   size_t slot_bytes = 0;
-  for (auto &b : bufs) slot_bytes += (sizeof(double) * (size_t)b.nslot * m * cp + 255) & ~size_t(255);
+  for (auto &b : bufs) slot_bytes += (sizeof(double) * (size_t)b.ew * b.nslot * m * cp + 255) & ~size_t(255);
   const size_t total = slot_bytes * slots;
   if (total > s->work_bytes) {
     if (s->work) cudaFree(s->work);
@@ -301,18 +324,20 @@ int with_device_buffers(std::vector<HostBuf> &bufs, int64_t np, int m, ChunkRun 
     size_t off = slot_bytes * slot;
     for (auto &b : bufs) {
       b.dev = reinterpret_cast<double *>(s->work + off);
-      off += (sizeof(double) * (size_t)b.nslot * m * cp + 255) & ~size_t(255);
-      if (b.src && cudaMemcpy2DAsync(b.dev, sizeof(double) * n, static_cast<const double *>(b.src) + p0,
-                                     sizeof(double) * np, sizeof(double) * n, (size_t)b.nslot * m,
-                                     cudaMemcpyHostToDevice, st) != cudaSuccess)
+      off += (sizeof(double) * (size_t)b.ew * b.nslot * m * cp + 255) & ~size_t(255);
+      const size_t w = sizeof(double) * b.ew;  // bytes per point in a row
+      if (b.src && cudaMemcpy2DAsync(b.dev, w * n, static_cast<const double *>(b.src) + b.ew * p0, w * np, w * n,
+                                     (size_t)b.nslot * m, cudaMemcpyHostToDevice, st) != cudaSuccess)
         rc = set_error(SFNL_ERR_CUDA, "host-to-device copy failed");
     }
     if (rc == SFNL_OK) rc = run(bufs, n, ctx, st);
-    for (auto &b : bufs)
+    for (auto &b : bufs) {
+      const size_t w = sizeof(double) * b.ew;
       if (rc == SFNL_OK && b.dst &&
-          cudaMemcpy2DAsync(static_cast<double *>(b.dst) + p0, sizeof(double) * np, b.dev, sizeof(double) * n,
-                            sizeof(double) * n, (size_t)b.nslot * m, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+          cudaMemcpy2DAsync(static_cast<double *>(b.dst) + b.ew * p0, w * np, b.dev, w * n, w * n,
+                            (size_t)b.nslot * m, cudaMemcpyDeviceToHost, st) != cudaSuccess)
         rc = set_error(SFNL_ERR_CUDA, "device-to-host copy failed");
+    }
   }
   for (int i = 0; i < slots; ++i)
     if (cudaStreamSynchronize(ps.st[i]) != cudaSuccess && rc == SFNL_OK)
@@ -352,11 +377,13 @@ int host_product(int op, const double *x, const double *y, double *out, int64_t 
   int N = 0;
   int rc = check_common(np, m, pad, n_theta, 1, &N);
   if (rc) return rc;
-  if (op < 0 || op > 2) return set_error(SFNL_ERR_ARG, "op must be 0, 1 or 2");
+  if (op < 0 || op >= kNumProducts) return set_error(SFNL_ERR_ARG, "op must be one of SFNL_OP_* (0..7)");
   if (np == 0) return SFNL_OK;
   if (!x || !y || !out) return set_error(SFNL_ERR_ARG, "null array");
-  const int nsl_in = op == OP_PROD ? 2 : 6, nsl_out = op == OP_CROSS ? 6 : 2;
-  std::vector<HostBuf> bufs = {{x, nullptr, nsl_in, nullptr}, {y, nullptr, nsl_in, nullptr}, {nullptr, out, nsl_out, nullptr}};
+  const ProductKind &pk = kProducts[op];
+  std::vector<HostBuf> bufs = {{x, nullptr, pk.nsl_a, nullptr},
+                               {y, nullptr, pk.nsl_b, nullptr},
+                               {nullptr, out, pk.nsl_out, nullptr, pk.tensor_out ? 3 : 1}};
   ProdCtx c{op, m, pad, n_theta, algo, np};
   return with_device_buffers(bufs, np, m, run_prod_dev, &c, temps);
 }
@@ -552,6 +579,51 @@ int sfnl_fft_par_prod_dcl(const double *c1_in, const double *c2_in, double *c_ou
   int rc = check_fortran_args(np, 2, m_max_c, nb_procs, bloc_size, false);
   if (rc) return rc;
   return host_product(OP_PROD, c1_in, c2_in, c_out, np, m_max_c * nb_procs, m_max_pad, 0, SFNL_ALGO_AUTO, temps);
+}
+
+int sfnl_fft_par_div_dcl(const double *c1_in, const double *c2_in, double *c_out, int np, int m_max_c, int nb_procs,
+                         int bloc_size, int m_max_pad, double *temps) {
+  int rc = check_fortran_args(np, 2, m_max_c, nb_procs, bloc_size, false);
+  if (rc) return rc;
+  return host_product(SFNL_OP_DIV, c1_in, c2_in, c_out, np, m_max_c * nb_procs, m_max_pad, 0, SFNL_ALGO_AUTO, temps);
+}
+
+int sfnl_fft_scalar_vect_dcl(const double *V1_in, const double *V2_in, double *V_out, int pb, int np, int nb_field1,
+                             int nb_field2, int m_max_c, int nb_procs, int bloc_size, int m_max_pad, double *temps) {
+  int rc = check_fortran_args(np, nb_field1, m_max_c, nb_procs, bloc_size, false);
+  if (rc) return rc;
+  if (nb_field2 % 2 != 0) return set_error(SFNL_ERR_ARG, "BUG in FFT_SCALAR_VECT_DCL: MOD(nb_field2,2)/=0");
+  if (nb_field1 != 6 || nb_field2 != 2)
+    return set_error(SFNL_ERR_SHAPE, "error in dimension of INPUT variables while calling FFT_SCALAR_VECT_DCL");
+  if (pb != 1 && pb != 2) return set_error(SFNL_ERR_ARG, "error in problem type while calling FFT_SCALAR_VECT_DCL");
+  return host_product(pb == 1 ? SFNL_OP_SCALAR_VECT : SFNL_OP_VECT_SCALAR, V1_in, V2_in, V_out, np,
+                      m_max_c * nb_procs, m_max_pad, 0, SFNL_ALGO_AUTO, temps);
+}
+
+int sfnl_fft_tensor_dcl(const double *V1_in, const double *V2_in, double *V_out, int np, int nb_field, int m_max_c,
+                        int nb_procs, int bloc_size, int m_max_pad, int opt_tension, double *temps) {
+  int rc = check_fortran_args(np, nb_field, m_max_c, nb_procs, bloc_size, false);
+  if (rc) return rc;
+  if (nb_field != 6) return set_error(SFNL_ERR_SHAPE, "FFT_TENSOR_DCL forms the tensor only for nb_field == 6");
+  if (opt_tension == 0) return set_error(SFNL_ERR_ARG, "BUG in FFT_TENSOR_DCL : opt_tension should be true if used");
+  return host_product(opt_tension > 0 ? SFNL_OP_TENSION : SFNL_OP_TENSOR, V1_in, V2_in, V_out, np, m_max_c * nb_procs,
+                      m_max_pad, 0, SFNL_ALGO_AUTO, temps);
+}
+
+int sfnl_scalar_vect_f64(const double *v, const double *s, double *out, int64_t np, int m_max, int m_max_pad, int pb,
+                         sfnl_stream_t stream) {
+  if (pb != 1 && pb != 2) return set_error(SFNL_ERR_ARG, "error in problem type while calling FFT_SCALAR_VECT_DCL");
+  return sfnl_product_f64(pb == 1 ? SFNL_OP_SCALAR_VECT : SFNL_OP_VECT_SCALAR, v, s, out, np, m_max, m_max_pad, 0,
+                          SFNL_ALGO_AUTO, stream);
+}
+int sfnl_tensor_f64(const double *v1, const double *v2, double *out, int64_t np, int m_max, int m_max_pad, int tension,
+                    sfnl_stream_t stream) {
+  return sfnl_product_f64(tension ? SFNL_OP_TENSION : SFNL_OP_TENSOR, v1, v2, out, np, m_max, m_max_pad, 0,
+                          SFNL_ALGO_AUTO, stream);
+}
+int sfnl_div_f64(const double *c1, const double *c2, double *out, int64_t np, int m_max, int m_max_pad,
+                 sfnl_stream_t stream) {
+  return sfnl_product_f64(SFNL_OP_DIV, c1, c2, out, np, m_max, m_max_pad, 0, SFNL_ALGO_AUTO, stream);
 }
 
 int sfnl_product_f64_host(int op, const double *a, const double *b, double *out, int64_t np, int m_max, int m_max_pad,

@@ -30,8 +30,10 @@
 // coefficients together, so L1 serves all but the first read), the folded
 // products go through shared memory in fragment order, then warp w owns output
 // mode tiles in the analysis.  Elementary programs are cross (6 -> 3), dot
-// (6 -> 1) and product (2 -> 1); the bundle and the linearised programs are
-// sequences of elementary launches on one stream (with accumulation).
+// (6 -> 1), product (2 -> 1), scalar x vector (4 -> 3, FFT_SCALAR_VECT_DCL
+// pb = 1) and tensor (6 -> 9, FFT_TENSOR_DCL); the bundle and the linearised
+// programs are sequences of elementary launches on one stream (with
+// accumulation).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -157,8 +159,9 @@ int get_tables(const Geo &g, Tables *out) {
 // ---------------------------------------------------------------------------
 struct FastArgs {
   const double *in[6];
-  double *out[3];
-  int64_t in_ldm[6], out_ldm[3], in_bs[6], out_bs[3];
+  double *out[9];
+  int64_t in_ldm[6], out_ldm[9], in_bs[6], out_bs[9];
+  int64_t out_ps;   // point stride of the outputs (3 in the tensor layout), sine at out_ps*np
   int64_t np;
   int m, N, NT;
   int ks_off[4], KS[4], nu_off[4], NU[4], ke[4];
@@ -193,6 +196,30 @@ struct EKDef<EK_PROD> {
   static constexpr int NI = 2, NO = 1;
   __device__ static void op(const double *x, double *y) { y[0] = x[0] * x[1]; }
 };
+template <>
+struct EKDef<EK_SVECT> {
+  static constexpr int NI = 4, NO = 3;
+  __device__ static void op(const double *x, double *y) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) y[k] = x[3] * x[k];
+  }
+};
+template <>
+struct EKDef<EK_TENSOR> {
+  static constexpr int NI = 6, NO = 9;
+  __device__ static void op(const double *x, double *y) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) y[3 * k + l] = x[k] * x[3 + l];
+  }
+};
+__host__ __device__ constexpr int ek_nin(int ek) { return ek == EK_PROD ? 2 : ek == EK_SVECT ? 4 : 6; }
+__host__ __device__ constexpr int ek_nout(int ek) { return ek == EK_CROSS || ek == EK_SVECT ? 3 : ek == EK_TENSOR ? 9 : 1; }
+// Shared memory of one CTA: folded products [NO][4][NT][2][32] and staged coefficients [NI][KT][8].
+inline size_t fast_smem_bytes(int ek, int NT, int KT) {
+  return sizeof(double) * ((size_t)ek_nout(ek) * 4 * NT * 2 * 32 + (size_t)ek_nin(ek) * KT * 8);
+}
 
 __device__ __forceinline__ void cp_async8(void *smem_dst, const void *gsrc) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
@@ -355,7 +382,8 @@ __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
       const int n = class_mode(c, kk);
 #pragma unroll
       for (int o = 0; o < NO; ++o) {
-        double *dst = a.out[o] + (int64_t)b * a.out_bs[o] + p + (int64_t)n * a.out_ldm[o] + (c >= 2 ? a.np : 0);
+        double *dst = a.out[o] + (int64_t)b * a.out_bs[o] + p * a.out_ps + (int64_t)n * a.out_ldm[o] +
+                      (c >= 2 ? a.np * a.out_ps : 0);
         const double v = (c == 2 && n == 0) ? 0.0 : y[o][h];
         if (a.accumulate)
           *dst += v;
@@ -369,8 +397,9 @@ __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
 template <int EK, int M, int ADJ>
 int launch_ek_m(FastArgs &fa, int batch, cudaStream_t st) {
   constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO;
+  static_assert(ek_nin(EK) == NI && ek_nout(EK) == NO, "elementary program table");
   fa.KT = 4 * (fa.KS[0] + fa.KS[1] + fa.KS[2] + fa.KS[3]);
-  const size_t smem = sizeof(double) * ((size_t)NO * 4 * fa.NT * 2 * 32 + (size_t)NI * fa.KT * 8);
+  const size_t smem = fast_smem_bytes(EK, fa.NT, fa.KT);
   if (smem > 200 * 1024) return set_error(SFNL_ERR_UNSUPPORTED, "FAST form: m too large for shared memory");
   int nw = fa.NT < 8 ? fa.NT : 8;
   if (nw < 2) nw = 2;
@@ -426,6 +455,8 @@ int decompose_program(int op, std::vector<Elem> &seq) {
     case OP_CROSS: add(EK_CROSS, {0, 1, 2, 3, 4, 5}, {0, 1, 2}, 0, 0); break;
     case OP_DOT: add(EK_DOT, {0, 1, 2, 3, 4, 5}, {0}, 0, 0); break;
     case OP_PROD: add(EK_PROD, {0, 1}, {0}, 0, 0); break;
+    case OP_SVECT: add(EK_SVECT, {0, 1, 2, 3}, {0, 1, 2}, 0, 0); break;
+    case OP_TENSOR: add(EK_TENSOR, {0, 1, 2, 3, 4, 5}, {0, 1, 2, 3, 4, 5, 6, 7, 8}, 0, 0); break;
     case OP_BUNDLE:
       add(EK_CROSS, {0, 1, 2, 3, 4, 5}, {0, 1, 2}, 0, 0);     // u x w
       add(EK_CROSS, {0, 1, 2, 6, 7, 8}, {3, 4, 5}, 0, 0);     // u x b
@@ -460,10 +491,10 @@ int decompose_program(int op, std::vector<Elem> &seq) {
 int fast_grid_length(int m) { return make_geo(m).N; }
 
 bool fast_supported(int op, int m, int N) {
-  (void)op;
-  if (m < 1 || m > 512) return false;
+  if (m < 1 || m > 512 || !op_bilinear(op)) return false;
   const Geo g = make_geo(m);
-  return g.N == N && sizeof(double) * ((size_t)3 * 4 * g.NT * 2 * 32 + (size_t)6 * 4 * g.KS_tot * 8) <= 200 * 1024;
+  // the largest elementary program of the op decides (the tensor's nine outputs, else a cross product)
+  return g.N == N && fast_smem_bytes(op == OP_TENSOR ? EK_TENSOR : EK_CROSS, g.NT, 4 * g.KS_tot) <= 200 * 1024;
 }
 
 int launch_fast(const ProgArgs &a, cudaStream_t st) {
@@ -480,7 +511,8 @@ int launch_fast(const ProgArgs &a, cudaStream_t st) {
   for (const Elem &e : seq) {
     FastArgs fa;
     std::memset(&fa, 0, sizeof(fa));
-    const int ni = e.ek == EK_PROD ? 2 : 6, no = e.ek == EK_CROSS ? 3 : 1;
+    const int ni = ek_nin(e.ek), no = ek_nout(e.ek);
+    fa.out_ps = a.out_ps;
     for (int i = 0; i < ni; ++i) {
       fa.in[i] = a.in[e.in[i]];
       fa.in_ldm[i] = a.in_ldm[e.in[i]];
@@ -508,9 +540,11 @@ int launch_fast(const ProgArgs &a, cudaStream_t st) {
     fa.accumulate = e.acc;
     fa.syn = T.syn;
     fa.ana = T.ana;
-    int r = e.ek == EK_CROSS ? launch_ek<EK_CROSS>(fa, a.batch, st)
-          : e.ek == EK_DOT   ? launch_ek<EK_DOT>(fa, a.batch, st)
-                             : launch_ek<EK_PROD>(fa, a.batch, st);
+    int r = e.ek == EK_CROSS  ? launch_ek<EK_CROSS>(fa, a.batch, st)
+          : e.ek == EK_DOT    ? launch_ek<EK_DOT>(fa, a.batch, st)
+          : e.ek == EK_PROD   ? launch_ek<EK_PROD>(fa, a.batch, st)
+          : e.ek == EK_SVECT  ? launch_ek<EK_SVECT>(fa, a.batch, st)
+                              : launch_ek<EK_TENSOR>(fa, a.batch, st);
     if (r) return r;
   }
   return SFNL_OK;
@@ -612,6 +646,7 @@ extern "C" int sfnl_cross_f64_noalloc(const double *v1, const double *v2, double
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   FastArgs fa;
   std::memset(&fa, 0, sizeof(fa));
+  fa.out_ps = 1;
   for (int k = 0; k < 3; ++k) {
     fa.in[k] = v1 + (int64_t)2 * k * np;
     fa.in[3 + k] = v2 + (int64_t)2 * k * np;

@@ -13,8 +13,9 @@
 // Parallel decomposition: one warp per point.  The point's coefficients are
 // staged in shared memory (read by all lanes as broadcasts), lanes own grid
 // angles during synthesis and modes during analysis.  This form is the
-// parity anchor and the fallback for any (m, N); the fast and split forms
-// carry the throughput.
+// parity anchor, the fallback for any (m, N), and the only form of the
+// programs that depend on the grid (the quotients and the tension tensor);
+// the fast and split forms carry the throughput of the products.
 #include <cuda_runtime.h>
 
 #include "sfnl_internal.h"
@@ -100,9 +101,9 @@ __global__ void __launch_bounds__(kGridThreads) grid_kernel(const ProgArgs a, in
       const double sc = op_adjoint_out(OP) ? 1.0 : (n == 0 ? invN : twoN);
 #pragma unroll
       for (int o = 0; o < NO; ++o) {
-        double *dst = a.out[o] + (int64_t)b * a.out_bs[o] + p + (int64_t)n * a.out_ldm[o];
+        double *dst = a.out[o] + (int64_t)b * a.out_bs[o] + p * a.out_ps + (int64_t)n * a.out_ldm[o];
         dst[0] = ya[o] * sc;
-        dst[a.np] = (n == 0) ? 0.0 : yb[o] * sc;
+        dst[a.np * a.out_ps] = (n == 0) ? 0.0 : yb[o] * sc;
       }
     }
     __syncwarp();
@@ -144,6 +145,11 @@ int launch_grid(const ProgArgs &a, cudaStream_t st) {
     case OP_CROSS_VJP: return launch_grid_op<OP_CROSS_VJP>(a, st);
     case OP_MHD_JVP: return launch_grid_op<OP_MHD_JVP>(a, st);
     case OP_MHD_VJP: return launch_grid_op<OP_MHD_VJP>(a, st);
+    case OP_DIV: return launch_grid_op<OP_DIV>(a, st);
+    case OP_SVECT: return launch_grid_op<OP_SVECT>(a, st);
+    case OP_SVDIV: return launch_grid_op<OP_SVDIV>(a, st);
+    case OP_TENSOR: return launch_grid_op<OP_TENSOR>(a, st);
+    case OP_TENSION: return launch_grid_op<OP_TENSION>(a, st);
   }
   return set_error(SFNL_ERR_ARG, "unknown program");
 }

@@ -28,15 +28,16 @@ void fast_release_tables();                             // sfnl_fast.cu
 int launch_split(const ProgArgs &a, int split, cudaStream_t st);  // sfnl_split.cu
 void split_release_tables();                            // sfnl_split.cu
 
-// Elementary programs: cross (6 -> 3), dot (6 -> 1), product (2 -> 1).  Every
-// program of sfnl_ops.cuh is a sequence of them on one stream (the bundle is
-// four, a linearised cross product two or four, accumulating where a term
-// adds to an earlier one).
-enum { EK_CROSS = 0, EK_DOT = 1, EK_PROD = 2 };
+// Elementary programs: cross (6 -> 3), dot (6 -> 1), product (2 -> 1),
+// scalar x vector (4 -> 3) and tensor (6 -> 9).  Every bilinear program of
+// sfnl_ops.cuh is a sequence of them on one stream (the bundle is four, a
+// linearised cross product two or four, accumulating where a term adds to an
+// earlier one).
+enum { EK_CROSS = 0, EK_DOT = 1, EK_PROD = 2, EK_SVECT = 3, EK_TENSOR = 4 };
 struct Elem {
   int ek;
   int in[6];     // field indices into ProgArgs.in
-  int out[3];    // indices into ProgArgs.out
+  int out[9];    // indices into ProgArgs.out
   unsigned adj;  // bit f: operand f is a cotangent (synthesised with the analysis weights)
   int acc;       // 1: add to the output instead of overwriting it
 };

@@ -1,7 +1,8 @@
 // sfnl_split.cu -- split-precision products on the tcgen05 tensor cores.
 //
 // Same mathematics as the FAST form (sfnl_fast.cu): the exact truncated
-// product of fft_parallel.F90:147-665 evaluated on an internal alias-free
+// product of fft_parallel.F90:147-665, :1021-1220 (pb = 1) and :1543-1796
+// (without opt_tension) evaluated on an internal alias-free
 // grid, N = 4Q angles theta_j = pi(2j+1)/N with Q a multiple of 16, the two
 // real-FFT symmetry levels folded out so that each field needs four small
 // class contractions (cos/sin x even/odd modes) each way.  Here those
@@ -28,7 +29,8 @@
 // Tile.  One launch runs a whole program (the MHD bundle: 15 fields in, 10
 // out).  The 128 MMA rows are (field slot, point) pairs: 16 slots x 8 points
 // for programs with more than 8 input fields, 8 x 16 for the cross and dot
-// products, 4 x 32 for the scalar product.  A row's TMEM accumulators hold its
+// products, 4 x 32 for the scalar and scalar x vector products (the tensor
+// product of FFT_TENSOR_DCL runs as three scalar x vector programs).  A row's TMEM accumulators hold its
 // field's four classes at all Q angles (8Q fp32 columns, 384 at m=64).  After
 // the synthesis each row is folded to the 4Q physical angles in FP64 and the
 // rows of one point meet in shared memory, 16 quarter-angles at a time; each
@@ -359,7 +361,7 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
 // ---------------------------------------------------------------------------
 // programs: each output is a sum of at most 4 signed products x[a]*x[b]
 // ---------------------------------------------------------------------------
-enum { PR_BUNDLE = 0, PR_CROSS, PR_DOT, PR_PROD, PR_CJVP, PR_CVJP, PR_MVJP, PR_COUNT };
+enum { PR_BUNDLE = 0, PR_CROSS, PR_DOT, PR_PROD, PR_CJVP, PR_CVJP, PR_MVJP, PR_SVECT, PR_COUNT };
 
 struct STerm {
   signed char a, b, s;
@@ -383,6 +385,11 @@ constexpr STerm kTerms[PR_COUNT][10][4] = {
     // transpose of (du x w + u x dw, du x b + u x db): [u, w, b, c1 9-11, c2 12-14] -> [w x c1 + b x c2, c1 x u, c2 x u]
     {T4(4, 11, 5, 10, 7, 14, 8, 13), T4(5, 9, 3, 11, 8, 12, 6, 14), T4(3, 10, 4, 9, 6, 13, 7, 12),
      T2(10, 2, 11, 1), T2(11, 0, 9, 2), T2(9, 1, 10, 0), T2(13, 2, 14, 1), T2(14, 0, 12, 2), T2(12, 1, 13, 0)},
+    // scalar x vector [v 0-2, s 3] -> s v (fft_parallel.F90:1150-1153); the tensor u_k v_l is three of
+    // these, [v, u_k] -> u_k v (:1676-1687)
+    {{{0, 3, 1}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}},
+     {{1, 3, 1}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}},
+     {{2, 3, 1}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}}},
 };
 #undef T2
 #undef T4
@@ -390,11 +397,11 @@ __constant__ STerm c_terms[PR_COUNT][10][4];  // filled from kTerms at first use
 
 __host__ __device__ constexpr int pr_nin(int pr) {
   return pr == PR_BUNDLE ? 15 : pr == PR_CROSS ? 6 : pr == PR_DOT ? 6 : pr == PR_PROD ? 2 : pr == PR_CJVP ? 12
-       : pr == PR_CVJP ? 9 : 15;
+       : pr == PR_CVJP ? 9 : pr == PR_MVJP ? 15 : 4;
 }
 __host__ __device__ constexpr int pr_nout(int pr) {
   return pr == PR_BUNDLE ? 10 : pr == PR_CROSS ? 3 : pr == PR_DOT ? 1 : pr == PR_PROD ? 1 : pr == PR_CJVP ? 3
-       : pr == PR_CVJP ? 6 : 9;
+       : pr == PR_CVJP ? 6 : pr == PR_MVJP ? 9 : 3;
 }
 __host__ __device__ constexpr int pr_slots(int pr) { return pr_nin(pr) > 8 ? 16 : pr_nin(pr) > 4 ? 8 : 4; }
 __host__ __device__ constexpr int pr_pts(int pr) { return 128 / pr_slots(pr); }
@@ -406,6 +413,7 @@ struct SplitArgs {
   const double *in[16];
   double *out[10];
   int64_t in_ldm[16], out_ldm[10], in_bs[16], out_bs[10];
+  int64_t out_ps;  // point stride of the outputs (3 in the tensor layout), sine at out_ps*np
   int64_t np;
   int nsl;
   SGeo g;
@@ -566,7 +574,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
         tmem_ld8(tmem + lane_base + (uint32_t)(acol + k0), v);
         tmem_wait_ld();
         if (!live) continue;
-        double *dst = a.out[o] + gp + (half ? a.np : 0);
+        double *dst = a.out[o] + gp * a.out_ps + (half ? a.np * a.out_ps : 0);
         const int64_t ldm = a.out_ldm[o];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
@@ -809,6 +817,7 @@ int run_split_program(const ProgArgs &pa, int split, const int *in_map, const in
   int rc = get_stables(sa.g, &T);
   if (rc) return rc;
   sa.np = pa.np;
+  sa.out_ps = pa.out_ps;
   sa.nsl = split;
   sa.bsyn = T.bsyn;
   sa.bana = T.bana;
@@ -827,8 +836,7 @@ int run_split_program(const ProgArgs &pa, int split, const int *in_map, const in
 }  // namespace
 
 bool split_supported(int op, int m) {
-  (void)op;
-  if (m < 1 || m > 64) return false;
+  if (m < 1 || m > 64 || !op_bilinear(op)) return false;
   SGeo g;
   return make_sgeo(m, 8, 16, &g) && make_sgeo(m, 16, 8, &g) && make_sgeo(m, 32, 4, &g);
 }
@@ -844,6 +852,14 @@ int launch_split(const ProgArgs &a, int split, cudaStream_t st) {
     case OP_CROSS_JVP: return run_split_program<PR_CJVP>(a, split, id, id, st);
     case OP_CROSS_VJP: return run_split_program<PR_CVJP>(a, split, id, id, st);
     case OP_MHD_VJP: return run_split_program<PR_MVJP>(a, split, id, id, st);
+    case OP_SVECT: return run_split_program<PR_SVECT>(a, split, id, id, st);
+    case OP_TENSOR: {  // [u, v] -> u_k v_l: one scalar x vector program per k, outputs 3k..3k+2
+      for (int k = 0; k < 3; ++k) {
+        const int in_k[4] = {3, 4, 5, k}, out_k[3] = {3 * k, 3 * k + 1, 3 * k + 2};
+        if (int rc = run_split_program<PR_SVECT>(a, split, in_k, out_k, st)) return rc;
+      }
+      return SFNL_OK;
+    }
     case OP_MHD_JVP: {  // [u, w, b, du, dw, db] -> two linearised cross products with disjoint outputs
       static const int in1[12] = {0, 1, 2, 3, 4, 5, 9, 10, 11, 12, 13, 14}, out1[3] = {0, 1, 2};
       static const int in2[12] = {0, 1, 2, 6, 7, 8, 9, 10, 11, 15, 16, 17}, out2[3] = {3, 4, 5};

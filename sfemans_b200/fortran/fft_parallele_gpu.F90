@@ -7,6 +7,9 @@
 !   FFT_PAR_CROSS_PROD_DCL  fft_parallel.F90:147
 !   FFT_PAR_DOT_PROD_DCL    fft_parallel.F90:330
 !   FFT_PAR_PROD_DCL        fft_parallel.F90:502
+!   FFT_PAR_DIV_DCL         fft_parallel.F90:667
+!   FFT_SCALAR_VECT_DCL     fft_parallel.F90:1021
+!   FFT_TENSOR_DCL          fft_parallel.F90:1543
 ! One GPU holds every Fourier mode, so the Fourier communicator must have
 ! one rank (nb_procs == 1).  bloc_size is checked (np <= nb_procs*bloc_size)
 ! and otherwise unused.  temps(3), when present, receives the data-movement
@@ -21,6 +24,7 @@ MODULE fft_parallele_gpu
   IMPLICIT NONE
   PRIVATE
   PUBLIC :: FFT_PAR_CROSS_PROD_DCL, FFT_PAR_DOT_PROD_DCL, FFT_PAR_PROD_DCL
+  PUBLIC :: FFT_PAR_DIV_DCL, FFT_SCALAR_VECT_DCL, FFT_TENSOR_DCL
 
   INTERFACE
      FUNCTION sfnl_fft_par_cross_prod_dcl(V1_in, V2_in, V_out, np, nb_field, m_max_c, nb_procs, &
@@ -52,6 +56,36 @@ MODULE fft_parallele_gpu
        TYPE(C_PTR), VALUE    :: temps
        INTEGER(C_INT)        :: rc
      END FUNCTION sfnl_fft_par_prod_dcl
+
+     FUNCTION sfnl_fft_par_div_dcl(c1_in, c2_in, c_out, np, m_max_c, nb_procs, &
+          bloc_size, m_max_pad, temps) RESULT(rc) BIND(C, NAME='sfnl_fft_par_div_dcl')
+       IMPORT :: C_INT, C_DOUBLE, C_PTR
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(IN)  :: c1_in, c2_in
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(OUT) :: c_out
+       INTEGER(C_INT), VALUE :: np, m_max_c, nb_procs, bloc_size, m_max_pad
+       TYPE(C_PTR), VALUE    :: temps
+       INTEGER(C_INT)        :: rc
+     END FUNCTION sfnl_fft_par_div_dcl
+
+     FUNCTION sfnl_fft_scalar_vect_dcl(V1_in, V2_in, V_out, pb, np, nb_field1, nb_field2, m_max_c, &
+          nb_procs, bloc_size, m_max_pad, temps) RESULT(rc) BIND(C, NAME='sfnl_fft_scalar_vect_dcl')
+       IMPORT :: C_INT, C_DOUBLE, C_PTR
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(IN)  :: V1_in, V2_in
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(OUT) :: V_out
+       INTEGER(C_INT), VALUE :: pb, np, nb_field1, nb_field2, m_max_c, nb_procs, bloc_size, m_max_pad
+       TYPE(C_PTR), VALUE    :: temps
+       INTEGER(C_INT)        :: rc
+     END FUNCTION sfnl_fft_scalar_vect_dcl
+
+     FUNCTION sfnl_fft_tensor_dcl(V1_in, V2_in, V_out, np, nb_field, m_max_c, nb_procs, &
+          bloc_size, m_max_pad, opt_tension, temps) RESULT(rc) BIND(C, NAME='sfnl_fft_tensor_dcl')
+       IMPORT :: C_INT, C_DOUBLE, C_PTR
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(IN)  :: V1_in, V2_in
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(OUT) :: V_out
+       INTEGER(C_INT), VALUE :: np, nb_field, m_max_c, nb_procs, bloc_size, m_max_pad, opt_tension
+       TYPE(C_PTR), VALUE    :: temps
+       INTEGER(C_INT)        :: rc
+     END FUNCTION sfnl_fft_tensor_dcl
 
      FUNCTION sfnl_last_error() RESULT(msg) BIND(C, NAME='sfnl_last_error')
        IMPORT :: C_PTR
@@ -143,5 +177,68 @@ CONTAINS
        temps(1:MIN(3,SIZE(temps))) = t3(1:MIN(3,SIZE(temps)))
     END IF
   END SUBROUTINE FFT_PAR_PROD_DCL
+
+  SUBROUTINE FFT_PAR_DIV_DCL(communicator, c1_in, c2_in, c_out, nb_procs, bloc_size, m_max_pad, temps)
+    MPI_Comm :: communicator
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(IN)  :: c1_in, c2_in
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(OUT) :: c_out
+    INTEGER, INTENT(IN) :: nb_procs, bloc_size, m_max_pad
+    REAL(KIND=8), DIMENSION(:), OPTIONAL, INTENT(INOUT) :: temps
+    REAL(C_DOUBLE), DIMENSION(3), TARGET :: t3
+    INTEGER(C_INT) :: rc
+    CALL check_comm(communicator, nb_procs, 'FFT_PAR_DIV_DCL')
+    rc = sfnl_fft_par_div_dcl(c1_in, c2_in, c_out, INT(SIZE(c1_in,1), C_INT), INT(SIZE(c1_in,3), C_INT), &
+         INT(nb_procs, C_INT), INT(bloc_size, C_INT), INT(m_max_pad, C_INT), C_LOC(t3))
+    CALL stop_on_error(rc, 'FFT_PAR_DIV_DCL')
+    IF (PRESENT(temps)) THEN
+       temps = 0.d0
+       temps(1:MIN(3,SIZE(temps))) = t3(1:MIN(3,SIZE(temps)))
+    END IF
+  END SUBROUTINE FFT_PAR_DIV_DCL
+
+  SUBROUTINE FFT_SCALAR_VECT_DCL(communicator, V1_in, V2_in, V_out, pb, nb_procs, bloc_size, m_max_pad, temps)
+    MPI_Comm :: communicator
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(IN)  :: V1_in ! VECTOR
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(IN)  :: V2_in ! SCALAR
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(OUT) :: V_out
+    INTEGER, INTENT(IN) :: pb, nb_procs, bloc_size, m_max_pad
+    REAL(KIND=8), DIMENSION(:), OPTIONAL, INTENT(INOUT) :: temps
+    REAL(C_DOUBLE), DIMENSION(3), TARGET :: t3
+    INTEGER(C_INT) :: rc
+    CALL check_comm(communicator, nb_procs, 'FFT_SCALAR_VECT_DCL')
+    rc = sfnl_fft_scalar_vect_dcl(V1_in, V2_in, V_out, INT(pb, C_INT), INT(SIZE(V1_in,1), C_INT), &
+         INT(SIZE(V1_in,2), C_INT), INT(SIZE(V2_in,2), C_INT), INT(SIZE(V1_in,3), C_INT), INT(nb_procs, C_INT), &
+         INT(bloc_size, C_INT), INT(m_max_pad, C_INT), C_LOC(t3))
+    CALL stop_on_error(rc, 'FFT_SCALAR_VECT_DCL')
+    IF (PRESENT(temps)) THEN
+       temps = 0.d0
+       temps(1:MIN(3,SIZE(temps))) = t3(1:MIN(3,SIZE(temps)))
+    END IF
+  END SUBROUTINE FFT_SCALAR_VECT_DCL
+
+  SUBROUTINE FFT_TENSOR_DCL(communicator, V1_in, V2_in, V_out, nb_procs, bloc_size, m_max_pad, temps, opt_tension)
+    MPI_Comm :: communicator
+    REAL(KIND=8), DIMENSION(:,:,:),   CONTIGUOUS, INTENT(IN)  :: V1_in, V2_in
+    REAL(KIND=8), DIMENSION(:,:,:,:), CONTIGUOUS, INTENT(OUT) :: V_out
+    INTEGER, INTENT(IN) :: nb_procs, bloc_size, m_max_pad
+    REAL(KIND=8), DIMENSION(:), OPTIONAL, INTENT(INOUT) :: temps
+    LOGICAL,                    OPTIONAL, INTENT(IN)    :: opt_tension
+    REAL(C_DOUBLE), DIMENSION(3), TARGET :: t3
+    INTEGER(C_INT) :: rc, tension
+    CALL check_comm(communicator, nb_procs, 'FFT_TENSOR_DCL')
+    tension = -1                     ! absent: plain tensor product
+    IF (PRESENT(opt_tension)) THEN
+       tension = 0                   ! present and .FALSE.: rejected by the library, as by the reference
+       IF (opt_tension) tension = 1
+    END IF
+    rc = sfnl_fft_tensor_dcl(V1_in, V2_in, V_out, INT(SIZE(V1_in,1), C_INT), INT(SIZE(V1_in,2), C_INT), &
+         INT(SIZE(V1_in,3), C_INT), INT(nb_procs, C_INT), INT(bloc_size, C_INT), INT(m_max_pad, C_INT), tension, &
+         C_LOC(t3))
+    CALL stop_on_error(rc, 'FFT_TENSOR_DCL')
+    IF (PRESENT(temps)) THEN
+       temps = 0.d0
+       temps(1:MIN(3,SIZE(temps))) = t3(1:MIN(3,SIZE(temps)))
+    END IF
+  END SUBROUTINE FFT_TENSOR_DCL
 
 END MODULE fft_parallele_gpu

@@ -30,19 +30,18 @@ def shard_range(npts: int, rank: int, world: int) -> tuple[int, int]:
 
 
 def _default_compute(kind, x, y, m_max_pad):
-    from . import OP_CROSS, OP_DOT, OP_PROD, product
+    from . import KINDS, product
 
-    op = {"cross": OP_CROSS, "dot": OP_DOT, "prod": OP_PROD}[kind]
-    return product(op, x, y, m_max_pad=m_max_pad)
+    return product(KINDS[kind][0], x, y, m_max_pad=m_max_pad)
 
 
 def fft_par_distributed(kind, group, x, y, out, nb_procs, bloc_size, m_max_pad, temps=None, compute=None):
-    """FFT_PAR_{CROSS_PROD,DOT_PROD,PROD}_DCL over a mode-distributed communicator.
+    """FFT_PAR_*_DCL, FFT_SCALAR_VECT_DCL or FFT_TENSOR_DCL over a mode-distributed communicator.
 
-    x, y: this rank's (np, nslot, m_max_c) tensors (Fortran layout); out:
-    (np, 6|2, m_max_c).  ``compute(kind, xb, yb, m_max_pad)`` maps the
-    gathered (bloc_size, nslot, m_max) blocks to (bloc_size, nout, m_max);
-    it defaults to the CUDA kernels.
+    kind: a key of ``sfemans_b200.KINDS``.  x, y: this rank's (np, nslot1, m_max_c) and
+    (np, nslot2, m_max_c) tensors (Fortran layout); out: (np, nout, m_max_c), or (3, np, 6,
+    m_max_c) for the tensor kinds.  ``compute(kind, xb, yb, m_max_pad)`` maps the gathered
+    (bloc_size, nslot, m_max) blocks to the block's output; it defaults to the CUDA kernels.
     """
     import torch
     import torch.distributed as dist
@@ -51,11 +50,12 @@ def fft_par_distributed(kind, group, x, y, out, nb_procs, bloc_size, m_max_pad, 
     if world != nb_procs:
         raise ValueError("nb_procs must equal the communicator size")
     npts, nsl, mc = x.shape
+    nsl2 = y.shape[1]
     np_tot = nb_procs * bloc_size
     if npts > np_tot:
         raise ValueError("np > nb_procs*bloc_size")
     compute = compute or _default_compute
-    nout = out.shape[1]
+    tensor_out = kind in ("tensor", "tension")
 
     def to_blocks(t, ns):
         # (np, ns, mc) -> send buffer [dest q][mode i][slot s][point n], points padded to np_tot.
@@ -63,21 +63,26 @@ def fft_par_distributed(kind, group, x, y, out, nb_procs, bloc_size, m_max_pad, 
         tp[:npts] = t
         return tp.reshape(nb_procs, bloc_size, ns, mc).permute(0, 3, 2, 1).contiguous()
 
-    send = torch.cat([to_blocks(x, nsl), to_blocks(y, nsl)], dim=2)          # (P, mc, 2ns, bloc)
+    send = torch.cat([to_blocks(x, nsl), to_blocks(y, nsl2)], dim=2)         # (P, mc, ns1+ns2, bloc)
     recv = torch.empty_like(send)
     dist.all_to_all_single(recv.view(-1), send.view(-1), group=group)       # fft_parallel.F90:217
     # recv[r] = source rank r's modes for my points -> (bloc, ns, m_max) Fortran layout with
     # global mode r*mc + i (the shiftl bookkeeping of :223-231).
-    full = recv.permute(3, 2, 0, 1).reshape(bloc_size, 2 * nsl, nb_procs * mc)
+    full = recv.permute(3, 2, 0, 1).reshape(bloc_size, nsl + nsl2, nb_procs * mc)
     xb = full[:, :nsl, :].contiguous().permute(2, 1, 0).contiguous().permute(2, 1, 0)
     yb = full[:, nsl:, :].contiguous().permute(2, 1, 0).contiguous().permute(2, 1, 0)
     pb = compute(kind, xb, yb, m_max_pad)                                     # (bloc, nout, m_max)
+    if tensor_out:  # (3, bloc, 6, m_max) -> (bloc, 18, m_max), slot 3*s + k
+        pb = pb.permute(1, 2, 0, 3).reshape(bloc_size, 18, nb_procs * mc)
+    nout = pb.shape[1]
     # send back modes [q*mc, (q+1)*mc) of my points to rank q (:306)
     back = pb.reshape(bloc_size, nout, nb_procs, mc).permute(2, 3, 1, 0).contiguous()  # (P, mc, nout, bloc)
     got = torch.empty_like(back)
     dist.all_to_all_single(got.view(-1), back.view(-1), group=group)
     # got[q] = my modes for rank q's points -> (np_tot, nout, mc), drop dummies (:311-324)
     res = got.permute(0, 3, 2, 1).reshape(np_tot, nout, mc)[:npts]
+    if tensor_out:
+        res = res.reshape(npts, 6, 3, mc).permute(2, 0, 1, 3)
     out.copy_(res)
     if temps is not None:
         temps[:] = 0.0

@@ -46,7 +46,7 @@ NULL = ctypes.c_void_p(0)
     ((0, NULL, NULL, NULL, -1, 4, 6, 0, 0, NULL), -1),        # np < 0
     ((0, NULL, NULL, NULL, 10, 4, 3, 0, 0, NULL), -3),        # m_max_pad < m_max
     ((0, NULL, NULL, NULL, 10, 4, 6, 5, 0, NULL), -3),        # explicit grid shorter than 2m-1
-    ((7, NULL, NULL, NULL, 10, 4, 6, 0, 0, NULL), -1),        # unknown op
+    ((8, NULL, NULL, NULL, 10, 4, 6, 0, 0, NULL), -1),        # unknown op
     ((0, NULL, NULL, NULL, 10, 4, 6, 0, 0, NULL), -1),        # null arrays with np > 0
 ])
 def test_product_argument_errors(args, code):
@@ -88,3 +88,48 @@ def test_batch_argument_errors():
     assert L.sfnl_cross_jvp_f64(a, a, a, a, 10, 4, 6, 0, NULL) == -1
     assert L.sfnl_mhd_vjp_f64(a, a, a, a, a, 10, 4, 6, 70000, NULL) == -1
     assert L.sfnl_mhd_jvp_f64(a, a, NULL, a, a, 10, 4, 6, 2, NULL) == -1
+
+
+def test_sibling_fortran_signature_checks():
+    L = sf.lib()
+    a = np.zeros((4, 6, 2), order="F")
+    p = ctypes.c_void_p(a.ctypes.data)
+    # FFT_SCALAR_VECT_DCL: odd slot count (fft_parallel.F90:1068), scalar with 6 slots (:1163), bad pb (:1160)
+    assert L.sfnl_fft_scalar_vect_dcl(p, p, p, 1, 4, 6, 3, 2, 1, 5, 3, NULL) == -1
+    assert L.sfnl_fft_scalar_vect_dcl(p, p, p, 1, 4, 6, 6, 2, 1, 5, 3, NULL) == -2
+    assert L.sfnl_fft_scalar_vect_dcl(p, p, p, 3, 4, 6, 2, 2, 1, 5, 3, NULL) == -1
+    assert "problem type" in sf.last_error()
+    # FFT_TENSOR_DCL: opt_tension present and .FALSE. (:1705), nb_field != 6, m_max_c == 0
+    assert L.sfnl_fft_tensor_dcl(p, p, p, 4, 6, 2, 1, 5, 3, 0, NULL) == -1
+    assert "opt_tension" in sf.last_error()
+    assert L.sfnl_fft_tensor_dcl(p, p, p, 4, 4, 2, 1, 5, 3, -1, NULL) == -2
+    assert L.sfnl_fft_tensor_dcl(p, p, p, 4, 6, 0, 1, 5, 3, 1, NULL) == -1
+    # FFT_PAR_DIV_DCL: m_max_c == 0 (:710), np > nb_procs*bloc_size
+    assert L.sfnl_fft_par_div_dcl(p, p, p, 4, 0, 1, 5, 3, NULL) == -1
+    assert L.sfnl_fft_par_div_dcl(p, p, p, 4, 2, 1, 3, 3, NULL) == -2
+
+
+def test_grid_dependent_products_refuse_the_fast_and_split_forms():
+    L = sf.lib()
+    a = ctypes.c_void_p(16)
+    for op in (sf.OP_DIV, sf.OP_VECT_SCALAR, sf.OP_TENSION):
+        assert L.sfnl_product_f64(op, a, a, a, 10, 4, 6, 0, sf.ALGO_FAST, NULL) == -4
+        assert L.sfnl_product_split(op, a, a, a, 10, 4, 6, 3, NULL) == -4
+    assert L.sfnl_scalar_vect_f64(a, a, a, 10, 4, 6, 0, NULL) == -1
+
+
+def test_python_mirror_rejects_what_the_reference_rejects():
+    V = np.zeros((4, 6, 2), order="F")
+    S = np.zeros((4, 2, 2), order="F")
+    with pytest.raises(sf.SfnlError) as e:
+        sf.FFT_SCALAR_VECT_DCL(None, V, V, V, 1, 1, 5, 3)
+    assert e.value.code == -2
+    with pytest.raises(sf.SfnlError) as e:
+        sf.FFT_SCALAR_VECT_DCL(None, V, S, V, 0, 1, 5, 3)
+    assert e.value.code == -1
+    with pytest.raises(sf.SfnlError) as e:
+        sf.FFT_TENSOR_DCL(None, V, V, np.zeros((3, 4, 6, 2), order="F"), 1, 5, 3, opt_tension=False)
+    assert e.value.code == -1
+    with pytest.raises(sf.SfnlError) as e:  # V_out of the wrong shape
+        sf.FFT_TENSOR_DCL(None, V, V, V, 1, 5, 3)
+    assert e.value.code == -2

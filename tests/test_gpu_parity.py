@@ -39,7 +39,7 @@ def _sync():
 def test_golden_fixtures(path, algo):
     z = np.load(path)
     npts, m, pad, procs = (int(v) for v in z["meta"])
-    op = {"cross": 0, "dot": 1, "prod": 2}[str(z["op"])]
+    op = sf.KINDS[str(z["op"])][0]
     out = sf.product(op, dev(z["V1"]), dev(z["V2"]), m_max_pad=pad, algo=algo)
     _sync()
     assert R.rel_l2(host(out), z["out"]) <= FP64_TOL

@@ -13,6 +13,7 @@ import torch.distributed as dist
 import torch.multiprocessing as mp
 
 from oracle import ref_fft as R
+from sfemans_b200 import KINDS
 from sfemans_b200.parallel import fft_par_distributed, shard_range
 
 
@@ -37,28 +38,34 @@ def _free_port():
 def _oracle_compute(kind, xb, yb, m_max_pad):
     to_np = lambda t: np.asfortranarray(t.permute(2, 1, 0).contiguous().numpy().T)  # noqa: E731
     out = R.c_oracle(kind, to_np(xb), to_np(yb), m_max_pad)
-    return torch.from_numpy(np.ascontiguousarray(out.T)).permute(2, 1, 0)
+    return torch.from_numpy(np.ascontiguousarray(out.T)).permute(*reversed(range(out.ndim)))
 
 
 def _worker(rank, world, port, kind, npts, m, pad, bloc, q):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        nsl = 2 if kind == "prod" else 6
-        V1 = R.synthetic_field(npts, nsl, m, 0.2, 41)
-        V2 = R.synthetic_field(npts, nsl, m, 0.2, 42)
+        _, nsl1, nsl2, nout = KINDS[kind]
+        V1 = R.synthetic_field(npts, nsl1, m, 0.2, 41)
+        V2 = R.synthetic_field(npts, nsl2, m, 0.2, 42)
+        if kind in ("div", "svdiv"):
+            V2[:, 0, 0] += 4.0  # keep the divisor away from 0
         mc = m // world
         loc = lambda V: torch.from_numpy(np.ascontiguousarray(V[:, :, rank * mc:(rank + 1) * mc].T)).permute(2, 1, 0)  # noqa: E731
-        nout = 6 if kind == "cross" else 2
-        out = torch.zeros((mc, nout, npts), dtype=torch.float64).permute(2, 1, 0)
+        if kind in ("tensor", "tension"):
+            out = torch.zeros((mc, 6, npts, 3), dtype=torch.float64).permute(3, 2, 1, 0)
+        else:
+            out = torch.zeros((mc, nout, npts), dtype=torch.float64).permute(2, 1, 0)
         fft_par_distributed(kind, None, loc(V1), loc(V2), out, world, bloc, pad, compute=_oracle_compute)
-        ref = R.c_oracle(kind, V1, V2, pad)[:, :, rank * mc:(rank + 1) * mc]
+        ref = R.c_oracle(kind, V1, V2, pad)[..., rank * mc:(rank + 1) * mc]
         q.put((rank, float(np.abs(out.numpy() - ref).max())))
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("kind,world,npts,m", [("cross", 2, 23, 6), ("dot", 3, 31, 9), ("prod", 2, 40, 4)])
+@pytest.mark.parametrize("kind,world,npts,m", [("cross", 2, 23, 6), ("dot", 3, 31, 9), ("prod", 2, 40, 4),
+                                                ("div", 2, 17, 4), ("svect", 2, 19, 6), ("svdiv", 3, 13, 6),
+                                                ("tensor", 2, 21, 4), ("tension", 3, 11, 6)])
 def test_mode_distributed_layout_matches_single_rank(kind, world, npts, m):
     pad = 3 * m // 2
     bloc = npts // world + 1  # the callers' bloc_size (subroutine_ns_with_velocity.F90:625)
