@@ -170,6 +170,7 @@ struct FastArgs {
   unsigned adj_in;  // bit f: input field f is a cotangent (synthesise with D)
   int adj_out;      // 1: analyse without D (transpose of the synthesis)
   int accumulate;   // 1: out += result
+  int vec16;        // 1: every input row starts 16-byte aligned (bases aligned, np even): 16-byte copies
   const double *syn, *ana;
 };
 
@@ -217,12 +218,20 @@ struct EKDef<EK_TENSOR> {
 __host__ __device__ constexpr int ek_nin(int ek) { return ek == EK_PROD ? 2 : ek == EK_SVECT ? 4 : 6; }
 __host__ __device__ constexpr int ek_nout(int ek) { return ek == EK_CROSS || ek == EK_SVECT ? 3 : ek == EK_TENSOR ? 9 : 1; }
 // Shared memory of one CTA: folded products [NO][4][NT][2][32] and staged coefficients [NI][KT][8].
+// With NT <= 8 angle tiles every warp owns one tile (the launch uses min(NT, 8) warps, at least 2)
+// and the products overlay the coefficients.
 inline size_t fast_smem_bytes(int ek, int NT, int KT) {
-  return sizeof(double) * ((size_t)ek_nout(ek) * 4 * NT * 2 * 32 + (size_t)ek_nin(ek) * KT * 8);
+  const size_t prod = (size_t)ek_nout(ek) * 4 * NT * 2 * 32, coef = (size_t)ek_nin(ek) * KT * 8;
+  return sizeof(double) * (NT <= 8 ? (prod > coef ? prod : coef) : prod + coef);
 }
 
 __device__ __forceinline__ void cp_async8(void *smem_dst, const void *gsrc) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
+               "l"(gsrc)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
                "l"(gsrc)
                : "memory");
 }
@@ -248,7 +257,10 @@ template <int EK, int M, int ADJ>
 __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
   constexpr bool CT = M > 0;
   constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO;
-  extern __shared__ double ps[];  // [NO][4][NT][2][32] folded products, then the staged coefficients
+  // [NO][4][NT][2][32] folded products and the staged coefficients; when every warp owns at most one
+  // angle tile (NT <= NW) the products overlay the coefficients, written after a barrier that ends
+  // the synthesis, which halves the shared memory and leaves L1 room for the DFT tables
+  extern __shared__ double ps[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, NW = blockDim.x >> 5;
   const int g = lane >> 2, q = lane & 3;
   const int64_t p0 = (int64_t)blockIdx.x * 8, p = p0 + g;
@@ -272,26 +284,34 @@ __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
   const double invN = 1.0 / (4.0 * 8.0 * NT), twoN = 2.0 * invN;
 
   // ---- stage the tile's coefficients ----
-  // Global row r = 4*ks + q of field f (class c, mode index k = r - 4*KOFF[c]) holds 8 points;
-  // it lands at xs[((f*KS_tot + ks)*8 + point)*4 + q], so that lane (g, q) of a warp reads the
-  // A fragment of k-step ks as xs[(f*KS_tot + ks)*32 + lane]: 256 contiguous bytes.
-  double *xs = ps + (size_t)NO * 4 * NT * 2 * 32;
+  // Global row r = 4*ks + q of field f (class c, mode index k = r - 4*KOFF[c]) holds 8 points; it
+  // lands contiguously at xs[(f*KS_tot + ks)*32 + q*8 + point], so that lane (g, q) of a warp reads
+  // the A fragment of k-step ks at xs[(f*KS_tot + ks)*32 + q*8 + g]: 256 contiguous bytes.  Four
+  // consecutive threads copy one row (two points each, one 16-byte copy when the row is 16-byte
+  // aligned), so a warp instruction moves 8 whole 64-byte rows.
+  const bool overlay = NT <= NW;
+  double *xs = overlay ? ps : ps + (size_t)NO * 4 * NT * 2 * 32;
   {
-    const int pp = threadIdx.x & 7, rstep = blockDim.x >> 3;
-    const int64_t gp = p0 + pp;
-    const bool pv = gp < a.np;
+    const int pc = 2 * (threadIdx.x & 3), rstep = blockDim.x >> 2;
+    const bool v16 = a.vec16 && p0 + 8 <= a.np;
+    const bool pv0 = p0 + pc < a.np, pv1 = p0 + pc + 1 < a.np;
 #pragma unroll
     for (int f = 0; f < NI; ++f) {
-      const double *base = a.in[f] + (int64_t)b * a.in_bs[f] + (pv ? gp : 0);
-      double *xf = xs + (size_t)f * KS_tot * 32 + pp * 4;
-      for (int r = threadIdx.x >> 3; r < KT; r += rstep) {
+      const double *base = a.in[f] + (int64_t)b * a.in_bs[f] + p0 + pc;
+      const int64_t ldm = a.in_ldm[f];
+      double *xf = xs + (size_t)f * KS_tot * 32 + pc;
+      for (int r = threadIdx.x >> 2; r < KT; r += rstep) {
         const int c = (r >= 4 * KOFF[1]) + (r >= 4 * KOFF[2]) + (r >= 4 * KOFF[3]);
         const int k = r - 4 * sel4(KOFF, c), n = class_mode(c, k);
-        double *dst = xf + (size_t)(r >> 2) * 32 + (r & 3);
-        if (pv && k < sel4(KE, c) && !(c == 2 && n == 0))  // the sine of mode 0 is ignored
-          cp_async8(dst, base + (int64_t)n * a.in_ldm[f] + (c >= 2 ? a.np : 0));
-        else
-          *dst = 0.0;
+        double *dst = xf + (size_t)(r >> 2) * 32 + (r & 3) * 8;
+        const bool live = k < sel4(KE, c) && !(c == 2 && n == 0);  // the sine of mode 0 is ignored
+        const double *src = base + (int64_t)n * ldm + (c >= 2 ? a.np : 0);
+        if (live && v16) {
+          cp_async16(dst, src);
+        } else {
+          if (live && pv0) cp_async8(dst, src); else dst[0] = 0.0;
+          if (live && pv1) cp_async8(dst + 1, src + 1); else dst[1] = 0.0;
+        }
       }
     }
   }
@@ -299,15 +319,17 @@ __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
   __syncthreads();
 
   // ---- synthesis, fold, program, analysis pre-fold ----
-  for (int t = warp; t < NT; t += NW) {
+  for (int t0 = 0; t0 < NT; t0 += NW) {  // one pass when the products overlay the coefficients
+    const int t = t0 + warp;
     double acc[NI][4][2];
 #pragma unroll
     for (int f = 0; f < NI; ++f)
 #pragma unroll
       for (int c = 0; c < 4; ++c) acc[f][c][0] = acc[f][c][1] = 0.0;
+    if (t < NT) {
     // k-steps outermost, the four classes inside: 4*NI independent accumulator chains per step
     const double *syn_t = a.syn + (size_t)t * 32 + lane;
-    const double *xs_l = xs + lane;
+    const double *xs_l = xs + (lane & 3) * 8 + (lane >> 2);
 #pragma unroll
     for (int s = 0; s < ks_max; ++s) {
 #pragma unroll
@@ -328,6 +350,9 @@ __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
         for (int f = 0; f < NI; ++f) dmma(acc[f][c], av[f], bv);
       }
     }
+    }
+    if (overlay) __syncthreads();  // every warp has read its last coefficient
+    if (t >= NT) continue;
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
       double v[4][NI];
@@ -363,17 +388,29 @@ __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
   for (int cu = warp; cu < NU_tot; cu += NW) {
     const int c = (cu >= NOFF[1]) + (cu >= NOFF[2]) + (cu >= NOFF[3]);
     const int u = cu - sel4(NOFF, c), kec = sel4(KE, c);
-    double y[NO][2];
+    // PC partial sums per output over alternating k-steps: NO*PC independent accumulator chains
+    constexpr int PC = NO >= 6 ? 1 : NO >= 3 ? 2 : 4;
+    double y[NO][2], yp[PC][NO][2];
 #pragma unroll
-    for (int o = 0; o < NO; ++o) y[o][0] = y[o][1] = 0.0;
+    for (int i = 0; i < PC; ++i)
+#pragma unroll
+      for (int o = 0; o < NO; ++o) yp[i][o][0] = yp[i][o][1] = 0.0;
     const double *bt = anav + (size_t)cu * NT * 2 * 32;
     const double *pa = ps + (size_t)c * NT * 2 * 32 + lane;
 #pragma unroll
     for (int te = 0; te < 2 * NT; ++te) {
       const double bv = __ldg(bt + (size_t)te * 32);
 #pragma unroll
-      for (int o = 0; o < NO; ++o) dmma(y[o], pa[((size_t)o * 4 * NT * 2 + te) * 32], bv);
+      for (int o = 0; o < NO; ++o) dmma(yp[te % PC][o], pa[((size_t)o * 4 * NT * 2 + te) * 32], bv);
     }
+#pragma unroll
+    for (int o = 0; o < NO; ++o)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        y[o][h] = yp[0][o][h];
+#pragma unroll
+        for (int i = 1; i < PC; ++i) y[o][h] += yp[i][o][h];
+      }
     if (!valid) continue;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -435,6 +472,17 @@ int launch_ek(FastArgs &fa, int batch, cudaStream_t st) {
   return launch_ek_adj<EK, 0>(fa, batch, st);
 }
 
+}  // namespace
+
+namespace {
+// 16-byte copies of whole rows need every row start 16-byte aligned: field bases, the sine offset np,
+// the mode stride and the batch stride all multiples of two doubles.
+int rows_aligned16(const FastArgs &fa, int ni) {
+  if (fa.np & 1) return 0;
+  for (int i = 0; i < ni; ++i)
+    if ((reinterpret_cast<uintptr_t>(fa.in[i]) & 15) || (fa.in_ldm[i] & 1) || (fa.in_bs[i] & 1)) return 0;
+  return 1;
+}
 }  // namespace
 
 int decompose_program(int op, std::vector<Elem> &seq) {
@@ -538,6 +586,7 @@ int launch_fast(const ProgArgs &a, cudaStream_t st) {
     fa.adj_in = e.adj;
     fa.adj_out = adj_out ? 1 : 0;
     fa.accumulate = e.acc;
+    fa.vec16 = rows_aligned16(fa, ni);
     fa.syn = T.syn;
     fa.ana = T.ana;
     int r = e.ek == EK_CROSS  ? launch_ek<EK_CROSS>(fa, a.batch, st)
@@ -666,6 +715,7 @@ extern "C" int sfnl_cross_f64_noalloc(const double *v1, const double *v2, double
     fa.ke[c] = g.ke[c];
   }
   fa.NU_tot = g.NU_tot;
+  fa.vec16 = rows_aligned16(fa, 6);
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
     return set_error(SFNL_ERR_CUDA, "sfnl_cross_f64_noalloc: no current device");

@@ -2,7 +2,8 @@
 
     python -m sfemans_b200.profile_case --program bundle --form fast --np 100000 --m 64 --reps 1
 
-Programs: cross, dot, prod (the three reference routines) and bundle (u x w, u x b, j x b, u . gradT).
+Programs: cross, dot, prod, div, svect, svdiv, tensor, tension (the reference routines, by the op names of
+sfemans_b200.KINDS) and bundle (u x w, u x b, j x b, u . gradT).
 Forms: fast (FP64, folded transforms), grid (FP64, caller's grid), split3 / split2 (bf16 slices on tcgen05).
 Inputs are N(0,1)*exp(-alpha*n) coefficients generated on the device; the padding is m_max_pad = 3*m/2.
 Prints the average milliseconds per call, timed with CUDA events after one untimed call.
@@ -27,7 +28,7 @@ def main(argv=None):
     import sfemans_b200 as sf
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--program", default="cross", choices=["cross", "dot", "prod", "bundle"])
+    ap.add_argument("--program", default="cross", choices=list(sf.KINDS) + ["bundle"])
     ap.add_argument("--form", default="fast", choices=["fast", "grid", "split3", "split2"])
     ap.add_argument("--np", type=int, default=100_000)
     ap.add_argument("--m", type=int, default=64)
@@ -42,10 +43,11 @@ def main(argv=None):
         outs = tuple(sf.fortran_empty(a.np, 6, a.m) for _ in range(3)) + (sf.fortran_empty(a.np, 2, a.m),)
         call = lambda: sf.bundle_mhd(*ins, m_max_pad=pad, outs=outs, **kw)  # noqa: E731
     else:
-        op = {"cross": sf.OP_CROSS, "dot": sf.OP_DOT, "prod": sf.OP_PROD}[a.program]
-        nsl = 2 if op == sf.OP_PROD else 6
-        x, y = _field(torch, a.np, nsl, a.m, a.alpha, 1), _field(torch, a.np, nsl, a.m, a.alpha, 2)
-        out = sf.fortran_empty(a.np, 6 if op == sf.OP_CROSS else 2, a.m)
+        op, nsl1, nsl2, _ = sf.KINDS[a.program]
+        x, y = _field(torch, a.np, nsl1, a.m, a.alpha, 1), _field(torch, a.np, nsl2, a.m, a.alpha, 2)
+        if a.program in ("div", "svdiv"):
+            y[:, 0, 0] += 4.0  # keep the divisor away from 0
+        out = sf.out_empty(op, a.np, a.m)
         call = lambda: sf.product(op, x, y, out=out, m_max_pad=pad, **kw)  # noqa: E731
     call()
     torch.cuda.synchronize()
