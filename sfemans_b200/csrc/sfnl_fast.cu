@@ -40,6 +40,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "sfnl_internal.h"
@@ -218,11 +219,17 @@ struct EKDef<EK_TENSOR> {
 __host__ __device__ constexpr int ek_nin(int ek) { return ek == EK_PROD ? 2 : ek == EK_SVECT ? 4 : 6; }
 __host__ __device__ constexpr int ek_nout(int ek) { return ek == EK_CROSS || ek == EK_SVECT ? 3 : ek == EK_TENSOR ? 9 : 1; }
 // Shared memory of one CTA: folded products [NO][4][NT][2][32] and staged coefficients [NI][KT][8].
-// With NT <= 8 angle tiles every warp owns one tile (the launch uses min(NT, 8) warps, at least 2)
-// and the products overlay the coefficients.
-inline size_t fast_smem_bytes(int ek, int NT, int KT) {
+// With NT <= 8 angle tiles every warp (pair, with the class split) owns one tile and the products
+// (and the exchange) overlay the coefficients.
+// The class split (two warps per angle tile, one per class pair) halves the accumulators of a warp
+// and doubles the warps per SM; it pays for the six-field programs at m >= 64, where the accumulator
+// registers limit residency, and costs shared memory and a barrier elsewhere (measured on B200).
+constexpr bool class_split(int ek, int M) { return (ek == EK_CROSS || ek == EK_DOT) && (M == 64 || M == 0); }
+inline size_t fast_smem_bytes(int ek, int NT, int KT, bool cs) {
+  const int nwt = NT < 8 ? NT : 8;
   const size_t prod = (size_t)ek_nout(ek) * 4 * NT * 2 * 32, coef = (size_t)ek_nin(ek) * KT * 8;
-  return sizeof(double) * (NT <= 8 ? (prod > coef ? prod : coef) : prod + coef);
+  const size_t xch = cs ? (size_t)nwt * ek_nin(ek) * 128 : 0;
+  return sizeof(double) * (NT <= 8 ? (prod + xch > coef ? prod + xch : coef) : prod + xch + coef);
 }
 
 __device__ __forceinline__ void cp_async8(void *smem_dst, const void *gsrc) {
@@ -253,14 +260,15 @@ __device__ __forceinline__ int sel4(const int (&v)[4], int c) { return c == 0 ? 
 
 // EK: elementary program; M: modes when specialised (0: any m, geometry at run time);
 // ADJ: 0 plain, 1 first operand (fields 0-2) a cotangent, 2 second operand (fields 3-5) a cotangent.
-template <int EK, int M, int ADJ>
-__global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
+template <int EK, int M, int ADJ, bool CS>
+__global__ void __launch_bounds__(CS ? 512 : 256) fast_kernel(const FastArgs a) {
   constexpr bool CT = M > 0;
   constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO;
-  // [NO][4][NT][2][32] folded products and the staged coefficients; when every warp owns at most one
-  // angle tile (NT <= NW) the products overlay the coefficients, written after a barrier that ends
-  // the synthesis, which halves the shared memory and leaves L1 room for the DFT tables
-  extern __shared__ double ps[];
+  // Shared memory: folded products ps [NO][4][NT][2][32], with the class split (CS) the exchange
+  // between the two warps of an angle tile xc [NW/2][2][NI][2][32], and the staged coefficients
+  // xs [NI][KT/4][4][8].  When every warp (pair) owns at most one angle tile, ps and xc overlay xs
+  // (written after a barrier that ends the synthesis), which leaves L1 room for the DFT tables.
+  extern __shared__ double smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, NW = blockDim.x >> 5;
   const int g = lane >> 2, q = lane & 3;
   const int64_t p0 = (int64_t)blockIdx.x * 8, p = p0 + g;
@@ -289,8 +297,11 @@ __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
   // the A fragment of k-step ks at xs[(f*KS_tot + ks)*32 + q*8 + g]: 256 contiguous bytes.  Four
   // consecutive threads copy one row (two points each, one 16-byte copy when the row is 16-byte
   // aligned), so a warp instruction moves 8 whole 64-byte rows.
-  const bool overlay = NT <= NW;
-  double *xs = overlay ? ps : ps + (size_t)NO * 4 * NT * 2 * 32;
+  const int NWT = CS ? NW >> 1 : NW;  // angle tiles per pass (two warps per tile with the class split)
+  const bool overlay = NT <= NWT;
+  const size_t prod_d = (size_t)NO * 4 * NT * 2 * 32, xch_d = CS ? (size_t)NWT * NI * 128 : 0;
+  double *ps = smem, *xc = smem + prod_d;
+  double *xs = overlay ? smem : smem + prod_d + xch_d;
   {
     const int pc = 2 * (threadIdx.x & 3), rstep = blockDim.x >> 2;
     const bool v16 = a.vec16 && p0 + 8 <= a.np;
@@ -318,70 +329,170 @@ __global__ void __launch_bounds__(256) fast_kernel(const FastArgs a) {
   cp_async_wait_all();
   __syncthreads();
 
-  // ---- synthesis, fold, program, analysis pre-fold ----
-  for (int t0 = 0; t0 < NT; t0 += NW) {  // one pass when the products overlay the coefficients
-    const int t = t0 + warp;
-    double acc[NI][4][2];
-#pragma unroll
-    for (int f = 0; f < NI; ++f)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) acc[f][c][0] = acc[f][c][1] = 0.0;
-    if (t < NT) {
-    // k-steps outermost, the four classes inside: 4*NI independent accumulator chains per step
-    const double *syn_t = a.syn + (size_t)t * 32 + lane;
-    const double *xs_l = xs + (lane & 3) * 8 + (lane >> 2);
-#pragma unroll
-    for (int s = 0; s < ks_max; ++s) {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        if (s >= KS[c]) continue;
-        const double bv = __ldg(syn_t + (size_t)(KOFF[c] + s) * NT * 32);
-        const double *xa = xs_l + (size_t)(KOFF[c] + s) * 32;
-        double av[NI];
-#pragma unroll
-        for (int f = 0; f < NI; ++f) av[f] = xa[(size_t)f * KS_tot * 32];
-        if constexpr (ADJ != 0) {
-          const double wn = (s == 0 && q == 0 && (c & 1) == 0) ? invN : twoN;  // n == 0 only there
-#pragma unroll
-          for (int f = 0; f < NI; ++f)
-            if ((ADJ == 1 && f < 3) || (ADJ == 2 && f >= 3)) av[f] *= wn;
+  if constexpr (CS) {
+    // ---- synthesis, fold, program, analysis pre-fold ----
+    // The two warps of angle tile t split the classes: warp half 0 accumulates the cosine classes
+    // (CE, CO), half 1 the sine classes (SE, SO), 2*NI accumulator chains each.  They then swap half of
+    // their folded sums (A = CE+CO, B = CE-CO against C = SE+SO, D = SO-SE) through shared memory, and
+    // half e evaluates the program and the analysis pre-fold for the angles of k-step parity e.
+    const int wp = warp >> 1, half = warp & 1;
+    for (int t0 = 0; t0 < NT; t0 += NWT) {  // one pass when ps and xc overlay the coefficients
+      const int t = t0 + wp;
+      double acc[NI][2][2];
+  #pragma unroll
+      for (int f = 0; f < NI; ++f)
+  #pragma unroll
+        for (int cc = 0; cc < 2; ++cc) acc[f][cc][0] = acc[f][cc][1] = 0.0;
+      auto synth = [&](auto cb_tag) {
+        constexpr int CB = decltype(cb_tag)::value;  // first class of this warp's pair
+        const double *syn_t = a.syn + (size_t)t * 32 + lane;
+        const double *xs_l = xs + (lane & 3) * 8 + (lane >> 2);
+  #pragma unroll
+        for (int s = 0; s < ks_max; ++s) {
+  #pragma unroll
+          for (int cc = 0; cc < 2; ++cc) {
+            const int c = CB + cc;
+            if (s >= KS[c]) continue;
+            const double bv = __ldg(syn_t + (size_t)(KOFF[c] + s) * NT * 32);
+            const double *xa = xs_l + (size_t)(KOFF[c] + s) * 32;
+            double av[NI];
+  #pragma unroll
+            for (int f = 0; f < NI; ++f) av[f] = xa[(size_t)f * KS_tot * 32];
+            if constexpr (ADJ != 0) {
+              const double wn = (s == 0 && q == 0 && (c & 1) == 0) ? invN : twoN;  // n == 0 only there
+  #pragma unroll
+              for (int f = 0; f < NI; ++f)
+                if ((ADJ == 1 && f < 3) || (ADJ == 2 && f >= 3)) av[f] *= wn;
+            }
+  #pragma unroll
+            for (int f = 0; f < NI; ++f) dmma(acc[f][cc], av[f], bv);
+          }
         }
-#pragma unroll
-        for (int f = 0; f < NI; ++f) dmma(acc[f][c], av[f], bv);
+      };
+      if (t < NT) {
+        if (half == 0)
+          synth(std::integral_constant<int, 0>{});
+        else
+          synth(std::integral_constant<int, 2>{});
+      }
+      if (overlay) __syncthreads();  // every warp has read its last coefficient
+      // sums and differences of the pair's classes at parity e: (A, B) for half 0, (C, D) for half 1
+      auto pair_sums = [&](int f, int e, double &X, double &Y) {
+        const double lo = e ? acc[f][0][1] : acc[f][0][0], hi = e ? acc[f][1][1] : acc[f][1][0];
+        X = lo + hi;
+        Y = half ? hi - lo : lo - hi;
+      };
+      double *xw = xc + (size_t)wp * 2 * NI * 64 + lane;  // [writer half][f][X, Y][32]
+      if (t < NT) {
+  #pragma unroll
+        for (int f = 0; f < NI; ++f) {
+          double X, Y;
+          pair_sums(f, 1 - half, X, Y);  // the parity the partner finishes
+          xw[((half * NI + f) * 2 + 0) * 32] = X;
+          xw[((half * NI + f) * 2 + 1) * 32] = Y;
+        }
+      }
+      __syncthreads();
+      if (t < NT) {
+        const int e = half;
+        double v[4][NI];
+  #pragma unroll
+        for (int f = 0; f < NI; ++f) {
+          double X, Y;
+          pair_sums(f, e, X, Y);
+          const double Xp = xw[(((1 - half) * NI + f) * 2 + 0) * 32], Yp = xw[(((1 - half) * NI + f) * 2 + 1) * 32];
+          const double A = half ? Xp : X, B = half ? Yp : Y, C = half ? X : Xp, D = half ? Y : Yp;
+          v[0][f] = A + C;  // theta
+          v[1][f] = B + D;  // pi - theta
+          v[2][f] = B - D;  // pi + theta
+          v[3][f] = A - C;  // 2 pi - theta
+        }
+        double gq[4][NO];
+  #pragma unroll
+        for (int r = 0; r < 4; ++r) EKDef<EK>::op(v[r], gq[r]);
+  #pragma unroll
+        for (int o = 0; o < NO; ++o) {
+          const double s14 = gq[0][o] + gq[3][o], d14 = gq[0][o] - gq[3][o];
+          const double s23 = gq[1][o] + gq[2][o], d32 = gq[2][o] - gq[1][o];
+          double *dst = ps + ((size_t)((o * 4) * NT + t) * 2 + e) * 32 + lane;
+          const size_t cstride = (size_t)NT * 2 * 32;
+          dst[0] = s14 + s23;            // PE
+          dst[cstride] = s14 - s23;      // PO
+          dst[2 * cstride] = d14 + d32;  // QE
+          dst[3 * cstride] = d14 - d32;  // QO
+        }
+      }
+      if (!overlay) __syncthreads();  // xc is rewritten by the next pass
+    }
+    __syncthreads();
+
+  } else {
+    // ---- synthesis, fold, program, analysis pre-fold ----
+    for (int t0 = 0; t0 < NT; t0 += NW) {  // one pass when the products overlay the coefficients
+      const int t = t0 + warp;
+      double acc[NI][4][2];
+  #pragma unroll
+      for (int f = 0; f < NI; ++f)
+  #pragma unroll
+        for (int c = 0; c < 4; ++c) acc[f][c][0] = acc[f][c][1] = 0.0;
+      if (t < NT) {
+      // k-steps outermost, the four classes inside: 4*NI independent accumulator chains per step
+      const double *syn_t = a.syn + (size_t)t * 32 + lane;
+      const double *xs_l = xs + (lane & 3) * 8 + (lane >> 2);
+  #pragma unroll
+      for (int s = 0; s < ks_max; ++s) {
+  #pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          if (s >= KS[c]) continue;
+          const double bv = __ldg(syn_t + (size_t)(KOFF[c] + s) * NT * 32);
+          const double *xa = xs_l + (size_t)(KOFF[c] + s) * 32;
+          double av[NI];
+  #pragma unroll
+          for (int f = 0; f < NI; ++f) av[f] = xa[(size_t)f * KS_tot * 32];
+          if constexpr (ADJ != 0) {
+            const double wn = (s == 0 && q == 0 && (c & 1) == 0) ? invN : twoN;  // n == 0 only there
+  #pragma unroll
+            for (int f = 0; f < NI; ++f)
+              if ((ADJ == 1 && f < 3) || (ADJ == 2 && f >= 3)) av[f] *= wn;
+          }
+  #pragma unroll
+          for (int f = 0; f < NI; ++f) dmma(acc[f][c], av[f], bv);
+        }
+      }
+      }
+      if (overlay) __syncthreads();  // every warp has read its last coefficient
+      if (t >= NT) continue;
+  #pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        double v[4][NI];
+  #pragma unroll
+        for (int f = 0; f < NI; ++f) {
+          const double A = acc[f][0][e] + acc[f][1][e], B = acc[f][0][e] - acc[f][1][e];
+          const double C = acc[f][2][e] + acc[f][3][e], D = acc[f][3][e] - acc[f][2][e];
+          v[0][f] = A + C;  // theta
+          v[1][f] = B + D;  // pi - theta
+          v[2][f] = B - D;  // pi + theta
+          v[3][f] = A - C;  // 2 pi - theta
+        }
+        double gq[4][NO];
+  #pragma unroll
+        for (int r = 0; r < 4; ++r) EKDef<EK>::op(v[r], gq[r]);
+  #pragma unroll
+        for (int o = 0; o < NO; ++o) {
+          const double s14 = gq[0][o] + gq[3][o], d14 = gq[0][o] - gq[3][o];
+          const double s23 = gq[1][o] + gq[2][o], d32 = gq[2][o] - gq[1][o];
+          double *dst = ps + ((size_t)((o * 4) * NT + t) * 2 + e) * 32 + lane;
+          const size_t cstride = (size_t)NT * 2 * 32;
+          dst[0] = s14 + s23;            // PE
+          dst[cstride] = s14 - s23;      // PO
+          dst[2 * cstride] = d14 + d32;  // QE
+          dst[3 * cstride] = d14 - d32;  // QO
+        }
       }
     }
-    }
-    if (overlay) __syncthreads();  // every warp has read its last coefficient
-    if (t >= NT) continue;
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      double v[4][NI];
-#pragma unroll
-      for (int f = 0; f < NI; ++f) {
-        const double A = acc[f][0][e] + acc[f][1][e], B = acc[f][0][e] - acc[f][1][e];
-        const double C = acc[f][2][e] + acc[f][3][e], D = acc[f][3][e] - acc[f][2][e];
-        v[0][f] = A + C;  // theta
-        v[1][f] = B + D;  // pi - theta
-        v[2][f] = B - D;  // pi + theta
-        v[3][f] = A - C;  // 2 pi - theta
-      }
-      double gq[4][NO];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) EKDef<EK>::op(v[r], gq[r]);
-#pragma unroll
-      for (int o = 0; o < NO; ++o) {
-        const double s14 = gq[0][o] + gq[3][o], d14 = gq[0][o] - gq[3][o];
-        const double s23 = gq[1][o] + gq[2][o], d32 = gq[2][o] - gq[1][o];
-        double *dst = ps + ((size_t)((o * 4) * NT + t) * 2 + e) * 32 + lane;
-        const size_t cstride = (size_t)NT * 2 * 32;
-        dst[0] = s14 + s23;            // PE
-        dst[cstride] = s14 - s23;      // PO
-        dst[2 * cstride] = d14 + d32;  // QE
-        dst[3 * cstride] = d14 - d32;  // QO
-      }
-    }
+    __syncthreads();
+
   }
-  __syncthreads();
 
   // ---- analysis: output tiles (class c, tile u) ----
   const double *anav = a.ana + (size_t)(a.adj_out ? 1 : 0) * NU_tot * NT * 2 * 32 + lane;
@@ -435,12 +546,13 @@ template <int EK, int M, int ADJ>
 int launch_ek_m(FastArgs &fa, int batch, cudaStream_t st) {
   constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO;
   static_assert(ek_nin(EK) == NI && ek_nout(EK) == NO, "elementary program table");
+  constexpr bool CS = class_split(EK, M);
   fa.KT = 4 * (fa.KS[0] + fa.KS[1] + fa.KS[2] + fa.KS[3]);
-  const size_t smem = fast_smem_bytes(EK, fa.NT, fa.KT);
+  const size_t smem = fast_smem_bytes(EK, fa.NT, fa.KT, CS);
   if (smem > 200 * 1024) return set_error(SFNL_ERR_UNSUPPORTED, "FAST form: m too large for shared memory");
-  int nw = fa.NT < 8 ? fa.NT : 8;
-  if (nw < 2) nw = 2;
-  auto kern = fast_kernel<EK, M, ADJ>;
+  const int tiles_per_pass = fa.NT < 8 ? fa.NT : 8;
+  const int nw = CS ? 2 * tiles_per_pass : (tiles_per_pass < 2 ? 2 : tiles_per_pass);
+  auto kern = fast_kernel<EK, M, ADJ, CS>;
   if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (fast form)");
   const int64_t tiles = (fa.np + 7) / 8;
@@ -542,7 +654,7 @@ bool fast_supported(int op, int m, int N) {
   if (m < 1 || m > 512 || !op_bilinear(op)) return false;
   const Geo g = make_geo(m);
   // the largest elementary program of the op decides (the tensor's nine outputs, else a cross product)
-  return g.N == N && fast_smem_bytes(op == OP_TENSOR ? EK_TENSOR : EK_CROSS, g.NT, 4 * g.KS_tot) <= 200 * 1024;
+  return g.N == N && fast_smem_bytes(op == OP_TENSOR ? EK_TENSOR : EK_CROSS, g.NT, 4 * g.KS_tot, true) <= 200 * 1024;
 }
 
 int launch_fast(const ProgArgs &a, cudaStream_t st) {
