@@ -260,8 +260,14 @@ __device__ __forceinline__ int sel4(const int (&v)[4], int c) { return c == 0 ? 
 
 // EK: elementary program; M: modes when specialised (0: any m, geometry at run time);
 // ADJ: 0 plain, 1 first operand (fields 0-2) a cotangent, 2 second operand (fields 3-5) a cotangent.
+// Launch bounds (measured on B200): the class-split cross product at m = 64 runs best at 3 CTAs of 12
+// warps per SM (56 registers); the tensor program wants registers (no residency target); the others
+// keep the compiler's default register target.
+constexpr int fast_max_threads(int M, bool cs) { return cs ? (M == 64 ? 384 : 512) : 256; }
+constexpr int fast_min_blocks(int ek, int M, bool cs) { return (cs && M == 64 && ek == EK_CROSS) ? 3 : ek == EK_TENSOR ? 1 : 0; }
+
 template <int EK, int M, int ADJ, bool CS>
-__global__ void __launch_bounds__(CS ? 512 : 256) fast_kernel(const FastArgs a) {
+__global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M, CS)) fast_kernel(const FastArgs a) {
   constexpr bool CT = M > 0;
   constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO;
   // Shared memory: folded products ps [NO][4][NT][2][32], with the class split (CS) the exchange
