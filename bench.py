@@ -2,7 +2,7 @@
 """Throughput of the dealiased MHD nonlinear bundle on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload mhd_bundle|cross_28k|jvp_700k] [--form auto|fp64|split2|split3]
+                    [--workload mhd_bundle|cross_28k|jvp_700k] [--form fp64|split3|split2|grid|auto]
 
 One step = one pass of the nonlinear term over one batch of synthetic
 coefficients.  The default workload is the full MHD bundle: 1.4M Gauss
@@ -17,6 +17,11 @@ library's host-array entry point (sfnl_bundle_mhd_host) with pinned host
 buffers, the copies inside the timed region.  Multi-GPU (torchrun) is weak
 scaling: every rank runs the full workload on its own points, no collective
 on the data path; the job time is the max over ranks.
+
+The line reports ``--form`` (default fp64: the FAST all-FP64 form, the
+library's default path); every other form is also timed on a few steps and
+listed under "forms".  ``--form auto`` reports the fastest form that meets
+its accuracy bar instead.
 """
 from __future__ import annotations
 
@@ -70,7 +75,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -80,6 +85,14 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+
+    def wait_first(self, timeout=5.0):
+        import time
+
+        t0 = time.time()
+        while self.proc and not self.lines and time.time() - t0 < timeout:
+            time.sleep(0.02)
+        self.lines.clear()  # keep only the samples taken during the timed region
 
     def stop(self):
         if not self.proc:
@@ -171,11 +184,11 @@ def run_reference(args, world, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mhd_bundle", choices=sorted(WORKLOADS))
-    ap.add_argument("--form", default="auto", choices=["auto", "fp64", "grid", "split2", "split3"])
+    ap.add_argument("--form", default="fp64", choices=["auto", "fp64", "grid", "split2", "split3"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-sample", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -212,7 +225,11 @@ def main():
              "split2": dict(split=sf.SPLIT_BF16X2), "grid": dict(algo=sf.ALGO_GRID)}
     launches = {"fp64": 4, "split3": 4, "split2": 4, "grid": 1} if args.workload == "mhd_bundle" else \
         {"fp64": 1, "split3": 1, "split2": 1, "grid": 1}
-    order = ["fp64", "split3", "split2", "grid"] if args.form == "auto" else [args.form if args.form != "fp64" else "fp64"]
+    # every form is timed (the others after the reported one, on fewer steps); the line reports --form,
+    # or with --form auto the fastest form that meets its accuracy bar
+    order = ["fp64", "split3", "split2", "grid"]
+    if args.form not in ("auto", "fp64"):
+        order = [args.form] + [f for f in order if f != args.form]
     stream = torch.cuda.current_stream()
 
     # reference outputs on a bounded sample (rank 0, one GPU): the CPU port, also timed as the CPU baseline
@@ -230,7 +247,7 @@ def main():
         except sf.SfnlError as e:
             results[form] = {"unavailable": str(e)}
             continue
-        steps = args.steps if form == order[0] or form == "fp64" else min(args.steps, 3)
+        steps = args.steps if form == order[0] else min(args.steps, 3)
         ms, clk = _time_steps(lambda: _call(sf, args.workload, ins, outs, pad, kw), steps, args.warmup, stream, world,
                               dist, local)
         r = {"ms_per_step": ms, "value": world * npts * m / (ms / 1e3), "steps": steps, "gpu_launches_per_step": launches[form]}
@@ -238,7 +255,7 @@ def main():
             names = ["uxw", "uxb", "jxb", "ugradt"] if args.workload == "mhd_bundle" else ["uxw"]
             r["rel_l2_vs_cpu_port"] = {n: R_rel_l2(sf.to_host(o[:sample]), rr) for n, o, rr in zip(names, outs, ref)}
         results[form] = r
-        if form == "fp64" or clk_all is None:
+        if form == order[0]:
             clk_all = clk
 
     def ok(f):
@@ -248,8 +265,13 @@ def main():
         if "rel_l2_vs_cpu_port" in r:
             return max(r["rel_l2_vs_cpu_port"].values()) <= 1e-7
         return f in ("fp64", "grid", "split3")  # bars enforced by the -m gpu tests
-    cands = [f for f in results if ok(f)]
-    best = min(cands, key=lambda f: results[f]["ms_per_step"])
+    if args.form == "auto":
+        cands = [f for f in results if ok(f)]
+        best = min(cands, key=lambda f: results[f]["ms_per_step"])
+    else:
+        best = order[0]
+        if "ms_per_step" not in results.get(best, {}):
+            raise SystemExit(f"form {best} unavailable: {results.get(best)}")
     ms = results[best]["ms_per_step"]
     value = results[best]["value"]
 
@@ -312,6 +334,7 @@ def _time_steps(step, steps, warmup, stream, world, dist, local):
         dist.barrier()
     clocks = ClockSampler(local)
     clocks.start()
+    clocks.wait_first()  # nvidia-smi takes a few hundred ms to start: sample the whole timed region
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
     ev[0].record(stream)
     for i in range(steps):
