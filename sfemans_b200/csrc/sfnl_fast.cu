@@ -156,6 +156,105 @@ int get_tables(const Geo &g, Tables *out) {
 }
 
 // ---------------------------------------------------------------------------
+// third fold: the mirror symmetry theta -> pi/2 - theta of the quadrant grid
+// ---------------------------------------------------------------------------
+// On theta_j = pi(2j+1)/(4Q) the quadrant is its own mirror: theta_{Q-1-j} = pi/2 - theta_j.  For even
+// n, cos(n(pi/2 - x)) = (-1)^(n/2) cos(nx) and sin(n(pi/2 - x)) = -(-1)^(n/2) sin(nx).  So an even class
+// split into its n = 0 mod 4 and n = 2 mod 4 parts (E0, E2) gives both mirror angles from one of them:
+// CE(x) = E0 + E2, CE(pi/2 - x) = E0 - E2 and SE(x) = S0 + S2, SE(pi/2 - x) = S2 - S0, each part having
+// half the modes; and the analysis of an even class contracts P(x) +- P(pi/2 - x) over half the quadrant
+// for each part.  The odd classes gain nothing (their mirror is the other trigonometric function).
+// With NT even, angle tile t and its mirror NT-1-t form a pair: local angle a of one is local angle 7-a
+// of the other, i.e. lane (g, 3-q) (lane ^ 3) and the other k-step parity e.  A quarter of the DMMAs of
+// both transforms goes.
+//
+// Row and output groups: 0 CE0, 1 CE2, 2 CO, 3 SE0, 4 SE2, 5 SO (cosine coefficients for 0-2, sine 3-5).
+__host__ __device__ constexpr int tf_ke(int m, int gr) {
+  return (gr % 3 == 0) ? (m + 3) / 4 : (gr % 3 == 1) ? (m + 1) / 4 : m / 2;
+}
+__host__ __device__ constexpr int tf_mode(int gr, int k) { return gr % 3 == 0 ? 4 * k : gr % 3 == 1 ? 4 * k + 2 : 2 * k + 1; }
+__host__ __device__ constexpr int tf_KS(int m, int gr) { return (tf_ke(m, gr) + 3) / 4; }
+__host__ __device__ constexpr int tf_koff(int m, int gr) { return gr == 0 ? 0 : tf_koff(m, gr - 1) + tf_KS(m, gr - 1); }
+__host__ __device__ constexpr int tf_NU(int m, int gr) { return (tf_ke(m, gr) + 7) / 8; }
+__host__ __device__ constexpr int tf_nuoff(int m, int gr) { return gr == 0 ? 0 : tf_nuoff(m, gr - 1) + tf_NU(m, gr - 1); }
+// quadrant angle tiles and analysis k-steps of an output group (half the quadrant for the even groups)
+__host__ __device__ constexpr int tf_NT(int m) { return ((3 * m - 2 + 3) / 4 + 7) / 8; }
+__host__ __device__ constexpr int tf_TE(int m, int gr) { return gr % 3 == 2 ? 2 * tf_NT(m) : tf_NT(m); }
+// first analysis k-step (units of 32 doubles) of group gr in the analysis table
+__host__ __device__ constexpr int tf_aoff(int m, int gr) {
+  return gr == 0 ? 0 : tf_aoff(m, gr - 1) + tf_NU(m, gr - 1) * tf_TE(m, gr - 1);
+}
+// the third fold needs an even number of angle tiles; it is built for the specialised m = 64 kernels
+constexpr bool third_fold(int M) { return M == 64 && tf_NT(M) % 2 == 0; }
+
+// Tables of the third fold for m (a Geo with make_geo(m).N): synthesis B fragments
+// [KS_tot][NT][32] (lane (g, q): mode tf_mode(gr, 4s + q), angle 8t + g) and analysis B fragments
+// [2 variants][sum of NU * TE][32] (lane (g, q): mode tf_mode(gr, 8u + g), angle 8t + 2q + e; variant 0
+// carries the analysis weights, variant 1 not).
+std::mutex g_tftab_mu;
+std::map<std::pair<int, int>, Tables> g_tftabs;  // (device, m) -> tables
+
+int get_tf_tables(const Geo &g, Tables *out) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_tftab_mu);
+  auto it = g_tftabs.find({dev, g.m});
+  if (it != g_tftabs.end()) {
+    *out = it->second;
+    return SFNL_OK;
+  }
+  const long double pi = acosl(-1.0L);
+  auto ang = [&](int j) { return pi * (long double)(2 * j + 1) / (long double)g.N; };
+  int ks_tot = 0, asteps = 0;
+  for (int gr = 0; gr < 6; ++gr) {
+    ks_tot += tf_KS(g.m, gr);
+    asteps += tf_NU(g.m, gr) * tf_TE(g.m, gr);
+  }
+  std::vector<double> syn((size_t)ks_tot * g.NT * 32, 0.0);
+  for (int gr = 0; gr < 6; ++gr)
+    for (int s = 0; s < tf_KS(g.m, gr); ++s)
+      for (int t = 0; t < g.NT; ++t)
+        for (int l = 0; l < 32; ++l) {
+          const int k = 4 * s + (l & 3), j = 8 * t + (l >> 2);
+          double v = 0.0;
+          if (k < tf_ke(g.m, gr)) {
+            const long double x = (long double)tf_mode(gr, k) * ang(j);
+            v = (double)(gr < 3 ? cosl(x) : sinl(x));
+          }
+          syn[(((size_t)(tf_koff(g.m, gr) + s)) * g.NT + t) * 32 + l] = v;
+        }
+  std::vector<double> ana((size_t)2 * asteps * 32, 0.0);
+  for (int var = 0; var < 2; ++var)
+    for (int gr = 0; gr < 6; ++gr)
+      for (int u = 0; u < tf_NU(g.m, gr); ++u)
+        for (int te = 0; te < tf_TE(g.m, gr); ++te)
+          for (int l = 0; l < 32; ++l) {
+            const int j = 8 * (te >> 1) + 2 * (l & 3) + (te & 1);
+            const int kk = 8 * u + (l >> 2);
+            double v = 0.0;
+            if (kk < tf_ke(g.m, gr)) {
+              const int n = tf_mode(gr, kk);
+              const long double x = (long double)n * ang(j);
+              const long double w = var == 1 ? 1.0L : (n == 0 ? 1.0L : 2.0L) / (long double)g.N;
+              v = (double)(w * (gr < 3 ? cosl(x) : sinl(x)));
+            }
+            ana[(((size_t)var * asteps + tf_aoff(g.m, gr) + u * tf_TE(g.m, gr) + te) * 32) + l] = v;
+          }
+  Tables T;
+  if (cudaMalloc(&T.syn, syn.size() * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&T.ana, ana.size() * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(SFNL_ERR_ALLOC, "cudaMalloc of the DFT tables failed");
+  }
+  if (cudaMemcpy(T.syn, syn.data(), syn.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(T.ana, ana.data(), ana.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    return set_error(SFNL_ERR_CUDA, "upload of the DFT tables failed");
+  g_tftabs[{dev, g.m}] = T;
+  *out = T;
+  return SFNL_OK;
+}
+
+// ---------------------------------------------------------------------------
 // kernel
 // ---------------------------------------------------------------------------
 struct FastArgs {
@@ -172,6 +271,7 @@ struct FastArgs {
   int adj_out;      // 1: analyse without D (transpose of the synthesis)
   int accumulate;   // 1: out += result
   int vec16;        // 1: every input row starts 16-byte aligned (bases aligned, np even): 16-byte copies
+  int allow_tf;     // 1: the third-fold kernel may be used (it allocates its own cached tables)
   const double *syn, *ana;
 };
 
@@ -345,32 +445,32 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M
     for (int t0 = 0; t0 < NT; t0 += NWT) {  // one pass when ps and xc overlay the coefficients
       const int t = t0 + wp;
       double acc[NI][2][2];
-  #pragma unroll
+#pragma unroll
       for (int f = 0; f < NI; ++f)
-  #pragma unroll
+#pragma unroll
         for (int cc = 0; cc < 2; ++cc) acc[f][cc][0] = acc[f][cc][1] = 0.0;
       auto synth = [&](auto cb_tag) {
         constexpr int CB = decltype(cb_tag)::value;  // first class of this warp's pair
         const double *syn_t = a.syn + (size_t)t * 32 + lane;
         const double *xs_l = xs + (lane & 3) * 8 + (lane >> 2);
-  #pragma unroll
+#pragma unroll
         for (int s = 0; s < ks_max; ++s) {
-  #pragma unroll
+#pragma unroll
           for (int cc = 0; cc < 2; ++cc) {
             const int c = CB + cc;
             if (s >= KS[c]) continue;
             const double bv = __ldg(syn_t + (size_t)(KOFF[c] + s) * NT * 32);
             const double *xa = xs_l + (size_t)(KOFF[c] + s) * 32;
             double av[NI];
-  #pragma unroll
+#pragma unroll
             for (int f = 0; f < NI; ++f) av[f] = xa[(size_t)f * KS_tot * 32];
             if constexpr (ADJ != 0) {
               const double wn = (s == 0 && q == 0 && (c & 1) == 0) ? invN : twoN;  // n == 0 only there
-  #pragma unroll
+#pragma unroll
               for (int f = 0; f < NI; ++f)
                 if ((ADJ == 1 && f < 3) || (ADJ == 2 && f >= 3)) av[f] *= wn;
             }
-  #pragma unroll
+#pragma unroll
             for (int f = 0; f < NI; ++f) dmma(acc[f][cc], av[f], bv);
           }
         }
@@ -390,7 +490,7 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M
       };
       double *xw = xc + (size_t)wp * 2 * NI * 64 + lane;  // [writer half][f][X, Y][32]
       if (t < NT) {
-  #pragma unroll
+#pragma unroll
         for (int f = 0; f < NI; ++f) {
           double X, Y;
           pair_sums(f, 1 - half, X, Y);  // the parity the partner finishes
@@ -402,7 +502,7 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M
       if (t < NT) {
         const int e = half;
         double v[4][NI];
-  #pragma unroll
+#pragma unroll
         for (int f = 0; f < NI; ++f) {
           double X, Y;
           pair_sums(f, e, X, Y);
@@ -414,9 +514,9 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M
           v[3][f] = A - C;  // 2 pi - theta
         }
         double gq[4][NO];
-  #pragma unroll
+#pragma unroll
         for (int r = 0; r < 4; ++r) EKDef<EK>::op(v[r], gq[r]);
-  #pragma unroll
+#pragma unroll
         for (int o = 0; o < NO; ++o) {
           const double s14 = gq[0][o] + gq[3][o], d14 = gq[0][o] - gq[3][o];
           const double s23 = gq[1][o] + gq[2][o], d32 = gq[2][o] - gq[1][o];
@@ -437,41 +537,41 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M
     for (int t0 = 0; t0 < NT; t0 += NW) {  // one pass when the products overlay the coefficients
       const int t = t0 + warp;
       double acc[NI][4][2];
-  #pragma unroll
+#pragma unroll
       for (int f = 0; f < NI; ++f)
-  #pragma unroll
+#pragma unroll
         for (int c = 0; c < 4; ++c) acc[f][c][0] = acc[f][c][1] = 0.0;
       if (t < NT) {
       // k-steps outermost, the four classes inside: 4*NI independent accumulator chains per step
       const double *syn_t = a.syn + (size_t)t * 32 + lane;
       const double *xs_l = xs + (lane & 3) * 8 + (lane >> 2);
-  #pragma unroll
+#pragma unroll
       for (int s = 0; s < ks_max; ++s) {
-  #pragma unroll
+#pragma unroll
         for (int c = 0; c < 4; ++c) {
           if (s >= KS[c]) continue;
           const double bv = __ldg(syn_t + (size_t)(KOFF[c] + s) * NT * 32);
           const double *xa = xs_l + (size_t)(KOFF[c] + s) * 32;
           double av[NI];
-  #pragma unroll
+#pragma unroll
           for (int f = 0; f < NI; ++f) av[f] = xa[(size_t)f * KS_tot * 32];
           if constexpr (ADJ != 0) {
             const double wn = (s == 0 && q == 0 && (c & 1) == 0) ? invN : twoN;  // n == 0 only there
-  #pragma unroll
+#pragma unroll
             for (int f = 0; f < NI; ++f)
               if ((ADJ == 1 && f < 3) || (ADJ == 2 && f >= 3)) av[f] *= wn;
           }
-  #pragma unroll
+#pragma unroll
           for (int f = 0; f < NI; ++f) dmma(acc[f][c], av[f], bv);
         }
       }
       }
       if (overlay) __syncthreads();  // every warp has read its last coefficient
       if (t >= NT) continue;
-  #pragma unroll
+#pragma unroll
       for (int e = 0; e < 2; ++e) {
         double v[4][NI];
-  #pragma unroll
+#pragma unroll
         for (int f = 0; f < NI; ++f) {
           const double A = acc[f][0][e] + acc[f][1][e], B = acc[f][0][e] - acc[f][1][e];
           const double C = acc[f][2][e] + acc[f][3][e], D = acc[f][3][e] - acc[f][2][e];
@@ -481,9 +581,9 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M
           v[3][f] = A - C;  // 2 pi - theta
         }
         double gq[4][NO];
-  #pragma unroll
+#pragma unroll
         for (int r = 0; r < 4; ++r) EKDef<EK>::op(v[r], gq[r]);
-  #pragma unroll
+#pragma unroll
         for (int o = 0; o < NO; ++o) {
           const double s14 = gq[0][o] + gq[3][o], d14 = gq[0][o] - gq[3][o];
           const double s23 = gq[1][o] + gq[2][o], d32 = gq[2][o] - gq[1][o];
@@ -548,6 +648,255 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M
   }
 }
 
+// The FAST kernel with the third fold (class split, NT even, one pass: M = 64).  Per 8-point tile,
+// warp pair tau (= angle tile) half h: the odd class of half h on tile tau, and one part of the even
+// class of half h on tile min(tau, NT-1-tau) -- E0 for the first half of the tiles, E2 for the second.
+// A first exchange (X1) assembles the even class on every tile from the two parts; from there on the
+// tile is processed as in the class split (second exchange, program, analysis pre-fold).  The analysis
+// contracts the even output groups over the first half of the tiles with P(t) +- P(mirror).
+template <int EK, int M, int ADJ>
+__global__ void __launch_bounds__(384, EK == EK_CROSS ? 3 : 0) fast_tf_kernel(const FastArgs a) {
+  static_assert(third_fold(M), "third fold needs the specialised geometry");
+  constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO;
+  constexpr int NT = tf_NT(M), NH = NT / 2;
+  constexpr int KS_tot = tf_koff(M, 6), KT = 4 * KS_tot, NU_tot = tf_nuoff(M, 6), ASTEPS = tf_aoff(M, 6);
+  extern __shared__ double smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int64_t p0 = (int64_t)blockIdx.x * 8, p = p0 + g;
+  const bool valid = p < a.np;
+  const int b = blockIdx.y;
+  const double invN = 1.0 / (4.0 * 8.0 * NT), twoN = 2.0 * invN;
+  constexpr size_t prod_d = (size_t)NO * 4 * NT * 2 * 32;
+  double *ps = smem, *xc = smem + prod_d, *xs = smem;  // ps and xc overlay xs after the synthesis
+
+  // ---- stage the tile's coefficients (rows in group order, otherwise as in fast_kernel) ----
+  {
+    const int pc = 2 * (threadIdx.x & 3), rstep = blockDim.x >> 2;
+    const bool v16 = a.vec16 && p0 + 8 <= a.np;
+    const bool pv0 = p0 + pc < a.np, pv1 = p0 + pc + 1 < a.np;
+#pragma unroll
+    for (int f = 0; f < NI; ++f) {
+      const double *base = a.in[f] + (int64_t)b * a.in_bs[f] + p0 + pc;
+      const int64_t ldm = a.in_ldm[f];
+      double *xf = xs + (size_t)f * KS_tot * 32 + pc;
+      for (int r = threadIdx.x >> 2; r < KT; r += rstep) {
+        const int gr = (r >= 4 * tf_koff(M, 1)) + (r >= 4 * tf_koff(M, 2)) + (r >= 4 * tf_koff(M, 3)) +
+                       (r >= 4 * tf_koff(M, 4)) + (r >= 4 * tf_koff(M, 5));
+        const int kg = gr == 0 ? 0 : gr == 1 ? tf_koff(M, 1) : gr == 2 ? tf_koff(M, 2) : gr == 3 ? tf_koff(M, 3)
+                     : gr == 4 ? tf_koff(M, 4) : tf_koff(M, 5);
+        const int keg = gr % 3 == 0 ? tf_ke(M, 0) : gr % 3 == 1 ? tf_ke(M, 1) : tf_ke(M, 2);
+        const int k = r - 4 * kg, n = tf_mode(gr, k);
+        double *dst = xf + (size_t)(r >> 2) * 32 + (r & 3) * 8;
+        const bool live = k < keg && !(gr == 3 && k == 0);  // the sine of mode 0 is ignored
+        const double *src = base + (int64_t)n * ldm + (gr >= 3 ? a.np : 0);
+        if (live && v16) {
+          cp_async16(dst, src);
+        } else {
+          if (live && pv0) cp_async8(dst, src); else dst[0] = 0.0;
+          if (live && pv1) cp_async8(dst + 1, src + 1); else dst[1] = 0.0;
+        }
+      }
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+
+  // ---- synthesis: even part on the pair's first tile, odd class on the own tile ----
+  const int tau = warp >> 1, half = warp & 1;
+  const bool first = tau < NH;
+  const int te_tile = first ? tau : NT - 1 - tau;
+  double acc_e[NI][2], acc_o[NI][2];
+#pragma unroll
+  for (int f = 0; f < NI; ++f) acc_e[f][0] = acc_e[f][1] = acc_o[f][0] = acc_o[f][1] = 0.0;
+  {
+    const int ge = 3 * half + (first ? 0 : 1);
+    const int koff_e = ge == 0 ? tf_koff(M, 0) : ge == 1 ? tf_koff(M, 1) : ge == 3 ? tf_koff(M, 3) : tf_koff(M, 4);
+    const int ks_e = (ge % 3 == 0) ? tf_KS(M, 0) : tf_KS(M, 1);
+    const int koff_o = half ? tf_koff(M, 5) : tf_koff(M, 2);
+    const double *xs_l = xs + (lane & 3) * 8 + (lane >> 2);
+    const double *syn_e = a.syn + (size_t)te_tile * 32 + lane, *syn_o = a.syn + (size_t)tau * 32 + lane;
+    constexpr int KSE = tf_KS(M, 0) > tf_KS(M, 1) ? tf_KS(M, 0) : tf_KS(M, 1);
+#pragma unroll
+    for (int s = 0; s < KSE; ++s) {
+      if (s >= ks_e) break;
+      const double bv = __ldg(syn_e + (size_t)(koff_e + s) * NT * 32);
+      const double *xa = xs_l + (size_t)(koff_e + s) * 32;
+      double av[NI];
+#pragma unroll
+      for (int f = 0; f < NI; ++f) av[f] = xa[(size_t)f * KS_tot * 32];
+      if constexpr (ADJ != 0) {
+        const double wn = (s == 0 && q == 0 && ge % 3 == 0) ? invN : twoN;  // n == 0 only there
+#pragma unroll
+        for (int f = 0; f < NI; ++f)
+          if ((ADJ == 1 && f < 3) || (ADJ == 2 && f >= 3)) av[f] *= wn;
+      }
+#pragma unroll
+      for (int f = 0; f < NI; ++f) dmma(acc_e[f], av[f], bv);
+    }
+#pragma unroll
+    for (int s = 0; s < tf_KS(M, 2); ++s) {
+      const double bv = __ldg(syn_o + (size_t)(koff_o + s) * NT * 32);
+      const double *xa = xs_l + (size_t)(koff_o + s) * 32;
+      double av[NI];
+#pragma unroll
+      for (int f = 0; f < NI; ++f) av[f] = xa[(size_t)f * KS_tot * 32];
+      if constexpr (ADJ != 0) {
+#pragma unroll
+        for (int f = 0; f < NI; ++f)
+          if ((ADJ == 1 && f < 3) || (ADJ == 2 && f >= 3)) av[f] *= twoN;
+      }
+#pragma unroll
+      for (int f = 0; f < NI; ++f) dmma(acc_o[f], av[f], bv);
+    }
+  }
+  __syncthreads();  // every warp has read its last coefficient: xc and ps may overwrite xs
+
+  // ---- first exchange: the even class on the own tile from the two parts ----
+  // X1[tau][half][f][e][32] holds the part each warp computed (on tile te_tile).  A first-half tile
+  // adds its partner's part at the same lane; a second-half tile takes both parts at the mirror lane
+  // (lane ^ 3) and parity (1 - e): CE = E0 - E2, SE = S2 - S0.
+  double acc[NI][2][2];  // [f][even, odd class][e], as in the class split
+  {
+    double *x1 = xc + (size_t)((tau * 2 + half) * NI) * 64 + lane;
+#pragma unroll
+    for (int f = 0; f < NI; ++f) {
+      x1[(f * 2 + 0) * 32] = acc_e[f][0];
+      x1[(f * 2 + 1) * 32] = acc_e[f][1];
+    }
+    __syncthreads();
+    const double *own = xc + (size_t)((tau * 2 + half) * NI) * 64;
+    const double *mate = xc + (size_t)(((NT - 1 - tau) * 2 + half) * NI) * 64;
+#pragma unroll
+    for (int f = 0; f < NI; ++f)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        double ev;
+        if (first) {
+          ev = acc_e[f][e] + mate[(f * 2 + e) * 32 + lane];
+        } else {
+          const double p0m = mate[(f * 2 + 1 - e) * 32 + (lane ^ 3)];  // E0 / S0 at the mirror angle
+          const double p2m = own[(f * 2 + 1 - e) * 32 + (lane ^ 3)];   // E2 / S2 at the mirror angle
+          ev = half ? p2m - p0m : p0m - p2m;
+        }
+        acc[f][0][e] = ev;
+        acc[f][1][e] = acc_o[f][e];
+      }
+    __syncthreads();  // X1 is read: the second exchange reuses xc
+  }
+
+  // ---- second exchange, program, analysis pre-fold (as in the class split) ----
+  {
+    const int t = tau;
+    auto pair_sums = [&](int f, int e, double &X, double &Y) {
+      const double lo = e ? acc[f][0][1] : acc[f][0][0], hi = e ? acc[f][1][1] : acc[f][1][0];
+      X = lo + hi;
+      Y = half ? hi - lo : lo - hi;
+    };
+    double *xw = xc + (size_t)tau * 2 * NI * 64 + lane;  // [writer half][f][X, Y][32]
+#pragma unroll
+    for (int f = 0; f < NI; ++f) {
+      double X, Y;
+      pair_sums(f, 1 - half, X, Y);
+      xw[((half * NI + f) * 2 + 0) * 32] = X;
+      xw[((half * NI + f) * 2 + 1) * 32] = Y;
+    }
+    __syncthreads();
+    const int e = half;
+    double v[4][NI];
+#pragma unroll
+    for (int f = 0; f < NI; ++f) {
+      double X, Y;
+      pair_sums(f, e, X, Y);
+      const double Xp = xw[(((1 - half) * NI + f) * 2 + 0) * 32], Yp = xw[(((1 - half) * NI + f) * 2 + 1) * 32];
+      const double A = half ? Xp : X, B = half ? Yp : Y, C = half ? X : Xp, D = half ? Y : Yp;
+      v[0][f] = A + C;  // theta
+      v[1][f] = B + D;  // pi - theta
+      v[2][f] = B - D;  // pi + theta
+      v[3][f] = A - C;  // 2 pi - theta
+    }
+    double gq[4][NO];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) EKDef<EK>::op(v[r], gq[r]);
+#pragma unroll
+    for (int o = 0; o < NO; ++o) {
+      const double s14 = gq[0][o] + gq[3][o], d14 = gq[0][o] - gq[3][o];
+      const double s23 = gq[1][o] + gq[2][o], d32 = gq[2][o] - gq[1][o];
+      double *dst = ps + ((size_t)((o * 4) * NT + t) * 2 + e) * 32 + lane;
+      const size_t cstride = (size_t)NT * 2 * 32;
+      dst[0] = s14 + s23;            // PE
+      dst[cstride] = s14 - s23;      // PO
+      dst[2 * cstride] = d14 + d32;  // QE
+      dst[3 * cstride] = d14 - d32;  // QO
+    }
+  }
+  __syncthreads();
+
+  // ---- analysis: output groups; the even ones over the first half of the tiles ----
+  const double *anav = a.ana + (size_t)(a.adj_out ? 1 : 0) * ASTEPS * 32 + lane;
+  const int NW = blockDim.x >> 5;
+  for (int cu = warp; cu < NU_tot; cu += NW) {
+    const int gr = (cu >= tf_nuoff(M, 1)) + (cu >= tf_nuoff(M, 2)) + (cu >= tf_nuoff(M, 3)) +
+                   (cu >= tf_nuoff(M, 4)) + (cu >= tf_nuoff(M, 5));
+    const int nuo = gr == 0 ? 0 : gr == 1 ? tf_nuoff(M, 1) : gr == 2 ? tf_nuoff(M, 2) : gr == 3 ? tf_nuoff(M, 3)
+                  : gr == 4 ? tf_nuoff(M, 4) : tf_nuoff(M, 5);
+    const int aof = gr == 0 ? 0 : gr == 1 ? tf_aoff(M, 1) : gr == 2 ? tf_aoff(M, 2) : gr == 3 ? tf_aoff(M, 3)
+                  : gr == 4 ? tf_aoff(M, 4) : tf_aoff(M, 5);
+    const bool odd = gr % 3 == 2;
+    const int u = cu - nuo, TE = odd ? 2 * NT : NT, c = gr < 3 ? (odd ? 1 : 0) : (odd ? 3 : 2);
+    const int keg = gr % 3 == 0 ? tf_ke(M, 0) : gr % 3 == 1 ? tf_ke(M, 1) : tf_ke(M, 2);
+    // mirror sign of the even groups: PE0 +, PE2 -, QE0 -, QE2 +
+    const double sg = (gr == 0 || gr == 4) ? 1.0 : -1.0;
+    constexpr int PC = NO >= 6 ? 1 : NO >= 3 ? 2 : 4;
+    double yp[PC][NO][2];
+#pragma unroll
+    for (int i = 0; i < PC; ++i)
+#pragma unroll
+      for (int o = 0; o < NO; ++o) yp[i][o][0] = yp[i][o][1] = 0.0;
+    const double *bt = anav + (size_t)(aof + u * TE) * 32;
+    const double *pa = ps + (size_t)c * NT * 2 * 32;
+#pragma unroll
+    for (int te = 0; te < 2 * NT; ++te) {
+      if (te >= TE) break;
+      const double bv = __ldg(bt + (size_t)te * 32);
+      const int t = te >> 1, e = te & 1;
+#pragma unroll
+      for (int o = 0; o < NO; ++o) {
+        const double *po = pa + (size_t)o * 4 * NT * 2 * 32;
+        double av = po[(t * 2 + e) * 32 + lane];
+        if (!odd) av += sg * po[((NT - 1 - t) * 2 + 1 - e) * 32 + (lane ^ 3)];
+        dmma(yp[te % PC][o], av, bv);
+      }
+    }
+    double y[NO][2];
+#pragma unroll
+    for (int o = 0; o < NO; ++o)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        y[o][h] = yp[0][o][h];
+#pragma unroll
+        for (int i = 1; i < PC; ++i) y[o][h] += yp[i][o][h];
+      }
+    if (!valid) continue;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int kk = 8 * u + 2 * q + h;
+      if (kk >= keg) continue;
+      const int n = tf_mode(gr, kk);
+#pragma unroll
+      for (int o = 0; o < NO; ++o) {
+        double *dst = a.out[o] + (int64_t)b * a.out_bs[o] + p * a.out_ps + (int64_t)n * a.out_ldm[o] +
+                      (gr >= 3 ? a.np * a.out_ps : 0);
+        const double v = (gr >= 3 && n == 0) ? 0.0 : y[o][h];
+        if (a.accumulate)
+          *dst += v;
+        else
+          *dst = v;
+      }
+    }
+  }
+}
+
 template <int EK, int M, int ADJ>
 int launch_ek_m(FastArgs &fa, int batch, cudaStream_t st) {
   constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO;
@@ -559,6 +908,15 @@ int launch_ek_m(FastArgs &fa, int batch, cudaStream_t st) {
   const int tiles_per_pass = fa.NT < 8 ? fa.NT : 8;
   const int nw = CS ? 2 * tiles_per_pass : (tiles_per_pass < 2 ? 2 : tiles_per_pass);
   auto kern = fast_kernel<EK, M, ADJ, CS>;
+  if constexpr (CS && third_fold(M)) {
+    if (fa.allow_tf) {  // the third-fold kernel (same shared memory and warps, its own tables)
+      Tables T;
+      if (int rc = get_tf_tables(make_geo(fa.m), &T)) return rc;
+      fa.syn = T.syn;
+      fa.ana = T.ana;
+      kern = fast_tf_kernel<EK, M, ADJ>;
+    }
+  }
   if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (fast form)");
   const int64_t tiles = (fa.np + 7) / 8;
@@ -705,6 +1063,7 @@ int launch_fast(const ProgArgs &a, cudaStream_t st) {
     fa.adj_out = adj_out ? 1 : 0;
     fa.accumulate = e.acc;
     fa.vec16 = rows_aligned16(fa, ni);
+    fa.allow_tf = 1;
     fa.syn = T.syn;
     fa.ana = T.ana;
     int r = e.ek == EK_CROSS  ? launch_ek<EK_CROSS>(fa, a.batch, st)
@@ -791,6 +1150,15 @@ void fast_release_tables() {
     cudaFree(kv.second.ana);
   }
   g_tabs.clear();
+  {
+    std::lock_guard<std::mutex> lk2(g_tftab_mu);
+    for (auto &kv : g_tftabs) {
+      cudaSetDevice(kv.first.first);
+      cudaFree(kv.second.syn);
+      cudaFree(kv.second.ana);
+    }
+    g_tftabs.clear();
+  }
   cudaSetDevice(prev);
 }
 

@@ -140,7 +140,7 @@ def _batched(npts, nslot, m, k, alpha, seed):
     return x
 
 
-@pytest.mark.parametrize("npts,m,k", [(120, 8, 3), (33, 17, 1)])
+@pytest.mark.parametrize("npts,m,k", [(120, 8, 3), (33, 17, 1), (41, 64, 2)])
 def test_cross_jvp_matches_linearisation(npts, m, k):
     pad = 3 * m // 2
     u = R.synthetic_field(npts, 6, m, 0.2, 1)
@@ -170,7 +170,7 @@ def test_cross_jvp_central_finite_differences():
     assert R.rel_l2(jv, fd) < 1e-8
 
 
-@pytest.mark.parametrize("npts,m,k", [(150, 8, 2), (40, 32, 1)])
+@pytest.mark.parametrize("npts,m,k", [(150, 8, 2), (40, 32, 1), (37, 64, 2)])
 def test_cross_vjp_dot_product_identity(npts, m, k):
     pad = 3 * m // 2
     u = R.synthetic_field(npts, 6, m, 0.2, 31)
@@ -186,9 +186,9 @@ def test_cross_vjp_dot_product_identity(npts, m, k):
         assert R.rel_l2(jtc[..., t], R.cross_vjp(u, w, np.asfortranarray(c[..., t]))) <= FP64_TOL
 
 
-def test_mhd_jvp_vjp():
-    npts, m, k = 90, 12, 2
-    pad = 18
+@pytest.mark.parametrize("npts,m,k", [(90, 12, 2), (43, 64, 2)])
+def test_mhd_jvp_vjp(npts, m, k):
+    pad = 3 * m // 2
     u, w, b = (R.synthetic_field(npts, 6, m, 0.2, 60 + i) for i in range(3))
     v = _batched(npts, 18, m, k, 0.2, 70)
     c = _batched(npts, 12, m, k, 0.2, 80)
