@@ -6,7 +6,9 @@ this module: it is the checker for the CUDA path, never part of it.
 Three independent CPU formulations of the dealiased products of
 SOURCES/POST_PROCESSING/fft_parallel.F90 (FFT_PAR_CROSS_PROD_DCL :147-328,
 FFT_PAR_DOT_PROD_DCL :330-500, FFT_PAR_PROD_DCL :502-665, FFT_PAR_DIV_DCL
-:667-830, FFT_SCALAR_VECT_DCL :1021-1220, FFT_TENSOR_DCL :1543-1796):
+:667-830, FFT_SCALAR_VECT_DCL :1021-1220, FFT_TENSOR_DCL :1543-1796), and
+of the synthesis-only FFT_PAR_REAL (:28-145) and FFT_MAX_VEL_DCL
+(:1426-1541) (``c_real``, ``c_max_vel``, ``synth_grid``):
 
 * ``c_oracle``   -- ctypes binding of oracle/sfnl_oracle.c, the step-by-step
   long-double restatement of the reference (pack, emulated MPI_ALLTOALL,
@@ -111,6 +113,12 @@ def _lib():
         f = lib.orc_apply_n
         f.restype = ctypes.c_int
         f.argtypes = [ctypes.c_int, P, ctypes.c_int, P, ctypes.c_int, P] + [ctypes.c_int] * 6
+        lib.orc_fft_par_real_planes.restype = ctypes.c_int
+        lib.orc_fft_par_real_planes.argtypes = [ctypes.c_int, ctypes.c_int]
+        lib.orc_fft_par_real.restype = ctypes.c_int
+        lib.orc_fft_par_real.argtypes = [P] + [ctypes.c_int] * 5 + [P]
+        lib.orc_fft_max_vel.restype = ctypes.c_int
+        lib.orc_fft_max_vel.argtypes = [P] + [ctypes.c_int] * 6 + [P]
         _LIB = lib
     return _LIB
 
@@ -146,6 +154,50 @@ def c_oracle(op: str, V1, V2, m_max_pad: int, nb_procs: int = 1, bloc_size: int 
     if rc != 0:
         raise ValueError(f"oracle rejected arguments (status {rc})")
     return out
+
+
+def real_planes(m_max: int, opt_nb_plane: int | None = None) -> int:
+    """Grid length of FFT_PAR_REAL: 2*m_max_pad-1, m_max_pad = (opt_nb_plane+1)/2 when opt_nb_plane > 2m-1."""
+    return _lib().orc_fft_par_real_planes(m_max, opt_nb_plane or 0)
+
+
+def c_real(V, nb_procs: int = 1, opt_nb_plane: int | None = None):
+    """Long-double restatement of FFT_PAR_REAL: (N, nslot/2, np) Fortran array of the values of every
+    field at the angles 2*pi*j/N (the ranks' V_out one after the other)."""
+    V = np.asfortranarray(V, dtype=np.float64)
+    npts, nsl, m = V.shape
+    if m % nb_procs:
+        raise ValueError("m_max must be a multiple of nb_procs")
+    N = real_planes(m, opt_nb_plane)
+    out = np.zeros((N, nsl // 2, npts), order="F")
+    rc = _lib().orc_fft_par_real(_ptr(V), nsl, npts, m // nb_procs, nb_procs, opt_nb_plane or 0, _ptr(out))
+    if rc != 0:
+        raise ValueError(f"oracle rejected arguments (status {rc})")
+    return out
+
+
+def c_max_vel(V, m_max_pad: int, nb_procs: int = 1, bloc_size: int | None = None) -> float:
+    """Long-double restatement of FFT_MAX_VEL_DCL: max over points and the 2*m_max_pad-1 angles of |v|."""
+    V = np.asfortranarray(V, dtype=np.float64)
+    npts, nsl, m = V.shape
+    if bloc_size is None:
+        bloc_size = npts // nb_procs + 1
+    res = np.zeros(1)
+    rc = _lib().orc_fft_max_vel(_ptr(V), nsl, npts, m // nb_procs, nb_procs, bloc_size, m_max_pad, _ptr(res))
+    if rc != 0:
+        raise ValueError(f"oracle rejected arguments (status {rc})")
+    return float(res[0])
+
+
+def synth_grid(V, N: int, workers: int = 1):
+    """pocketfft synthesis of every field on N angles 2*pi*j/N: (N, nslot/2, np) Fortran array."""
+    import scipy.fft as sfft
+
+    npts, nsl, m = V.shape
+    cu = np.zeros((npts, nsl // 2, N // 2 + 1), dtype=np.complex128)
+    cu[:, :, :m] = _to_complex(V, nsl // 2)
+    ru = sfft.irfft(cu, n=N, axis=2, norm="forward", workers=workers)  # (np, nf, N)
+    return np.asfortranarray(np.transpose(ru, (2, 1, 0)))
 
 
 # ----------------------------------------------------------------------------

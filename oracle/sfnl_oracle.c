@@ -15,6 +15,8 @@
  *   FFT_PAR_DIV_DCL         fft_parallel.F90:667-830
  *   FFT_SCALAR_VECT_DCL     fft_parallel.F90:1021-1220  (pb = 1 product, pb = 2 quotient)
  *   FFT_TENSOR_DCL          fft_parallel.F90:1543-1796  (with and without opt_tension)
+ *   FFT_PAR_REAL            fft_parallel.F90:28-145     (synthesis only)
+ *   FFT_MAX_VEL_DCL         fft_parallel.F90:1426-1541  (synthesis, |v|, maximum)
  *
  * including the nb_procs / bloc_size bookkeeping: each emulated rank owns
  * m_max_c contiguous Fourier modes, packs a mode-major dist_field with dummy
@@ -291,5 +293,105 @@ done:
   free(dist); free(comb); free(cpr); free(cpi); free(dpr); free(dpi);
   free(cur); free(cui); free(ru); free(pru); free(pcr); free(pci);
   free(ct); free(st);
+  return rc;
+}
+
+/* Shared by the two synthesis-only routines: every emulated rank packs dist_field(m_max_c, nsl,
+ * np_tot) (dummy points set to `dummy`), the MPI_ALLTOALL is emulated, and rank q synthesises its
+ * bloc_size points: ru_q(N, nsl/2, bloc_size) = c2r of the half-complex pack of every field
+ * (fft_parallel.F90:88-131, :1474-1519).  `visit(ctx, q, n, ru)` receives ru (N, nsl/2) of point n of
+ * rank q. */
+typedef void (*synth_visit)(void *ctx, int q, int n, const ld *ru, int N, int nfc);
+
+static int synth_ranks(const double *V1, int nsl, int np, int m_max_c, int nb_procs, int bloc_size, int m_max_pad,
+                       double dummy, synth_visit visit, void *ctx) {
+  const int np_tot = nb_procs * bloc_size, N = 2 * m_max_pad - 1, nfc = nsl / 2;
+  const int m_max = m_max_c * nb_procs;
+  if (m_max_pad < m_max) return -3;
+  if (np > np_tot) return -2; /* dist_field(:,:,np_tot) would overflow */
+  ld *ct = NULL, *st = NULL;
+  if (make_tables(N, &ct, &st)) return -4;
+  const size_t dsz = (size_t)m_max_c * nsl * np_tot, blk = (size_t)m_max_c * nsl * bloc_size;
+  double *dist = (double *)malloc(sizeof(double) * (dsz ? dsz : 1) * (size_t)nb_procs);
+  double *comb = (double *)malloc(sizeof(double) * (dsz ? dsz : 1) * (size_t)nb_procs);
+  ld *cur = (ld *)malloc(sizeof(ld) * (size_t)m_max_pad * nfc), *cui = (ld *)malloc(sizeof(ld) * (size_t)m_max_pad * nfc);
+  ld *ru = (ld *)malloc(sizeof(ld) * (size_t)N * nfc);
+  int rc = (!dist || !comb || !cur || !cui || !ru) ? -4 : 0;
+  if (!rc) {
+    for (int r = 0; r < nb_procs; ++r) { /* TRANSPOSE pack, dummy points */
+      double *d = dist + (size_t)r * dsz;
+      for (size_t t = 0; t < dsz; ++t) d[t] = dummy;
+      for (int i = 0; i < m_max_c; ++i)
+        for (int p = 0; p < np; ++p)
+          for (int s2 = 0; s2 < nsl; ++s2) d[IDX3(i, s2, p, m_max_c, nsl)] = V1[IDX3(p, s2, r * m_max_c + i, np, nsl)];
+    }
+    for (int r = 0; r < nb_procs; ++r) /* MPI_ALLTOALL */
+      for (int q = 0; q < nb_procs; ++q)
+        memcpy(comb + (size_t)q * dsz + (size_t)r * blk, dist + (size_t)r * dsz + (size_t)q * blk, sizeof(double) * blk);
+    for (int q = 0; q < nb_procs; ++q)
+      for (int n = 0; n < bloc_size; ++n) {
+        for (size_t t = 0; t < (size_t)m_max_pad * nfc; ++t) cur[t] = cui[t] = 0.0L;
+        for (int nb = 0; nb < nb_procs; ++nb) {
+          const int shiftc = nb * bloc_size, shiftl = nb * m_max_c, jindex = n + shiftc;
+          for (int nf = 0; nf < nfc; ++nf)
+            for (int i = 0; i < m_max_c; ++i) {
+              cur[(shiftl + i) + m_max_pad * nf] = 0.5L * (ld)comb[(size_t)q * dsz + IDX3(i, 2 * nf, jindex, m_max_c, nsl)];
+              cui[(shiftl + i) + m_max_pad * nf] = -0.5L * (ld)comb[(size_t)q * dsz + IDX3(i, 2 * nf + 1, jindex, m_max_c, nsl)];
+            }
+        }
+        for (int nf = 0; nf < nfc; ++nf) {
+          cur[m_max_pad * nf] *= 2.0L;
+          cui[m_max_pad * nf] = 0.0L;
+        }
+        for (int nf = 0; nf < nfc; ++nf)
+          c2r_ld(N, m_max_pad, cur + (size_t)m_max_pad * nf, cui + (size_t)m_max_pad * nf, ru + (size_t)N * nf, ct, st);
+        visit(ctx, q, n, ru, N, nfc);
+      }
+  }
+  free(dist); free(comb); free(cur); free(cui); free(ru); free(ct); free(st);
+  return rc;
+}
+
+int orc_fft_par_real_planes(int m_max, int opt_nb_plane) {
+  /* m_max_pad = (opt_nb_plane+1)/2 if opt_nb_plane > 2*m_max-1, else m_max (fft_parallel.F90:71-79) */
+  const int m_max_pad = (opt_nb_plane > 2 * m_max - 1) ? (opt_nb_plane + 1) / 2 : m_max;
+  return 2 * m_max_pad - 1;
+}
+
+struct real_ctx { double *Vout; int bloc_size, N; };
+static void real_visit(void *c, int q, int n, const ld *ru, int N, int nfc) {
+  struct real_ctx *x = (struct real_ctx *)c;
+  const int p = q * x->bloc_size + n; /* rank q holds points q*bloc_size .. */
+  for (int f = 0; f < nfc; ++f)
+    for (int j = 0; j < N; ++j) x->Vout[IDX3(j, f, p, N, nfc)] = (double)ru[(size_t)N * f + j];
+}
+
+int orc_fft_par_real(const double *V1, int nsl, int np, int m_max_c, int nb_procs, int opt_nb_plane, double *Vout) {
+  if ((nsl % 2) != 0 || m_max_c <= 0 || nb_procs < 1 || np < 0) return -1; /* :59-61 */
+  if (np % nb_procs) return -2;                                              /* :65-71 */
+  const int m_max = m_max_c * nb_procs, N = orc_fft_par_real_planes(m_max, opt_nb_plane);
+  struct real_ctx c = {Vout, np / nb_procs, N};
+  return synth_ranks(V1, nsl, np, m_max_c, nb_procs, np / nb_procs, (N + 1) / 2, 0.0, real_visit, &c);
+}
+
+struct maxv_ctx { ld vmax; int nsl; };
+static void maxv_visit(void *c, int q, int n, const ld *ru, int N, int nfc) {
+  struct maxv_ctx *x = (struct maxv_ctx *)c;
+  (void)q; (void)n; (void)nfc;
+  for (int j = 0; j < N; ++j) {
+    /* |v| of the first vector for nb_field == 6, |first field| otherwise (:1528-1532) */
+    const ld v = (x->nsl == 6) ? sqrtl(ru[j] * ru[j] + ru[N + j] * ru[N + j] + ru[2 * N + j] * ru[2 * N + j])
+                               : sqrtl(ru[j] * ru[j]);
+    if (v > x->vmax) x->vmax = v;
+  }
+}
+
+int orc_fft_max_vel(const double *V1, int nsl, int np, int m_max_c, int nb_procs, int bloc_size, int m_max_pad,
+                    double *vmax) {
+  if ((nsl % 2) != 0 || m_max_c <= 0 || nb_procs < 1 || bloc_size < 1 || np < 0) return -1; /* :1457-1460 */
+  struct maxv_ctx c = {0.0L, nsl};
+  /* dummy points are 0 (:1478): their |v| = 0 never exceeds the maximum of the others */
+  const int rc = synth_ranks(V1, nsl, np, m_max_c, nb_procs, bloc_size, m_max_pad, 0.0, maxv_visit, &c);
+  *vmax = (double)c.vmax; /* MAXVAL per rank, then MPI_ALLREDUCE MAX (:1533-1535) */
   return rc;
 }

@@ -23,6 +23,16 @@ int orc_fft_par_dcl_n(int op, const double *V1, const double *V2, double *Vout, 
 int orc_apply_n(int op, const double *V1, int nsl1, const double *V2, int nsl2, double *Vout, int np,
                 int m_max_c, int nb_procs, int bloc_size, int m_max_pad, int N);
 
+/* FFT_PAR_REAL (fft_parallel.F90:28-145): values of every field at the N angles 2*pi*j/N, N =
+ * orc_fft_par_real_planes(m_max, opt_nb_plane) (opt_nb_plane <= 0: absent).  Vout(N, nsl/2, np): the
+ * ranks' V_out(N, nsl/2, np/nb_procs) one after the other (rank r holds points r*np/nb_procs ..). */
+int orc_fft_par_real_planes(int m_max, int opt_nb_plane);
+int orc_fft_par_real(const double *V1, int nsl, int np, int m_max_c, int nb_procs, int opt_nb_plane, double *Vout);
+/* FFT_MAX_VEL_DCL (fft_parallel.F90:1426-1541): the maximum over points and the N = 2*m_max_pad-1
+ * angles of |V1| (first 3-vector for nsl == 6, |first field| otherwise). */
+int orc_fft_max_vel(const double *V1, int nsl, int np, int m_max_c, int nb_procs, int bloc_size, int m_max_pad,
+                    double *vmax);
+
 #ifdef __cplusplus
 }
 #endif

@@ -74,6 +74,34 @@ def make(case):
     return name, err
 
 
+# synthesis-only routines: name, kind, np, nslot, m, nb_procs, opt_nb_plane (real) or m_max_pad (maxvel), alpha, seed
+SYNTH_CASES = [
+    ("real_np11_m6", "real", 11, 6, 6, 1, 0, 0.3, 31),          # FFT_PAR_REAL, N = 2m-1
+    ("real_np12_m6_p3_opt20", "real", 12, 2, 6, 3, 20, 0.2, 32),  # 3 ranks, opt_nb_plane: N = 19
+    ("maxvel_np13_m5", "maxvel", 13, 6, 5, 1, 7, 0.3, 33),       # FFT_MAX_VEL_DCL, |3-vector|
+    ("maxvel_np13_m6_p2", "maxvel", 13, 2, 6, 2, 9, 0.2, 34),    # |scalar|, 2 ranks, dummy points
+]
+
+
+def make_synth(case):
+    name, kind, npts, nsl, m, procs, extra, alpha, seed = case
+    V = R.synthetic_field(npts, nsl, m, alpha, 3000 + seed)
+    if kind == "real":
+        out = R.c_real(V, nb_procs=procs, opt_nb_plane=extra or None)
+        err = R.rel_l2(out, R.synth_grid(V, out.shape[0]))
+    else:
+        out = np.array([R.c_max_vel(V, extra, nb_procs=procs)])
+        g = R.synth_grid(V, 2 * extra - 1)
+        ex = np.sqrt((g[:, :3] ** 2).sum(axis=1)).max() if nsl == 6 else np.abs(g[:, 0]).max()
+        err = abs(out[0] - ex) / ex
+    assert err < 1e-14, (name, err)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), V1=V, out=out,
+                        meta=np.array([npts, m, extra, procs], dtype=np.int64), kind=np.array(kind))
+    return name, err
+
+
 if __name__ == "__main__":
     for c in CASES:
         print(*make(c))
+    for c in SYNTH_CASES:
+        print(*make_synth(c))

@@ -107,7 +107,13 @@ def test_sine_of_mode_zero_is_ignored():
     assert np.all(ref[:, 1::2, 0] == 0.0) or np.abs(ref[:, 1::2, 0]).max() < 1e-15
 
 
-@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLD, "*.npz"))))
+PRODUCT_FIXTURES = sorted(p for p in glob.glob(os.path.join(GOLD, "*.npz"))
+                          if not os.path.basename(p).startswith(("real_", "maxvel_")))
+SYNTH_FIXTURES = sorted(p for p in glob.glob(os.path.join(GOLD, "*.npz"))
+                        if os.path.basename(p).startswith(("real_", "maxvel_")))
+
+
+@pytest.mark.parametrize("path", PRODUCT_FIXTURES)
 def test_golden_fixtures_reproduce(path):
     z = np.load(path)
     npts, m, pad, procs = (int(v) for v in z["meta"])
@@ -217,3 +223,50 @@ def test_vjp_restatement_is_the_transpose():
         J[:, i] = R.cross_jvp(u, w, np.asfortranarray(v[:, :6]), np.asfortranarray(v[:, 6:]), pad).reshape(-1, order="F")
     jt = (J.T @ cot.reshape(-1, order="F")).reshape((npts, 12, m), order="F")
     np.testing.assert_allclose(R.cross_vjp(u, w, cot), jt, rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize("path", SYNTH_FIXTURES)
+def test_synthesis_fixtures_reproduce(path):
+    z = np.load(path)
+    npts, m, extra, procs = (int(v) for v in z["meta"])
+    if str(z["kind"]) == "real":
+        np.testing.assert_array_equal(R.c_real(z["V1"], nb_procs=procs, opt_nb_plane=extra or None), z["out"])
+    else:
+        assert R.c_max_vel(z["V1"], extra, nb_procs=procs) == z["out"][0]
+
+
+def test_fft_par_real_known_answers():
+    # FFT_PAR_REAL (fft_parallel.F90:28-145): a mode-1 field a cos t + b sin t at t_j = 2 pi j / N,
+    # N = 2 m_max - 1, or 2 m_max_pad - 1 with m_max_pad = (opt_nb_plane + 1) / 2 when that is larger.
+    m, npts = 4, 6
+    V = np.zeros((npts, 4, m), order="F")
+    rng = np.random.default_rng(9)
+    V[:, 0, 0] = rng.standard_normal(npts)          # mean of field 1
+    V[:, 0:2, 1] = rng.standard_normal((npts, 2))   # a, b of field 1
+    V[:, 3, 3] = rng.standard_normal(npts)          # sin 3t of field 2
+    for opt, N in ((None, 7), (5, 7), (12, 11), (13, 13)):
+        out = R.c_real(V, nb_procs=2, opt_nb_plane=opt)
+        assert out.shape == (N, 2, npts)
+        t = 2 * np.pi * np.arange(N) / N
+        want1 = V[None, :, 0, 0] + V[None, :, 0, 1] * np.cos(t)[:, None] + V[None, :, 1, 1] * np.sin(t)[:, None]
+        np.testing.assert_allclose(out[:, 0, :], want1, atol=1e-14)
+        np.testing.assert_allclose(out[:, 1, :], V[None, :, 3, 3] * np.sin(3 * t)[:, None], atol=1e-14)
+    with pytest.raises(ValueError):
+        R.c_real(np.zeros((5, 3, 4), order="F"))            # odd nb_field (:59)
+    with pytest.raises(ValueError):
+        R.c_real(np.zeros((5, 2, 4), order="F"), nb_procs=2)  # np not a multiple of nb_procs (:66-70)
+
+
+def test_fft_max_vel_known_answers():
+    # FFT_MAX_VEL_DCL (fft_parallel.F90:1426-1541): u = (cos t, sin t, 0) has |u| = 1 everywhere; a
+    # scalar a0 + a1 cos t peaks at t = 0, which is on every grid.
+    npts, m = 7, 3
+    U = np.zeros((npts, 6, m), order="F")
+    U[:, 0, 1] = 1.0   # u_r = cos t
+    U[:, 3, 1] = 1.0   # u_theta = sin t
+    assert abs(R.c_max_vel(U, 3) - 1.0) < 1e-15
+    assert abs(R.c_max_vel(U, 3, nb_procs=3, bloc_size=3) - 1.0) < 1e-15
+    S = np.zeros((npts, 2, m), order="F")
+    S[:, 0, 0] = np.arange(npts)
+    S[:, 0, 2] = 0.5
+    assert abs(R.c_max_vel(S, 4) - (npts - 1 + 0.5)) < 1e-13
