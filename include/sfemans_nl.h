@@ -11,6 +11,9 @@
  *   FFT_SCALAR_VECT_DCL     :1021-1220 V_out = s V (pb = 1) or V / s (pb = 2)
  *   FFT_TENSOR_DCL          :1543-1796 V_out(k, :, 2l-1:2l, :) = V1_k V2_l, or with
  *                                      opt_tension V1_k V2_l / (|V2| + 1e-14) - |V2| delta_kl
+ * and the synthesis-only routines:
+ *   FFT_PAR_REAL            :28-145    V_out(N, nb_field/2, np) = values on the grid
+ *   FFT_MAX_VEL_DCL         :1426-1541 V_out = max over points and angles of |V1|
  *
  * Array layout: every coefficient array is the Fortran array V(np, nslot, m)
  * in column-major order, point index fastest: element (p, s, n) is at
@@ -126,6 +129,16 @@ int sfnl_scalar_vect_f64(const double *v, const double *s, double *out, int64_t 
 int sfnl_tensor_f64(const double *v1, const double *v2, double *out, int64_t np, int m_max, int m_max_pad,
                     int tension, sfnl_stream_t stream);
 
+/* FFT_PAR_REAL (fft_parallel.F90:28-145): v (np, nslot, m_max) -> out (n_theta, nslot/2, np), the
+ * value of every field (slot pair) at theta_j = 2 pi j / n_theta, angle fastest.  The reference grid is
+ * n_theta = sfnl_fft_par_real_planes(m_max, opt_nb_plane); n_theta < 2*m_max-1 is SFNL_ERR_ALIAS. */
+int sfnl_real_f64(const double *v, double *out, int64_t np, int nslot, int m_max, int n_theta, sfnl_stream_t stream);
+/* FFT_MAX_VEL_DCL (fft_parallel.F90:1426-1541): *vmax (one double in device memory, written on `stream`)
+ * = the maximum over the points and the 2*m_max_pad-1 angles of |v|: the first 3-vector's length when
+ * nslot == 6, |first field| otherwise (:1527-1532).  A NaN in the field propagates to the result. */
+int sfnl_max_vel_f64(const double *v, double *vmax, int64_t np, int nslot, int m_max, int m_max_pad,
+                     sfnl_stream_t stream);
+
 /* The MHD nonlinear bundle in one launch, each term with the semantics of
  * the reference routine that computes it today:
  *   uxw   = u x w     (FFT_PAR_CROSS_PROD_DCL, subroutine_ns_with_velocity.F90:627 passes (RotV, W))
@@ -205,6 +218,19 @@ int sfnl_fft_scalar_vect_dcl(const double *V1_in, const double *V2_in, double *V
  * reference rejects (error_petsc at :1705): SFNL_ERR_ARG.  nb_field != 6: SFNL_ERR_SHAPE. */
 int sfnl_fft_tensor_dcl(const double *V1_in, const double *V2_in, double *V_out, int np, int nb_field, int m_max_c,
                         int nb_procs, int bloc_size, int m_max_pad, int opt_tension, double *temps);
+
+/* fft_parallel.F90:71-80: the grid length of FFT_PAR_REAL, 2*m_max_pad-1 with m_max_pad =
+ * (opt_nb_plane+1)/2 when opt_nb_plane > 2*m_max-1, else m_max (opt_nb_plane <= 0: argument absent). */
+int sfnl_fft_par_real_planes(int m_max, int opt_nb_plane);
+/* fft_parallel.F90:28 (FFT_PAR_REAL): V_out, allocated by the caller, holds
+ * N * (nb_field/2) * np doubles, N = sfnl_fft_par_real_planes(m_max_c, opt_nb_plane): with one rank
+ * every point is local (the reference's bloc_size = np/nb_procs).  nb_procs must be 1. */
+int sfnl_fft_par_real(const double *V1_in, double *V_out, int np, int nb_field, int m_max_c, int nb_procs,
+                      int opt_nb_plane);
+/* fft_parallel.F90:1426 (FFT_MAX_VEL_DCL): *V_out (host) = the maximum of |V1_in| on the
+ * 2*m_max_pad-1 angles; the per-point maxima come back from the GPU and are reduced on the host. */
+int sfnl_fft_max_vel_dcl(const double *V1_in, double *V_out, int np, int nb_field, int m_max_c, int nb_procs,
+                         int bloc_size, int m_max_pad);
 
 /* Host-array variants of the device entry points (copy in, compute, copy out). */
 int sfnl_product_f64_host(int op, const double *a, const double *b, double *out, int64_t np, int m_max,

@@ -12,6 +12,11 @@ dealiased products, with the same names, argument order and meaning:
     FFT_SCALAR_VECT_DCL   (communicator, V1_in, V2_in, V_out, pb, nb_procs, bloc_size, m_max_pad, temps=None)
     FFT_TENSOR_DCL        (communicator, V1_in, V2_in, V_out, nb_procs, bloc_size, m_max_pad, temps=None,
                            opt_tension=None)
+    FFT_PAR_REAL          (communicator, V1_in, V_out=None, opt_nb_plane=None) -> V_out
+    FFT_MAX_VEL_DCL       (communicator, V1_in, nb_procs, bloc_size, m_max_pad) -> V_out (a float)
+
+(FFT_PAR_REAL's V_out is ALLOCATABLE in the reference and FFT_MAX_VEL_DCL's a scalar INTENT(OUT):
+here both are returned.)
 
 Arrays are Fortran-ordered (np, nslot, m): numpy arrays in host memory
 (copied through the library's host entry points) or CUDA tensors with
@@ -85,6 +90,11 @@ _SIGS = {
     "sfnl_fft_par_div_dcl": [_P, _P, _P, _I, _I, _I, _I, _I, _P],
     "sfnl_fft_scalar_vect_dcl": [_P, _P, _P] + [_I] * 8 + [_P],
     "sfnl_fft_tensor_dcl": [_P, _P, _P] + [_I] * 7 + [_P],
+    "sfnl_real_f64": [_P, _P, _L, _I, _I, _I, _P],
+    "sfnl_max_vel_f64": [_P, _P, _L, _I, _I, _I, _P],
+    "sfnl_fft_par_real_planes": [_I, _I],
+    "sfnl_fft_par_real": [_P, _P] + [_I] * 5,
+    "sfnl_fft_max_vel_dcl": [_P, _P] + [_I] * 6,
     "sfnl_bundle_mhd_host": [_P] * 9 + [_L, _I, _I, _I],
     "sfnl_set_check_finite": [_I],
     "sfnl_finalize": [],
@@ -240,6 +250,39 @@ def tensor(v1, v2, tension: bool = False, out=None, m_max_pad=None, split=None, 
                    stream=stream)
 
 
+def real_planes(m_max: int, opt_nb_plane: int | None = None) -> int:
+    """Grid length of FFT_PAR_REAL (fft_parallel.F90:71-80)."""
+    n = lib().sfnl_fft_par_real_planes(m_max, opt_nb_plane or 0)
+    _check(min(n, 0))
+    return n
+
+
+def synthesis(v, n_theta: int | None = None, out=None, stream=None):
+    """Values of every field of v (np, nslot, m) at theta_j = 2 pi j / N: a CUDA tensor (N, nslot/2, np)
+    in Fortran order (FFT_PAR_REAL, fft_parallel.F90:28-145; N = 2*m_max-1 by default)."""
+    import torch
+
+    npts, nsl, m = v.shape
+    N = n_theta or real_planes(m)
+    if out is None:
+        out = torch.empty((npts, nsl // 2, N), device=v.device, dtype=torch.float64).permute(2, 1, 0)
+    if tuple(out.shape) != (N, nsl // 2, npts):
+        raise SfnlError(-2, f"out must be {(N, nsl // 2, npts)}")
+    _check(lib().sfnl_real_f64(_dptr(v, "v"), _dptr(out, "out"), npts, nsl, m, N, _stream(stream)))
+    return out
+
+
+def max_vel(v, m_max_pad: int | None = None, stream=None) -> float:
+    """FFT_MAX_VEL_DCL (fft_parallel.F90:1426-1541): max over points and the 2*m_max_pad-1 angles of |v|."""
+    import torch
+
+    npts, nsl, m = v.shape
+    res = torch.empty(1, device=v.device, dtype=torch.float64)
+    _check(lib().sfnl_max_vel_f64(_dptr(v, "v"), ctypes.c_void_p(res.data_ptr()), npts, nsl, m, m_max_pad or m,
+                                  _stream(stream)))
+    return float(res.item())
+
+
 def bundle_mhd(u, w, b, j, gradt, m_max_pad: int | None = None, outs=None, algo: int = ALGO_AUTO,
                split: int | None = None, stream=None):
     """(u x w, u x b, j x b, u . gradT) in one launch."""
@@ -392,3 +435,47 @@ def FFT_TENSOR_DCL(communicator, V1_in, V2_in, V_out, nb_procs, bloc_size, m_max
         raise SfnlError(-1, "BUG in FFT_TENSOR_DCL : opt_tension should be true if used")
     return _fortran_call("tension" if opt_tension else "tensor", communicator, V1_in, V2_in, V_out, nb_procs,
                          bloc_size, m_max_pad, temps)
+
+
+def FFT_PAR_REAL(communicator, V1_in, V_out=None, opt_nb_plane=None):
+    """Values of the fields of V1_in (np, nb_field, m) on the N = 2*m_max_pad-1 angles 2*pi*j/N
+    (fft_parallel.F90:28-145): V_out (N, nb_field/2, np), returned (and filled in when given)."""
+    import numpy as np
+
+    npts, nf, mc = V1_in.shape
+    if communicator is not None:
+        from .parallel import fft_par_real_distributed
+
+        return fft_par_real_distributed(communicator, V1_in, opt_nb_plane)
+    N = real_planes(mc, opt_nb_plane)
+    if hasattr(V1_in, "is_cuda"):
+        return synthesis(V1_in, n_theta=N, out=V_out)
+    V1_in = np.asfortranarray(V1_in, dtype=np.float64)
+    if V_out is None:
+        V_out = np.zeros((N, nf // 2, npts), order="F")
+    if V_out.shape != (N, nf // 2, npts) or not V_out.flags.f_contiguous or V_out.dtype != np.float64:
+        raise SfnlError(-2, f"V_out must be a float64 Fortran array of shape {(N, nf // 2, npts)}")
+    _check(lib().sfnl_fft_par_real(_host_ptr(V1_in), _host_ptr(V_out), npts, nf, mc, 1, opt_nb_plane or 0))
+    return V_out
+
+
+def FFT_MAX_VEL_DCL(communicator, V1_in, nb_procs, bloc_size, m_max_pad):
+    """Maximum over the points and the 2*m_max_pad-1 angles of |V1_in| (its first 3-vector for
+    nb_field == 6, |first field| otherwise) (fft_parallel.F90:1426-1541)."""
+    import numpy as np
+
+    npts, nf, mc = V1_in.shape
+    if communicator is not None:
+        from .parallel import fft_max_vel_distributed
+
+        return fft_max_vel_distributed(communicator, V1_in, nb_procs, bloc_size, m_max_pad)
+    if hasattr(V1_in, "is_cuda"):
+        if nb_procs != 1:
+            raise SfnlError(-4, "one GPU holds all modes: nb_procs must be 1")
+        if npts > nb_procs * bloc_size:
+            raise SfnlError(-2, "np > nb_procs*bloc_size")
+        return max_vel(V1_in, m_max_pad)
+    V1_in = np.asfortranarray(V1_in, dtype=np.float64)
+    res = np.zeros(1)
+    _check(lib().sfnl_fft_max_vel_dcl(_host_ptr(V1_in), _host_ptr(res), npts, nf, mc, nb_procs, bloc_size, m_max_pad))
+    return float(res[0])

@@ -272,7 +272,9 @@ struct HostBuf {
   int nslot;        // slots of the Fortran array (np, nslot, m), or (ew, np, nslot, m)
   double *dev;      // device buffer of the current chunk, same layout with np_chunk points
   int ew = 1;       // leading extent (3 for the tensor layout V(3, np, 6, m))
+  int mrows = 0;    // > 0: the array has nslot * mrows rows of points instead of nslot * m
 };
+size_t buf_rows(const HostBuf &b, int m) { return (size_t)b.nslot * (b.mrows > 0 ? b.mrows : m); }
 
 constexpr int kPipe = 3;
 constexpr size_t kChunkBytes = size_t(192) << 20;  // target bytes per chunk (inputs + outputs)
@@ -295,7 +297,7 @@ int with_device_buffers(std::vector<HostBuf> &bufs, int64_t np, int m, ChunkRun 
     if (!ps.st[i] && cudaStreamCreateWithFlags(&ps.st[i], cudaStreamNonBlocking) != cudaSuccess)
       return set_error(SFNL_ERR_CUDA, "cudaStreamCreate failed");
   size_t per_point = 0;
-  for (auto &b : bufs) per_point += sizeof(double) * (size_t)b.ew * b.nslot * m;
+  for (auto &b : bufs) per_point += sizeof(double) * (size_t)b.ew * buf_rows(b, m);
   int64_t cp = (int64_t)(kChunkBytes / (per_point ? per_point : 1));
   cp = (cp / 128) * 128;
   if (cp < 128) cp = 128;
@@ -303,7 +305,7 @@ int with_device_buffers(std::vector<HostBuf> &bufs, int64_t np, int m, ChunkRun 
   const int64_t nchunks = (np + cp - 1) / cp;
   const int slots = nchunks < kPipe ? (int)nchunks : kPipe;
   size_t slot_bytes = 0;
-  for (auto &b : bufs) slot_bytes += (sizeof(double) * (size_t)b.ew * b.nslot * m * cp + 255) & ~size_t(255);
+  for (auto &b : bufs) slot_bytes += (sizeof(double) * (size_t)b.ew * buf_rows(b, m) * cp + 255) & ~size_t(255);
   const size_t total = slot_bytes * slots;
   if (total > s->work_bytes) {
     if (s->work) cudaFree(s->work);
@@ -324,10 +326,10 @@ int with_device_buffers(std::vector<HostBuf> &bufs, int64_t np, int m, ChunkRun 
     size_t off = slot_bytes * slot;
     for (auto &b : bufs) {
       b.dev = reinterpret_cast<double *>(s->work + off);
-      off += (sizeof(double) * (size_t)b.ew * b.nslot * m * cp + 255) & ~size_t(255);
+      off += (sizeof(double) * (size_t)b.ew * buf_rows(b, m) * cp + 255) & ~size_t(255);
       const size_t w = sizeof(double) * b.ew;  // bytes per point in a row
       if (b.src && cudaMemcpy2DAsync(b.dev, w * n, static_cast<const double *>(b.src) + b.ew * p0, w * np, w * n,
-                                     (size_t)b.nslot * m, cudaMemcpyHostToDevice, st) != cudaSuccess)
+                                     buf_rows(b, m), cudaMemcpyHostToDevice, st) != cudaSuccess)
         rc = set_error(SFNL_ERR_CUDA, "host-to-device copy failed");
     }
     if (rc == SFNL_OK) rc = run(bufs, n, ctx, st);
@@ -335,7 +337,7 @@ int with_device_buffers(std::vector<HostBuf> &bufs, int64_t np, int m, ChunkRun 
       const size_t w = sizeof(double) * b.ew;
       if (rc == SFNL_OK && b.dst &&
           cudaMemcpy2DAsync(static_cast<double *>(b.dst) + b.ew * p0, w * np, b.dev, w * n, w * n,
-                            (size_t)b.nslot * m, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+                            buf_rows(b, m), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         rc = set_error(SFNL_ERR_CUDA, "device-to-host copy failed");
     }
   }
@@ -395,6 +397,28 @@ int check_fortran_args(int np, int nb_field, int m_max_c, int nb_procs, int bloc
   if (nb_procs != 1) return set_error(SFNL_ERR_UNSUPPORTED, "one GPU holds all modes: nb_procs must be 1");
   if (bloc_size < 1 || (int64_t)np > (int64_t)nb_procs * bloc_size)
     return set_error(SFNL_ERR_SHAPE, "np > nb_procs*bloc_size");
+  return SFNL_OK;
+}
+
+// Synthesis-only routines (sfnl_synth.cu) on host arrays: grid values, or per-point maxima of |v|
+// reduced on the host.
+struct SynthCtx {
+  int nslot, m, N;
+  bool maxv;
+};
+
+int run_synth_dev(std::vector<HostBuf> &b, int64_t np_chunk, void *vctx, cudaStream_t st) {
+  auto *c = static_cast<SynthCtx *>(vctx);
+  return c->maxv ? launch_point_max_vel(b[0].dev, b[1].dev, np_chunk, c->nslot, c->m, c->N, st)
+                 : launch_real(b[0].dev, b[1].dev, np_chunk, c->nslot, c->m, c->N, st);
+}
+
+int check_synth(int64_t np, int nslot, int m, const char *what) {
+  if (np < 0 || m < 1 || nslot < 2 || (nslot % 2) != 0) {
+    std::string msg = std::string("Bug in ") + what + ": MOD(nb_field,2)/=0 .OR. m_max_c==0";
+    return set_error(SFNL_ERR_ARG, msg.c_str());
+  }
+  if (m > 4096) return set_error(SFNL_ERR_UNSUPPORTED, "m_max beyond this build's limits");
   return SFNL_OK;
 }
 
@@ -624,6 +648,70 @@ int sfnl_tensor_f64(const double *v1, const double *v2, double *out, int64_t np,
 int sfnl_div_f64(const double *c1, const double *c2, double *out, int64_t np, int m_max, int m_max_pad,
                  sfnl_stream_t stream) {
   return sfnl_product_f64(SFNL_OP_DIV, c1, c2, out, np, m_max, m_max_pad, 0, SFNL_ALGO_AUTO, stream);
+}
+
+int sfnl_fft_par_real_planes(int m_max, int opt_nb_plane) {
+  if (m_max < 1) return set_error(SFNL_ERR_ARG, "m_max < 1");
+  const int m_max_pad = opt_nb_plane > 2 * m_max - 1 ? (opt_nb_plane + 1) / 2 : m_max;
+  return 2 * m_max_pad - 1;
+}
+
+int sfnl_real_f64(const double *v, double *out, int64_t np, int nslot, int m_max, int n_theta, sfnl_stream_t stream) {
+  int rc = check_synth(np, nslot, m_max, "FFT_PAR_REAL");
+  if (rc) return rc;
+  if (n_theta < 2 * m_max - 1) return set_error(SFNL_ERR_ALIAS, "n_theta < 2*m_max-1: the grid cannot hold the modes");
+  if (n_theta > (1 << 21)) return set_error(SFNL_ERR_UNSUPPORTED, "n_theta beyond this build's limits");
+  if (np == 0) return SFNL_OK;
+  if (!v || !out) return set_error(SFNL_ERR_ARG, "null array");
+  return launch_real(v, out, np, nslot, m_max, n_theta, as_stream(stream));
+}
+
+int sfnl_max_vel_f64(const double *v, double *vmax, int64_t np, int nslot, int m_max, int m_max_pad,
+                     sfnl_stream_t stream) {
+  int rc = check_synth(np, nslot, m_max, "FFT_MAX_VEL_DCL");
+  if (rc) return rc;
+  if (m_max_pad < m_max) return set_error(SFNL_ERR_ALIAS, "m_max_pad < m_max: the padded spectrum cannot hold the modes");
+  if (m_max_pad > (1 << 20)) return set_error(SFNL_ERR_UNSUPPORTED, "m_max_pad beyond this build's limits");
+  if (!vmax || (np > 0 && !v)) return set_error(SFNL_ERR_ARG, "null array");
+  cudaStream_t st = as_stream(stream);
+  if (cudaMemsetAsync(vmax, 0, sizeof(double), st) != cudaSuccess) return set_error(SFNL_ERR_CUDA, "memset of the result failed");
+  return launch_max_vel(v, vmax, np, nslot, m_max, 2 * m_max_pad - 1, st);
+}
+
+int sfnl_fft_par_real(const double *V1_in, double *V_out, int np, int nb_field, int m_max_c, int nb_procs,
+                      int opt_nb_plane) {
+  int rc = check_synth(np, nb_field, m_max_c, "FFT_PAR_REAL");
+  if (rc) return rc;
+  if (nb_procs != 1) return set_error(SFNL_ERR_UNSUPPORTED, "one GPU holds all modes: nb_procs must be 1");
+  const int N = sfnl_fft_par_real_planes(m_max_c, opt_nb_plane);
+  if (np == 0) return SFNL_OK;
+  if (!V1_in || !V_out) return set_error(SFNL_ERR_ARG, "null array");
+  std::vector<HostBuf> bufs = {{V1_in, nullptr, nb_field, nullptr}, {nullptr, V_out, 1, nullptr, N * (nb_field / 2), 1}};
+  SynthCtx c{nb_field, m_max_c, N, false};
+  return with_device_buffers(bufs, np, m_max_c, run_synth_dev, &c, nullptr);
+}
+
+int sfnl_fft_max_vel_dcl(const double *V1_in, double *V_out, int np, int nb_field, int m_max_c, int nb_procs,
+                         int bloc_size, int m_max_pad) {
+  int rc = check_synth(np, nb_field, m_max_c, "FFT_MAX_VEL_DCL");
+  if (rc) return rc;
+  if (nb_procs != 1) return set_error(SFNL_ERR_UNSUPPORTED, "one GPU holds all modes: nb_procs must be 1");
+  if (bloc_size < 1 || (int64_t)np > (int64_t)nb_procs * bloc_size) return set_error(SFNL_ERR_SHAPE, "np > nb_procs*bloc_size");
+  if (m_max_pad < m_max_c) return set_error(SFNL_ERR_ALIAS, "m_max_pad < m_max: the padded spectrum cannot hold the modes");
+  if (!V_out) return set_error(SFNL_ERR_ARG, "null result");
+  *V_out = 0.0;
+  if (np == 0) return SFNL_OK;
+  if (!V1_in) return set_error(SFNL_ERR_ARG, "null array");
+  std::vector<double> pmax((size_t)np);
+  std::vector<HostBuf> bufs = {{V1_in, nullptr, nb_field, nullptr}, {nullptr, pmax.data(), 1, nullptr, 1, 1}};
+  SynthCtx c{nb_field, m_max_c, 2 * m_max_pad - 1, true};
+  rc = with_device_buffers(bufs, np, m_max_c, run_synth_dev, &c, nullptr);
+  if (rc) return rc;
+  double best = 0.0;
+  for (double x : pmax)
+    if (!(x <= best)) best = x;  // a NaN propagates, as in the device entry
+  *V_out = best;
+  return SFNL_OK;
 }
 
 int sfnl_product_f64_host(int op, const double *a, const double *b, double *out, int64_t np, int m_max, int m_max_pad,

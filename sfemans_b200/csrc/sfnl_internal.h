@@ -27,6 +27,11 @@ int fast_grid_length(int m);                            // sfnl_fast.cu
 void fast_release_tables();                             // sfnl_fast.cu
 int launch_split(const ProgArgs &a, int split, cudaStream_t st);  // sfnl_split.cu
 void split_release_tables();                            // sfnl_split.cu
+// Synthesis only (sfnl_synth.cu): out (N, nslot/2, np); vmax a zeroed device double that receives the
+// maximum of |v|; pmax (np) the maximum of |v| of each point.
+int launch_real(const double *v, double *out, int64_t np, int nslot, int m, int N, cudaStream_t st);
+int launch_max_vel(const double *v, double *vmax, int64_t np, int nslot, int m, int N, cudaStream_t st);
+int launch_point_max_vel(const double *v, double *pmax, int64_t np, int nslot, int m, int N, cudaStream_t st);
 
 // Elementary programs: cross (6 -> 3), dot (6 -> 1), product (2 -> 1),
 // scalar x vector (4 -> 3) and tensor (6 -> 9).  Every bilinear program of

@@ -10,6 +10,8 @@
 !   FFT_PAR_DIV_DCL         fft_parallel.F90:667
 !   FFT_SCALAR_VECT_DCL     fft_parallel.F90:1021
 !   FFT_TENSOR_DCL          fft_parallel.F90:1543
+!   FFT_PAR_REAL            fft_parallel.F90:28    (V_out ALLOCATABLE, allocated here as in the reference)
+!   FFT_MAX_VEL_DCL         fft_parallel.F90:1426
 ! One GPU holds every Fourier mode, so the Fourier communicator must have
 ! one rank (nb_procs == 1).  bloc_size is checked (np <= nb_procs*bloc_size)
 ! and otherwise unused.  temps(3), when present, receives the data-movement
@@ -25,6 +27,7 @@ MODULE fft_parallele_gpu
   PRIVATE
   PUBLIC :: FFT_PAR_CROSS_PROD_DCL, FFT_PAR_DOT_PROD_DCL, FFT_PAR_PROD_DCL
   PUBLIC :: FFT_PAR_DIV_DCL, FFT_SCALAR_VECT_DCL, FFT_TENSOR_DCL
+  PUBLIC :: FFT_PAR_REAL, FFT_MAX_VEL_DCL
 
   INTERFACE
      FUNCTION sfnl_fft_par_cross_prod_dcl(V1_in, V2_in, V_out, np, nb_field, m_max_c, nb_procs, &
@@ -86,6 +89,30 @@ MODULE fft_parallele_gpu
        TYPE(C_PTR), VALUE    :: temps
        INTEGER(C_INT)        :: rc
      END FUNCTION sfnl_fft_tensor_dcl
+
+     FUNCTION sfnl_fft_par_real_planes(m_max, opt_nb_plane) RESULT(n) BIND(C, NAME='sfnl_fft_par_real_planes')
+       IMPORT :: C_INT
+       INTEGER(C_INT), VALUE :: m_max, opt_nb_plane
+       INTEGER(C_INT)        :: n
+     END FUNCTION sfnl_fft_par_real_planes
+
+     FUNCTION sfnl_fft_par_real(V1_in, V_out, np, nb_field, m_max_c, nb_procs, opt_nb_plane) RESULT(rc) &
+          BIND(C, NAME='sfnl_fft_par_real')
+       IMPORT :: C_INT, C_DOUBLE
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(IN)  :: V1_in
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(OUT) :: V_out
+       INTEGER(C_INT), VALUE :: np, nb_field, m_max_c, nb_procs, opt_nb_plane
+       INTEGER(C_INT)        :: rc
+     END FUNCTION sfnl_fft_par_real
+
+     FUNCTION sfnl_fft_max_vel_dcl(V1_in, V_out, np, nb_field, m_max_c, nb_procs, bloc_size, m_max_pad) RESULT(rc) &
+          BIND(C, NAME='sfnl_fft_max_vel_dcl')
+       IMPORT :: C_INT, C_DOUBLE
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(IN) :: V1_in
+       REAL(C_DOUBLE), INTENT(OUT)              :: V_out
+       INTEGER(C_INT), VALUE :: np, nb_field, m_max_c, nb_procs, bloc_size, m_max_pad
+       INTEGER(C_INT)        :: rc
+     END FUNCTION sfnl_fft_max_vel_dcl
 
      FUNCTION sfnl_last_error() RESULT(msg) BIND(C, NAME='sfnl_last_error')
        IMPORT :: C_PTR
@@ -240,5 +267,37 @@ CONTAINS
        temps(1:MIN(3,SIZE(temps))) = t3(1:MIN(3,SIZE(temps)))
     END IF
   END SUBROUTINE FFT_TENSOR_DCL
+
+  SUBROUTINE FFT_PAR_REAL(communicator, V1_in, V_out, opt_nb_plane)
+    MPI_Comm :: communicator
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(IN) :: V1_in
+    REAL(KIND=8), DIMENSION(:,:,:), ALLOCATABLE            :: V_out
+    INTEGER, OPTIONAL                                      :: opt_nb_plane
+    INTEGER(C_INT) :: rc, nplane, n_r
+    CALL check_comm(communicator, 1, 'FFT_PAR_REAL')
+    nplane = 0
+    IF (PRESENT(opt_nb_plane)) nplane = INT(opt_nb_plane, C_INT)
+    n_r = sfnl_fft_par_real_planes(INT(SIZE(V1_in,3), C_INT), nplane)
+    IF (n_r < 1) CALL stop_on_error(n_r, 'FFT_PAR_REAL')
+    IF (ALLOCATED(V_out)) DEALLOCATE(V_out)
+    ALLOCATE(V_out(n_r, SIZE(V1_in,2)/2, SIZE(V1_in,1)))
+    rc = sfnl_fft_par_real(V1_in, V_out, INT(SIZE(V1_in,1), C_INT), INT(SIZE(V1_in,2), C_INT), &
+         INT(SIZE(V1_in,3), C_INT), 1_C_INT, nplane)
+    CALL stop_on_error(rc, 'FFT_PAR_REAL')
+  END SUBROUTINE FFT_PAR_REAL
+
+  SUBROUTINE FFT_MAX_VEL_DCL(communicator, V1_in, V_out, nb_procs, bloc_size, m_max_pad)
+    MPI_Comm :: communicator
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(IN) :: V1_in
+    REAL(KIND=8), INTENT(OUT)                              :: V_out
+    INTEGER, INTENT(IN) :: bloc_size, m_max_pad, nb_procs
+    REAL(C_DOUBLE) :: vmax
+    INTEGER(C_INT) :: rc
+    CALL check_comm(communicator, nb_procs, 'FFT_MAX_VEL_DCL')
+    rc = sfnl_fft_max_vel_dcl(V1_in, vmax, INT(SIZE(V1_in,1), C_INT), INT(SIZE(V1_in,2), C_INT), &
+         INT(SIZE(V1_in,3), C_INT), INT(nb_procs, C_INT), INT(bloc_size, C_INT), INT(m_max_pad, C_INT))
+    CALL stop_on_error(rc, 'FFT_MAX_VEL_DCL')
+    V_out = vmax
+  END SUBROUTINE FFT_MAX_VEL_DCL
 
 END MODULE fft_parallele_gpu

@@ -87,3 +87,64 @@ def fft_par_distributed(kind, group, x, y, out, nb_procs, bloc_size, m_max_pad, 
     if temps is not None:
         temps[:] = 0.0
     return out
+
+
+def _gather_modes(group, x, nb_procs, bloc_size):
+    """The first MPI_ALLTOALL of the reference (fft_parallel.F90:217, :93, :1482): this rank's m_max_c
+    modes of all points -> all modes of its bloc_size points, (bloc_size, nslot, m_max) Fortran layout."""
+    import torch
+    import torch.distributed as dist
+
+    npts, nsl, mc = x.shape
+    np_tot = nb_procs * bloc_size
+    tp = torch.zeros((np_tot, nsl, mc), dtype=x.dtype, device=x.device)
+    tp[:npts] = x
+    send = tp.reshape(nb_procs, bloc_size, nsl, mc).permute(0, 3, 2, 1).contiguous()  # (P, mc, nsl, bloc)
+    recv = torch.empty_like(send)
+    dist.all_to_all_single(recv.view(-1), send.view(-1), group=group)
+    full = recv.permute(3, 2, 0, 1).reshape(bloc_size, nsl, nb_procs * mc)
+    return full.contiguous().permute(2, 1, 0).contiguous().permute(2, 1, 0)
+
+
+def _default_real(xb, N):
+    from . import synthesis
+
+    return synthesis(xb, n_theta=N)
+
+
+def _default_max_vel(xb, m_max_pad):
+    from . import max_vel
+
+    return max_vel(xb, m_max_pad)
+
+
+def fft_par_real_distributed(group, x, opt_nb_plane=None, compute=None):
+    """FFT_PAR_REAL over a mode-distributed communicator: the rank's V_out (N, nslot/2, np/nb_procs)
+    for its block of points (fft_parallel.F90:65-71: np must be a multiple of nb_procs).
+    ``compute(xb, N)`` synthesises the gathered block; it defaults to the CUDA kernel."""
+    import torch.distributed as dist
+
+    nb_procs = dist.get_world_size(group)
+    npts, nsl, mc = x.shape
+    if npts % nb_procs:
+        raise ValueError("Bug in FFT_PAR_REAL: np is not a multiple of nb_procs")
+    m_max = mc * nb_procs
+    m_max_pad = (opt_nb_plane + 1) // 2 if opt_nb_plane and opt_nb_plane > 2 * m_max - 1 else m_max
+    xb = _gather_modes(group, x, nb_procs, npts // nb_procs)
+    return (compute or _default_real)(xb, 2 * m_max_pad - 1)
+
+
+def fft_max_vel_distributed(group, x, nb_procs, bloc_size, m_max_pad, compute=None):
+    """FFT_MAX_VEL_DCL over a mode-distributed communicator: the gathered block's maximum, then the
+    reference's MPI_ALLREDUCE(MAX) (fft_parallel.F90:1533-1535).  Dummy points are zero (:1478)."""
+    import torch
+    import torch.distributed as dist
+
+    if dist.get_world_size(group) != nb_procs:
+        raise ValueError("nb_procs must equal the communicator size")
+    if x.shape[0] > nb_procs * bloc_size:
+        raise ValueError("np > nb_procs*bloc_size")
+    xb = _gather_modes(group, x, nb_procs, bloc_size)
+    t = torch.tensor([float((compute or _default_max_vel)(xb, m_max_pad))], dtype=torch.float64, device=x.device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return float(t.item())

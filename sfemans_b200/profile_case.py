@@ -3,7 +3,8 @@
     python -m sfemans_b200.profile_case --program bundle --form fast --np 100000 --m 64 --reps 1
 
 Programs: cross, dot, prod, div, svect, svdiv, tensor, tension (the reference routines, by the op names of
-sfemans_b200.KINDS) and bundle (u x w, u x b, j x b, u . gradT).
+sfemans_b200.KINDS), bundle (u x w, u x b, j x b, u . gradT), and the synthesis-only real (grid values of a
+3-vector, FFT_PAR_REAL) and maxvel (FFT_MAX_VEL_DCL).
 Forms: fast (FP64, folded transforms), grid (FP64, caller's grid), split3 / split2 (bf16 slices on tcgen05).
 Inputs are N(0,1)*exp(-alpha*n) coefficients generated on the device; the padding is m_max_pad = 3*m/2.
 Prints the average milliseconds per call, timed with CUDA events after one untimed call.
@@ -28,7 +29,7 @@ def main(argv=None):
     import sfemans_b200 as sf
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--program", default="cross", choices=list(sf.KINDS) + ["bundle"])
+    ap.add_argument("--program", default="cross", choices=list(sf.KINDS) + ["bundle", "real", "maxvel"])
     ap.add_argument("--form", default="fast", choices=["fast", "grid", "split3", "split2"])
     ap.add_argument("--np", type=int, default=100_000)
     ap.add_argument("--m", type=int, default=64)
@@ -38,7 +39,14 @@ def main(argv=None):
     kw = {"fast": dict(algo=sf.ALGO_FAST), "grid": dict(algo=sf.ALGO_GRID), "split3": dict(split=sf.SPLIT_BF16X3),
           "split2": dict(split=sf.SPLIT_BF16X2)}[a.form]
     pad = 3 * a.m // 2 if a.m > 1 else 1
-    if a.program == "bundle":
+    if a.program in ("real", "maxvel"):
+        x = _field(torch, a.np, 6, a.m, a.alpha, 1)
+        if a.program == "real":
+            out = sf.synthesis(x)
+            call = lambda: sf.synthesis(x, out=out)  # noqa: E731
+        else:
+            call = lambda: sf.max_vel(x, pad)  # noqa: E731
+    elif a.program == "bundle":
         ins = [_field(torch, a.np, 6, a.m, a.alpha, 10 + i) for i in range(5)]
         outs = tuple(sf.fortran_empty(a.np, 6, a.m) for _ in range(3)) + (sf.fortran_empty(a.np, 2, a.m),)
         call = lambda: sf.bundle_mhd(*ins, m_max_pad=pad, outs=outs, **kw)  # noqa: E731

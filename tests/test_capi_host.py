@@ -133,3 +133,22 @@ def test_python_mirror_rejects_what_the_reference_rejects():
     with pytest.raises(sf.SfnlError) as e:  # V_out of the wrong shape
         sf.FFT_TENSOR_DCL(None, V, V, V, 1, 5, 3)
     assert e.value.code == -2
+
+
+def test_synthesis_argument_checks():
+    L = sf.lib()
+    a = np.zeros((4, 6, 2), order="F")
+    p = ctypes.c_void_p(a.ctypes.data)
+    # FFT_PAR_REAL: grid length (fft_parallel.F90:71-80), odd nb_field, more than one Fourier rank
+    assert L.sfnl_fft_par_real_planes(4, 0) == 7 and L.sfnl_fft_par_real_planes(4, 12) == 11
+    assert L.sfnl_fft_par_real(p, p, 4, 5, 2, 1, 0) == -1
+    assert L.sfnl_fft_par_real(p, p, 4, 6, 0, 1, 0) == -1
+    assert L.sfnl_fft_par_real(p, p, 4, 6, 2, 2, 0) == -4
+    # device entry: a grid shorter than 2m-1 cannot hold the modes
+    d = ctypes.c_void_p(16)
+    assert L.sfnl_real_f64(d, d, 10, 6, 8, 14, NULL) == -3
+    # FFT_MAX_VEL_DCL: odd nb_field, np > nb_procs*bloc_size, short pad, null result
+    assert L.sfnl_fft_max_vel_dcl(p, p, 4, 3, 2, 1, 5, 3) == -1
+    assert L.sfnl_fft_max_vel_dcl(p, p, 4, 6, 2, 1, 3, 3) == -2
+    assert L.sfnl_fft_max_vel_dcl(p, p, 4, 6, 2, 1, 5, 1) == -3
+    assert L.sfnl_max_vel_f64(d, NULL, 10, 6, 4, 6, NULL) == -1

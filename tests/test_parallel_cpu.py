@@ -14,7 +14,7 @@ import torch.multiprocessing as mp
 
 from oracle import ref_fft as R
 from sfemans_b200 import KINDS
-from sfemans_b200.parallel import fft_par_distributed, shard_range
+from sfemans_b200.parallel import fft_max_vel_distributed, fft_par_distributed, fft_par_real_distributed, shard_range
 
 
 @pytest.mark.parametrize("npts,world", [(0, 1), (7, 3), (28000, 8), (1_400_000, 8), (5, 8)])
@@ -73,6 +73,47 @@ def test_mode_distributed_layout_matches_single_rank(kind, world, npts, m):
     q = ctx.Queue()
     port = _free_port()
     procs = [ctx.Process(target=_worker, args=(r, world, port, kind, npts, m, pad, bloc, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    res = dict(q.get(timeout=5) for _ in range(world))
+    assert all(p.exitcode == 0 for p in procs)
+    for r in range(world):
+        assert res[r] < 1e-14, res
+
+
+def _synth_worker(rank, world, port, kind, npts, nsl, m, extra, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        V = R.synthetic_field(npts, nsl, m, 0.2, 61)
+        mc = m // world
+        loc = torch.from_numpy(np.ascontiguousarray(V[:, :, rank * mc:(rank + 1) * mc].T)).permute(2, 1, 0)
+        to_np = lambda t: np.asfortranarray(t.permute(2, 1, 0).contiguous().numpy().T)  # noqa: E731
+        if kind == "real":
+            out = fft_par_real_distributed(None, loc, extra or None,
+                                           compute=lambda xb, N: torch.from_numpy(
+                                               np.ascontiguousarray(R.synth_grid(to_np(xb), N).T)).permute(2, 1, 0))
+            bloc = npts // world
+            ref = R.c_real(V, nb_procs=world, opt_nb_plane=extra or None)[:, :, rank * bloc:(rank + 1) * bloc]
+            q.put((rank, float(np.abs(out.numpy() - ref).max())))
+        else:
+            bloc = npts // world + 1
+            got = fft_max_vel_distributed(None, loc, world, bloc, extra,
+                                          compute=lambda xb, pad: R.c_max_vel(to_np(xb), pad))
+            q.put((rank, abs(got - R.c_max_vel(V, extra))))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("kind,world,npts,nsl,m,extra", [("real", 2, 10, 6, 4, 0), ("real", 3, 9, 2, 6, 20),
+                                                        ("maxvel", 2, 11, 6, 4, 6), ("maxvel", 3, 7, 2, 6, 9)])
+def test_synthesis_routines_over_a_mode_distributed_communicator(kind, world, npts, nsl, m, extra):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_synth_worker, args=(r, world, port, kind, npts, nsl, m, extra, q)) for r in range(world)]
     for p in procs:
         p.start()
     for p in procs:
