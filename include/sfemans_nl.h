@@ -151,6 +151,33 @@ int sfnl_bundle_mhd_f64(const double *u, const double *w, const double *b, const
                         int m_max_pad, int algo, sfnl_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * The Navier-Stokes caller of the cross product, smb_cross_prod_gauss_sft_par
+ * (SOURCES/SIMULATION/subroutine_ns_with_velocity.F90:512-629): from the nodal
+ * velocity it builds, at every Gauss point and for every mode, the velocity W, the
+ * curl RotV in cylindrical coordinates (mode list_mode[i]) and, with precession, the
+ * rotation Om, and returns out = (RotV + 2 Om) x W (FFT_PAR_CROSS_PROD_DCL).
+ *   v, omega   (np_nodes, 6, nmod) nodal coefficients; omega NULL: no precession
+ *   jj         (n_w, me) int, 1-based node numbers of each element (mesh%jj); numbers
+ *              outside 1..np_nodes are clamped on the device (the host entry rejects them)
+ *   ww         (n_w, l_G) basis values at the Gauss points (mesh%gauss%ww)
+ *   dw         (2, n_w, l_G, me) basis (d/dr, d/dz) on each element (mesh%gauss%dw)
+ *   rr         (2, np_nodes) node coordinates (r, z) (mesh%rr)
+ *   list_mode  (nmod) int, the Fourier mode numbers
+ *   out        (l_G*me, 6, nmod), Gauss points element by element
+ *   m_max_pad  <= 0: 3*nmod/2, the caller's choice (:625)
+ *   work       device buffer of 12*l_G*me*nmod doubles for RotV and W, or NULL: a buffer
+ *              owned by the library (one per device, grown with cudaMalloc when too small;
+ *              calls that overlap on the GPU then share it and race)
+ * ------------------------------------------------------------------------- */
+int sfnl_cross_gauss_f64(const double *v, const int *jj, const double *ww, const double *dw, const double *rr,
+                         const int *list_mode, const double *omega, double *out, int np_nodes, int me, int n_w,
+                         int l_G, int nmod, int m_max_pad, double *work, sfnl_stream_t stream);
+/* The same on host arrays (k_d = SIZE(mesh%rr,1) must be 2; nb_procs must be 1), for the Fortran shim. */
+int sfnl_smb_cross_prod_gauss(const double *V_in, const int *jj, const double *ww, const double *dw, const double *rr,
+                              int k_d, const int *list_mode, const double *omega, double *V_out, int np_nodes, int me,
+                              int n_w, int l_G, int nmod, int nb_procs);
+
+/* ---------------------------------------------------------------------------
  * Linearised cross product N(u, w) = u x w about a base state (u, w).
  * New capability: the reference's LightKrylov operator binds rmatvec to the
  * forward map (LIGHTKRYLOV_OBJECTS/exponential_propagator.F90:61-62).

@@ -119,6 +119,9 @@ def _lib():
         lib.orc_fft_par_real.argtypes = [P] + [ctypes.c_int] * 5 + [P]
         lib.orc_fft_max_vel.restype = ctypes.c_int
         lib.orc_fft_max_vel.argtypes = [P] + [ctypes.c_int] * 6 + [P]
+        IP = ctypes.POINTER(ctypes.c_int)
+        lib.orc_cross_gauss.restype = ctypes.c_int
+        lib.orc_cross_gauss.argtypes = [P, IP, P, P, P, IP, P] + [ctypes.c_int] * 5 + [P, P, P]
         _LIB = lib
     return _LIB
 
@@ -198,6 +201,95 @@ def synth_grid(V, N: int, workers: int = 1):
     cu[:, :, :m] = _to_complex(V, nsl // 2)
     ru = sfft.irfft(cu, n=N, axis=2, norm="forward", workers=workers)  # (np, nf, N)
     return np.asfortranarray(np.transpose(ru, (2, 1, 0)))
+
+
+def synthetic_p2_mesh(nr: int, nz: int, seed: int = 0):
+    """A P2 triangle mesh of the meridian rectangle r in [0.1, 1.1], z in [0, 1] (nr x nz squares, two
+    triangles each, vertices jittered by a seeded generator), in the arrays the Gauss-point callers
+    read: jj (6, me) 1-based nodes (3 vertices, then the midpoints of edges 2-3, 3-1, 1-2), rr (2, np)
+    coordinates (r, z), and at 7 interior quadrature points ww (6, 7) = the P2 basis and
+    dw (2, 6, 7, me) = its (d/dr, d/dz) on each element.  Geometry only matters for realistic sizes."""
+    rng = np.random.default_rng(seed)
+    hr, hz = 1.0 / nr, 1.0 / nz
+    vr = np.array([[0.1 + i * hr for j in range(nz + 1)] for i in range(nr + 1)])
+    vz = np.array([[j * hz for j in range(nz + 1)] for i in range(nr + 1)])
+    jit = 0.15 * rng.uniform(-1, 1, size=(2, nr + 1, nz + 1))
+    vr[1:-1, :] += jit[0, 1:-1, :] * hr
+    vz[:, 1:-1] += jit[1, :, 1:-1] * hz
+    coords = [(vr[i, j], vz[i, j]) for i in range(nr + 1) for j in range(nz + 1)]
+    vid = lambda i, j: i * (nz + 1) + j  # noqa: E731
+    mid = {}
+    tris = []
+    for i in range(nr):
+        for j in range(nz):
+            a, b, c, d = vid(i, j), vid(i + 1, j), vid(i + 1, j + 1), vid(i, j + 1)
+            tris += [(a, b, c), (a, c, d)]
+    jj = []
+    for (a, b, c) in tris:
+        e = []
+        for (x, y) in ((b, c), (c, a), (a, b)):
+            key = (min(x, y), max(x, y))
+            if key not in mid:
+                mid[key] = len(coords)
+                coords.append(((coords[x][0] + coords[y][0]) / 2, (coords[x][1] + coords[y][1]) / 2))
+            e.append(mid[key])
+        jj.append([a, b, c] + e)
+    jj = np.asfortranarray(np.array(jj, dtype=np.int32).T + 1)
+    rr = np.asfortranarray(np.array(coords).T)
+    # 7 interior points (barycentric): the centroid and two orbits of 3
+    bary = np.array([[1 / 3, 1 / 3, 1 / 3], [2 / 3, 1 / 6, 1 / 6], [1 / 6, 2 / 3, 1 / 6], [1 / 6, 1 / 6, 2 / 3],
+                     [0.1, 0.45, 0.45], [0.45, 0.1, 0.45], [0.45, 0.45, 0.1]])
+    L = bary.T  # (3, 7)
+    ww = np.asfortranarray(np.vstack([L[0] * (2 * L[0] - 1), L[1] * (2 * L[1] - 1), L[2] * (2 * L[2] - 1),
+                                      4 * L[1] * L[2], 4 * L[2] * L[0], 4 * L[0] * L[1]]))
+    # d(basis)/d(lambda_k) at the points: (6, 3, 7)
+    dl = np.zeros((6, 3, 7))
+    for k in range(3):
+        dl[k, k] = 4 * L[k] - 1
+    for e, (x, y) in enumerate(((1, 2), (2, 0), (0, 1))):
+        dl[3 + e, x] = 4 * L[y]
+        dl[3 + e, y] = 4 * L[x]
+    me = len(tris)
+    dw = np.zeros((2, 6, 7, me), order="F")
+    for m, (a, b, c) in enumerate(tris):
+        P = np.array([coords[a], coords[b], coords[c]])  # (3, 2)
+        T = np.array([[P[0, 0] - P[2, 0], P[1, 0] - P[2, 0]], [P[0, 1] - P[2, 1], P[1, 1] - P[2, 1]]])
+        G = np.linalg.inv(T)  # rows: d(lambda_1, lambda_2)/d(r, z)
+        dlam = np.array([G[0], G[1], -G[0] - G[1]])  # (3 lambdas, 2 coords)
+        dw[:, :, :, m] = np.einsum("nkl,kd->dnl", dl, dlam)
+    return {"jj": jj, "rr": rr, "ww": ww, "dw": dw, "np": rr.shape[1], "me": me, "n_w": 6, "l_G": 7}
+
+
+def c_cross_gauss(V, mesh, list_mode, omega=None, product=True):
+    """Long-double / FP64 restatement of smb_cross_prod_gauss_sft_par (subroutine_ns_with_velocity.F90:
+    512-629): returns (V_out, RotV, W), each (l_G*me, 6, nmod) Fortran (V_out zero when product=False:
+    the operands only, for sizes where the O(N^2) oracle product is too slow)."""
+    V = np.asfortranarray(V, dtype=np.float64)
+    npn, _, nmod = V.shape
+    ng = mesh["l_G"] * mesh["me"]
+    outs = [np.zeros((ng, 6, nmod), order="F") for _ in range(3)]
+    lm = np.ascontiguousarray(list_mode, dtype=np.int32)
+    om = None if omega is None else np.asfortranarray(omega, dtype=np.float64)
+    IP = ctypes.POINTER(ctypes.c_int)
+    rc = _lib().orc_cross_gauss(_ptr(V), mesh["jj"].ctypes.data_as(IP), _ptr(mesh["ww"]), _ptr(mesh["dw"]),
+                                _ptr(mesh["rr"]), lm.ctypes.data_as(IP), None if om is None else _ptr(om), npn,
+                                mesh["me"], mesh["n_w"], mesh["l_G"], nmod, _ptr(outs[0]) if product else None,
+                                _ptr(outs[1]), _ptr(outs[2]))
+    if rc != 0:
+        raise ValueError(f"oracle rejected arguments (status {rc})")
+    return tuple(outs)
+
+
+def precession_omega(npn: int, list_mode, taux: float, angle_s_pi: float):
+    """The nodal rotation field of the precession case (subroutine_ns_with_velocity.F90:540-554)."""
+    om = np.zeros((npn, 6, len(list_mode)), order="F")
+    for i, mode in enumerate(list_mode):
+        if mode == 1:
+            om[:, 0, i] = taux * np.sin(angle_s_pi * np.pi)
+            om[:, 3, i] = -taux * np.sin(angle_s_pi * np.pi)
+        elif mode == 0:
+            om[:, 4, i] = taux * np.cos(angle_s_pi * np.pi)
+    return om
 
 
 # ----------------------------------------------------------------------------

@@ -18,6 +18,10 @@
  *   FFT_PAR_REAL            fft_parallel.F90:28-145     (synthesis only)
  *   FFT_MAX_VEL_DCL         fft_parallel.F90:1426-1541  (synthesis, |v|, maximum)
  *
+ * and the Navier-Stokes caller that builds the operands of the cross product at the Gauss points:
+ *
+ *   smb_cross_prod_gauss_sft_par  SOURCES/SIMULATION/subroutine_ns_with_velocity.F90:512-629
+ *
  * including the nb_procs / bloc_size bookkeeping: each emulated rank owns
  * m_max_c contiguous Fourier modes, packs a mode-major dist_field with dummy
  * points set to 1.d100 (:205-211), the MPI_ALLTOALL is emulated by block
@@ -393,5 +397,67 @@ int orc_fft_max_vel(const double *V1, int nsl, int np, int m_max_c, int nb_procs
   /* dummy points are 0 (:1478): their |v| = 0 never exceeds the maximum of the others */
   const int rc = synth_ranks(V1, nsl, np, m_max_c, nb_procs, bloc_size, m_max_pad, 0.0, maxv_visit, &c);
   *vmax = (double)c.vmax; /* MAXVAL per rank, then MPI_ALLREDUCE MAX (:1533-1535) */
+  return rc;
+}
+
+/* smb_cross_prod_gauss_sft_par (subroutine_ns_with_velocity.F90:512-629), one Fourier rank holding
+ * the nmod modes list_mode[0..nmod): for every mode i, element m and Gauss point l (Gauss index
+ * (m l_G + l), :563-574) the velocity W = sum_n V(jj(n,m)) ww(n,l), the rotation Om likewise from
+ * omega (NULL: no precession, Om = 0, :615-617), the radius ray = sum_n rr(1,jj(n,m)) ww(n,l) (:573)
+ * and the curl in cylindrical coordinates of Fourier mode `mode` (:592-607); RotV += 2 Om (:620);
+ * then FFT_PAR_CROSS_PROD_DCL(RotV, W) with m_max_pad = 3*nmod/2 (:624-626).  jj is 1-based
+ * (n_w, me); ww (n_w, l_G); dw (2, n_w, l_G, me); rr (2, np_nodes); V, omega (np_nodes, 6, nmod);
+ * Vout (l_G*me, 6, nmod), or NULL to skip the product.  RotV and W (l_G*me, 6, nmod) may be returned
+ * (NULL: not wanted). */
+int orc_cross_gauss(const double *V, const int *jj, const double *ww, const double *dw, const double *rr,
+                    const int *list_mode, const double *omega, int np_nodes, int me, int n_w, int l_G, int nmod,
+                    double *Vout, double *RotV_out, double *W_out) {
+  if (np_nodes < 1 || me < 0 || n_w < 1 || l_G < 1 || nmod < 1) return -1;
+  const int ng = l_G * me;
+  double *RotV = (double *)calloc((size_t)ng * 6 * nmod + 1, sizeof(double));
+  double *W = (double *)calloc((size_t)ng * 6 * nmod + 1, sizeof(double));
+  if (!RotV || !W) { free(RotV); free(W); return -4; }
+  for (int m = 0; m < me; ++m)
+    for (int n = 0; n < n_w; ++n)
+      if (jj[n + (size_t)n_w * m] < 1 || jj[n + (size_t)n_w * m] > np_nodes) { free(RotV); free(W); return -2; }
+  for (int i = 0; i < nmod; ++i) {
+    const double mode = (double)list_mode[i];
+    for (int m = 0; m < me; ++m)
+      for (int l = 0; l < l_G; ++l) {
+        const size_t idx = (size_t)m * l_G + l;
+        const double *dwl = dw + (size_t)2 * n_w * (l + (size_t)l_G * m); /* dw_loc = dw(:,:,l,m) */
+        double ray = 0.0, w[6] = {0, 0, 0, 0, 0, 0}, om[6] = {0, 0, 0, 0, 0, 0};
+        double d1[6] = {0, 0, 0, 0, 0, 0}, d2[6] = {0, 0, 0, 0, 0, 0}; /* SUM(Vs(:,k)*dw_loc(1|2,:)) */
+        for (int n = 0; n < n_w; ++n) {
+          const int node = jj[n + (size_t)n_w * m] - 1;
+          const double wv = ww[n + (size_t)n_w * l];
+          ray += rr[2 * (size_t)node] * wv;
+          for (int k = 0; k < 6; ++k) {
+            const double vs = V[IDX3(node, k, i, np_nodes, 6)];
+            w[k] += vs * wv;
+            d1[k] += vs * dwl[2 * n];
+            d2[k] += vs * dwl[2 * n + 1];
+            if (omega) om[k] += omega[IDX3(node, k, i, np_nodes, 6)] * wv;
+          }
+        }
+        double *R = RotV + idx, *Wo = W + idx;
+#define AT(a, k) a[(size_t)ng * ((k) + 6 * (size_t)i)]
+        for (int k = 0; k < 6; ++k) AT(Wo, k) = w[k];
+        AT(R, 0) = mode / ray * w[5] - d2[2];
+        AT(R, 3) = d2[1] - d1[5];
+        AT(R, 4) = 1 / ray * w[2] + d1[2] - mode / ray * w[1];
+        AT(R, 1) = -mode / ray * w[4] - d2[3];
+        AT(R, 2) = d2[0] - d1[4];
+        AT(R, 5) = 1 / ray * w[3] + d1[3] + mode / ray * w[0];
+        for (int k = 0; k < 6; ++k) AT(R, k) = AT(R, k) + 2.0 * om[k];
+#undef AT
+      }
+  }
+  const int pad = 3 * nmod / 2 < nmod ? nmod : 3 * nmod / 2;
+  int rc = Vout ? orc_apply_n(ORC_CROSS, RotV, 6, W, 6, Vout, ng, nmod, 1, ng + 1, pad, 2 * pad - 1) : 0;
+  if (RotV_out) memcpy(RotV_out, RotV, sizeof(double) * (size_t)ng * 6 * nmod);
+  if (W_out) memcpy(W_out, W, sizeof(double) * (size_t)ng * 6 * nmod);
+  free(RotV);
+  free(W);
   return rc;
 }

@@ -32,6 +32,13 @@ int orc_fft_par_real(const double *V1, int nsl, int np, int m_max_c, int nb_proc
  * angles of |V1| (first 3-vector for nsl == 6, |first field| otherwise). */
 int orc_fft_max_vel(const double *V1, int nsl, int np, int m_max_c, int nb_procs, int bloc_size, int m_max_pad,
                     double *vmax);
+/* smb_cross_prod_gauss_sft_par (subroutine_ns_with_velocity.F90:512-629): W, RotV (+2 Om) at the Gauss
+ * points of a P-k mesh from nodal V, then RotV x W.  jj 1-based (n_w, me); ww (n_w, l_G); dw (2, n_w,
+ * l_G, me); rr (2, np_nodes); V, omega (np_nodes, 6, nmod), omega may be NULL; Vout (l_G*me, 6, nmod);
+ * RotV_out / W_out (same shape) may be NULL. */
+int orc_cross_gauss(const double *V, const int *jj, const double *ww, const double *dw, const double *rr,
+                    const int *list_mode, const double *omega, int np_nodes, int me, int n_w, int l_G, int nmod,
+                    double *Vout, double *RotV_out, double *W_out);
 
 #ifdef __cplusplus
 }

@@ -91,6 +91,8 @@ _SIGS = {
     "sfnl_fft_scalar_vect_dcl": [_P, _P, _P] + [_I] * 8 + [_P],
     "sfnl_fft_tensor_dcl": [_P, _P, _P] + [_I] * 7 + [_P],
     "sfnl_real_f64": [_P, _P, _L, _I, _I, _I, _P],
+    "sfnl_cross_gauss_f64": [_P] * 8 + [_I] * 6 + [_P, _P],
+    "sfnl_smb_cross_prod_gauss": [_P] * 5 + [_I] + [_P] * 3 + [_I] * 6,
     "sfnl_max_vel_f64": [_P, _P, _L, _I, _I, _I, _P],
     "sfnl_fft_par_real_planes": [_I, _I],
     "sfnl_fft_par_real": [_P, _P] + [_I] * 5,
@@ -281,6 +283,24 @@ def max_vel(v, m_max_pad: int | None = None, stream=None) -> float:
     _check(lib().sfnl_max_vel_f64(_dptr(v, "v"), ctypes.c_void_p(res.data_ptr()), npts, nsl, m, m_max_pad or m,
                                   _stream(stream)))
     return float(res.item())
+
+
+def cross_gauss(v, mesh, list_mode, omega=None, m_max_pad=None, out=None, work=None, stream=None):
+    """(curl v + 2 omega) x v at the Gauss points from the nodal v (np_nodes, 6, nmod): the operands and
+    product of smb_cross_prod_gauss_sft_par (subroutine_ns_with_velocity.F90:512-629).  ``mesh``: CUDA
+    tensors jj (n_w, me) int32 1-based, ww (n_w, l_G), dw (2, n_w, l_G, me), rr (2, np_nodes), all in
+    Fortran order; list_mode: int32 CUDA tensor of the nmod mode numbers.  Returns (l_G*me, 6, nmod)."""
+    npn, _, nmod = v.shape
+    n_w, me = mesh["jj"].shape
+    l_G = mesh["ww"].shape[1]
+    if out is None:
+        out = fortran_empty(l_G * me, 6, nmod, device=v.device)
+    ptr = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    _check(lib().sfnl_cross_gauss_f64(_dptr(v, "v"), ptr(mesh["jj"]), ptr(mesh["ww"]), ptr(mesh["dw"]),
+                                      ptr(mesh["rr"]), ptr(list_mode), None if omega is None else _dptr(omega, "omega"),
+                                      _dptr(out, "out"), npn, me, n_w, l_G, nmod, m_max_pad or 0, ptr(work),
+                                      _stream(stream)))
+    return out
 
 
 def bundle_mhd(u, w, b, j, gradt, m_max_pad: int | None = None, outs=None, algo: int = ALGO_AUTO,
@@ -479,3 +499,39 @@ def FFT_MAX_VEL_DCL(communicator, V1_in, nb_procs, bloc_size, m_max_pad):
     res = np.zeros(1)
     _check(lib().sfnl_fft_max_vel_dcl(_host_ptr(V1_in), _host_ptr(res), npts, nf, mc, nb_procs, bloc_size, m_max_pad))
     return float(res[0])
+
+
+def smb_cross_prod_gauss_sft_par(communicator, mesh, list_mode, V_in, V_out=None, precession_in=False,
+                                 taux_precession=0.0, angle_s_pi=0.0):
+    """The Navier-Stokes nonlinear term at the Gauss points (subroutine_ns_with_velocity.F90:512-629) on
+    host arrays: ``mesh`` holds the numpy arrays jj (n_w, me, 1-based), ww, dw, rr of mesh%... ; the
+    precession parameters stand for the reference's inputs%taux_precession and inputs%angle_s_pi.
+    Returns V_out (l_G*me, 6, nmod)."""
+    import numpy as np
+
+    if communicator is not None:
+        raise SfnlError(-4, "one GPU holds all modes: the Gauss-point entry runs on one Fourier rank")
+    V_in = np.asfortranarray(V_in, dtype=np.float64)
+    npn, _, nmod = V_in.shape
+    jj = np.asfortranarray(mesh["jj"], dtype=np.int32)
+    n_w, me = jj.shape
+    ww = np.asfortranarray(mesh["ww"], dtype=np.float64)
+    dw = np.asfortranarray(mesh["dw"], dtype=np.float64)
+    rr = np.asfortranarray(mesh["rr"], dtype=np.float64)
+    l_G = ww.shape[1]
+    lm = np.ascontiguousarray(list_mode, dtype=np.int32)
+    om = None
+    if precession_in:  # the nodal rotation field of :540-554
+        om = np.zeros_like(V_in)
+        for i, mode in enumerate(lm):
+            if mode == 1:
+                om[:, 0, i] = taux_precession * np.sin(angle_s_pi * np.pi)
+                om[:, 3, i] = -taux_precession * np.sin(angle_s_pi * np.pi)
+            elif mode == 0:
+                om[:, 4, i] = taux_precession * np.cos(angle_s_pi * np.pi)
+    if V_out is None:
+        V_out = np.zeros((l_G * me, 6, nmod), order="F")
+    _check(lib().sfnl_smb_cross_prod_gauss(_host_ptr(V_in), _host_ptr(jj), _host_ptr(ww), _host_ptr(dw), _host_ptr(rr),
+                                           rr.shape[0], _host_ptr(lm), None if om is None else _host_ptr(om),
+                                           _host_ptr(V_out), npn, me, n_w, l_G, nmod, 1))
+    return V_out

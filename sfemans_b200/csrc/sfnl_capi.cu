@@ -33,8 +33,25 @@ struct DevState {
   int *d_flag = nullptr;
   char *work = nullptr;
   size_t work_bytes = 0;
-  std::mutex mu;
+  char *gwork = nullptr;  // Gauss-point operands (device entry without a caller workspace, host entry)
+  size_t gwork_bytes = 0;
+  std::mutex mu;       // workspaces (held for a whole host call)
+  std::mutex flag_mu;  // the finite-check flag (taken inside host calls too)
 };
+
+// Grows the per-device Gauss-point buffer to `bytes` (caller holds s->mu).
+int grow_gwork(DevState *s, size_t bytes) {
+  if (bytes <= s->gwork_bytes) return SFNL_OK;
+  if (s->gwork) cudaFree(s->gwork);
+  s->gwork = nullptr;
+  s->gwork_bytes = 0;
+  if (cudaMalloc(&s->gwork, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(SFNL_ERR_ALLOC, "cudaMalloc of the Gauss-point workspace failed");
+  }
+  s->gwork_bytes = bytes;
+  return SFNL_OK;
+}
 constexpr int kMaxDev = 64;
 DevState g_dev[kMaxDev];
 std::mutex g_dev_mu;
@@ -86,7 +103,7 @@ __global__ void finite_scan(const double *p, int64_t n, int *flag) {
 int scan_outputs(const ProgArgs &a, cudaStream_t st) {
   DevState *s = dev_state();
   if (!s) return set_error(SFNL_ERR_CUDA, "no current device");
-  std::lock_guard<std::mutex> lk(s->mu);
+  std::lock_guard<std::mutex> lk(s->flag_mu);
   if (!s->d_flag && cudaMalloc(&s->d_flag, sizeof(int)) != cudaSuccess)
     return set_error(SFNL_ERR_ALLOC, "cudaMalloc of the finite-check flag failed");
   if (cudaMemsetAsync(s->d_flag, 0, sizeof(int), st) != cudaSuccess) return set_error(SFNL_ERR_CUDA, "memset failed");
@@ -454,12 +471,15 @@ int sfnl_finalize(void) {
   for (int d = 0; d < kMaxDev; ++d) {
     DevState &s = g_dev[d];
     std::lock_guard<std::mutex> lk(s.mu);
-    if (!s.work && !s.d_flag) continue;
+    if (!s.work && !s.d_flag && !s.gwork) continue;
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(d);
     if (s.work) cudaFree(s.work);
     if (s.d_flag) cudaFree(s.d_flag);
+    if (s.gwork) cudaFree(s.gwork);
+    s.gwork = nullptr;
+    s.gwork_bytes = 0;
     for (int i = 0; i < kPipe; ++i)
       if (g_pipe[d].st[i]) {
         cudaStreamDestroy(g_pipe[d].st[i]);
@@ -711,6 +731,91 @@ int sfnl_fft_max_vel_dcl(const double *V1_in, double *V_out, int np, int nb_fiel
   for (double x : pmax)
     if (!(x <= best)) best = x;  // a NaN propagates, as in the device entry
   *V_out = best;
+  return SFNL_OK;
+}
+
+static int check_gauss(int np_nodes, int me, int n_w, int l_G, int nmod) {
+  if (np_nodes < 1 || me < 0 || n_w < 1 || l_G < 1 || nmod < 1)
+    return set_error(SFNL_ERR_ARG, "np_nodes, n_w, l_G and the number of modes must be >= 1, me >= 0");
+  if (n_w > 10) return set_error(SFNL_ERR_UNSUPPORTED, "more than 10 nodes per element");
+  if ((int64_t)l_G * me > ((int64_t)1 << 31)) return set_error(SFNL_ERR_UNSUPPORTED, "too many Gauss points");
+  return SFNL_OK;
+}
+
+int sfnl_cross_gauss_f64(const double *v, const int *jj, const double *ww, const double *dw, const double *rr,
+                         const int *list_mode, const double *omega, double *out, int np_nodes, int me, int n_w,
+                         int l_G, int nmod, int m_max_pad, double *work, sfnl_stream_t stream) {
+  int rc = check_gauss(np_nodes, me, n_w, l_G, nmod);
+  if (rc) return rc;
+  const int pad = m_max_pad > 0 ? m_max_pad : (3 * nmod / 2 < nmod ? nmod : 3 * nmod / 2);
+  const int64_t ng = (int64_t)l_G * me;
+  int N = 0;
+  if ((rc = check_common(ng, nmod, pad, 0, 1, &N))) return rc;
+  if (ng == 0) return SFNL_OK;
+  if (!v || !jj || !ww || !dw || !rr || !list_mode || !out) return set_error(SFNL_ERR_ARG, "null array");
+  cudaStream_t st = as_stream(stream);
+  const size_t opnd = (size_t)ng * 6 * nmod;  // doubles of RotV (and of W)
+  double *rotv = work;
+  if (!rotv) {
+    DevState *s = dev_state();
+    if (!s) return set_error(SFNL_ERR_CUDA, "no current device");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if ((rc = grow_gwork(s, 2 * opnd * sizeof(double)))) return rc;
+    rotv = reinterpret_cast<double *>(s->gwork);
+  }
+  GaussArgs ga{v, omega, ww, dw, rr, jj, list_mode, np_nodes, me, n_w, l_G, nmod};
+  if ((rc = launch_gauss_eval(ga, rotv, rotv + opnd, st))) return rc;
+  ProgArgs pa;
+  if ((rc = build_product(OP_CROSS, rotv, rotv + opnd, out, ng, nmod, N, &pa))) return rc;
+  return run_fp64(pa, SFNL_ALGO_AUTO, N, st);
+}
+
+int sfnl_smb_cross_prod_gauss(const double *V_in, const int *jj, const double *ww, const double *dw, const double *rr,
+                              int k_d, const int *list_mode, const double *omega, double *V_out, int np_nodes, int me,
+                              int n_w, int l_G, int nmod, int nb_procs) {
+  int rc = check_gauss(np_nodes, me, n_w, l_G, nmod);
+  if (rc) return rc;
+  if (k_d != 2) return set_error(SFNL_ERR_UNSUPPORTED, "meridian meshes only (k_d == 2)");
+  if (nb_procs != 1) return set_error(SFNL_ERR_UNSUPPORTED, "one GPU holds all modes: nb_procs must be 1");
+  if (!V_in || !jj || !ww || !dw || !rr || !list_mode || !V_out) return set_error(SFNL_ERR_ARG, "null array");
+  for (int64_t t = 0; t < (int64_t)n_w * me; ++t)
+    if (jj[t] < 1 || jj[t] > np_nodes) return set_error(SFNL_ERR_ARG, "jj holds a node number outside 1..np_nodes");
+  using clk = std::chrono::steady_clock;
+  const auto t0 = clk::now();
+  const int64_t ng = (int64_t)l_G * me;
+  const size_t nv = (size_t)np_nodes * 6 * nmod, nout = (size_t)ng * 6 * nmod;
+  const size_t nww = (size_t)n_w * l_G, ndw = (size_t)2 * n_w * l_G * me, nrr = (size_t)2 * np_nodes;
+  auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+  const size_t bytes = al(8 * nv) * (omega ? 2 : 1) + al(8 * nout) * 3 + al(8 * nww) + al(8 * ndw) + al(8 * nrr) +
+                       al(4 * (size_t)n_w * me) + al(4 * (size_t)nmod);
+  DevState *s = dev_state();
+  if (!s) return set_error(SFNL_ERR_CUDA, "no current device");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if ((rc = grow_gwork(s, bytes))) return rc;
+  char *q = s->gwork;
+  auto take = [&](size_t b) { char *r = q; q += al(b); return r; };
+  double *d_v = (double *)take(8 * nv), *d_om = omega ? (double *)take(8 * nv) : nullptr;
+  double *d_out = (double *)take(8 * nout), *d_work = (double *)take(16 * nout);
+  double *d_ww = (double *)take(8 * nww), *d_dw = (double *)take(8 * ndw), *d_rr = (double *)take(8 * nrr);
+  int *d_jj = (int *)take(4 * (size_t)n_w * me), *d_lm = (int *)take(4 * (size_t)nmod);
+  cudaStream_t st = nullptr;
+  bool ok = cudaMemcpyAsync(d_v, V_in, 8 * nv, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+            (!omega || cudaMemcpyAsync(d_om, omega, 8 * nv, cudaMemcpyHostToDevice, st) == cudaSuccess) &&
+            cudaMemcpyAsync(d_ww, ww, 8 * nww, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+            cudaMemcpyAsync(d_dw, dw, 8 * ndw, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+            cudaMemcpyAsync(d_rr, rr, 8 * nrr, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+            cudaMemcpyAsync(d_jj, jj, 4 * (size_t)n_w * me, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+            cudaMemcpyAsync(d_lm, list_mode, 4 * (size_t)nmod, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  if (!ok) return set_error(SFNL_ERR_CUDA, "host-to-device copy failed");
+  rc = sfnl_cross_gauss_f64(d_v, d_jj, d_ww, d_dw, d_rr, d_lm, d_om, d_out, np_nodes, me, n_w, l_G, nmod, 0, d_work,
+                            reinterpret_cast<sfnl_stream_t>(st));
+  if (rc) return rc;
+  if (cudaMemcpyAsync(V_out, d_out, 8 * nout, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return set_error(SFNL_ERR_CUDA, "device-to-host copy failed");
+  g_host_timing[0] = 0.0;
+  g_host_timing[1] = std::chrono::duration<double>(clk::now() - t0).count();
+  g_host_timing[2] = 0.0;
   return SFNL_OK;
 }
 

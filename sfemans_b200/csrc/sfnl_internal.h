@@ -33,6 +33,17 @@ int launch_real(const double *v, double *out, int64_t np, int nslot, int m, int 
 int launch_max_vel(const double *v, double *vmax, int64_t np, int nslot, int m, int N, cudaStream_t st);
 int launch_point_max_vel(const double *v, double *pmax, int64_t np, int nslot, int m, int N, cudaStream_t st);
 
+// Operands of the Navier-Stokes cross product at the Gauss points (sfnl_gauss.cu): device arrays of
+// the mesh (jj 1-based (n_w, me), ww (n_w, l_G), dw (2, n_w, l_G, me), rr (2, np_nodes)), the nodal
+// velocity v and rotation omega (np_nodes, 6, nmod; omega may be null) and the modes list_mode (nmod).
+struct GaussArgs {
+  const double *v, *omega, *ww, *dw, *rr;
+  const int *jj, *list_mode;
+  int np_nodes, me, n_w, l_G, nmod;
+};
+// rotv, w: (l_G*me, 6, nmod) outputs (RotV + 2 Om, W).
+int launch_gauss_eval(const GaussArgs &a, double *rotv, double *w, cudaStream_t st);
+
 // Elementary programs: cross (6 -> 3), dot (6 -> 1), product (2 -> 1),
 // scalar x vector (4 -> 3) and tensor (6 -> 9).  Every bilinear program of
 // sfnl_ops.cuh is a sequence of them on one stream (the bundle is four, a

@@ -301,3 +301,77 @@ CONTAINS
   END SUBROUTINE FFT_MAX_VEL_DCL
 
 END MODULE fft_parallele_gpu
+
+!
+! smb_cross_prod_gauss_sft_par_gpu -- the Navier-Stokes caller of the cross product
+! (SOURCES/SIMULATION/subroutine_ns_with_velocity.F90:512-629) on the GPU: same arguments as
+! smb_cross_prod_gauss_sft_par; the Gauss-point velocity, curl and precession rotation are built
+! on the GPU from the nodal V_in and the mesh arrays, then (RotV + 2 Om) x W.  A caller switches by
+! calling this routine instead (one Fourier rank).
+!
+MODULE sfemans_gauss_gpu
+#include "petsc/finclude/petsc.h"
+  USE petsc
+  USE ISO_C_BINDING
+  USE def_type_mesh
+  USE input_data
+  IMPLICIT NONE
+  PRIVATE
+  PUBLIC :: smb_cross_prod_gauss_sft_par_gpu
+
+  INTERFACE
+     FUNCTION sfnl_smb_cross_prod_gauss(V_in, jj, ww, dw, rr, k_d, list_mode, omega, V_out, np_nodes, me, n_w, &
+          l_G, nmod, nb_procs) RESULT(rc) BIND(C, NAME='sfnl_smb_cross_prod_gauss')
+       IMPORT :: C_INT, C_DOUBLE, C_PTR
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(IN)  :: V_in, ww, dw, rr
+       INTEGER(C_INT), DIMENSION(*), INTENT(IN)  :: jj, list_mode
+       TYPE(C_PTR), VALUE                        :: omega
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(OUT) :: V_out
+       INTEGER(C_INT), VALUE :: k_d, np_nodes, me, n_w, l_G, nmod, nb_procs
+       INTEGER(C_INT)        :: rc
+     END FUNCTION sfnl_smb_cross_prod_gauss
+  END INTERFACE
+
+CONTAINS
+
+  SUBROUTINE smb_cross_prod_gauss_sft_par_gpu(communicator, mesh, list_mode, V_in, V_out, precession_in)
+    TYPE(mesh_type),                            INTENT(IN)  :: mesh
+    INTEGER,      DIMENSION(:),                 INTENT(IN)  :: list_mode
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(IN)  :: V_in
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(OUT) :: V_out
+    LOGICAL,                                    INTENT(IN)  :: precession_in
+    MPI_Comm :: communicator
+    REAL(C_DOUBLE), DIMENSION(:,:,:), ALLOCATABLE, TARGET :: omega
+    INTEGER(C_INT), DIMENSION(SIZE(list_mode)) :: modes
+    INTEGER(C_INT) :: rc
+    INTEGER :: nproc, code, i
+    REAL(KIND=8) :: PI
+    TYPE(C_PTR) :: om_ptr
+    CALL MPI_COMM_SIZE(communicator, nproc, code)
+    modes = INT(list_mode, C_INT)
+    om_ptr = C_NULL_PTR
+    IF (precession_in) THEN  ! the nodal rotation of :540-554
+       PI = ACOS(-1.d0)
+       ALLOCATE(omega(mesh%np, 6, SIZE(list_mode)))
+       omega = 0.d0
+       DO i = 1, SIZE(list_mode)
+          IF (list_mode(i) == 1) THEN
+             omega(:,1,i) = inputs%taux_precession * SIN(inputs%angle_s_pi*PI)
+             omega(:,4,i) = -inputs%taux_precession * SIN(inputs%angle_s_pi*PI)
+          ELSE IF (list_mode(i) == 0) THEN
+             omega(:,5,i) = inputs%taux_precession * COS(inputs%angle_s_pi*PI)
+          END IF
+       END DO
+       om_ptr = C_LOC(omega)
+    END IF
+    rc = sfnl_smb_cross_prod_gauss(V_in, INT(mesh%jj, C_INT), mesh%gauss%ww, mesh%gauss%dw, mesh%rr, &
+         INT(SIZE(mesh%rr,1), C_INT), modes, om_ptr, V_out, INT(mesh%np, C_INT), INT(mesh%me, C_INT), &
+         INT(mesh%gauss%n_w, C_INT), INT(mesh%gauss%l_G, C_INT), INT(SIZE(list_mode), C_INT), INT(nproc, C_INT))
+    IF (rc /= 0) THEN
+       WRITE(*,*) ' BUG in smb_cross_prod_gauss_sft_par_gpu (status ', rc, ')'
+       STOP
+    END IF
+    IF (ALLOCATED(omega)) DEALLOCATE(omega)
+  END SUBROUTINE smb_cross_prod_gauss_sft_par_gpu
+
+END MODULE sfemans_gauss_gpu

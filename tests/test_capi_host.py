@@ -152,3 +152,22 @@ def test_synthesis_argument_checks():
     assert L.sfnl_fft_max_vel_dcl(p, p, 4, 6, 2, 1, 3, 3) == -2
     assert L.sfnl_fft_max_vel_dcl(p, p, 4, 6, 2, 1, 5, 1) == -3
     assert L.sfnl_max_vel_f64(d, NULL, 10, 6, 4, 6, NULL) == -1
+
+
+def test_gauss_point_entry_checks():
+    L = sf.lib()
+    mesh = {"jj": np.ones((6, 2), dtype=np.int32, order="F"), "ww": np.zeros((6, 7), order="F"),
+            "dw": np.zeros((2, 6, 7, 2), order="F"), "rr": np.ones((2, 5), order="F")}
+    V = np.zeros((5, 6, 2), order="F")
+    mesh["jj"][3, 1] = 9  # node 9 of 5
+    with pytest.raises(sf.SfnlError) as e:
+        sf.smb_cross_prod_gauss_sft_par(None, mesh, [0, 1], V)
+    assert e.value.code == -1 and "jj" in sf.last_error()
+    mesh["jj"][3, 1] = 2
+    mesh["rr"] = np.ones((3, 5), order="F")  # k_d = 3
+    with pytest.raises(sf.SfnlError) as e:
+        sf.smb_cross_prod_gauss_sft_par(None, mesh, [0, 1], V)
+    assert e.value.code == -4
+    d = ctypes.c_void_p(16)
+    assert L.sfnl_cross_gauss_f64(d, d, d, d, d, d, None, d, 5, 2, 11, 7, 2, 0, None, NULL) == -4  # n_w > 10
+    assert L.sfnl_cross_gauss_f64(d, d, d, d, d, d, None, d, 0, 2, 6, 7, 2, 0, None, NULL) == -1

@@ -270,3 +270,22 @@ def test_fft_max_vel_known_answers():
     S[:, 0, 0] = np.arange(npts)
     S[:, 0, 2] = 0.5
     assert abs(R.c_max_vel(S, 4) - (npts - 1 + 0.5)) < 1e-13
+
+
+def test_gauss_point_curl_known_answer():
+    # smb_cross_prod_gauss_sft_par (subroutine_ns_with_velocity.F90:512-629) on solid-body rotation
+    # u = (0, r, 0), mode 0: curl u = (0, 0, 2) (u_theta/r + d u_theta/dr), which P2 elements reproduce
+    # exactly, and (curl u) x u = (-2 r, 0, 0).
+    mesh = R.synthetic_p2_mesh(4, 3, 2)
+    V = np.zeros((mesh["np"], 6, 1), order="F")
+    V[:, 2, 0] = mesh["rr"][0]
+    out, rot, w = R.c_cross_gauss(V, mesh, [0])
+    ray = np.einsum("nl,nm->lm", mesh["ww"], mesh["rr"][0][mesh["jj"] - 1]).T.ravel()  # Gauss radii
+    np.testing.assert_allclose(rot[:, 4, 0], 2.0, atol=1e-12)
+    np.testing.assert_allclose(np.delete(rot[:, :, 0], 4, axis=1), 0.0, atol=1e-12)
+    np.testing.assert_allclose(w[:, 2, 0], ray, atol=1e-14)
+    np.testing.assert_allclose(out[:, 0, 0], -2.0 * ray, atol=1e-12)
+    # precession adds 2 Om to the curl: mode 0 carries Om_z = taux cos(angle pi)
+    om = R.precession_omega(mesh["np"], [0], 0.5, 0.25)
+    _, rot2, _ = R.c_cross_gauss(V, mesh, [0], om)
+    np.testing.assert_allclose(rot2[:, 4, 0], 2.0 + 2 * 0.5 * np.cos(0.25 * np.pi), atol=1e-12)
