@@ -286,8 +286,8 @@ def main():
     if args.workload == "mhd_bundle" and args.e2e_steps > 0:
         e2e = _e2e_bundle(sf, torch, ins, npts, m, pad, best, args.e2e_steps, world, dist)
 
-    kname = {"fp64": "fast_kernel<EK_CROSS>", "split3": "split_kernel<EK_CROSS>", "split2": "split_kernel<EK_CROSS>",
-             "grid": "grid_kernel<OP_BUNDLE>"}[best]
+    kname = {"fp64": "fast_tf_kernel<EK_CROSS, 64>" if m == 64 else "fast_kernel<EK_CROSS>",
+             "split3": "split_kernel<EK_CROSS>", "split2": "split_kernel<EK_CROSS>", "grid": "grid_kernel<OP_BUNDLE>"}[best]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": results[best]["steps"],
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
