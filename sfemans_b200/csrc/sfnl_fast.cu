@@ -345,6 +345,8 @@ __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc) {
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Geometry of make_geo as constant expressions (the kernels specialise on m).
 __host__ __device__ constexpr int cg_qmin(int m) { return (3 * m - 2 + 3) / 4 < 1 ? 1 : (3 * m - 2 + 3) / 4; }
@@ -648,127 +650,138 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M
   }
 }
 
-// The FAST kernel with the third fold (class split, NT even, one pass: M = 64).  Per 8-point tile,
-// warp pair tau (= angle tile) half h: the odd class of half h on tile tau, and one part of the even
-// class of half h on tile min(tau, NT-1-tau) -- E0 for the first half of the tiles, E2 for the second.
-// A first exchange (X1) assembles the even class on every tile from the two parts; from there on the
-// tile is processed as in the class split (second exchange, program, analysis pre-fold).  The analysis
-// contracts the even output groups over the first half of the tiles with P(t) +- P(mirror).
-template <int EK, int M, int ADJ>
-__global__ void __launch_bounds__(384, EK == EK_CROSS ? 3 : 0) fast_tf_kernel(const FastArgs a) {
-  static_assert(third_fold(M), "third fold needs the specialised geometry");
-  constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO;
-  constexpr int NT = tf_NT(M), NH = NT / 2;
-  constexpr int KS_tot = tf_koff(M, 6), KT = 4 * KS_tot, NU_tot = tf_nuoff(M, 6), ASTEPS = tf_aoff(M, 6);
-  extern __shared__ double smem[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int g = lane >> 2, q = lane & 3;
-  const int64_t p0 = (int64_t)blockIdx.x * 8, p = p0 + g;
-  const bool valid = p < a.np;
-  const int b = blockIdx.y;
-  const double invN = 1.0 / (4.0 * 8.0 * NT), twoN = 2.0 * invN;
-  constexpr size_t prod_d = (size_t)NO * 4 * NT * 2 * 32;
-  double *ps = smem, *xc = smem + prod_d, *xs = smem;  // ps and xc overlay xs after the synthesis
+// ---------------------------------------------------------------------------
+// third-fold building blocks (class split, one angle tile per warp pair, M with tf_NT(M) even)
+// ---------------------------------------------------------------------------
+// Warp w of a CTA: angle tile tau = w / 2, half h = w % 2 (0: cosine classes, 1: sine classes).  It
+// accumulates the odd class of half h on tile tau and one part of the even class of half h on tile
+// min(tau, NT-1-tau): E0 (n = 0 mod 4) for the first half of the tiles, E2 (n = 2 mod 4) for the second.
+template <int M>
+struct TfGeo {
+  static constexpr int NT = tf_NT(M), NH = NT / 2, KS_tot = tf_koff(M, 6), KT = 4 * KS_tot;
+  static constexpr int NU_tot = tf_nuoff(M, 6), ASTEPS = tf_aoff(M, 6);
+};
+template <int NG>
+struct FieldSet {  // NG scalar fields: cos of mode n, point p at p[f][p + n*ldm[f]], sine np further
+  const double *p[NG];
+  int64_t ldm[NG];
+};
 
-  // ---- stage the tile's coefficients (rows in group order, otherwise as in fast_kernel) ----
-  {
-    const int pc = 2 * (threadIdx.x & 3), rstep = blockDim.x >> 2;
-    const bool v16 = a.vec16 && p0 + 8 <= a.np;
-    const bool pv0 = p0 + pc < a.np, pv1 = p0 + pc + 1 < a.np;
+// Stages the NG fields of the 8-point tile at p0 into xs [NG][KS_tot][4][8] (rows in group order:
+// CE0, CE2, CO, SE0, SE2, SO) with cp.async and commits one group.  Four consecutive threads copy one
+// row (two points each, one 16-byte copy when the row is 16-byte aligned).
+template <int M, int NG>
+__device__ __forceinline__ void tf_stage(double *xs, const FieldSet<NG> &fs, int64_t p0, int64_t np, bool vec16) {
+  constexpr int KS_tot = TfGeo<M>::KS_tot, KT = TfGeo<M>::KT;
+  const int pc = 2 * (threadIdx.x & 3), rstep = blockDim.x >> 2;
+  const bool v16 = vec16 && p0 + 8 <= np;
+  const bool pv0 = p0 + pc < np, pv1 = p0 + pc + 1 < np;
 #pragma unroll
-    for (int f = 0; f < NI; ++f) {
-      const double *base = a.in[f] + (int64_t)b * a.in_bs[f] + p0 + pc;
-      const int64_t ldm = a.in_ldm[f];
-      double *xf = xs + (size_t)f * KS_tot * 32 + pc;
-      for (int r = threadIdx.x >> 2; r < KT; r += rstep) {
-        const int gr = (r >= 4 * tf_koff(M, 1)) + (r >= 4 * tf_koff(M, 2)) + (r >= 4 * tf_koff(M, 3)) +
-                       (r >= 4 * tf_koff(M, 4)) + (r >= 4 * tf_koff(M, 5));
-        const int kg = gr == 0 ? 0 : gr == 1 ? tf_koff(M, 1) : gr == 2 ? tf_koff(M, 2) : gr == 3 ? tf_koff(M, 3)
-                     : gr == 4 ? tf_koff(M, 4) : tf_koff(M, 5);
-        const int keg = gr % 3 == 0 ? tf_ke(M, 0) : gr % 3 == 1 ? tf_ke(M, 1) : tf_ke(M, 2);
-        const int k = r - 4 * kg, n = tf_mode(gr, k);
-        double *dst = xf + (size_t)(r >> 2) * 32 + (r & 3) * 8;
-        const bool live = k < keg && !(gr == 3 && k == 0);  // the sine of mode 0 is ignored
-        const double *src = base + (int64_t)n * ldm + (gr >= 3 ? a.np : 0);
-        if (live && v16) {
-          cp_async16(dst, src);
-        } else {
-          if (live && pv0) cp_async8(dst, src); else dst[0] = 0.0;
-          if (live && pv1) cp_async8(dst + 1, src + 1); else dst[1] = 0.0;
-        }
+  for (int f = 0; f < NG; ++f) {
+    const double *base = fs.p[f] + p0 + pc;
+    const int64_t ldm = fs.ldm[f];
+    double *xf = xs + (size_t)f * KS_tot * 32 + pc;
+    for (int r = threadIdx.x >> 2; r < KT; r += rstep) {
+      const int gr = (r >= 4 * tf_koff(M, 1)) + (r >= 4 * tf_koff(M, 2)) + (r >= 4 * tf_koff(M, 3)) +
+                     (r >= 4 * tf_koff(M, 4)) + (r >= 4 * tf_koff(M, 5));
+      const int kg = gr == 0 ? 0 : gr == 1 ? tf_koff(M, 1) : gr == 2 ? tf_koff(M, 2) : gr == 3 ? tf_koff(M, 3)
+                   : gr == 4 ? tf_koff(M, 4) : tf_koff(M, 5);
+      const int keg = gr % 3 == 0 ? tf_ke(M, 0) : gr % 3 == 1 ? tf_ke(M, 1) : tf_ke(M, 2);
+      const int k = r - 4 * kg, n = tf_mode(gr, k);
+      double *dst = xf + (size_t)(r >> 2) * 32 + (r & 3) * 8;
+      const bool live = k < keg && !(gr == 3 && k == 0);  // the sine of mode 0 is ignored
+      const double *src = base + (int64_t)n * ldm + (gr >= 3 ? np : 0);
+      if (live && v16) {
+        cp_async16(dst, src);
+      } else {
+        if (live && pv0) cp_async8(dst, src); else dst[0] = 0.0;
+        if (live && pv1) cp_async8(dst + 1, src + 1); else dst[1] = 0.0;
       }
     }
   }
-  cp_async_wait_all();
-  __syncthreads();
+  cp_async_commit();
+}
 
-  // ---- synthesis: even part on the pair's first tile, odd class on the own tile ----
+// Synthesis of NG staged fields: the warp's even part and odd class.  ADJ: bit f set = field f is a
+// cotangent (synthesised with the analysis weights).
+template <int M, int NG, unsigned ADJ>
+__device__ __forceinline__ void tf_synth(const double *xs, const double *syn, double (&acc_e)[NG][2],
+                                         double (&acc_o)[NG][2]) {
+  constexpr int NT = TfGeo<M>::NT, NH = TfGeo<M>::NH, KS_tot = TfGeo<M>::KS_tot;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, q = lane & 3;
   const int tau = warp >> 1, half = warp & 1;
   const bool first = tau < NH;
   const int te_tile = first ? tau : NT - 1 - tau;
-  double acc_e[NI][2], acc_o[NI][2];
+  const double invN = 1.0 / (4.0 * 8.0 * NT), twoN = 2.0 * invN;
 #pragma unroll
-  for (int f = 0; f < NI; ++f) acc_e[f][0] = acc_e[f][1] = acc_o[f][0] = acc_o[f][1] = 0.0;
-  {
-    const int ge = 3 * half + (first ? 0 : 1);
-    const int koff_e = ge == 0 ? tf_koff(M, 0) : ge == 1 ? tf_koff(M, 1) : ge == 3 ? tf_koff(M, 3) : tf_koff(M, 4);
-    const int ks_e = (ge % 3 == 0) ? tf_KS(M, 0) : tf_KS(M, 1);
-    const int koff_o = half ? tf_koff(M, 5) : tf_koff(M, 2);
-    const double *xs_l = xs + (lane & 3) * 8 + (lane >> 2);
-    const double *syn_e = a.syn + (size_t)te_tile * 32 + lane, *syn_o = a.syn + (size_t)tau * 32 + lane;
-    constexpr int KSE = tf_KS(M, 0) > tf_KS(M, 1) ? tf_KS(M, 0) : tf_KS(M, 1);
+  for (int f = 0; f < NG; ++f) acc_e[f][0] = acc_e[f][1] = acc_o[f][0] = acc_o[f][1] = 0.0;
+  const int ge = 3 * half + (first ? 0 : 1);
+  const int koff_e = ge == 0 ? tf_koff(M, 0) : ge == 1 ? tf_koff(M, 1) : ge == 3 ? tf_koff(M, 3) : tf_koff(M, 4);
+  const int ks_e = (ge % 3 == 0) ? tf_KS(M, 0) : tf_KS(M, 1);
+  const int koff_o = half ? tf_koff(M, 5) : tf_koff(M, 2);
+  const double *xs_l = xs + (lane & 3) * 8 + (lane >> 2);
+  const double *syn_e = syn + (size_t)te_tile * 32 + lane, *syn_o = syn + (size_t)tau * 32 + lane;
+  constexpr int KSE = tf_KS(M, 0) > tf_KS(M, 1) ? tf_KS(M, 0) : tf_KS(M, 1);
 #pragma unroll
-    for (int s = 0; s < KSE; ++s) {
-      if (s >= ks_e) break;
-      const double bv = __ldg(syn_e + (size_t)(koff_e + s) * NT * 32);
-      const double *xa = xs_l + (size_t)(koff_e + s) * 32;
-      double av[NI];
+  for (int s = 0; s < KSE; ++s) {
+    if (s >= ks_e) break;
+    const double bv = __ldg(syn_e + (size_t)(koff_e + s) * NT * 32);
+    const double *xa = xs_l + (size_t)(koff_e + s) * 32;
+    double av[NG];
 #pragma unroll
-      for (int f = 0; f < NI; ++f) av[f] = xa[(size_t)f * KS_tot * 32];
-      if constexpr (ADJ != 0) {
-        const double wn = (s == 0 && q == 0 && ge % 3 == 0) ? invN : twoN;  // n == 0 only there
+    for (int f = 0; f < NG; ++f) av[f] = xa[(size_t)f * KS_tot * 32];
+    if constexpr (ADJ != 0) {
+      const double wn = (s == 0 && q == 0 && ge % 3 == 0) ? invN : twoN;  // n == 0 only there
 #pragma unroll
-        for (int f = 0; f < NI; ++f)
-          if ((ADJ == 1 && f < 3) || (ADJ == 2 && f >= 3)) av[f] *= wn;
-      }
-#pragma unroll
-      for (int f = 0; f < NI; ++f) dmma(acc_e[f], av[f], bv);
+      for (int f = 0; f < NG; ++f)
+        if ((ADJ >> f) & 1u) av[f] *= wn;
     }
 #pragma unroll
-    for (int s = 0; s < tf_KS(M, 2); ++s) {
-      const double bv = __ldg(syn_o + (size_t)(koff_o + s) * NT * 32);
-      const double *xa = xs_l + (size_t)(koff_o + s) * 32;
-      double av[NI];
-#pragma unroll
-      for (int f = 0; f < NI; ++f) av[f] = xa[(size_t)f * KS_tot * 32];
-      if constexpr (ADJ != 0) {
-#pragma unroll
-        for (int f = 0; f < NI; ++f)
-          if ((ADJ == 1 && f < 3) || (ADJ == 2 && f >= 3)) av[f] *= twoN;
-      }
-#pragma unroll
-      for (int f = 0; f < NI; ++f) dmma(acc_o[f], av[f], bv);
-    }
+    for (int f = 0; f < NG; ++f) dmma(acc_e[f], av[f], bv);
   }
-  __syncthreads();  // every warp has read its last coefficient: xc and ps may overwrite xs
-
-  // ---- first exchange: the even class on the own tile from the two parts ----
-  // X1[tau][half][f][e][32] holds the part each warp computed (on tile te_tile).  A first-half tile
-  // adds its partner's part at the same lane; a second-half tile takes both parts at the mirror lane
-  // (lane ^ 3) and parity (1 - e): CE = E0 - E2, SE = S2 - S0.
-  double acc[NI][2][2];  // [f][even, odd class][e], as in the class split
-  {
-    double *x1 = xc + (size_t)((tau * 2 + half) * NI) * 64 + lane;
 #pragma unroll
-    for (int f = 0; f < NI; ++f) {
+  for (int s = 0; s < tf_KS(M, 2); ++s) {
+    const double bv = __ldg(syn_o + (size_t)(koff_o + s) * NT * 32);
+    const double *xa = xs_l + (size_t)(koff_o + s) * 32;
+    double av[NG];
+#pragma unroll
+    for (int f = 0; f < NG; ++f) av[f] = xa[(size_t)f * KS_tot * 32];
+    if constexpr (ADJ != 0) {
+#pragma unroll
+      for (int f = 0; f < NG; ++f)
+        if ((ADJ >> f) & 1u) av[f] *= twoN;
+    }
+#pragma unroll
+    for (int f = 0; f < NG; ++f) dmma(acc_o[f], av[f], bv);
+  }
+}
+
+// Both exchanges (call with every thread, after a barrier that ends the reads of whatever xc overlays):
+// X1 assembles the even class on the warp's own tile from the two parts (a first-half tile adds its
+// partner's part at the same lane; a second-half tile takes both parts at the mirror lane (lane ^ 3) and
+// parity 1 - e: CE = E0 - E2, SE = S2 - S0); X2 swaps half of the folded sums (A = CE+CO, B = CE-CO against
+// C = SE+SO, D = SO-SE) with the other half, so that half e ends with the four quadrant values
+// v[r][f] of its angles of parity e.  xc holds 2 * NT * NG * 64 doubles.  Returns after the X2 reads.
+template <int M, int NG>
+__device__ __forceinline__ void tf_fold(const double (&acc_e)[NG][2], const double (&acc_o)[NG][2], double *xc,
+                                        double (&v)[4][NG]) {
+  constexpr int NT = TfGeo<M>::NT, NH = TfGeo<M>::NH;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tau = warp >> 1, half = warp & 1;
+  const bool first = tau < NH;
+  double acc[NG][2][2];  // [f][even, odd class][e]
+  {
+    double *x1 = xc + (size_t)((tau * 2 + half) * NG) * 64 + lane;
+#pragma unroll
+    for (int f = 0; f < NG; ++f) {
       x1[(f * 2 + 0) * 32] = acc_e[f][0];
       x1[(f * 2 + 1) * 32] = acc_e[f][1];
     }
     __syncthreads();
-    const double *own = xc + (size_t)((tau * 2 + half) * NI) * 64;
-    const double *mate = xc + (size_t)(((NT - 1 - tau) * 2 + half) * NI) * 64;
+    const double *own = xc + (size_t)((tau * 2 + half) * NG) * 64;
+    const double *mate = xc + (size_t)(((NT - 1 - tau) * 2 + half) * NG) * 64;
 #pragma unroll
-    for (int f = 0; f < NI; ++f)
+    for (int f = 0; f < NG; ++f)
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         double ev;
@@ -782,59 +795,74 @@ __global__ void __launch_bounds__(384, EK == EK_CROSS ? 3 : 0) fast_tf_kernel(co
         acc[f][0][e] = ev;
         acc[f][1][e] = acc_o[f][e];
       }
-    __syncthreads();  // X1 is read: the second exchange reuses xc
+    __syncthreads();  // X1 is read: X2 reuses xc
   }
-
-  // ---- second exchange, program, analysis pre-fold (as in the class split) ----
-  {
-    const int t = tau;
-    auto pair_sums = [&](int f, int e, double &X, double &Y) {
-      const double lo = e ? acc[f][0][1] : acc[f][0][0], hi = e ? acc[f][1][1] : acc[f][1][0];
-      X = lo + hi;
-      Y = half ? hi - lo : lo - hi;
-    };
-    double *xw = xc + (size_t)tau * 2 * NI * 64 + lane;  // [writer half][f][X, Y][32]
+  auto pair_sums = [&](int f, int e, double &X, double &Y) {
+    const double lo = e ? acc[f][0][1] : acc[f][0][0], hi = e ? acc[f][1][1] : acc[f][1][0];
+    X = lo + hi;
+    Y = half ? hi - lo : lo - hi;
+  };
+  double *xw = xc + (size_t)tau * 2 * NG * 64 + lane;  // [writer half][f][X, Y][32]
 #pragma unroll
-    for (int f = 0; f < NI; ++f) {
-      double X, Y;
-      pair_sums(f, 1 - half, X, Y);
-      xw[((half * NI + f) * 2 + 0) * 32] = X;
-      xw[((half * NI + f) * 2 + 1) * 32] = Y;
-    }
-    __syncthreads();
-    const int e = half;
-    double v[4][NI];
-#pragma unroll
-    for (int f = 0; f < NI; ++f) {
-      double X, Y;
-      pair_sums(f, e, X, Y);
-      const double Xp = xw[(((1 - half) * NI + f) * 2 + 0) * 32], Yp = xw[(((1 - half) * NI + f) * 2 + 1) * 32];
-      const double A = half ? Xp : X, B = half ? Yp : Y, C = half ? X : Xp, D = half ? Y : Yp;
-      v[0][f] = A + C;  // theta
-      v[1][f] = B + D;  // pi - theta
-      v[2][f] = B - D;  // pi + theta
-      v[3][f] = A - C;  // 2 pi - theta
-    }
-    double gq[4][NO];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) EKDef<EK>::op(v[r], gq[r]);
-#pragma unroll
-    for (int o = 0; o < NO; ++o) {
-      const double s14 = gq[0][o] + gq[3][o], d14 = gq[0][o] - gq[3][o];
-      const double s23 = gq[1][o] + gq[2][o], d32 = gq[2][o] - gq[1][o];
-      double *dst = ps + ((size_t)((o * 4) * NT + t) * 2 + e) * 32 + lane;
-      const size_t cstride = (size_t)NT * 2 * 32;
-      dst[0] = s14 + s23;            // PE
-      dst[cstride] = s14 - s23;      // PO
-      dst[2 * cstride] = d14 + d32;  // QE
-      dst[3 * cstride] = d14 - d32;  // QO
-    }
+  for (int f = 0; f < NG; ++f) {
+    double X, Y;
+    pair_sums(f, 1 - half, X, Y);
+    xw[((half * NG + f) * 2 + 0) * 32] = X;
+    xw[((half * NG + f) * 2 + 1) * 32] = Y;
   }
   __syncthreads();
+  const int e = half;
+#pragma unroll
+  for (int f = 0; f < NG; ++f) {
+    double X, Y;
+    pair_sums(f, e, X, Y);
+    const double Xp = xw[(((1 - half) * NG + f) * 2 + 0) * 32], Yp = xw[(((1 - half) * NG + f) * 2 + 1) * 32];
+    const double A = half ? Xp : X, B = half ? Yp : Y, C = half ? X : Xp, D = half ? Y : Yp;
+    v[0][f] = A + C;  // theta
+    v[1][f] = B + D;  // pi - theta
+    v[2][f] = B - D;  // pi + theta
+    v[3][f] = A - C;  // 2 pi - theta
+  }
+}
 
-  // ---- analysis: output groups; the even ones over the first half of the tiles ----
-  const double *anav = a.ana + (size_t)(a.adj_out ? 1 : 0) * ASTEPS * 32 + lane;
-  const int NW = blockDim.x >> 5;
+// Analysis pre-fold of NO program outputs gq[quadrant][o] at the warp's angles (tile tau, parity half)
+// into ps slots slot0 .. slot0+NO-1 ([slot][class][NT][2][32]).
+template <int M, int NO>
+__device__ __forceinline__ void tf_prefold(const double (&gq)[4][NO], double *ps, int slot0) {
+  constexpr int NT = TfGeo<M>::NT;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int t = warp >> 1, e = warp & 1;
+#pragma unroll
+  for (int o = 0; o < NO; ++o) {
+    const double s14 = gq[0][o] + gq[3][o], d14 = gq[0][o] - gq[3][o];
+    const double s23 = gq[1][o] + gq[2][o], d32 = gq[2][o] - gq[1][o];
+    double *dst = ps + ((size_t)(((slot0 + o) * 4) * NT + t) * 2 + e) * 32 + lane;
+    const size_t cstride = (size_t)NT * 2 * 32;
+    dst[0] = s14 + s23;            // PE
+    dst[cstride] = s14 - s23;      // PO
+    dst[2 * cstride] = d14 + d32;  // QE
+    dst[3 * cstride] = d14 - d32;  // QO
+  }
+}
+
+template <int NO>
+struct OutSet {  // NO output fields: cos of mode n, point p at p[o][p*ps + n*ldm[o]], sine np*ps further
+  double *p[NO];
+  int64_t ldm[NO];
+};
+
+// Analysis of ps slots 0..NO-1 into the outputs (every warp, output tiles cu = warp, warp + NW, ...): the
+// even output groups over the first half of the tiles with P(t) +- P(mirror).  ana: the analysis table
+// variant (weights or not); accumulate: add to the outputs.
+template <int M, int NO>
+__device__ __forceinline__ void tf_analysis(const double *ps, const double *ana, const OutSet<NO> &os, int64_t p0,
+                                            int64_t np, int64_t out_ps, bool accumulate) {
+  constexpr int NT = TfGeo<M>::NT, NU_tot = TfGeo<M>::NU_tot;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, NW = blockDim.x >> 5;
+  const int q = lane & 3;
+  const int64_t p = p0 + (lane >> 2);
+  const bool valid = p < np;
+  const double *anav = ana + lane;
   for (int cu = warp; cu < NU_tot; cu += NW) {
     const int gr = (cu >= tf_nuoff(M, 1)) + (cu >= tf_nuoff(M, 2)) + (cu >= tf_nuoff(M, 3)) +
                    (cu >= tf_nuoff(M, 4)) + (cu >= tf_nuoff(M, 5));
@@ -885,16 +913,158 @@ __global__ void __launch_bounds__(384, EK == EK_CROSS ? 3 : 0) fast_tf_kernel(co
       const int n = tf_mode(gr, kk);
 #pragma unroll
       for (int o = 0; o < NO; ++o) {
-        double *dst = a.out[o] + (int64_t)b * a.out_bs[o] + p * a.out_ps + (int64_t)n * a.out_ldm[o] +
-                      (gr >= 3 ? a.np * a.out_ps : 0);
+        double *dst = os.p[o] + p * out_ps + (int64_t)n * os.ldm[o] + (gr >= 3 ? np * out_ps : 0);
         const double v = (gr >= 3 && n == 0) ? 0.0 : y[o][h];
-        if (a.accumulate)
+        if (accumulate)
           *dst += v;
         else
           *dst = v;
       }
     }
   }
+}
+
+// The FAST kernel with the third fold (one elementary program, class split, NT even: M = 64).
+template <int EK, int M, int ADJ>
+__global__ void __launch_bounds__(384, EK == EK_CROSS ? 3 : 0) fast_tf_kernel(const FastArgs a) {
+  static_assert(third_fold(M), "third fold needs the specialised geometry");
+  constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO, NT = TfGeo<M>::NT;
+  constexpr unsigned ADJMASK = ADJ == 1 ? 0x07u : ADJ == 2 ? 0x38u : 0u;
+  extern __shared__ double smem[];
+  const int b = blockIdx.y;
+  const int64_t p0 = (int64_t)blockIdx.x * 8;
+  constexpr size_t prod_d = (size_t)NO * 4 * NT * 2 * 32;
+  double *ps = smem, *xc = smem + prod_d, *xs = smem;  // ps and xc overlay xs after the synthesis
+  FieldSet<NI> fs;
+#pragma unroll
+  for (int f = 0; f < NI; ++f) {
+    fs.p[f] = a.in[f] + (int64_t)b * a.in_bs[f];
+    fs.ldm[f] = a.in_ldm[f];
+  }
+  tf_stage<M, NI>(xs, fs, p0, a.np, a.vec16);
+  cp_async_wait_0();
+  __syncthreads();
+  double acc_e[NI][2], acc_o[NI][2];
+  tf_synth<M, NI, ADJMASK>(xs, a.syn, acc_e, acc_o);
+  __syncthreads();  // every warp has read its last coefficient: xc and ps may overwrite xs
+  double v[4][NI];
+  tf_fold<M, NI>(acc_e, acc_o, xc, v);
+  double gq[4][NO];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) EKDef<EK>::op(v[r], gq[r]);
+  tf_prefold<M, NO>(gq, ps, 0);
+  __syncthreads();
+  OutSet<NO> os;
+#pragma unroll
+  for (int o = 0; o < NO; ++o) {
+    os.p[o] = a.out[o] + (int64_t)b * a.out_bs[o];
+    os.ldm[o] = a.out_ldm[o];
+  }
+  tf_analysis<M, NO>(ps, a.ana + (size_t)(a.adj_out ? 1 : 0) * TfGeo<M>::ASTEPS * 32, os, p0, a.np, a.out_ps,
+                     a.accumulate != 0);
+}
+
+// The MHD bundle (u x w, u x b, j x b, u . gradT) in one launch with the third fold (M = 64): the five
+// vector operands are staged and synthesised one at a time (u, w, gradT, b, j), so u and b are
+// transformed once instead of three and two times (15 field transforms instead of 24); u's and b's
+// quadrant values stay in registers while their partners are synthesised.  Each operand's copies are
+// issued during the previous operand's exchanges; the outputs are analysed in three rounds (u x w;
+// u x b with u . gradT; j x b) through a four-output product buffer.
+struct BundleArgs {
+  const double *in[15];  // u 0-2, w 3-5, b 6-8, j 9-11, gradT 12-14
+  double *out[10];       // u x w 0-2, u x b 3-5, j x b 6-8, u . gradT 9
+  int64_t in_ldm[15], out_ldm[10];
+  int64_t np;
+  int vec16;
+  const double *syn, *ana;
+};
+
+template <int M>
+__global__ void __launch_bounds__(384, 2) fast_bundle_tf_kernel(const BundleArgs a) {
+  static_assert(third_fold(M), "third fold needs the specialised geometry");
+  constexpr int NT = TfGeo<M>::NT, KS_tot = TfGeo<M>::KS_tot;
+  extern __shared__ double smem[];
+  double *xs = smem;                                  // one operand: 3 x KS_tot x 32
+  double *xc = xs + (size_t)3 * KS_tot * 32;          // exchanges: 2 x NT x 3 x 64
+  double *ps = xc + (size_t)2 * NT * 3 * 64;          // products: 4 slots x 4 x NT x 2 x 32
+  const int64_t p0 = (int64_t)blockIdx.x * 8;
+  auto fields = [&](int first) {
+    FieldSet<3> fs;
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      fs.p[f] = a.in[first + f];
+      fs.ldm[f] = a.in_ldm[first + f];
+    }
+    return fs;
+  };
+  auto outs3 = [&](int first) {
+    OutSet<3> os;
+#pragma unroll
+    for (int o = 0; o < 3; ++o) {
+      os.p[o] = a.out[first + o];
+      os.ldm[o] = a.out_ldm[first + o];
+    }
+    return os;
+  };
+  // one operand: wait for its copies, synthesise, issue the next operand's copies, fold
+  auto operand = [&](int next_first, double (&v)[4][3]) {
+    cp_async_wait_0();
+    __syncthreads();
+    double acc_e[3][2], acc_o[3][2];
+    tf_synth<M, 3, 0u>(xs, a.syn, acc_e, acc_o);
+    __syncthreads();  // xs is read
+    if (next_first >= 0) tf_stage<M, 3>(xs, fields(next_first), p0, a.np, a.vec16 != 0);
+    tf_fold<M, 3>(acc_e, acc_o, xc, v);
+  };
+  double vu[4][3], vb[4][3], vx[4][3];
+  tf_stage<M, 3>(xs, fields(0), p0, a.np, a.vec16 != 0);  // u
+  operand(3, vu);                                        // u; next w
+  operand(12, vx);                                       // w; next gradT
+  {
+    double gq[4][3];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) cross3(vu[r], vx[r], gq[r]);
+    tf_prefold<M, 3>(gq, ps, 0);
+  }
+  __syncthreads();
+  tf_analysis<M, 3>(ps, a.ana, outs3(0), p0, a.np, 1, false);  // u x w
+  operand(6, vx);                                              // gradT; next b
+  {
+    double gq[4][1];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) gq[r][0] = vu[r][0] * vx[r][0] + vu[r][1] * vx[r][1] + vu[r][2] * vx[r][2];
+    __syncthreads();  // the u x w analysis has read ps
+    tf_prefold<M, 1>(gq, ps, 3);
+  }
+  operand(9, vb);  // b; next j
+  {
+    double gq[4][3];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) cross3(vu[r], vb[r], gq[r]);
+    tf_prefold<M, 3>(gq, ps, 0);
+  }
+  __syncthreads();
+  {
+    OutSet<4> os;
+#pragma unroll
+    for (int o = 0; o < 3; ++o) {
+      os.p[o] = a.out[3 + o];
+      os.ldm[o] = a.out_ldm[3 + o];
+    }
+    os.p[3] = a.out[9];
+    os.ldm[3] = a.out_ldm[9];
+    tf_analysis<M, 4>(ps, a.ana, os, p0, a.np, 1, false);  // u x b, u . gradT
+  }
+  operand(-1, vx);  // j
+  {
+    double gq[4][3];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) cross3(vx[r], vb[r], gq[r]);
+    __syncthreads();  // the previous analysis has read ps
+    tf_prefold<M, 3>(gq, ps, 0);
+  }
+  __syncthreads();
+  tf_analysis<M, 3>(ps, a.ana, outs3(6), p0, a.np, 1, false);  // j x b
 }
 
 template <int EK, int M, int ADJ>
@@ -1021,10 +1191,45 @@ bool fast_supported(int op, int m, int N) {
   return g.N == N && fast_smem_bytes(op == OP_TENSOR ? EK_TENSOR : EK_CROSS, g.NT, 4 * g.KS_tot, true) <= 200 * 1024;
 }
 
+namespace {
+// The MHD bundle in one third-fold launch (m = 64, one batch entry, plain layouts).
+int launch_bundle_tf(const ProgArgs &a, cudaStream_t st) {
+  constexpr int M = 64;
+  BundleArgs ba;
+  std::memset(&ba, 0, sizeof(ba));
+  int v16 = (a.np & 1) ? 0 : 1;
+  for (int f = 0; f < 15; ++f) {
+    ba.in[f] = a.in[f];
+    ba.in_ldm[f] = a.in_ldm[f];
+    if ((reinterpret_cast<uintptr_t>(a.in[f]) & 15) || (a.in_ldm[f] & 1)) v16 = 0;
+  }
+  for (int o = 0; o < 10; ++o) {
+    ba.out[o] = a.out[o];
+    ba.out_ldm[o] = a.out_ldm[o];
+  }
+  ba.np = a.np;
+  ba.vec16 = v16;
+  Tables T;
+  if (int rc = get_tf_tables(make_geo(M), &T)) return rc;
+  ba.syn = T.syn;
+  ba.ana = T.ana;  // variant 0: with the analysis weights
+  constexpr int NT = TfGeo<M>::NT, KS_tot = TfGeo<M>::KS_tot;
+  const size_t smem = sizeof(double) * ((size_t)3 * KS_tot * 32 + (size_t)2 * NT * 3 * 64 + (size_t)4 * 4 * NT * 2 * 32);
+  auto kern = fast_bundle_tf_kernel<M>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (fast bundle)");
+  const int64_t tiles = (a.np + 7) / 8;
+  if (tiles > 0x7fffffff) return set_error(SFNL_ERR_UNSUPPORTED, "np too large");
+  kern<<<(unsigned)tiles, 2 * NT * 32, smem, st>>>(ba);
+  return check_launch("fast form (bundle)");
+}
+}  // namespace
+
 int launch_fast(const ProgArgs &a, cudaStream_t st) {
   if (a.np == 0) return SFNL_OK;
   const Geo g = make_geo(a.m);
   if (g.N != a.N) return set_error(SFNL_ERR_ARG, "FAST form: unexpected grid length");
+  if (a.op == OP_BUNDLE && a.m == 64 && a.batch == 1 && a.out_ps == 1) return launch_bundle_tf(a, st);
   Tables T;
   int rc = get_tables(g, &T);
   if (rc) return rc;

@@ -34,7 +34,11 @@ def _sync():
     torch.cuda.synchronize()
 
 
-@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLD, "*.npz"))))
+PRODUCT_FIXTURES = sorted(p for p in glob.glob(os.path.join(GOLD, "*.npz"))
+                          if not os.path.basename(p).startswith(("real_", "maxvel_")))  # synthesis: test_gpu_synthesis
+
+
+@pytest.mark.parametrize("path", PRODUCT_FIXTURES)
 @pytest.mark.parametrize("algo", ALGOS)
 def test_golden_fixtures(path, algo):
     z = np.load(path)
@@ -107,7 +111,7 @@ def test_reference_signature_on_device_tensors():
     assert R.rel_l2(host(out), R.c_oracle("cross", V1, V2, 12)) <= FP64_TOL
 
 
-@pytest.mark.parametrize("npts,m", [(200, 8), (65, 21)])
+@pytest.mark.parametrize("npts,m", [(200, 8), (65, 21), (61, 64), (200, 64)])
 @pytest.mark.parametrize("algo", ALGOS)
 def test_mhd_bundle(npts, m, algo):
     pad = 3 * m // 2
@@ -119,11 +123,11 @@ def test_mhd_bundle(npts, m, algo):
         assert R.rel_l2(host(o), r) <= FP64_TOL
 
 
-def test_host_bundle_entry_point():
+@pytest.mark.parametrize("npts,m", [(90, 10), (3001, 64)])
+def test_host_bundle_entry_point(npts, m):
     import ctypes
 
-    npts, m = 90, 10
-    pad = 15
+    pad = 3 * m // 2
     f = [R.synthetic_field(npts, 6, m, 0.1, 400 + i) for i in range(5)]
     outs = [np.zeros((npts, 6, m), order="F") for _ in range(3)] + [np.zeros((npts, 2, m), order="F")]
     P = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
