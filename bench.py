@@ -223,8 +223,10 @@ def main():
 
     forms = {"fp64": dict(algo=sf.ALGO_FAST), "split3": dict(split=sf.SPLIT_BF16X3),
              "split2": dict(split=sf.SPLIT_BF16X2), "grid": dict(algo=sf.ALGO_GRID)}
-    launches = {"fp64": 4, "split3": 4, "split2": 4, "grid": 1} if args.workload == "mhd_bundle" else \
-        {"fp64": 1, "split3": 1, "split2": 1, "grid": 1}
+    # kernel launches per step: the bundle is one launch in every form except FAST at m != 64 (four
+    # elementary launches); the other workloads are one launch
+    launches = {"fp64": 1 if m == 64 else 4, "split3": 1, "split2": 1, "grid": 1} if args.workload == "mhd_bundle" \
+        else {"fp64": 1, "split3": 1, "split2": 1, "grid": 1}
     # every form is timed (the others after the reported one, on fewer steps); the line reports --form,
     # or with --form auto the fastest form that meets its accuracy bar
     order = ["fp64", "split3", "split2", "grid"]
@@ -275,10 +277,16 @@ def main():
     ms = results[best]["ms_per_step"]
     value = results[best]["value"]
 
-    # dominant kernel: the elementary cross product of the chosen form, timed per launch at full size
-    dom_ms = _time_steps(lambda: sf.product(sf.OP_CROSS, ins[0], ins[1], out=outs[0], m_max_pad=pad, **forms[best]),
-                         args.steps, args.warmup, stream, world, dist, local)[0] if best != "grid" or args.workload != "mhd_bundle" else ms
-    dom_bytes = 8.0 * m * ((12 + 6) if dom_ms != ms or args.workload != "mhd_bundle" else 50) * npts
+    # dominant kernel: the step's own launch when the step is one launch (bytes: all 50 slots of the
+    # bundle); otherwise the elementary cross product of the chosen form, timed per launch at full size
+    single = args.workload != "mhd_bundle" or launches[best] == 1
+    if single:
+        dom_ms = ms
+        dom_bytes = 8.0 * m * (50 if args.workload == "mhd_bundle" else 18) * npts
+    else:
+        dom_ms = _time_steps(lambda: sf.product(sf.OP_CROSS, ins[0], ins[1], out=outs[0], m_max_pad=pad, **forms[best]),
+                             args.steps, args.warmup, stream, world, dist, local)[0]
+        dom_bytes = 8.0 * m * 18 * npts
     hbm, _, peak_kind = _peaks()
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
 
@@ -286,8 +294,12 @@ def main():
     if args.workload == "mhd_bundle" and args.e2e_steps > 0:
         e2e = _e2e_bundle(sf, torch, ins, npts, m, pad, best, args.e2e_steps, world, dist)
 
-    kname = {"fp64": "fast_tf_kernel<EK_CROSS, 64>" if m == 64 else "fast_kernel<EK_CROSS>",
-             "split3": "split_kernel<EK_CROSS>", "split2": "split_kernel<EK_CROSS>", "grid": "grid_kernel<OP_BUNDLE>"}[best]
+    if args.workload == "mhd_bundle":
+        kname = {"fp64": "fast_bundle_tf_kernel<64>" if m == 64 else "fast_kernel<EK_CROSS>",
+                 "split3": "split_kernel<PR_BUNDLE>", "split2": "split_kernel<PR_BUNDLE>", "grid": "grid_kernel<OP_BUNDLE>"}[best]
+    else:
+        kname = {"fp64": "fast_kernel<EK_CROSS>", "split3": "split_kernel<PR_CROSS>", "split2": "split_kernel<PR_CROSS>",
+                 "grid": "grid_kernel<OP_CROSS>"}[best]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": results[best]["steps"],
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
