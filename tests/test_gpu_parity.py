@@ -218,3 +218,57 @@ def test_finite_check_mode():
         assert e.value.code == -6
     finally:
         sf.set_check_finite(False)
+
+
+LARGE = [(37, 100, 150), (20, 128, 192), (9, 256, 384)]
+
+
+@pytest.mark.parametrize("op", [0, 1, 2])
+@pytest.mark.parametrize("npts,m,pad", LARGE)
+@pytest.mark.parametrize("algo", [sf.ALGO_AUTO, sf.ALGO_FAST])
+def test_large_m_products(op, npts, m, pad, algo):
+    # m beyond what one CTA holds: the two-kernel FAST form (synthesis to grid values, then program + analysis)
+    name = ("cross", "dot", "prod")[op]
+    nsl = 2 if op == 2 else 6
+    V1 = R.synthetic_field(npts, nsl, m, 0.05, 900 + m)
+    V2 = R.synthetic_field(npts, nsl, m, 0.05, 950 + m)
+    out = sf.product(op, dev(V1), dev(V2), m_max_pad=pad, algo=algo)
+    _sync()
+    assert R.rel_l2(host(out), R.c_oracle(name, V1, V2, pad)) <= FP64_TOL
+
+
+@pytest.mark.parametrize("kind", ["svect", "tensor"])
+def test_large_m_siblings(kind):
+    npts, m, pad = 11, 200, 300
+    _, n1, n2, _ = sf.KINDS[kind]
+    V1 = R.synthetic_field(npts, n1, m, 0.05, 31)
+    V2 = R.synthetic_field(npts, n2, m, 0.05, 32)
+    out = sf.product(sf.KINDS[kind][0], dev(V1), dev(V2), m_max_pad=pad, algo=sf.ALGO_FAST)
+    _sync()
+    assert R.rel_l2(host(out), R.c_oracle(kind, V1, V2, pad)) <= FP64_TOL
+
+
+def test_large_m_linearised_batched():
+    # the 16-tangent linearised configuration's shape (m = 256), on few points and 3 tangents
+    npts, m, k, pad = 13, 256, 3, 384
+    u, w, b = (R.synthetic_field(npts, 6, m, 0.05, 70 + i) for i in range(3))
+    v = _batched(npts, 18, m, k, 0.05, 80)
+    c = _batched(npts, 12, m, k, 0.05, 90)
+    jv = host(sf.mhd_jvp(dev(u), dev(w), dev(b), dev(v), m_max_pad=pad))
+    jtc = host(sf.mhd_vjp(dev(u), dev(w), dev(b), dev(c), m_max_pad=pad))
+    for t in range(k):
+        du, dw, db = (np.asfortranarray(v[:, 6 * i:6 * i + 6, :, t]) for i in range(3))
+        assert R.rel_l2(jv[:, :6, :, t], R.cross_jvp(u, w, du, dw, pad)) <= FP64_TOL
+        assert R.rel_l2(jv[:, 6:, :, t], R.cross_jvp(u, b, du, db, pad)) <= FP64_TOL
+        lhs = np.dot(jv[..., t].ravel(), c[..., t].ravel())
+        rhs = np.dot(v[..., t].ravel(), jtc[..., t].ravel())
+        assert abs(lhs - rhs) <= 1e-12 * np.linalg.norm(jv[..., t]) * np.linalg.norm(c[..., t])
+
+
+def test_large_m_point_chunks():
+    # more points than one workspace chunk of grid values holds (about 29k points at m = 256)
+    npts, m, pad = 70_001, 256, 384
+    V1 = R.synthetic_field(npts, 6, m, 0.05, 41)
+    V2 = R.synthetic_field(npts, 6, m, 0.05, 42)
+    out = host(sf.product(0, dev(V1), dev(V2), m_max_pad=pad, algo=sf.ALGO_FAST))
+    assert R.rel_l2(out, R.fft_par("cross", V1, V2, pad, workers=8)) <= FP64_TOL
