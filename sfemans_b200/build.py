@@ -10,12 +10,14 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libsfemans_nl.so")
-SOURCES = ["sfnl_capi.cu", "sfnl_grid.cu", "sfnl_fast.cu", "sfnl_split.cu", "sfnl_synth.cu", "sfnl_gauss.cu"]
+SOURCES = ["sfnl_capi.cu", "sfnl_grid.cu", "sfnl_fast.cu", "sfnl_large.cu", "sfnl_split.cu", "sfnl_synth.cu",
+           "sfnl_gauss.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -26,7 +28,7 @@ def nvcc() -> str:
 
 def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(OUT_DIR, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for s in SOURCES:
         src = os.path.join(SRC, s)
         obj = os.path.join(OUT_DIR, s.replace(".cu", ".o"))
@@ -39,8 +41,12 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
                 cmd.insert(1, "-Xptxas=-v")
             if verbose:
                 print(" ".join(cmd))
-            subprocess.check_call(cmd)
+            cmds.append(cmd)
         objs.append(obj)
+    # the translation units are independent: compile them side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(subprocess.check_call, c) for c in cmds]:
+            f.result()
     if not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs]  # static cudart (nvcc default)
         if verbose:

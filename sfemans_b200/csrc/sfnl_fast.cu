@@ -43,6 +43,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "sfnl_fold.cuh"
 #include "sfnl_internal.h"
 #include "sfnl_ops.cuh"
 
@@ -50,53 +51,12 @@ namespace sfnl {
 
 namespace {
 
-// ---------------------------------------------------------------------------
-// geometry of the folded transforms
-// ---------------------------------------------------------------------------
-struct Geo {
-  int m, Q, N;   // modes, quarter angles, grid length
-  int NT;        // quarter-angle tiles of 8
-  int ke[4];     // modes per class (0 cos-even, 1 cos-odd, 2 sin-even, 3 sin-odd)
-  int KS[4];     // synthesis k-steps per class (modes padded to 4)
-  int NU[4];     // analysis output tiles per class (modes padded to 8)
-  int ks_off[4]; // prefix offsets
-  int nu_off[4];
-  int KS_tot, NU_tot;
-};
 
-Geo make_geo(int m) {
-  Geo g;
-  g.m = m;
-  int qmin = (3 * m - 2 + 3) / 4;
-  if (qmin < 1) qmin = 1;
-  g.Q = ((qmin + 7) / 8) * 8;
-  g.N = 4 * g.Q;
-  g.NT = g.Q / 8;
-  const int ev = (m + 1) / 2, od = m / 2;
-  const int cnt[4] = {ev, od, ev, od};
-  g.KS_tot = g.NU_tot = 0;
-  for (int c = 0; c < 4; ++c) {
-    g.ke[c] = cnt[c];
-    g.KS[c] = (cnt[c] + 3) / 4;
-    g.NU[c] = (cnt[c] + 7) / 8;
-    g.ks_off[c] = g.KS_tot;
-    g.nu_off[c] = g.NU_tot;
-    g.KS_tot += g.KS[c];
-    g.NU_tot += g.NU[c];
-  }
-  return g;
-}
-
-__host__ __device__ inline int class_mode(int c, int k) { return 2 * k + (c & 1); }
-
-// Device tables for one m: synthesis B fragments and two analysis variants.
-struct Tables {
-  double *syn = nullptr;   // [KS_tot][NT][32]
-  double *ana = nullptr;   // [2 variants][NU_tot][NT][2][32]
-};
 
 std::mutex g_tab_mu;
 std::map<std::pair<int, int>, Tables> g_tabs;  // (device, m) -> tables
+
+}  // namespace
 
 int get_tables(const Geo &g, Tables *out) {
   int dev = 0;
@@ -154,6 +114,8 @@ int get_tables(const Geo &g, Tables *out) {
   *out = T;
   return SFNL_OK;
 }
+
+namespace {
 
 // ---------------------------------------------------------------------------
 // third fold: the mirror symmetry theta -> pi/2 - theta of the quadrant grid
@@ -275,11 +237,6 @@ struct FastArgs {
   const double *syn, *ana;
 };
 
-__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d[0]), "+d"(d[1])
-               : "d"(a), "d"(b));
-}
 
 template <int EK>
 struct EKDef;
@@ -332,21 +289,6 @@ inline size_t fast_smem_bytes(int ek, int NT, int KT, bool cs) {
   return sizeof(double) * (NT <= 8 ? (prod + xch > coef ? prod + xch : coef) : prod + xch + coef);
 }
 
-__device__ __forceinline__ void cp_async8(void *smem_dst, const void *gsrc) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
-               "l"(gsrc)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
-               "l"(gsrc)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Geometry of make_geo as constant expressions (the kernels specialise on m).
 __host__ __device__ constexpr int cg_qmin(int m) { return (3 * m - 2 + 3) / 4 < 1 ? 1 : (3 * m - 2 + 3) / 4; }
@@ -357,8 +299,6 @@ __host__ __device__ constexpr int cg_NU(int m, int c) { return (cg_ke(m, c) + 7)
 __host__ __device__ constexpr int cg_ksoff(int m, int c) { return c == 0 ? 0 : cg_ksoff(m, c - 1) + cg_KS(m, c - 1); }
 __host__ __device__ constexpr int cg_nuoff(int m, int c) { return c == 0 ? 0 : cg_nuoff(m, c - 1) + cg_NU(m, c - 1); }
 
-// Element c of a 4-array without dynamic indexing (keeps the arrays in registers).
-__device__ __forceinline__ int sel4(const int (&v)[4], int c) { return c == 0 ? v[0] : c == 1 ? v[1] : c == 2 ? v[2] : v[3]; }
 
 // EK: elementary program; M: modes when specialised (0: any m, geometry at run time);
 // ADJ: 0 plain, 1 first operand (fields 0-2) a cotangent, 2 second operand (fields 3-5) a cotangent.
@@ -1182,369 +1122,10 @@ int decompose_program(int op, std::vector<Elem> &seq) {
   return SFNL_OK;
 }
 
-namespace {
-// ---------------------------------------------------------------------------
-// large m: the same folded transforms in two kernels
-// ---------------------------------------------------------------------------
-// Beyond m ~ 80 one CTA cannot hold an 8-point tile's coefficients of six fields and its folded
-// products at once (at m = 256: 196 KB and 147 KB), so the transforms are split at the grid values:
-//   large_syn_kernel  one CTA per (8-point tile, field): stages the field's 2m coefficient rows,
-//                     runs the four class contractions on every angle tile (the tiles of a warp
-//                     interleaved for independent DMMA chains), folds to the four quadrants and writes
-//                     the grid values in fragment order, G[field][tile][t][quadrant][e][32];
-//   large_prod_kernel one CTA per 8-point tile: for chunks of LCT angle tiles it reads the fields'
-//                     grid values (each lane its own fragment elements), evaluates the program and the
-//                     analysis pre-fold into shared memory, and every warp adds the chunk's k-steps to
-//                     the accumulators of its output tiles; the outputs are written at the end.
-// G lives in a per-(device, stream) workspace; the points are processed in chunks that bound it.
-constexpr int kLargeSynWarps = 8, kLargeProdWarps = 16, kLCT = 4;
-
-struct LargeArgs {
-  const double *in[6];
-  double *out[3];
-  int64_t in_ldm[6], out_ldm[3], in_bs[6], out_bs[3];
-  int64_t npts;     // points of this chunk (fields are offset to its first point)
-  int64_t in_sin;   // sine offset of the inputs (the arrays' np)
-  int64_t out_sin;  // sine offset of the outputs (np * point stride)
-  int64_t out_ps;   // point stride of the outputs
-  int NT, NU_tot, KS_tot;
-  int ks_off[4], KS[4], nu_off[4], ke[4];
-  unsigned adj_in;
-  int adj_out, accumulate, vec16, ni;
-  const double *syn, *ana;
-  double *G;  // [batch][field][tile][NT][8][32]
-  int64_t tiles;
-};
-
-template <int TPW>
-__global__ void __launch_bounds__(kLargeSynWarps * 32) large_syn_kernel(const LargeArgs a) {
-  extern __shared__ double xs[];  // [KS_tot][4][8] of one field
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, q = lane & 3;
-  const int f = blockIdx.y, b = blockIdx.z;
-  const int64_t tile = blockIdx.x, p0 = tile * 8;
-  const int NT = a.NT, KT = 4 * a.KS_tot;
-  const double invN = 1.0 / (4.0 * 8.0 * NT), twoN = 2.0 * invN;
-  const double *in_f = f == 0 ? a.in[0] : f == 1 ? a.in[1] : f == 2 ? a.in[2] : f == 3 ? a.in[3] : f == 4 ? a.in[4] : a.in[5];
-  const int64_t ldm = f == 0 ? a.in_ldm[0] : f == 1 ? a.in_ldm[1] : f == 2 ? a.in_ldm[2] : f == 3 ? a.in_ldm[3]
-                    : f == 4 ? a.in_ldm[4] : a.in_ldm[5];
-  const int64_t bs = f == 0 ? a.in_bs[0] : f == 1 ? a.in_bs[1] : f == 2 ? a.in_bs[2] : f == 3 ? a.in_bs[3]
-                   : f == 4 ? a.in_bs[4] : a.in_bs[5];
-  const bool cot = (a.adj_in >> f) & 1u;
-  int KS[4], KOFF[4], KE[4];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    KS[c] = a.KS[c];
-    KOFF[c] = a.ks_off[c];
-    KE[c] = a.ke[c];
-  }
-  {  // stage: four threads per row, 16-byte copies when aligned
-    const int pc = 2 * (threadIdx.x & 3), rstep = blockDim.x >> 2;
-    const bool v16 = a.vec16 && p0 + 8 <= a.npts;
-    const bool pv0 = p0 + pc < a.npts, pv1 = p0 + pc + 1 < a.npts;
-    const double *base = in_f + (int64_t)b * bs + p0 + pc;
-    for (int r = threadIdx.x >> 2; r < KT; r += rstep) {
-      const int c = (r >= 4 * KOFF[1]) + (r >= 4 * KOFF[2]) + (r >= 4 * KOFF[3]);
-      const int k = r - 4 * sel4(KOFF, c), n = class_mode(c, k);
-      double *dst = xs + (size_t)(r >> 2) * 32 + (r & 3) * 8 + pc;
-      const bool live = k < sel4(KE, c) && !(c == 2 && n == 0);  // the sine of mode 0 is ignored
-      const double *src = base + (int64_t)n * ldm + (c >= 2 ? a.in_sin : 0);
-      if (live && v16) {
-        cp_async16(dst, src);
-      } else {
-        if (live && pv0) cp_async8(dst, src); else dst[0] = 0.0;
-        if (live && pv1) cp_async8(dst + 1, src + 1); else dst[1] = 0.0;
-      }
-    }
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  double acc[TPW][4][2];
-#pragma unroll
-  for (int j = 0; j < TPW; ++j)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) acc[j][c][0] = acc[j][c][1] = 0.0;
-  const double *xs_l = xs + (lane & 3) * 8 + (lane >> 2);
-  int ks_max = KS[0];
-#pragma unroll
-  for (int c = 1; c < 4; ++c) ks_max = KS[c] > ks_max ? KS[c] : ks_max;
-  for (int s = 0; s < ks_max; ++s) {
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      if (s >= sel4(KS, c)) continue;
-      const int ks = sel4(KOFF, c) + s;
-      double av = xs_l[(size_t)ks * 32];
-      if (cot) av *= (s == 0 && q == 0 && (c & 1) == 0) ? invN : twoN;  // n == 0 only there
-      const double *bt = a.syn + (size_t)ks * NT * 32 + lane;
-#pragma unroll
-      for (int j = 0; j < TPW; ++j) {
-        const int t = warp + kLargeSynWarps * j;
-        if (t < NT) dmma(acc[j][c], av, __ldg(bt + (size_t)t * 32));
-      }
-    }
-  }
-  double *Gt = a.G + ((((int64_t)b * a.ni + f) * a.tiles + tile) * NT) * 256 + lane;
-#pragma unroll
-  for (int j = 0; j < TPW; ++j) {
-    const int t = warp + kLargeSynWarps * j;
-    if (t >= NT) continue;
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      const double A = acc[j][0][e] + acc[j][1][e], B = acc[j][0][e] - acc[j][1][e];
-      const double C = acc[j][2][e] + acc[j][3][e], D = acc[j][3][e] - acc[j][2][e];
-      double *g = Gt + (size_t)t * 256 + e * 32;
-      g[0 * 64] = A + C;  // theta
-      g[1 * 64] = B + D;  // pi - theta
-      g[2 * 64] = B - D;  // pi + theta
-      g[3 * 64] = A - C;  // 2 pi - theta
-    }
-  }
-}
-
-template <int EK, int CPW>
-__global__ void __launch_bounds__(kLargeProdWarps * 32) large_prod_kernel(const LargeArgs a) {
-  constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO;
-  extern __shared__ double pc_s[];  // [NO][4][LCT][2][32]
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, q = lane & 3;
-  const int b = blockIdx.y;
-  const int64_t tile = blockIdx.x, p = tile * 8 + (lane >> 2);
-  const int NT = a.NT;
-  const double invN = 1.0 / (4.0 * 8.0 * NT), twoN = 2.0 * invN;
-  double y[CPW][NO][2];
-#pragma unroll
-  for (int j = 0; j < CPW; ++j)
-#pragma unroll
-    for (int o = 0; o < NO; ++o) y[j][o][0] = y[j][o][1] = 0.0;
-  const double *Gb = a.G + (((int64_t)b * a.ni) * a.tiles + tile) * NT * 256 + lane;
-  const int64_t fstride = a.tiles * NT * 256;
-  const double *anav = a.ana + (size_t)(a.adj_out ? 1 : 0) * a.NU_tot * NT * 2 * 32 + lane;
-  const size_t cst = (size_t)kLCT * 2 * 32;  // class stride in pc_s
-  for (int t0 = 0; t0 < NT; t0 += kLCT) {
-    const int ct = NT - t0 < kLCT ? NT - t0 : kLCT;
-    // program and analysis pre-fold of (tile t0 + tt, parity e) = warp
-    if (warp < 2 * ct) {
-      const int tt = warp >> 1, e = warp & 1, t = t0 + tt;
-      double v[4][NI];
-#pragma unroll
-      for (int f = 0; f < NI; ++f)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) v[r][f] = Gb[(size_t)f * fstride + (size_t)t * 256 + r * 64 + e * 32];
-      double gq[4][NO];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) EKDef<EK>::op(v[r], gq[r]);
-#pragma unroll
-      for (int o = 0; o < NO; ++o) {
-        const double s14 = gq[0][o] + gq[3][o], d14 = gq[0][o] - gq[3][o];
-        const double s23 = gq[1][o] + gq[2][o], d32 = gq[2][o] - gq[1][o];
-        double *dst = pc_s + ((size_t)(o * 4) * kLCT + tt) * 64 + e * 32 + lane;
-        dst[0] = s14 + s23;        // PE
-        dst[cst] = s14 - s23;      // PO
-        dst[2 * cst] = d14 + d32;  // QE
-        dst[3 * cst] = d14 - d32;  // QO
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < CPW; ++j) {
-      const int cu = warp + kLargeProdWarps * j;
-      if (cu >= a.NU_tot) continue;
-      const int c = (cu >= a.nu_off[1]) + (cu >= a.nu_off[2]) + (cu >= a.nu_off[3]);
-      const double *bt = anav + ((size_t)cu * NT + t0) * 2 * 32;
-      const double *pa = pc_s + (size_t)c * cst + lane;
-      for (int te = 0; te < 2 * ct; ++te) {
-        const double bv = __ldg(bt + (size_t)te * 32);
-#pragma unroll
-        for (int o = 0; o < NO; ++o) dmma(y[j][o], pa[(size_t)o * 4 * cst + (size_t)te * 32], bv);
-      }
-    }
-    __syncthreads();
-  }
-  if (p >= a.npts) return;
-#pragma unroll
-  for (int j = 0; j < CPW; ++j) {
-    const int cu = warp + kLargeProdWarps * j;
-    if (cu >= a.NU_tot) continue;
-    const int c = (cu >= a.nu_off[1]) + (cu >= a.nu_off[2]) + (cu >= a.nu_off[3]);
-    const int u = cu - (c == 0 ? 0 : c == 1 ? a.nu_off[1] : c == 2 ? a.nu_off[2] : a.nu_off[3]);
-    const int kec = c == 0 ? a.ke[0] : c == 1 ? a.ke[1] : c == 2 ? a.ke[2] : a.ke[3];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int kk = 8 * u + 2 * q + h;
-      if (kk >= kec) continue;
-      const int n = class_mode(c, kk);
-#pragma unroll
-      for (int o = 0; o < NO; ++o) {
-        double *dst = a.out[o] + (int64_t)b * a.out_bs[o] + p * a.out_ps + (int64_t)n * a.out_ldm[o] +
-                      (c >= 2 ? a.out_sin : 0);
-        const double v = (c == 2 && n == 0) ? 0.0 : y[j][o][h];
-        if (a.accumulate)
-          *dst += v;
-        else
-          *dst = v;
-      }
-    }
-  }
-  (void)invN;
-  (void)twoN;
-}
-
-// workspace of the grid values, one per (device, stream): calls on different streams do not share it
-std::mutex g_lws_mu;
-std::map<std::pair<int, cudaStream_t>, std::pair<double *, size_t>> g_lws;
-
-int large_workspace(cudaStream_t st, size_t bytes, double **out) {
-  int dev = 0;
-  cudaGetDevice(&dev);
-  std::lock_guard<std::mutex> lk(g_lws_mu);
-  auto &w = g_lws[{dev, st}];
-  if (w.second < bytes) {
-    if (w.first) {
-      cudaStreamSynchronize(st);  // the previous call on this stream may still read it
-      cudaFree(w.first);
-    }
-    w.first = nullptr;
-    w.second = 0;
-    if (cudaMalloc(&w.first, bytes) != cudaSuccess) {
-      cudaGetLastError();
-      return set_error(SFNL_ERR_ALLOC, "cudaMalloc of the large-m workspace failed");
-    }
-    w.second = bytes;
-  }
-  *out = w.first;
-  return SFNL_OK;
-}
-
-template <int EK, int CPW>
-int launch_large_prod(const LargeArgs &la, int batch, cudaStream_t st) {
-  constexpr int NO = EKDef<EK>::NO;
-  const size_t smem = sizeof(double) * (size_t)NO * 4 * kLCT * 2 * 32;
-  auto kern = large_prod_kernel<EK, CPW>;
-  if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-    return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (large-m product)");
-  kern<<<dim3((unsigned)la.tiles, (unsigned)batch), kLargeProdWarps * 32, smem, st>>>(la);
-  return check_launch("large-m product");
-}
-
-template <int EK>
-int launch_large_prod_c(const LargeArgs &la, int batch, cudaStream_t st) {
-  const int cpw = (la.NU_tot + kLargeProdWarps - 1) / kLargeProdWarps;
-  switch (cpw) {
-    case 1: return launch_large_prod<EK, 1>(la, batch, st);
-    case 2: return launch_large_prod<EK, 2>(la, batch, st);
-    case 3: return launch_large_prod<EK, 3>(la, batch, st);
-    case 4: return launch_large_prod<EK, 4>(la, batch, st);
-    case 5: return launch_large_prod<EK, 5>(la, batch, st);
-    case 6: return launch_large_prod<EK, 6>(la, batch, st);
-    case 7: return launch_large_prod<EK, 7>(la, batch, st);
-    case 8: return launch_large_prod<EK, 8>(la, batch, st);
-  }
-  return set_error(SFNL_ERR_UNSUPPORTED, "large-m FAST form: too many output tiles");
-}
-
-int launch_large_syn(const LargeArgs &la, int batch, cudaStream_t st) {
-  const size_t smem = sizeof(double) * (size_t)la.KS_tot * 32;
-  const int tpw = (la.NT + kLargeSynWarps - 1) / kLargeSynWarps;
-  auto go = [&](auto kern) {
-    if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-      return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (large-m synthesis)");
-    kern<<<dim3((unsigned)la.tiles, (unsigned)la.ni, (unsigned)batch), kLargeSynWarps * 32, smem, st>>>(la);
-    return check_launch("large-m synthesis");
-  };
-  switch (tpw) {
-    case 1: return go(large_syn_kernel<1>);
-    case 2: return go(large_syn_kernel<2>);
-    case 3: return go(large_syn_kernel<3>);
-    case 4: return go(large_syn_kernel<4>);
-    case 5: return go(large_syn_kernel<5>);
-    case 6: return go(large_syn_kernel<6>);
-  }
-  return set_error(SFNL_ERR_UNSUPPORTED, "large-m FAST form: too many angle tiles");
-}
-
-constexpr size_t kLargeWorkspaceBytes = size_t(1) << 30;  // grid values of one point chunk
-
-}  // namespace
-
-// The fused kernels do not fit: the two-kernel form, elementary program by elementary program and point
-// chunk by point chunk (the tensor as three scalar x vector programs).
 bool fast_fused_fits(int op, int m) {
   const Geo g = make_geo(m);
   return fast_smem_bytes(op == OP_TENSOR ? EK_TENSOR : EK_CROSS, g.NT, 4 * g.KS_tot, true) <= 200 * 1024;
 }
-
-int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStream_t st) {
-  std::vector<Elem> seq;
-  if (a.op == OP_TENSOR) {
-    for (int k = 0; k < 3; ++k) {
-      Elem e{};
-      e.ek = EK_SVECT;
-      e.in[0] = 3; e.in[1] = 4; e.in[2] = 5; e.in[3] = k;
-      e.out[0] = 3 * k; e.out[1] = 3 * k + 1; e.out[2] = 3 * k + 2;
-      seq.push_back(e);
-    }
-  } else if (int rc = decompose_program(a.op, seq)) {
-    return rc;
-  }
-  const bool adj_out = op_adjoint_out(a.op);
-  const size_t per_point = sizeof(double) * 6 * (size_t)g.N * a.batch;  // grid values of up to 6 fields
-  int64_t chunk = (int64_t)(kLargeWorkspaceBytes / per_point);
-  chunk = (chunk / 8) * 8;
-  if (chunk < 8) chunk = 8;
-  if (chunk > a.np) chunk = ((a.np + 7) / 8) * 8;
-  double *G = nullptr;
-  if (int rc = large_workspace(st, per_point * (size_t)chunk, &G)) return rc;
-  for (const Elem &e : seq) {
-    const int ni = ek_nin(e.ek), no = ek_nout(e.ek);
-    for (int64_t c0 = 0; c0 < a.np; c0 += chunk) {
-      LargeArgs la;
-      std::memset(&la, 0, sizeof(la));
-      la.npts = a.np - c0 < chunk ? a.np - c0 : chunk;
-      la.tiles = (la.npts + 7) / 8;
-      la.in_sin = a.np;
-      la.out_ps = a.out_ps;
-      la.out_sin = a.np * a.out_ps;
-      int v16 = (a.np & 1) ? 0 : 1;
-      for (int i = 0; i < ni; ++i) {
-        la.in[i] = a.in[e.in[i]] + c0;
-        la.in_ldm[i] = a.in_ldm[e.in[i]];
-        la.in_bs[i] = a.in_bs[e.in[i]];
-        if ((reinterpret_cast<uintptr_t>(la.in[i]) & 15) || (la.in_ldm[i] & 1) || (la.in_bs[i] & 1)) v16 = 0;
-      }
-      for (int o = 0; o < no; ++o) {
-        la.out[o] = a.out[e.out[o]] + c0 * a.out_ps;
-        la.out_ldm[o] = a.out_ldm[e.out[o]];
-        la.out_bs[o] = a.out_bs[e.out[o]];
-      }
-      la.NT = g.NT;
-      la.NU_tot = g.NU_tot;
-      la.KS_tot = g.KS_tot;
-      for (int c = 0; c < 4; ++c) {
-        la.ks_off[c] = g.ks_off[c];
-        la.KS[c] = g.KS[c];
-        la.nu_off[c] = g.nu_off[c];
-        la.ke[c] = g.ke[c];
-      }
-      la.adj_in = e.adj;
-      la.adj_out = adj_out ? 1 : 0;
-      la.accumulate = e.acc;
-      la.vec16 = v16;
-      la.ni = ni;
-      la.syn = T.syn;
-      la.ana = T.ana;
-      la.G = G;
-      int rc = launch_large_syn(la, a.batch, st);
-      if (!rc)
-        rc = e.ek == EK_CROSS  ? launch_large_prod_c<EK_CROSS>(la, a.batch, st)
-           : e.ek == EK_DOT    ? launch_large_prod_c<EK_DOT>(la, a.batch, st)
-           : e.ek == EK_PROD   ? launch_large_prod_c<EK_PROD>(la, a.batch, st)
-                               : launch_large_prod_c<EK_SVECT>(la, a.batch, st);
-      if (rc) return rc;
-    }
-  }
-  return SFNL_OK;
-}
-
-namespace {
-}  // namespace
 
 int fast_grid_length(int m) { return make_geo(m).N; }
 

@@ -1,0 +1,90 @@
+// sfnl_fold.cuh -- geometry, DFT tables and device helpers shared by the FAST
+// form's kernels (sfnl_fast.cu: one fused kernel per 8-point tile; sfnl_large.cu:
+// synthesis and program+analysis as two kernels for large m).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "sfnl_ops.cuh"
+
+namespace sfnl {
+
+// ---------------------------------------------------------------------------
+// geometry of the folded transforms
+// ---------------------------------------------------------------------------
+struct Geo {
+  int m, Q, N;   // modes, quarter angles, grid length
+  int NT;        // quarter-angle tiles of 8
+  int ke[4];     // modes per class (0 cos-even, 1 cos-odd, 2 sin-even, 3 sin-odd)
+  int KS[4];     // synthesis k-steps per class (modes padded to 4)
+  int NU[4];     // analysis output tiles per class (modes padded to 8)
+  int ks_off[4]; // prefix offsets
+  int nu_off[4];
+  int KS_tot, NU_tot;
+};
+
+inline Geo make_geo(int m) {
+  Geo g;
+  g.m = m;
+  int qmin = (3 * m - 2 + 3) / 4;
+  if (qmin < 1) qmin = 1;
+  g.Q = ((qmin + 7) / 8) * 8;
+  g.N = 4 * g.Q;
+  g.NT = g.Q / 8;
+  const int ev = (m + 1) / 2, od = m / 2;
+  const int cnt[4] = {ev, od, ev, od};
+  g.KS_tot = g.NU_tot = 0;
+  for (int c = 0; c < 4; ++c) {
+    g.ke[c] = cnt[c];
+    g.KS[c] = (cnt[c] + 3) / 4;
+    g.NU[c] = (cnt[c] + 7) / 8;
+    g.ks_off[c] = g.KS_tot;
+    g.nu_off[c] = g.NU_tot;
+    g.KS_tot += g.KS[c];
+    g.NU_tot += g.NU[c];
+  }
+  return g;
+}
+
+__host__ __device__ inline int class_mode(int c, int k) { return 2 * k + (c & 1); }
+
+// Device tables for one m: synthesis B fragments and two analysis variants.
+struct Tables {
+  double *syn = nullptr;   // [KS_tot][NT][32]
+  double *ana = nullptr;   // [2 variants][NU_tot][NT][2][32]
+};
+// Cached per (device, m); built on first use (sfnl_fast.cu).
+int get_tables(const Geo &g, Tables *out);
+
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp_async8(void *smem_dst, const void *gsrc) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
+               "l"(gsrc)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
+               "l"(gsrc)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Element c of a 4-array without dynamic indexing (keeps the arrays in registers).
+__device__ __forceinline__ int sel4(const int (&v)[4], int c) { return c == 0 ? v[0] : c == 1 ? v[1] : c == 2 ? v[2] : v[3]; }
+
+// The fused kernels hold an 8-point tile's coefficients and folded products in shared memory; beyond
+// that (m ~ 100 for six fields) the two-kernel form runs (sfnl_large.cu).
+bool fast_fused_fits(int op, int m);
+int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStream_t st);
+
+}  // namespace sfnl

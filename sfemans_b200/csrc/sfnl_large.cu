@@ -1,0 +1,414 @@
+// sfnl_large.cu -- the FAST form's folded transforms for large m (SFNL_ALGO_FAST,
+// m up to 512), as two kernels that meet at the grid values.
+//
+// Same grid, folds and DFT tables as the fused kernels of sfnl_fast.cu (the
+// exact truncated product of fft_parallel.F90:147-665 evaluated on an
+// alias-free grid N = 4Q); only the split of the work differs.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <map>
+#include <mutex>
+
+#include "sfnl_fold.cuh"
+#include "sfnl_internal.h"
+#include "sfnl_ops.cuh"
+
+namespace sfnl {
+
+namespace {
+// ---------------------------------------------------------------------------
+// large m: the same folded transforms in two kernels, program by program
+// ---------------------------------------------------------------------------
+// Beyond m ~ 100 one CTA cannot hold an 8-point tile's coefficients of six fields and its folded
+// products at once (at m = 256: 196 KB and 147 KB), so the transforms are split at the grid values:
+//   large_syn_kernel  one CTA per (four 8-point tiles, field): stages the field's 2m coefficient rows,
+//                     runs the four class contractions on every angle tile (each B fragment of the
+//                     table shared by the four point tiles), folds to the four quadrants and writes
+//                     the grid values in fragment order, G[field][tile][t][quadrant][e][32];
+//   large_prod_kernel one CTA per 8-point tile and group of up to three outputs: for chunks of LCT angle
+//                     tiles it reads the program's grid values (each lane its own fragment elements),
+//                     evaluates the whole program (sfnl_ops.cuh) and the analysis pre-fold of the group's
+//                     outputs into shared memory, and every warp adds the chunk's k-steps to the
+//                     accumulators of its output tiles; the outputs are written at the end.
+// The whole program is evaluated on the grid, so a linearised product du x w + u x dw is analysed once,
+// and the fields shared by all tangents of a batch (the base state) are transformed once per point chunk.
+// G lives in a per-(device, stream) workspace; the points are processed in chunks that bound it.
+constexpr int kLargeSynMaxWarps = 12, kLargeProdWarps = 16, kLCT = 4, kLargeGroup = 3;
+constexpr size_t kLargeSynSmem = 200 * 1024;  // staged coefficients of one synthesis CTA
+
+struct LargeArgs {
+  const double *in[kMaxIn];
+  double *out[kMaxOut];
+  int64_t in_ldm[kMaxIn], out_ldm[kMaxOut], in_bs[kMaxIn], out_bs[kMaxOut];
+  int64_t gslot[kMaxIn];  // G offset of each field (units of tiles * NT * 256 doubles)
+  int syn_f[kMaxIn];      // large_syn_kernel: the fields this launch synthesises (blockIdx.y indexes it)
+  int64_t npts;     // points of this chunk (fields are offset to its first point)
+  int64_t in_sin;   // sine offset of the inputs (the arrays' np)
+  int64_t out_sin;  // sine offset of the outputs (np * point stride)
+  int64_t out_ps;   // point stride of the outputs
+  int NT, NU_tot, KS_tot;
+  int ks_off[4], KS[4], nu_off[4], ke[4];
+  unsigned adj_in;  // bit f: field f is a cotangent
+  int adj_out, vec16, batch_entry;
+  const double *syn, *ana;
+  double *G;
+  int64_t tiles;
+};
+
+// PT 8-point tiles of one field per CTA: each B fragment of the DFT table (read from L2) feeds PT
+// DMMAs.  With one tile per CTA the whole table (786 KB at m = 256) streams from L2 for every 8 points
+// of every field, and L2 bandwidth, not the FP64 pipe, sets the time.  Warps take the angle tiles in turn.
+template <int PT>
+__global__ void __launch_bounds__(kLargeSynMaxWarps * 32) large_syn_kernel(const LargeArgs a) {
+  extern __shared__ double xs[];  // [PT][KS_tot][4][8] of one field
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int f = a.syn_f[blockIdx.y];
+  const int64_t tile0 = (int64_t)blockIdx.x * PT, p0 = tile0 * 8;
+  const int NT = a.NT, KT = 4 * a.KS_tot;
+  const size_t pts = (size_t)a.KS_tot * 32;  // point-tile stride in xs
+  const double *in_f = a.in[f] + (int64_t)a.batch_entry * a.in_bs[f];
+  const int64_t ldm = a.in_ldm[f];
+  int KS[4], KOFF[4], KE[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    KS[c] = a.KS[c];
+    KOFF[c] = a.ks_off[c];
+    KE[c] = a.ke[c];
+  }
+  {  // stage: 4*PT threads per row, two points each (16-byte copies when aligned)
+    constexpr int tpr = 4 * PT;
+    const int pc = 2 * (threadIdx.x % tpr), rstep = blockDim.x / tpr;
+    const bool v16 = a.vec16 && p0 + pc + 2 <= a.npts;
+    const bool pv0 = p0 + pc < a.npts, pv1 = p0 + pc + 1 < a.npts;
+    const double *base = in_f + p0 + pc;
+    double *dst0 = xs + (size_t)(pc >> 3) * pts + (pc & 7);
+    for (int r = threadIdx.x / tpr; r < KT; r += rstep) {
+      const int c = (r >= 4 * KOFF[1]) + (r >= 4 * KOFF[2]) + (r >= 4 * KOFF[3]);
+      const int k = r - 4 * sel4(KOFF, c), n = class_mode(c, k);
+      double *dst = dst0 + (size_t)(r >> 2) * 32 + (r & 3) * 8;
+      const bool live = k < sel4(KE, c) && !(c == 2 && n == 0);  // the sine of mode 0 is ignored
+      const double *src = base + (int64_t)n * ldm + (c >= 2 ? a.in_sin : 0);
+      if (live && v16) {
+        cp_async16(dst, src);
+      } else {
+        if (live && pv0) cp_async8(dst, src); else dst[0] = 0.0;
+        if (live && pv1) cp_async8(dst + 1, src + 1); else dst[1] = 0.0;
+      }
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  if ((a.adj_in >> f) & 1u) {  // a cotangent: synthesised with the analysis weights 1/N (n = 0), 2/N
+    const double invN = 1.0 / (4.0 * 8.0 * NT), twoN = 2.0 * invN;
+    for (size_t i = threadIdx.x; i < PT * pts; i += blockDim.x) {
+      const int ks = (int)((i % pts) >> 5);
+      const bool n0 = (ks == KOFF[0] || ks == KOFF[2]) && ((i >> 3) & 3) == 0;  // k = 0 of an even class
+      xs[i] *= n0 ? invN : twoN;
+    }
+    __syncthreads();
+  }
+  const double *xs_l = xs + (lane & 3) * 8 + (lane >> 2);
+  int ks_max = KS[0];
+#pragma unroll
+  for (int c = 1; c < 4; ++c) ks_max = KS[c] > ks_max ? KS[c] : ks_max;
+  for (int t = warp; t < NT; t += nw) {
+    double acc[PT][4][2];
+#pragma unroll
+    for (int pt = 0; pt < PT; ++pt)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[pt][c][0] = acc[pt][c][1] = 0.0;
+    const double *bt = a.syn + (size_t)t * 32 + lane;
+#pragma unroll 2
+    for (int s = 0; s < ks_max; ++s) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        if (s >= sel4(KS, c)) continue;
+        const int ks = sel4(KOFF, c) + s;
+        const double bv = __ldg(bt + (size_t)ks * NT * 32);
+#pragma unroll
+        for (int pt = 0; pt < PT; ++pt) dmma(acc[pt][c], xs_l[pt * pts + (size_t)ks * 32], bv);
+      }
+    }
+#pragma unroll
+    for (int pt = 0; pt < PT; ++pt) {
+      const int64_t tile = tile0 + pt;
+      if (tile >= a.tiles) break;
+      double *gp0 = a.G + ((a.gslot[f] * a.tiles + tile) * NT + t) * 256 + lane;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const double A = acc[pt][0][e] + acc[pt][1][e], B = acc[pt][0][e] - acc[pt][1][e];
+        const double C = acc[pt][2][e] + acc[pt][3][e], D = acc[pt][3][e] - acc[pt][2][e];
+        double *gp = gp0 + e * 32;
+        gp[0 * 64] = A + C;  // theta
+        gp[1 * 64] = B + D;  // pi - theta
+        gp[2 * 64] = B - D;  // pi + theta
+        gp[3 * 64] = A - C;  // 2 pi - theta
+      }
+    }
+  }
+}
+
+// Outputs O0 .. O0+NOG-1 of program OP for batch entry a.batch_entry (the output group is a template
+// parameter so that the program's values stay in registers).
+template <int OP, int O0, int CPW>
+__global__ void __launch_bounds__(kLargeProdWarps * 32) large_prod_kernel(const LargeArgs a) {
+  constexpr int NI = op_nin(OP), NO = op_nout(OP);
+  constexpr int NOG = NO - O0 < kLargeGroup ? NO - O0 : kLargeGroup;
+  extern __shared__ double pc_s[];  // [NOG][4][LCT][2][32]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, q = lane & 3;
+  const int b = a.batch_entry;
+  const int64_t tile = blockIdx.x, p = tile * 8 + (lane >> 2);
+  const int NT = a.NT;
+  double y[CPW][NOG][2];
+#pragma unroll
+  for (int j = 0; j < CPW; ++j)
+#pragma unroll
+    for (int o = 0; o < NOG; ++o) y[j][o][0] = y[j][o][1] = 0.0;
+  const int64_t fstride = a.tiles * NT * 256;
+  const double *Gl = a.G + tile * NT * 256 + lane;
+  const double *anav = a.ana + (size_t)(a.adj_out ? 1 : 0) * a.NU_tot * NT * 2 * 32 + lane;
+  const size_t cst = (size_t)kLCT * 2 * 32;  // class stride in pc_s
+  for (int t0 = 0; t0 < NT; t0 += kLCT) {
+    const int ct = NT - t0 < kLCT ? NT - t0 : kLCT;
+    // the program and the analysis pre-fold of the group at (tile t0 + tt, parity e) = warp
+    if (warp < 2 * ct) {
+      const int tt = warp >> 1, e = warp & 1, t = t0 + tt;
+      double gq[4][NOG];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        double x[NI], yy[NO];
+#pragma unroll
+        for (int f = 0; f < NI; ++f) x[f] = Gl[a.gslot[f] * fstride + (size_t)t * 256 + r * 64 + e * 32];
+        apply_op<OP>(x, yy);
+#pragma unroll
+        for (int o = 0; o < NOG; ++o) gq[r][o] = yy[O0 + o];
+      }
+#pragma unroll
+      for (int o = 0; o < NOG; ++o) {
+        const double s14 = gq[0][o] + gq[3][o], d14 = gq[0][o] - gq[3][o];
+        const double s23 = gq[1][o] + gq[2][o], d32 = gq[2][o] - gq[1][o];
+        double *dst = pc_s + ((size_t)(o * 4) * kLCT + tt) * 64 + e * 32 + lane;
+        dst[0] = s14 + s23;        // PE
+        dst[cst] = s14 - s23;      // PO
+        dst[2 * cst] = d14 + d32;  // QE
+        dst[3 * cst] = d14 - d32;  // QO
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < CPW; ++j) {
+      const int cu = warp + kLargeProdWarps * j;
+      if (cu >= a.NU_tot) continue;
+      const int c = (cu >= a.nu_off[1]) + (cu >= a.nu_off[2]) + (cu >= a.nu_off[3]);
+      const double *bt = anav + ((size_t)cu * NT + t0) * 2 * 32;
+      const double *pa = pc_s + (size_t)c * cst + lane;
+      for (int te = 0; te < 2 * ct; ++te) {
+        const double bv = __ldg(bt + (size_t)te * 32);
+#pragma unroll
+        for (int o = 0; o < NOG; ++o) dmma(y[j][o], pa[(size_t)o * 4 * cst + (size_t)te * 32], bv);
+      }
+    }
+    __syncthreads();
+  }
+  if (p >= a.npts) return;
+#pragma unroll
+  for (int j = 0; j < CPW; ++j) {
+    const int cu = warp + kLargeProdWarps * j;
+    if (cu >= a.NU_tot) continue;
+    const int c = (cu >= a.nu_off[1]) + (cu >= a.nu_off[2]) + (cu >= a.nu_off[3]);
+    const int u = cu - (c == 0 ? 0 : c == 1 ? a.nu_off[1] : c == 2 ? a.nu_off[2] : a.nu_off[3]);
+    const int kec = c == 0 ? a.ke[0] : c == 1 ? a.ke[1] : c == 2 ? a.ke[2] : a.ke[3];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int kk = 8 * u + 2 * q + h;
+      if (kk >= kec) continue;
+      const int n = class_mode(c, kk);
+#pragma unroll
+      for (int o = 0; o < NOG; ++o) {
+        const int og = O0 + o;
+        double *dst = a.out[og] + (int64_t)b * a.out_bs[og] + p * a.out_ps + (int64_t)n * a.out_ldm[og] +
+                      (c >= 2 ? a.out_sin : 0);
+        *dst = (c == 2 && n == 0) ? 0.0 : y[j][o][h];
+      }
+    }
+  }
+}
+
+// workspace of the grid values, one per (device, stream): calls on different streams do not share it
+std::mutex g_lws_mu;
+std::map<std::pair<int, cudaStream_t>, std::pair<double *, size_t>> g_lws;
+
+int large_workspace(cudaStream_t st, size_t bytes, double **out) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_lws_mu);
+  auto &w = g_lws[{dev, st}];
+  if (w.second < bytes) {
+    if (w.first) {
+      cudaStreamSynchronize(st);  // the previous call on this stream may still read it
+      cudaFree(w.first);
+    }
+    w.first = nullptr;
+    w.second = 0;
+    if (cudaMalloc(&w.first, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return set_error(SFNL_ERR_ALLOC, "cudaMalloc of the large-m workspace failed");
+    }
+    w.second = bytes;
+  }
+  *out = w.first;
+  return SFNL_OK;
+}
+
+template <int OP, int O0, int CPW>
+int launch_large_prod(const LargeArgs &la, cudaStream_t st) {
+  constexpr int NO = op_nout(OP), NOG = NO - O0 < kLargeGroup ? NO - O0 : kLargeGroup;
+  const size_t smem = sizeof(double) * (size_t)NOG * 4 * kLCT * 2 * 32;
+  large_prod_kernel<OP, O0, CPW><<<(unsigned)la.tiles, kLargeProdWarps * 32, smem, st>>>(la);
+  return check_launch("large-m program and analysis");
+}
+
+// Output group G (outputs 3G .. 3G+2) of program OP.
+template <int OP, int G>
+int launch_large_group(const LargeArgs &la, cudaStream_t st) {
+  constexpr int O0 = kLargeGroup * G;
+  if constexpr (O0 >= op_nout(OP)) {
+    return SFNL_OK;
+  } else {
+    switch ((la.NU_tot + kLargeProdWarps - 1) / kLargeProdWarps) {
+      case 1: return launch_large_prod<OP, O0, 1>(la, st);
+      case 2: return launch_large_prod<OP, O0, 2>(la, st);
+      case 3: return launch_large_prod<OP, O0, 3>(la, st);
+      case 4: return launch_large_prod<OP, O0, 4>(la, st);
+      case 5: return launch_large_prod<OP, O0, 5>(la, st);
+      case 6: return launch_large_prod<OP, O0, 6>(la, st);
+      case 7: return launch_large_prod<OP, O0, 7>(la, st);
+      case 8: return launch_large_prod<OP, O0, 8>(la, st);
+    }
+    return set_error(SFNL_ERR_UNSUPPORTED, "large-m FAST form: too many output tiles");
+  }
+}
+
+template <int OP>
+int launch_large_prod_all(const LargeArgs &la, cudaStream_t st) {
+  static_assert(op_nout(OP) <= 4 * kLargeGroup, "output groups");
+  if (int rc = launch_large_group<OP, 0>(la, st)) return rc;
+  if (int rc = launch_large_group<OP, 1>(la, st)) return rc;
+  if (int rc = launch_large_group<OP, 2>(la, st)) return rc;
+  return launch_large_group<OP, 3>(la, st);
+}
+
+int launch_large_prod_op(int op, const LargeArgs &la, cudaStream_t st) {
+  switch (op) {
+    case OP_CROSS: return launch_large_prod_all<OP_CROSS>(la, st);
+    case OP_DOT: return launch_large_prod_all<OP_DOT>(la, st);
+    case OP_PROD: return launch_large_prod_all<OP_PROD>(la, st);
+    case OP_BUNDLE: return launch_large_prod_all<OP_BUNDLE>(la, st);
+    case OP_CROSS_JVP: return launch_large_prod_all<OP_CROSS_JVP>(la, st);
+    case OP_CROSS_VJP: return launch_large_prod_all<OP_CROSS_VJP>(la, st);
+    case OP_MHD_JVP: return launch_large_prod_all<OP_MHD_JVP>(la, st);
+    case OP_MHD_VJP: return launch_large_prod_all<OP_MHD_VJP>(la, st);
+    case OP_SVECT: return launch_large_prod_all<OP_SVECT>(la, st);
+    case OP_TENSOR: return launch_large_prod_all<OP_TENSOR>(la, st);
+  }
+  return set_error(SFNL_ERR_ARG, "large-m FAST form: program not bilinear");
+}
+
+int launch_large_syn(const LargeArgs &la, int nfields, cudaStream_t st) {
+  if (nfields == 0) return SFNL_OK;
+  // angle tiles spread evenly over at most kLargeSynMaxWarps warps
+  const int rounds = (la.NT + kLargeSynMaxWarps - 1) / kLargeSynMaxWarps, nw = (la.NT + rounds - 1) / rounds;
+  const size_t tile_bytes = sizeof(double) * (size_t)la.KS_tot * 32;
+  auto go = [&](auto kern, int pt) {
+    const size_t smem = tile_bytes * pt;
+    if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (large-m synthesis)");
+    const int64_t blocks = (la.tiles + pt - 1) / pt;
+    kern<<<dim3((unsigned)blocks, (unsigned)nfields), nw * 32, smem, st>>>(la);
+    return check_launch("large-m synthesis");
+  };
+  if (4 * tile_bytes <= kLargeSynSmem) return go(large_syn_kernel<4>, 4);
+  if (2 * tile_bytes <= kLargeSynSmem) return go(large_syn_kernel<2>, 2);
+  return set_error(SFNL_ERR_UNSUPPORTED, "large-m FAST form: m too large");
+}
+
+constexpr size_t kLargeWorkspaceBytes = size_t(1) << 30;  // grid values of one point chunk
+
+}  // namespace
+
+// The two-kernel form: per point chunk, the batch-invariant fields (base state) once, then per batch
+// entry its own fields and the program's outputs in groups of three (one launch per group).
+int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStream_t st) {
+  const int ni = op_nin(a.op), no = op_nout(a.op);
+  int nshared = 0, nown = 0;  // batch-invariant fields take the first G slots, the batched ones the next
+  int64_t gslot[kMaxIn];
+  for (int f = 0; f < ni; ++f) gslot[f] = a.in_bs[f] == 0 ? nshared++ : -1;
+  for (int f = 0; f < ni; ++f)
+    if (gslot[f] < 0) gslot[f] = nshared + nown++;
+  const size_t per_point = sizeof(double) * (size_t)(nshared + nown) * g.N;
+  int64_t chunk = (int64_t)(kLargeWorkspaceBytes / per_point);
+  chunk = (chunk / 32) * 32;
+  if (chunk < 32) chunk = 32;
+  if (chunk > a.np) chunk = ((a.np + 7) / 8) * 8;
+  double *G = nullptr;
+  if (int rc = large_workspace(st, per_point * (size_t)chunk, &G)) return rc;
+  const bool adj_out = op_adjoint_out(a.op);
+  unsigned adj = 0;
+  for (int f = 0; f < ni; ++f)
+    if (op_adjoint_in(a.op, f)) adj |= 1u << f;
+  for (int64_t c0 = 0; c0 < a.np; c0 += chunk) {
+    LargeArgs la;
+    std::memset(&la, 0, sizeof(la));
+    la.npts = a.np - c0 < chunk ? a.np - c0 : chunk;
+    la.tiles = (la.npts + 7) / 8;
+    la.in_sin = a.np;
+    la.out_ps = a.out_ps;
+    la.out_sin = a.np * a.out_ps;
+    int v16 = (a.np & 1) ? 0 : 1;
+    for (int f = 0; f < ni; ++f) {
+      la.in[f] = a.in[f] + c0;
+      la.in_ldm[f] = a.in_ldm[f];
+      la.in_bs[f] = a.in_bs[f];
+      la.gslot[f] = gslot[f];
+      if ((reinterpret_cast<uintptr_t>(la.in[f]) & 15) || (la.in_ldm[f] & 1) || (la.in_bs[f] & 1)) v16 = 0;
+    }
+    for (int o = 0; o < no; ++o) {
+      la.out[o] = a.out[o] + c0 * a.out_ps;
+      la.out_ldm[o] = a.out_ldm[o];
+      la.out_bs[o] = a.out_bs[o];
+    }
+    la.NT = g.NT;
+    la.NU_tot = g.NU_tot;
+    la.KS_tot = g.KS_tot;
+    for (int c = 0; c < 4; ++c) {
+      la.ks_off[c] = g.ks_off[c];
+      la.KS[c] = g.KS[c];
+      la.nu_off[c] = g.nu_off[c];
+      la.ke[c] = g.ke[c];
+    }
+    la.adj_in = adj;
+    la.adj_out = adj_out ? 1 : 0;
+    la.vec16 = v16;
+    la.syn = T.syn;
+    la.ana = T.ana;
+    la.G = G;
+    // the batch-invariant fields, once per chunk
+    int k = 0;
+    for (int f = 0; f < ni; ++f)
+      if (a.in_bs[f] == 0) la.syn_f[k++] = f;
+    la.batch_entry = 0;
+    if (int rc = launch_large_syn(la, k, st)) return rc;
+    for (int b = 0; b < a.batch; ++b) {
+      la.batch_entry = b;
+      k = 0;
+      for (int f = 0; f < ni; ++f)
+        if (a.in_bs[f] != 0) la.syn_f[k++] = f;
+      if (int rc = launch_large_syn(la, k, st)) return rc;
+      if (int rc = launch_large_prod_op(a.op, la, st)) return rc;
+    }
+  }
+  return SFNL_OK;
+}
+
+}  // namespace sfnl

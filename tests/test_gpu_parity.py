@@ -265,6 +265,46 @@ def test_large_m_linearised_batched():
         assert abs(lhs - rhs) <= 1e-12 * np.linalg.norm(jv[..., t]) * np.linalg.norm(c[..., t])
 
 
+@pytest.mark.parametrize("npts,m", [(21, 128), (6, 300)])
+def test_large_m_bundle(npts, m):
+    # ten outputs: four output groups of the program kernel over one set of grid values
+    pad = 3 * m // 2
+    f = [R.synthetic_field(npts, 6, m, 0.05, 500 + i) for i in range(5)]
+    outs = sf.bundle_mhd(*[dev(x) for x in f], m_max_pad=pad, algo=sf.ALGO_FAST)
+    _sync()
+    for o, r in zip(outs, R.mhd_bundle(*f, pad)):
+        assert R.rel_l2(host(o), r) <= FP64_TOL
+
+
+@pytest.mark.parametrize("npts,m,k", [(17, 112, 2), (10, 160, 1)])
+def test_large_m_cross_jvp_vjp(npts, m, k):
+    pad = 3 * m // 2
+    u = R.synthetic_field(npts, 6, m, 0.05, 531)
+    w = R.synthetic_field(npts, 6, m, 0.05, 532)
+    v = _batched(npts, 12, m, k, 0.05, 540)
+    c = _batched(npts, 6, m, k, 0.05, 550)
+    jv = host(sf.cross_jvp(dev(u), dev(w), dev(v), m_max_pad=pad))
+    jtc = host(sf.cross_vjp(dev(u), dev(w), dev(c), m_max_pad=pad))
+    for t in range(k):
+        du, dw = (np.asfortranarray(v[:, 6 * i:6 * i + 6, :, t]) for i in range(2))
+        assert R.rel_l2(jv[..., t], R.cross_jvp(u, w, du, dw, pad)) <= FP64_TOL
+        assert R.rel_l2(jtc[..., t], R.cross_vjp(u, w, np.asfortranarray(c[..., t]))) <= FP64_TOL
+
+
+def test_large_m_linearised_point_chunks():
+    # the base state is synthesised once per point chunk and the tangents per batch entry: more points
+    # than one chunk of grid values (about 9.7k points at m = 256 for the 18 fields of the MHD JVP)
+    npts, m, k, pad = 12_001, 256, 2, 384
+    u, w, b = (R.synthetic_field(npts, 6, m, 0.05, 570 + i) for i in range(3))
+    v = _batched(npts, 18, m, k, 0.05, 580)
+    jv = host(sf.mhd_jvp(dev(u), dev(w), dev(b), dev(v), m_max_pad=pad))
+    eng = lambda op, x, y: R.fft_par(op, x, y, pad, workers=8)  # noqa: E731
+    for t in range(k):
+        du, dw, db = (np.asfortranarray(v[:, 6 * i:6 * i + 6, :, t]) for i in range(3))
+        assert R.rel_l2(jv[:, :6, :, t], R.cross_jvp(u, w, du, dw, pad, engine=eng)) <= FP64_TOL
+        assert R.rel_l2(jv[:, 6:, :, t], R.cross_jvp(u, b, du, db, pad, engine=eng)) <= FP64_TOL
+
+
 def test_large_m_point_chunks():
     # more points than one workspace chunk of grid values holds (about 29k points at m = 256)
     npts, m, pad = 70_001, 256, 384

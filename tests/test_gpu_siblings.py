@@ -81,15 +81,15 @@ def test_fast_form_of_the_bilinear_siblings(kind, npts, m, pad):
     assert _worst(kind, host(out), ref) <= FP64_TOL
 
 
-def test_tensor_beyond_the_fast_form_falls_back_to_the_grid():
-    # m = 96: the tensor's nine outputs do not fit the FAST form's shared memory; AUTO takes GRID.
+def test_tensor_beyond_the_fused_kernel():
+    # m = 96: the tensor's nine outputs do not fit the fused kernel's shared memory; FAST (and AUTO)
+    # take the two-kernel form, whose program kernel analyses the outputs in three groups.
     V1, V2 = _inputs("tensor", 20, 96, 0.1, 7)
-    with pytest.raises(sf.SfnlError) as e:
-        sf.product(sf.OP_TENSOR, dev(V1), dev(V2), m_max_pad=144, algo=sf.ALGO_FAST)
-    assert e.value.code == -4
-    out = sf.tensor(dev(V1), dev(V2), m_max_pad=144)
-    _sync()
-    assert _worst("tensor", host(out), R.c_oracle("tensor", V1, V2, 144)) <= FP64_TOL
+    ref = R.c_oracle("tensor", V1, V2, 144)
+    for algo in (sf.ALGO_FAST, sf.ALGO_AUTO):
+        out = sf.product(sf.OP_TENSOR, dev(V1), dev(V2), m_max_pad=144, algo=algo)
+        _sync()
+        assert _worst("tensor", host(out), ref) <= FP64_TOL
 
 
 @pytest.mark.parametrize("kind", ["div", "svdiv", "tension"])
