@@ -341,8 +341,8 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M
 
   // ---- stage the tile's coefficients ----
   // Global row r = 4*ks + q of field f (class c, mode index k = r - 4*KOFF[c]) holds 8 points; it
-  // lands contiguously at xs[(f*KS_tot + ks)*32 + q*8 + point], so that lane (g, q) of a warp reads
-  // the A fragment of k-step ks at xs[(f*KS_tot + ks)*32 + q*8 + g]: 256 contiguous bytes.  Four
+  // lands at xs[(f*KS_tot + ks)*32 + a_frag_slot(q, point)], so that lane (g, q) of a warp reads the
+  // A fragment of k-step ks from one 256-byte block without bank conflicts.  Four
   // consecutive threads copy one row (two points each, one 16-byte copy when the row is 16-byte
   // aligned), so a warp instruction moves 8 whole 64-byte rows.
   const int NWT = CS ? NW >> 1 : NW;  // angle tiles per pass (two warps per tile with the class split)
@@ -358,11 +358,11 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M
     for (int f = 0; f < NI; ++f) {
       const double *base = a.in[f] + (int64_t)b * a.in_bs[f] + p0 + pc;
       const int64_t ldm = a.in_ldm[f];
-      double *xf = xs + (size_t)f * KS_tot * 32 + pc;
+      double *xf = xs + (size_t)f * KS_tot * 32;
       for (int r = threadIdx.x >> 2; r < KT; r += rstep) {
         const int c = (r >= 4 * KOFF[1]) + (r >= 4 * KOFF[2]) + (r >= 4 * KOFF[3]);
         const int k = r - 4 * sel4(KOFF, c), n = class_mode(c, k);
-        double *dst = xf + (size_t)(r >> 2) * 32 + (r & 3) * 8;
+        double *dst = xf + (size_t)(r >> 2) * 32 + a_frag_slot(r & 3, pc);
         const bool live = k < sel4(KE, c) && !(c == 2 && n == 0);  // the sine of mode 0 is ignored
         const double *src = base + (int64_t)n * ldm + (c >= 2 ? a.np : 0);
         if (live && v16) {
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M
       auto synth = [&](auto cb_tag) {
         constexpr int CB = decltype(cb_tag)::value;  // first class of this warp's pair
         const double *syn_t = a.syn + (size_t)t * 32 + lane;
-        const double *xs_l = xs + (lane & 3) * 8 + (lane >> 2);
+        const double *xs_l = xs + a_frag_slot(lane & 3, lane >> 2);
 #pragma unroll
         for (int s = 0; s < ks_max; ++s) {
 #pragma unroll
@@ -486,7 +486,7 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M
       if (t < NT) {
       // k-steps outermost, the four classes inside: 4*NI independent accumulator chains per step
       const double *syn_t = a.syn + (size_t)t * 32 + lane;
-      const double *xs_l = xs + (lane & 3) * 8 + (lane >> 2);
+      const double *xs_l = xs + a_frag_slot(lane & 3, lane >> 2);
 #pragma unroll
       for (int s = 0; s < ks_max; ++s) {
 #pragma unroll
@@ -620,7 +620,7 @@ __device__ __forceinline__ void tf_stage(double *xs, const FieldSet<NG> &fs, int
   for (int f = 0; f < NG; ++f) {
     const double *base = fs.p[f] + p0 + pc;
     const int64_t ldm = fs.ldm[f];
-    double *xf = xs + (size_t)f * KS_tot * 32 + pc;
+    double *xf = xs + (size_t)f * KS_tot * 32;
     for (int r = threadIdx.x >> 2; r < KT; r += rstep) {
       const int gr = (r >= 4 * tf_koff(M, 1)) + (r >= 4 * tf_koff(M, 2)) + (r >= 4 * tf_koff(M, 3)) +
                      (r >= 4 * tf_koff(M, 4)) + (r >= 4 * tf_koff(M, 5));
@@ -628,7 +628,7 @@ __device__ __forceinline__ void tf_stage(double *xs, const FieldSet<NG> &fs, int
                    : gr == 4 ? tf_koff(M, 4) : tf_koff(M, 5);
       const int keg = gr % 3 == 0 ? tf_ke(M, 0) : gr % 3 == 1 ? tf_ke(M, 1) : tf_ke(M, 2);
       const int k = r - 4 * kg, n = tf_mode(gr, k);
-      double *dst = xf + (size_t)(r >> 2) * 32 + (r & 3) * 8;
+      double *dst = xf + (size_t)(r >> 2) * 32 + a_frag_slot(r & 3, pc);
       const bool live = k < keg && !(gr == 3 && k == 0);  // the sine of mode 0 is ignored
       const double *src = base + (int64_t)n * ldm + (gr >= 3 ? np : 0);
       if (live && v16) {
@@ -659,7 +659,7 @@ __device__ __forceinline__ void tf_synth(const double *xs, const double *syn, do
   const int koff_e = ge == 0 ? tf_koff(M, 0) : ge == 1 ? tf_koff(M, 1) : ge == 3 ? tf_koff(M, 3) : tf_koff(M, 4);
   const int ks_e = (ge % 3 == 0) ? tf_KS(M, 0) : tf_KS(M, 1);
   const int koff_o = half ? tf_koff(M, 5) : tf_koff(M, 2);
-  const double *xs_l = xs + (lane & 3) * 8 + (lane >> 2);
+  const double *xs_l = xs + a_frag_slot(lane & 3, lane >> 2);
   const double *syn_e = syn + (size_t)te_tile * 32 + lane, *syn_o = syn + (size_t)tau * 32 + lane;
   constexpr int KSE = tf_KS(M, 0) > tf_KS(M, 1) ? tf_KS(M, 0) : tf_KS(M, 1);
 #pragma unroll

@@ -79,6 +79,13 @@ __device__ __forceinline__ void cp_async_wait_all() {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
+// Slot of (k-value kq, point p) in a 32-double A-fragment block [4 k][8 points].  A lane (g, q) of
+// m8n8k4 reads (q, g); a 64-bit shared load is served per half-warp, and with the plain order q*8 + g
+// the lanes q and q + 2 of a half-warp hit the same banks (two wavefronts per half-warp).  Flipping
+// bit 2 of the point for q >= 2 spreads a half-warp over all 32 banks and keeps point pairs (2h, 2h+1)
+// adjacent, so 16-byte stores of two points stay possible.
+__host__ __device__ __forceinline__ int a_frag_slot(int kq, int p) { return kq * 8 + (p ^ ((kq & 2) << 1)); }
+
 // Element c of a 4-array without dynamic indexing (keeps the arrays in registers).
 __device__ __forceinline__ int sel4(const int (&v)[4], int c) { return c == 0 ? v[0] : c == 1 ? v[1] : c == 2 ? v[2] : v[3]; }
 

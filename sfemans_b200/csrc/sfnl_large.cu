@@ -61,7 +61,7 @@ struct LargeArgs {
 // of every field, and L2 bandwidth, not the FP64 pipe, sets the time.  Warps take the angle tiles in turn.
 template <int PT>
 __global__ void __launch_bounds__(kLargeSynMaxWarps * 32) large_syn_kernel(const LargeArgs a) {
-  extern __shared__ double xs[];  // [PT][KS_tot][4][8] of one field
+  extern __shared__ double xs[];  // [PT][KS_tot][4][8] of one field, points swizzled (a_frag_slot)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int f = a.syn_f[blockIdx.y];
   const int64_t tile0 = (int64_t)blockIdx.x * PT, p0 = tile0 * 8;
@@ -82,11 +82,11 @@ __global__ void __launch_bounds__(kLargeSynMaxWarps * 32) large_syn_kernel(const
     const bool v16 = a.vec16 && p0 + pc + 2 <= a.npts;
     const bool pv0 = p0 + pc < a.npts, pv1 = p0 + pc + 1 < a.npts;
     const double *base = in_f + p0 + pc;
-    double *dst0 = xs + (size_t)(pc >> 3) * pts + (pc & 7);
+    double *dst0 = xs + (size_t)(pc >> 3) * pts;
     for (int r = threadIdx.x / tpr; r < KT; r += rstep) {
       const int c = (r >= 4 * KOFF[1]) + (r >= 4 * KOFF[2]) + (r >= 4 * KOFF[3]);
       const int k = r - 4 * sel4(KOFF, c), n = class_mode(c, k);
-      double *dst = dst0 + (size_t)(r >> 2) * 32 + (r & 3) * 8;
+      double *dst = dst0 + (size_t)(r >> 2) * 32 + a_frag_slot(r & 3, pc & 7);
       const bool live = k < sel4(KE, c) && !(c == 2 && n == 0);  // the sine of mode 0 is ignored
       const double *src = base + (int64_t)n * ldm + (c >= 2 ? a.in_sin : 0);
       if (live && v16) {
@@ -108,10 +108,11 @@ __global__ void __launch_bounds__(kLargeSynMaxWarps * 32) large_syn_kernel(const
     }
     __syncthreads();
   }
-  const double *xs_l = xs + (lane & 3) * 8 + (lane >> 2);
+  const double *xs_l = xs + a_frag_slot(lane & 3, lane >> 2);
   int ks_max = KS[0];
 #pragma unroll
   for (int c = 1; c < 4; ++c) ks_max = KS[c] > ks_max ? KS[c] : ks_max;
+  const size_t bstride = (size_t)NT * 32;
   for (int t = warp; t < NT; t += nw) {
     double acc[PT][4][2];
 #pragma unroll
@@ -119,15 +120,23 @@ __global__ void __launch_bounds__(kLargeSynMaxWarps * 32) large_syn_kernel(const
 #pragma unroll
       for (int c = 0; c < 4; ++c) acc[pt][c][0] = acc[pt][c][1] = 0.0;
     const double *bt = a.syn + (size_t)t * 32 + lane;
-#pragma unroll 2
+    // B fragments of k-step s + 1 are loaded while those of s feed the DMMAs (the table is read from L2)
+    double bn[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) bn[c] = KS[c] > 0 ? __ldg(bt + (size_t)KOFF[c] * bstride) : 0.0;
     for (int s = 0; s < ks_max; ++s) {
+      double bc[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        bc[c] = bn[c];
+        if (s + 1 < sel4(KS, c)) bn[c] = __ldg(bt + (size_t)(sel4(KOFF, c) + s + 1) * bstride);
+      }
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         if (s >= sel4(KS, c)) continue;
-        const int ks = sel4(KOFF, c) + s;
-        const double bv = __ldg(bt + (size_t)ks * NT * 32);
+        const size_t ks = (size_t)(sel4(KOFF, c) + s);
 #pragma unroll
-        for (int pt = 0; pt < PT; ++pt) dmma(acc[pt][c], xs_l[pt * pts + (size_t)ks * 32], bv);
+        for (int pt = 0; pt < PT; ++pt) dmma(acc[pt][c], xs_l[pt * pts + ks * 32], bc[c]);
       }
     }
 #pragma unroll
