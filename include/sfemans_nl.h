@@ -177,6 +177,40 @@ int sfnl_smb_cross_prod_gauss(const double *V_in, const int *jj, const double *w
                               int k_d, const int *list_mode, const double *omega, double *V_out, int np_nodes, int me,
                               int n_w, int l_G, int nmod, int nb_procs);
 
+/* The Lorentz-force caller, smb_CurlH_cross_B_gauss_sft_par (SOURCES/SIMULATION/
+ * subroutine_ns_with_m.F90:788-883): out = (curl h) x b at the Gauss points from two
+ * nodal fields h (the magnetic field H) and b (the induction B), both (np_nodes, 6, nmod);
+ * no precession term.  Mesh arrays, list_mode, out and m_max_pad as above; work: 12*l_G*me*nmod
+ * doubles or NULL. */
+int sfnl_curlh_cross_b_gauss_f64(const double *h, const double *b, const int *jj, const double *ww, const double *dw,
+                                 const double *rr, const int *list_mode, double *out, int np_nodes, int me, int n_w,
+                                 int l_G, int nmod, int m_max_pad, double *work, sfnl_stream_t stream);
+/* The same on host arrays (V_in = H, W_in = B; k_d must be 2, nb_procs 1). */
+int sfnl_smb_curlh_cross_b_gauss(const double *V_in, const double *W_in, const int *jj, const double *ww,
+                                 const double *dw, const double *rr, int k_d, const int *list_mode, double *V_out,
+                                 int np_nodes, int me, int n_w, int l_G, int nmod, int nb_procs);
+
+/* The scalar-advection callers, smb_ugradc_gauss_fft_par of the level set
+ * (SOURCES/SIMULATION/subroutine_level_set.F90:434-534: conservative = 0, heat = NULL), of the
+ * temperature (subroutine_temperature_with_T.F90:247-350: conservative = 1, heat = the
+ * volumetric heat capacity of each element) and smb_ugradc_gauss_fft_par_conc of the
+ * concentration (subroutine_concentration.F90:243-341: conservative = 1, heat = NULL):
+ *   out (l_G*me, 2, nmod) = (heat grad c) . u  [+ div u (heat c) when conservative]
+ * with FFT_PAR_DOT_PROD_DCL (+ FFT_PAR_PROD_DCL, the two analyses added, computed here as one
+ * program analysed once).
+ *   v     (np_nodes, 6, nmod) nodal velocity;  c (np_nodes, 2, nmod) nodal scalar
+ *   heat  (me) per-element factor of grad c and c, or NULL (factor 1)
+ *   work  16*l_G*me*nmod doubles (12 when conservative == 0) or NULL. */
+int sfnl_ugradc_gauss_f64(const double *v, const double *c, const double *heat, int conservative, const int *jj,
+                          const double *ww, const double *dw, const double *rr, const int *list_mode, double *out,
+                          int np_nodes, int me, int n_w, int l_G, int nmod, int m_max_pad, double *work,
+                          sfnl_stream_t stream);
+/* The same on host arrays (k_d must be 2, nb_procs 1). */
+int sfnl_smb_ugradc_gauss(const double *V_in, const double *c_in, const double *heat_capa, int conservative,
+                          const int *jj, const double *ww, const double *dw, const double *rr, int k_d,
+                          const int *list_mode, double *c_out, int np_nodes, int me, int n_w, int l_G, int nmod,
+                          int nb_procs);
+
 /* ---------------------------------------------------------------------------
  * Linearised cross product N(u, w) = u x w about a base state (u, w).
  * New capability: the reference's LightKrylov operator binds rmatvec to the

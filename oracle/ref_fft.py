@@ -122,6 +122,10 @@ def _lib():
         IP = ctypes.POINTER(ctypes.c_int)
         lib.orc_cross_gauss.restype = ctypes.c_int
         lib.orc_cross_gauss.argtypes = [P, IP, P, P, P, IP, P] + [ctypes.c_int] * 5 + [P, P, P]
+        lib.orc_curlh_cross_b_gauss.restype = ctypes.c_int
+        lib.orc_curlh_cross_b_gauss.argtypes = [P, P, IP, P, P, P, IP] + [ctypes.c_int] * 5 + [P, P, P]
+        lib.orc_ugradc_gauss.restype = ctypes.c_int
+        lib.orc_ugradc_gauss.argtypes = [P, P, P, ctypes.c_int, IP, P, P, P, IP] + [ctypes.c_int] * 5 + [P] * 5
         _LIB = lib
     return _LIB
 
@@ -275,6 +279,47 @@ def c_cross_gauss(V, mesh, list_mode, omega=None, product=True):
                                 _ptr(mesh["rr"]), lm.ctypes.data_as(IP), None if om is None else _ptr(om), npn,
                                 mesh["me"], mesh["n_w"], mesh["l_G"], nmod, _ptr(outs[0]) if product else None,
                                 _ptr(outs[1]), _ptr(outs[2]))
+    if rc != 0:
+        raise ValueError(f"oracle rejected arguments (status {rc})")
+    return tuple(outs)
+
+
+def c_curlh_cross_b_gauss(H, B, mesh, list_mode, product=True):
+    """FP64 restatement of smb_CurlH_cross_B_gauss_sft_par (subroutine_ns_with_m.F90:788-883): returns
+    (V_out, RotV, W), each (l_G*me, 6, nmod) Fortran, V_out = (curl H) x B (zero when product=False)."""
+    H = np.asfortranarray(H, dtype=np.float64)
+    B = np.asfortranarray(B, dtype=np.float64)
+    npn, _, nmod = H.shape
+    ng = mesh["l_G"] * mesh["me"]
+    outs = [np.zeros((ng, 6, nmod), order="F") for _ in range(3)]
+    lm = np.ascontiguousarray(list_mode, dtype=np.int32)
+    IP = ctypes.POINTER(ctypes.c_int)
+    rc = _lib().orc_curlh_cross_b_gauss(_ptr(H), _ptr(B), mesh["jj"].ctypes.data_as(IP), _ptr(mesh["ww"]),
+                                        _ptr(mesh["dw"]), _ptr(mesh["rr"]), lm.ctypes.data_as(IP), npn, mesh["me"],
+                                        mesh["n_w"], mesh["l_G"], nmod, _ptr(outs[0]) if product else None,
+                                        _ptr(outs[1]), _ptr(outs[2]))
+    if rc != 0:
+        raise ValueError(f"oracle rejected arguments (status {rc})")
+    return tuple(outs)
+
+
+def c_ugradc_gauss(V, C, mesh, list_mode, heat=None, conservative=False, product=True):
+    """FP64 restatement of smb_ugradc_gauss_fft_par (subroutine_level_set.F90:434-534: conservative
+    False, heat None; subroutine_temperature_with_T.F90:247-350: conservative, heat per element) and
+    smb_ugradc_gauss_fft_par_conc (subroutine_concentration.F90:243-341: conservative, no heat).
+    Returns (c_out (l_G*me, 2, nmod), Gradc, W, Div, Cgauss); c_out is zero when product=False."""
+    V = np.asfortranarray(V, dtype=np.float64)
+    C = np.asfortranarray(C, dtype=np.float64)
+    npn, _, nmod = V.shape
+    ng = mesh["l_G"] * mesh["me"]
+    outs = [np.zeros((ng, n, nmod), order="F") for n in (2, 6, 6, 2, 2)]
+    lm = np.ascontiguousarray(list_mode, dtype=np.int32)
+    hc = None if heat is None else np.ascontiguousarray(heat, dtype=np.float64)
+    IP = ctypes.POINTER(ctypes.c_int)
+    rc = _lib().orc_ugradc_gauss(_ptr(V), _ptr(C), None if hc is None else _ptr(hc), 1 if conservative else 0,
+                                 mesh["jj"].ctypes.data_as(IP), _ptr(mesh["ww"]), _ptr(mesh["dw"]), _ptr(mesh["rr"]),
+                                 lm.ctypes.data_as(IP), npn, mesh["me"], mesh["n_w"], mesh["l_G"], nmod,
+                                 _ptr(outs[0]) if product else None, *[_ptr(o) for o in outs[1:]])
     if rc != 0:
         raise ValueError(f"oracle rejected arguments (status {rc})")
     return tuple(outs)

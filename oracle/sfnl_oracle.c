@@ -461,3 +461,143 @@ int orc_cross_gauss(const double *V, const int *jj, const double *ww, const doub
   free(W);
   return rc;
 }
+
+/* smb_CurlH_cross_B_gauss_sft_par (subroutine_ns_with_m.F90:788-883): W = B and RotV = curl H at the
+ * Gauss points (loop :812-869, the same curl formulas as the Navier-Stokes caller, no precession), then
+ * FFT_PAR_CROSS_PROD_DCL(RotV, W) with m_max_pad = 3*nmod/2 (:876-878). */
+int orc_curlh_cross_b_gauss(const double *H, const double *B, const int *jj, const double *ww, const double *dw,
+                            const double *rr, const int *list_mode, int np_nodes, int me, int n_w, int l_G, int nmod,
+                            double *Vout, double *RotV_out, double *W_out) {
+  if (np_nodes < 1 || me < 0 || n_w < 1 || l_G < 1 || nmod < 1) return -1;
+  const int ng = l_G * me;
+  double *RotV = (double *)calloc((size_t)ng * 6 * nmod + 1, sizeof(double));
+  double *W = (double *)calloc((size_t)ng * 6 * nmod + 1, sizeof(double));
+  if (!RotV || !W) { free(RotV); free(W); return -4; }
+  for (int m = 0; m < me; ++m)
+    for (int n = 0; n < n_w; ++n)
+      if (jj[n + (size_t)n_w * m] < 1 || jj[n + (size_t)n_w * m] > np_nodes) { free(RotV); free(W); return -2; }
+  for (int i = 0; i < nmod; ++i) {
+    const double mode = (double)list_mode[i];
+    for (int m = 0; m < me; ++m)
+      for (int l = 0; l < l_G; ++l) {
+        const size_t idx = (size_t)m * l_G + l;
+        const double *dwl = dw + (size_t)2 * n_w * (l + (size_t)l_G * m);
+        double ray = 0.0, v[6] = {0, 0, 0, 0, 0, 0}, w[6] = {0, 0, 0, 0, 0, 0};
+        double d1[6] = {0, 0, 0, 0, 0, 0}, d2[6] = {0, 0, 0, 0, 0, 0};
+        for (int n = 0; n < n_w; ++n) {
+          const int node = jj[n + (size_t)n_w * m] - 1;
+          const double wv = ww[n + (size_t)n_w * l];
+          ray += rr[2 * (size_t)node] * wv;
+          for (int k = 0; k < 6; ++k) {
+            const double vs = H[IDX3(node, k, i, np_nodes, 6)];
+            v[k] += vs * wv;
+            d1[k] += vs * dwl[2 * n];
+            d2[k] += vs * dwl[2 * n + 1];
+            w[k] += B[IDX3(node, k, i, np_nodes, 6)] * wv;
+          }
+        }
+        double *R = RotV + idx, *Wo = W + idx;
+#define AT(a, k) a[(size_t)ng * ((k) + 6 * (size_t)i)]
+        for (int k = 0; k < 6; ++k) AT(Wo, k) = w[k];
+        AT(R, 0) = mode / ray * v[5] - d2[2];
+        AT(R, 3) = d2[1] - d1[5];
+        AT(R, 4) = 1 / ray * v[2] + d1[2] - mode / ray * v[1];
+        AT(R, 1) = -mode / ray * v[4] - d2[3];
+        AT(R, 2) = d2[0] - d1[4];
+        AT(R, 5) = 1 / ray * v[3] + d1[3] + mode / ray * v[0];
+#undef AT
+      }
+  }
+  const int pad = 3 * nmod / 2 < nmod ? nmod : 3 * nmod / 2;
+  int rc = Vout ? orc_apply_n(ORC_CROSS, RotV, 6, W, 6, Vout, ng, nmod, 1, ng + 1, pad, 2 * pad - 1) : 0;
+  if (RotV_out) memcpy(RotV_out, RotV, sizeof(double) * (size_t)ng * 6 * nmod);
+  if (W_out) memcpy(W_out, W, sizeof(double) * (size_t)ng * 6 * nmod);
+  free(RotV);
+  free(W);
+  return rc;
+}
+
+/* smb_ugradc_gauss_fft_par (subroutine_level_set.F90:434-534; subroutine_temperature_with_T.F90:247-350
+ * with heat != NULL; smb_ugradc_gauss_fft_par_conc, subroutine_concentration.F90:243-341): W = u,
+ * Gradc = grad c, Div = div u and Cgauss = c at the Gauss points (:469-514), Gradc and Cgauss times
+ * heat(m); c_out = FFT_PAR_DOT_PROD_DCL(Gradc, W) [+ FFT_PAR_PROD_DCL(Div, Cgauss) when conservative,
+ * the two results added as the reference does].  V (np_nodes, 6, nmod), C (np_nodes, 2, nmod), heat (me)
+ * or NULL, Vout (l_G*me, 2, nmod); the operand outputs (l_G*me, 6 | 6 | 2 | 2, nmod) may be NULL. */
+int orc_ugradc_gauss(const double *V, const double *C, const double *heat, int conservative, const int *jj,
+                     const double *ww, const double *dw, const double *rr, const int *list_mode, int np_nodes, int me,
+                     int n_w, int l_G, int nmod, double *Vout, double *Gradc_out, double *W_out, double *Div_out,
+                     double *Cg_out) {
+  if (np_nodes < 1 || me < 0 || n_w < 1 || l_G < 1 || nmod < 1) return -1;
+  const int ng = l_G * me;
+  const size_t n6 = (size_t)ng * 6 * nmod, n2 = (size_t)ng * 2 * nmod;
+  double *G = (double *)calloc(n6 + 1, sizeof(double)), *W = (double *)calloc(n6 + 1, sizeof(double));
+  double *D = (double *)calloc(n2 + 1, sizeof(double)), *Cg = (double *)calloc(n2 + 1, sizeof(double));
+  double *T = (double *)calloc(n2 + 1, sizeof(double));
+  if (!G || !W || !D || !Cg || !T) { free(G); free(W); free(D); free(Cg); free(T); return -4; }
+  int rc = 0;
+  for (int m = 0; m < me && !rc; ++m)
+    for (int n = 0; n < n_w; ++n)
+      if (jj[n + (size_t)n_w * m] < 1 || jj[n + (size_t)n_w * m] > np_nodes) rc = -2;
+  for (int i = 0; i < nmod && !rc; ++i) {
+    const double mode = (double)list_mode[i];
+    for (int m = 0; m < me; ++m)
+      for (int l = 0; l < l_G; ++l) {
+        const size_t idx = (size_t)m * l_G + l;
+        const double *dwl = dw + (size_t)2 * n_w * (l + (size_t)l_G * m);
+        double ray = 0.0, w[6] = {0, 0, 0, 0, 0, 0}, d1[6] = {0, 0, 0, 0, 0, 0}, d2[6] = {0, 0, 0, 0, 0, 0};
+        double cw[2] = {0, 0}, c1[2] = {0, 0}, c2[2] = {0, 0};
+        for (int n = 0; n < n_w; ++n) {
+          const int node = jj[n + (size_t)n_w * m] - 1;
+          const double wv = ww[n + (size_t)n_w * l];
+          ray += rr[2 * (size_t)node] * wv;
+          for (int k = 0; k < 6; ++k) {
+            const double vs = V[IDX3(node, k, i, np_nodes, 6)];
+            w[k] += vs * wv;
+            d1[k] += vs * dwl[2 * n];
+            d2[k] += vs * dwl[2 * n + 1];
+          }
+          for (int k = 0; k < 2; ++k) {
+            const double cs = C[IDX3(node, k, i, np_nodes, 2)];
+            cw[k] += cs * wv;
+            c1[k] += cs * dwl[2 * n];
+            c2[k] += cs * dwl[2 * n + 1];
+          }
+        }
+        const double hc = heat ? heat[m] : 1.0;
+#define AT6(a, k) a[idx + (size_t)ng * ((k) + 6 * (size_t)i)]
+#define AT2(a, k) a[idx + (size_t)ng * ((k) + 2 * (size_t)i)]
+        for (int k = 0; k < 6; ++k) AT6(W, k) = w[k];
+        AT2(D, 0) = d1[0] + w[0] / ray + (mode / ray) * w[3] + d2[4];
+        AT2(D, 1) = d1[1] + w[1] / ray - (mode / ray) * w[2] + d2[5];
+        AT6(G, 0) = c1[0];
+        AT6(G, 1) = c1[1];
+        AT6(G, 2) = mode / ray * cw[1];
+        AT6(G, 3) = -mode / ray * cw[0];
+        AT6(G, 4) = c2[0];
+        AT6(G, 5) = c2[1];
+        AT2(Cg, 0) = cw[0];
+        AT2(Cg, 1) = cw[1];
+        if (heat) {
+          for (int k = 0; k < 6; ++k) AT6(G, k) = hc * AT6(G, k);
+          AT2(Cg, 0) = hc * AT2(Cg, 0);
+          AT2(Cg, 1) = hc * AT2(Cg, 1);
+        }
+#undef AT6
+#undef AT2
+      }
+  }
+  const int pad = 3 * nmod / 2 < nmod ? nmod : 3 * nmod / 2;
+  if (!rc && Vout) {
+    rc = orc_apply_n(ORC_DOT, G, 6, W, 6, Vout, ng, nmod, 1, ng + 1, pad, 2 * pad - 1);
+    if (!rc && conservative) {
+      rc = orc_apply_n(ORC_PROD, D, 2, Cg, 2, T, ng, nmod, 1, ng + 1, pad, 2 * pad - 1);
+      for (size_t t = 0; t < n2; ++t) Vout[t] += T[t];
+    }
+  }
+  if (Gradc_out) memcpy(Gradc_out, G, sizeof(double) * n6);
+  if (W_out) memcpy(W_out, W, sizeof(double) * n6);
+  if (Div_out) memcpy(Div_out, D, sizeof(double) * n2);
+  if (Cg_out) memcpy(Cg_out, Cg, sizeof(double) * n2);
+  free(G); free(W); free(D); free(Cg); free(T);
+  return rc;
+}

@@ -39,6 +39,19 @@ int orc_fft_max_vel(const double *V1, int nsl, int np, int m_max_c, int nb_procs
 int orc_cross_gauss(const double *V, const int *jj, const double *ww, const double *dw, const double *rr,
                     const int *list_mode, const double *omega, int np_nodes, int me, int n_w, int l_G, int nmod,
                     double *Vout, double *RotV_out, double *W_out);
+/* smb_CurlH_cross_B_gauss_sft_par (subroutine_ns_with_m.F90:788-883): (curl H) x B at the Gauss points
+ * from nodal H, B (np_nodes, 6, nmod); outputs as orc_cross_gauss. */
+int orc_curlh_cross_b_gauss(const double *H, const double *B, const int *jj, const double *ww, const double *dw,
+                            const double *rr, const int *list_mode, int np_nodes, int me, int n_w, int l_G, int nmod,
+                            double *Vout, double *RotV_out, double *W_out);
+/* smb_ugradc_gauss_fft_par (subroutine_level_set.F90:434-534, subroutine_temperature_with_T.F90:247-350)
+ * and smb_ugradc_gauss_fft_par_conc (subroutine_concentration.F90:243-341): (heat grad c) . u
+ * [+ div u (heat c) when conservative]; V (np_nodes, 6, nmod), C (np_nodes, 2, nmod), heat (me) or NULL;
+ * Vout (l_G*me, 2, nmod); operand outputs Gradc, W (l_G*me, 6, nmod), Div, Cg (l_G*me, 2, nmod) or NULL. */
+int orc_ugradc_gauss(const double *V, const double *C, const double *heat, int conservative, const int *jj,
+                     const double *ww, const double *dw, const double *rr, const int *list_mode, int np_nodes, int me,
+                     int n_w, int l_G, int nmod, double *Vout, double *Gradc_out, double *W_out, double *Div_out,
+                     double *Cg_out);
 
 #ifdef __cplusplus
 }

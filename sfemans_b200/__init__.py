@@ -93,6 +93,10 @@ _SIGS = {
     "sfnl_real_f64": [_P, _P, _L, _I, _I, _I, _P],
     "sfnl_cross_gauss_f64": [_P] * 8 + [_I] * 6 + [_P, _P],
     "sfnl_smb_cross_prod_gauss": [_P] * 5 + [_I] + [_P] * 3 + [_I] * 6,
+    "sfnl_curlh_cross_b_gauss_f64": [_P] * 8 + [_I] * 6 + [_P, _P],
+    "sfnl_smb_curlh_cross_b_gauss": [_P] * 6 + [_I] + [_P] * 2 + [_I] * 6,
+    "sfnl_ugradc_gauss_f64": [_P] * 3 + [_I] + [_P] * 6 + [_I] * 6 + [_P, _P],
+    "sfnl_smb_ugradc_gauss": [_P] * 3 + [_I] + [_P] * 4 + [_I] + [_P] * 2 + [_I] * 6,
     "sfnl_max_vel_f64": [_P, _P, _L, _I, _I, _I, _P],
     "sfnl_fft_par_real_planes": [_I, _I],
     "sfnl_fft_par_real": [_P, _P] + [_I] * 5,
@@ -300,6 +304,43 @@ def cross_gauss(v, mesh, list_mode, omega=None, m_max_pad=None, out=None, work=N
                                       ptr(mesh["rr"]), ptr(list_mode), None if omega is None else _dptr(omega, "omega"),
                                       _dptr(out, "out"), npn, me, n_w, l_G, nmod, m_max_pad or 0, ptr(work),
                                       _stream(stream)))
+    return out
+
+
+def _gauss_dims(v, mesh):
+    npn, _, nmod = v.shape
+    n_w, me = mesh["jj"].shape
+    return npn, nmod, n_w, me, mesh["ww"].shape[1]
+
+
+def curlh_cross_b_gauss(h, b, mesh, list_mode, m_max_pad=None, out=None, work=None, stream=None):
+    """(curl h) x b at the Gauss points from the nodal h, b (np_nodes, 6, nmod): the Lorentz-force term
+    of smb_CurlH_cross_B_gauss_sft_par (subroutine_ns_with_m.F90:788-883).  ``mesh`` and ``list_mode`` as
+    in :func:`cross_gauss`.  Returns (l_G*me, 6, nmod)."""
+    npn, nmod, n_w, me, l_G = _gauss_dims(h, mesh)
+    if out is None:
+        out = fortran_empty(l_G * me, 6, nmod, device=h.device)
+    ptr = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    _check(lib().sfnl_curlh_cross_b_gauss_f64(_dptr(h, "h"), _dptr(b, "b"), ptr(mesh["jj"]), ptr(mesh["ww"]),
+                                              ptr(mesh["dw"]), ptr(mesh["rr"]), ptr(list_mode), _dptr(out, "out"),
+                                              npn, me, n_w, l_G, nmod, m_max_pad or 0, ptr(work), _stream(stream)))
+    return out
+
+
+def ugradc_gauss(v, c, mesh, list_mode, heat=None, conservative=False, m_max_pad=None, out=None, work=None,
+                 stream=None):
+    """(heat grad c) . v [+ div v (heat c) when conservative] at the Gauss points from the nodal velocity
+    v (np_nodes, 6, nmod) and scalar c (np_nodes, 2, nmod): the advection term of smb_ugradc_gauss_fft_par
+    (level set: conservative False; temperature: conservative, heat = the heat capacity of each element;
+    concentration: conservative).  Returns (l_G*me, 2, nmod)."""
+    npn, nmod, n_w, me, l_G = _gauss_dims(v, mesh)
+    if out is None:
+        out = fortran_empty(l_G * me, 2, nmod, device=v.device)
+    ptr = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    _check(lib().sfnl_ugradc_gauss_f64(_dptr(v, "v"), _dptr(c, "c"), ptr(heat), 1 if conservative else 0,
+                                       ptr(mesh["jj"]), ptr(mesh["ww"]), ptr(mesh["dw"]), ptr(mesh["rr"]),
+                                       ptr(list_mode), _dptr(out, "out"), npn, me, n_w, l_G, nmod, m_max_pad or 0,
+                                       ptr(work), _stream(stream)))
     return out
 
 
@@ -535,3 +576,77 @@ def smb_cross_prod_gauss_sft_par(communicator, mesh, list_mode, V_in, V_out=None
                                            rr.shape[0], _host_ptr(lm), None if om is None else _host_ptr(om),
                                            _host_ptr(V_out), npn, me, n_w, l_G, nmod, 1))
     return V_out
+
+
+def _host_mesh(mesh, list_mode):
+    import numpy as np
+
+    jj = np.asfortranarray(mesh["jj"], dtype=np.int32)
+    ww = np.asfortranarray(mesh["ww"], dtype=np.float64)
+    dw = np.asfortranarray(mesh["dw"], dtype=np.float64)
+    rr = np.asfortranarray(mesh["rr"], dtype=np.float64)
+    return jj, ww, dw, rr, np.ascontiguousarray(list_mode, dtype=np.int32)
+
+
+def smb_CurlH_cross_B_gauss_sft_par(communicator, mesh, list_mode, V_in, W_in, V_out=None):
+    """The Lorentz force (curl H) x B at the Gauss points (subroutine_ns_with_m.F90:788-883) on host
+    arrays: V_in = H, W_in = B (np_nodes, 6, nmod).  Returns V_out (l_G*me, 6, nmod)."""
+    import numpy as np
+
+    if communicator is not None:
+        raise SfnlError(-4, "one GPU holds all modes: the Gauss-point entry runs on one Fourier rank")
+    V_in = np.asfortranarray(V_in, dtype=np.float64)
+    W_in = np.asfortranarray(W_in, dtype=np.float64)
+    npn, _, nmod = V_in.shape
+    jj, ww, dw, rr, lm = _host_mesh(mesh, list_mode)
+    n_w, me = jj.shape
+    l_G = ww.shape[1]
+    if V_out is None:
+        V_out = np.zeros((l_G * me, 6, nmod), order="F")
+    _check(lib().sfnl_smb_curlh_cross_b_gauss(_host_ptr(V_in), _host_ptr(W_in), _host_ptr(jj), _host_ptr(ww),
+                                              _host_ptr(dw), _host_ptr(rr), rr.shape[0], _host_ptr(lm),
+                                              _host_ptr(V_out), npn, me, n_w, l_G, nmod, 1))
+    return V_out
+
+
+def _host_ugradc(communicator, mesh, list_mode, V_in, c_in, c_out, heat, conservative):
+    import numpy as np
+
+    if communicator is not None:
+        raise SfnlError(-4, "one GPU holds all modes: the Gauss-point entry runs on one Fourier rank")
+    V_in = np.asfortranarray(V_in, dtype=np.float64)
+    c_in = np.asfortranarray(c_in, dtype=np.float64)
+    npn, _, nmod = V_in.shape
+    jj, ww, dw, rr, lm = _host_mesh(mesh, list_mode)
+    n_w, me = jj.shape
+    l_G = ww.shape[1]
+    hc = None if heat is None else np.ascontiguousarray(heat, dtype=np.float64)
+    if hc is not None and hc.shape[0] < me:
+        raise SfnlError(-1, "heat_capa_in holds fewer values than elements")
+    if c_out is None:
+        c_out = np.zeros((l_G * me, 2, nmod), order="F")
+    _check(lib().sfnl_smb_ugradc_gauss(_host_ptr(V_in), _host_ptr(c_in), None if hc is None else _host_ptr(hc),
+                                       1 if conservative else 0, _host_ptr(jj), _host_ptr(ww), _host_ptr(dw),
+                                       _host_ptr(rr), rr.shape[0], _host_ptr(lm), _host_ptr(c_out), npn, me, n_w,
+                                       l_G, nmod, 1))
+    return c_out
+
+
+def smb_ugradc_gauss_fft_par(communicator, mesh, list_mode, V_in, c_in, nb_procs=1, c_out=None):
+    """The level-set advection term grad c . u at the Gauss points (subroutine_level_set.F90:434-534)
+    on host arrays: V_in (np_nodes, 6, nmod), c_in (np_nodes, 2, nmod).  Returns c_out (l_G*me, 2, nmod)."""
+    if nb_procs != 1:
+        raise SfnlError(-4, "one GPU holds all modes: nb_procs must be 1")
+    return _host_ugradc(communicator, mesh, list_mode, V_in, c_in, c_out, None, False)
+
+
+def smb_ugradc_gauss_fft_par_temperature(communicator, mesh, list_mode, heat_capa_in, V_in, c_in, c_out=None):
+    """The temperature equation's smb_ugradc_gauss_fft_par (subroutine_temperature_with_T.F90:247-350):
+    (C grad T) . u + div u (C T), C = heat_capa_in(m) of each element."""
+    return _host_ugradc(communicator, mesh, list_mode, V_in, c_in, c_out, heat_capa_in, True)
+
+
+def smb_ugradc_gauss_fft_par_conc(communicator, mesh, list_mode, V_in, c_in, c_out=None):
+    """The concentration equation's advection term grad c . u + c div u
+    (subroutine_concentration.F90:243-341)."""
+    return _host_ugradc(communicator, mesh, list_mode, V_in, c_in, c_out, None, True)

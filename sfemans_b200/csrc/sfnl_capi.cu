@@ -742,9 +742,18 @@ static int check_gauss(int np_nodes, int me, int n_w, int l_G, int nmod) {
   return SFNL_OK;
 }
 
-int sfnl_cross_gauss_f64(const double *v, const int *jj, const double *ww, const double *dw, const double *rr,
-                         const int *list_mode, const double *omega, double *out, int np_nodes, int me, int n_w,
-                         int l_G, int nmod, int m_max_pad, double *work, sfnl_stream_t stream) {
+// Doubles of the Gauss-point operands of one caller.
+static size_t gauss_operand_doubles(int kind, int conservative, int64_t ng, int nmod) {
+  const size_t o6 = (size_t)ng * 6 * nmod, o2 = (size_t)ng * 2 * nmod;
+  return 2 * o6 + (kind == sfnl::GK_ADVECT && conservative ? 2 * o2 : 0);
+}
+
+// A Gauss-point caller on device arrays: the operands into `work` (or the library's per-device buffer,
+// held for the whole call), then the product on the FAST form.
+static int gauss_product(int kind, const double *v, const double *v2, const double *omega, const double *heat,
+                         int conservative, const int *jj, const double *ww, const double *dw, const double *rr,
+                         const int *list_mode, double *out, int np_nodes, int me, int n_w, int l_G, int nmod,
+                         int m_max_pad, double *work, sfnl_stream_t stream) {
   int rc = check_gauss(np_nodes, me, n_w, l_G, nmod);
   if (rc) return rc;
   const int pad = m_max_pad > 0 ? m_max_pad : (3 * nmod / 2 < nmod ? nmod : 3 * nmod / 2);
@@ -752,42 +761,66 @@ int sfnl_cross_gauss_f64(const double *v, const int *jj, const double *ww, const
   int N = 0;
   if ((rc = check_common(ng, nmod, pad, 0, 1, &N))) return rc;
   if (ng == 0) return SFNL_OK;
-  if (!v || !jj || !ww || !dw || !rr || !list_mode || !out) return set_error(SFNL_ERR_ARG, "null array");
+  if (!v || !jj || !ww || !dw || !rr || !list_mode || !out || (kind != GK_NS && !v2))
+    return set_error(SFNL_ERR_ARG, "null array");
   cudaStream_t st = as_stream(stream);
-  const size_t opnd = (size_t)ng * 6 * nmod;  // doubles of RotV (and of W)
-  double *rotv = work;
-  if (!rotv) {
+  std::unique_lock<std::mutex> lk;
+  double *wk = work;
+  if (!wk) {
     DevState *s = dev_state();
     if (!s) return set_error(SFNL_ERR_CUDA, "no current device");
-    std::lock_guard<std::mutex> lk(s->mu);
-    if ((rc = grow_gwork(s, 2 * opnd * sizeof(double)))) return rc;
-    rotv = reinterpret_cast<double *>(s->gwork);
+    lk = std::unique_lock<std::mutex>(s->mu);
+    if ((rc = grow_gwork(s, gauss_operand_doubles(kind, conservative, ng, nmod) * sizeof(double)))) return rc;
+    wk = reinterpret_cast<double *>(s->gwork);
   }
-  GaussArgs ga{v, omega, ww, dw, rr, jj, list_mode, np_nodes, me, n_w, l_G, nmod};
-  if ((rc = launch_gauss_eval(ga, rotv, rotv + opnd, st))) return rc;
+  const size_t o6 = (size_t)ng * 6 * nmod, o2 = (size_t)ng * 2 * nmod;
+  double *g0 = wk, *g1 = wk + o6;
+  double *g2 = kind == GK_ADVECT && conservative ? wk + 2 * o6 : nullptr, *g3 = g2 ? g2 + o2 : nullptr;
+  GaussArgs ga{v, kind == GK_NS ? omega : nullptr, ww, dw, rr, jj, list_mode, np_nodes, me, n_w, l_G, nmod,
+               v2, kind == GK_ADVECT ? heat : nullptr};
+  if ((rc = launch_gauss_eval(ga, kind, g0, g1, g2, g3, st))) return rc;
   ProgArgs pa;
-  if ((rc = build_product(OP_CROSS, rotv, rotv + opnd, out, ng, nmod, N, &pa))) return rc;
+  if (kind != GK_ADVECT) {
+    if ((rc = build_product(OP_CROSS, g0, g1, out, ng, nmod, N, &pa))) return rc;  // RotV x W
+  } else if (!conservative) {
+    if ((rc = build_product(OP_DOT, g0, g1, out, ng, nmod, N, &pa))) return rc;    // Gradc . W
+  } else {  // Gradc . W + Div Cgauss, analysed once
+    pa = make_args(OP_ADVECT, ng, nmod, N, 1);
+    for (int k = 0; k < 3; ++k) {
+      set_in(pa, k, g0, ng, 6, k, nmod, false);
+      set_in(pa, 3 + k, g1, ng, 6, k, nmod, false);
+    }
+    set_in(pa, 6, g2, ng, 2, 0, nmod, false);
+    set_in(pa, 7, g3, ng, 2, 0, nmod, false);
+    set_out(pa, 0, out, ng, 2, 0, nmod, false);
+  }
   return run_fp64(pa, SFNL_ALGO_AUTO, N, st);
 }
 
-int sfnl_smb_cross_prod_gauss(const double *V_in, const int *jj, const double *ww, const double *dw, const double *rr,
-                              int k_d, const int *list_mode, const double *omega, double *V_out, int np_nodes, int me,
-                              int n_w, int l_G, int nmod, int nb_procs) {
+// A Gauss-point caller on host arrays (the reference signatures): every array copied to the device,
+// the device caller, the result copied back.
+static int host_gauss(int kind, const double *V_in, const double *V2_in, int nslot2, const double *omega,
+                      const double *heat, int conservative, const int *jj, const double *ww, const double *dw,
+                      const double *rr, int k_d, const int *list_mode, double *V_out, int nslot_out, int np_nodes,
+                      int me, int n_w, int l_G, int nmod, int nb_procs) {
   int rc = check_gauss(np_nodes, me, n_w, l_G, nmod);
   if (rc) return rc;
   if (k_d != 2) return set_error(SFNL_ERR_UNSUPPORTED, "meridian meshes only (k_d == 2)");
   if (nb_procs != 1) return set_error(SFNL_ERR_UNSUPPORTED, "one GPU holds all modes: nb_procs must be 1");
-  if (!V_in || !jj || !ww || !dw || !rr || !list_mode || !V_out) return set_error(SFNL_ERR_ARG, "null array");
+  if (!V_in || !jj || !ww || !dw || !rr || !list_mode || !V_out || (nslot2 && !V2_in))
+    return set_error(SFNL_ERR_ARG, "null array");
   for (int64_t t = 0; t < (int64_t)n_w * me; ++t)
     if (jj[t] < 1 || jj[t] > np_nodes) return set_error(SFNL_ERR_ARG, "jj holds a node number outside 1..np_nodes");
   using clk = std::chrono::steady_clock;
   const auto t0 = clk::now();
   const int64_t ng = (int64_t)l_G * me;
-  const size_t nv = (size_t)np_nodes * 6 * nmod, nout = (size_t)ng * 6 * nmod;
+  const size_t nv = (size_t)np_nodes * 6 * nmod, nv2 = (size_t)np_nodes * nslot2 * nmod;
+  const size_t nout = (size_t)ng * nslot_out * nmod, nwork = gauss_operand_doubles(kind, conservative, ng, nmod);
   const size_t nww = (size_t)n_w * l_G, ndw = (size_t)2 * n_w * l_G * me, nrr = (size_t)2 * np_nodes;
   auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
-  const size_t bytes = al(8 * nv) * (omega ? 2 : 1) + al(8 * nout) * 3 + al(8 * nww) + al(8 * ndw) + al(8 * nrr) +
-                       al(4 * (size_t)n_w * me) + al(4 * (size_t)nmod);
+  const size_t bytes = al(8 * nv) * (omega ? 2 : 1) + al(8 * nv2) + al(8 * (size_t)me) + al(8 * nout) +
+                       al(8 * nwork) + al(8 * nww) + al(8 * ndw) + al(8 * nrr) + al(4 * (size_t)n_w * me) +
+                       al(4 * (size_t)nmod);
   DevState *s = dev_state();
   if (!s) return set_error(SFNL_ERR_CUDA, "no current device");
   std::lock_guard<std::mutex> lk(s->mu);
@@ -795,20 +828,23 @@ int sfnl_smb_cross_prod_gauss(const double *V_in, const int *jj, const double *w
   char *q = s->gwork;
   auto take = [&](size_t b) { char *r = q; q += al(b); return r; };
   double *d_v = (double *)take(8 * nv), *d_om = omega ? (double *)take(8 * nv) : nullptr;
-  double *d_out = (double *)take(8 * nout), *d_work = (double *)take(16 * nout);
+  double *d_v2 = nslot2 ? (double *)take(8 * nv2) : nullptr, *d_heat = heat ? (double *)take(8 * (size_t)me) : nullptr;
+  double *d_out = (double *)take(8 * nout), *d_work = (double *)take(8 * nwork);
   double *d_ww = (double *)take(8 * nww), *d_dw = (double *)take(8 * ndw), *d_rr = (double *)take(8 * nrr);
   int *d_jj = (int *)take(4 * (size_t)n_w * me), *d_lm = (int *)take(4 * (size_t)nmod);
   cudaStream_t st = nullptr;
   bool ok = cudaMemcpyAsync(d_v, V_in, 8 * nv, cudaMemcpyHostToDevice, st) == cudaSuccess &&
             (!omega || cudaMemcpyAsync(d_om, omega, 8 * nv, cudaMemcpyHostToDevice, st) == cudaSuccess) &&
+            (!nslot2 || cudaMemcpyAsync(d_v2, V2_in, 8 * nv2, cudaMemcpyHostToDevice, st) == cudaSuccess) &&
+            (!heat || cudaMemcpyAsync(d_heat, heat, 8 * (size_t)me, cudaMemcpyHostToDevice, st) == cudaSuccess) &&
             cudaMemcpyAsync(d_ww, ww, 8 * nww, cudaMemcpyHostToDevice, st) == cudaSuccess &&
             cudaMemcpyAsync(d_dw, dw, 8 * ndw, cudaMemcpyHostToDevice, st) == cudaSuccess &&
             cudaMemcpyAsync(d_rr, rr, 8 * nrr, cudaMemcpyHostToDevice, st) == cudaSuccess &&
             cudaMemcpyAsync(d_jj, jj, 4 * (size_t)n_w * me, cudaMemcpyHostToDevice, st) == cudaSuccess &&
             cudaMemcpyAsync(d_lm, list_mode, 4 * (size_t)nmod, cudaMemcpyHostToDevice, st) == cudaSuccess;
   if (!ok) return set_error(SFNL_ERR_CUDA, "host-to-device copy failed");
-  rc = sfnl_cross_gauss_f64(d_v, d_jj, d_ww, d_dw, d_rr, d_lm, d_om, d_out, np_nodes, me, n_w, l_G, nmod, 0, d_work,
-                            reinterpret_cast<sfnl_stream_t>(st));
+  rc = gauss_product(kind, d_v, d_v2, d_om, d_heat, conservative, d_jj, d_ww, d_dw, d_rr, d_lm, d_out, np_nodes, me,
+                     n_w, l_G, nmod, 0, d_work, reinterpret_cast<sfnl_stream_t>(st));
   if (rc) return rc;
   if (cudaMemcpyAsync(V_out, d_out, 8 * nout, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
@@ -817,6 +853,52 @@ int sfnl_smb_cross_prod_gauss(const double *V_in, const int *jj, const double *w
   g_host_timing[1] = std::chrono::duration<double>(clk::now() - t0).count();
   g_host_timing[2] = 0.0;
   return SFNL_OK;
+}
+
+int sfnl_cross_gauss_f64(const double *v, const int *jj, const double *ww, const double *dw, const double *rr,
+                         const int *list_mode, const double *omega, double *out, int np_nodes, int me, int n_w,
+                         int l_G, int nmod, int m_max_pad, double *work, sfnl_stream_t stream) {
+  return gauss_product(GK_NS, v, nullptr, omega, nullptr, 0, jj, ww, dw, rr, list_mode, out, np_nodes, me, n_w, l_G,
+                       nmod, m_max_pad, work, stream);
+}
+
+int sfnl_smb_cross_prod_gauss(const double *V_in, const int *jj, const double *ww, const double *dw, const double *rr,
+                              int k_d, const int *list_mode, const double *omega, double *V_out, int np_nodes, int me,
+                              int n_w, int l_G, int nmod, int nb_procs) {
+  return host_gauss(GK_NS, V_in, nullptr, 0, omega, nullptr, 0, jj, ww, dw, rr, k_d, list_mode, V_out, 6, np_nodes,
+                    me, n_w, l_G, nmod, nb_procs);
+}
+
+int sfnl_curlh_cross_b_gauss_f64(const double *h, const double *b, const int *jj, const double *ww, const double *dw,
+                                 const double *rr, const int *list_mode, double *out, int np_nodes, int me, int n_w,
+                                 int l_G, int nmod, int m_max_pad, double *work, sfnl_stream_t stream) {
+  return gauss_product(GK_LORENTZ, h, b, nullptr, nullptr, 0, jj, ww, dw, rr, list_mode, out, np_nodes, me, n_w, l_G,
+                       nmod, m_max_pad, work, stream);
+}
+
+int sfnl_smb_curlh_cross_b_gauss(const double *V_in, const double *W_in, const int *jj, const double *ww,
+                                 const double *dw, const double *rr, int k_d, const int *list_mode, double *V_out,
+                                 int np_nodes, int me, int n_w, int l_G, int nmod, int nb_procs) {
+  return host_gauss(GK_LORENTZ, V_in, W_in, 6, nullptr, nullptr, 0, jj, ww, dw, rr, k_d, list_mode, V_out, 6,
+                    np_nodes, me, n_w, l_G, nmod, nb_procs);
+}
+
+int sfnl_ugradc_gauss_f64(const double *v, const double *c, const double *heat, int conservative, const int *jj,
+                          const double *ww, const double *dw, const double *rr, const int *list_mode, double *out,
+                          int np_nodes, int me, int n_w, int l_G, int nmod, int m_max_pad, double *work,
+                          sfnl_stream_t stream) {
+  if (conservative != 0 && conservative != 1) return set_error(SFNL_ERR_ARG, "conservative must be 0 or 1");
+  return gauss_product(GK_ADVECT, v, c, nullptr, heat, conservative, jj, ww, dw, rr, list_mode, out, np_nodes, me,
+                       n_w, l_G, nmod, m_max_pad, work, stream);
+}
+
+int sfnl_smb_ugradc_gauss(const double *V_in, const double *c_in, const double *heat_capa, int conservative,
+                          const int *jj, const double *ww, const double *dw, const double *rr, int k_d,
+                          const int *list_mode, double *c_out, int np_nodes, int me, int n_w, int l_G, int nmod,
+                          int nb_procs) {
+  if (conservative != 0 && conservative != 1) return set_error(SFNL_ERR_ARG, "conservative must be 0 or 1");
+  return host_gauss(GK_ADVECT, V_in, c_in, 2, nullptr, heat_capa, conservative, jj, ww, dw, rr, k_d, list_mode,
+                    c_out, 2, np_nodes, me, n_w, l_G, nmod, nb_procs);
 }
 
 int sfnl_product_f64_host(int op, const double *a, const double *b, double *out, int64_t np, int m_max, int m_max_pad,

@@ -1097,6 +1097,10 @@ int decompose_program(int op, std::vector<Elem> &seq) {
       add(EK_CROSS, {9, 10, 11, 6, 7, 8}, {6, 7, 8}, 0, 0);   // j x b
       add(EK_DOT, {0, 1, 2, 12, 13, 14}, {9}, 0, 0);          // u . gradT
       break;
+    case OP_ADVECT:  // [g, w, d, c]
+      add(EK_DOT, {0, 1, 2, 3, 4, 5}, {0}, 0, 0);            // g . w
+      add(EK_PROD, {6, 7}, {0}, 0, 1);                       // + d c
+      break;
     case OP_CROSS_JVP:  // [u, w, du, dw]
       add(EK_CROSS, {6, 7, 8, 3, 4, 5}, {0, 1, 2}, 0, 0);     // du x w
       add(EK_CROSS, {0, 1, 2, 9, 10, 11}, {0, 1, 2}, 0, 1);   // + u x dw

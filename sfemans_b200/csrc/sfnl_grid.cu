@@ -150,6 +150,7 @@ int launch_grid(const ProgArgs &a, cudaStream_t st) {
     case OP_SVDIV: return launch_grid_op<OP_SVDIV>(a, st);
     case OP_TENSOR: return launch_grid_op<OP_TENSOR>(a, st);
     case OP_TENSION: return launch_grid_op<OP_TENSION>(a, st);
+    case OP_ADVECT: return launch_grid_op<OP_ADVECT>(a, st);
   }
   return set_error(SFNL_ERR_ARG, "unknown program");
 }

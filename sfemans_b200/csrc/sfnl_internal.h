@@ -33,16 +33,22 @@ int launch_real(const double *v, double *out, int64_t np, int nslot, int m, int 
 int launch_max_vel(const double *v, double *vmax, int64_t np, int nslot, int m, int N, cudaStream_t st);
 int launch_point_max_vel(const double *v, double *pmax, int64_t np, int nslot, int m, int N, cudaStream_t st);
 
-// Operands of the Navier-Stokes cross product at the Gauss points (sfnl_gauss.cu): device arrays of
-// the mesh (jj 1-based (n_w, me), ww (n_w, l_G), dw (2, n_w, l_G, me), rr (2, np_nodes)), the nodal
-// velocity v and rotation omega (np_nodes, 6, nmod; omega may be null) and the modes list_mode (nmod).
+// Operands of the Gauss-point callers (sfnl_gauss.cu): device arrays of the mesh (jj 1-based (n_w, me),
+// ww (n_w, l_G), dw (2, n_w, l_G, me), rr (2, np_nodes)), the nodal vector field v (np_nodes, 6, nmod),
+// the precession rotation omega (same shape, GK_NS, may be null), the second nodal field v2 (GK_LORENTZ:
+// B (np_nodes, 6, nmod); GK_ADVECT: the scalar c (np_nodes, 2, nmod)), the heat capacity of each element
+// heat (me, GK_ADVECT, may be null) and the modes list_mode (nmod).
+enum { GK_NS = 0, GK_LORENTZ = 1, GK_ADVECT = 2 };
 struct GaussArgs {
   const double *v, *omega, *ww, *dw, *rr;
   const int *jj, *list_mode;
   int np_nodes, me, n_w, l_G, nmod;
+  const double *v2, *heat;
 };
-// rotv, w: (l_G*me, 6, nmod) outputs (RotV + 2 Om, W).
-int launch_gauss_eval(const GaussArgs &a, double *rotv, double *w, cudaStream_t st);
+// Outputs, each (l_G*me, nslot, nmod): GK_NS o0 = RotV + 2 Om, o1 = W (6 slots); GK_LORENTZ o0 = curl v,
+// o1 = v2 (6 slots); GK_ADVECT o0 = Gradc, o1 = W (6 slots), o2 = Div, o3 = Cgauss (2 slots; both
+// null: no conservative term).
+int launch_gauss_eval(const GaussArgs &a, int kind, double *o0, double *o1, double *o2, double *o3, cudaStream_t st);
 
 // Elementary programs: cross (6 -> 3), dot (6 -> 1), product (2 -> 1),
 // scalar x vector (4 -> 3) and tensor (6 -> 9).  Every bilinear program of

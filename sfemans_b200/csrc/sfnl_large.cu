@@ -320,6 +320,7 @@ int launch_large_prod_op(int op, const LargeArgs &la, cudaStream_t st) {
     case OP_MHD_VJP: return launch_large_prod_all<OP_MHD_VJP>(la, st);
     case OP_SVECT: return launch_large_prod_all<OP_SVECT>(la, st);
     case OP_TENSOR: return launch_large_prod_all<OP_TENSOR>(la, st);
+    case OP_ADVECT: return launch_large_prod_all<OP_ADVECT>(la, st);
   }
   return set_error(SFNL_ERR_ARG, "large-m FAST form: program not bilinear");
 }

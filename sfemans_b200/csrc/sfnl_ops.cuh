@@ -11,7 +11,10 @@
 // ...), :449-451 (dot), :617 (scalar product), :786 (quotient), :1150-1157
 // (scalar x vector, vector / scalar) and :1676-1706 (tensor u_k v_l, and the
 // tension form u_k v_l / (|v| + 1e-14) - |v| delta_kl), plus the
-// linearisations and transposes used by the JVP/VJP entry points.
+// linearisations and transposes used by the JVP/VJP entry points and the
+// advection term of the scalar equations (grad c . u + c div u,
+// SOURCES/SIMULATION/subroutine_temperature_with_T.F90:339-342: a dot product
+// and a product whose analyses the reference adds).
 #pragma once
 #include <cstdint>
 
@@ -31,7 +34,8 @@ enum Op : int {
   OP_SVDIV = 10,    // [v(3), s]                      -> [v / s] (3)
   OP_TENSOR = 11,   // [u(3), v(3)]                   -> [u_k v_l] (9, o = 3k + l)
   OP_TENSION = 12,  // [u(3), v(3)]                   -> [u_k v_l / (|v| + 1e-14) - |v| delta_kl] (9)
-  OP_COUNT = 13
+  OP_ADVECT = 13,   // [g(3), w(3), d, c] (8)         -> [g . w + d c] (advection of a scalar, conservative form)
+  OP_COUNT = 14
 };
 
 constexpr int kMaxIn = 18;
@@ -40,12 +44,12 @@ constexpr int kMaxOut = 10;
 __host__ __device__ constexpr int op_nin(int op) {
   return op == OP_CROSS ? 6 : op == OP_DOT ? 6 : op == OP_PROD ? 2 : op == OP_BUNDLE ? 15
        : op == OP_CROSS_JVP ? 12 : op == OP_CROSS_VJP ? 9 : op == OP_MHD_JVP ? 18 : op == OP_MHD_VJP ? 15
-       : op == OP_DIV ? 2 : op == OP_SVECT || op == OP_SVDIV ? 4 : 6;
+       : op == OP_DIV ? 2 : op == OP_SVECT || op == OP_SVDIV ? 4 : op == OP_ADVECT ? 8 : 6;
 }
 __host__ __device__ constexpr int op_nout(int op) {
   return op == OP_CROSS ? 3 : op == OP_DOT ? 1 : op == OP_PROD ? 1 : op == OP_BUNDLE ? 10
        : op == OP_CROSS_JVP ? 3 : op == OP_CROSS_VJP ? 6 : op == OP_MHD_JVP ? 6 : op == OP_MHD_VJP ? 9
-       : op == OP_DIV ? 1 : op == OP_SVECT || op == OP_SVDIV ? 3 : 9;
+       : op == OP_DIV ? 1 : op == OP_SVECT || op == OP_SVDIV ? 3 : op == OP_ADVECT ? 1 : 9;
 }
 // Programs whose result is the exact truncated product on any alias-free grid
 // (bilinear in the synthesised fields); the quotients and the tension tensor
@@ -117,6 +121,8 @@ __device__ __forceinline__ void apply_op(const T *x, T *y) {
     for (int k = 0; k < 3; ++k)
 #pragma unroll
       for (int l = 0; l < 3; ++l) y[3 * k + l] = x[k] * x[3 + l];
+  } else if constexpr (OP == OP_ADVECT) {
+    y[0] = x[0] * x[3] + x[1] * x[4] + x[2] * x[5] + x[6] * x[7];
   } else if constexpr (OP == OP_TENSION) {
     const T nrm = sqrt(x[3] * x[3] + x[4] * x[4] + x[5] * x[5]);
     const T den = nrm + T(1.0e-14);

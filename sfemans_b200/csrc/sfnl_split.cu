@@ -836,7 +836,7 @@ int run_split_program(const ProgArgs &pa, int split, const int *in_map, const in
 }  // namespace
 
 bool split_supported(int op, int m) {
-  if (m < 1 || m > 64 || !op_bilinear(op)) return false;
+  if (m < 1 || m > 64 || !op_bilinear(op) || op == OP_ADVECT) return false;
   SGeo g;
   return make_sgeo(m, 8, 16, &g) && make_sgeo(m, 16, 8, &g) && make_sgeo(m, 32, 4, &g);
 }

@@ -317,7 +317,8 @@ MODULE sfemans_gauss_gpu
   USE input_data
   IMPLICIT NONE
   PRIVATE
-  PUBLIC :: smb_cross_prod_gauss_sft_par_gpu
+  PUBLIC :: smb_cross_prod_gauss_sft_par_gpu, smb_CurlH_cross_B_gauss_sft_par_gpu, smb_ugradc_gauss_fft_par_gpu, &
+       smb_ugradc_gauss_fft_par_temperature_gpu, smb_ugradc_gauss_fft_par_conc_gpu
 
   INTERFACE
      FUNCTION sfnl_smb_cross_prod_gauss(V_in, jj, ww, dw, rr, k_d, list_mode, omega, V_out, np_nodes, me, n_w, &
@@ -330,6 +331,25 @@ MODULE sfemans_gauss_gpu
        INTEGER(C_INT), VALUE :: k_d, np_nodes, me, n_w, l_G, nmod, nb_procs
        INTEGER(C_INT)        :: rc
      END FUNCTION sfnl_smb_cross_prod_gauss
+     FUNCTION sfnl_smb_curlh_cross_b_gauss(V_in, W_in, jj, ww, dw, rr, k_d, list_mode, V_out, np_nodes, me, n_w, &
+          l_G, nmod, nb_procs) RESULT(rc) BIND(C, NAME='sfnl_smb_curlh_cross_b_gauss')
+       IMPORT :: C_INT, C_DOUBLE
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(IN)  :: V_in, W_in, ww, dw, rr
+       INTEGER(C_INT), DIMENSION(*), INTENT(IN)  :: jj, list_mode
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(OUT) :: V_out
+       INTEGER(C_INT), VALUE :: k_d, np_nodes, me, n_w, l_G, nmod, nb_procs
+       INTEGER(C_INT)        :: rc
+     END FUNCTION sfnl_smb_curlh_cross_b_gauss
+     FUNCTION sfnl_smb_ugradc_gauss(V_in, c_in, heat_capa, conservative, jj, ww, dw, rr, k_d, list_mode, c_out, &
+          np_nodes, me, n_w, l_G, nmod, nb_procs) RESULT(rc) BIND(C, NAME='sfnl_smb_ugradc_gauss')
+       IMPORT :: C_INT, C_DOUBLE, C_PTR
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(IN)  :: V_in, c_in, ww, dw, rr
+       TYPE(C_PTR), VALUE                        :: heat_capa
+       INTEGER(C_INT), DIMENSION(*), INTENT(IN)  :: jj, list_mode
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(OUT) :: c_out
+       INTEGER(C_INT), VALUE :: conservative, k_d, np_nodes, me, n_w, l_G, nmod, nb_procs
+       INTEGER(C_INT)        :: rc
+     END FUNCTION sfnl_smb_ugradc_gauss
   END INTERFACE
 
 CONTAINS
@@ -373,5 +393,86 @@ CONTAINS
     END IF
     IF (ALLOCATED(omega)) DEALLOCATE(omega)
   END SUBROUTINE smb_cross_prod_gauss_sft_par_gpu
+
+  ! The Lorentz force (curl H) x B of subroutine_ns_with_m.F90:788-883 (V_in = H, W_in = B).
+  SUBROUTINE smb_CurlH_cross_B_gauss_sft_par_gpu(communicator, mesh, list_mode, V_in, W_in, V_out)
+    TYPE(mesh_type),                            INTENT(IN)  :: mesh
+    INTEGER,      DIMENSION(:),                 INTENT(IN)  :: list_mode
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(IN)  :: V_in, W_in
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS              :: V_out
+    MPI_Comm :: communicator
+    INTEGER(C_INT) :: rc
+    INTEGER :: nproc, code
+    CALL MPI_COMM_SIZE(communicator, nproc, code)
+    rc = sfnl_smb_curlh_cross_b_gauss(V_in, W_in, INT(mesh%jj, C_INT), mesh%gauss%ww, mesh%gauss%dw, mesh%rr, &
+         INT(SIZE(mesh%rr,1), C_INT), INT(list_mode, C_INT), V_out, INT(mesh%np, C_INT), INT(mesh%me, C_INT), &
+         INT(mesh%gauss%n_w, C_INT), INT(mesh%gauss%l_G, C_INT), INT(SIZE(list_mode), C_INT), INT(nproc, C_INT))
+    IF (rc /= 0) THEN
+       WRITE(*,*) ' BUG in smb_CurlH_cross_B_gauss_sft_par_gpu (status ', rc, ')'
+       STOP
+    END IF
+  END SUBROUTINE smb_CurlH_cross_B_gauss_sft_par_gpu
+
+  ! The three advection callers share one entry: heat_capa (C_NULL_PTR: none) and the conservative term.
+  ! All mesh%me elements are evaluated (the reference loops over mesh%dom_me, equal to me on these meshes).
+  SUBROUTINE ugradc_gpu(mesh, list_mode, V_in, c_in, c_out, heat_ptr, conservative, nproc, who)
+    TYPE(mesh_type),                            INTENT(IN)  :: mesh
+    INTEGER,      DIMENSION(:),                 INTENT(IN)  :: list_mode
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(IN)  :: V_in, c_in
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(OUT) :: c_out
+    TYPE(C_PTR),  INTENT(IN) :: heat_ptr
+    INTEGER,      INTENT(IN) :: conservative, nproc
+    CHARACTER(*), INTENT(IN) :: who
+    INTEGER(C_INT) :: rc
+    rc = sfnl_smb_ugradc_gauss(V_in, c_in, heat_ptr, INT(conservative, C_INT), INT(mesh%jj, C_INT), mesh%gauss%ww, &
+         mesh%gauss%dw, mesh%rr, INT(SIZE(mesh%rr,1), C_INT), INT(list_mode, C_INT), c_out, INT(mesh%np, C_INT), &
+         INT(mesh%me, C_INT), INT(mesh%gauss%n_w, C_INT), INT(mesh%gauss%l_G, C_INT), INT(SIZE(list_mode), C_INT), &
+         INT(nproc, C_INT))
+    IF (rc /= 0) THEN
+       WRITE(*,*) ' BUG in ', who, ' (status ', rc, ')'
+       STOP
+    END IF
+  END SUBROUTINE ugradc_gpu
+
+  ! Level set, subroutine_level_set.F90:434-534: grad c . u.
+  SUBROUTINE smb_ugradc_gauss_fft_par_gpu(communicator, mesh, list_mode, V_in, c_in, nb_procs, c_out)
+    TYPE(mesh_type),                            INTENT(IN)  :: mesh
+    INTEGER,                                    INTENT(IN)  :: nb_procs
+    INTEGER,      DIMENSION(:),                 INTENT(IN)  :: list_mode
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(IN)  :: V_in, c_in
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(OUT) :: c_out
+    MPI_Comm :: communicator
+    CALL ugradc_gpu(mesh, list_mode, V_in, c_in, c_out, C_NULL_PTR, 0, nb_procs, 'smb_ugradc_gauss_fft_par_gpu')
+  END SUBROUTINE smb_ugradc_gauss_fft_par_gpu
+
+  ! Temperature, subroutine_temperature_with_T.F90:247-350: (C grad T) . u + div u (C T).
+  SUBROUTINE smb_ugradc_gauss_fft_par_temperature_gpu(communicator, mesh, list_mode, heat_capa_in, V_in, c_in, c_out)
+    TYPE(mesh_type),                            INTENT(IN)  :: mesh
+    INTEGER,      DIMENSION(:),                 INTENT(IN)  :: list_mode
+    REAL(KIND=8), DIMENSION(:),     CONTIGUOUS, INTENT(IN), TARGET :: heat_capa_in
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(IN)  :: V_in, c_in
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(OUT) :: c_out
+    MPI_Comm :: communicator
+    INTEGER :: nproc, code
+    IF (SIZE(heat_capa_in) < mesh%me) THEN
+       WRITE(*,*) ' BUG in smb_ugradc_gauss_fft_par_temperature_gpu: heat_capa_in shorter than mesh%me'
+       STOP
+    END IF
+    CALL MPI_COMM_SIZE(communicator, nproc, code)
+    CALL ugradc_gpu(mesh, list_mode, V_in, c_in, c_out, C_LOC(heat_capa_in), 1, nproc, &
+         'smb_ugradc_gauss_fft_par_temperature_gpu')
+  END SUBROUTINE smb_ugradc_gauss_fft_par_temperature_gpu
+
+  ! Concentration, subroutine_concentration.F90:243-341: grad c . u + div u c.
+  SUBROUTINE smb_ugradc_gauss_fft_par_conc_gpu(communicator, mesh, list_mode, V_in, c_in, c_out)
+    TYPE(mesh_type),                            INTENT(IN)  :: mesh
+    INTEGER,      DIMENSION(:),                 INTENT(IN)  :: list_mode
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(IN)  :: V_in, c_in
+    REAL(KIND=8), DIMENSION(:,:,:), CONTIGUOUS, INTENT(OUT) :: c_out
+    MPI_Comm :: communicator
+    INTEGER :: nproc, code
+    CALL MPI_COMM_SIZE(communicator, nproc, code)
+    CALL ugradc_gpu(mesh, list_mode, V_in, c_in, c_out, C_NULL_PTR, 1, nproc, 'smb_ugradc_gauss_fft_par_conc_gpu')
+  END SUBROUTINE smb_ugradc_gauss_fft_par_conc_gpu
 
 END MODULE sfemans_gauss_gpu

@@ -171,3 +171,32 @@ def test_gauss_point_entry_checks():
     d = ctypes.c_void_p(16)
     assert L.sfnl_cross_gauss_f64(d, d, d, d, d, d, None, d, 5, 2, 11, 7, 2, 0, None, NULL) == -4  # n_w > 10
     assert L.sfnl_cross_gauss_f64(d, d, d, d, d, d, None, d, 0, 2, 6, 7, 2, 0, None, NULL) == -1
+
+
+def test_other_gauss_point_entry_checks():
+    # the Lorentz-force and advection callers reject what the Navier-Stokes one rejects, before any copy
+    L = sf.lib()
+    mesh = {"jj": np.ones((6, 2), dtype=np.int32, order="F"), "ww": np.zeros((6, 7), order="F"),
+            "dw": np.zeros((2, 6, 7, 2), order="F"), "rr": np.ones((2, 5), order="F")}
+    V = np.zeros((5, 6, 2), order="F")
+    C = np.zeros((5, 2, 2), order="F")
+    mesh["jj"][0, 0] = 0  # node numbers are 1-based
+    for call in (lambda: sf.smb_CurlH_cross_B_gauss_sft_par(None, mesh, [0, 1], V, V),
+                 lambda: sf.smb_ugradc_gauss_fft_par(None, mesh, [0, 1], V, C),
+                 lambda: sf.smb_ugradc_gauss_fft_par_conc(None, mesh, [0, 1], V, C)):
+        with pytest.raises(sf.SfnlError) as e:
+            call()
+        assert e.value.code == -1 and "jj" in sf.last_error()
+    mesh["jj"][0, 0] = 1
+    with pytest.raises(sf.SfnlError) as e:
+        sf.smb_ugradc_gauss_fft_par(None, mesh, [0, 1], V, C, nb_procs=2)
+    assert e.value.code == -4
+    with pytest.raises(sf.SfnlError) as e:
+        sf.smb_ugradc_gauss_fft_par_temperature(None, mesh, [0, 1], np.ones(1), V, C)  # 1 value, 2 elements
+    assert e.value.code == -1
+    d = ctypes.c_void_p(16)
+    assert L.sfnl_ugradc_gauss_f64(d, d, None, 2, d, d, d, d, d, d, 5, 2, 6, 7, 2, 0, None, NULL) == -1
+    assert L.sfnl_ugradc_gauss_f64(d, None, None, 0, d, d, d, d, d, d, 5, 2, 6, 7, 2, 0, None, NULL) == -1
+    assert L.sfnl_curlh_cross_b_gauss_f64(d, None, d, d, d, d, d, d, 5, 2, 6, 7, 2, 0, None, NULL) == -1
+    assert L.sfnl_curlh_cross_b_gauss_f64(d, d, d, d, d, d, d, d, 5, 2, 11, 7, 2, 0, None, NULL) == -4
+    assert L.sfnl_smb_ugradc_gauss(d, d, None, 3, d, d, d, d, 2, d, d, 5, 2, 6, 7, 2, 1) == -1

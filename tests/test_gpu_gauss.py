@@ -65,3 +65,88 @@ def test_medium_mesh_against_operands_and_library_product():
     ref = R.fft_par("cross", rot, w, 96, workers=8)
     out = sf.smb_cross_prod_gauss_sft_par(None, mesh, lm, V)
     assert _worst(out, ref) <= FP64_TOL
+
+
+# ---- the Lorentz-force caller: smb_CurlH_cross_B_gauss_sft_par (subroutine_ns_with_m.F90:788-883) ----
+@pytest.mark.parametrize("nr,nz,m,modes", [(2, 1, 1, None), (6, 4, 8, None), (9, 5, 16, "sparse"), (5, 3, 64, None)])
+@pytest.mark.parametrize("own_work", [False, True])
+def test_lorentz_device_entry_matches_oracle(nr, nz, m, modes, own_work):
+    mesh = R.synthetic_p2_mesh(nr, nz, 8)
+    lm = list(range(m)) if modes is None else [3 * i + (i % 2) for i in range(m)]
+    H = R.synthetic_field(mesh["np"], 6, m, 0.2, 21 + m)
+    B = R.synthetic_field(mesh["np"], 6, m, 0.2, 31 + m)
+    ref, _, _ = R.c_curlh_cross_b_gauss(H, B, mesh, lm)
+    work = torch.empty(12 * 7 * mesh["me"] * m, device="cuda", dtype=torch.float64) if own_work else None
+    out = sf.curlh_cross_b_gauss(sf.to_device(H), sf.to_device(B), _dev_mesh(mesh),
+                                 torch.tensor(lm, dtype=torch.int32, device="cuda"), work=work)
+    torch.cuda.synchronize()
+    assert _worst(sf.to_host(out), ref) <= FP64_TOL
+
+
+def test_lorentz_reference_signature_on_host_arrays():
+    mesh = R.synthetic_p2_mesh(7, 6, 9)
+    lm = list(range(12))
+    H = R.synthetic_field(mesh["np"], 6, 12, 0.3, 41)
+    B = R.synthetic_field(mesh["np"], 6, 12, 0.3, 42)
+    ref, _, _ = R.c_curlh_cross_b_gauss(H, B, mesh, lm)
+    assert _worst(sf.smb_CurlH_cross_B_gauss_sft_par(None, mesh, lm, H, B), ref) <= FP64_TOL
+
+
+# ---- the advection callers: smb_ugradc_gauss_fft_par (level set, temperature) and _conc ----
+VARIANTS = {"level_set": (False, False), "temperature": (True, True), "concentration": (True, False)}
+
+
+def _heat(mesh, on):
+    return np.linspace(0.5, 2.0, mesh["me"]) if on else None
+
+
+@pytest.mark.parametrize("variant", list(VARIANTS))
+@pytest.mark.parametrize("nr,nz,m,modes", [(2, 1, 1, None), (6, 4, 8, None), (9, 5, 16, "sparse"), (5, 3, 64, None)])
+def test_advection_device_entry_matches_oracle(variant, nr, nz, m, modes):
+    cons, heat_on = VARIANTS[variant]
+    mesh = R.synthetic_p2_mesh(nr, nz, 10)
+    lm = list(range(m)) if modes is None else [3 * i + (i % 2) for i in range(m)]
+    V = R.synthetic_field(mesh["np"], 6, m, 0.2, 51 + m)
+    C = R.synthetic_field(mesh["np"], 2, m, 0.2, 61 + m)
+    heat = _heat(mesh, heat_on)
+    ref = R.c_ugradc_gauss(V, C, mesh, lm, heat=heat, conservative=cons)[0]
+    out = sf.ugradc_gauss(sf.to_device(V), sf.to_device(C), _dev_mesh(mesh),
+                          torch.tensor(lm, dtype=torch.int32, device="cuda"),
+                          heat=None if heat is None else torch.tensor(heat, device="cuda"), conservative=cons)
+    torch.cuda.synchronize()
+    assert R.rel_l2(sf.to_host(out), ref) <= FP64_TOL
+
+
+@pytest.mark.parametrize("variant", list(VARIANTS))
+def test_advection_reference_signatures_on_host_arrays(variant):
+    cons, heat_on = VARIANTS[variant]
+    mesh = R.synthetic_p2_mesh(7, 6, 11)
+    lm = list(range(12))
+    V = R.synthetic_field(mesh["np"], 6, 12, 0.3, 71)
+    C = R.synthetic_field(mesh["np"], 2, 12, 0.3, 72)
+    heat = _heat(mesh, heat_on)
+    ref = R.c_ugradc_gauss(V, C, mesh, lm, heat=heat, conservative=cons)[0]
+    if variant == "level_set":
+        out = sf.smb_ugradc_gauss_fft_par(None, mesh, lm, V, C, 1)
+    elif variant == "temperature":
+        out = sf.smb_ugradc_gauss_fft_par_temperature(None, mesh, lm, heat, V, C)
+    else:
+        out = sf.smb_ugradc_gauss_fft_par_conc(None, mesh, lm, V, C)
+    assert R.rel_l2(out, ref) <= FP64_TOL
+
+
+def test_medium_mesh_other_callers_against_operands_and_library_products():
+    # 20k Gauss points, m = 64: operands from the CPU restatement, products by the pocketfft restatement
+    mesh = R.synthetic_p2_mesh(40, 36, 12)
+    m = 64
+    lm = list(range(m))
+    H = R.synthetic_field(mesh["np"], 6, m, 0.1, 81)
+    B = R.synthetic_field(mesh["np"], 6, m, 0.1, 82)
+    _, rot, w = R.c_curlh_cross_b_gauss(H, B, mesh, lm, product=False)
+    assert _worst(sf.smb_CurlH_cross_B_gauss_sft_par(None, mesh, lm, H, B),
+                  R.fft_par("cross", rot, w, 96, workers=8)) <= FP64_TOL
+    C = R.synthetic_field(mesh["np"], 2, m, 0.1, 83)
+    heat = _heat(mesh, True)
+    _, g, w, d, cg = R.c_ugradc_gauss(H, C, mesh, lm, heat=heat, conservative=True, product=False)
+    ref = R.fft_par("dot", g, w, 96, workers=8) + R.fft_par("prod", d, cg, 96, workers=8)
+    assert R.rel_l2(sf.smb_ugradc_gauss_fft_par_temperature(None, mesh, lm, heat, H, C), ref) <= FP64_TOL

@@ -289,3 +289,63 @@ def test_gauss_point_curl_known_answer():
     om = R.precession_omega(mesh["np"], [0], 0.5, 0.25)
     _, rot2, _ = R.c_cross_gauss(V, mesh, [0], om)
     np.testing.assert_allclose(rot2[:, 4, 0], 2.0 + 2 * 0.5 * np.cos(0.25 * np.pi), atol=1e-12)
+
+
+def test_lorentz_caller_on_equal_fields_is_the_navier_stokes_caller():
+    # smb_CurlH_cross_B_gauss_sft_par (subroutine_ns_with_m.F90:788-883) with H = B builds the same
+    # curl and values as smb_cross_prod_gauss_sft_par without precession: (curl u) x u
+    mesh = R.synthetic_p2_mesh(4, 3, 6)
+    lm = [0, 1, 2, 3]
+    V = R.synthetic_field(mesh["np"], 6, 4, 0.3, 61)
+    out_l, rot_l, w_l = R.c_curlh_cross_b_gauss(V, V, mesh, lm)
+    out_n, rot_n, w_n = R.c_cross_gauss(V, mesh, lm)
+    np.testing.assert_array_equal(rot_l, rot_n)
+    np.testing.assert_array_equal(w_l, w_n)
+    np.testing.assert_array_equal(out_l, out_n)
+    # and W comes from the second field
+    B = R.synthetic_field(mesh["np"], 6, 4, 0.3, 62)
+    _, rot_b, w_b = R.c_curlh_cross_b_gauss(V, B, mesh, lm, product=False)
+    np.testing.assert_array_equal(rot_b, rot_n)
+    _, _, w_ref = R.c_cross_gauss(B, mesh, lm, product=False)
+    np.testing.assert_array_equal(w_b, w_ref)
+
+
+def test_advection_caller_known_answers():
+    # smb_ugradc_gauss_fft_par (subroutine_level_set.F90:434-534 and the temperature / concentration
+    # versions): P2 elements reproduce linear fields exactly.
+    mesh = R.synthetic_p2_mesh(4, 3, 7)
+    npn, ng = mesh["np"], mesh["l_G"] * mesh["me"]
+    r, z = mesh["rr"]
+    # u = (0, 0, 1), c = z: grad c . u = 1; div u = 0
+    V = np.zeros((npn, 6, 1), order="F")
+    V[:, 4, 0] = 1.0
+    C = np.zeros((npn, 2, 1), order="F")
+    C[:, 0, 0] = z
+    for cons in (False, True):
+        out = R.c_ugradc_gauss(V, C, mesh, [0], conservative=cons)[0]
+        np.testing.assert_allclose(out[:, 0, 0], 1.0, atol=1e-12)
+        np.testing.assert_allclose(out[:, 1, 0], 0.0, atol=1e-15)
+    # u = (r, 0, 0), c = 1: grad c = 0, div u = (1/r) d(r u_r)/dr = 2; the conservative form gives 2 c,
+    # times the element's heat capacity in the temperature version
+    V = np.zeros((npn, 6, 1), order="F")
+    V[:, 0, 0] = r
+    C = np.zeros((npn, 2, 1), order="F")
+    C[:, 0, 0] = 1.0
+    heat = np.linspace(1.0, 3.0, mesh["me"])
+    out, gradc, w, div, cg = R.c_ugradc_gauss(V, C, mesh, [0], heat=heat, conservative=True)
+    np.testing.assert_allclose(div[:, 0, 0], 2.0, atol=1e-12)
+    np.testing.assert_allclose(cg[:, 0, 0], np.repeat(heat, mesh["l_G"]), atol=1e-14)
+    np.testing.assert_allclose(out[:, 0, 0], 2.0 * np.repeat(heat, mesh["l_G"]), atol=1e-12)
+    assert np.abs(R.c_ugradc_gauss(V, C, mesh, [0], conservative=False)[0]).max() < 1e-14
+    # c = r cos(theta) (mode 1), u_theta = sin(theta): the theta gradient -sin(theta) gives
+    # u . grad c = -sin^2 = -1/2 + cos(2 theta)/2
+    V = np.zeros((npn, 6, 3), order="F")
+    V[:, 3, 1] = 1.0
+    C = np.zeros((npn, 2, 3), order="F")
+    C[:, 0, 1] = r
+    out, gradc, _, _, _ = R.c_ugradc_gauss(V, C, mesh, [0, 1, 2])
+    np.testing.assert_allclose(gradc[:, 3, 1], -1.0, atol=1e-12)
+    np.testing.assert_allclose(out[:, 0, 0], -0.5, atol=1e-12)
+    np.testing.assert_allclose(out[:, 0, 2], 0.5, atol=1e-12)
+    np.testing.assert_allclose(out[:, 0, 1], 0.0, atol=1e-12)
+    assert out.shape == (ng, 2, 3)
