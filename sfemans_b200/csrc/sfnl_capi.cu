@@ -764,14 +764,42 @@ static int gauss_product(int kind, const double *v, const double *v2, const doub
   if (!v || !jj || !ww || !dw || !rr || !list_mode || !out || (kind != GK_NS && !v2))
     return set_error(SFNL_ERR_ARG, "null array");
   cudaStream_t st = as_stream(stream);
+  // The curl callers at m = 64: node-major copies of the nodal fields (NF x np_nodes x 6 x nmod doubles),
+  // then one kernel that builds the operands in the product's staging.  A caller's work buffer
+  // (12*l_G*me*nmod doubles) holds the copies when NF*np_nodes <= 2*l_G*me (P2 meshes: about 4 me <= 14 me).
+  const int nf = 1 + (kind == GK_LORENTZ || (kind == GK_NS && omega) ? 1 : 0);
+  const size_t nodal = (size_t)np_nodes * 6 * nmod;
+  const bool fused = kind != GK_ADVECT && gauss_cross_fused_supported(nmod, n_w) && dealiased(nmod, N) &&
+                     (!work || (size_t)nf * np_nodes <= (size_t)2 * ng);
   std::unique_lock<std::mutex> lk;
   double *wk = work;
   if (!wk) {
     DevState *s = dev_state();
     if (!s) return set_error(SFNL_ERR_CUDA, "no current device");
     lk = std::unique_lock<std::mutex>(s->mu);
-    if ((rc = grow_gwork(s, gauss_operand_doubles(kind, conservative, ng, nmod) * sizeof(double)))) return rc;
+    const size_t need = fused ? nf * nodal : gauss_operand_doubles(kind, conservative, ng, nmod);
+    if ((rc = grow_gwork(s, need * sizeof(double)))) return rc;
     wk = reinterpret_cast<double *>(s->gwork);
+  }
+  if (fused) {
+    double *vt = wk, *xt = wk + nodal;
+    if ((rc = launch_nodal_transpose(v, vt, np_nodes, nmod, st))) return rc;
+    const double *v2t = nullptr, *omt = nullptr;
+    if (kind == GK_LORENTZ) {
+      if ((rc = launch_nodal_transpose(v2, xt, np_nodes, nmod, st))) return rc;
+      v2t = xt;
+    } else if (omega) {
+      if ((rc = launch_nodal_transpose(omega, xt, np_nodes, nmod, st))) return rc;
+      omt = xt;
+    }
+    GaussArgs ga{vt, omt, ww, dw, rr, jj, list_mode, np_nodes, me, n_w, l_G, nmod, v2t, nullptr};
+    if ((rc = launch_gauss_cross_fused(ga, kind, out, ng, nmod, st))) return rc;
+    if (g_check_finite) {
+      ProgArgs pa;
+      if ((rc = build_product(OP_CROSS, out, out, out, ng, nmod, N, &pa))) return rc;
+      rc = scan_outputs(pa, st);
+    }
+    return rc;
   }
   const size_t o6 = (size_t)ng * 6 * nmod, o2 = (size_t)ng * 2 * nmod;
   double *g0 = wk, *g1 = wk + o6;

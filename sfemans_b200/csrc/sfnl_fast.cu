@@ -44,6 +44,7 @@
 #include <vector>
 
 #include "sfnl_fold.cuh"
+#include "sfnl_gauss.cuh"
 #include "sfnl_internal.h"
 #include "sfnl_ops.cuh"
 
@@ -904,6 +905,83 @@ __global__ void __launch_bounds__(384, EK == EK_CROSS ? 3 : 0) fast_tf_kernel(co
                      a.accumulate != 0);
 }
 
+// The Gauss-point cross products with their operands built in the staging (third fold, M = 64):
+// Navier-Stokes (curl u + 2 Om) x u (GK_NS) and Lorentz force (curl H) x B (GK_LORENTZ).  The tile's
+// 8 Gauss points get the curl and values of every mode straight from the nodal fields (node-major
+// copies: the element's nodes gathered through jj, the lanes of a warp reading 32 consecutive modes of
+// one node) into the coefficient layout, so the (l_G*me, 6, m) operand arrays never go through HBM.
+template <int M, int KIND>
+__global__ void __launch_bounds__(384, 2) gauss_tf_cross_kernel(const FastArgs a, const GaussArgs ga) {
+  static_assert(third_fold(M), "third fold needs the specialised geometry");
+  constexpr int NI = 6, NO = 3, NT = TfGeo<M>::NT, KS_tot = TfGeo<M>::KS_tot;
+  constexpr size_t fstride = (size_t)KS_tot * 32;
+  extern __shared__ double smem[];
+  const int64_t p0 = (int64_t)blockIdx.x * 8;
+  constexpr size_t prod_d = (size_t)NO * 4 * NT * 2 * 32;
+  double *ps = smem, *xc = smem + prod_d, *xs = smem;  // ps and xc overlay xs after the synthesis
+  constexpr int NW = 6;  // P2 elements
+  __shared__ int s_node[8][NW];
+  __shared__ double s_wt[8][NW], s_g1[8][NW], s_g2[8][NW], s_ray[8];
+  for (int t = threadIdx.x; t < NI * (int)fstride; t += blockDim.x) xs[t] = 0.0;  // padding rows, sine of mode 0
+  if (threadIdx.x < 8 * NW) {  // the points' nodes, basis values and derivatives (mesh%jj, ww, dw)
+    const int g = threadIdx.x / NW, n = threadIdx.x % NW;
+    const int64_t p = p0 + g < a.np ? p0 + g : a.np - 1;
+    const int me = (int)(p / ga.l_G), l = (int)(p % ga.l_G);
+    int node = ga.jj[n + (size_t)NW * me] - 1;
+    node = node < 0 ? 0 : node >= ga.np_nodes ? ga.np_nodes - 1 : node;  // no access outside the fields
+    s_node[g][n] = node;
+    s_wt[g][n] = ga.ww[n + (size_t)NW * l];
+    const double *dwl = ga.dw + (size_t)2 * NW * (l + (size_t)ga.l_G * me);
+    s_g1[g][n] = dwl[2 * n];
+    s_g2[g][n] = dwl[2 * n + 1];
+  }
+  __syncthreads();
+  if (threadIdx.x < 8) {  // radius of the point: sum rr(1, nodes) ww
+    double ray = 0.0;
+#pragma unroll
+    for (int n = 0; n < NW; ++n) ray = fma(ga.rr[2 * (size_t)s_node[threadIdx.x][n]], s_wt[threadIdx.x][n], ray);
+    s_ray[threadIdx.x] = ray;
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < 8 * M; it += blockDim.x) {
+    const int i = it % M, g = it / M;  // mode index, point of the tile: a warp reads 32 modes of a node
+    if (p0 + g >= a.np) continue;
+    double rot[6], w[6];
+    gauss_curl_gathered<KIND, M, NW>(ga, s_node[g], s_wt[g], s_g1[g], s_g2[g], s_ray[g], i, rot, w);
+    // rows of mode i: cosine group CE0 (i = 0 mod 4), CE2 (i = 2 mod 4) or CO (odd), sine group 3 further
+    const int gc = (i & 1) ? 2 : (i & 3) == 0 ? 0 : 1, k = (i & 1) ? i >> 1 : i >> 2;
+    const int rc = 4 * tf_koff(M, gc) + k, rs = 4 * tf_koff(M, gc + 3) + k;
+    const int oc = (rc >> 2) * 32 + a_frag_slot(rc & 3, g), os = (rs >> 2) * 32 + a_frag_slot(rs & 3, g);
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      xs[f * fstride + oc] = rot[2 * f];
+      xs[(3 + f) * fstride + oc] = w[2 * f];
+      if (i != 0) {  // the sine of mode 0 is ignored
+        xs[f * fstride + os] = rot[2 * f + 1];
+        xs[(3 + f) * fstride + os] = w[2 * f + 1];
+      }
+    }
+  }
+  __syncthreads();
+  double acc_e[NI][2], acc_o[NI][2];
+  tf_synth<M, NI, 0u>(xs, a.syn, acc_e, acc_o);
+  __syncthreads();  // every warp has read its last coefficient: xc and ps may overwrite xs
+  double v[4][NI];
+  tf_fold<M, NI>(acc_e, acc_o, xc, v);
+  double gq[4][NO];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) EKDef<EK_CROSS>::op(v[r], gq[r]);
+  tf_prefold<M, NO>(gq, ps, 0);
+  __syncthreads();
+  OutSet<NO> os;
+#pragma unroll
+  for (int o = 0; o < NO; ++o) {
+    os.p[o] = a.out[o];
+    os.ldm[o] = a.out_ldm[o];
+  }
+  tf_analysis<M, NO>(ps, a.ana, os, p0, a.np, a.out_ps, false);
+}
+
 // The MHD bundle (u x w, u x b, j x b, u . gradT) in one launch with the third fold (M = 64): the five
 // vector operands are staged and synthesised one at a time (u, w, gradT, b, j), so u and b are
 // transformed once instead of three and two times (15 field transforms instead of 24); u's and b's
@@ -1132,6 +1210,38 @@ bool fast_fused_fits(int op, int m) {
 }
 
 int fast_grid_length(int m) { return make_geo(m).N; }
+
+bool gauss_cross_fused_supported(int m, int n_w) { return third_fold(64) && m == 64 && n_w == 6; }
+
+int launch_gauss_cross_fused(const GaussArgs &ga, int kind, double *out, int64_t ng, int m, cudaStream_t st) {
+  constexpr int M = 64;
+  if (m != M) return set_error(SFNL_ERR_UNSUPPORTED, "fused Gauss-point cross product: m = 64 only");
+  if (ng == 0) return SFNL_OK;
+  const Geo g = make_geo(M);
+  Tables T;
+  if (int rc = get_tf_tables(g, &T)) return rc;
+  FastArgs fa;
+  std::memset(&fa, 0, sizeof(fa));
+  for (int o = 0; o < 3; ++o) {
+    fa.out[o] = out + (int64_t)2 * o * ng;  // V_out(l_G*me, 6, m): component o in slots 2o, 2o+1
+    fa.out_ldm[o] = 6 * ng;
+  }
+  fa.out_ps = 1;
+  fa.np = ng;
+  fa.m = M;
+  fa.N = g.N;
+  fa.NT = g.NT;
+  fa.syn = T.syn;
+  fa.ana = T.ana;  // variant 0: with the analysis weights
+  const size_t smem = fast_smem_bytes(EK_CROSS, g.NT, 4 * g.KS_tot, true);
+  auto kern = kind == GK_NS ? gauss_tf_cross_kernel<M, GK_NS> : gauss_tf_cross_kernel<M, GK_LORENTZ>;
+  if (kind != GK_NS && kind != GK_LORENTZ) return set_error(SFNL_ERR_ARG, "fused Gauss-point cross product: curl callers only");
+  if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (fused Gauss-point cross product)");
+  const int64_t tiles = (ng + 7) / 8;
+  kern<<<(unsigned)tiles, 384, smem, st>>>(fa, ga);
+  return check_launch("fused Gauss-point cross product");
+}
 
 bool fast_supported(int op, int m, int N) {
   if (m < 1 || m > 512 || !op_bilinear(op)) return false;

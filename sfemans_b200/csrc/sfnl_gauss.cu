@@ -16,6 +16,7 @@
 // FAST products then read.
 #include <cuda_runtime.h>
 
+#include "sfnl_gauss.cuh"
 #include "sfnl_internal.h"
 
 namespace sfnl {
@@ -30,36 +31,34 @@ __global__ void __launch_bounds__(256) gauss_eval_kernel(GaussArgs a, double *o0
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
     const int64_t p = idx % ng;
     const int i = (int)(idx / ng);
-    const int m = (int)(p / a.l_G), l = (int)(p % a.l_G);
-    const double mode = (double)a.list_mode[i];
-    const double *dwl = a.dw + (size_t)2 * a.n_w * (l + (size_t)a.l_G * m);  // dw_loc = dw(:,:,l,m)
-    double ray = 0.0, wv[6] = {0, 0, 0, 0, 0, 0}, om[6] = {0, 0, 0, 0, 0, 0}, w2[6] = {0, 0, 0, 0, 0, 0};
-    double d1[6] = {0, 0, 0, 0, 0, 0}, d2[6] = {0, 0, 0, 0, 0, 0};  // sum Vs(:,k) dw_loc(1|2,:)
-    double cw[2] = {0, 0}, c1[2] = {0, 0}, c2[2] = {0, 0};            // the scalar: values, d/dr, d/dz
-    for (int n = 0; n < a.n_w; ++n) {
-      int node = a.jj[n + (size_t)a.n_w * m] - 1;  // 1-based node numbers
-      node = node < 0 ? 0 : node >= a.np_nodes ? a.np_nodes - 1 : node;  // no access outside V
-      const double wt = a.ww[n + (size_t)a.n_w * l], g1 = dwl[2 * n], g2 = dwl[2 * n + 1];
-      ray = fma(a.rr[2 * (size_t)node], wt, ray);
-      const double *vn = a.v + node + (size_t)a.np_nodes * 6 * i;
+    if constexpr (KIND == GK_NS || KIND == GK_LORENTZ) {
+      double r[6], w[6];
+      gauss_curl_point<KIND>(a, p, i, r, w);
 #pragma unroll
       for (int k = 0; k < 6; ++k) {
-        const double vs = vn[(size_t)a.np_nodes * k];
-        wv[k] = fma(vs, wt, wv[k]);
-        d1[k] = fma(vs, g1, d1[k]);
-        d2[k] = fma(vs, g2, d2[k]);
+        const size_t at = (size_t)p + (size_t)ng * (k + 6 * (size_t)i);
+        o0[at] = r[k];
+        o1[at] = w[k];
       }
-      if (KIND == GK_NS && a.omega) {
-        const double *on = a.omega + node + (size_t)a.np_nodes * 6 * i;
+    } else {
+      const int m = (int)(p / a.l_G), l = (int)(p % a.l_G);
+      const double mode = (double)a.list_mode[i];
+      const double *dwl = a.dw + (size_t)2 * a.n_w * (l + (size_t)a.l_G * m);  // dw_loc = dw(:,:,l,m)
+      double ray = 0.0, wv[6] = {0, 0, 0, 0, 0, 0}, d1[6] = {0, 0, 0, 0, 0, 0}, d2[6] = {0, 0, 0, 0, 0, 0};
+      double cw[2] = {0, 0}, c1[2] = {0, 0}, c2[2] = {0, 0};  // the scalar: values, d/dr, d/dz
+      for (int n = 0; n < a.n_w; ++n) {
+        int node = a.jj[n + (size_t)a.n_w * m] - 1;  // 1-based node numbers
+        node = node < 0 ? 0 : node >= a.np_nodes ? a.np_nodes - 1 : node;  // no access outside V
+        const double wt = a.ww[n + (size_t)a.n_w * l], g1 = dwl[2 * n], g2 = dwl[2 * n + 1];
+        ray = fma(a.rr[2 * (size_t)node], wt, ray);
+        const double *vn = a.v + node + (size_t)a.np_nodes * 6 * i;
 #pragma unroll
-        for (int k = 0; k < 6; ++k) om[k] = fma(on[(size_t)a.np_nodes * k], wt, om[k]);
-      }
-      if (KIND == GK_LORENTZ) {
-        const double *bn = a.v2 + node + (size_t)a.np_nodes * 6 * i;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) w2[k] = fma(bn[(size_t)a.np_nodes * k], wt, w2[k]);
-      }
-      if (KIND == GK_ADVECT) {
+        for (int k = 0; k < 6; ++k) {
+          const double vs = vn[(size_t)a.np_nodes * k];
+          wv[k] = fma(vs, wt, wv[k]);
+          d1[k] = fma(vs, g1, d1[k]);
+          d2[k] = fma(vs, g2, d2[k]);
+        }
         const double *cn = a.v2 + node + (size_t)a.np_nodes * 2 * i;
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
@@ -69,23 +68,7 @@ __global__ void __launch_bounds__(256) gauss_eval_kernel(GaussArgs a, double *o0
           c2[k] = fma(cs, g2, c2[k]);
         }
       }
-    }
-    const double mr = mode / ray, ir = 1.0 / ray;
-    if (KIND == GK_NS || KIND == GK_LORENTZ) {
-      double r[6];
-      r[0] = mr * wv[5] - d2[2];               // cos, r:     mode/ray W6 - d/dz W3
-      r[3] = d2[1] - d1[5];                    // sin, theta: d/dz W2 - d/dr W6
-      r[4] = ir * wv[2] + d1[2] - mr * wv[1];  // cos, z:     W3/ray + d/dr W3 - mode/ray W2
-      r[1] = -mr * wv[4] - d2[3];              // sin, r
-      r[2] = d2[0] - d1[4];                    // cos, theta
-      r[5] = ir * wv[3] + d1[3] + mr * wv[0];  // sin, z
-#pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        const size_t at = (size_t)p + (size_t)ng * (k + 6 * (size_t)i);
-        o0[at] = KIND == GK_NS ? r[k] + 2.0 * om[k] : r[k];
-        o1[at] = KIND == GK_NS ? wv[k] : w2[k];
-      }
-    } else {
+      const double mr = mode / ray;
       const double hc = a.heat ? a.heat[m] : 1.0;  // heat_capa_in(m), temperature version
       const double gc[6] = {c1[0], c1[1], mr * cw[1], -mr * cw[0], c2[0], c2[1]};
 #pragma unroll
@@ -105,7 +88,35 @@ __global__ void __launch_bounds__(256) gauss_eval_kernel(GaussArgs a, double *o0
   }
 }
 
+// vt[node][k][i] = v[node + np_nodes*(k + 6 i)]: 32 modes x 32 nodes per CTA through shared memory, both
+// sides coalesced.
+__global__ void __launch_bounds__(256) nodal_transpose_kernel(const double *__restrict__ v, double *__restrict__ vt,
+                                                              int np_nodes, int m) {
+  __shared__ double t[32][33];
+  const int64_t node0 = (int64_t)blockIdx.x * 32;
+  const int k = blockIdx.y, i0 = blockIdx.z * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 8 rows of 32
+  for (int r = ty; r < 32; r += 8) {
+    const int i = i0 + r;
+    const int64_t node = node0 + tx;
+    if (i < m && node < np_nodes) t[r][tx] = v[node + (int64_t)np_nodes * (k + 6 * (int64_t)i)];
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const int64_t node = node0 + r;
+    const int i = i0 + tx;
+    if (i < m && node < np_nodes) vt[node * 6 * m + (int64_t)k * m + i] = t[tx][r];
+  }
+}
+
 }  // namespace
+
+int launch_nodal_transpose(const double *v, double *vt, int np_nodes, int m, cudaStream_t st) {
+  if (np_nodes == 0) return SFNL_OK;
+  dim3 grid((unsigned)((np_nodes + 31) / 32), 6, (unsigned)((m + 31) / 32));
+  nodal_transpose_kernel<<<grid, 256, 0, st>>>(v, vt, np_nodes, m);
+  return check_launch("nodal transpose");
+}
 
 int launch_gauss_eval(const GaussArgs &a, int kind, double *o0, double *o1, double *o2, double *o3, cudaStream_t st) {
   if (a.n_w < 1 || a.n_w > kMaxNw) return set_error(SFNL_ERR_UNSUPPORTED, "nodes per element outside 1..10");
