@@ -804,7 +804,30 @@ __device__ __forceinline__ void tf_analysis(const double *ps, const double *ana,
   const int64_t p = p0 + (lane >> 2);
   const bool valid = p < np;
   const double *anav = ana + lane;
-  for (int cu = warp; cu < NU_tot; cu += NW) {
+  // Output tiles of the odd groups cost 2*NT k-steps, those of the even groups NT (mirror-folded): the
+  // odd tiles go one per warp and the even ones two per remaining warp (M = 64, 12 warps: 8 + 4 x 2, every
+  // warp 12 k-steps), else round robin.
+  constexpr int NU0 = tf_NU(M, 0), NU1 = tf_NU(M, 1), NU3 = tf_NU(M, 3), NU4 = tf_NU(M, 4);
+  constexpr int n_odd = tf_NU(M, 2) + tf_NU(M, 5), n_even = NU_tot - n_odd;
+  const bool balanced = n_odd < NW;
+  const int nwe = NW - n_odd;
+  for (int j = 0;; ++j) {
+    int cu;
+    if (balanced) {
+      if (warp < n_odd) {
+        if (j > 0) break;
+        cu = warp < tf_NU(M, 2) ? tf_nuoff(M, 2) + warp : tf_nuoff(M, 5) + warp - tf_NU(M, 2);
+      } else {
+        const int k = warp - n_odd + j * nwe;
+        if (k >= n_even) break;
+        cu = k < NU0 ? k : k < NU0 + NU1 ? tf_nuoff(M, 1) + k - NU0
+           : k < NU0 + NU1 + NU3 ? tf_nuoff(M, 3) + k - NU0 - NU1 : tf_nuoff(M, 4) + k - NU0 - NU1 - NU3;
+      }
+    } else {
+      cu = warp + j * NW;
+      if (cu >= NU_tot) break;
+    }
+    (void)NU4;
     const int gr = (cu >= tf_nuoff(M, 1)) + (cu >= tf_nuoff(M, 2)) + (cu >= tf_nuoff(M, 3)) +
                    (cu >= tf_nuoff(M, 4)) + (cu >= tf_nuoff(M, 5));
     const int nuo = gr == 0 ? 0 : gr == 1 ? tf_nuoff(M, 1) : gr == 2 ? tf_nuoff(M, 2) : gr == 3 ? tf_nuoff(M, 3)
