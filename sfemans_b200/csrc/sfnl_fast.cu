@@ -355,22 +355,44 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M
     const int pc = 2 * (threadIdx.x & 3), rstep = blockDim.x >> 2;
     const bool v16 = a.vec16 && p0 + 8 <= a.np;
     const bool pv0 = p0 + pc < a.np, pv1 = p0 + pc + 1 < a.np;
-#pragma unroll
-    for (int f = 0; f < NI; ++f) {
-      const double *base = a.in[f] + (int64_t)b * a.in_bs[f] + p0 + pc;
-      const int64_t ldm = a.in_ldm[f];
-      double *xf = xs + (size_t)f * KS_tot * 32;
+    if constexpr (M != 0) {
+      // rows outermost: the row's class, mode and sine offset are decoded once for the NI fields
       for (int r = threadIdx.x >> 2; r < KT; r += rstep) {
         const int c = (r >= 4 * KOFF[1]) + (r >= 4 * KOFF[2]) + (r >= 4 * KOFF[3]);
         const int k = r - 4 * sel4(KOFF, c), n = class_mode(c, k);
-        double *dst = xf + (size_t)(r >> 2) * 32 + a_frag_slot(r & 3, pc);
+        double *dst0 = xs + (size_t)(r >> 2) * 32 + a_frag_slot(r & 3, pc);
         const bool live = k < sel4(KE, c) && !(c == 2 && n == 0);  // the sine of mode 0 is ignored
-        const double *src = base + (int64_t)n * ldm + (c >= 2 ? a.np : 0);
-        if (live && v16) {
-          cp_async16(dst, src);
-        } else {
-          if (live && pv0) cp_async8(dst, src); else dst[0] = 0.0;
-          if (live && pv1) cp_async8(dst + 1, src + 1); else dst[1] = 0.0;
+        const int64_t off = p0 + pc + (c >= 2 ? a.np : 0);
+#pragma unroll
+        for (int f = 0; f < NI; ++f) {
+          double *dst = dst0 + (size_t)f * KS_tot * 32;
+          const double *src = a.in[f] + (int64_t)b * a.in_bs[f] + off + (int64_t)n * a.in_ldm[f];
+          if (live && v16) {
+            cp_async16(dst, src);
+          } else {
+            if (live && pv0) cp_async8(dst, src); else dst[0] = 0.0;
+            if (live && pv1) cp_async8(dst + 1, src + 1); else dst[1] = 0.0;
+          }
+        }
+      }
+    } else {  // run-time geometry: fields outermost (measured faster there)
+#pragma unroll
+      for (int f = 0; f < NI; ++f) {
+        const double *base = a.in[f] + (int64_t)b * a.in_bs[f] + p0 + pc;
+        const int64_t ldm = a.in_ldm[f];
+        double *xf = xs + (size_t)f * KS_tot * 32;
+        for (int r = threadIdx.x >> 2; r < KT; r += rstep) {
+          const int c = (r >= 4 * KOFF[1]) + (r >= 4 * KOFF[2]) + (r >= 4 * KOFF[3]);
+          const int k = r - 4 * sel4(KOFF, c), n = class_mode(c, k);
+          double *dst = xf + (size_t)(r >> 2) * 32 + a_frag_slot(r & 3, pc);
+          const bool live = k < sel4(KE, c) && !(c == 2 && n == 0);  // the sine of mode 0 is ignored
+          const double *src = base + (int64_t)n * ldm + (c >= 2 ? a.np : 0);
+          if (live && v16) {
+            cp_async16(dst, src);
+          } else {
+            if (live && pv0) cp_async8(dst, src); else dst[0] = 0.0;
+            if (live && pv1) cp_async8(dst + 1, src + 1); else dst[1] = 0.0;
+          }
         }
       }
     }
@@ -617,21 +639,21 @@ __device__ __forceinline__ void tf_stage(double *xs, const FieldSet<NG> &fs, int
   const int pc = 2 * (threadIdx.x & 3), rstep = blockDim.x >> 2;
   const bool v16 = vec16 && p0 + 8 <= np;
   const bool pv0 = p0 + pc < np, pv1 = p0 + pc + 1 < np;
+  // rows outermost: the row's group, mode and sine offset are decoded once for the NG fields
+  for (int r = threadIdx.x >> 2; r < KT; r += rstep) {
+    const int gr = (r >= 4 * tf_koff(M, 1)) + (r >= 4 * tf_koff(M, 2)) + (r >= 4 * tf_koff(M, 3)) +
+                   (r >= 4 * tf_koff(M, 4)) + (r >= 4 * tf_koff(M, 5));
+    const int kg = gr == 0 ? 0 : gr == 1 ? tf_koff(M, 1) : gr == 2 ? tf_koff(M, 2) : gr == 3 ? tf_koff(M, 3)
+                 : gr == 4 ? tf_koff(M, 4) : tf_koff(M, 5);
+    const int keg = gr % 3 == 0 ? tf_ke(M, 0) : gr % 3 == 1 ? tf_ke(M, 1) : tf_ke(M, 2);
+    const int k = r - 4 * kg, n = tf_mode(gr, k);
+    double *dst0 = xs + (size_t)(r >> 2) * 32 + a_frag_slot(r & 3, pc);
+    const bool live = k < keg && !(gr == 3 && k == 0);  // the sine of mode 0 is ignored
+    const int64_t off = p0 + pc + (gr >= 3 ? np : 0);
 #pragma unroll
-  for (int f = 0; f < NG; ++f) {
-    const double *base = fs.p[f] + p0 + pc;
-    const int64_t ldm = fs.ldm[f];
-    double *xf = xs + (size_t)f * KS_tot * 32;
-    for (int r = threadIdx.x >> 2; r < KT; r += rstep) {
-      const int gr = (r >= 4 * tf_koff(M, 1)) + (r >= 4 * tf_koff(M, 2)) + (r >= 4 * tf_koff(M, 3)) +
-                     (r >= 4 * tf_koff(M, 4)) + (r >= 4 * tf_koff(M, 5));
-      const int kg = gr == 0 ? 0 : gr == 1 ? tf_koff(M, 1) : gr == 2 ? tf_koff(M, 2) : gr == 3 ? tf_koff(M, 3)
-                   : gr == 4 ? tf_koff(M, 4) : tf_koff(M, 5);
-      const int keg = gr % 3 == 0 ? tf_ke(M, 0) : gr % 3 == 1 ? tf_ke(M, 1) : tf_ke(M, 2);
-      const int k = r - 4 * kg, n = tf_mode(gr, k);
-      double *dst = xf + (size_t)(r >> 2) * 32 + a_frag_slot(r & 3, pc);
-      const bool live = k < keg && !(gr == 3 && k == 0);  // the sine of mode 0 is ignored
-      const double *src = base + (int64_t)n * ldm + (gr >= 3 ? np : 0);
+    for (int f = 0; f < NG; ++f) {
+      double *dst = dst0 + (size_t)f * KS_tot * 32;
+      const double *src = fs.p[f] + off + (int64_t)n * fs.ldm[f];
       if (live && v16) {
         cp_async16(dst, src);
       } else {
