@@ -38,6 +38,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "nonlinear-term Gauss-pt·modes/s: split-prec vs FP64 on 1 B200 at ≤1e-7 rel err"
 UNIT = "Gauss-pt*modes/s"
+FP64_PIPE_TFLOPS = 36.6  # FP64 tensor (DMMA) and DFMA throughput shared on B200, measured by a throughput probe
 
 # name: points, modes, pad, decay, input fields (6-slot), output slots, description
 WORKLOADS = {
@@ -300,6 +301,16 @@ def main():
     else:
         kname = {"fp64": "fast_kernel<EK_CROSS>", "split3": "split_kernel<PR_CROSS>", "split2": "split_kernel<PR_CROSS>",
                  "grid": "grid_kernel<OP_CROSS>"}[best]
+    # The FAST FP64 kernels are bound by the FP64 pipe, not HBM: the third-fold bundle at m = 64 issues
+    # 3,600 mma.sync.m8n8k4.f64 (512 flops each) per 8-point tile (5 operands x 12 warps x 12 k-steps x 3
+    # fields, 10 outputs x 144 k-steps); DMMA and DFMA share about 36.6 TFLOP/s on B200 (a throughput probe).
+    fp64_pipe = None
+    if single and best == "fp64" and args.workload == "mhd_bundle" and m == 64:
+        flops = 3600.0 * 512.0 * ((npts + 7) // 8)
+        fp64_pipe = {"kernel": "fast_bundle_tf_kernel<64>", "flops_per_launch": flops,
+                     "achieved_tflops": flops / (dom_ms / 1e3) / 1e12, "peak_tflops": FP64_PIPE_TFLOPS,
+                     "peak_source": "probe: mma.sync f64 and DFMA throughput on this pool's B200 (not in MEASURED_PEAKS.json)",
+                     "frac": flops / (dom_ms / 1e3) / 1e12 / FP64_PIPE_TFLOPS}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": results[best]["steps"],
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -314,6 +325,7 @@ def main():
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": _traffic(args.workload, best), "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": dom_ms},
+        "fp64_pipe": fp64_pipe,
         "clocks": clk_all,
         "gpu_launches": results[best]["steps"] * launches[best],
         "e2e": e2e,
