@@ -79,6 +79,42 @@ __device__ __forceinline__ void cp_async_wait_all() {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
+// ---------------------------------------------------------------------------
+// third fold: the mirror symmetry theta -> pi/2 - theta of the quadrant grid
+// ---------------------------------------------------------------------------
+// On theta_j = pi(2j+1)/(4Q) the quadrant is its own mirror: theta_{Q-1-j} = pi/2 - theta_j.  For even
+// n, cos(n(pi/2 - x)) = (-1)^(n/2) cos(nx) and sin(n(pi/2 - x)) = -(-1)^(n/2) sin(nx).  So an even class
+// split into its n = 0 mod 4 and n = 2 mod 4 parts (E0, E2) gives both mirror angles from one of them:
+// CE(x) = E0 + E2, CE(pi/2 - x) = E0 - E2 and SE(x) = S0 + S2, SE(pi/2 - x) = S2 - S0, each part having
+// half the modes; and the analysis of an even class contracts P(x) +- P(pi/2 - x) over half the quadrant
+// for each part.  The odd classes gain nothing (their mirror is the other trigonometric function).
+// With NT even, angle tile t and its mirror NT-1-t form a pair: local angle a of one is local angle 7-a
+// of the other, i.e. lane (g, 3-q) (lane ^ 3) and the other k-step parity e.  A quarter of the DMMAs of
+// both transforms goes.
+//
+// Row and output groups: 0 CE0, 1 CE2, 2 CO, 3 SE0, 4 SE2, 5 SO (cosine coefficients for 0-2, sine 3-5).
+__host__ __device__ constexpr int tf_ke(int m, int gr) {
+  return (gr % 3 == 0) ? (m + 3) / 4 : (gr % 3 == 1) ? (m + 1) / 4 : m / 2;
+}
+__host__ __device__ constexpr int tf_mode(int gr, int k) { return gr % 3 == 0 ? 4 * k : gr % 3 == 1 ? 4 * k + 2 : 2 * k + 1; }
+__host__ __device__ constexpr int tf_KS(int m, int gr) { return (tf_ke(m, gr) + 3) / 4; }
+__host__ __device__ constexpr int tf_koff(int m, int gr) { return gr == 0 ? 0 : tf_koff(m, gr - 1) + tf_KS(m, gr - 1); }
+__host__ __device__ constexpr int tf_NU(int m, int gr) { return (tf_ke(m, gr) + 7) / 8; }
+__host__ __device__ constexpr int tf_nuoff(int m, int gr) { return gr == 0 ? 0 : tf_nuoff(m, gr - 1) + tf_NU(m, gr - 1); }
+// quadrant angle tiles and analysis k-steps of an output group (half the quadrant for the even groups)
+__host__ __device__ constexpr int tf_NT(int m) { return ((3 * m - 2 + 3) / 4 + 7) / 8; }
+__host__ __device__ constexpr int tf_TE(int m, int gr) { return gr % 3 == 2 ? 2 * tf_NT(m) : tf_NT(m); }
+// first analysis k-step (units of 32 doubles) of group gr in the analysis table
+__host__ __device__ constexpr int tf_aoff(int m, int gr) {
+  return gr == 0 ? 0 : tf_aoff(m, gr - 1) + tf_NU(m, gr - 1) * tf_TE(m, gr - 1);
+}
+// the third fold needs an even number of angle tiles; it is built for the specialised m = 64 kernels
+// Tables of the third fold for m (a Geo with make_geo(m).N; sfnl_fast.cu): synthesis B fragments
+// [KS_tot][NT][32] (lane (g, q): mode tf_mode(gr, 4s + q), angle 8t + g) and analysis B fragments
+// [2 variants][tf_aoff(m, 6)][32] (lane (g, q): mode tf_mode(gr, 8u + g), angle 8t + 2q + e; variant 0
+// with the analysis weights).  Cached per (device, m).
+int get_tf_tables(const Geo &g, Tables *out);
+
 // Slot of (k-value kq, point p) in a 32-double A-fragment block [4 k][8 points].  A lane (g, q) of
 // m8n8k4 reads (q, g); a 64-bit shared load is served per half-warp, and with the plain order q*8 + g
 // the lanes q and q + 2 of a half-warp hit the same banks (two wavefronts per half-warp).  Flipping

@@ -54,6 +54,9 @@ struct LargeArgs {
   const double *syn, *ana;
   double *G;
   int64_t tiles;
+  // third fold (NT even): groups 0 CE0, 1 CE2, 2 CO, 3 SE0, 4 SE2, 5 SO
+  int tkoff[7], tks[6], tnuoff[7], tnu[6], taoff[7], tke[3];
+  int asteps;  // k-steps of one analysis-table variant
 };
 
 // PT 8-point tiles of one field per CTA: each B fragment of the DFT table (read from L2) feeds PT
@@ -153,6 +156,260 @@ __global__ void __launch_bounds__(kLargeSynMaxWarps * 32) large_syn_kernel(const
         gp[1 * 64] = B + D;  // pi - theta
         gp[2 * 64] = B - D;  // pi + theta
         gp[3 * 64] = A - C;  // 2 pi - theta
+      }
+    }
+  }
+}
+
+// The synthesis with the third fold (NT even): the quadrant grid is its own mirror (theta -> pi/2 - theta
+// maps tile t to NT-1-t, local angle a to 7-a: lane (g, q) to (g, 3-q), parity e to 1-e), and for even n
+// cos(n(pi/2 - x)) = (-1)^(n/2) cos(nx), sin(n(pi/2 - x)) = -(-1)^(n/2) sin(nx).  So a warp takes a pair
+// (t, NT-1-t): the even classes split into n = 0 and n = 2 (mod 4) parts are contracted on tile t only
+// (CE = E0 + E2 there, E0 - E2 at the mirror tile; SE = S0 + S2, S2 - S0), the odd classes on both tiles.
+// A quarter of the DMMAs goes.  Staged rows in group order CE0, CE2, CO, SE0, SE2, SO.
+template <int PT>
+__global__ void __launch_bounds__(kLargeSynMaxWarps * 32, 1) large_syn_tf_kernel(const LargeArgs a) {
+  extern __shared__ double xs[];  // [PT][KS_tot][4][8], points swizzled (a_frag_slot)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int f = a.syn_f[blockIdx.y];
+  const int64_t tile0 = (int64_t)blockIdx.x * PT, p0 = tile0 * 8;
+  const int NT = a.NT, NH = NT >> 1, KS_tot = a.tkoff[6], KT = 4 * KS_tot;
+  const size_t pts = (size_t)KS_tot * 32;
+  const double *in_f = a.in[f] + (int64_t)a.batch_entry * a.in_bs[f];
+  const int64_t ldm = a.in_ldm[f];
+  {  // stage: 4*PT threads per row, two points each
+    constexpr int tpr = 4 * PT;
+    const int pc = 2 * (threadIdx.x % tpr), rstep = blockDim.x / tpr;
+    const bool v16 = a.vec16 && p0 + pc + 2 <= a.npts;
+    const bool pv0 = p0 + pc < a.npts, pv1 = p0 + pc + 1 < a.npts;
+    const double *base = in_f + p0 + pc;
+    double *dst0 = xs + (size_t)(pc >> 3) * pts;
+    for (int r = threadIdx.x / tpr; r < KT; r += rstep) {
+      const int ks = r >> 2;
+      const int gr = (ks >= a.tkoff[1]) + (ks >= a.tkoff[2]) + (ks >= a.tkoff[3]) + (ks >= a.tkoff[4]) + (ks >= a.tkoff[5]);
+      const int kg = gr == 0 ? 0 : gr == 1 ? a.tkoff[1] : gr == 2 ? a.tkoff[2] : gr == 3 ? a.tkoff[3]
+                   : gr == 4 ? a.tkoff[4] : a.tkoff[5];
+      const int keg = gr % 3 == 0 ? a.tke[0] : gr % 3 == 1 ? a.tke[1] : a.tke[2];
+      const int k = r - 4 * kg, n = tf_mode(gr, k);
+      double *dst = dst0 + (size_t)ks * 32 + a_frag_slot(r & 3, pc & 7);
+      const bool live = k < keg && !(gr == 3 && k == 0);  // the sine of mode 0 is ignored
+      const double *src = base + (int64_t)n * ldm + (gr >= 3 ? a.in_sin : 0);
+      if (live && v16) {
+        cp_async16(dst, src);
+      } else {
+        if (live && pv0) cp_async8(dst, src); else dst[0] = 0.0;
+        if (live && pv1) cp_async8(dst + 1, src + 1); else dst[1] = 0.0;
+      }
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  if ((a.adj_in >> f) & 1u) {  // a cotangent: synthesised with the analysis weights 1/N (n = 0), 2/N
+    const double invN = 1.0 / (4.0 * 8.0 * NT), twoN = 2.0 * invN;
+    for (size_t i = threadIdx.x; i < PT * pts; i += blockDim.x) {
+      const int ks = (int)((i % pts) >> 5);
+      const bool n0 = (ks == 0 || ks == a.tkoff[3]) && ((i >> 3) & 3) == 0;  // k = 0 of CE0 / SE0
+      xs[i] *= n0 ? invN : twoN;
+    }
+    __syncthreads();
+  }
+  const double *xs_l = xs + a_frag_slot(lane & 3, lane >> 2);
+  const size_t bstride = (size_t)NT * 32;
+  const int ks0 = a.tks[0], ks1 = a.tks[1], ks2 = a.tks[2];
+  const int ko0 = a.tkoff[0], ko1 = a.tkoff[1], ko2 = a.tkoff[2], ko3 = a.tkoff[3], ko4 = a.tkoff[4], ko5 = a.tkoff[5];
+  for (int tau = warp; tau < NH; tau += nw) {
+    const int tm = NT - 1 - tau;
+    // even parts on tile tau: E0 (CE0), E2 (CE2), S0 (SE0), S2 (SE2)
+    double ev[4][PT][2];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int pt = 0; pt < PT; ++pt) ev[j][pt][0] = ev[j][pt][1] = 0.0;
+    {
+      const double *bt = a.syn + (size_t)tau * 32 + lane;
+      const int kse = ks0 > ks1 ? ks0 : ks1;
+      for (int s = 0; s < kse; ++s) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int kso = j == 0 ? ko0 : j == 1 ? ko1 : j == 2 ? ko3 : ko4;
+          if (s >= ((j & 1) ? ks1 : ks0)) continue;
+          const size_t ks = (size_t)(kso + s);
+          const double bv = __ldg(bt + ks * bstride);
+#pragma unroll
+          for (int pt = 0; pt < PT; ++pt) dmma(ev[j][pt], xs_l[pt * pts + ks * 32], bv);
+        }
+      }
+    }
+    // the even classes on both tiles: own lane on tau, mirror lane (lane ^ 3) and parity 1 - e on tm
+    double ce[2][PT][2], se[2][PT][2];
+#pragma unroll
+    for (int pt = 0; pt < PT; ++pt)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        ce[0][pt][e] = ev[0][pt][e] + ev[1][pt][e];
+        se[0][pt][e] = ev[2][pt][e] + ev[3][pt][e];
+        const double e0 = __shfl_xor_sync(0xffffffffu, ev[0][pt][1 - e], 3);
+        const double e2 = __shfl_xor_sync(0xffffffffu, ev[1][pt][1 - e], 3);
+        const double s0 = __shfl_xor_sync(0xffffffffu, ev[2][pt][1 - e], 3);
+        const double s2 = __shfl_xor_sync(0xffffffffu, ev[3][pt][1 - e], 3);
+        ce[1][pt][e] = e0 - e2;
+        se[1][pt][e] = s2 - s0;
+      }
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const int t = side ? tm : tau;
+      double od[2][PT][2];  // CO, SO
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int pt = 0; pt < PT; ++pt) od[j][pt][0] = od[j][pt][1] = 0.0;
+      const double *bt = a.syn + (size_t)t * 32 + lane;
+      for (int s = 0; s < ks2; ++s) {
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const size_t ks = (size_t)((j ? ko5 : ko2) + s);
+          const double bv = __ldg(bt + ks * bstride);
+#pragma unroll
+          for (int pt = 0; pt < PT; ++pt) dmma(od[j][pt], xs_l[pt * pts + ks * 32], bv);
+        }
+      }
+#pragma unroll
+      for (int pt = 0; pt < PT; ++pt) {
+        const int64_t tile = tile0 + pt;
+        if (tile >= a.tiles) break;
+        double *gp0 = a.G + ((a.gslot[f] * a.tiles + tile) * NT + t) * 256 + lane;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const double CE = ce[side][pt][e], SE = se[side][pt][e], CO = od[0][pt][e], SO = od[1][pt][e];
+          const double A = CE + CO, B = CE - CO, C = SE + SO, D = SO - SE;
+          double *gp = gp0 + e * 32;
+          gp[0 * 64] = A + C;  // theta
+          gp[1 * 64] = B + D;  // pi - theta
+          gp[2 * 64] = B - D;  // pi + theta
+          gp[3 * 64] = A - C;  // 2 pi - theta
+        }
+      }
+    }
+  }
+}
+
+// Program and analysis with the third fold: chunks of two angle-tile pairs (t, t+1 and their mirrors); the
+// odd output groups contract all four tiles, the even ones P(t) +- P(mirror) over the first-half tiles
+// (signs PE0 +, PE2 -, QE0 -, QE2 +).
+template <int OP, int O0, int CPW>
+__global__ void __launch_bounds__(kLargeProdWarps * 32) large_prod_tf_kernel(const LargeArgs a) {
+  constexpr int NI = op_nin(OP), NO = op_nout(OP);
+  constexpr int NOG = NO - O0 < kLargeGroup ? NO - O0 : kLargeGroup;
+  extern __shared__ double pc_s[];  // [NOG][4 classes][4 local tiles][2][32]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, q = lane & 3;
+  const int b = a.batch_entry;
+  const int64_t tile = blockIdx.x, p = tile * 8 + (lane >> 2);
+  const int NT = a.NT, NH = NT >> 1;
+  double y[CPW][NOG][2];
+#pragma unroll
+  for (int j = 0; j < CPW; ++j)
+#pragma unroll
+    for (int o = 0; o < NOG; ++o) y[j][o][0] = y[j][o][1] = 0.0;
+  const int64_t fstride = a.tiles * NT * 256;
+  const double *Gl = a.G + tile * NT * 256 + lane;
+  const double *anav = a.ana + (size_t)(a.adj_out ? 1 : 0) * a.asteps * 32 + lane;
+  const int NU_tot = a.tnuoff[6];
+  const size_t cst = (size_t)4 * 2 * 32;  // class stride in pc_s
+  for (int c0 = 0; c0 < NH; c0 += 2) {
+    const int npr = NH - c0 < 2 ? NH - c0 : 2;  // pairs in this chunk
+    // local tiles 0, 1: c0, c0+1; 2, 3: their mirrors NT-1-c0, NT-2-c0
+    if (warp < 4 * npr) {
+      const int li = warp >> 1, e = warp & 1;
+      const int lt = li < npr ? li : 2 + li - npr;
+      const int t = lt < 2 ? c0 + lt : NT - 1 - (c0 + lt - 2);
+      double gq[4][NOG];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        double x[NI], yy[NO];
+#pragma unroll
+        for (int f = 0; f < NI; ++f) x[f] = Gl[a.gslot[f] * fstride + (size_t)t * 256 + r * 64 + e * 32];
+        apply_op<OP>(x, yy);
+#pragma unroll
+        for (int o = 0; o < NOG; ++o) gq[r][o] = yy[O0 + o];
+      }
+#pragma unroll
+      for (int o = 0; o < NOG; ++o) {
+        const double s14 = gq[0][o] + gq[3][o], d14 = gq[0][o] - gq[3][o];
+        const double s23 = gq[1][o] + gq[2][o], d32 = gq[2][o] - gq[1][o];
+        double *dst = pc_s + ((size_t)(o * 4) * 4 + lt) * 64 + e * 32 + lane;
+        dst[0] = s14 + s23;        // PE
+        dst[cst] = s14 - s23;      // PO
+        dst[2 * cst] = d14 + d32;  // QE
+        dst[3 * cst] = d14 - d32;  // QO
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < CPW; ++j) {
+      const int cu = warp + kLargeProdWarps * j;
+      if (cu >= NU_tot) continue;
+      const int gr = (cu >= a.tnuoff[1]) + (cu >= a.tnuoff[2]) + (cu >= a.tnuoff[3]) + (cu >= a.tnuoff[4]) +
+                     (cu >= a.tnuoff[5]);
+      const int nuo = gr == 0 ? 0 : gr == 1 ? a.tnuoff[1] : gr == 2 ? a.tnuoff[2] : gr == 3 ? a.tnuoff[3]
+                    : gr == 4 ? a.tnuoff[4] : a.tnuoff[5];
+      const int aof = gr == 0 ? 0 : gr == 1 ? a.taoff[1] : gr == 2 ? a.taoff[2] : gr == 3 ? a.taoff[3]
+                    : gr == 4 ? a.taoff[4] : a.taoff[5];
+      const bool odd = gr % 3 == 2;
+      const int u = cu - nuo, TE = odd ? 2 * NT : NT, c = gr < 3 ? (odd ? 1 : 0) : (odd ? 3 : 2);
+      const double sg = (gr == 0 || gr == 4) ? 1.0 : -1.0;
+      const double *bt = anav + (size_t)(aof + u * TE) * 32;
+      const double *pa = pc_s + (size_t)c * cst + lane;
+      if (odd) {
+        for (int li = 0; li < 2 * npr; ++li) {
+          const int lt = li < npr ? li : 2 + li - npr;
+          const int t = lt < 2 ? c0 + lt : NT - 1 - (c0 + lt - 2);
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const double bv = __ldg(bt + (size_t)(2 * t + e) * 32);
+#pragma unroll
+            for (int o = 0; o < NOG; ++o) dmma(y[j][o], pa[(size_t)o * 4 * cst + (size_t)(lt * 2 + e) * 32], bv);
+          }
+        }
+      } else {
+        const int lx = (lane ^ 3) - lane;  // mirror lane offset
+        for (int lt = 0; lt < npr; ++lt) {
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const double bv = __ldg(bt + (size_t)(2 * (c0 + lt) + e) * 32);
+#pragma unroll
+            for (int o = 0; o < NOG; ++o) {
+              const double *po = pa + (size_t)o * 4 * cst;
+              const double av = po[(size_t)(lt * 2 + e) * 32] + sg * po[(size_t)((2 + lt) * 2 + 1 - e) * 32 + lx];
+              dmma(y[j][o], av, bv);
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (p >= a.npts) return;
+#pragma unroll
+  for (int j = 0; j < CPW; ++j) {
+    const int cu = warp + kLargeProdWarps * j;
+    if (cu >= NU_tot) continue;
+    const int gr = (cu >= a.tnuoff[1]) + (cu >= a.tnuoff[2]) + (cu >= a.tnuoff[3]) + (cu >= a.tnuoff[4]) +
+                   (cu >= a.tnuoff[5]);
+    const int nuo = gr == 0 ? 0 : gr == 1 ? a.tnuoff[1] : gr == 2 ? a.tnuoff[2] : gr == 3 ? a.tnuoff[3]
+                  : gr == 4 ? a.tnuoff[4] : a.tnuoff[5];
+    const int keg = gr % 3 == 0 ? a.tke[0] : gr % 3 == 1 ? a.tke[1] : a.tke[2];
+    const int u = cu - nuo;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int kk = 8 * u + 2 * q + h;
+      if (kk >= keg) continue;
+      const int n = tf_mode(gr, kk);
+#pragma unroll
+      for (int o = 0; o < NOG; ++o) {
+        const int og = O0 + o;
+        double *dst = a.out[og] + (int64_t)b * a.out_bs[og] + p * a.out_ps + (int64_t)n * a.out_ldm[og] +
+                      (gr >= 3 ? a.out_sin : 0);
+        *dst = (gr >= 3 && n == 0) ? 0.0 : y[j][o][h];
       }
     }
   }
@@ -271,65 +528,70 @@ int large_workspace(cudaStream_t st, size_t bytes, double **out) {
 }
 
 template <int OP, int O0, int CPW>
-int launch_large_prod(const LargeArgs &la, cudaStream_t st) {
+int launch_large_prod(const LargeArgs &la, bool tf, cudaStream_t st) {
   constexpr int NO = op_nout(OP), NOG = NO - O0 < kLargeGroup ? NO - O0 : kLargeGroup;
   const size_t smem = sizeof(double) * (size_t)NOG * 4 * kLCT * 2 * 32;
-  large_prod_kernel<OP, O0, CPW><<<(unsigned)la.tiles, kLargeProdWarps * 32, smem, st>>>(la);
+  if (tf)
+    large_prod_tf_kernel<OP, O0, CPW><<<(unsigned)la.tiles, kLargeProdWarps * 32, smem, st>>>(la);
+  else
+    large_prod_kernel<OP, O0, CPW><<<(unsigned)la.tiles, kLargeProdWarps * 32, smem, st>>>(la);
   return check_launch("large-m program and analysis");
 }
 
 // Output group G (outputs 3G .. 3G+2) of program OP.
 template <int OP, int G>
-int launch_large_group(const LargeArgs &la, cudaStream_t st) {
+int launch_large_group(const LargeArgs &la, bool tf, cudaStream_t st) {
   constexpr int O0 = kLargeGroup * G;
   if constexpr (O0 >= op_nout(OP)) {
     return SFNL_OK;
   } else {
-    switch ((la.NU_tot + kLargeProdWarps - 1) / kLargeProdWarps) {
-      case 1: return launch_large_prod<OP, O0, 1>(la, st);
-      case 2: return launch_large_prod<OP, O0, 2>(la, st);
-      case 3: return launch_large_prod<OP, O0, 3>(la, st);
-      case 4: return launch_large_prod<OP, O0, 4>(la, st);
-      case 5: return launch_large_prod<OP, O0, 5>(la, st);
-      case 6: return launch_large_prod<OP, O0, 6>(la, st);
-      case 7: return launch_large_prod<OP, O0, 7>(la, st);
-      case 8: return launch_large_prod<OP, O0, 8>(la, st);
+    const int nu = tf ? la.tnuoff[6] : la.NU_tot;
+    switch ((nu + kLargeProdWarps - 1) / kLargeProdWarps) {
+      case 1: return launch_large_prod<OP, O0, 1>(la, tf, st);
+      case 2: return launch_large_prod<OP, O0, 2>(la, tf, st);
+      case 3: return launch_large_prod<OP, O0, 3>(la, tf, st);
+      case 4: return launch_large_prod<OP, O0, 4>(la, tf, st);
+      case 5: return launch_large_prod<OP, O0, 5>(la, tf, st);
+      case 6: return launch_large_prod<OP, O0, 6>(la, tf, st);
+      case 7: return launch_large_prod<OP, O0, 7>(la, tf, st);
+      case 8: return launch_large_prod<OP, O0, 8>(la, tf, st);
     }
     return set_error(SFNL_ERR_UNSUPPORTED, "large-m FAST form: too many output tiles");
   }
 }
 
 template <int OP>
-int launch_large_prod_all(const LargeArgs &la, cudaStream_t st) {
+int launch_large_prod_all(const LargeArgs &la, bool tf, cudaStream_t st) {
   static_assert(op_nout(OP) <= 4 * kLargeGroup, "output groups");
-  if (int rc = launch_large_group<OP, 0>(la, st)) return rc;
-  if (int rc = launch_large_group<OP, 1>(la, st)) return rc;
-  if (int rc = launch_large_group<OP, 2>(la, st)) return rc;
-  return launch_large_group<OP, 3>(la, st);
+  if (int rc = launch_large_group<OP, 0>(la, tf, st)) return rc;
+  if (int rc = launch_large_group<OP, 1>(la, tf, st)) return rc;
+  if (int rc = launch_large_group<OP, 2>(la, tf, st)) return rc;
+  return launch_large_group<OP, 3>(la, tf, st);
 }
 
-int launch_large_prod_op(int op, const LargeArgs &la, cudaStream_t st) {
+int launch_large_prod_op(int op, const LargeArgs &la, bool tf, cudaStream_t st) {
   switch (op) {
-    case OP_CROSS: return launch_large_prod_all<OP_CROSS>(la, st);
-    case OP_DOT: return launch_large_prod_all<OP_DOT>(la, st);
-    case OP_PROD: return launch_large_prod_all<OP_PROD>(la, st);
-    case OP_BUNDLE: return launch_large_prod_all<OP_BUNDLE>(la, st);
-    case OP_CROSS_JVP: return launch_large_prod_all<OP_CROSS_JVP>(la, st);
-    case OP_CROSS_VJP: return launch_large_prod_all<OP_CROSS_VJP>(la, st);
-    case OP_MHD_JVP: return launch_large_prod_all<OP_MHD_JVP>(la, st);
-    case OP_MHD_VJP: return launch_large_prod_all<OP_MHD_VJP>(la, st);
-    case OP_SVECT: return launch_large_prod_all<OP_SVECT>(la, st);
-    case OP_TENSOR: return launch_large_prod_all<OP_TENSOR>(la, st);
-    case OP_ADVECT: return launch_large_prod_all<OP_ADVECT>(la, st);
+    case OP_CROSS: return launch_large_prod_all<OP_CROSS>(la, tf, st);
+    case OP_DOT: return launch_large_prod_all<OP_DOT>(la, tf, st);
+    case OP_PROD: return launch_large_prod_all<OP_PROD>(la, tf, st);
+    case OP_BUNDLE: return launch_large_prod_all<OP_BUNDLE>(la, tf, st);
+    case OP_CROSS_JVP: return launch_large_prod_all<OP_CROSS_JVP>(la, tf, st);
+    case OP_CROSS_VJP: return launch_large_prod_all<OP_CROSS_VJP>(la, tf, st);
+    case OP_MHD_JVP: return launch_large_prod_all<OP_MHD_JVP>(la, tf, st);
+    case OP_MHD_VJP: return launch_large_prod_all<OP_MHD_VJP>(la, tf, st);
+    case OP_SVECT: return launch_large_prod_all<OP_SVECT>(la, tf, st);
+    case OP_TENSOR: return launch_large_prod_all<OP_TENSOR>(la, tf, st);
+    case OP_ADVECT: return launch_large_prod_all<OP_ADVECT>(la, tf, st);
   }
   return set_error(SFNL_ERR_ARG, "large-m FAST form: program not bilinear");
 }
 
-int launch_large_syn(const LargeArgs &la, int nfields, cudaStream_t st) {
+int launch_large_syn(const LargeArgs &la, int nfields, bool tf, cudaStream_t st) {
   if (nfields == 0) return SFNL_OK;
-  // angle tiles spread evenly over at most kLargeSynMaxWarps warps
-  const int rounds = (la.NT + kLargeSynMaxWarps - 1) / kLargeSynMaxWarps, nw = (la.NT + rounds - 1) / rounds;
-  const size_t tile_bytes = sizeof(double) * (size_t)la.KS_tot * 32;
+  // angle tiles (pairs of mirror tiles with the third fold) spread evenly over at most kLargeSynMaxWarps warps
+  const int units = tf ? la.NT / 2 : la.NT;
+  const int rounds = (units + kLargeSynMaxWarps - 1) / kLargeSynMaxWarps, nw = (units + rounds - 1) / rounds;
+  const size_t tile_bytes = sizeof(double) * (size_t)(tf ? la.tkoff[6] : la.KS_tot) * 32;
   auto go = [&](auto kern, int pt) {
     const size_t smem = tile_bytes * pt;
     if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -338,8 +600,13 @@ int launch_large_syn(const LargeArgs &la, int nfields, cudaStream_t st) {
     kern<<<dim3((unsigned)blocks, (unsigned)nfields), nw * 32, smem, st>>>(la);
     return check_launch("large-m synthesis");
   };
-  if (4 * tile_bytes <= kLargeSynSmem) return go(large_syn_kernel<4>, 4);
-  if (2 * tile_bytes <= kLargeSynSmem) return go(large_syn_kernel<2>, 2);
+  if (tf) {
+    if (4 * tile_bytes <= kLargeSynSmem) return go(large_syn_tf_kernel<4>, 4);
+    if (2 * tile_bytes <= kLargeSynSmem) return go(large_syn_tf_kernel<2>, 2);
+  } else {
+    if (4 * tile_bytes <= kLargeSynSmem) return go(large_syn_kernel<4>, 4);
+    if (2 * tile_bytes <= kLargeSynSmem) return go(large_syn_kernel<2>, 2);
+  }
   return set_error(SFNL_ERR_UNSUPPORTED, "large-m FAST form: m too large");
 }
 
@@ -363,6 +630,11 @@ int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStre
   if (chunk > a.np) chunk = ((a.np + 7) / 8) * 8;
   double *G = nullptr;
   if (int rc = large_workspace(st, per_point * (size_t)chunk, &G)) return rc;
+  // the third fold needs mirror pairs of angle tiles
+  const bool tf = g.NT % 2 == 0;
+  Tables TT = T;
+  if (tf)
+    if (int rc = get_tf_tables(g, &TT)) return rc;
   const bool adj_out = op_adjoint_out(a.op);
   unsigned adj = 0;
   for (int f = 0; f < ni; ++f)
@@ -400,22 +672,33 @@ int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStre
     la.adj_in = adj;
     la.adj_out = adj_out ? 1 : 0;
     la.vec16 = v16;
-    la.syn = T.syn;
-    la.ana = T.ana;
+    la.syn = TT.syn;
+    la.ana = TT.ana;
     la.G = G;
+    for (int gr = 0; gr < 7; ++gr) {
+      la.tkoff[gr] = tf_koff(g.m, gr);
+      la.tnuoff[gr] = tf_nuoff(g.m, gr);
+      la.taoff[gr] = tf_aoff(g.m, gr);
+    }
+    for (int gr = 0; gr < 6; ++gr) {
+      la.tks[gr] = tf_KS(g.m, gr);
+      la.tnu[gr] = tf_NU(g.m, gr);
+    }
+    for (int gr = 0; gr < 3; ++gr) la.tke[gr] = tf_ke(g.m, gr);
+    la.asteps = tf_aoff(g.m, 6);
     // the batch-invariant fields, once per chunk
     int k = 0;
     for (int f = 0; f < ni; ++f)
       if (a.in_bs[f] == 0) la.syn_f[k++] = f;
     la.batch_entry = 0;
-    if (int rc = launch_large_syn(la, k, st)) return rc;
+    if (int rc = launch_large_syn(la, k, tf, st)) return rc;
     for (int b = 0; b < a.batch; ++b) {
       la.batch_entry = b;
       k = 0;
       for (int f = 0; f < ni; ++f)
         if (a.in_bs[f] != 0) la.syn_f[k++] = f;
-      if (int rc = launch_large_syn(la, k, st)) return rc;
-      if (int rc = launch_large_prod_op(a.op, la, st)) return rc;
+      if (int rc = launch_large_syn(la, k, tf, st)) return rc;
+      if (int rc = launch_large_prod_op(a.op, la, tf, st)) return rc;
     }
   }
   return SFNL_OK;
