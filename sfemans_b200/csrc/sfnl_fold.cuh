@@ -29,7 +29,10 @@ inline Geo make_geo(int m) {
   g.m = m;
   int qmin = (3 * m - 2 + 3) / 4;
   if (qmin < 1) qmin = 1;
-  g.Q = ((qmin + 7) / 8) * 8;
+  // Q a multiple of 8 (angle tiles of 8); beyond m = 96 a multiple of 16, so that the tiles pair with their
+  // mirrors and the third fold applies (a few more angles, a quarter fewer DMMAs)
+  const int qa = m > 96 ? 16 : 8;
+  g.Q = ((qmin + qa - 1) / qa) * qa;
   g.N = 4 * g.Q;
   g.NT = g.Q / 8;
   const int ev = (m + 1) / 2, od = m / 2;
@@ -102,7 +105,9 @@ __host__ __device__ constexpr int tf_koff(int m, int gr) { return gr == 0 ? 0 : 
 __host__ __device__ constexpr int tf_NU(int m, int gr) { return (tf_ke(m, gr) + 7) / 8; }
 __host__ __device__ constexpr int tf_nuoff(int m, int gr) { return gr == 0 ? 0 : tf_nuoff(m, gr - 1) + tf_NU(m, gr - 1); }
 // quadrant angle tiles and analysis k-steps of an output group (half the quadrant for the even groups)
-__host__ __device__ constexpr int tf_NT(int m) { return ((3 * m - 2 + 3) / 4 + 7) / 8; }
+__host__ __device__ constexpr int tf_NT(int m) {  // make_geo(m).NT
+  return m > 96 ? 2 * (((3 * m - 2 + 3) / 4 + 15) / 16) : ((3 * m - 2 + 3) / 4 + 7) / 8;
+}
 __host__ __device__ constexpr int tf_TE(int m, int gr) { return gr % 3 == 2 ? 2 * tf_NT(m) : tf_NT(m); }
 // first analysis k-step (units of 32 doubles) of group gr in the analysis table
 __host__ __device__ constexpr int tf_aoff(int m, int gr) {
