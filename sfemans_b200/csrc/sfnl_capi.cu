@@ -293,11 +293,11 @@ struct HostBuf {
 };
 size_t buf_rows(const HostBuf &b, int m) { return (size_t)b.nslot * (b.mrows > 0 ? b.mrows : m); }
 
-constexpr int kPipe = 3;
-constexpr size_t kChunkBytes = size_t(192) << 20;  // target bytes per chunk (inputs + outputs)
+constexpr int kPipe = 4;
+constexpr size_t kChunkBytes = size_t(512) << 20;  // target bytes per chunk (inputs + outputs)
 
 struct PipeState {
-  cudaStream_t st[kPipe] = {nullptr, nullptr, nullptr};
+  cudaStream_t st[kPipe] = {nullptr, nullptr, nullptr, nullptr};
 };
 PipeState g_pipe[kMaxDev];
 
