@@ -35,6 +35,7 @@ namespace {
 // and the fields shared by all tangents of a batch (the base state) are transformed once per point chunk.
 // G lives in a per-(device, stream) workspace; the points are processed in chunks that bound it.
 constexpr int kLargeSynMaxWarps = 12, kLargeProdWarps = 16, kLCT = 4, kLargeGroup = 3;
+constexpr int kLargeTfPairs = 4;  // mirror pairs per chunk of the third-fold program kernel (16 warps: 8 tiles x 2)
 constexpr size_t kLargeSynSmem = 200 * 1024;  // staged coefficients of one synthesis CTA
 
 struct LargeArgs {
@@ -300,7 +301,8 @@ template <int OP, int O0, int CPW>
 __global__ void __launch_bounds__(kLargeProdWarps * 32) large_prod_tf_kernel(const LargeArgs a) {
   constexpr int NI = op_nin(OP), NO = op_nout(OP);
   constexpr int NOG = NO - O0 < kLargeGroup ? NO - O0 : kLargeGroup;
-  extern __shared__ double pc_s[];  // [NOG][4 classes][4 local tiles][2][32]
+  constexpr int KP = kLargeTfPairs, LT = 2 * KP;  // pairs per chunk, local tiles
+  extern __shared__ double pc_s[];  // [NOG][4 classes][LT local tiles][2][32]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, q = lane & 3;
   const int b = a.batch_entry;
   const int64_t tile = blockIdx.x, p = tile * 8 + (lane >> 2);
@@ -314,14 +316,14 @@ __global__ void __launch_bounds__(kLargeProdWarps * 32) large_prod_tf_kernel(con
   const double *Gl = a.G + tile * NT * 256 + lane;
   const double *anav = a.ana + (size_t)(a.adj_out ? 1 : 0) * a.asteps * 32 + lane;
   const int NU_tot = a.tnuoff[6];
-  const size_t cst = (size_t)4 * 2 * 32;  // class stride in pc_s
-  for (int c0 = 0; c0 < NH; c0 += 2) {
-    const int npr = NH - c0 < 2 ? NH - c0 : 2;  // pairs in this chunk
-    // local tiles 0, 1: c0, c0+1; 2, 3: their mirrors NT-1-c0, NT-2-c0
+  const size_t cst = (size_t)LT * 2 * 32;  // class stride in pc_s
+  for (int c0 = 0; c0 < NH; c0 += KP) {
+    const int npr = NH - c0 < KP ? NH - c0 : KP;  // pairs in this chunk
+    // local tiles 0 .. KP-1: c0 + lt; KP .. 2KP-1: their mirrors NT-1-(c0 + lt - KP)
     if (warp < 4 * npr) {
       const int li = warp >> 1, e = warp & 1;
-      const int lt = li < npr ? li : 2 + li - npr;
-      const int t = lt < 2 ? c0 + lt : NT - 1 - (c0 + lt - 2);
+      const int lt = li < npr ? li : KP + li - npr;
+      const int t = lt < KP ? c0 + lt : NT - 1 - (c0 + lt - KP);
       double gq[4][NOG];
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
@@ -336,7 +338,7 @@ __global__ void __launch_bounds__(kLargeProdWarps * 32) large_prod_tf_kernel(con
       for (int o = 0; o < NOG; ++o) {
         const double s14 = gq[0][o] + gq[3][o], d14 = gq[0][o] - gq[3][o];
         const double s23 = gq[1][o] + gq[2][o], d32 = gq[2][o] - gq[1][o];
-        double *dst = pc_s + ((size_t)(o * 4) * 4 + lt) * 64 + e * 32 + lane;
+        double *dst = pc_s + ((size_t)(o * 4) * LT + lt) * 64 + e * 32 + lane;
         dst[0] = s14 + s23;        // PE
         dst[cst] = s14 - s23;      // PO
         dst[2 * cst] = d14 + d32;  // QE
@@ -361,8 +363,8 @@ __global__ void __launch_bounds__(kLargeProdWarps * 32) large_prod_tf_kernel(con
       const double *pa = pc_s + (size_t)c * cst + lane;
       if (odd) {
         for (int li = 0; li < 2 * npr; ++li) {
-          const int lt = li < npr ? li : 2 + li - npr;
-          const int t = lt < 2 ? c0 + lt : NT - 1 - (c0 + lt - 2);
+          const int lt = li < npr ? li : KP + li - npr;
+          const int t = lt < KP ? c0 + lt : NT - 1 - (c0 + lt - KP);
 #pragma unroll
           for (int e = 0; e < 2; ++e) {
             const double bv = __ldg(bt + (size_t)(2 * t + e) * 32);
@@ -379,7 +381,7 @@ __global__ void __launch_bounds__(kLargeProdWarps * 32) large_prod_tf_kernel(con
 #pragma unroll
             for (int o = 0; o < NOG; ++o) {
               const double *po = pa + (size_t)o * 4 * cst;
-              const double av = po[(size_t)(lt * 2 + e) * 32] + sg * po[(size_t)((2 + lt) * 2 + 1 - e) * 32 + lx];
+              const double av = po[(size_t)(lt * 2 + e) * 32] + sg * po[(size_t)((KP + lt) * 2 + 1 - e) * 32 + lx];
               dmma(y[j][o], av, bv);
             }
           }
@@ -530,11 +532,11 @@ int large_workspace(cudaStream_t st, size_t bytes, double **out) {
 template <int OP, int O0, int CPW>
 int launch_large_prod(const LargeArgs &la, bool tf, cudaStream_t st) {
   constexpr int NO = op_nout(OP), NOG = NO - O0 < kLargeGroup ? NO - O0 : kLargeGroup;
-  const size_t smem = sizeof(double) * (size_t)NOG * 4 * kLCT * 2 * 32;
-  if (tf)
-    large_prod_tf_kernel<OP, O0, CPW><<<(unsigned)la.tiles, kLargeProdWarps * 32, smem, st>>>(la);
-  else
-    large_prod_kernel<OP, O0, CPW><<<(unsigned)la.tiles, kLargeProdWarps * 32, smem, st>>>(la);
+  const size_t smem = sizeof(double) * (size_t)NOG * 4 * (tf ? 2 * kLargeTfPairs : kLCT) * 2 * 32;
+  auto kern = tf ? large_prod_tf_kernel<OP, O0, CPW> : large_prod_kernel<OP, O0, CPW>;
+  if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (large-m program and analysis)");
+  kern<<<(unsigned)la.tiles, kLargeProdWarps * 32, smem, st>>>(la);
   return check_launch("large-m program and analysis");
 }
 
