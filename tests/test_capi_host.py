@@ -200,3 +200,13 @@ def test_other_gauss_point_entry_checks():
     assert L.sfnl_curlh_cross_b_gauss_f64(d, None, d, d, d, d, d, d, 5, 2, 6, 7, 2, 0, None, NULL) == -1
     assert L.sfnl_curlh_cross_b_gauss_f64(d, d, d, d, d, d, d, d, 5, 2, 11, 7, 2, 0, None, NULL) == -4
     assert L.sfnl_smb_ugradc_gauss(d, d, None, 3, d, d, d, d, 2, d, d, 5, 2, 6, 7, 2, 1) == -1
+
+
+def test_gauss_point_entries_with_no_elements_do_nothing():
+    # me = 0: no Gauss points, nothing to launch (and no device needed)
+    L = sf.lib()
+    d = ctypes.c_void_p(16)
+    assert L.sfnl_cross_gauss_f64(d, d, d, d, d, d, None, d, 5, 0, 6, 7, 4, 0, None, NULL) == 0
+    assert L.sfnl_curlh_cross_b_gauss_f64(d, d, d, d, d, d, d, d, 5, 0, 6, 7, 4, 0, None, NULL) == 0
+    for cons in (0, 1):
+        assert L.sfnl_ugradc_gauss_f64(d, d, None, cons, d, d, d, d, d, d, 5, 0, 6, 7, 4, 0, None, NULL) == 0
