@@ -3,7 +3,7 @@
  *
  * TEST INFRASTRUCTURE ONLY.  This file is the checker: the parity tests,
  * __graft_entry__.smoke() and the CPU-baseline leg of bench.py call it to
- * judge the CUDA path.  The product library (sfemans_b200/csrc) never links,
+ * check the CUDA path.  The product library (sfemans_b200/csrc) never links,
  * loads or calls it.
  *
  * It restates, step by step and in long double arithmetic, the three SFEMaNS
