@@ -167,7 +167,10 @@ int sfnl_bundle_mhd_f64(const double *u, const double *w, const double *b, const
  *   m_max_pad  <= 0: 3*nmod/2, the caller's choice (:625)
  *   work       device buffer of 12*l_G*me*nmod doubles for RotV and W, or NULL: a buffer
  *              owned by the library (one per device, grown with cudaMalloc when too small;
- *              calls that overlap on the GPU then share it and race)
+ *              calls that overlap on the GPU then share it and race).  At nmod = 64 on P2
+ *              elements (n_w = 6) RotV and W are built inside the product kernel and work
+ *              holds node-major copies of the nodal fields instead (6*np_nodes*nmod doubles per
+ *              field, v and omega), when they fit in it
  * ------------------------------------------------------------------------- */
 int sfnl_cross_gauss_f64(const double *v, const int *jj, const double *ww, const double *dw, const double *rr,
                          const int *list_mode, const double *omega, double *out, int np_nodes, int me, int n_w,
