@@ -33,6 +33,9 @@ namespace {
 //                     accumulators of its output tiles; the outputs are written at the end.
 // The whole program is evaluated on the grid, so a linearised product du x w + u x dw is analysed once,
 // and the fields shared by all tangents of a batch (the base state) are transformed once per point chunk.
+// With an even number of quadrant angle tiles (every m > 96: the quadrant is a multiple of 16 angles)
+// large_syn_tf_kernel and large_prod_tf_kernel do the same with the third fold (mirror tile pairs),
+// a quarter fewer DMMAs.
 // G lives in a per-(device, stream) workspace; the points are processed in chunks that bound it.
 constexpr int kLargeSynMaxWarps = 12, kLargeProdWarps = 16, kLCT = 4, kLargeGroup = 3;
 constexpr int kLargeTfPairs = 4;  // mirror pairs per chunk of the third-fold program kernel (16 warps: 8 tiles x 2)
