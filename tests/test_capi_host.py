@@ -210,3 +210,22 @@ def test_gauss_point_entries_with_no_elements_do_nothing():
     assert L.sfnl_curlh_cross_b_gauss_f64(d, d, d, d, d, d, d, d, 5, 0, 6, 7, 4, 0, None, NULL) == 0
     for cons in (0, 1):
         assert L.sfnl_ugradc_gauss_f64(d, d, None, cons, d, d, d, d, d, d, 5, 0, 6, 7, 4, 0, None, NULL) == 0
+
+
+def test_profiling_mesh_is_a_consistent_p2_mesh():
+    # the structured P2 mesh of the profiling driver: partition of unity, exact derivatives of linear
+    # fields, and the solid-body-rotation curl of the Navier-Stokes caller's restatement
+    from sfemans_b200.profile_case import p2_rectangle
+    from oracle import ref_fft as R
+
+    m = p2_rectangle(5, 4)
+    assert m["jj"].shape == (6, 40) and m["jj"].min() == 1 and m["jj"].max() == m["np"]
+    assert np.abs(m["ww"].sum(axis=0) - 1.0).max() < 1e-14
+    assert np.abs(m["dw"].sum(axis=1)).max() < 1e-12
+    for c in range(2):
+        d = np.einsum("dnle,ne->dle", m["dw"], m["rr"][c][m["jj"] - 1])
+        assert np.abs(d[c] - 1.0).max() < 1e-12 and np.abs(d[1 - c]).max() < 1e-12
+    V = np.zeros((m["np"], 6, 1), order="F")
+    V[:, 2, 0] = m["rr"][0]
+    _, rot, _ = R.c_cross_gauss(V, dict(m, n_w=6, l_G=7), [0], product=False)
+    assert np.abs(rot[:, 4, 0] - 2.0).max() < 1e-12
