@@ -214,6 +214,19 @@ int sfnl_smb_ugradc_gauss(const double *V_in, const double *c_in, const double *
                           const int *list_mode, double *c_out, int np_nodes, int me, int n_w, int l_G, int nmod,
                           int nb_procs);
 
+/* The Gauss-point operands alone (the loops before the FFT call in the three callers above), for
+ * callers that run the product themselves, e.g. over a mode-distributed communicator with
+ * sfemans_b200.parallel.  Device arrays; every output (l_G*me, nslot, nmod) Fortran:
+ *   SFNL_GAUSS_NS       v (+ omega, may be NULL)  o0 = RotV + 2 Om, o1 = W           (6 slots each)
+ *   SFNL_GAUSS_LORENTZ  v = H, v2 = B            o0 = curl H, o1 = B at the points  (6 slots each)
+ *   SFNL_GAUSS_ADVECT   v = u, v2 = c, heat      o0 = heat grad c, o1 = W (6 slots); conservative: o2 =
+ *                       div u, o3 = heat c (2 slots each), else o2, o3 ignored.  */
+enum { SFNL_GAUSS_NS = 0, SFNL_GAUSS_LORENTZ = 1, SFNL_GAUSS_ADVECT = 2 };
+int sfnl_gauss_operands_f64(int kind, const double *v, const double *v2, const double *omega, const double *heat,
+                            int conservative, const int *jj, const double *ww, const double *dw, const double *rr,
+                            const int *list_mode, double *o0, double *o1, double *o2, double *o3, int np_nodes,
+                            int me, int n_w, int l_G, int nmod, sfnl_stream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Linearised cross product N(u, w) = u x w about a base state (u, w).
  * New capability: the reference's LightKrylov operator binds rmatvec to the

@@ -97,6 +97,7 @@ _SIGS = {
     "sfnl_smb_curlh_cross_b_gauss": [_P] * 6 + [_I] + [_P] * 2 + [_I] * 6,
     "sfnl_ugradc_gauss_f64": [_P] * 3 + [_I] + [_P] * 6 + [_I] * 6 + [_P, _P],
     "sfnl_smb_ugradc_gauss": [_P] * 3 + [_I] + [_P] * 4 + [_I] + [_P] * 2 + [_I] * 6,
+    "sfnl_gauss_operands_f64": [_I] + [_P] * 4 + [_I] + [_P] * 9 + [_I] * 5 + [_P],
     "sfnl_max_vel_f64": [_P, _P, _L, _I, _I, _I, _P],
     "sfnl_fft_par_real_planes": [_I, _I],
     "sfnl_fft_par_real": [_P, _P] + [_I] * 5,
@@ -342,6 +343,30 @@ def ugradc_gauss(v, c, mesh, list_mode, heat=None, conservative=False, m_max_pad
                                        ptr(list_mode), _dptr(out, "out"), npn, me, n_w, l_G, nmod, m_max_pad or 0,
                                        ptr(work), _stream(stream)))
     return out
+
+
+GAUSS_NS, GAUSS_LORENTZ, GAUSS_ADVECT = 0, 1, 2
+
+
+def gauss_operands(kind, v, mesh, list_mode, v2=None, omega=None, heat=None, conservative=False, stream=None):
+    """The Gauss-point operands of one caller without the product (CUDA tensors, ``mesh`` and
+    ``list_mode`` as in :func:`cross_gauss`): GAUSS_NS -> (RotV + 2 omega, W); GAUSS_LORENTZ (v = H,
+    v2 = B) -> (curl H, B); GAUSS_ADVECT (v = u, v2 = c) -> (heat grad c, W[, div u, heat c] when
+    conservative).  Each (l_G*me, nslot, nmod)."""
+    npn, nmod, n_w, me, l_G = _gauss_dims(v, mesh)
+    ng = l_G * me
+    outs = [fortran_empty(ng, 6, nmod, device=v.device), fortran_empty(ng, 6, nmod, device=v.device)]
+    cons = kind == GAUSS_ADVECT and conservative
+    if cons:
+        outs += [fortran_empty(ng, 2, nmod, device=v.device), fortran_empty(ng, 2, nmod, device=v.device)]
+    ptr = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    o = outs + [None] * (4 - len(outs))
+    _check(lib().sfnl_gauss_operands_f64(kind, _dptr(v, "v"), None if v2 is None else _dptr(v2, "v2"),
+                                         None if omega is None else _dptr(omega, "omega"), ptr(heat),
+                                         1 if cons else 0, ptr(mesh["jj"]), ptr(mesh["ww"]), ptr(mesh["dw"]),
+                                         ptr(mesh["rr"]), ptr(list_mode), *[ptr(t) for t in o], npn, me, n_w, l_G,
+                                         nmod, _stream(stream)))
+    return tuple(outs)
 
 
 def bundle_mhd(u, w, b, j, gradt, m_max_pad: int | None = None, outs=None, algo: int = ALGO_AUTO,

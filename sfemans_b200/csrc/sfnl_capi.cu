@@ -911,6 +911,25 @@ int sfnl_smb_curlh_cross_b_gauss(const double *V_in, const double *W_in, const i
                     np_nodes, me, n_w, l_G, nmod, nb_procs);
 }
 
+int sfnl_gauss_operands_f64(int kind, const double *v, const double *v2, const double *omega, const double *heat,
+                            int conservative, const int *jj, const double *ww, const double *dw, const double *rr,
+                            const int *list_mode, double *o0, double *o1, double *o2, double *o3, int np_nodes,
+                            int me, int n_w, int l_G, int nmod, sfnl_stream_t stream) {
+  static_assert(SFNL_GAUSS_NS == GK_NS && SFNL_GAUSS_LORENTZ == GK_LORENTZ && SFNL_GAUSS_ADVECT == GK_ADVECT,
+                "caller kinds");
+  if (kind < SFNL_GAUSS_NS || kind > SFNL_GAUSS_ADVECT) return set_error(SFNL_ERR_ARG, "kind must be SFNL_GAUSS_*");
+  if (conservative != 0 && conservative != 1) return set_error(SFNL_ERR_ARG, "conservative must be 0 or 1");
+  int rc = check_gauss(np_nodes, me, n_w, l_G, nmod);
+  if (rc) return rc;
+  if ((int64_t)l_G * me == 0) return SFNL_OK;
+  const bool cons = kind == GK_ADVECT && conservative;
+  if (!v || !jj || !ww || !dw || !rr || !list_mode || !o0 || !o1 || (kind != GK_NS && !v2) || (cons && (!o2 || !o3)))
+    return set_error(SFNL_ERR_ARG, "null array");
+  GaussArgs ga{v, kind == GK_NS ? omega : nullptr, ww, dw, rr, jj, list_mode, np_nodes, me, n_w, l_G, nmod, v2,
+               kind == GK_ADVECT ? heat : nullptr};
+  return launch_gauss_eval(ga, kind, o0, o1, cons ? o2 : nullptr, cons ? o3 : nullptr, as_stream(stream));
+}
+
 int sfnl_ugradc_gauss_f64(const double *v, const double *c, const double *heat, int conservative, const int *jj,
                           const double *ww, const double *dw, const double *rr, const int *list_mode, double *out,
                           int np_nodes, int me, int n_w, int l_G, int nmod, int m_max_pad, double *work,

@@ -148,3 +148,44 @@ def fft_max_vel_distributed(group, x, nb_procs, bloc_size, m_max_pad, compute=No
     t = torch.tensor([float((compute or _default_max_vel)(xb, m_max_pad))], dtype=torch.float64, device=x.device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
     return float(t.item())
+
+
+def _default_gauss_operands(kind, V_in, mesh, list_mode, V2_in, omega, heat, conservative):
+    from . import gauss_operands
+
+    return gauss_operands(kind, V_in, mesh, list_mode, v2=V2_in, omega=omega, heat=heat, conservative=conservative)
+
+
+def smb_gauss_distributed(kind, group, mesh, list_mode, V_in, nb_procs, V2_in=None, omega=None, heat=None,
+                          conservative=False, temps=None, operands=None, compute=None):
+    """The Gauss-point callers over the reference's mode-distributed communicator (comm_one_d(2)):
+    smb_cross_prod_gauss_sft_par (kind GAUSS_NS, subroutine_ns_with_velocity.F90:512-629),
+    smb_CurlH_cross_B_gauss_sft_par (GAUSS_LORENTZ, V_in = H, V2_in = B; subroutine_ns_with_m.F90:788-883)
+    and smb_ugradc_gauss_fft_par (GAUSS_ADVECT, V_in = u, V2_in = c; subroutine_level_set.F90:434-534, and
+    with ``conservative`` and ``heat`` subroutine_temperature_with_T.F90:247-350).
+
+    Every rank holds its m_max_c modes of the nodal fields (``list_mode``: their mode numbers); the
+    operands are built for those modes, and the product runs through :func:`fft_par_distributed` with the
+    callers' bloc_size = l_G*me/nb_procs + 1 and m_max_pad = 3*m_max_c*nb_procs/2 (:625-626).  Returns
+    this rank's modes of the result, (l_G*me, 6 | 2, m_max_c).  ``operands(kind, V_in, mesh, list_mode,
+    V2_in, omega, heat, conservative)`` builds the Gauss-point arrays (default: the CUDA kernel, ``mesh``
+    holding CUDA tensors as for :func:`sfemans_b200.cross_gauss`); ``compute`` is passed to
+    :func:`fft_par_distributed`.
+    """
+    import torch
+
+    from . import GAUSS_ADVECT, GAUSS_LORENTZ, GAUSS_NS
+
+    if kind not in (GAUSS_NS, GAUSS_LORENTZ, GAUSS_ADVECT):
+        raise ValueError("kind must be GAUSS_NS, GAUSS_LORENTZ or GAUSS_ADVECT")
+    ops = (operands or _default_gauss_operands)(kind, V_in, mesh, list_mode, V2_in, omega, heat, conservative)
+    ng, _, mc = ops[0].shape
+    bloc = ng // nb_procs + 1
+    pad = 3 * mc * nb_procs // 2
+    empty = lambda nsl: torch.zeros((mc, nsl, ng), dtype=ops[0].dtype, device=ops[0].device).permute(2, 1, 0)  # noqa: E731
+    if kind != GAUSS_ADVECT:
+        return fft_par_distributed("cross", group, ops[0], ops[1], empty(6), nb_procs, bloc, pad, temps, compute)
+    out = fft_par_distributed("dot", group, ops[0], ops[1], empty(2), nb_procs, bloc, pad, temps, compute)
+    if conservative:  # + FFT_PAR_PROD_DCL(Div, Cgauss) (subroutine_temperature_with_T.F90:339-342)
+        out += fft_par_distributed("prod", group, ops[2], ops[3], empty(2), nb_procs, bloc, pad, None, compute)
+    return out

@@ -150,3 +150,32 @@ def test_medium_mesh_other_callers_against_operands_and_library_products():
     _, g, w, d, cg = R.c_ugradc_gauss(H, C, mesh, lm, heat=heat, conservative=True, product=False)
     ref = R.fft_par("dot", g, w, 96, workers=8) + R.fft_par("prod", d, cg, 96, workers=8)
     assert R.rel_l2(sf.smb_ugradc_gauss_fft_par_temperature(None, mesh, lm, heat, H, C), ref) <= FP64_TOL
+
+
+@pytest.mark.parametrize("kind,cons", [(sf.GAUSS_NS, False), (sf.GAUSS_LORENTZ, False), (sf.GAUSS_ADVECT, False),
+                                       (sf.GAUSS_ADVECT, True)])
+def test_operands_alone_match_the_restatement(kind, cons):
+    # sfnl_gauss_operands_f64: the operand arrays the callers pass to the products (for callers that run
+    # the product themselves, e.g. over a mode-distributed communicator)
+    mesh = R.synthetic_p2_mesh(6, 4, 13)
+    m = 8
+    lm = [2 * i + 1 for i in range(m)]
+    V = R.synthetic_field(mesh["np"], 6, m, 0.2, 91)
+    V2 = R.synthetic_field(mesh["np"], 6 if kind == sf.GAUSS_LORENTZ else 2, m, 0.2, 92)
+    om = R.precession_omega(mesh["np"], lm, 0.4, 0.3) if kind == sf.GAUSS_NS else None
+    heat = np.linspace(0.5, 2.0, mesh["me"]) if cons else None
+    if kind == sf.GAUSS_NS:
+        ref = R.c_cross_gauss(V, mesh, lm, om, product=False)[1:]
+    elif kind == sf.GAUSS_LORENTZ:
+        ref = R.c_curlh_cross_b_gauss(V, V2, mesh, lm, product=False)[1:]
+    else:
+        ref = R.c_ugradc_gauss(V, V2, mesh, lm, heat=heat, conservative=cons, product=False)[1:]
+        ref = ref if cons else ref[:2]
+    got = sf.gauss_operands(kind, sf.to_device(V), _dev_mesh(mesh), torch.tensor(lm, dtype=torch.int32, device="cuda"),
+                            v2=None if kind == sf.GAUSS_NS else sf.to_device(V2),
+                            omega=None if om is None else sf.to_device(om),
+                            heat=None if heat is None else torch.tensor(heat, device="cuda"), conservative=cons)
+    torch.cuda.synchronize()
+    assert len(got) == len(ref)
+    for g, r in zip(got, ref):
+        assert R.rel_l2(sf.to_host(g), r) <= 1e-13

@@ -13,8 +13,10 @@ import torch.distributed as dist
 import torch.multiprocessing as mp
 
 from oracle import ref_fft as R
+import sfemans_b200 as sf
 from sfemans_b200 import KINDS
-from sfemans_b200.parallel import fft_max_vel_distributed, fft_par_distributed, fft_par_real_distributed, shard_range
+from sfemans_b200.parallel import (fft_max_vel_distributed, fft_par_distributed, fft_par_real_distributed, shard_range,
+                                   smb_gauss_distributed)
 
 
 @pytest.mark.parametrize("npts,world", [(0, 1), (7, 3), (28000, 8), (1_400_000, 8), (5, 8)])
@@ -122,3 +124,63 @@ def test_synthesis_routines_over_a_mode_distributed_communicator(kind, world, np
     assert all(p.exitcode == 0 for p in procs)
     for r in range(world):
         assert res[r] < 1e-14, res
+
+
+def _t(a):
+    return torch.from_numpy(np.ascontiguousarray(a.T)).permute(*reversed(range(a.ndim)))
+
+
+def _oracle_operands(kind, V, mesh, lm, V2, omega, heat, conservative):
+    to_np = lambda t: None if t is None else np.asfortranarray(t.permute(2, 1, 0).contiguous().numpy().T)  # noqa: E731
+    if kind == sf.GAUSS_NS:
+        _, rot, w = R.c_cross_gauss(to_np(V), mesh, lm, to_np(omega), product=False)
+        return _t(rot), _t(w)
+    if kind == sf.GAUSS_LORENTZ:
+        _, rot, w = R.c_curlh_cross_b_gauss(to_np(V), to_np(V2), mesh, lm, product=False)
+        return _t(rot), _t(w)
+    _, g, w, d, cg = R.c_ugradc_gauss(to_np(V), to_np(V2), mesh, lm, heat=heat, conservative=conservative,
+                                      product=False)
+    return _t(g), _t(w), _t(d), _t(cg)
+
+
+def _gauss_worker(rank, world, port, kind, cons, m, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        mesh = R.synthetic_p2_mesh(4, 3, 9)
+        lm = [2 * i + 1 for i in range(m)]  # a select_mode-like list of mode numbers
+        V = R.synthetic_field(mesh["np"], 6, m, 0.2, 71)
+        V2 = R.synthetic_field(mesh["np"], 6 if kind == sf.GAUSS_LORENTZ else 2, m, 0.2, 72)
+        om = R.precession_omega(mesh["np"], lm, 0.4, 0.3) if kind == sf.GAUSS_NS else None
+        heat = np.linspace(0.5, 2.0, mesh["me"]) if cons else None
+        mc = m // world
+        sl = slice(rank * mc, (rank + 1) * mc)
+        loc = lambda A: None if A is None else _t(np.asfortranarray(A[:, :, sl]))  # noqa: E731
+        out = smb_gauss_distributed(kind, None, mesh, lm[sl], loc(V), world, V2_in=loc(V2), omega=loc(om),
+                                    heat=heat, conservative=cons, operands=_oracle_operands,
+                                    compute=_oracle_compute)
+        if kind == sf.GAUSS_NS:
+            ref = R.c_cross_gauss(V, mesh, lm, om)[0]
+        elif kind == sf.GAUSS_LORENTZ:
+            ref = R.c_curlh_cross_b_gauss(V, V2, mesh, lm)[0]
+        else:
+            ref = R.c_ugradc_gauss(V, V2, mesh, lm, heat=heat, conservative=cons)[0]
+        q.put((rank, float(np.abs(out.numpy() - ref[..., sl]).max() / np.abs(ref).max())))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("kind,cons,world,m", [(0, False, 2, 4), (1, False, 3, 6), (2, False, 2, 4), (2, True, 2, 6)])
+def test_gauss_point_callers_over_a_mode_distributed_communicator(kind, cons, world, m):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gauss_worker, args=(r, world, port, kind, cons, m, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    res = dict(q.get(timeout=5) for _ in range(world))
+    assert all(p.exitcode == 0 for p in procs)
+    for r in range(world):
+        assert res[r] < 1e-13, res
