@@ -229,3 +229,15 @@ def test_profiling_mesh_is_a_consistent_p2_mesh():
     V[:, 2, 0] = m["rr"][0]
     _, rot, _ = R.c_cross_gauss(V, dict(m, n_w=6, l_G=7), [0], product=False)
     assert np.abs(rot[:, 4, 0] - 2.0).max() < 1e-12
+
+
+def test_gauss_operands_entry_checks():
+    L = sf.lib()
+    d = ctypes.c_void_p(16)
+    ops = [d, d, None, None]
+    assert L.sfnl_gauss_operands_f64(3, d, d, None, None, 0, d, d, d, d, d, *ops, 5, 2, 6, 7, 2, NULL) == -1  # kind
+    assert L.sfnl_gauss_operands_f64(2, d, d, None, None, 2, d, d, d, d, d, *ops, 5, 2, 6, 7, 2, NULL) == -1  # flag
+    assert L.sfnl_gauss_operands_f64(1, d, None, None, None, 0, d, d, d, d, d, *ops, 5, 2, 6, 7, 2, NULL) == -1  # no B
+    assert L.sfnl_gauss_operands_f64(2, d, d, None, None, 1, d, d, d, d, d, *ops, 5, 2, 6, 7, 2, NULL) == -1  # no o2/o3
+    assert L.sfnl_gauss_operands_f64(0, d, None, None, None, 0, d, d, d, d, d, *ops, 5, 2, 11, 7, 2, NULL) == -4  # n_w
+    assert L.sfnl_gauss_operands_f64(0, d, None, None, None, 0, d, d, d, d, d, *ops, 5, 0, 6, 7, 2, NULL) == 0  # me = 0
