@@ -340,7 +340,7 @@ int sfnl_cross_f64_noalloc(const double *v1, const double *v2, double *out, int6
 const char *sfnl_last_error(void); /* message of the last failing call on this thread */
 const char *sfnl_version(void);
 int sfnl_set_check_finite(int on); /* 1: scan outputs for NaN/Inf after each call (synchronises) */
-int sfnl_finalize(void);           /* release cached device tables and pinned staging buffers */
+int sfnl_finalize(void);           /* release cached device tables, workspaces and staging buffers */
 /* Seconds spent in the last *_host call of this thread: [copy in, kernels, copy out]. */
 int sfnl_last_host_timing(double *seconds3);
 

@@ -467,6 +467,7 @@ int sfnl_last_host_timing(double *s3) {
 
 int sfnl_finalize(void) {
   fast_release_tables();
+  large_release_workspaces();
   split_release_tables();
   for (int d = 0; d < kMaxDev; ++d) {
     DevState &s = g_dev[d];

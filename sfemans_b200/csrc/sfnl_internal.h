@@ -25,6 +25,7 @@ int launch_fast(const ProgArgs &a, cudaStream_t st);   // sfnl_fast.cu
 bool fast_supported(int op, int m, int N_int);          // sfnl_fast.cu
 int fast_grid_length(int m);                            // sfnl_fast.cu
 void fast_release_tables();                             // sfnl_fast.cu
+void large_release_workspaces();                        // sfnl_large.cu: the grid-value workspaces
 int launch_split(const ProgArgs &a, int split, cudaStream_t st);  // sfnl_split.cu
 void split_release_tables();                            // sfnl_split.cu
 // Synthesis only (sfnl_synth.cu): out (N, nslot/2, np); vmax a zeroed device double that receives the

@@ -619,6 +619,19 @@ constexpr size_t kLargeWorkspaceBytes = size_t(1) << 30;  // grid values of one 
 
 }  // namespace
 
+void large_release_workspaces() {
+  std::lock_guard<std::mutex> lk(g_lws_mu);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  for (auto &kv : g_lws)
+    if (kv.second.first) {
+      cudaSetDevice(kv.first.first);
+      cudaFree(kv.second.first);  // waits for the work still reading it
+    }
+  g_lws.clear();
+  cudaSetDevice(prev);
+}
+
 // The two-kernel form: per point chunk, the batch-invariant fields (base state) once, then per batch
 // entry its own fields and the program's outputs in groups of three (one launch per group).
 int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStream_t st) {
