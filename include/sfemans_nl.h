@@ -60,7 +60,9 @@ enum {
   SFNL_ERR_UNSUPPORTED = -4, /* size beyond this build's limits, nb_procs != 1 on one GPU */
   SFNL_ERR_CUDA = -5,        /* a CUDA runtime call or kernel launch failed */
   SFNL_ERR_NONFINITE = -6,   /* (check mode) a NaN/Inf was found in the output */
-  SFNL_ERR_ALLOC = -7        /* device or pinned host allocation failed */
+  SFNL_ERR_ALLOC = -7,       /* device or pinned host allocation failed */
+  SFNL_ERR_TIMEOUT = -8      /* a split-form kernel gave up a bounded wait on its tensor-core
+                                operations; the outputs of that call are incomplete */
 };
 
 /* Algorithm of the all-FP64 forms. */
@@ -271,7 +273,10 @@ int sfnl_mhd_vjp_split(const double *u, const double *w, const double *b, const 
  * shim.  Arguments are those of fft_parallel.F90:147 / :330 / :502:
  *   np, nb_field, m_max_c = SIZE(V1_in,1..3); nb_procs, bloc_size, m_max_pad as
  *   passed by the caller; temps (may be NULL) = the optional REAL(8) temps(3):
- *   zeroed, then temps[1] += seconds spent on the GPU (copies included).
+ *   zeroed (fft_parallel.F90:179), then temps[0] += device seconds of the
+ *   host<->device copies (where the reference counts its MPI_ALLTOALLs),
+ *   temps[1] += device seconds of the kernels (its FFTs and product), temps[2]
+ *   stays 0 (no repacking); sums over point chunks that overlap on streams.
  * One GPU holds all modes, so nb_procs must be 1 (SFNL_ERR_UNSUPPORTED
  * otherwise); bloc_size is checked (np <= nb_procs*bloc_size, the reference's
  * buffer bound) and otherwise unused: there are no dummy points.
@@ -340,8 +345,22 @@ int sfnl_cross_f64_noalloc(const double *v1, const double *v2, double *out, int6
 const char *sfnl_last_error(void); /* message of the last failing call on this thread */
 const char *sfnl_version(void);
 int sfnl_set_check_finite(int on); /* 1: scan outputs for NaN/Inf after each call (synchronises) */
-int sfnl_finalize(void);           /* release cached device tables, workspaces and staging buffers */
-/* Seconds spent in the last *_host call of this thread: [copy in, kernels, copy out]. */
+/* Releases cached device tables, workspaces and staging buffers, and forgets the
+ * per-device set-up of sfnl_cross_f64_noalloc.  Call it before cudaDeviceReset or
+ * any other teardown of a device's primary context while the library stays
+ * loaded: cached device addresses do not survive the context. */
+int sfnl_finalize(void);
+/* Host-side fault injection for tests of the error path: marks the split-form
+ * status word as a kernel does when a bounded wait on its tensor-core
+ * operations gives up (no GPU work is involved).  The next split-form call
+ * returns SFNL_ERR_TIMEOUT and clears the word, as after a real timeout. */
+int sfnl_test_inject_timeout(void);
+/* Device-timed seconds of the last host-array call of this thread (the *_host,
+ * sfnl_fft_* and sfnl_smb_* entries): [0] host<->device copies, [1] kernels,
+ * [2] 0 (nothing is repacked).  Each is a sum over the call's point chunks; the
+ * chunks run on several streams, so [0] + [1] may exceed the call's wall time.
+ * The same two sums are added to temps(1) and temps(2) where a temps argument
+ * is passed. */
 int sfnl_last_host_timing(double *seconds3);
 
 #ifdef __cplusplus

@@ -134,6 +134,61 @@ def _ptr(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
+# ----------------------------------------------------------------------------
+# O(N log N) C restatement on host threads (the timed CPU baseline)
+# ----------------------------------------------------------------------------
+_CPU = None
+
+
+def _cpu_lib():
+    global _CPU
+    if _CPU is None:
+        so = os.path.join(HERE, "_build", "libsfnl_cpu.so")
+        if not os.path.exists(so):
+            subprocess.check_call(["make", "-s", "-C", HERE])
+        lib = ctypes.CDLL(so)
+        P = ctypes.POINTER(ctypes.c_double)
+        lib.sfnl_cpu_product.restype = ctypes.c_int
+        lib.sfnl_cpu_product.argtypes = [ctypes.c_int, P, P, P, ctypes.c_int64] + [ctypes.c_int] * 3
+        lib.sfnl_cpu_mhd_bundle.restype = ctypes.c_int
+        lib.sfnl_cpu_mhd_bundle.argtypes = [P] * 9 + [ctypes.c_int64] + [ctypes.c_int] * 3
+        lib.sfnl_cpu_threads.restype = ctypes.c_int
+        lib.sfnl_cpu_threads.argtypes = []
+        _CPU = lib
+    return _CPU
+
+
+def cpu_threads() -> int:
+    return int(_cpu_lib().sfnl_cpu_threads())
+
+
+def cpu_product(op: str, V1, V2, m_max_pad: int, n_theta: int | None = None, threads: int = 0):
+    """FFT_PAR_{CROSS,DOT,}_PROD_DCL by the C restatement with O(N log N) real FFTs on ``threads``
+    host threads (0: all), grid N = n_theta or the reference's 2*m_max_pad - 1."""
+    V1 = np.asfortranarray(V1, dtype=np.float64)
+    V2 = np.asfortranarray(V2, dtype=np.float64)
+    npts, _, m = V1.shape
+    N = n_theta or 2 * m_max_pad - 1
+    out = np.zeros(out_shape(op, npts, m), order="F")
+    rc = _cpu_lib().sfnl_cpu_product({"cross": 0, "dot": 1, "prod": 2}[op], _ptr(V1), _ptr(V2), _ptr(out), npts, m, N,
+                                     threads)
+    if rc:
+        raise RuntimeError(f"sfnl_cpu_product failed ({rc})")
+    return out
+
+
+def cpu_mhd_bundle(u, w, b, j, gradT, m_max_pad: int, n_theta: int | None = None, threads: int = 0):
+    """(u x w, u x b, j x b, u . gradT) by the C restatement, point block by point block."""
+    ins = [np.asfortranarray(x, dtype=np.float64) for x in (u, w, b, j, gradT)]
+    npts, _, m = ins[0].shape
+    N = n_theta or 2 * m_max_pad - 1
+    outs = [np.zeros((npts, 6, m), order="F") for _ in range(3)] + [np.zeros((npts, 2, m), order="F")]
+    rc = _cpu_lib().sfnl_cpu_mhd_bundle(*[_ptr(x) for x in ins + outs], npts, m, N, threads)
+    if rc:
+        raise RuntimeError(f"sfnl_cpu_mhd_bundle failed ({rc})")
+    return tuple(outs)
+
+
 def c_oracle(op: str, V1, V2, m_max_pad: int, nb_procs: int = 1, bloc_size: int | None = None,
              n_theta: int | None = None):
     """Long-double restatement of FFT_PAR_*_DCL on global arrays.

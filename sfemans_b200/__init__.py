@@ -50,7 +50,7 @@ SPLIT_BF16X2, SPLIT_BF16X3 = 2, 3
 
 ERRORS = {
     0: "OK", -1: "SFNL_ERR_ARG", -2: "SFNL_ERR_SHAPE", -3: "SFNL_ERR_ALIAS", -4: "SFNL_ERR_UNSUPPORTED",
-    -5: "SFNL_ERR_CUDA", -6: "SFNL_ERR_NONFINITE", -7: "SFNL_ERR_ALLOC",
+    -5: "SFNL_ERR_CUDA", -6: "SFNL_ERR_NONFINITE", -7: "SFNL_ERR_ALLOC", -8: "SFNL_ERR_TIMEOUT",
 }
 
 
@@ -106,6 +106,7 @@ _SIGS = {
     "sfnl_set_check_finite": [_I],
     "sfnl_finalize": [],
     "sfnl_last_host_timing": [_P],
+    "sfnl_test_inject_timeout": [],
 }
 
 

@@ -10,7 +10,6 @@
 //   SPLIT sfnl_split.cu  bf16-sliced tcgen05 contractions, FP64 recombination
 #include <cuda_runtime.h>
 
-#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -188,14 +187,25 @@ int run_fp64(ProgArgs a, int algo, int N_caller, cudaStream_t st) {
   return rc;
 }
 
+int timeout_error() {
+  return set_error(SFNL_ERR_TIMEOUT,
+                   "a split-form kernel gave up waiting for its tensor-core operations: the outputs of that call are "
+                   "incomplete");
+}
+
 int run_split(ProgArgs a, int split, int N_caller, cudaStream_t st) {
   if (split != SFNL_SPLIT_BF16X2 && split != SFNL_SPLIT_BF16X3) return set_error(SFNL_ERR_ARG, "split must be 2 or 3");
   if (!op_bilinear(a.op))
     return set_error(SFNL_ERR_UNSUPPORTED, "split forms: quotients and the tension tensor depend on the grid (use GRID)");
   if (!dealiased(a.m, N_caller)) return set_error(SFNL_ERR_ALIAS, "split forms need a dealiasing pad (2*m_max_pad-1 >= 3*m_max-2)");
   if (!split_supported(a.op, a.m)) return set_error(SFNL_ERR_UNSUPPORTED, "split form not built for this program/size");
+  // The split kernels report a bounded wait that gave up through a mapped status word; the device entry
+  // points do not synchronise, so a failure of an earlier call surfaces at the next split call (or after
+  // the synchronisation of a host-array call or of the finite-check mode).
+  if (split_take_status()) return timeout_error();
   int rc = launch_split(a, split, st);
   if (rc == SFNL_OK && g_check_finite) rc = scan_outputs(a, st);
+  if (rc == SFNL_OK && g_check_finite && split_take_status()) rc = timeout_error();
   return rc;
 }
 
@@ -296,6 +306,66 @@ size_t buf_rows(const HostBuf &b, int m) { return (size_t)b.nslot * (b.mrows > 0
 constexpr int kPipe = 4;
 constexpr size_t kChunkBytes = size_t(512) << 20;  // target bytes per chunk (inputs + outputs)
 
+// Device-timed intervals of a host call: each interval is a pair of CUDA events on the stream that
+// runs it, tagged 0 (host<->device copies) or 1 (kernels).  sum() adds the durations per tag after
+// the streams have been synchronised.  The reference's temps(1) is the MPI_ALLTOALL time, temps(2)
+// the FFTs and the product and temps(3) the repacking (fft_parallel.F90:203-290); here the copies
+// stand where the all-to-alls stood, and nothing is repacked.
+struct Intervals {
+  std::vector<cudaEvent_t> ev;  // begin, end, begin, end, ...
+  std::vector<int> tag;
+  bool ok = true;
+  int begin(cudaStream_t st) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+      cudaGetLastError();
+      if (a) cudaEventDestroy(a);
+      ok = false;
+      return -1;
+    }
+    ev.push_back(a);
+    ev.push_back(b);
+    tag.push_back(0);
+    if (cudaEventRecord(a, st) != cudaSuccess) ok = false;
+    return (int)tag.size() - 1;
+  }
+  void end(int i, cudaStream_t st, int t) {
+    if (i < 0) return;
+    tag[i] = t;
+    if (cudaEventRecord(ev[2 * i + 1], st) != cudaSuccess) ok = false;
+  }
+  // Adds the seconds of each tag to s[0] (copies) and s[1] (kernels); false if any event failed.
+  bool sum(double *s) {
+    if (!ok) return false;
+    for (size_t i = 0; i < tag.size(); ++i) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+      }
+      s[tag[i]] += 1e-3 * ms;
+    }
+    return true;
+  }
+  ~Intervals() {
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  }
+};
+
+// Publishes the copy and kernel seconds of a host call: to the thread's sfnl_last_host_timing record
+// and, when given, to the reference's temps(3) (zeroed on entry by the callers, then added to).
+void report_timing(Intervals &iv, double *temps) {
+  double s[2] = {0.0, 0.0};
+  if (!iv.sum(s)) s[0] = s[1] = 0.0;
+  g_host_timing[0] = s[0];
+  g_host_timing[1] = s[1];
+  g_host_timing[2] = 0.0;
+  if (temps) {
+    temps[0] += s[0];
+    temps[1] += s[1];
+  }
+}
+
 struct PipeState {
   cudaStream_t st[kPipe] = {nullptr, nullptr, nullptr, nullptr};
 };
@@ -304,7 +374,6 @@ PipeState g_pipe[kMaxDev];
 using ChunkRun = int (*)(std::vector<HostBuf> &, int64_t np_chunk, void *, cudaStream_t);
 
 int with_device_buffers(std::vector<HostBuf> &bufs, int64_t np, int m, ChunkRun run, void *ctx, double *temps) {
-  using clk = std::chrono::steady_clock;
   int d = 0;
   if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDev) return set_error(SFNL_ERR_CUDA, "no current CUDA device");
   DevState *s = &g_dev[d];
@@ -334,13 +403,14 @@ int with_device_buffers(std::vector<HostBuf> &bufs, int64_t np, int m, ChunkRun 
     }
     s->work_bytes = total;
   }
-  auto t0 = clk::now();
+  Intervals iv;
   int rc = SFNL_OK;
   for (int64_t c = 0; c < nchunks && rc == SFNL_OK; ++c) {
     const int slot = (int)(c % slots);
     cudaStream_t st = ps.st[slot];
     const int64_t p0 = c * cp, n = (p0 + cp <= np) ? cp : np - p0;
     size_t off = slot_bytes * slot;
+    int ic = iv.begin(st);
     for (auto &b : bufs) {
       b.dev = reinterpret_cast<double *>(s->work + off);
       off += (sizeof(double) * (size_t)b.ew * buf_rows(b, m) * cp + 255) & ~size_t(255);
@@ -349,7 +419,11 @@ int with_device_buffers(std::vector<HostBuf> &bufs, int64_t np, int m, ChunkRun 
                                      buf_rows(b, m), cudaMemcpyHostToDevice, st) != cudaSuccess)
         rc = set_error(SFNL_ERR_CUDA, "host-to-device copy failed");
     }
+    iv.end(ic, st, 0);
+    const int ik = iv.begin(st);
     if (rc == SFNL_OK) rc = run(bufs, n, ctx, st);
+    iv.end(ik, st, 1);
+    ic = iv.begin(st);
     for (auto &b : bufs) {
       const size_t w = sizeof(double) * b.ew;
       if (rc == SFNL_OK && b.dst &&
@@ -357,20 +431,16 @@ int with_device_buffers(std::vector<HostBuf> &bufs, int64_t np, int m, ChunkRun 
                             buf_rows(b, m), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         rc = set_error(SFNL_ERR_CUDA, "device-to-host copy failed");
     }
+    iv.end(ic, st, 0);
   }
   for (int i = 0; i < slots; ++i)
     if (cudaStreamSynchronize(ps.st[i]) != cudaSuccess && rc == SFNL_OK)
       rc = set_error(SFNL_ERR_CUDA, "host call failed on the device");
   if (rc != SFNL_OK) return rc;
-  const double wall = std::chrono::duration<double>(clk::now() - t0).count();
-  g_host_timing[0] = 0.0;   // copies overlap the kernels: the whole pipelined call is reported in [1]
-  g_host_timing[1] = wall;
-  g_host_timing[2] = 0.0;
-  if (temps) {
-    temps[0] = 0.0;
-    temps[1] = wall;
-    temps[2] = 0.0;
-  }
+  if (split_take_status()) return timeout_error();
+  // Sums over the chunks: a chunk's copies overlap other chunks' kernels on the other streams, so
+  // temps(1) + temps(2) may exceed the wall time of the call.
+  report_timing(iv, temps);
   return SFNL_OK;
 }
 
@@ -459,6 +529,7 @@ int sfnl_set_check_finite(int on) {
   g_check_finite = on ? 1 : 0;
   return SFNL_OK;
 }
+int sfnl_test_inject_timeout(void) { return split_inject_timeout(); }
 int sfnl_last_host_timing(double *s3) {
   if (!s3) return set_error(SFNL_ERR_ARG, "null pointer");
   for (int i = 0; i < 3; ++i) s3[i] = g_host_timing[i];
@@ -840,8 +911,6 @@ static int host_gauss(int kind, const double *V_in, const double *V2_in, int nsl
     return set_error(SFNL_ERR_ARG, "null array");
   for (int64_t t = 0; t < (int64_t)n_w * me; ++t)
     if (jj[t] < 1 || jj[t] > np_nodes) return set_error(SFNL_ERR_ARG, "jj holds a node number outside 1..np_nodes");
-  using clk = std::chrono::steady_clock;
-  const auto t0 = clk::now();
   const int64_t ng = (int64_t)l_G * me;
   const size_t nv = (size_t)np_nodes * 6 * nmod, nv2 = (size_t)np_nodes * nslot2 * nmod;
   const size_t nout = (size_t)ng * nslot_out * nmod, nwork = gauss_operand_doubles(kind, conservative, ng, nmod);
@@ -862,6 +931,8 @@ static int host_gauss(int kind, const double *V_in, const double *V2_in, int nsl
   double *d_ww = (double *)take(8 * nww), *d_dw = (double *)take(8 * ndw), *d_rr = (double *)take(8 * nrr);
   int *d_jj = (int *)take(4 * (size_t)n_w * me), *d_lm = (int *)take(4 * (size_t)nmod);
   cudaStream_t st = nullptr;
+  Intervals iv;
+  const int ic = iv.begin(st);
   bool ok = cudaMemcpyAsync(d_v, V_in, 8 * nv, cudaMemcpyHostToDevice, st) == cudaSuccess &&
             (!omega || cudaMemcpyAsync(d_om, omega, 8 * nv, cudaMemcpyHostToDevice, st) == cudaSuccess) &&
             (!nslot2 || cudaMemcpyAsync(d_v2, V2_in, 8 * nv2, cudaMemcpyHostToDevice, st) == cudaSuccess) &&
@@ -872,15 +943,18 @@ static int host_gauss(int kind, const double *V_in, const double *V2_in, int nsl
             cudaMemcpyAsync(d_jj, jj, 4 * (size_t)n_w * me, cudaMemcpyHostToDevice, st) == cudaSuccess &&
             cudaMemcpyAsync(d_lm, list_mode, 4 * (size_t)nmod, cudaMemcpyHostToDevice, st) == cudaSuccess;
   if (!ok) return set_error(SFNL_ERR_CUDA, "host-to-device copy failed");
+  iv.end(ic, st, 0);
+  const int ik = iv.begin(st);
   rc = gauss_product(kind, d_v, d_v2, d_om, d_heat, conservative, d_jj, d_ww, d_dw, d_rr, d_lm, d_out, np_nodes, me,
                      n_w, l_G, nmod, 0, d_work, reinterpret_cast<sfnl_stream_t>(st));
   if (rc) return rc;
-  if (cudaMemcpyAsync(V_out, d_out, 8 * nout, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-      cudaStreamSynchronize(st) != cudaSuccess)
+  iv.end(ik, st, 1);
+  const int io = iv.begin(st);
+  if (cudaMemcpyAsync(V_out, d_out, 8 * nout, cudaMemcpyDeviceToHost, st) != cudaSuccess)
     return set_error(SFNL_ERR_CUDA, "device-to-host copy failed");
-  g_host_timing[0] = 0.0;
-  g_host_timing[1] = std::chrono::duration<double>(clk::now() - t0).count();
-  g_host_timing[2] = 0.0;
+  iv.end(io, st, 0);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return set_error(SFNL_ERR_CUDA, "device-to-host copy failed");
+  report_timing(iv, nullptr);
   return SFNL_OK;
 }
 

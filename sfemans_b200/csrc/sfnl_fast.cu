@@ -1445,6 +1445,15 @@ void fast_release_tables() {
     g_tftabs.clear();
   }
   cudaSetDevice(prev);
+  {
+    // The no-allocation entry's cached array addresses and table state belong to the current
+    // contexts; after a device reset they would be stale, so the next call sets them up again.
+    std::lock_guard<std::mutex> lk3(g_na_mu);
+    for (int d = 0; d < 64; ++d) {
+      g_na_ptr[d] = nullptr;
+      g_na_m[d] = 0;
+    }
+  }
 }
 
 }  // namespace sfnl

@@ -64,7 +64,12 @@ namespace {
 constexpr int kW = 8;            // bits of the first slice (integers up to 2^8)
 constexpr int kKeMax = 32;       // modes per class held in registers (m <= 64)
 
-__device__ int g_split_status;   // 0 ok; 1 an mbarrier wait timed out
+// Status word of the split kernels: a pinned host word mapped into the device address space, set to 1
+// by a CTA whose bounded wait on its tensor-core operations gave up.  The host reads it without a copy
+// or a synchronisation (split_take_status); it is shared by every device and stream of the process.
+std::mutex g_status_mu;
+int *g_status_host = nullptr;  // pinned, mapped
+int *g_status_dev = nullptr;   // its device address
 
 // ---------------------------------------------------------------------------
 // geometry
@@ -302,6 +307,14 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
   return false;
 }
 
+// Marks the call as failed in the mapped status word (visible to the host without a copy).
+__device__ __forceinline__ void report_timeout(int *status) {
+  if (status) {
+    *reinterpret_cast<volatile int *>(status) = 1;
+    __threadfence_system();
+  }
+}
+
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
   uint32_t r[8];
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
@@ -419,6 +432,7 @@ struct SplitArgs {
   SGeo g;
   const void *bsyn, *bana;
   int bsyn_bytes, bana_bytes;
+  int *status;  // the mapped status word
 };
 
 constexpr int kThreads = 256;
@@ -666,11 +680,14 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
       umma_commit(mbar);
     }
     __syncwarp();
-    if (!mbar_wait(mbar, phase)) {
+    // Every thread waits (bounded) and the CTA agrees on the outcome before any barrier or loop
+    // condition depends on it; on a timeout the phase stays, so the final drain waits for it again.
+    if (!__syncthreads_and(mbar_wait(mbar, phase))) {
       ok = false;
-      g_split_status = 1;
+      if (t == 0) report_timeout(a.status);
+    } else {
+      phase ^= 1;
     }
-    phase ^= 1;
     tc_fence_after();
 
     for (int ch = 0; ch < NC && ok; ++ch) {
@@ -704,9 +721,10 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
       __syncthreads();
       // The previous chunk's analysis must be complete before its A operand is rewritten.
       if (ch > 0) {
-        if (!mbar_wait(mbar, phase)) {
+        if (!__syncthreads_and(mbar_wait(mbar, phase))) {
           ok = false;
-          g_split_status = 1;
+          if (t == 0) report_timeout(a.status);
+          break;
         }
         phase ^= 1;
         tc_fence_after();
@@ -743,11 +761,12 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
     }
     // ---- 4. the last chunk into the outputs ----
     if (ok) {
-      if (!mbar_wait(mbar, phase)) {
+      if (!__syncthreads_and(mbar_wait(mbar, phase))) {
         ok = false;
-        g_split_status = 1;
+        if (t == 0) report_timeout(a.status);
+      } else {
+        phase ^= 1;
       }
-      phase ^= 1;
     }
     tc_fence_after();
     if (ok) flush_chunk(tile, NC - 1);
@@ -755,6 +774,14 @@ __global__ void __launch_bounds__(kThreads, 1) split_kernel(const SplitArgs a) {
     __syncthreads();
   }
   __syncthreads();
+  // After a timeout the last commit's phase is still pending: wait for it once more (bounded) so that
+  // no tensor-core operation still writes the columns being freed; the status word already reports
+  // the call as failed either way.
+  if (!ok) {
+    const bool drained = mbar_wait(mbar, phase);
+    __syncthreads();
+    (void)drained;
+  }
   if (warp == 0) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(g.tmem_alloc));
@@ -807,11 +834,36 @@ int upload_terms() {
   return SFNL_OK;
 }
 
+// The mapped status word, allocated on first use (pinned host memory, portable to every device).
+int status_word(int **dev) {
+  std::lock_guard<std::mutex> lk(g_status_mu);
+  if (!g_status_host) {
+    int *h = nullptr;
+    if (cudaHostAlloc(reinterpret_cast<void **>(&h), sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      return set_error(SFNL_ERR_ALLOC, "pinned allocation of the split-form status word failed");
+    }
+    *h = 0;
+    int *d = nullptr;
+    if (cudaHostGetDevicePointer(reinterpret_cast<void **>(&d), h, 0) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFreeHost(h);
+      return set_error(SFNL_ERR_CUDA, "the split-form status word cannot be mapped");
+    }
+    g_status_host = h;
+    g_status_dev = d;
+  }
+  *dev = g_status_dev;
+  return SFNL_OK;
+}
+
 template <int PR>
 int run_split_program(const ProgArgs &pa, int split, const int *in_map, const int *out_map, cudaStream_t st) {
   if (int rc = upload_terms()) return rc;
   SplitArgs sa;
   std::memset(&sa, 0, sizeof(sa));
+  if (int rc = status_word(&sa.status)) return rc;
   if (!make_sgeo(pa.m, pr_pts(PR), pr_nin(PR), &sa.g)) return set_error(SFNL_ERR_UNSUPPORTED, "split form: m too large");
   STables T;
   int rc = get_stables(sa.g, &T);
@@ -871,11 +923,18 @@ int launch_split(const ProgArgs &a, int split, cudaStream_t st) {
   return set_error(SFNL_ERR_ARG, "unknown program");
 }
 
-int split_status_and_clear() {
-  int h = 0, z = 0;
-  if (cudaMemcpyFromSymbol(&h, g_split_status, sizeof(int)) != cudaSuccess) return -1;
-  cudaMemcpyToSymbol(g_split_status, &z, sizeof(int));
-  return h;
+int split_take_status() {
+  std::lock_guard<std::mutex> lk(g_status_mu);
+  if (!g_status_host) return 0;
+  return __atomic_exchange_n(reinterpret_cast<volatile int *>(g_status_host), 0, __ATOMIC_SEQ_CST);
+}
+
+int split_inject_timeout() {
+  int *d = nullptr;
+  if (int rc = status_word(&d)) return rc;
+  std::lock_guard<std::mutex> lk(g_status_mu);
+  __atomic_store_n(reinterpret_cast<volatile int *>(g_status_host), 1, __ATOMIC_SEQ_CST);
+  return SFNL_OK;
 }
 
 void split_release_tables() {

@@ -43,12 +43,26 @@ def fft_par_distributed(kind, group, x, y, out, nb_procs, bloc_size, m_max_pad, 
     m_max_c) for the tensor kinds.  ``compute(kind, xb, yb, m_max_pad)`` maps the gathered
     (bloc_size, nslot, m_max) blocks to the block's output; it defaults to the CUDA kernels.
     """
+    import time
+
     import torch
     import torch.distributed as dist
 
     world = dist.get_world_size(group)
     if world != nb_procs:
         raise ValueError("nb_procs must equal the communicator size")
+    if temps is not None:  # zeroed, then accumulated per stage as the reference does (:179, :203-290)
+        temps[:] = 0.0
+    sync = torch.cuda.synchronize if (temps is not None and x.is_cuda) else (lambda: None)
+    clock = [time.perf_counter()]
+
+    def lap(i):  # adds the time since the last lap to temps[i]: 0 exchange, 1 product, 2 repacking
+        if temps is not None:
+            sync()
+            t = time.perf_counter()
+            temps[i] += t - clock[0]
+            clock[0] = t
+
     npts, nsl, mc = x.shape
     nsl2 = y.shape[1]
     np_tot = nb_procs * bloc_size
@@ -65,27 +79,32 @@ def fft_par_distributed(kind, group, x, y, out, nb_procs, bloc_size, m_max_pad, 
 
     send = torch.cat([to_blocks(x, nsl), to_blocks(y, nsl2)], dim=2)         # (P, mc, ns1+ns2, bloc)
     recv = torch.empty_like(send)
+    lap(2)
     dist.all_to_all_single(recv.view(-1), send.view(-1), group=group)       # fft_parallel.F90:217
+    lap(0)
     # recv[r] = source rank r's modes for my points -> (bloc, ns, m_max) Fortran layout with
     # global mode r*mc + i (the shiftl bookkeeping of :223-231).
     full = recv.permute(3, 2, 0, 1).reshape(bloc_size, nsl + nsl2, nb_procs * mc)
     xb = full[:, :nsl, :].contiguous().permute(2, 1, 0).contiguous().permute(2, 1, 0)
     yb = full[:, nsl:, :].contiguous().permute(2, 1, 0).contiguous().permute(2, 1, 0)
+    lap(2)
     pb = compute(kind, xb, yb, m_max_pad)                                     # (bloc, nout, m_max)
+    lap(1)
     if tensor_out:  # (3, bloc, 6, m_max) -> (bloc, 18, m_max), slot 3*s + k
         pb = pb.permute(1, 2, 0, 3).reshape(bloc_size, 18, nb_procs * mc)
     nout = pb.shape[1]
     # send back modes [q*mc, (q+1)*mc) of my points to rank q (:306)
     back = pb.reshape(bloc_size, nout, nb_procs, mc).permute(2, 3, 1, 0).contiguous()  # (P, mc, nout, bloc)
     got = torch.empty_like(back)
+    lap(2)
     dist.all_to_all_single(got.view(-1), back.view(-1), group=group)
+    lap(0)
     # got[q] = my modes for rank q's points -> (np_tot, nout, mc), drop dummies (:311-324)
     res = got.permute(0, 3, 2, 1).reshape(np_tot, nout, mc)[:npts]
     if tensor_out:
         res = res.reshape(npts, 6, 3, mc).permute(2, 0, 1, 3)
     out.copy_(res)
-    if temps is not None:
-        temps[:] = 0.0
+    lap(2)
     return out
 
 
@@ -187,5 +206,5 @@ def smb_gauss_distributed(kind, group, mesh, list_mode, V_in, nb_procs, V2_in=No
         return fft_par_distributed("cross", group, ops[0], ops[1], empty(6), nb_procs, bloc, pad, temps, compute)
     out = fft_par_distributed("dot", group, ops[0], ops[1], empty(2), nb_procs, bloc, pad, temps, compute)
     if conservative:  # + FFT_PAR_PROD_DCL(Div, Cgauss) (subroutine_temperature_with_T.F90:339-342)
-        out += fft_par_distributed("prod", group, ops[2], ops[3], empty(2), nb_procs, bloc, pad, None, compute)
+        out += fft_par_distributed("prod", group, ops[2], ops[3], empty(2), nb_procs, bloc, pad, temps, compute)
     return out

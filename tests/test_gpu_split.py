@@ -59,7 +59,9 @@ def test_split_bundle_m64():
         assert R.rel_l2(host(o), r) <= SPLIT_TOL
 
 
-def test_split_mhd_linearised_against_fp64():
+def test_split_mhd_linearised_against_the_oracle():
+    # linearised u x w and u x b about (u, w, b): the JVP against the oracle's cross products
+    # (du x w + u x dw, du x b + u x db), the VJP against the oracle's transposes of both
     npts, m, k, pad = 400, 32, 3, 48
     u, w, b = (R.synthetic_field(npts, 6, m, 0.2, 900 + i) for i in range(3))
     v = np.empty((npts, 18, m, k), order="F")
@@ -68,13 +70,16 @@ def test_split_mhd_linearised_against_fp64():
         v[..., t] = R.synthetic_field(npts, 18, m, 0.2, 910 + t)
         c[..., t] = R.synthetic_field(npts, 12, m, 0.2, 920 + t)
     U, W, B = dev(u), dev(w), dev(b)
-    jv64 = host(sf.mhd_jvp(U, W, B, dev(v), m_max_pad=pad))
     jvs = host(sf.mhd_jvp(U, W, B, dev(v), m_max_pad=pad, split=sf.SPLIT_BF16X3))
-    jt64 = host(sf.mhd_vjp(U, W, B, dev(c), m_max_pad=pad))
     jts = host(sf.mhd_vjp(U, W, B, dev(c), m_max_pad=pad, split=sf.SPLIT_BF16X3))
     for t in range(k):
-        assert R.rel_l2(jvs[..., t], jv64[..., t]) <= SPLIT_TOL
-        assert R.rel_l2(jts[..., t], jt64[..., t]) <= SPLIT_TOL
+        du, dw, db = v[:, 0:6, :, t], v[:, 6:12, :, t], v[:, 12:18, :, t]
+        jv = np.concatenate([R.cross_jvp(u, w, du, dw, pad), R.cross_jvp(u, b, du, db, pad)], axis=1)
+        g1 = R.cross_vjp(u, w, np.asfortranarray(c[:, 0:6, :, t]))
+        g2 = R.cross_vjp(u, b, np.asfortranarray(c[:, 6:12, :, t]))
+        jt = np.concatenate([g1[:, :6] + g2[:, :6], g1[:, 6:], g2[:, 6:]], axis=1)
+        assert R.rel_l2(jvs[..., t], jv) <= SPLIT_TOL
+        assert R.rel_l2(jts[..., t], jt) <= SPLIT_TOL
 
 
 def test_split_refuses_aliasing_pad_and_large_m():
@@ -86,3 +91,26 @@ def test_split_refuses_aliasing_pad_and_large_m():
     with pytest.raises(sf.SfnlError) as e:
         sf.product(0, W, W, m_max_pad=120, split=sf.SPLIT_BF16X3)
     assert e.value.code == -4
+
+
+def test_split_timeout_status_is_reported_once_and_cleared():
+    # Host-side injection: the status word is marked as a split kernel marks it when a bounded wait on
+    # its tensor-core operations gives up; no device wait is made to run out.
+    L = sf.lib()
+    npts, m, pad = 200, 16, 24
+    V1 = R.synthetic_field(npts, 6, m, 0.3, 901)
+    V2 = R.synthetic_field(npts, 6, m, 0.3, 902)
+    ref = R.c_oracle("cross", V1, V2, pad)
+    assert L.sfnl_test_inject_timeout() == 0
+    with pytest.raises(sf.SfnlError) as e:
+        sf.product(0, dev(V1), dev(V2), m_max_pad=pad, split=sf.SPLIT_BF16X3)
+    assert e.value.code == -8 and "tensor-core" in str(e.value)
+    out = host(sf.product(0, dev(V1), dev(V2), m_max_pad=pad, split=sf.SPLIT_BF16X3))  # cleared
+    assert R.rel_l2(out, ref) <= SPLIT_TOL
+    # the FP64 forms do not use the word: an injected status waits for the next split call
+    assert L.sfnl_test_inject_timeout() == 0
+    fp = host(sf.product(0, dev(V1), dev(V2), m_max_pad=pad))
+    assert R.rel_l2(fp, ref) <= 1e-12
+    with pytest.raises(sf.SfnlError) as e:
+        sf.product(0, dev(V1), dev(V2), m_max_pad=pad, split=sf.SPLIT_BF16X2)
+    assert e.value.code == -8

@@ -349,3 +349,21 @@ def test_advection_caller_known_answers():
     np.testing.assert_allclose(out[:, 0, 2], 0.5, atol=1e-12)
     np.testing.assert_allclose(out[:, 0, 1], 0.0, atol=1e-12)
     assert out.shape == (ng, 2, 3)
+
+
+@pytest.mark.parametrize("npts,m,pad,n_theta", [(37, 16, 24, None), (37, 16, 24, 48), (50, 64, 96, 192),
+                                                  (21, 5, 7, None), (9, 1, 1, None), (17, 40, 60, 130)])
+def test_cpu_baseline_port_matches_the_oracle(npts, m, pad, n_theta):
+    # the O(N log N) C restatement timed as the CPU baseline: odd (reference) and even grids, partial
+    # point blocks, every product and the bundle
+    V1 = R.synthetic_field(npts, 6, m, 0.2, 11)
+    V2 = R.synthetic_field(npts, 6, m, 0.2, 12)
+    for op in ("cross", "dot"):
+        ref = R.c_oracle(op, V1, V2, pad, n_theta=n_theta)
+        assert R.rel_l2(R.cpu_product(op, V1, V2, pad, n_theta=n_theta, threads=3), ref) <= 1e-14
+    S1, S2 = V1[:, :2].copy(order="F"), V2[:, :2].copy(order="F")
+    ref = R.c_oracle("prod", S1, S2, pad, n_theta=n_theta)
+    assert R.rel_l2(R.cpu_product("prod", S1, S2, pad, n_theta=n_theta), ref) <= 1e-14
+    f = [R.synthetic_field(npts, 6, m, 0.1, 20 + i) for i in range(5)]
+    for o, r in zip(R.cpu_mhd_bundle(*f, pad, n_theta=n_theta, threads=2), R.mhd_bundle(*f, pad)):
+        assert R.rel_l2(o, r) <= 1e-14

@@ -58,9 +58,13 @@ def _worker(rank, world, port, kind, npts, m, pad, bloc, q):
             out = torch.zeros((mc, 6, npts, 3), dtype=torch.float64).permute(3, 2, 1, 0)
         else:
             out = torch.zeros((mc, nout, npts), dtype=torch.float64).permute(2, 1, 0)
-        fft_par_distributed(kind, None, loc(V1), loc(V2), out, world, bloc, pad, compute=_oracle_compute)
+        temps = np.full(3, 7.0)  # the reference zeroes temps on entry, then adds each stage's seconds
+        fft_par_distributed(kind, None, loc(V1), loc(V2), out, world, bloc, pad, temps=temps, compute=_oracle_compute)
         ref = R.c_oracle(kind, V1, V2, pad)[..., rank * mc:(rank + 1) * mc]
-        q.put((rank, float(np.abs(out.numpy() - ref).max())))
+        err = float(np.abs(out.numpy() - ref).max())
+        if not (np.all(temps >= 0.0) and np.all(temps < 7.0) and temps[1] > 0.0):
+            err = float("inf")  # temps not zeroed on entry, or the product's seconds missing
+        q.put((rank, err))
     finally:
         dist.destroy_process_group()
 
