@@ -22,6 +22,17 @@ The line reports ``--form`` (default fp64: the FAST all-FP64 form, the
 library's default path); every other form is also timed on a few steps and
 listed under "forms".  ``--form auto`` reports the fastest form that meets
 its accuracy bar instead.
+
+The other configurations of the benchmark are measured in the same run and
+reported under "configs" (``--no-configs`` skips them): the 28k-point cross
+product at m_max = 16 (eight rotated buffer sets, 430 MB, so that every step
+reads from HBM rather than L2), the 700k-point linearised cross product at
+m_max = 32 (JVP and VJP), and the 16-tangent linearised MHD product (u x w,
+u x b) at 350k points, m_max = 256, in point chunks that fit the device.
+
+CPU baseline: the O(N log N) C restatement of the reference's FFTW path
+(oracle/sfnl_cpu_fft.c) on all host threads, over a bounded sample of the
+same workload; its outputs are also the checker of the GPU results.
 """
 from __future__ import annotations
 
@@ -141,26 +152,30 @@ def synthetic_device(npts, nslot, m, alpha, seed, device):
     return t.permute(2, 1, 0)
 
 
+def _cpu_sample(workload, npts):
+    """Points of the bounded CPU sample of a workload (about 10-30 s of CPU work over the run)."""
+    return min(npts, {"mhd_bundle": 100_000, "cross_28k": 28_000}.get(workload, 100_000))
+
+
 def run_reference(args, world, rank):
-    """CPU baseline: the oracle's pocketfft port of the reference path on host cores."""
+    """The reference's CPU path: the C restatement of fft_parallel.F90 (pack, c2r, product, r2c, scale,
+    truncate) with O(N log N) real FFTs, all host threads, on a bounded sample of the workload."""
     if rank != 0:
         return
-    import numpy as np
-
     from oracle import ref_fft as R
 
     wl = WORKLOADS[args.workload]
     m, pad, alpha = wl["m"], wl["pad"], wl["alpha"]
-    sample = args.cpu_sample or (2000 if args.workload == "mhd_bundle" else 28_000)
-    cores = os.cpu_count() or 1
+    N = 2 * pad  # the configuration's grid (N_theta = 2 m_max_pad)
+    sample = args.cpu_sample or _cpu_sample(args.workload, wl["np"])
+    cores = R.cpu_threads()
     if args.workload == "mhd_bundle":
         f = [R.synthetic_field(sample, 6, m, alpha, 1000 + i) for i in range(5)]
-        eng = lambda op, x, y: R.fft_par(op, x, y, pad, workers=cores)  # noqa: E731
-        step = lambda: R.mhd_bundle(*f, pad, engine=eng)  # noqa: E731
+        step = lambda: R.cpu_mhd_bundle(*f, pad, n_theta=N, threads=cores)  # noqa: E731
     else:
         V1 = R.synthetic_field(sample, 6, m, alpha, 1001)
         V2 = R.synthetic_field(sample, 6, m, alpha, 1002)
-        step = lambda: R.fft_par("cross", V1, V2, pad, workers=cores)  # noqa: E731
+        step = lambda: R.cpu_product("cross", V1, V2, pad, n_theta=N, threads=cores)  # noqa: E731
     for _ in range(args.warmup):
         step()
     t0 = time.perf_counter()
@@ -172,11 +187,12 @@ def run_reference(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "np": wl["np"], "m_max": m, "m_max_pad": pad, "alpha": alpha,
-                   "sample_points_per_step": sample, "desc": wl["desc"]},
+        "config": {"workload": args.workload, "np": wl["np"], "m_max": m, "m_max_pad": pad, "n_theta": N,
+                   "alpha": alpha, "sample_points_per_step": sample, "desc": wl["desc"]},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{sample} of {wl['np']} points per step, all {m} modes; pocketfft (scipy.fft, "
-                                   f"{cores} workers) restatement of fft_parallel.F90, no MPI_ALLTOALL cost"},
+                         "sample": f"{sample} of {wl['np']} points per step, all {m} modes, N = {N}; C restatement of "
+                                   f"fft_parallel.F90 with O(N log N) real FFTs (oracle/sfnl_cpu_fft.c), {cores} host "
+                                   "threads standing for the Fourier ranks, no MPI_ALLTOALL cost"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -193,6 +209,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-sample", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other configurations")
     args = ap.parse_args()
     world, rank, local = _dist_env()
     if args.impl == "reference":
@@ -295,6 +312,12 @@ def main():
     if args.workload == "mhd_bundle" and args.e2e_steps > 0:
         e2e = _e2e_bundle(sf, torch, ins, npts, m, pad, best, args.e2e_steps, world, dist)
 
+    configs = None
+    if args.workload == "mhd_bundle" and not args.no_configs:
+        del ins, outs
+        torch.cuda.empty_cache()
+        configs = _extra_configs(args, sf, torch, dev, world, rank, dist, local, stream)
+
     if args.workload == "mhd_bundle":
         kname = {"fp64": "fast_bundle_tf_kernel<64>" if m == 64 else "fast_kernel<EK_CROSS>",
                  "split3": "split_kernel<PR_BUNDLE>", "split2": "split_kernel<PR_BUNDLE>", "grid": "grid_kernel<OP_BUNDLE>"}[best]
@@ -330,6 +353,7 @@ def main():
         "gpu_launches": results[best]["steps"] * launches[best],
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "configs": configs,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -347,7 +371,7 @@ def R_rel_l2(x, ref):
     return float(np.linalg.norm(x - ref) / (den if den > 0 else 1.0))
 
 
-def _time_steps(step, steps, warmup, stream, world, dist, local):
+def _time_steps(step, steps, warmup, stream, world, dist, local, clocks=True):
     """CUDA-event timing of `steps` calls after `warmup` (>= 3), barrier + sync on both sides, max over ranks."""
     import torch
 
@@ -356,9 +380,10 @@ def _time_steps(step, steps, warmup, stream, world, dist, local):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
-    clocks.wait_first()  # nvidia-smi takes a few hundred ms to start: sample the whole timed region
+    sampler = ClockSampler(local) if clocks else None
+    if sampler:
+        sampler.start()
+        sampler.wait_first()  # nvidia-smi takes a few hundred ms to start: sample the whole timed region
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
     ev[0].record(stream)
     for i in range(steps):
@@ -367,7 +392,7 @@ def _time_steps(step, steps, warmup, stream, world, dist, local):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clk = clocks.stop()
+    clk = sampler.stop() if sampler else None
     ms = sum(ev[i].elapsed_time(ev[i + 1]) for i in range(steps)) / steps
     if world > 1:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
@@ -425,21 +450,20 @@ def _e2e_bundle(sf, torch, ins, npts, m, pad, form, steps, world, dist):
 
 
 def _cpu_baseline(args, ins, npts, m, pad):
-    """Oracle port timed on the host cores over a bounded sample; its output is also the checker of this run."""
+    """The C restatement timed on the host threads over a bounded sample; its output is also the checker."""
     import numpy as np
 
     import sfemans_b200 as sf
     from oracle import ref_fft as R
 
-    sample = args.cpu_sample or (2000 if args.workload == "mhd_bundle" else 28_000)
-    sample = min(sample, npts)
-    cores = os.cpu_count() or 1
+    sample = min(args.cpu_sample or _cpu_sample(args.workload, npts), npts)
+    cores = R.cpu_threads()
+    N = 2 * pad
     h = [np.asfortranarray(sf.to_host(x[:sample])) for x in ins]
-    eng = lambda op, x, y: R.fft_par(op, x, y, pad, workers=cores)  # noqa: E731
     if args.workload == "mhd_bundle":
-        run = lambda: R.mhd_bundle(*h, pad, engine=eng)  # noqa: E731
+        run = lambda: R.cpu_mhd_bundle(*h, pad, n_theta=N, threads=cores)  # noqa: E731
     else:
-        run = lambda: (R.fft_par("cross", h[0], h[1], pad, workers=cores),)  # noqa: E731
+        run = lambda: (R.cpu_product("cross", h[0], h[1], pad, n_theta=N, threads=cores),)  # noqa: E731
     run()
     reps, t0 = 0, time.perf_counter()
     while True:
@@ -449,9 +473,180 @@ def _cpu_baseline(args, ins, npts, m, pad):
             break
     dt = (time.perf_counter() - t0) / reps
     cpu = {"value": sample * m / dt, "unit": UNIT, "cores": cores, "kind": "port",
-           "sample": f"{sample} of {npts} points x {m} modes, {reps} reps; pocketfft (scipy.fft) restatement of "
-                     "fft_parallel.F90 with all modes on one process (no MPI_ALLTOALL)"}
+           "sample": f"{sample} of {npts} points x {m} modes, N = {N}, {reps} reps; C restatement of fft_parallel.F90 "
+                     f"with O(N log N) real FFTs on {cores} host threads, all modes on one process (no MPI_ALLTOALL)"}
     return cpu, ref, sample
+
+
+def _extra_configs(args, sf, torch, dev, world, rank, dist, local, stream):
+    """The benchmark's other configurations on this device (weak scaling under torchrun): value in the same
+    unit (Gauss-pt*modes/s, whole job), HBM roofline of the step, CPU baseline and parity on a sample."""
+    import numpy as np
+
+    from oracle import ref_fft as R
+
+    hbm, _, peak_kind = _peaks()
+    cpu_on = rank == 0 and world == 1 and not args.no_cpu
+    cores = R.cpu_threads()
+    H = sf.to_host
+
+    def roof(nbytes, ms, kernel):
+        ach = nbytes / (ms / 1e3) / 1e9
+        return {"bound": "hbm", "kernel": kernel, "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "peak_source": peak_kind, "algorithmic_bytes_per_step": nbytes, "avg_step_ms": ms}
+
+    def time_cpu(fn, budget=5.0):
+        out = fn()
+        reps, t0 = 0, time.perf_counter()
+        while reps < 20 and (reps == 0 or time.perf_counter() - t0 < budget):
+            out = fn()
+            reps += 1
+        return (time.perf_counter() - t0) / reps, out, reps
+
+    def tstep(fn, steps):
+        return _time_steps(fn, steps, args.warmup, stream, world, dist, local, clocks=False)[0]
+
+    res = {}
+    # ---- 28k-point cross product, m_max = 16 (eight rotated buffer sets) ----
+    npts, m, pad, alpha, nsets = 28_000, 16, 24, 0.3, 8
+    sets = [(synthetic_device(npts, 6, m, alpha, 2000 + 2 * q + 97 * rank, dev),
+             synthetic_device(npts, 6, m, alpha, 2001 + 2 * q + 97 * rank, dev),
+             sf.fortran_empty(npts, 6, m, device=dev)) for q in range(nsets)]
+    nbytes = 8.0 * m * 18 * npts
+    cfg = {"desc": "cross product u x w; 28k Gauss pts (4000 P2 triangles x 7), m_max=16 padded to 24, N_theta=48",
+           "np": npts, "m_max": m, "m_max_pad": pad, "alpha": alpha,
+           "l2": f"{nsets} rotated buffer sets ({nsets * 18 * npts * m * 8 / 1e6:.0f} MB, over the 126 MB L2), "
+                 "the next set every step", "forms": {}}
+    ref = None
+    if cpu_on:
+        a0, b0 = H(sets[0][0]), H(sets[0][1])
+        dt, ref, reps = time_cpu(lambda: R.cpu_product("cross", a0, b0, pad, n_theta=2 * pad, threads=cores))
+        cfg["cpu_baseline"] = {"value": npts * m / dt, "unit": UNIT, "cores": cores, "kind": "port",
+                               "sample": f"all {npts} points, {reps} reps; C restatement (oracle/sfnl_cpu_fft.c)"}
+    for form, kw in (("fp64", dict(algo=sf.ALGO_FAST)), ("split3", dict(split=sf.SPLIT_BF16X3)),
+                     ("grid", dict(algo=sf.ALGO_GRID))):
+        it = [0]
+
+        def step(kw=kw):
+            a, b, o = sets[it[0] % nsets]
+            it[0] += 1
+            sf.product(sf.OP_CROSS, a, b, out=o, m_max_pad=pad, **kw)
+
+        ms = tstep(step, 8 * nsets)
+        r = {"ms_per_step": ms, "value": world * npts * m / (ms / 1e3), "gpu_launches_per_step": 1}
+        if ref is not None:
+            o = sf.product(sf.OP_CROSS, sets[0][0], sets[0][1], m_max_pad=pad, **kw)
+            r["rel_l2_vs_cpu_port"] = R_rel_l2(H(o), ref)
+        cfg["forms"][form] = r
+    cfg["roofline"] = roof(nbytes, cfg["forms"]["fp64"]["ms_per_step"], "fast_kernel<EK_CROSS, 16>")
+    res["cross_28k"] = cfg
+    del sets
+
+    # ---- 700k-point linearised cross product u x w, m_max = 32: JVP and VJP (FP64) ----
+    npts, m, pad, alpha = 700_000, 32, 48, 0.2
+    u = synthetic_device(npts, 6, m, alpha, 3000 + 97 * rank, dev)
+    w = synthetic_device(npts, 6, m, alpha, 3001 + 97 * rank, dev)
+    tan = synthetic_device(npts, 12, m, alpha, 3002 + 97 * rank, dev)
+    cot = synthetic_device(npts, 6, m, alpha, 3003 + 97 * rank, dev)
+    jv, jt = sf.fortran_empty(npts, 6, m, device=dev), sf.fortran_empty(npts, 12, m, device=dev)
+    nbytes = 8.0 * m * 30 * npts  # JVP: u, w, (du, dw) in, 6 out; VJP: u, w, c in, 12 out
+    cfg = {"desc": "JVP and VJP of N(u, w) = u x w about a random base state; 700k Gauss pts, m_max=32 padded to 48",
+           "np": npts, "m_max": m, "m_max_pad": pad, "alpha": alpha, "l2": "inputs larger than L2"}
+    ms_j = tstep(lambda: sf.cross_jvp(u, w, tan, m_max_pad=pad, out=jv), 10)
+    ms_t = tstep(lambda: sf.cross_vjp(u, w, cot, m_max_pad=pad, out=jt), 10)
+    cfg["jvp"] = {"ms_per_step": ms_j, "value": world * npts * m / (ms_j / 1e3)}
+    cfg["vjp"] = {"ms_per_step": ms_t, "value": world * npts * m / (ms_t / 1e3)}
+    cfg["roofline"] = {"jvp": roof(nbytes, ms_j, "fast_kernel (JVP as two accumulating cross products)"),
+                       "vjp": roof(nbytes, ms_t, "fast_kernel (VJP as two cross products)")}
+    sf.cross_jvp(u, w, tan, m_max_pad=pad, out=jv)
+    sf.cross_vjp(u, w, cot, m_max_pad=pad, out=jt)
+    # full-size checks: central differences of the cross product (h = 1e-6) and <J v, c> = <v, J^T c>
+    hstep = 1e-6
+    du, dw = tan[:, 0:6, :], tan[:, 6:12, :]
+
+    def fortran(t):  # a Fortran-layout copy of an expression
+        o = sf.fortran_empty(*t.shape, device=dev)
+        o.copy_(t)
+        return o
+
+    plus = sf.product(sf.OP_CROSS, fortran(u + hstep * du), fortran(w + hstep * dw), m_max_pad=pad, algo=sf.ALGO_FAST)
+    minus = sf.product(sf.OP_CROSS, fortran(u - hstep * du), fortran(w - hstep * dw), m_max_pad=pad,
+                       algo=sf.ALGO_FAST)
+    fd = (plus - minus) / (2 * hstep)
+    cfg["fd_rel_l2"] = float(torch.linalg.vector_norm(fd - jv) / torch.linalg.vector_norm(jv))
+    lhs, rhs = float(torch.sum(jv * cot)), float(torch.sum(tan * jt))
+    cfg["dot_product_rel"] = abs(lhs - rhs) / abs(lhs)
+    del plus, minus, fd
+    if cpu_on:
+        n_s = 20_000
+        hu, hw, hdu, hdw = (np.asfortranarray(H(x[:n_s])) for x in (u, w, du, dw))
+        cpu_jvp = lambda: (R.cpu_product("cross", hdu, hw, pad, n_theta=2 * pad, threads=cores)  # noqa: E731
+                           + R.cpu_product("cross", hu, hdw, pad, n_theta=2 * pad, threads=cores))
+        dt, ref_j, reps = time_cpu(cpu_jvp)
+        cfg["cpu_baseline"] = {"value": n_s * m / dt, "unit": UNIT, "cores": cores, "kind": "port",
+                               "sample": f"JVP on {n_s} of {npts} points, {reps} reps; two cross products of the C "
+                                         "restatement (oracle/sfnl_cpu_fft.c)"}
+        cfg["jvp"]["rel_l2_vs_cpu_port"] = R_rel_l2(H(jv[:n_s]), ref_j)
+        n_v = 2000
+        ref_t = R.cross_vjp(H(u[:n_v]), H(w[:n_v]), np.asfortranarray(H(cot[:n_v])))
+        cfg["vjp"]["rel_l2_vs_oracle"] = R_rel_l2(H(jt[:n_v]), ref_t)
+    res["jvp_700k"] = cfg
+    del u, w, tan, cot, jv, jt
+    torch.cuda.empty_cache()
+
+    # ---- 16-tangent linearised MHD product (u x w, u x b) at m_max = 256: 350k points in chunks ----
+    npts, m, pad, alpha, k, chunk = 350_000, 256, 384, 0.2, 16, 35_000
+    nch = (npts + chunk - 1) // chunk
+    U, W, B = (synthetic_device(chunk, 6, m, alpha, 4000 + i + 97 * rank, dev) for i in range(3))
+    tan = torch.empty((k, m, 18, chunk), dtype=torch.float64, device=dev).permute(3, 2, 1, 0)
+    cot = torch.empty((k, m, 12, chunk), dtype=torch.float64, device=dev).permute(3, 2, 1, 0)
+    for t in range(k):
+        tan[..., t] = synthetic_device(chunk, 18, m, alpha, 4100 + t + 97 * rank, dev)
+        cot[..., t] = synthetic_device(chunk, 12, m, alpha, 4200 + t + 97 * rank, dev)
+    jv = sf.fortran_empty(chunk, 12, m, k, device=dev)
+    jt = sf.fortran_empty(chunk, 18, m, k, device=dev)
+    cfg = {"desc": "16 tangents per call of the linearised u x w and u x b (JVP) and its transpose (VJP); 350k Gauss "
+                   "pts, m_max=256 padded to 384, in 10 chunks of 35k points (the step's 357 GB exceed HBM)",
+           "np": npts, "m_max": m, "m_max_pad": pad, "k_batch": k, "alpha": alpha, "chunk_points": chunk,
+           "l2": "inputs larger than L2"}
+    steps5 = 2
+    ms_j = tstep(lambda: [sf.mhd_jvp(U, W, B, tan, m_max_pad=pad, out=jv) for _ in range(nch)], steps5)
+    ms_t = tstep(lambda: [sf.mhd_vjp(U, W, B, cot, m_max_pad=pad, out=jt) for _ in range(nch)], steps5)
+    cfg["jvp"] = {"ms_per_step": ms_j, "value": world * npts * m / (ms_j / 1e3), "steps": steps5}
+    cfg["vjp"] = {"ms_per_step": ms_t, "value": world * npts * m / (ms_t / 1e3), "steps": steps5}
+    try:
+        ms_s = tstep(lambda: [sf.mhd_jvp(U, W, B, tan, m_max_pad=pad, out=jv, split=sf.SPLIT_BF16X3)
+                              for _ in range(nch)], steps5)
+        cfg["split3"] = {"ms_per_step": ms_s, "value": world * npts * m / (ms_s / 1e3), "steps": steps5}
+    except sf.SfnlError as e:
+        cfg["split3"] = {"unavailable": str(e)}
+    nb = 8.0 * m * npts * (18 + k * (18 + 12))
+    cfg["roofline"] = {"jvp": roof(nb, ms_j, "large_syn_tf_kernel + large_prod_tf_kernel (per tangent)"),
+                       "vjp": roof(nb, ms_t, "large_syn_tf_kernel + large_prod_tf_kernel (per tangent)")}
+    if cpu_on:
+        n_s, kt = 500, 2
+        hU, hW, hB = (np.asfortranarray(H(x[:n_s])) for x in (U, W, B))
+        hT = [np.asfortranarray(H(tan[:n_s, :, :, t])) for t in range(kt)]
+
+        def cpu5():
+            outs = []
+            for t in range(kt):
+                du, dw, db = hT[t][:, 0:6], hT[t][:, 6:12], hT[t][:, 12:18]
+                c = lambda x, y: R.cpu_product("cross", np.asfortranarray(x), np.asfortranarray(y), pad,  # noqa: E731
+                                               n_theta=2 * pad, threads=cores)
+                outs.append(np.concatenate([c(du, hW) + c(hU, dw), c(du, hB) + c(hU, db)], axis=1))
+            return outs
+
+        dt, refs, reps = time_cpu(cpu5)
+        cfg["cpu_baseline"] = {"value": n_s * m * kt / k / dt, "unit": UNIT, "cores": cores, "kind": "port",
+                               "sample": f"{kt} of {k} tangents on {n_s} of {npts} points, {reps} reps (value scaled to "
+                                         "16 tangents); four cross products per tangent by the C restatement"}
+        sf.mhd_jvp(U, W, B, tan, m_max_pad=pad, out=jv)
+        cfg["jvp"]["rel_l2_vs_cpu_port"] = max(R_rel_l2(H(jv[:n_s, :, :, t]), refs[t]) for t in range(kt))
+    res["mhd_jvp_350k_m256_k16"] = cfg
+    del U, W, B, tan, cot, jv, jt
+    torch.cuda.empty_cache()
+    return res
 
 
 def _traffic(workload, form):

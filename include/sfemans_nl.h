@@ -350,6 +350,11 @@ int sfnl_set_check_finite(int on); /* 1: scan outputs for NaN/Inf after each cal
  * any other teardown of a device's primary context while the library stays
  * loaded: cached device addresses do not survive the context. */
 int sfnl_finalize(void);
+/* Diagnostic (no counterpart in the reference): FP64 throughput of the current
+ * device in TFLOP/s for mma.sync.m8n8k4.f64 and for FP64 FMAs, each measured
+ * alone with CUDA events (long register-only chains, every SM busy, best of
+ * five launches): the compute roofline of the all-FP64 forms. */
+int sfnl_probe_fp64_tflops(double *dmma_tflops, double *dfma_tflops);
 /* Host-side fault injection for tests of the error path: marks the split-form
  * status word as a kernel does when a bounded wait on its tensor-core
  * operations gives up (no GPU work is involved).  The next split-form call

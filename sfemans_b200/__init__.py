@@ -107,6 +107,7 @@ _SIGS = {
     "sfnl_finalize": [],
     "sfnl_last_host_timing": [_P],
     "sfnl_test_inject_timeout": [],
+    "sfnl_probe_fp64_tflops": [_P, _P],
 }
 
 

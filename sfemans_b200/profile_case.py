@@ -4,7 +4,7 @@
 
 Programs: cross, dot, prod, div, svect, svdiv, tensor, tension (the reference routines, by the op names of
 sfemans_b200.KINDS), bundle (u x w, u x b, j x b, u . gradT), and the synthesis-only real (grid values of a
-3-vector, FFT_PAR_REAL) and maxvel (FFT_MAX_VEL_DCL), and the linearised programs cross_jvp, cross_vjp,
+3-vector, FFT_PAR_REAL) and maxvel (FFT_MAX_VEL_DCL), fp64peak (the FP64 pipe's DMMA and DFMA throughput), and the linearised programs cross_jvp, cross_vjp,
 mhd_jvp, mhd_vjp on --k tangents (or cotangents) at one base state, and the Gauss-point callers gauss_ns,
 gauss_lorentz and gauss_advect on a P2 mesh of about --np Gauss points (nodal fields as inputs).
 Forms: fast (FP64, folded transforms), grid (FP64, caller's grid), split3 / split2 (bf16 slices on tcgen05).
@@ -87,7 +87,8 @@ def main(argv=None):
     import sfemans_b200 as sf
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--program", default="cross", choices=list(sf.KINDS) + ["bundle", "real", "maxvel"] + list(LINEAR) + list(GAUSS))
+    ap.add_argument("--program", default="cross",
+                    choices=list(sf.KINDS) + ["bundle", "real", "maxvel", "fp64peak"] + list(LINEAR) + list(GAUSS))
     ap.add_argument("--form", default="fast", choices=["fast", "grid", "split3", "split2"])
     ap.add_argument("--np", type=int, default=100_000)
     ap.add_argument("--m", type=int, default=64)
@@ -98,6 +99,13 @@ def main(argv=None):
     kw = {"fast": dict(algo=sf.ALGO_FAST), "grid": dict(algo=sf.ALGO_GRID), "split3": dict(split=sf.SPLIT_BF16X3),
           "split2": dict(split=sf.SPLIT_BF16X2)}[a.form]
     pad = 3 * a.m // 2 if a.m > 1 else 1
+    if a.program == "fp64peak":  # FP64 pipe throughput (the FP64 forms' compute roofline)
+        import ctypes
+
+        dm, df = ctypes.c_double(), ctypes.c_double()
+        sf._check(sf.lib().sfnl_probe_fp64_tflops(ctypes.byref(dm), ctypes.byref(df)))
+        print(f"fp64peak: mma.sync.m8n8k4.f64 {dm.value:.2f} TFLOP/s, DFMA {df.value:.2f} TFLOP/s", flush=True)
+        return
     if a.program in ("real", "maxvel"):
         x = _field(torch, a.np, 6, a.m, a.alpha, 1)
         if a.program == "real":

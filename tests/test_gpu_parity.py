@@ -98,7 +98,8 @@ def test_reference_signature_on_host_arrays(kind):
     bloc = npts + 1  # the callers' bloc_size = np/nb_procs+1
     fn(None, V1, V2, out, 1, bloc, 3 * m // 2, temps)
     assert R.rel_l2(out, R.c_oracle(kind, V1, V2, 3 * m // 2)) <= FP64_TOL
-    assert temps[1] > 0 and temps[2] == 0.0
+    # zeroed on entry, then device seconds: copies (where the reference has its all-to-alls), kernels, 0
+    assert temps[0] > 0 and temps[0] < 7.0 and temps[1] > 0 and temps[1] < 7.0 and temps[2] == 0.0
 
 
 def test_reference_signature_on_device_tensors():

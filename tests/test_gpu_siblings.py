@@ -138,7 +138,8 @@ def test_reference_signature_on_host_arrays(kind):
     else:
         sf.FFT_TENSOR_DCL(None, V1, V2, out, 1, bloc, pad, temps, opt_tension=True if kind == "tension" else None)
     assert _worst(kind, out, ref) <= FP64_TOL
-    assert temps[0] == 0.0 and temps[1] > 0.0
+    # temps(1) = host<->device copy seconds, temps(2) = kernel seconds, temps(3) = 0 (nothing repacked)
+    assert temps[0] > 0.0 and temps[1] > 0.0 and temps[2] == 0.0
 
 
 @pytest.mark.parametrize("kind", ["svect", "tensor", "tension"])
