@@ -49,7 +49,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "nonlinear-term Gauss-pt·modes/s: split-prec vs FP64 on 1 B200 at ≤1e-7 rel err"
 UNIT = "Gauss-pt*modes/s"
-FP64_PIPE_TFLOPS = 36.6  # FP64 tensor (DMMA) and DFMA throughput shared on B200, measured by a throughput probe
+FP64_PIPE_TFLOPS = 36.6  # FP64 DMMA/DFMA throughput on B200 (sfnl_probe_fp64_tflops: 37.1 DMMA, 34.1 DFMA)
 
 # name: points, modes, pad, decay, input fields (6-slot), output slots, description
 WORKLOADS = {
@@ -332,7 +332,8 @@ def main():
         flops = 3600.0 * 512.0 * ((npts + 7) // 8)
         fp64_pipe = {"kernel": "fast_bundle_tf_kernel<64>", "flops_per_launch": flops,
                      "achieved_tflops": flops / (dom_ms / 1e3) / 1e12, "peak_tflops": FP64_PIPE_TFLOPS,
-                     "peak_source": "probe: mma.sync f64 and DFMA throughput on this pool's B200 (not in MEASURED_PEAKS.json)",
+                     "peak_source": "sfnl_probe_fp64_tflops (python -m sfemans_b200.profile_case --program fp64peak: "
+                                    "DMMA 37.1, DFMA 34.1 TFLOP/s); not in MEASURED_PEAKS.json",
                      "frac": flops / (dom_ms / 1e3) / 1e12 / FP64_PIPE_TFLOPS}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": results[best]["steps"],
@@ -445,7 +446,8 @@ def _e2e_bundle(sf, torch, ins, npts, m, pad, form, steps, world, dist):
     sf.finalize()
     return {"value": world * npts * m / dt, "unit": UNIT, "h2d_bytes_per_step": 8 * npts * m * 30,
             "d2h_bytes_per_step": 8 * npts * m * 20, "ms_per_step": dt * 1e3,
-            "last_step_split_s": {"h2d": t_split[0], "kernels": t_split[1], "d2h": t_split[2]},
+            "last_step_device_s": {"copies": t_split[0], "kernels": t_split[1],
+                                   "note": "sums over the call's chunks on four streams (overlapping)"},
             "api": "sfnl_bundle_mhd_host (host arrays, pinned)"}
 
 

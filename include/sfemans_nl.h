@@ -340,6 +340,29 @@ int sfnl_cross_f64_noalloc(const double *v1, const double *v2, double *out, int6
                            sfnl_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Fourier-mode-distributed callers, nb_procs > 1 (replace the body of the
+ * reference routines of fft_parallel.F90:147 / :330 / :502 / :667 / :1021 /
+ * :1543 between and around its two MPI_ALLTOALLs, :205-217 and :306-324).
+ * Every rank holds m_max_c modes of np points; block q = points
+ * [q*bloc_size, (q+1)*bloc_size).  The caller keeps its MPI:
+ *   pack_modes(V1) -> send1, pack_modes(V2) -> send2   (per peer q: block q of my modes)
+ *   MPI_ALLTOALL(send1 -> recv1), MPI_ALLTOALL(send2 -> recv2)
+ *   fft_par_block(op, recv1, recv2 -> back)            (my block, all modes, on the GPU)
+ *   MPI_ALLTOALL(back -> got)
+ *   unpack_modes(got) -> V_out                          (my modes of all points)
+ * Buffers hold nb_procs peers of bloc_size*nslot*m_max_c*ew doubles, ordered
+ * [peer][mode][slot][point][e]; ew = 3 only for the output of the tensor
+ * products (V_out(3, np, 6, m)), else 1.  op: SFNL_OP_*; its slot counts are
+ * those of sfnl_product_f64.  temps as in the reference-signature entries.
+ * ------------------------------------------------------------------------- */
+int sfnl_fft_par_pack_modes(const double *V, double *send, int np, int nslot, int m_max_c, int nb_procs, int bloc_size,
+                            int ew);
+int sfnl_fft_par_block(int op, const double *recv1, const double *recv2, double *back, int bloc_size, int m_max_c,
+                       int nb_procs, int m_max_pad, double *temps);
+int sfnl_fft_par_unpack_modes(const double *got, double *V_out, int np, int nslot, int m_max_c, int nb_procs,
+                              int bloc_size, int ew);
+
+/* ---------------------------------------------------------------------------
  * Library state.
  * ------------------------------------------------------------------------- */
 const char *sfnl_last_error(void); /* message of the last failing call on this thread */

@@ -108,6 +108,9 @@ _SIGS = {
     "sfnl_last_host_timing": [_P],
     "sfnl_test_inject_timeout": [],
     "sfnl_probe_fp64_tflops": [_P, _P],
+    "sfnl_fft_par_pack_modes": [_P, _P] + [_I] * 6,
+    "sfnl_fft_par_block": [_I, _P, _P, _P] + [_I] * 4 + [_P],
+    "sfnl_fft_par_unpack_modes": [_P, _P] + [_I] * 6,
 }
 
 

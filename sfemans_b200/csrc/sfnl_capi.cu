@@ -726,6 +726,87 @@ int sfnl_fft_tensor_dcl(const double *V1_in, const double *V2_in, double *V_out,
                       m_max_pad, 0, SFNL_ALGO_AUTO, temps);
 }
 
+// ---------------------------------------------------------------------------
+// Fourier-mode-distributed callers (nb_procs > 1).  The reference splits the modes over the ranks of its
+// Fourier communicator and exchanges them twice per call (fft_parallel.F90:205-217 and :306-324): each
+// rank sends every peer q the points of q's block [q*bloc_size, (q+1)*bloc_size) of its own m_max_c
+// modes, computes the product on its block with all m_max = nb_procs*m_max_c modes, and sends the modes
+// of peer q back.  The exchanges stay with the caller's MPI (the Fortran shim calls MPI_ALLTOALL); these
+// entries lay the buffers out and run the block's product on the GPU.  Buffer layout, per peer:
+// [mode i < m_max_c][slot s < nslot][point n < bloc_size][e < ew] (ew = 3 for the tensor's V(3, np, 6, m)),
+// bloc_size*nslot*m_max_c*ew doubles per peer; points beyond np are zero.
+// ---------------------------------------------------------------------------
+int sfnl_fft_par_pack_modes(const double *V, double *send, int np, int nslot, int m_max_c, int nb_procs, int bloc_size,
+                            int ew) {
+  if (np < 0 || nslot < 1 || m_max_c < 1 || nb_procs < 1 || bloc_size < 1 || (ew != 1 && ew != 3))
+    return set_error(SFNL_ERR_ARG, "sfnl_fft_par_pack_modes: bad sizes");
+  if ((int64_t)np > (int64_t)nb_procs * bloc_size) return set_error(SFNL_ERR_SHAPE, "np > nb_procs*bloc_size");
+  if ((np > 0 && !V) || !send) return set_error(SFNL_ERR_ARG, "null array");
+  for (int q = 0; q < nb_procs; ++q)
+    for (int i = 0; i < m_max_c; ++i)
+      for (int sl = 0; sl < nslot; ++sl) {
+        double *dst = send + (((size_t)q * m_max_c + i) * nslot + sl) * (size_t)bloc_size * ew;
+        for (int n = 0; n < bloc_size; ++n) {
+          const int64_t gp = (int64_t)q * bloc_size + n;
+          for (int e = 0; e < ew; ++e)
+            dst[(size_t)n * ew + e] = gp < np ? V[e + ew * (gp + (int64_t)np * (sl + (int64_t)nslot * i))] : 0.0;
+        }
+      }
+  return SFNL_OK;
+}
+
+int sfnl_fft_par_unpack_modes(const double *got, double *V_out, int np, int nslot, int m_max_c, int nb_procs,
+                              int bloc_size, int ew) {
+  if (np < 0 || nslot < 1 || m_max_c < 1 || nb_procs < 1 || bloc_size < 1 || (ew != 1 && ew != 3))
+    return set_error(SFNL_ERR_ARG, "sfnl_fft_par_unpack_modes: bad sizes");
+  if ((int64_t)np > (int64_t)nb_procs * bloc_size) return set_error(SFNL_ERR_SHAPE, "np > nb_procs*bloc_size");
+  if (!got || (np > 0 && !V_out)) return set_error(SFNL_ERR_ARG, "null array");
+  for (int q = 0; q < nb_procs; ++q)
+    for (int i = 0; i < m_max_c; ++i)
+      for (int sl = 0; sl < nslot; ++sl) {
+        const double *src = got + (((size_t)q * m_max_c + i) * nslot + sl) * (size_t)bloc_size * ew;
+        for (int n = 0; n < bloc_size; ++n) {
+          const int64_t gp = (int64_t)q * bloc_size + n;
+          if (gp >= np) break;  // dummy points are dropped (fft_parallel.F90:317)
+          for (int e = 0; e < ew; ++e) V_out[e + ew * (gp + (int64_t)np * (sl + (int64_t)nslot * i))] = src[(size_t)n * ew + e];
+        }
+      }
+  return SFNL_OK;
+}
+
+int sfnl_fft_par_block(int op, const double *recv1, const double *recv2, double *back, int bloc_size, int m_max_c,
+                       int nb_procs, int m_max_pad, double *temps) {
+  if (temps) temps[0] = temps[1] = temps[2] = 0.0;
+  if (op < 0 || op >= kNumProducts) return set_error(SFNL_ERR_ARG, "op must be one of SFNL_OP_* (0..7)");
+  if (bloc_size < 1 || m_max_c < 1 || nb_procs < 1) return set_error(SFNL_ERR_ARG, "sfnl_fft_par_block: bad sizes");
+  if (!recv1 || !recv2 || !back) return set_error(SFNL_ERR_ARG, "null array");
+  const ProductKind &pk = kProducts[op];
+  const int m = m_max_c * nb_procs, ew = pk.tensor_out ? 3 : 1;
+  const size_t b1 = (size_t)bloc_size * pk.nsl_a * m, b2 = (size_t)bloc_size * pk.nsl_b * m;
+  const size_t bo = (size_t)bloc_size * pk.nsl_out * m * ew;
+  std::vector<double> x(b1), y(b2), z(bo);
+  // gathered block (bloc_size, nslot, m_max): global mode r*m_max_c + i from peer r (:223-231)
+  auto gather = [&](const double *recv, int nsl, double *blk) {
+    for (int r = 0; r < nb_procs; ++r)
+      for (int i = 0; i < m_max_c; ++i)
+        for (int sl = 0; sl < nsl; ++sl)
+          std::memcpy(blk + (size_t)bloc_size * (sl + (size_t)nsl * (r * m_max_c + i)),
+                      recv + (((size_t)r * m_max_c + i) * nsl + sl) * bloc_size, sizeof(double) * bloc_size);
+  };
+  gather(recv1, pk.nsl_a, x.data());
+  gather(recv2, pk.nsl_b, y.data());
+  int rc = host_product(op, x.data(), y.data(), z.data(), bloc_size, m, m_max_pad, 0, SFNL_ALGO_AUTO, temps);
+  if (rc) return rc;
+  // modes of peer q back to q (:306-324)
+  for (int q = 0; q < nb_procs; ++q)
+    for (int i = 0; i < m_max_c; ++i)
+      for (int sl = 0; sl < pk.nsl_out; ++sl)
+        std::memcpy(back + (((size_t)q * m_max_c + i) * pk.nsl_out + sl) * bloc_size * ew,
+                    z.data() + (size_t)ew * bloc_size * (sl + (size_t)pk.nsl_out * (q * m_max_c + i)),
+                    sizeof(double) * bloc_size * ew);
+  return SFNL_OK;
+}
+
 int sfnl_scalar_vect_f64(const double *v, const double *s, double *out, int64_t np, int m_max, int m_max_pad, int pb,
                          sfnl_stream_t stream) {
   if (pb != 1 && pb != 2) return set_error(SFNL_ERR_ARG, "error in problem type while calling FFT_SCALAR_VECT_DCL");

@@ -12,10 +12,16 @@
 !   FFT_TENSOR_DCL          fft_parallel.F90:1543
 !   FFT_PAR_REAL            fft_parallel.F90:28    (V_out ALLOCATABLE, allocated here as in the reference)
 !   FFT_MAX_VEL_DCL         fft_parallel.F90:1426
-! One GPU holds every Fourier mode, so the Fourier communicator must have
-! one rank (nb_procs == 1).  bloc_size is checked (np <= nb_procs*bloc_size)
-! and otherwise unused.  temps(3), when present, receives the data-movement
-! seconds in temps(1) and the kernel seconds in temps(2).  A non-zero status
+! With one Fourier rank (nb_procs == 1) the library holds every mode and
+! bloc_size is only checked (np <= nb_procs*bloc_size).  With nb_procs > 1
+! the products keep the reference's exchange (fft_parallel.F90:205-217 and
+! :306-324): the library lays out the send buffers, MPI_ALLTOALL gathers the
+! rank's block of bloc_size points with all modes, the library computes the
+! block's product on the GPU, a second MPI_ALLTOALL returns every rank its
+! modes, and the library unpacks them (dummy points dropped).  temps(3), when
+! present, is zeroed and receives the exchange and host<->device copy seconds
+! in temps(1), the kernel seconds in temps(2) and the buffer layout seconds in
+! temps(3).  FFT_PAR_REAL and FFT_MAX_VEL_DCL run on one rank.  A non-zero status
 ! from the library prints 'BUG in FFT_PAR_...' with the library's message and
 ! STOPs, as the reference does (fft_parallel.F90:188-191).
 !
@@ -114,6 +120,35 @@ MODULE fft_parallele_gpu
        INTEGER(C_INT)        :: rc
      END FUNCTION sfnl_fft_max_vel_dcl
 
+     FUNCTION sfnl_fft_par_pack_modes(V, send, np, nslot, m_max_c, nb_procs, bloc_size, ew) RESULT(rc) &
+          BIND(C, NAME='sfnl_fft_par_pack_modes')
+       IMPORT :: C_INT, C_DOUBLE
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(IN)  :: V
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(OUT) :: send
+       INTEGER(C_INT), VALUE :: np, nslot, m_max_c, nb_procs, bloc_size, ew
+       INTEGER(C_INT)        :: rc
+     END FUNCTION sfnl_fft_par_pack_modes
+
+     FUNCTION sfnl_fft_par_block(op, recv1, recv2, back, bloc_size, m_max_c, nb_procs, m_max_pad, temps) RESULT(rc) &
+          BIND(C, NAME='sfnl_fft_par_block')
+       IMPORT :: C_INT, C_DOUBLE, C_PTR
+       INTEGER(C_INT), VALUE :: op
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(IN)  :: recv1, recv2
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(OUT) :: back
+       INTEGER(C_INT), VALUE :: bloc_size, m_max_c, nb_procs, m_max_pad
+       TYPE(C_PTR), VALUE    :: temps
+       INTEGER(C_INT)        :: rc
+     END FUNCTION sfnl_fft_par_block
+
+     FUNCTION sfnl_fft_par_unpack_modes(got, V_out, np, nslot, m_max_c, nb_procs, bloc_size, ew) RESULT(rc) &
+          BIND(C, NAME='sfnl_fft_par_unpack_modes')
+       IMPORT :: C_INT, C_DOUBLE
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(IN)  :: got
+       REAL(C_DOUBLE), DIMENSION(*), INTENT(OUT) :: V_out
+       INTEGER(C_INT), VALUE :: np, nslot, m_max_c, nb_procs, bloc_size, ew
+       INTEGER(C_INT)        :: rc
+     END FUNCTION sfnl_fft_par_unpack_modes
+
      FUNCTION sfnl_last_error() RESULT(msg) BIND(C, NAME='sfnl_last_error')
        IMPORT :: C_PTR
        TYPE(C_PTR) :: msg
@@ -133,6 +168,77 @@ CONTAINS
        STOP
     END IF
   END SUBROUTINE check_comm
+
+  ! .TRUE. when the products run mode-distributed (nb_procs > 1); the communicator must have nb_procs ranks.
+  LOGICAL FUNCTION distributed(communicator, nb_procs, what)
+    MPI_Comm,         INTENT(IN) :: communicator
+    INTEGER,          INTENT(IN) :: nb_procs
+    CHARACTER(LEN=*), INTENT(IN) :: what
+    INTEGER :: nproc, code
+    CALL MPI_COMM_SIZE(communicator, nproc, code)
+    IF (nproc /= nb_procs) THEN
+       WRITE(*,*) ' BUG in ', what, ': nb_procs differs from the size of the communicator'
+       STOP
+    END IF
+    distributed = nb_procs > 1
+  END FUNCTION distributed
+
+  ! The body of a product routine on a mode-distributed communicator: library op code op (SFNL_OP_*),
+  ! inputs of nsl1 and nsl2 slots, output of nout slots (ew = 3 for the tensor's V_out(3, np, 6, m)).
+  SUBROUTINE mode_distributed(communicator, op, V1_in, nsl1, V2_in, nsl2, V_out, nout, ew, np, m_max_c, &
+       nb_procs, bloc_size, m_max_pad, what, temps)
+    MPI_Comm :: communicator
+    INTEGER, INTENT(IN) :: op, nsl1, nsl2, nout, ew, np, m_max_c, nb_procs, bloc_size, m_max_pad
+    REAL(KIND=8), DIMENSION(*), INTENT(IN)  :: V1_in, V2_in
+    REAL(KIND=8), DIMENSION(*), INTENT(OUT) :: V_out
+    CHARACTER(LEN=*), INTENT(IN) :: what
+    REAL(KIND=8), DIMENSION(:), OPTIONAL, INTENT(INOUT) :: temps
+    REAL(KIND=8), DIMENSION(:), ALLOCATABLE :: s1, s2, r1, r2, back, got
+    REAL(C_DOUBLE), DIMENSION(3), TARGET :: t3
+    REAL(KIND=8) :: t, tcomm, tpack
+    INTEGER :: n1, n2, no, code
+    INTEGER(C_INT) :: rc
+    n1 = bloc_size*nsl1*m_max_c
+    n2 = bloc_size*nsl2*m_max_c
+    no = bloc_size*nout*m_max_c*ew
+    ALLOCATE(s1(n1*nb_procs), r1(n1*nb_procs), s2(n2*nb_procs), r2(n2*nb_procs), back(no*nb_procs), got(no*nb_procs))
+    t = MPI_WTIME()
+    rc = sfnl_fft_par_pack_modes(V1_in, s1, INT(np, C_INT), INT(nsl1, C_INT), INT(m_max_c, C_INT), &
+         INT(nb_procs, C_INT), INT(bloc_size, C_INT), 1_C_INT)
+    CALL stop_on_error(rc, what)
+    rc = sfnl_fft_par_pack_modes(V2_in, s2, INT(np, C_INT), INT(nsl2, C_INT), INT(m_max_c, C_INT), &
+         INT(nb_procs, C_INT), INT(bloc_size, C_INT), 1_C_INT)
+    CALL stop_on_error(rc, what)
+    tpack = MPI_WTIME() - t
+    t = MPI_WTIME()
+    CALL MPI_ALLTOALL(s1, n1, MPI_DOUBLE_PRECISION, r1, n1, MPI_DOUBLE_PRECISION, communicator, code)
+    CALL MPI_ALLTOALL(s2, n2, MPI_DOUBLE_PRECISION, r2, n2, MPI_DOUBLE_PRECISION, communicator, code)
+    tcomm = MPI_WTIME() - t
+    rc = sfnl_fft_par_block(INT(op, C_INT), r1, r2, back, INT(bloc_size, C_INT), INT(m_max_c, C_INT), &
+         INT(nb_procs, C_INT), INT(m_max_pad, C_INT), C_LOC(t3))
+    CALL stop_on_error(rc, what)
+    t = MPI_WTIME()
+    CALL MPI_ALLTOALL(back, no, MPI_DOUBLE_PRECISION, got, no, MPI_DOUBLE_PRECISION, communicator, code)
+    tcomm = tcomm + MPI_WTIME() - t
+    t = MPI_WTIME()
+    rc = sfnl_fft_par_unpack_modes(got, V_out, INT(np, C_INT), INT(nout, C_INT), INT(m_max_c, C_INT), &
+         INT(nb_procs, C_INT), INT(bloc_size, C_INT), INT(ew, C_INT))
+    CALL stop_on_error(rc, what)
+    tpack = tpack + MPI_WTIME() - t
+    DEALLOCATE(s1, r1, s2, r2, back, got)
+    IF (PRESENT(temps)) THEN
+       temps = 0.d0
+       temps(1) = tcomm + t3(1)
+       IF (SIZE(temps) > 1) temps(2) = t3(2)
+       IF (SIZE(temps) > 2) temps(3) = tpack
+    END IF
+  END SUBROUTINE mode_distributed
+
+  SUBROUTINE usage_stop(what, why)
+    CHARACTER(LEN=*), INTENT(IN) :: what, why
+    WRITE(*,*) ' BUG in ', what, ' : ', why
+    STOP
+  END SUBROUTINE usage_stop
 
   SUBROUTINE stop_on_error(rc, what)
     INTEGER(C_INT),   INTENT(IN) :: rc
@@ -159,7 +265,13 @@ CONTAINS
     REAL(KIND=8), DIMENSION(:), OPTIONAL, INTENT(INOUT) :: temps
     REAL(C_DOUBLE), DIMENSION(3), TARGET :: t3
     INTEGER(C_INT) :: rc
-    CALL check_comm(communicator, nb_procs, 'FFT_PAR_CROSS_PROD_DCL')
+    IF (distributed(communicator, nb_procs, 'FFT_PAR_CROSS_PROD_DCL')) THEN
+       IF (SIZE(V1_in,2) /= 6 .OR. SIZE(V2_in,2) /= 6) &
+            CALL usage_stop('FFT_PAR_CROSS_PROD_DCL', 'the number of slots SIZE(V,2) does not fit the product')
+       CALL mode_distributed(communicator, 0, V1_in, 6, V2_in, 6, V_out, 6, 1, SIZE(V1_in,1), SIZE(V1_in,3), &
+            nb_procs, bloc_size, m_max_pad, 'FFT_PAR_CROSS_PROD_DCL', temps)
+       RETURN
+    END IF
     rc = sfnl_fft_par_cross_prod_dcl(V1_in, V2_in, V_out, INT(SIZE(V1_in,1), C_INT), INT(SIZE(V1_in,2), C_INT), &
          INT(SIZE(V1_in,3), C_INT), INT(nb_procs, C_INT), INT(bloc_size, C_INT), INT(m_max_pad, C_INT), C_LOC(t3))
     CALL stop_on_error(rc, 'FFT_PAR_CROSS_PROD_DCL')
@@ -177,7 +289,13 @@ CONTAINS
     REAL(KIND=8), DIMENSION(:), OPTIONAL, INTENT(INOUT) :: temps
     REAL(C_DOUBLE), DIMENSION(3), TARGET :: t3
     INTEGER(C_INT) :: rc
-    CALL check_comm(communicator, nb_procs, 'FFT_PAR_DOT_PROD_DCL')
+    IF (distributed(communicator, nb_procs, 'FFT_PAR_DOT_PROD_DCL')) THEN
+       IF (SIZE(V1_in,2) /= 6 .OR. SIZE(V2_in,2) /= 6) &
+            CALL usage_stop('FFT_PAR_DOT_PROD_DCL', 'the number of slots SIZE(V,2) does not fit the product')
+       CALL mode_distributed(communicator, 1, V1_in, 6, V2_in, 6, c_out, 2, 1, SIZE(V1_in,1), SIZE(V1_in,3), &
+            nb_procs, bloc_size, m_max_pad, 'FFT_PAR_DOT_PROD_DCL', temps)
+       RETURN
+    END IF
     rc = sfnl_fft_par_dot_prod_dcl(V1_in, V2_in, c_out, INT(SIZE(V1_in,1), C_INT), INT(SIZE(V1_in,2), C_INT), &
          INT(SIZE(V1_in,3), C_INT), INT(nb_procs, C_INT), INT(bloc_size, C_INT), INT(m_max_pad, C_INT), C_LOC(t3))
     CALL stop_on_error(rc, 'FFT_PAR_DOT_PROD_DCL')
@@ -195,7 +313,13 @@ CONTAINS
     REAL(KIND=8), DIMENSION(:), OPTIONAL, INTENT(INOUT) :: temps
     REAL(C_DOUBLE), DIMENSION(3), TARGET :: t3
     INTEGER(C_INT) :: rc
-    CALL check_comm(communicator, nb_procs, 'FFT_PAR_PROD_DCL')
+    IF (distributed(communicator, nb_procs, 'FFT_PAR_PROD_DCL')) THEN
+       IF (SIZE(c1_in,2) /= 2 .OR. SIZE(c2_in,2) /= 2) &
+            CALL usage_stop('FFT_PAR_PROD_DCL', 'the number of slots SIZE(V,2) does not fit the product')
+       CALL mode_distributed(communicator, 2, c1_in, 2, c2_in, 2, c_out, 2, 1, SIZE(c1_in,1), SIZE(c1_in,3), &
+            nb_procs, bloc_size, m_max_pad, 'FFT_PAR_PROD_DCL', temps)
+       RETURN
+    END IF
     rc = sfnl_fft_par_prod_dcl(c1_in, c2_in, c_out, INT(SIZE(c1_in,1), C_INT), INT(SIZE(c1_in,3), C_INT), &
          INT(nb_procs, C_INT), INT(bloc_size, C_INT), INT(m_max_pad, C_INT), C_LOC(t3))
     CALL stop_on_error(rc, 'FFT_PAR_PROD_DCL')
@@ -213,7 +337,13 @@ CONTAINS
     REAL(KIND=8), DIMENSION(:), OPTIONAL, INTENT(INOUT) :: temps
     REAL(C_DOUBLE), DIMENSION(3), TARGET :: t3
     INTEGER(C_INT) :: rc
-    CALL check_comm(communicator, nb_procs, 'FFT_PAR_DIV_DCL')
+    IF (distributed(communicator, nb_procs, 'FFT_PAR_DIV_DCL')) THEN
+       IF (SIZE(c1_in,2) /= 2 .OR. SIZE(c2_in,2) /= 2) &
+            CALL usage_stop('FFT_PAR_DIV_DCL', 'the number of slots SIZE(V,2) does not fit the product')
+       CALL mode_distributed(communicator, 3, c1_in, 2, c2_in, 2, c_out, 2, 1, SIZE(c1_in,1), SIZE(c1_in,3), &
+            nb_procs, bloc_size, m_max_pad, 'FFT_PAR_DIV_DCL', temps)
+       RETURN
+    END IF
     rc = sfnl_fft_par_div_dcl(c1_in, c2_in, c_out, INT(SIZE(c1_in,1), C_INT), INT(SIZE(c1_in,3), C_INT), &
          INT(nb_procs, C_INT), INT(bloc_size, C_INT), INT(m_max_pad, C_INT), C_LOC(t3))
     CALL stop_on_error(rc, 'FFT_PAR_DIV_DCL')
@@ -232,7 +362,14 @@ CONTAINS
     REAL(KIND=8), DIMENSION(:), OPTIONAL, INTENT(INOUT) :: temps
     REAL(C_DOUBLE), DIMENSION(3), TARGET :: t3
     INTEGER(C_INT) :: rc
-    CALL check_comm(communicator, nb_procs, 'FFT_SCALAR_VECT_DCL')
+    IF (distributed(communicator, nb_procs, 'FFT_SCALAR_VECT_DCL')) THEN
+       IF (SIZE(V1_in,2) /= 6 .OR. SIZE(V2_in,2) /= 2) &
+            CALL usage_stop('FFT_SCALAR_VECT_DCL', 'the number of slots SIZE(V,2) does not fit the product')
+       IF (pb /= 1 .AND. pb /= 2) CALL usage_stop('FFT_SCALAR_VECT_DCL', 'error in problem type')
+       CALL mode_distributed(communicator, 3 + pb, V1_in, 6, V2_in, 2, V_out, 6, 1, SIZE(V1_in,1), SIZE(V1_in,3), &
+            nb_procs, bloc_size, m_max_pad, 'FFT_SCALAR_VECT_DCL', temps)
+       RETURN
+    END IF
     rc = sfnl_fft_scalar_vect_dcl(V1_in, V2_in, V_out, INT(pb, C_INT), INT(SIZE(V1_in,1), C_INT), &
          INT(SIZE(V1_in,2), C_INT), INT(SIZE(V2_in,2), C_INT), INT(SIZE(V1_in,3), C_INT), INT(nb_procs, C_INT), &
          INT(bloc_size, C_INT), INT(m_max_pad, C_INT), C_LOC(t3))
@@ -252,11 +389,18 @@ CONTAINS
     LOGICAL,                    OPTIONAL, INTENT(IN)    :: opt_tension
     REAL(C_DOUBLE), DIMENSION(3), TARGET :: t3
     INTEGER(C_INT) :: rc, tension
-    CALL check_comm(communicator, nb_procs, 'FFT_TENSOR_DCL')
     tension = -1                     ! absent: plain tensor product
     IF (PRESENT(opt_tension)) THEN
        tension = 0                   ! present and .FALSE.: rejected by the library, as by the reference
        IF (opt_tension) tension = 1
+    END IF
+    IF (distributed(communicator, nb_procs, 'FFT_TENSOR_DCL')) THEN
+       IF (SIZE(V1_in,2) /= 6 .OR. SIZE(V2_in,2) /= 6) &
+            CALL usage_stop('FFT_TENSOR_DCL', 'the number of slots SIZE(V,2) does not fit the product')
+       IF (tension == 0) CALL usage_stop('FFT_TENSOR_DCL', 'opt_tension should be true if used')
+       CALL mode_distributed(communicator, MERGE(7, 6, tension > 0), V1_in, 6, V2_in, 6, V_out, 6, 3, &
+            SIZE(V1_in,1), SIZE(V1_in,3), nb_procs, bloc_size, m_max_pad, 'FFT_TENSOR_DCL', temps)
+       RETURN
     END IF
     rc = sfnl_fft_tensor_dcl(V1_in, V2_in, V_out, INT(SIZE(V1_in,1), C_INT), INT(SIZE(V1_in,2), C_INT), &
          INT(SIZE(V1_in,3), C_INT), INT(nb_procs, C_INT), INT(bloc_size, C_INT), INT(m_max_pad, C_INT), tension, &

@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 import sfemans_b200 as sf
+from oracle import ref_fft as R
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -241,3 +242,53 @@ def test_gauss_operands_entry_checks():
     assert L.sfnl_gauss_operands_f64(2, d, d, None, None, 1, d, d, d, d, d, *ops, 5, 2, 6, 7, 2, NULL) == -1  # no o2/o3
     assert L.sfnl_gauss_operands_f64(0, d, None, None, None, 0, d, d, d, d, d, *ops, 5, 2, 11, 7, 2, NULL) == -4  # n_w
     assert L.sfnl_gauss_operands_f64(0, d, None, None, None, 0, d, d, d, d, d, *ops, 5, 0, 6, 7, 2, NULL) == 0  # me = 0
+
+
+def _pack(L, V, nslot, mc, P, bloc, ew=1):
+    npts = V.shape[-3] if ew == 3 else V.shape[0]
+    send = np.zeros(P * bloc * nslot * mc * ew)
+    assert L.sfnl_fft_par_pack_modes(ctypes.c_void_p(V.ctypes.data), ctypes.c_void_p(send.ctypes.data), npts, nslot,
+                                     mc, P, bloc, ew) == 0
+    return send.reshape(P, mc, nslot, bloc * ew)
+
+
+@pytest.mark.parametrize("npts,nslot,m,P", [(23, 6, 6, 2), (31, 2, 9, 3), (7, 6, 4, 4), (1, 6, 2, 2)])
+def test_mode_exchange_layout(npts, nslot, m, P):
+    # rank r holds modes [r*mc, (r+1)*mc); after pack + all-to-all, rank q's received buffers hold block q of
+    # every mode (global mode r*mc + i from peer r); sending the block's modes back and unpacking returns each
+    # rank its own modes of every point (fft_parallel.F90:205-217, :306-324)
+    L = sf.lib()
+    mc, bloc = m // P, npts // P + 1
+    V = R.synthetic_field(npts, nslot, m, 0.1, 5)
+    local = [np.asfortranarray(V[:, :, r * mc:(r + 1) * mc]) for r in range(P)]
+    sends = [_pack(L, local[r], nslot, mc, P, bloc) for r in range(P)]
+    for q in range(P):
+        recv = np.stack([sends[r][q] for r in range(P)])  # (P, mc, nslot, bloc)
+        block = np.zeros((bloc, nslot, m))
+        for r in range(P):
+            block[:, :, r * mc:(r + 1) * mc] = recv[r].transpose(2, 1, 0)
+        want = np.zeros((bloc, nslot, m))
+        hi = min(npts, (q + 1) * bloc)
+        if hi > q * bloc:
+            want[:hi - q * bloc] = V[q * bloc:hi]
+        assert np.array_equal(block, want)
+    # identity "product": back[q'] = modes of q' of my block; then unpack
+    backs = []
+    for q in range(P):
+        recv = np.stack([sends[r][q] for r in range(P)])
+        backs.append(recv)  # modes of peer r are exactly what r sent: back[r] = recv[r]
+    for r in range(P):
+        got = np.ascontiguousarray(np.stack([backs[q][r] for q in range(P)]))
+        out = np.zeros((npts, nslot, mc), order="F")
+        assert L.sfnl_fft_par_unpack_modes(ctypes.c_void_p(got.ctypes.data), ctypes.c_void_p(out.ctypes.data), npts,
+                                           nslot, mc, P, bloc, 1) == 0
+        assert np.array_equal(out, local[r])
+
+
+def test_mode_exchange_argument_checks():
+    L = sf.lib()
+    a = ctypes.c_void_p(16)
+    assert L.sfnl_fft_par_pack_modes(a, a, 10, 6, 2, 2, 4, 1) == -2  # np > nb_procs*bloc_size
+    assert L.sfnl_fft_par_pack_modes(a, a, 10, 6, 2, 2, 5, 2) == -1  # ew must be 1 or 3
+    assert L.sfnl_fft_par_unpack_modes(a, a, 10, 6, 0, 2, 5, 1) == -1
+    assert L.sfnl_fft_par_block(9, a, a, a, 5, 2, 2, 3, None) == -1  # unknown op

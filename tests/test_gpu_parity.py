@@ -313,3 +313,62 @@ def test_large_m_point_chunks():
     V2 = R.synthetic_field(npts, 6, m, 0.05, 42)
     out = host(sf.product(0, dev(V1), dev(V2), m_max_pad=pad, algo=sf.ALGO_FAST))
     assert R.rel_l2(out, R.fft_par("cross", V1, V2, pad, workers=8)) <= FP64_TOL
+
+
+def _ranks_run(kind, V1, V2, P, pad):
+    """The mode-distributed path of the reference-signature routines with P emulated Fourier ranks: pack
+    on every rank, the all-to-all as a buffer transpose, the block's product on the GPU, back, unpack."""
+    import ctypes
+
+    L = sf.lib()
+    op, nsl1, nsl2, nout = sf.KINDS[kind]
+    tensor = kind in ("tensor", "tension")
+    ew = 3 if tensor else 1
+    npts, _, m = V1.shape
+    mc, bloc = m // P, npts // P + 1
+    ptr = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+
+    def pack(V, nsl, r):
+        loc = np.asfortranarray(V[:, :, r * mc:(r + 1) * mc])
+        buf = np.zeros(P * mc * nsl * bloc)
+        assert L.sfnl_fft_par_pack_modes(ptr(loc), ptr(buf), npts, nsl, mc, P, bloc, 1) == 0
+        return buf.reshape(P, -1)
+
+    s1 = [pack(V1, nsl1, r) for r in range(P)]
+    s2 = [pack(V2, nsl2, r) for r in range(P)]
+    backs = []
+    for q in range(P):
+        r1 = np.ascontiguousarray(np.stack([s1[r][q] for r in range(P)]))
+        r2 = np.ascontiguousarray(np.stack([s2[r][q] for r in range(P)]))
+        back = np.zeros(P * mc * nout * bloc * ew)
+        temps = np.zeros(3)
+        rc = L.sfnl_fft_par_block(op, ptr(r1), ptr(r2), ptr(back), bloc, mc, P, pad, ptr(temps))
+        assert rc == 0, sf.last_error()
+        assert temps[1] > 0.0
+        backs.append(back.reshape(P, -1))
+    outs = []
+    for r in range(P):
+        got = np.ascontiguousarray(np.stack([backs[q][r] for q in range(P)]))
+        shape = (3, npts, 6, mc) if tensor else (npts, nout, mc)
+        out = np.zeros(shape, order="F")
+        assert L.sfnl_fft_par_unpack_modes(ptr(got), ptr(out), npts, nout, mc, P, bloc, ew) == 0
+        outs.append(out)
+    return outs
+
+
+@pytest.mark.parametrize("kind,P,npts,m", [("cross", 2, 61, 8), ("cross", 3, 100, 12), ("dot", 3, 47, 9),
+                                           ("prod", 2, 33, 16), ("svect", 2, 29, 6), ("div", 3, 20, 6),
+                                           ("tensor", 2, 25, 4), ("tension", 3, 17, 6)])
+def test_mode_distributed_block_path(kind, P, npts, m):
+    # the body of FFT_PAR_*_DCL between and around its two MPI_ALLTOALLs (fft_parallel.F90:205-217, :306-324),
+    # each emulated rank's block on the GPU, against the oracle on the global arrays
+    _, nsl1, nsl2, _ = sf.KINDS[kind]
+    V1 = R.synthetic_field(npts, nsl1, m, 0.2, 301)
+    V2 = R.synthetic_field(npts, nsl2, m, 0.2, 302)
+    if kind == "div":
+        V2[:, 0, 0] += 4.0
+    pad = 3 * m // 2
+    ref = R.c_oracle(kind, V1, V2, pad)
+    mc = m // P
+    for r, out in enumerate(_ranks_run(kind, V1, V2, P, pad)):
+        assert R.rel_l2(out, ref[..., r * mc:(r + 1) * mc]) <= FP64_TOL, r
