@@ -252,6 +252,20 @@ int sfnl_mhd_jvp_f64(const double *u, const double *w, const double *b, const do
 int sfnl_mhd_vjp_f64(const double *u, const double *w, const double *b, const double *cot, double *out, int64_t np,
                      int m_max, int m_max_pad, int k_batch, sfnl_stream_t stream);
 
+/* The four linearised programs on HOST arrays (same layouts and meaning; the
+ * points are copied through the device in chunks, as by the *_host entries).
+ * For operators applied from host code, e.g. a LightKrylov linear operator
+ * (sfemans_b200/fortran/nl_linop.F90) whose matvec is the JVP and whose
+ * rmatvec is the VJP. */
+int sfnl_cross_jvp_host(const double *u, const double *w, const double *tan, double *out, int64_t np, int m_max,
+                        int m_max_pad, int k_batch);
+int sfnl_cross_vjp_host(const double *u, const double *w, const double *cot, double *out, int64_t np, int m_max,
+                        int m_max_pad, int k_batch);
+int sfnl_mhd_jvp_host(const double *u, const double *w, const double *b, const double *tan, double *out, int64_t np,
+                      int m_max, int m_max_pad, int k_batch);
+int sfnl_mhd_vjp_host(const double *u, const double *w, const double *b, const double *cot, double *out, int64_t np,
+                      int m_max, int m_max_pad, int k_batch);
+
 /* ---------------------------------------------------------------------------
  * Split-precision forms: operands split into bf16 slices with a per-point
  * power-of-two scale, DFT contractions on the tcgen05 tensor cores with FP32

@@ -111,6 +111,10 @@ _SIGS = {
     "sfnl_fft_par_pack_modes": [_P, _P] + [_I] * 6,
     "sfnl_fft_par_block": [_I, _P, _P, _P] + [_I] * 4 + [_P],
     "sfnl_fft_par_unpack_modes": [_P, _P] + [_I] * 6,
+    "sfnl_cross_jvp_host": [_P] * 4 + [_L, _I, _I, _I],
+    "sfnl_cross_vjp_host": [_P] * 4 + [_L, _I, _I, _I],
+    "sfnl_mhd_jvp_host": [_P] * 5 + [_L, _I, _I, _I],
+    "sfnl_mhd_vjp_host": [_P] * 5 + [_L, _I, _I, _I],
 }
 
 

@@ -632,6 +632,58 @@ int sfnl_mhd_vjp_f64(const double *u, const double *w, const double *b, const do
   return linear_f64(3, u, w, b, cot, out, np, m_max, m_max_pad, k_batch, stream);
 }
 
+}  // extern "C"
+
+namespace sfnl {
+namespace {
+struct LinCtx {
+  int kind, m, pad, kb;
+};
+// One point chunk of a linearised program on the device copies of the host arrays.
+int run_linear_dev(std::vector<HostBuf> &b, int64_t np_chunk, void *vctx, cudaStream_t st) {
+  auto *c = static_cast<LinCtx *>(vctx);
+  const bool mhd = c->kind >= 2;
+  return linear_f64(c->kind, b[0].dev, b[1].dev, mhd ? b[2].dev : nullptr, b[mhd ? 3 : 2].dev, b[mhd ? 4 : 3].dev,
+                    np_chunk, c->m, c->pad, c->kb, reinterpret_cast<sfnl_stream_t>(st));
+}
+// The linearised programs on host arrays (point chunks through the pipelined copies of the host entries).
+int linear_host(int kind, const double *u, const double *w, const double *b, const double *x, double *out, int64_t np,
+                int m, int pad, int kb) {
+  int N = 0;
+  int rc = check_common(np, m, pad, 0, kb, &N);
+  if (rc) return rc;
+  if (np == 0) return SFNL_OK;
+  if (!u || !w || !x || !out || (kind >= 2 && !b)) return set_error(SFNL_ERR_ARG, "null array");
+  static const int xs[4] = {12, 6, 18, 12}, os[4] = {6, 12, 12, 18};
+  std::vector<HostBuf> bufs = {{u, nullptr, 6, nullptr}, {w, nullptr, 6, nullptr}};
+  if (kind >= 2) bufs.push_back({b, nullptr, 6, nullptr});
+  bufs.push_back({x, nullptr, xs[kind], nullptr, 1, m * kb});
+  bufs.push_back({nullptr, out, os[kind], nullptr, 1, m * kb});
+  LinCtx c{kind, m, pad, kb};
+  return with_device_buffers(bufs, np, m, run_linear_dev, &c, nullptr);
+}
+}  // namespace
+}  // namespace sfnl
+
+extern "C" {
+
+int sfnl_cross_jvp_host(const double *u, const double *w, const double *tan, double *out, int64_t np, int m_max,
+                        int m_max_pad, int k_batch) {
+  return linear_host(0, u, w, nullptr, tan, out, np, m_max, m_max_pad, k_batch);
+}
+int sfnl_cross_vjp_host(const double *u, const double *w, const double *cot, double *out, int64_t np, int m_max,
+                        int m_max_pad, int k_batch) {
+  return linear_host(1, u, w, nullptr, cot, out, np, m_max, m_max_pad, k_batch);
+}
+int sfnl_mhd_jvp_host(const double *u, const double *w, const double *b, const double *tan, double *out, int64_t np,
+                      int m_max, int m_max_pad, int k_batch) {
+  return linear_host(2, u, w, b, tan, out, np, m_max, m_max_pad, k_batch);
+}
+int sfnl_mhd_vjp_host(const double *u, const double *w, const double *b, const double *cot, double *out, int64_t np,
+                      int m_max, int m_max_pad, int k_batch) {
+  return linear_host(3, u, w, b, cot, out, np, m_max, m_max_pad, k_batch);
+}
+
 int sfnl_product_split(int op, const double *a, const double *b, double *out, int64_t np, int m_max, int m_max_pad,
                        int split, sfnl_stream_t stream) {
   int N = 0;

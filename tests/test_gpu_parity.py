@@ -372,3 +372,51 @@ def test_mode_distributed_block_path(kind, P, npts, m):
     mc = m // P
     for r, out in enumerate(_ranks_run(kind, V1, V2, P, pad)):
         assert R.rel_l2(out, ref[..., r * mc:(r + 1) * mc]) <= FP64_TOL, r
+
+
+def test_cross_jacobian_operator_drives_a_krylov_svd():
+    # the linearised term as a Krylov operator (matvec = JVP, rmatvec = VJP): the leading singular values
+    # that scipy's svds finds through it match those of the dense Jacobian built column by column from
+    # the oracle's bilinear products
+    from scipy.sparse.linalg import svds
+
+    from sfemans_b200.linop import CrossJacobian
+
+    npts, m = 3, 5
+    pad = 3 * m // 2
+    u = R.synthetic_field(npts, 6, m, 0.2, 71)
+    w = R.synthetic_field(npts, 6, m, 0.2, 72)
+    n_in, n_out = npts * 12 * m, npts * 6 * m
+    J = np.zeros((n_out, n_in))
+    for i in range(n_in):
+        e = np.zeros(n_in)
+        e[i] = 1.0
+        v = e.reshape((npts, 12, m), order="F")
+        col = R.cross_jvp(u, w, np.asfortranarray(v[:, :6]), np.asfortranarray(v[:, 6:]), pad)
+        J[:, i] = col.ravel(order="F")
+    ref = np.sort(np.linalg.svd(J, compute_uv=False))[::-1][:6]
+    op = CrossJacobian(dev(u), dev(w), m_max_pad=pad).as_linear_operator()
+    x = np.random.default_rng(3).standard_normal(n_in)
+    c = np.random.default_rng(4).standard_normal(n_out)
+    assert np.linalg.norm(op.matvec(x) - J @ x) <= 1e-12 * np.linalg.norm(J @ x)
+    assert np.linalg.norm(op.rmatvec(c) - J.T @ c) <= 1e-12 * np.linalg.norm(J.T @ c)
+    sv = np.sort(svds(op, k=6, tol=1e-12, random_state=0, return_singular_vectors=False))[::-1]
+    assert np.allclose(sv, ref, rtol=1e-9, atol=0.0)
+
+
+@pytest.mark.parametrize("kind,k", [("cross_jvp", 3), ("cross_vjp", 2), ("mhd_jvp", 2), ("mhd_vjp", 1)])
+def test_linearised_host_entries(kind, k):
+    # the host-array forms of the linearised programs equal the device forms
+    import ctypes
+
+    npts, m, pad = 517, 12, 18
+    nin, nout = {"cross_jvp": (12, 6), "cross_vjp": (6, 12), "mhd_jvp": (18, 12), "mhd_vjp": (12, 18)}[kind]
+    nb = 3 if kind.startswith("mhd") else 2
+    base = [R.synthetic_field(npts, 6, m, 0.2, 80 + i) for i in range(nb)]
+    x = np.asfortranarray(np.stack([R.synthetic_field(npts, nin, m, 0.2, 90 + t) for t in range(k)], axis=-1))
+    out = np.zeros((npts, nout, m, k), order="F")
+    P = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+    rc = getattr(sf.lib(), f"sfnl_{kind}_host")(*[P(b) for b in base], P(x), P(out), npts, m, pad, k)
+    assert rc == 0, sf.last_error()
+    ref = host(getattr(sf, kind)(*[dev(b) for b in base], dev(x), m_max_pad=pad))
+    assert R.rel_l2(out, ref) <= FP64_TOL
