@@ -972,19 +972,35 @@ static int gauss_product(int kind, const double *v, const double *v2, const doub
   // The curl callers at m = 64: node-major copies of the nodal fields (NF x np_nodes x 6 x nmod doubles),
   // then one kernel that builds the operands in the product's staging.  A caller's work buffer
   // (12*l_G*me*nmod doubles) holds the copies when NF*np_nodes <= 2*l_G*me (P2 meshes: about 4 me <= 14 me).
+  // The advection callers likewise: node-major copies of the velocity and of the scalar (8 x np_nodes x nmod
+  // doubles, within a caller's 12*l_G*me*nmod work buffer when 8*np_nodes <= 12*l_G*me).
   const int nf = 1 + (kind == GK_LORENTZ || (kind == GK_NS && omega) ? 1 : 0);
   const size_t nodal = (size_t)np_nodes * 6 * nmod;
-  const bool fused = kind != GK_ADVECT && gauss_cross_fused_supported(nmod, n_w) && dealiased(nmod, N) &&
-                     (!work || (size_t)nf * np_nodes <= (size_t)2 * ng);
+  const size_t fused_doubles = kind == GK_ADVECT ? (size_t)np_nodes * 8 * nmod : nf * nodal;
+  const bool fused = gauss_cross_fused_supported(nmod, n_w) && dealiased(nmod, N) &&
+                     (!work || fused_doubles <= gauss_operand_doubles(kind, conservative, ng, nmod));
   std::unique_lock<std::mutex> lk;
   double *wk = work;
   if (!wk) {
     DevState *s = dev_state();
     if (!s) return set_error(SFNL_ERR_CUDA, "no current device");
     lk = std::unique_lock<std::mutex>(s->mu);
-    const size_t need = fused ? nf * nodal : gauss_operand_doubles(kind, conservative, ng, nmod);
+    const size_t need = fused ? fused_doubles : gauss_operand_doubles(kind, conservative, ng, nmod);
     if ((rc = grow_gwork(s, need * sizeof(double)))) return rc;
     wk = reinterpret_cast<double *>(s->gwork);
+  }
+  if (fused && kind == GK_ADVECT) {
+    double *vt = wk, *ct = wk + nodal;
+    if ((rc = launch_nodal_transpose(v, vt, np_nodes, nmod, st))) return rc;
+    if ((rc = launch_nodal_transpose(v2, ct, np_nodes, nmod, st, 2))) return rc;
+    GaussArgs ga{vt, nullptr, ww, dw, rr, jj, list_mode, np_nodes, me, n_w, l_G, nmod, ct, heat};
+    if ((rc = launch_gauss_advect_fused(ga, conservative != 0, out, ng, nmod, st))) return rc;
+    if (g_check_finite) {
+      ProgArgs pa;
+      if ((rc = build_product(OP_PROD, out, out, out, ng, nmod, N, &pa))) return rc;
+      rc = scan_outputs(pa, st);
+    }
+    return rc;
   }
   if (fused) {
     double *vt = wk, *xt = wk + nodal;

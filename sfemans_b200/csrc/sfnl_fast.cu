@@ -1001,6 +1001,123 @@ __global__ void __launch_bounds__(384, 2) gauss_tf_cross_kernel(const FastArgs a
   tf_analysis<M, NO>(ps, a.ana, os, p0, a.np, a.out_ps, false);
 }
 
+// The advection callers with their operands built in the staging (third fold, M = 64, P2 elements):
+// smb_ugradc_gauss_fft_par (subroutine_level_set.F90:434-534) and the temperature and concentration
+// versions (subroutine_temperature_with_T.F90:247-350, subroutine_concentration.F90:243-341).  Fields 0-2:
+// Gradc = heat grad c, 3-5: W = u, and for the conservative form 6: Div = div u, 7: Cgauss = heat c; the
+// program Gradc . W (+ Div Cgauss) is evaluated on the grid and analysed once.  ga.v is the node-major
+// velocity (np_nodes, 6, nmod), ga.v2 the node-major scalar (np_nodes, 2, nmod), ga.heat the element's heat
+// capacity or null.
+template <int M, bool CONS>
+__global__ void __launch_bounds__(384, 2) gauss_tf_advect_kernel(const FastArgs a, const GaussArgs ga) {
+  static_assert(third_fold(M), "third fold needs the specialised geometry");
+  constexpr int NI = CONS ? 8 : 6, NT = TfGeo<M>::NT, KS_tot = TfGeo<M>::KS_tot;
+  constexpr size_t fstride = (size_t)KS_tot * 32;
+  extern __shared__ double smem[];
+  const int64_t p0 = (int64_t)blockIdx.x * 8;
+  constexpr size_t prod_d = (size_t)1 * 4 * NT * 2 * 32;
+  double *ps = smem, *xc = smem + prod_d, *xs = smem;  // ps and xc overlay xs after the synthesis
+  constexpr int NW = 6;  // P2 elements
+  __shared__ int s_node[8][NW];
+  __shared__ double s_wt[8][NW], s_g1[8][NW], s_g2[8][NW], s_ray[8], s_heat[8];
+  for (int t = threadIdx.x; t < NI * (int)fstride; t += blockDim.x) xs[t] = 0.0;  // padding rows, sine of mode 0
+  if (threadIdx.x < 8 * NW) {  // the points' nodes, basis values and derivatives (mesh%jj, ww, dw)
+    const int g = threadIdx.x / NW, n = threadIdx.x % NW;
+    const int64_t p = p0 + g < a.np ? p0 + g : a.np - 1;
+    const int me = (int)(p / ga.l_G), l = (int)(p % ga.l_G);
+    int node = ga.jj[n + (size_t)NW * me] - 1;
+    node = node < 0 ? 0 : node >= ga.np_nodes ? ga.np_nodes - 1 : node;  // no access outside the fields
+    s_node[g][n] = node;
+    s_wt[g][n] = ga.ww[n + (size_t)NW * l];
+    const double *dwl = ga.dw + (size_t)2 * NW * (l + (size_t)ga.l_G * me);
+    s_g1[g][n] = dwl[2 * n];
+    s_g2[g][n] = dwl[2 * n + 1];
+    if (n == 0) s_heat[g] = ga.heat ? ga.heat[me] : 1.0;  // heat_capa_in(m), temperature version
+  }
+  __syncthreads();
+  if (threadIdx.x < 8) {  // radius of the point: sum rr(1, nodes) ww
+    double ray = 0.0;
+#pragma unroll
+    for (int n = 0; n < NW; ++n) ray = fma(ga.rr[2 * (size_t)s_node[threadIdx.x][n]], s_wt[threadIdx.x][n], ray);
+    s_ray[threadIdx.x] = ray;
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < 8 * M; it += blockDim.x) {
+    const int i = it % M, g = it / M;  // mode index, point of the tile: a warp reads 32 modes of a node
+    if (p0 + g >= a.np) continue;
+    double wv[6] = {0, 0, 0, 0, 0, 0}, d1[6] = {0, 0, 0, 0, 0, 0}, d2[6] = {0, 0, 0, 0, 0, 0};
+    double cw[2] = {0, 0}, c1[2] = {0, 0}, c2[2] = {0, 0};
+#pragma unroll
+    for (int n = 0; n < NW; ++n) {
+      const double wt = s_wt[g][n], g1 = s_g1[g][n], g2 = s_g2[g][n];
+      const double *vn = ga.v + (size_t)s_node[g][n] * 6 * M + i;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const double vs = vn[(size_t)k * M];
+        wv[k] = fma(vs, wt, wv[k]);
+        d1[k] = fma(vs, g1, d1[k]);
+        d2[k] = fma(vs, g2, d2[k]);
+      }
+      const double *cn = ga.v2 + (size_t)s_node[g][n] * 2 * M + i;
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const double cs = cn[(size_t)k * M];
+        cw[k] = fma(cs, wt, cw[k]);
+        c1[k] = fma(cs, g1, c1[k]);
+        c2[k] = fma(cs, g2, c2[k]);
+      }
+    }
+    // the cylindrical gradient of the scalar's mode and the divergence of the velocity's mode
+    // (subroutine_temperature_with_T.F90:300-331, subroutine_level_set.F90:470-500)
+    const double ray = s_ray[g], hc = s_heat[g], mr = (double)ga.list_mode[i] / ray;
+    double f[NI][2];
+    f[0][0] = hc * c1[0];
+    f[0][1] = hc * c1[1];
+    f[1][0] = hc * (mr * cw[1]);
+    f[1][1] = hc * (-mr * cw[0]);
+    f[2][0] = hc * c2[0];
+    f[2][1] = hc * c2[1];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      f[3 + k][0] = wv[2 * k];
+      f[3 + k][1] = wv[2 * k + 1];
+    }
+    if constexpr (CONS) {
+      f[6][0] = d1[0] + wv[0] / ray + mr * wv[3] + d2[4];
+      f[6][1] = d1[1] + wv[1] / ray - mr * wv[2] + d2[5];
+      f[7][0] = hc * cw[0];
+      f[7][1] = hc * cw[1];
+    }
+    // rows of mode i: cosine group CE0 (i = 0 mod 4), CE2 (i = 2 mod 4) or CO (odd), sine group 3 further
+    const int gc = (i & 1) ? 2 : (i & 3) == 0 ? 0 : 1, k = (i & 1) ? i >> 1 : i >> 2;
+    const int rc = 4 * tf_koff(M, gc) + k, rs = 4 * tf_koff(M, gc + 3) + k;
+    const int oc = (rc >> 2) * 32 + a_frag_slot(rc & 3, g), os = (rs >> 2) * 32 + a_frag_slot(rs & 3, g);
+#pragma unroll
+    for (int fi = 0; fi < NI; ++fi) {
+      xs[fi * fstride + oc] = f[fi][0];
+      if (i != 0) xs[fi * fstride + os] = f[fi][1];  // the sine of mode 0 is ignored
+    }
+  }
+  __syncthreads();
+  double acc_e[NI][2], acc_o[NI][2];
+  tf_synth<M, NI, 0u>(xs, a.syn, acc_e, acc_o);
+  __syncthreads();  // every warp has read its last coefficient: xc and ps may overwrite xs
+  double v[4][NI];
+  tf_fold<M, NI>(acc_e, acc_o, xc, v);
+  double gq[4][1];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    gq[r][0] = v[r][0] * v[r][3] + v[r][1] * v[r][4] + v[r][2] * v[r][5];
+    if constexpr (CONS) gq[r][0] = fma(v[r][6], v[r][7], gq[r][0]);
+  }
+  tf_prefold<M, 1>(gq, ps, 0);
+  __syncthreads();
+  OutSet<1> os1;
+  os1.p[0] = a.out[0];
+  os1.ldm[0] = a.out_ldm[0];
+  tf_analysis<M, 1>(ps, a.ana, os1, p0, a.np, 1, false);
+}
+
 // The MHD bundle (u x w, u x b, j x b, u . gradT) in one launch with the third fold (M = 64): the five
 // vector operands are staged and synthesised one at a time (u, w, gradT, b, j), so u and b are
 // transformed once instead of three and two times (15 field transforms instead of 24); u's and b's
@@ -1231,6 +1348,37 @@ bool fast_fused_fits(int op, int m) {
 int fast_grid_length(int m) { return make_geo(m).N; }
 
 bool gauss_cross_fused_supported(int m, int n_w) { return third_fold(64) && m == 64 && n_w == 6; }
+
+int launch_gauss_advect_fused(const GaussArgs &ga, bool conservative, double *out, int64_t ng, int m,
+                              cudaStream_t st) {
+  constexpr int M = 64;
+  if (m != M) return set_error(SFNL_ERR_UNSUPPORTED, "fused Gauss-point advection: m = 64 only");
+  if (ng == 0) return SFNL_OK;
+  const Geo g = make_geo(M);
+  Tables T;
+  if (int rc = get_tf_tables(g, &T)) return rc;
+  FastArgs fa;
+  std::memset(&fa, 0, sizeof(fa));
+  fa.out[0] = out;  // c_out(l_G*me, 2, m)
+  fa.out_ldm[0] = 2 * ng;
+  fa.out_ps = 1;
+  fa.np = ng;
+  fa.m = M;
+  fa.N = g.N;
+  fa.NT = g.NT;
+  fa.syn = T.syn;
+  fa.ana = T.ana;  // variant 0: with the analysis weights
+  const int ni = conservative ? 8 : 6;
+  const size_t xs = sizeof(double) * (size_t)ni * g.KS_tot * 32;
+  const size_t ovl = sizeof(double) * ((size_t)4 * g.NT * 2 * 32 + (size_t)2 * g.NT * ni * 64);
+  const size_t smem = xs > ovl ? xs : ovl;
+  auto kern = conservative ? gauss_tf_advect_kernel<M, true> : gauss_tf_advect_kernel<M, false>;
+  if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (fused Gauss-point advection)");
+  const int64_t tiles = (ng + 7) / 8;
+  kern<<<(unsigned)tiles, 384, smem, st>>>(fa, ga);
+  return check_launch("fused Gauss-point advection");
+}
 
 int launch_gauss_cross_fused(const GaussArgs &ga, int kind, double *out, int64_t ng, int m, cudaStream_t st) {
   constexpr int M = 64;

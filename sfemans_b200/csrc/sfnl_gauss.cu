@@ -88,10 +88,10 @@ __global__ void __launch_bounds__(256) gauss_eval_kernel(GaussArgs a, double *o0
   }
 }
 
-// vt[node][k][i] = v[node + np_nodes*(k + 6 i)]: 32 modes x 32 nodes per CTA through shared memory, both
+// vt[node][k][i] = v[node + np_nodes*(k + nslot i)]: 32 modes x 32 nodes per CTA through shared memory, both
 // sides coalesced.
 __global__ void __launch_bounds__(256) nodal_transpose_kernel(const double *__restrict__ v, double *__restrict__ vt,
-                                                              int np_nodes, int m) {
+                                                              int np_nodes, int m, int nslot) {
   __shared__ double t[32][33];
   const int64_t node0 = (int64_t)blockIdx.x * 32;
   const int k = blockIdx.y, i0 = blockIdx.z * 32;
@@ -99,22 +99,22 @@ __global__ void __launch_bounds__(256) nodal_transpose_kernel(const double *__re
   for (int r = ty; r < 32; r += 8) {
     const int i = i0 + r;
     const int64_t node = node0 + tx;
-    if (i < m && node < np_nodes) t[r][tx] = v[node + (int64_t)np_nodes * (k + 6 * (int64_t)i)];
+    if (i < m && node < np_nodes) t[r][tx] = v[node + (int64_t)np_nodes * (k + nslot * (int64_t)i)];
   }
   __syncthreads();
   for (int r = ty; r < 32; r += 8) {
     const int64_t node = node0 + r;
     const int i = i0 + tx;
-    if (i < m && node < np_nodes) vt[node * 6 * m + (int64_t)k * m + i] = t[tx][r];
+    if (i < m && node < np_nodes) vt[node * nslot * m + (int64_t)k * m + i] = t[tx][r];
   }
 }
 
 }  // namespace
 
-int launch_nodal_transpose(const double *v, double *vt, int np_nodes, int m, cudaStream_t st) {
+int launch_nodal_transpose(const double *v, double *vt, int np_nodes, int m, cudaStream_t st, int nslot) {
   if (np_nodes == 0) return SFNL_OK;
-  dim3 grid((unsigned)((np_nodes + 31) / 32), 6, (unsigned)((m + 31) / 32));
-  nodal_transpose_kernel<<<grid, 256, 0, st>>>(v, vt, np_nodes, m);
+  dim3 grid((unsigned)((np_nodes + 31) / 32), (unsigned)nslot, (unsigned)((m + 31) / 32));
+  nodal_transpose_kernel<<<grid, 256, 0, st>>>(v, vt, np_nodes, m, nslot);
   return check_launch("nodal transpose");
 }
 

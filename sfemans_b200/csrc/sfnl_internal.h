@@ -52,14 +52,18 @@ struct GaussArgs {
 // o1 = v2 (6 slots); GK_ADVECT o0 = Gradc, o1 = W (6 slots), o2 = Div, o3 = Cgauss (2 slots; both
 // null: no conservative term).
 int launch_gauss_eval(const GaussArgs &a, int kind, double *o0, double *o1, double *o2, double *o3, cudaStream_t st);
-// Node-major copy of a nodal field (sfnl_gauss.cu): vt (np_nodes, 6, m) with vt[node*6m + k*m + i] =
-// v[node + np_nodes*(k + 6 i)].
-int launch_nodal_transpose(const double *v, double *vt, int np_nodes, int m, cudaStream_t st);
+// Node-major copy of a nodal field (sfnl_gauss.cu): vt (np_nodes, nslot, m) with vt[node*nslot*m + k*m + i] =
+// v[node + np_nodes*(k + nslot i)].
+int launch_nodal_transpose(const double *v, double *vt, int np_nodes, int m, cudaStream_t st, int nslot = 6);
 // The curl callers (GK_NS, GK_LORENTZ) in one kernel with the FAST cross product (sfnl_fast.cu): the
 // operands are built in the product kernel's staging from node-major nodal fields (ga.v, ga.v2,
 // ga.omega as written by launch_nodal_transpose); out (l_G*me, 6, m).  m = 64 and P2 elements (n_w = 6) only.
 bool gauss_cross_fused_supported(int m, int n_w);
 int launch_gauss_cross_fused(const GaussArgs &ga, int kind, double *out, int64_t ng, int m, cudaStream_t st);
+// The advection callers (GK_ADVECT) the same way: ga.v the node-major velocity (np_nodes, 6, m), ga.v2 the
+// node-major scalar (np_nodes, 2, m), ga.heat per element or null; out (l_G*me, 2, m).  m = 64, n_w = 6.
+int launch_gauss_advect_fused(const GaussArgs &ga, bool conservative, double *out, int64_t ng, int m,
+                              cudaStream_t st);
 
 // Elementary programs: cross (6 -> 3), dot (6 -> 1), product (2 -> 1),
 // scalar x vector (4 -> 3) and tensor (6 -> 9).  Every bilinear program of

@@ -118,6 +118,29 @@ def test_advection_device_entry_matches_oracle(variant, nr, nz, m, modes):
 
 
 @pytest.mark.parametrize("variant", list(VARIANTS))
+@pytest.mark.parametrize("modes,own_work", [(None, True), ("sparse", False), ("sparse", True)])
+def test_advection_fused_m64(variant, modes, own_work):
+    # m = 64 on P2 elements: the operands are built inside the product kernel (node-major copies of the
+    # velocity and the scalar in the caller's work buffer or the library's), select_mode-like mode lists
+    cons, heat_on = VARIANTS[variant]
+    m = 64
+    mesh = R.synthetic_p2_mesh(7, 4, 14)
+    lm = list(range(m)) if modes is None else [3 * i + (i % 2) for i in range(m)]
+    V = R.synthetic_field(mesh["np"], 6, m, 0.1, 151)
+    C = R.synthetic_field(mesh["np"], 2, m, 0.1, 152)
+    heat = _heat(mesh, heat_on)
+    ref = R.c_ugradc_gauss(V, C, mesh, lm, heat=heat, conservative=cons)[0]
+    nwork = (16 if cons else 12) * 7 * mesh["me"] * m
+    work = torch.full((nwork,), float("nan"), device="cuda", dtype=torch.float64) if own_work else None
+    out = sf.ugradc_gauss(sf.to_device(V), sf.to_device(C), _dev_mesh(mesh),
+                          torch.tensor(lm, dtype=torch.int32, device="cuda"),
+                          heat=None if heat is None else torch.tensor(heat, device="cuda"), conservative=cons,
+                          work=work)
+    torch.cuda.synchronize()
+    assert R.rel_l2(sf.to_host(out), ref) <= FP64_TOL
+
+
+@pytest.mark.parametrize("variant", list(VARIANTS))
 def test_advection_reference_signatures_on_host_arrays(variant):
     cons, heat_on = VARIANTS[variant]
     mesh = R.synthetic_p2_mesh(7, 6, 11)
