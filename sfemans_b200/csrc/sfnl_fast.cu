@@ -1373,7 +1373,8 @@ int launch_gauss_advect_fused(const GaussArgs &ga, bool conservative, double *ou
   const size_t ovl = sizeof(double) * ((size_t)4 * g.NT * 2 * 32 + (size_t)2 * g.NT * ni * 64);
   const size_t smem = xs > ovl ? xs : ovl;
   auto kern = conservative ? gauss_tf_advect_kernel<M, true> : gauss_tf_advect_kernel<M, false>;
-  if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+  // opt in whatever the size: the kernel's static shared memory counts against the 48 KB default too
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (fused Gauss-point advection)");
   const int64_t tiles = (ng + 7) / 8;
   kern<<<(unsigned)tiles, 384, smem, st>>>(fa, ga);
@@ -1403,7 +1404,7 @@ int launch_gauss_cross_fused(const GaussArgs &ga, int kind, double *out, int64_t
   const size_t smem = fast_smem_bytes(EK_CROSS, g.NT, 4 * g.KS_tot, true);
   auto kern = kind == GK_NS ? gauss_tf_cross_kernel<M, GK_NS> : gauss_tf_cross_kernel<M, GK_LORENTZ>;
   if (kind != GK_NS && kind != GK_LORENTZ) return set_error(SFNL_ERR_ARG, "fused Gauss-point cross product: curl callers only");
-  if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)  // static smem too
     return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (fused Gauss-point cross product)");
   const int64_t tiles = (ng + 7) / 8;
   kern<<<(unsigned)tiles, 384, smem, st>>>(fa, ga);

@@ -68,8 +68,8 @@ class CrossJacobian:
             t = torch.from_numpy(np.ascontiguousarray(a.T)).to(dev)
             return t.permute(2, 1, 0)
 
-        def to_flat(t):
-            return t.permute(2, 1, 0).contiguous().cpu().numpy().ravel()  # Fortran order of (np, nslot, m)
+        def to_flat(t):  # Fortran order of (np, nslot, m[, 1])
+            return t.permute(*reversed(range(t.dim()))).contiguous().cpu().numpy().ravel()
 
         def mv(v):
             return to_flat(self.matvec(to_dev(v, 12)))

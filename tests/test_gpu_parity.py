@@ -420,3 +420,56 @@ def test_linearised_host_entries(kind, k):
     assert rc == 0, sf.last_error()
     ref = host(getattr(sf, kind)(*[dev(b) for b in base], dev(x), m_max_pad=pad))
     assert R.rel_l2(out, ref) <= FP64_TOL
+
+
+def test_mhd_linearised_k16_m256_against_the_port():
+    # the 16-tangent linearised pair (u x w, u x b) at m = 256 (two-kernel large-m form), every tangent
+    # against the C restatement (itself pinned to the long-double oracle), and the adjoint identity
+    npts, m, k = 96, 256, 16
+    pad = 3 * m // 2
+    u, w, b = (R.synthetic_field(npts, 6, m, 0.2, 400 + i) for i in range(3))
+    tan = np.asfortranarray(np.stack([R.synthetic_field(npts, 18, m, 0.2, 410 + t) for t in range(k)], axis=-1))
+    cot = np.asfortranarray(np.stack([R.synthetic_field(npts, 12, m, 0.2, 430 + t) for t in range(k)], axis=-1))
+    U, W, B = dev(u), dev(w), dev(b)
+    jv = host(sf.mhd_jvp(U, W, B, dev(tan), m_max_pad=pad))
+    jt = host(sf.mhd_vjp(U, W, B, dev(cot), m_max_pad=pad))
+    c = lambda x, y: R.cpu_product("cross", np.asfortranarray(x), np.asfortranarray(y), pad, n_theta=2 * pad)  # noqa: E731
+    for t in range(k):
+        du, dw, db = tan[:, 0:6, :, t], tan[:, 6:12, :, t], tan[:, 12:18, :, t]
+        ref = np.concatenate([c(du, w) + c(u, dw), c(du, b) + c(u, db)], axis=1)
+        assert R.rel_l2(jv[..., t], ref) <= FP64_TOL, t
+    lhs, rhs = float(np.sum(jv * cot)), float(np.sum(tan * jt))
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+def test_linearised_700k_points_full_size():
+    # the linearised cross product at its configuration's size (700k points, m = 32): central differences
+    # of the FP64 product at h = 1e-6 and the adjoint identity, both on the device over every point
+    import torch
+
+    npts, m, pad, h = 700_000, 32, 48, 1e-6
+
+    def field(nslot, seed):
+        g = torch.Generator(device="cuda")
+        g.manual_seed(seed)
+        t = torch.randn((m, nslot, npts), generator=g, device="cuda", dtype=torch.float64)
+        t *= torch.exp(-0.2 * torch.arange(m, device="cuda", dtype=torch.float64))[:, None, None]
+        t[0, 1::2, :] = 0.0
+        return t.permute(2, 1, 0)
+
+    u, w, tan, cot = field(6, 1), field(6, 2), field(12, 3), field(6, 4)
+    jv = sf.cross_jvp(u, w, tan, m_max_pad=pad)[..., 0]
+    jt = sf.cross_vjp(u, w, cot, m_max_pad=pad)[..., 0]
+
+    def fortran(t):
+        o = sf.fortran_empty(*t.shape)
+        o.copy_(t)
+        return o
+
+    du, dw = tan[:, 0:6, :], tan[:, 6:12, :]
+    plus = sf.product(sf.OP_CROSS, fortran(u + h * du), fortran(w + h * dw), m_max_pad=pad)
+    minus = sf.product(sf.OP_CROSS, fortran(u - h * du), fortran(w - h * dw), m_max_pad=pad)
+    fd = (plus - minus) / (2 * h)
+    assert float(torch.linalg.vector_norm(fd - jv) / torch.linalg.vector_norm(jv)) <= 1e-8
+    lhs, rhs = float(torch.sum(jv * cot)), float(torch.sum(tan * jt))
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
