@@ -237,7 +237,11 @@ int sfnl_gauss_operands_f64(int kind, const double *v, const double *v2, const d
  *   VJP  cot (np, 6, m, k) -> out (np, 12, m, k) = J^T cot, the transpose for the
  *        plain Euclidean inner product of the coefficient arrays, so that
  *        <J v, c> = <v, J^T c> exactly in exact arithmetic.
- * u, w: (np, 6, m) shared by all k_batch tangents.
+ * u, w: (np, 6, m) shared by all k_batch tangents.  Beyond m = 96 (the
+ * two-kernel form) the base state is synthesised once per point chunk and the
+ * tangents in one launch per chunk; the grid-value workspace then grows to
+ * hold every tangent of a chunk of at least 4096 points, up to 8 GiB or a
+ * quarter of the free device memory (kept until sfnl_finalize).
  * ------------------------------------------------------------------------- */
 int sfnl_cross_jvp_f64(const double *u, const double *w, const double *tan, double *out, int64_t np, int m_max,
                        int m_max_pad, int k_batch, sfnl_stream_t stream);

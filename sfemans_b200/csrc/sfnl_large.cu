@@ -54,7 +54,9 @@ struct LargeArgs {
   int NT, NU_tot, KS_tot;
   int ks_off[4], KS[4], nu_off[4], ke[4];
   unsigned adj_in;  // bit f: field f is a cotangent
-  int adj_out, vec16, batch_entry;
+  int adj_out, vec16, batch_entry;  // batch entry of blockIdx.z == 0 (synthesis) / blockIdx.y == 0 (program)
+  int nown;                          // workspace slots per batch entry (the batched fields)
+  int nbl;                           // batch entries per launch (gridDim.z of the synthesis, gridDim.y of the program)
   const double *syn, *ana;
   double *G;
   int64_t tiles;
@@ -74,7 +76,9 @@ __global__ void __launch_bounds__(kLargeSynMaxWarps * 32) large_syn_kernel(const
   const int64_t tile0 = (int64_t)blockIdx.x * PT, p0 = tile0 * 8;
   const int NT = a.NT, KT = 4 * a.KS_tot;
   const size_t pts = (size_t)a.KS_tot * 32;  // point-tile stride in xs
-  const double *in_f = a.in[f] + (int64_t)a.batch_entry * a.in_bs[f];
+  const int bz = blockIdx.z;  // entries a.batch_entry + bz (batched fields only; 0 for the shared ones)
+  const double *in_f = a.in[f] + (int64_t)(a.batch_entry + bz) * a.in_bs[f];
+  const int64_t gslot_f = a.gslot[f] + (a.in_bs[f] ? (int64_t)bz * a.nown : 0);
   const int64_t ldm = a.in_ldm[f];
   int KS[4], KOFF[4], KE[4];
 #pragma unroll
@@ -150,7 +154,7 @@ __global__ void __launch_bounds__(kLargeSynMaxWarps * 32) large_syn_kernel(const
     for (int pt = 0; pt < PT; ++pt) {
       const int64_t tile = tile0 + pt;
       if (tile >= a.tiles) break;
-      double *gp0 = a.G + ((a.gslot[f] * a.tiles + tile) * NT + t) * 256 + lane;
+      double *gp0 = a.G + ((gslot_f * a.tiles + tile) * NT + t) * 256 + lane;
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const double A = acc[pt][0][e] + acc[pt][1][e], B = acc[pt][0][e] - acc[pt][1][e];
@@ -179,7 +183,9 @@ __global__ void __launch_bounds__(kLargeSynMaxWarps * 32, 1) large_syn_tf_kernel
   const int64_t tile0 = (int64_t)blockIdx.x * PT, p0 = tile0 * 8;
   const int NT = a.NT, NH = NT >> 1, KS_tot = a.tkoff[6], KT = 4 * KS_tot;
   const size_t pts = (size_t)KS_tot * 32;
-  const double *in_f = a.in[f] + (int64_t)a.batch_entry * a.in_bs[f];
+  const int bz = blockIdx.z;  // entries a.batch_entry + bz (batched fields only; 0 for the shared ones)
+  const double *in_f = a.in[f] + (int64_t)(a.batch_entry + bz) * a.in_bs[f];
+  const int64_t gslot_f = a.gslot[f] + (a.in_bs[f] ? (int64_t)bz * a.nown : 0);
   const int64_t ldm = a.in_ldm[f];
   {  // stage: 4*PT threads per row, two points each
     constexpr int tpr = 4 * PT;
@@ -281,7 +287,7 @@ __global__ void __launch_bounds__(kLargeSynMaxWarps * 32, 1) large_syn_tf_kernel
       for (int pt = 0; pt < PT; ++pt) {
         const int64_t tile = tile0 + pt;
         if (tile >= a.tiles) break;
-        double *gp0 = a.G + ((a.gslot[f] * a.tiles + tile) * NT + t) * 256 + lane;
+        double *gp0 = a.G + ((gslot_f * a.tiles + tile) * NT + t) * 256 + lane;
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
           const double CE = ce[side][pt][e], SE = se[side][pt][e], CO = od[0][pt][e], SO = od[1][pt][e];
@@ -307,7 +313,7 @@ __global__ void __launch_bounds__(kLargeProdWarps * 32) large_prod_tf_kernel(con
   constexpr int KP = kLargeTfPairs, LT = 2 * KP;  // pairs per chunk, local tiles
   extern __shared__ double pc_s[];  // [NOG][4 classes][LT local tiles][2][32]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, q = lane & 3;
-  const int b = a.batch_entry;
+  const int by = blockIdx.y, b = a.batch_entry + by;  // batch entry of this CTA
   const int64_t tile = blockIdx.x, p = tile * 8 + (lane >> 2);
   const int NT = a.NT, NH = NT >> 1;
   double y[CPW][NOG][2];
@@ -332,7 +338,8 @@ __global__ void __launch_bounds__(kLargeProdWarps * 32) large_prod_tf_kernel(con
       for (int r = 0; r < 4; ++r) {
         double x[NI], yy[NO];
 #pragma unroll
-        for (int f = 0; f < NI; ++f) x[f] = Gl[a.gslot[f] * fstride + (size_t)t * 256 + r * 64 + e * 32];
+        for (int f = 0; f < NI; ++f)
+          x[f] = Gl[(a.gslot[f] + (a.in_bs[f] ? (int64_t)by * a.nown : 0)) * fstride + (size_t)t * 256 + r * 64 + e * 32];
         apply_op<OP>(x, yy);
 #pragma unroll
         for (int o = 0; o < NOG; ++o) gq[r][o] = yy[O0 + o];
@@ -428,7 +435,7 @@ __global__ void __launch_bounds__(kLargeProdWarps * 32) large_prod_kernel(const 
   constexpr int NOG = NO - O0 < kLargeGroup ? NO - O0 : kLargeGroup;
   extern __shared__ double pc_s[];  // [NOG][4][LCT][2][32]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, q = lane & 3;
-  const int b = a.batch_entry;
+  const int by = blockIdx.y, b = a.batch_entry + by;  // batch entry of this CTA
   const int64_t tile = blockIdx.x, p = tile * 8 + (lane >> 2);
   const int NT = a.NT;
   double y[CPW][NOG][2];
@@ -450,7 +457,8 @@ __global__ void __launch_bounds__(kLargeProdWarps * 32) large_prod_kernel(const 
       for (int r = 0; r < 4; ++r) {
         double x[NI], yy[NO];
 #pragma unroll
-        for (int f = 0; f < NI; ++f) x[f] = Gl[a.gslot[f] * fstride + (size_t)t * 256 + r * 64 + e * 32];
+        for (int f = 0; f < NI; ++f)
+          x[f] = Gl[(a.gslot[f] + (a.in_bs[f] ? (int64_t)by * a.nown : 0)) * fstride + (size_t)t * 256 + r * 64 + e * 32];
         apply_op<OP>(x, yy);
 #pragma unroll
         for (int o = 0; o < NOG; ++o) gq[r][o] = yy[O0 + o];
@@ -539,7 +547,7 @@ int launch_large_prod(const LargeArgs &la, bool tf, cudaStream_t st) {
   auto kern = tf ? large_prod_tf_kernel<OP, O0, CPW> : large_prod_kernel<OP, O0, CPW>;
   if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (large-m program and analysis)");
-  kern<<<(unsigned)la.tiles, kLargeProdWarps * 32, smem, st>>>(la);
+  kern<<<dim3((unsigned)la.tiles, (unsigned)la.nbl), kLargeProdWarps * 32, smem, st>>>(la);
   return check_launch("large-m program and analysis");
 }
 
@@ -591,7 +599,8 @@ int launch_large_prod_op(int op, const LargeArgs &la, bool tf, cudaStream_t st) 
   return set_error(SFNL_ERR_ARG, "large-m FAST form: program not bilinear");
 }
 
-int launch_large_syn(const LargeArgs &la, int nfields, bool tf, cudaStream_t st) {
+// nbz: batch entries (blockIdx.z) of the launch, 1 for the batch-invariant fields.
+int launch_large_syn(const LargeArgs &la, int nfields, int nbz, bool tf, cudaStream_t st) {
   if (nfields == 0) return SFNL_OK;
   // angle tiles (pairs of mirror tiles with the third fold) spread evenly over at most kLargeSynMaxWarps warps
   const int units = tf ? la.NT / 2 : la.NT;
@@ -602,7 +611,7 @@ int launch_large_syn(const LargeArgs &la, int nfields, bool tf, cudaStream_t st)
     if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
       return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (large-m synthesis)");
     const int64_t blocks = (la.tiles + pt - 1) / pt;
-    kern<<<dim3((unsigned)blocks, (unsigned)nfields), nw * 32, smem, st>>>(la);
+    kern<<<dim3((unsigned)blocks, (unsigned)nfields, (unsigned)nbz), nw * 32, smem, st>>>(la);
     return check_launch("large-m synthesis");
   };
   if (tf) {
@@ -616,6 +625,10 @@ int launch_large_syn(const LargeArgs &la, int nfields, bool tf, cudaStream_t st)
 }
 
 constexpr size_t kLargeWorkspaceBytes = size_t(1) << 30;  // grid values of one point chunk
+// Batched programs (tangents): the workspace may grow to this, or to a quarter of the free device memory,
+// so that one launch serves every batch entry of a point chunk of at least kLargeMinChunk points.
+constexpr size_t kLargeBatchWorkspaceBytes = size_t(8) << 30;
+constexpr int64_t kLargeMinChunk = 4096;
 
 }  // namespace
 
@@ -632,8 +645,11 @@ void large_release_workspaces() {
   cudaSetDevice(prev);
 }
 
-// The two-kernel form: per point chunk, the batch-invariant fields (base state) once, then per batch
-// entry its own fields and the program's outputs in groups of three (one launch per group).
+// The two-kernel form: per point chunk, the batch-invariant fields (base state) once, then the batch
+// entries in groups of kb: one synthesis launch for the group's own fields (blockIdx.z = entry) and one
+// launch per group of three outputs (blockIdx.y = entry).  The grid-value workspace holds the shared
+// fields and kb entries' own fields of one point chunk: kb = the whole batch when a chunk of at least
+// kLargeMinChunk points fits the batched workspace bound, else as many entries as such a chunk allows.
 int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStream_t st) {
   const int ni = op_nin(a.op), no = op_nout(a.op);
   int nshared = 0, nown = 0;  // batch-invariant fields take the first G slots, the batched ones the next
@@ -641,8 +657,25 @@ int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStre
   for (int f = 0; f < ni; ++f) gslot[f] = a.in_bs[f] == 0 ? nshared++ : -1;
   for (int f = 0; f < ni; ++f)
     if (gslot[f] < 0) gslot[f] = nshared + nown++;
-  const size_t per_point = sizeof(double) * (size_t)(nshared + nown) * g.N;
-  int64_t chunk = (int64_t)(kLargeWorkspaceBytes / per_point);
+  const size_t field_bytes = sizeof(double) * (size_t)g.N;  // one field's grid values per point
+  size_t cap = kLargeWorkspaceBytes;
+  int kb = 1;
+  if (a.batch > 1 && nown > 0) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+      cudaGetLastError();
+      free_b = 0;
+    }
+    size_t bcap = kLargeBatchWorkspaceBytes < free_b / 4 ? kLargeBatchWorkspaceBytes : free_b / 4;
+    if (bcap < cap) bcap = cap;
+    const size_t per_entry = field_bytes * nown * (size_t)kLargeMinChunk;
+    const size_t shared_b = field_bytes * nshared * (size_t)kLargeMinChunk;
+    const int64_t fit = bcap > shared_b ? (int64_t)((bcap - shared_b) / per_entry) : 0;
+    kb = (int)(fit < 1 ? 1 : fit > a.batch ? a.batch : fit);
+    cap = bcap;
+  }
+  const size_t per_point = field_bytes * (size_t)(nshared + (int64_t)kb * nown);
+  int64_t chunk = (int64_t)(cap / per_point);
   chunk = (chunk / 32) * 32;
   if (chunk < 32) chunk = 32;
   if (chunk > a.np) chunk = ((a.np + 7) / 8) * 8;
@@ -665,6 +698,7 @@ int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStre
     la.in_sin = a.np;
     la.out_ps = a.out_ps;
     la.out_sin = a.np * a.out_ps;
+    la.nown = nown;
     int v16 = (a.np & 1) ? 0 : 1;
     for (int f = 0; f < ni; ++f) {
       la.in[f] = a.in[f] + c0;
@@ -709,13 +743,15 @@ int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStre
     for (int f = 0; f < ni; ++f)
       if (a.in_bs[f] == 0) la.syn_f[k++] = f;
     la.batch_entry = 0;
-    if (int rc = launch_large_syn(la, k, tf, st)) return rc;
-    for (int b = 0; b < a.batch; ++b) {
-      la.batch_entry = b;
+    la.nbl = 1;
+    if (int rc = launch_large_syn(la, k, 1, tf, st)) return rc;
+    for (int b0 = 0; b0 < a.batch; b0 += kb) {
+      la.batch_entry = b0;
+      la.nbl = a.batch - b0 < kb ? a.batch - b0 : kb;
       k = 0;
       for (int f = 0; f < ni; ++f)
         if (a.in_bs[f] != 0) la.syn_f[k++] = f;
-      if (int rc = launch_large_syn(la, k, tf, st)) return rc;
+      if (int rc = launch_large_syn(la, k, la.nbl, tf, st)) return rc;
       if (int rc = launch_large_prod_op(a.op, la, tf, st)) return rc;
     }
   }
