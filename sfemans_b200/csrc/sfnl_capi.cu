@@ -977,7 +977,10 @@ static int gauss_product(int kind, const double *v, const double *v2, const doub
   const int nf = 1 + (kind == GK_LORENTZ || (kind == GK_NS && omega) ? 1 : 0);
   const size_t nodal = (size_t)np_nodes * 6 * nmod;
   const size_t fused_doubles = kind == GK_ADVECT ? (size_t)np_nodes * 8 * nmod : nf * nodal;
-  const bool fused = gauss_cross_fused_supported(nmod, n_w) && dealiased(nmod, N) &&
+  // m = 64 on P2 elements: the third-fold kernels; other m up to 96 (any element): the general FAST kernel
+  const bool fused_tf = gauss_cross_fused_supported(nmod, n_w);
+  const bool fused_gen = !fused_tf && gauss_general_fused_supported(kind, conservative != 0, nmod);
+  const bool fused = (fused_tf || fused_gen) && dealiased(nmod, N) &&
                      (!work || fused_doubles <= gauss_operand_doubles(kind, conservative, ng, nmod));
   std::unique_lock<std::mutex> lk;
   double *wk = work;
@@ -994,7 +997,9 @@ static int gauss_product(int kind, const double *v, const double *v2, const doub
     if ((rc = launch_nodal_transpose(v, vt, np_nodes, nmod, st))) return rc;
     if ((rc = launch_nodal_transpose(v2, ct, np_nodes, nmod, st, 2))) return rc;
     GaussArgs ga{vt, nullptr, ww, dw, rr, jj, list_mode, np_nodes, me, n_w, l_G, nmod, ct, heat};
-    if ((rc = launch_gauss_advect_fused(ga, conservative != 0, out, ng, nmod, st))) return rc;
+    if ((rc = fused_gen ? launch_gauss_general_fused(ga, GK_ADVECT, conservative != 0, out, ng, nmod, st)
+                        : launch_gauss_advect_fused(ga, conservative != 0, out, ng, nmod, st)))
+      return rc;
     if (g_check_finite) {
       ProgArgs pa;
       if ((rc = build_product(OP_PROD, out, out, out, ng, nmod, N, &pa))) return rc;
@@ -1014,7 +1019,9 @@ static int gauss_product(int kind, const double *v, const double *v2, const doub
       omt = xt;
     }
     GaussArgs ga{vt, omt, ww, dw, rr, jj, list_mode, np_nodes, me, n_w, l_G, nmod, v2t, nullptr};
-    if ((rc = launch_gauss_cross_fused(ga, kind, out, ng, nmod, st))) return rc;
+    if ((rc = fused_gen ? launch_gauss_general_fused(ga, kind, false, out, ng, nmod, st)
+                        : launch_gauss_cross_fused(ga, kind, out, ng, nmod, st)))
+      return rc;
     if (g_check_finite) {
       ProgArgs pa;
       if ((rc = build_product(OP_CROSS, out, out, out, ng, nmod, N, &pa))) return rc;

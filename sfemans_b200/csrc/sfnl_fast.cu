@@ -210,6 +210,7 @@ struct FastArgs {
   int vec16;        // 1: every input row starts 16-byte aligned (bases aligned, np even): 16-byte copies
   int allow_tf;     // 1: the third-fold kernel may be used (it allocates its own cached tables)
   const double *syn, *ana;
+  GaussArgs ga;     // the Gauss-point staging of fast_kernel<..., GK >= 0>: node-major nodal fields (stride m)
 };
 
 
@@ -239,6 +240,13 @@ struct EKDef<EK_SVECT> {
   }
 };
 template <>
+struct EKDef<EK_ADVECT> {  // [heat grad c 0-2, u 3-5, div u 6, heat c 7] -> grad c . u + div u c
+  static constexpr int NI = 8, NO = 1;
+  __device__ static void op(const double *x, double *y) {
+    y[0] = fma(x[6], x[7], x[0] * x[3] + x[1] * x[4] + x[2] * x[5]);
+  }
+};
+template <>
 struct EKDef<EK_TENSOR> {
   static constexpr int NI = 6, NO = 9;
   __device__ static void op(const double *x, double *y) {
@@ -248,7 +256,7 @@ struct EKDef<EK_TENSOR> {
       for (int l = 0; l < 3; ++l) y[3 * k + l] = x[k] * x[3 + l];
   }
 };
-__host__ __device__ constexpr int ek_nin(int ek) { return ek == EK_PROD ? 2 : ek == EK_SVECT ? 4 : 6; }
+__host__ __device__ constexpr int ek_nin(int ek) { return ek == EK_PROD ? 2 : ek == EK_SVECT ? 4 : ek == EK_ADVECT ? 8 : 6; }
 __host__ __device__ constexpr int ek_nout(int ek) { return ek == EK_CROSS || ek == EK_SVECT ? 3 : ek == EK_TENSOR ? 9 : 1; }
 // Shared memory of one CTA: folded products [NO][4][NT][2][32] and staged coefficients [NI][KT][8].
 // With NT <= 8 angle tiles every warp (pair, with the class split) owns one tile and the products
@@ -283,7 +291,9 @@ __host__ __device__ constexpr int cg_nuoff(int m, int c) { return c == 0 ? 0 : c
 constexpr int fast_max_threads(int M, bool cs) { return cs ? (M == 64 ? 384 : 512) : 256; }
 constexpr int fast_min_blocks(int ek, int M, bool cs) { return (cs && M == 64 && ek == EK_CROSS) ? 3 : ek == EK_TENSOR ? 1 : 0; }
 
-template <int EK, int M, int ADJ, bool CS>
+// GK >= 0 (a Gauss-point caller, GK_*): the operands are built in the staging from the node-major nodal
+// fields of a.ga instead of read from a.in (M = 0, one batch entry).
+template <int EK, int M, int ADJ, bool CS, int GK = -1>
 __global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M, CS)) fast_kernel(const FastArgs a) {
   constexpr bool CT = M > 0;
   constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO;
@@ -325,7 +335,27 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M
   const size_t prod_d = (size_t)NO * 4 * NT * 2 * 32, xch_d = CS ? (size_t)NWT * NI * 128 : 0;
   double *ps = smem, *xc = smem + prod_d;
   double *xs = overlay ? smem : smem + prod_d + xch_d;
-  {
+  if constexpr (GK >= 0) {
+    // the operands of the tile's 8 Gauss points and every mode, from the nodal fields: mode i's cosine
+    // row is 4*KOFF[i & 1] + (i >> 1), its sine row 4*KOFF[2 + (i & 1)] + (i >> 1); other rows stay 0
+    for (int t = threadIdx.x; t < NI * KS_tot * 32; t += blockDim.x) xs[t] = 0.0;
+    __syncthreads();
+    const int m = a.m;
+    for (int it = threadIdx.x; it < 8 * m; it += blockDim.x) {
+      const int i = it % m, gp = it / m;  // a warp takes consecutive modes of one point
+      if (p0 + gp >= a.np) continue;
+      double f[8][2];
+      gauss_operands_nm<GK>(a.ga, p0 + gp, i, m, f);
+      const int c = i & 1, k = i >> 1;
+      const int rc = 4 * sel4(KOFF, c) + k, rs = 4 * sel4(KOFF, 2 + c) + k;
+      const int oc = (rc >> 2) * 32 + a_frag_slot(rc & 3, gp), os = (rs >> 2) * 32 + a_frag_slot(rs & 3, gp);
+#pragma unroll
+      for (int fi = 0; fi < NI; ++fi) {
+        xs[(size_t)fi * KS_tot * 32 + oc] = f[fi][0];
+        if (i != 0) xs[(size_t)fi * KS_tot * 32 + os] = f[fi][1];  // the sine of mode 0 is ignored
+      }
+    }
+  } else {
     const int pc = 2 * (threadIdx.x & 3), rstep = blockDim.x >> 2;
     const bool v16 = a.vec16 && p0 + 8 <= a.np;
     const bool pv0 = p0 + pc < a.np, pv1 = p0 + pc + 1 < a.np;
@@ -1348,6 +1378,75 @@ bool fast_fused_fits(int op, int m) {
 int fast_grid_length(int m) { return make_geo(m).N; }
 
 bool gauss_cross_fused_supported(int m, int n_w) { return third_fold(64) && m == 64 && n_w == 6; }
+
+namespace {
+template <int EK, int GK>
+int launch_gauss_general(FastArgs &fa, int64_t ng, cudaStream_t st) {
+  constexpr bool CS = class_split(EK, 0);
+  fa.KT = 4 * (fa.KS[0] + fa.KS[1] + fa.KS[2] + fa.KS[3]);
+  const size_t smem = fast_smem_bytes(EK, fa.NT, fa.KT, CS);
+  if (smem > 200 * 1024) return set_error(SFNL_ERR_UNSUPPORTED, "fused Gauss-point product: m too large");
+  const int tiles_per_pass = fa.NT < 8 ? fa.NT : 8;
+  const int nw = CS ? 2 * tiles_per_pass : (tiles_per_pass < 2 ? 2 : tiles_per_pass);
+  auto kern = fast_kernel<EK, 0, 0, CS, GK>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (fused Gauss-point product)");
+  const int64_t tiles = (ng + 7) / 8;
+  if (tiles > 0x7fffffff) return set_error(SFNL_ERR_UNSUPPORTED, "np too large");
+  kern<<<(unsigned)tiles, nw * 32, smem, st>>>(fa);
+  return check_launch("fused Gauss-point product");
+}
+constexpr int gauss_ek(int kind, bool conservative) {
+  return kind == GK_ADVECT ? (conservative ? EK_ADVECT : EK_DOT) : EK_CROSS;
+}
+}  // namespace
+
+bool gauss_general_fused_supported(int kind, bool conservative, int m) {
+  if (m < 1 || m > 96 || kind < GK_NS || kind > GK_ADVECT) return false;
+  const int ek = gauss_ek(kind, conservative);
+  const Geo g = make_geo(m);
+  return fast_smem_bytes(ek, g.NT, 4 * g.KS_tot, class_split(ek, 0)) <= 200 * 1024;
+}
+
+int launch_gauss_general_fused(const GaussArgs &ga, int kind, bool conservative, double *out, int64_t ng, int m,
+                               cudaStream_t st) {
+  if (!gauss_general_fused_supported(kind, conservative, m))
+    return set_error(SFNL_ERR_UNSUPPORTED, "fused Gauss-point product: not built for this size");
+  if (ng == 0) return SFNL_OK;
+  const Geo g = make_geo(m);
+  Tables T;
+  if (int rc = get_tables(g, &T)) return rc;
+  FastArgs fa;
+  std::memset(&fa, 0, sizeof(fa));
+  const int nout = kind == GK_ADVECT ? 1 : 3, nsl = kind == GK_ADVECT ? 2 : 6;
+  for (int o = 0; o < nout; ++o) {
+    fa.out[o] = out + (int64_t)2 * o * ng;  // V_out(l_G*me, nsl, m): component o in slots 2o, 2o+1
+    fa.out_ldm[o] = (int64_t)nsl * ng;
+  }
+  fa.out_ps = 1;
+  fa.np = ng;
+  fa.m = g.m;
+  fa.N = g.N;
+  fa.NT = g.NT;
+  for (int c = 0; c < 4; ++c) {
+    fa.ks_off[c] = g.ks_off[c];
+    fa.KS[c] = g.KS[c];
+    fa.nu_off[c] = g.nu_off[c];
+    fa.NU[c] = g.NU[c];
+    fa.ke[c] = g.ke[c];
+  }
+  fa.NU_tot = g.NU_tot;
+  fa.syn = T.syn;
+  fa.ana = T.ana;  // variant 0: with the analysis weights
+  fa.ga = ga;
+  switch (kind) {
+    case GK_NS: return launch_gauss_general<EK_CROSS, GK_NS>(fa, ng, st);
+    case GK_LORENTZ: return launch_gauss_general<EK_CROSS, GK_LORENTZ>(fa, ng, st);
+    default:
+      return conservative ? launch_gauss_general<EK_ADVECT, GK_ADVECT>(fa, ng, st)
+                          : launch_gauss_general<EK_DOT, GK_ADVECT>(fa, ng, st);
+  }
+}
 
 int launch_gauss_advect_fused(const GaussArgs &ga, bool conservative, double *out, int64_t ng, int m,
                               cudaStream_t st) {

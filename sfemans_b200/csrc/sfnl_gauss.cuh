@@ -1,5 +1,5 @@
-// sfnl_gauss.cuh -- the curl-type Gauss-point operands of one (Gauss point, mode), shared by the
-// operand kernel (sfnl_gauss.cu) and the fused Gauss-point cross product (sfnl_fast.cu).
+// sfnl_gauss.cuh -- the Gauss-point operands of one (Gauss point, mode), shared by the operand kernel
+// (sfnl_gauss.cu) and the fused Gauss-point products (sfnl_fast.cu).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -101,6 +101,84 @@ __device__ __forceinline__ void gauss_curl_gathered(const GaussArgs &a, const in
     }
   }
   curl_from_sums<KIND>(mode, ray, wv, d1, d2, om, w2, rot, w);
+}
+
+// The operands of one (Gauss point p, mode index i) from node-major nodal fields with a run-time mode
+// stride tm (launch_nodal_transpose: value (node, k, i) at node*ns*tm + k*tm + i, ns = 6 for a.v, a.omega
+// and the Lorentz field a.v2, 2 for the advection scalar a.v2).  f[field][cos, sin]:
+//   GK_NS, GK_LORENTZ: fields 0-2 = RotV (r, theta, z), 3-5 = W;
+//   GK_ADVECT: 0-2 = heat grad c, 3-5 = u, 6 = div u, 7 = heat c (subroutine_temperature_with_T.F90:300-331).
+template <int KIND>
+__device__ __forceinline__ void gauss_operands_nm(const GaussArgs &a, int64_t p, int i, int tm, double (&f)[8][2]) {
+  const int me = (int)(p / a.l_G), l = (int)(p % a.l_G);
+  const double mode = (double)a.list_mode[i];
+  const double *dwl = a.dw + (size_t)2 * a.n_w * (l + (size_t)a.l_G * me);
+  double ray = 0.0, wv[6] = {0, 0, 0, 0, 0, 0}, d1[6] = {0, 0, 0, 0, 0, 0}, d2[6] = {0, 0, 0, 0, 0, 0};
+  double om[6] = {0, 0, 0, 0, 0, 0}, w2[6] = {0, 0, 0, 0, 0, 0};
+  double cw[2] = {0, 0}, c1[2] = {0, 0}, c2[2] = {0, 0};
+  for (int n = 0; n < a.n_w; ++n) {
+    int node = a.jj[n + (size_t)a.n_w * me] - 1;  // 1-based node numbers
+    node = node < 0 ? 0 : node >= a.np_nodes ? a.np_nodes - 1 : node;  // no access outside the fields
+    const double wt = a.ww[n + (size_t)a.n_w * l], g1 = dwl[2 * n], g2 = dwl[2 * n + 1];
+    ray = fma(a.rr[2 * (size_t)node], wt, ray);
+    const double *vn = a.v + (size_t)node * 6 * tm + i;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const double vs = vn[(size_t)k * tm];
+      wv[k] = fma(vs, wt, wv[k]);
+      d1[k] = fma(vs, g1, d1[k]);
+      d2[k] = fma(vs, g2, d2[k]);
+    }
+    if (KIND == GK_NS && a.omega) {
+      const double *on = a.omega + (size_t)node * 6 * tm + i;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) om[k] = fma(on[(size_t)k * tm], wt, om[k]);
+    }
+    if (KIND == GK_LORENTZ) {
+      const double *bn = a.v2 + (size_t)node * 6 * tm + i;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) w2[k] = fma(bn[(size_t)k * tm], wt, w2[k]);
+    }
+    if (KIND == GK_ADVECT) {
+      const double *cn = a.v2 + (size_t)node * 2 * tm + i;
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const double cs = cn[(size_t)k * tm];
+        cw[k] = fma(cs, wt, cw[k]);
+        c1[k] = fma(cs, g1, c1[k]);
+        c2[k] = fma(cs, g2, c2[k]);
+      }
+    }
+  }
+  if constexpr (KIND == GK_ADVECT) {
+    const double mr = mode / ray, hc = a.heat ? a.heat[me] : 1.0;
+    f[0][0] = hc * c1[0];
+    f[0][1] = hc * c1[1];
+    f[1][0] = hc * (mr * cw[1]);
+    f[1][1] = hc * (-mr * cw[0]);
+    f[2][0] = hc * c2[0];
+    f[2][1] = hc * c2[1];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      f[3 + k][0] = wv[2 * k];
+      f[3 + k][1] = wv[2 * k + 1];
+    }
+    f[6][0] = d1[0] + wv[0] / ray + mr * wv[3] + d2[4];
+    f[6][1] = d1[1] + wv[1] / ray - mr * wv[2] + d2[5];
+    f[7][0] = hc * cw[0];
+    f[7][1] = hc * cw[1];
+  } else {
+    double rot[6], w[6];
+    curl_from_sums<KIND>(mode, ray, wv, d1, d2, om, w2, rot, w);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      f[k][0] = rot[2 * k];
+      f[k][1] = rot[2 * k + 1];
+      f[3 + k][0] = w[2 * k];
+      f[3 + k][1] = w[2 * k + 1];
+    }
+    f[6][0] = f[6][1] = f[7][0] = f[7][1] = 0.0;
+  }
 }
 
 }  // namespace sfnl

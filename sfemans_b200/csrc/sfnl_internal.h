@@ -64,13 +64,20 @@ int launch_gauss_cross_fused(const GaussArgs &ga, int kind, double *out, int64_t
 // node-major scalar (np_nodes, 2, m), ga.heat per element or null; out (l_G*me, 2, m).  m = 64, n_w = 6.
 int launch_gauss_advect_fused(const GaussArgs &ga, bool conservative, double *out, int64_t ng, int m,
                               cudaStream_t st);
+// Every caller at the other m that the fused FAST kernels serve (any n_w): the operands staged from the
+// node-major nodal fields (stride m) by the general FAST kernel.  out: (l_G*me, 6, m) for the curl
+// callers, (l_G*me, 2, m) for the advection callers.
+bool gauss_general_fused_supported(int kind, bool conservative, int m);
+int launch_gauss_general_fused(const GaussArgs &ga, int kind, bool conservative, double *out, int64_t ng, int m,
+                               cudaStream_t st);
 
 // Elementary programs: cross (6 -> 3), dot (6 -> 1), product (2 -> 1),
 // scalar x vector (4 -> 3) and tensor (6 -> 9).  Every bilinear program of
 // sfnl_ops.cuh is a sequence of them on one stream (the bundle is four, a
 // linearised cross product two or four, accumulating where a term adds to an
 // earlier one).
-enum { EK_CROSS = 0, EK_DOT = 1, EK_PROD = 2, EK_SVECT = 3, EK_TENSOR = 4 };
+enum { EK_CROSS = 0, EK_DOT = 1, EK_PROD = 2, EK_SVECT = 3, EK_TENSOR = 4,
+       EK_ADVECT = 5 };  // g . w + d c (8 -> 1): the fused conservative advection callers only
 struct Elem {
   int ek;
   int in[6];     // field indices into ProgArgs.in
