@@ -202,3 +202,47 @@ def test_operands_alone_match_the_restatement(kind, cons):
     assert len(got) == len(ref)
     for g, r in zip(got, ref):
         assert R.rel_l2(sf.to_host(g), r) <= 1e-13
+
+
+def _p1_mesh(nr, nz, seed):
+    # the vertices of a P2 mesh as a P1 mesh (3 nodes per element, linear basis at the same 7 points)
+    m2 = R.synthetic_p2_mesh(nr, nz, seed)
+    L = np.array([[1 / 3, 2 / 3, 1 / 6, 1 / 6, 0.1, 0.45, 0.45], [1 / 3, 1 / 6, 2 / 3, 1 / 6, 0.45, 0.1, 0.45],
+                  [1 / 3, 1 / 6, 1 / 6, 2 / 3, 0.45, 0.45, 0.1]])
+    jj = np.asfortranarray(m2["jj"][:3])
+    me = jj.shape[1]
+    dw = np.zeros((2, 3, 7, me), order="F")
+    for e in range(me):
+        P = m2["rr"][:, jj[:, e] - 1].T  # (3 vertices, (r, z))
+        T = np.array([[P[0, 0] - P[2, 0], P[1, 0] - P[2, 0]], [P[0, 1] - P[2, 1], P[1, 1] - P[2, 1]]])
+        G = np.linalg.inv(T)
+        dlam = np.array([G[0], G[1], -G[0] - G[1]])  # (3 lambdas, 2 coords)
+        dw[:, :, :, e] = dlam.T[:, :, None]
+    return {"jj": jj, "rr": m2["rr"], "ww": np.asfortranarray(L), "dw": dw, "np": m2["np"], "me": me, "n_w": 3,
+            "l_G": 7}
+
+
+@pytest.mark.parametrize("m", [12, 64, 96])
+def test_fused_general_kernel_p1_elements(m):
+    # the general fused kernel (any element type; at m = 64 it serves the elements the third-fold kernels
+    # do not): P1 elements, every caller, against the restatements
+    mesh = _p1_mesh(5, 4, 21)
+    lm = list(range(m))
+    dm, lmd = _dev_mesh(mesh), torch.tensor(lm, dtype=torch.int32, device="cuda")
+    V = R.synthetic_field(mesh["np"], 6, m, 0.2, 161)
+    W2 = R.synthetic_field(mesh["np"], 6, m, 0.2, 162)
+    C = R.synthetic_field(mesh["np"], 2, m, 0.2, 163)
+    om = R.precession_omega(mesh["np"], lm, 0.3, 0.2)
+    heat = _heat(mesh, True)
+    ref = R.c_cross_gauss(V, mesh, lm, om)[0]
+    out = sf.cross_gauss(sf.to_device(V), dm, lmd, omega=sf.to_device(om))
+    assert _worst(sf.to_host(out), ref) <= FP64_TOL
+    ref = R.c_curlh_cross_b_gauss(V, W2, mesh, lm)[0]
+    out = sf.curlh_cross_b_gauss(sf.to_device(V), sf.to_device(W2), dm, lmd)
+    assert _worst(sf.to_host(out), ref) <= FP64_TOL
+    for cons, ht in ((False, None), (True, heat)):
+        ref = R.c_ugradc_gauss(V, C, mesh, lm, heat=ht, conservative=cons)[0]
+        out = sf.ugradc_gauss(sf.to_device(V), sf.to_device(C), dm, lmd,
+                              heat=None if ht is None else torch.tensor(ht, device="cuda"), conservative=cons)
+        torch.cuda.synchronize()
+        assert R.rel_l2(sf.to_host(out), ref) <= FP64_TOL
