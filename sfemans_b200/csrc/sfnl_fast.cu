@@ -292,9 +292,11 @@ constexpr int fast_max_threads(int M, bool cs) { return cs ? (M == 64 ? 384 : 51
 constexpr int fast_min_blocks(int ek, int M, bool cs) { return (cs && M == 64 && ek == EK_CROSS) ? 3 : ek == EK_TENSOR ? 1 : 0; }
 
 // GK >= 0 (a Gauss-point caller, GK_*): the operands are built in the staging from the node-major nodal
-// fields of a.ga instead of read from a.in (M = 0, one batch entry).
+// fields of a.ga instead of read from a.in (one batch entry).
 template <int EK, int M, int ADJ, bool CS, int GK = -1>
-__global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M, CS)) fast_kernel(const FastArgs a) {
+__global__ void __launch_bounds__(fast_max_threads(M, CS),
+                                  GK >= 0 && fast_min_blocks(EK, M, CS) > 2 ? 2 : fast_min_blocks(EK, M, CS))
+    fast_kernel(const FastArgs a) {
   constexpr bool CT = M > 0;
   constexpr int NI = EKDef<EK>::NI, NO = EKDef<EK>::NO;
   // Shared memory: folded products ps [NO][4][NT][2][32], with the class split (CS) the exchange
@@ -340,7 +342,7 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS), fast_min_blocks(EK, M
     // row is 4*KOFF[i & 1] + (i >> 1), its sine row 4*KOFF[2 + (i & 1)] + (i >> 1); other rows stay 0
     for (int t = threadIdx.x; t < NI * KS_tot * 32; t += blockDim.x) xs[t] = 0.0;
     __syncthreads();
-    const int m = a.m;
+    const int m = CT ? M : a.m;
     for (int it = threadIdx.x; it < 8 * m; it += blockDim.x) {
       const int i = it % m, gp = it / m;  // a warp takes consecutive modes of one point
       if (p0 + gp >= a.np) continue;
@@ -689,10 +691,13 @@ __device__ __forceinline__ void tf_synth(const double *xs, const double *syn, do
   const double *xs_l = xs + a_frag_slot(lane & 3, lane >> 2);
   const double *syn_e = syn + (size_t)te_tile * 32 + lane, *syn_o = syn + (size_t)tau * 32 + lane;
   constexpr int KSE = tf_KS(M, 0) > tf_KS(M, 1) ? tf_KS(M, 0) : tf_KS(M, 1);
+  // the next k-step's B fragment is loaded while the current one feeds the DMMAs (the table is read from L2)
+  double bnext = __ldg(syn_e + (size_t)koff_e * NT * 32);
 #pragma unroll
   for (int s = 0; s < KSE; ++s) {
     if (s >= ks_e) break;
-    const double bv = __ldg(syn_e + (size_t)(koff_e + s) * NT * 32);
+    const double bv = bnext;
+    bnext = s + 1 < ks_e ? __ldg(syn_e + (size_t)(koff_e + s + 1) * NT * 32) : __ldg(syn_o + (size_t)koff_o * NT * 32);
     const double *xa = xs_l + (size_t)(koff_e + s) * 32;
     double av[NG];
 #pragma unroll
@@ -708,7 +713,8 @@ __device__ __forceinline__ void tf_synth(const double *xs, const double *syn, do
   }
 #pragma unroll
   for (int s = 0; s < tf_KS(M, 2); ++s) {
-    const double bv = __ldg(syn_o + (size_t)(koff_o + s) * NT * 32);
+    const double bv = bnext;
+    if (s + 1 < tf_KS(M, 2)) bnext = __ldg(syn_o + (size_t)(koff_o + s + 1) * NT * 32);
     const double *xa = xs_l + (size_t)(koff_o + s) * 32;
     double av[NG];
 #pragma unroll
@@ -873,10 +879,12 @@ __device__ __forceinline__ void tf_analysis(const double *ps, const double *ana,
       for (int o = 0; o < NO; ++o) yp[i][o][0] = yp[i][o][1] = 0.0;
     const double *bt = anav + (size_t)(aof + u * TE) * 32;
     const double *pa = ps + (size_t)c * NT * 2 * 32;
+    double bnext = __ldg(bt);  // the next k-step's B fragment is loaded while the current one is used
 #pragma unroll
     for (int te = 0; te < 2 * NT; ++te) {
       if (te >= TE) break;
-      const double bv = __ldg(bt + (size_t)te * 32);
+      const double bv = bnext;
+      if (te + 1 < TE) bnext = __ldg(bt + (size_t)(te + 1) * 32);
       const int t = te >> 1, e = te & 1;
 #pragma unroll
       for (int o = 0; o < NO; ++o) {
@@ -1380,21 +1388,31 @@ int fast_grid_length(int m) { return make_geo(m).N; }
 bool gauss_cross_fused_supported(int m, int n_w) { return third_fold(64) && m == 64 && n_w == 6; }
 
 namespace {
-template <int EK, int GK>
-int launch_gauss_general(FastArgs &fa, int64_t ng, cudaStream_t st) {
-  constexpr bool CS = class_split(EK, 0);
+template <int EK, int GK, int M>
+int launch_gauss_general_m(FastArgs &fa, int64_t ng, cudaStream_t st) {
+  constexpr bool CS = class_split(EK, M);
   fa.KT = 4 * (fa.KS[0] + fa.KS[1] + fa.KS[2] + fa.KS[3]);
   const size_t smem = fast_smem_bytes(EK, fa.NT, fa.KT, CS);
   if (smem > 200 * 1024) return set_error(SFNL_ERR_UNSUPPORTED, "fused Gauss-point product: m too large");
   const int tiles_per_pass = fa.NT < 8 ? fa.NT : 8;
   const int nw = CS ? 2 * tiles_per_pass : (tiles_per_pass < 2 ? 2 : tiles_per_pass);
-  auto kern = fast_kernel<EK, 0, 0, CS, GK>;
+  auto kern = fast_kernel<EK, M, 0, CS, GK>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (fused Gauss-point product)");
   const int64_t tiles = (ng + 7) / 8;
   if (tiles > 0x7fffffff) return set_error(SFNL_ERR_UNSUPPORTED, "np too large");
   kern<<<(unsigned)tiles, nw * 32, smem, st>>>(fa);
   return check_launch("fused Gauss-point product");
+}
+// the geometries the plain products specialise (m = 16, 32, 64), else run-time geometry
+template <int EK, int GK>
+int launch_gauss_general(FastArgs &fa, int64_t ng, cudaStream_t st) {
+  switch (fa.m) {
+    case 16: return launch_gauss_general_m<EK, GK, 16>(fa, ng, st);
+    case 32: return launch_gauss_general_m<EK, GK, 32>(fa, ng, st);
+    case 64: return launch_gauss_general_m<EK, GK, 64>(fa, ng, st);
+    default: return launch_gauss_general_m<EK, GK, 0>(fa, ng, st);
+  }
 }
 constexpr int gauss_ek(int kind, bool conservative) {
   return kind == GK_ADVECT ? (conservative ? EK_ADVECT : EK_DOT) : EK_CROSS;
