@@ -473,3 +473,28 @@ def test_linearised_700k_points_full_size():
     assert float(torch.linalg.vector_norm(fd - jv) / torch.linalg.vector_norm(jv)) <= 1e-8
     lhs, rhs = float(torch.sum(jv * cot)), float(torch.sum(tan * jt))
     assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+def test_bundle_full_size_matches_the_elementary_products():
+    # the MHD bundle at its configuration's size (1.4 M points, m = 64): the one-launch kernel against the
+    # elementary cross and dot products (other kernels, each pinned to the oracle above) over every point
+    import torch
+
+    npts, m, pad = 1_400_000, 64, 96
+
+    def field(seed):
+        g = torch.Generator(device="cuda")
+        g.manual_seed(seed)
+        t = torch.randn((m, 6, npts), generator=g, device="cuda", dtype=torch.float64)
+        t *= torch.exp(-0.1 * torch.arange(m, device="cuda", dtype=torch.float64))[:, None, None]
+        t[0, 1::2, :] = 0.0
+        return t.permute(2, 1, 0)
+
+    u, w, b, j, gt = (field(500 + i) for i in range(5))
+    outs = sf.bundle_mhd(u, w, b, j, gt, m_max_pad=pad)
+    refs = (sf.product(sf.OP_CROSS, u, w, m_max_pad=pad, algo=sf.ALGO_FAST),
+            sf.product(sf.OP_CROSS, u, b, m_max_pad=pad, algo=sf.ALGO_FAST),
+            sf.product(sf.OP_CROSS, j, b, m_max_pad=pad, algo=sf.ALGO_FAST),
+            sf.product(sf.OP_DOT, u, gt, m_max_pad=pad, algo=sf.ALGO_FAST))
+    for o, r in zip(outs, refs):
+        assert float(torch.linalg.vector_norm(o - r) / torch.linalg.vector_norm(r)) <= FP64_TOL
