@@ -1,6 +1,6 @@
 """GPU parity of the all-FP64 forms against the CPU oracle.
 
-Bar (north star): rel-L2 <= 1e-12 per output array against the long-double
+Bar: rel-L2 <= 1e-12 per output array against the long-double
 restatement of fft_parallel.F90 (FP64_TOL below).  Every call goes through
 the C-ABI library (ctypes), on device tensors or on host arrays.
 """

@@ -1,6 +1,6 @@
 """Split-precision (tcgen05, bf16-sliced) forms against the FP64 oracle.
 
-Bar (north star): rel-L2 <= 1e-7 per output array for the 3-slice form
+Bar: rel-L2 <= 1e-7 per output array for the 3-slice form
 (SPLIT_TOL).  The 2-slice "bf16 hi/lo" form is reported and held to 1e-4.
 """
 import numpy as np
