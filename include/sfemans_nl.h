@@ -57,7 +57,7 @@ enum {
   SFNL_ERR_ARG = -1,         /* null pointer, np < 0, m < 1, k_batch < 1, odd nb_field ... */
   SFNL_ERR_SHAPE = -2,       /* nb_field/nslot not what the product needs, np > nb_procs*bloc_size */
   SFNL_ERR_ALIAS = -3,       /* m_max_pad < m_max, or (fast/split forms) grid too short to dealias */
-  SFNL_ERR_UNSUPPORTED = -4, /* size beyond this build's limits, nb_procs != 1 on one GPU */
+  SFNL_ERR_UNSUPPORTED = -4, /* size beyond this library's limits, nb_procs != 1 on one GPU */
   SFNL_ERR_CUDA = -5,        /* a CUDA runtime call or kernel launch failed */
   SFNL_ERR_NONFINITE = -6,   /* (check mode) a NaN/Inf was found in the output */
   SFNL_ERR_ALLOC = -7,       /* device or pinned host allocation failed */

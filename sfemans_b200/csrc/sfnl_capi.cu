@@ -131,7 +131,7 @@ int check_common(int64_t np, int m, int pad, int n_theta, int k_batch, int *N_ou
   if (m < 1) return set_error(SFNL_ERR_ARG, "m_max < 1 (the reference stops on m_max_c==0)");
   if (k_batch < 1 || k_batch > 65535) return set_error(SFNL_ERR_ARG, "k_batch outside [1, 65535]");
   if (pad < m) return set_error(SFNL_ERR_ALIAS, "m_max_pad < m_max: the padded spectrum cannot hold the modes");
-  if (m > 4096 || pad > (1 << 20)) return set_error(SFNL_ERR_UNSUPPORTED, "m_max or m_max_pad beyond this build's limits");
+  if (m > 4096 || pad > (1 << 20)) return set_error(SFNL_ERR_UNSUPPORTED, "m_max or m_max_pad beyond this library's limits");
   const int N = n_theta > 0 ? n_theta : 2 * pad - 1;
   if (m > N / 2 + 1) return set_error(SFNL_ERR_ALIAS, "grid shorter than 2*m_max-1 angles");
   *N_out = N;
@@ -505,7 +505,7 @@ int check_synth(int64_t np, int nslot, int m, const char *what) {
     std::string msg = std::string("Bug in ") + what + ": MOD(nb_field,2)/=0 .OR. m_max_c==0";
     return set_error(SFNL_ERR_ARG, msg.c_str());
   }
-  if (m > 4096) return set_error(SFNL_ERR_UNSUPPORTED, "m_max beyond this build's limits");
+  if (m > 4096) return set_error(SFNL_ERR_UNSUPPORTED, "m_max beyond this library's limits");
   return SFNL_OK;
 }
 
@@ -885,7 +885,7 @@ int sfnl_real_f64(const double *v, double *out, int64_t np, int nslot, int m_max
   int rc = check_synth(np, nslot, m_max, "FFT_PAR_REAL");
   if (rc) return rc;
   if (n_theta < 2 * m_max - 1) return set_error(SFNL_ERR_ALIAS, "n_theta < 2*m_max-1: the grid cannot hold the modes");
-  if (n_theta > (1 << 21)) return set_error(SFNL_ERR_UNSUPPORTED, "n_theta beyond this build's limits");
+  if (n_theta > (1 << 21)) return set_error(SFNL_ERR_UNSUPPORTED, "n_theta beyond this library's limits");
   if (np == 0) return SFNL_OK;
   if (!v || !out) return set_error(SFNL_ERR_ARG, "null array");
   return launch_real(v, out, np, nslot, m_max, n_theta, as_stream(stream));
@@ -896,7 +896,7 @@ int sfnl_max_vel_f64(const double *v, double *vmax, int64_t np, int nslot, int m
   int rc = check_synth(np, nslot, m_max, "FFT_MAX_VEL_DCL");
   if (rc) return rc;
   if (m_max_pad < m_max) return set_error(SFNL_ERR_ALIAS, "m_max_pad < m_max: the padded spectrum cannot hold the modes");
-  if (m_max_pad > (1 << 20)) return set_error(SFNL_ERR_UNSUPPORTED, "m_max_pad beyond this build's limits");
+  if (m_max_pad > (1 << 20)) return set_error(SFNL_ERR_UNSUPPORTED, "m_max_pad beyond this library's limits");
   if (!vmax || (np > 0 && !v)) return set_error(SFNL_ERR_ARG, "null array");
   cudaStream_t st = as_stream(stream);
   if (cudaMemsetAsync(vmax, 0, sizeof(double), st) != cudaSuccess) return set_error(SFNL_ERR_CUDA, "memset of the result failed");
