@@ -169,10 +169,11 @@ int sfnl_bundle_mhd_f64(const double *u, const double *w, const double *b, const
  *   m_max_pad  <= 0: 3*nmod/2, the caller's choice (:625)
  *   work       device buffer of 12*l_G*me*nmod doubles for RotV and W, or NULL: a buffer
  *              owned by the library (one per device, grown with cudaMalloc when too small;
- *              calls that overlap on the GPU then share it and race).  At nmod = 64 on P2
- *              elements (n_w = 6) RotV and W are built inside the product kernel and work
- *              holds node-major copies of the nodal fields instead (6*np_nodes*nmod doubles per
- *              field, v and omega), when they fit in it
+ *              calls that overlap on the GPU then share it and race).  For nmod <= 96 RotV
+ *              and W are built inside the product kernel (the third-fold kernel at nmod = 64 on
+ *              P2 elements, the general FAST kernel otherwise) and work holds node-major copies
+ *              of the nodal fields instead (6*np_nodes*nmod doubles per field, v and omega),
+ *              when they fit in it; larger nmod write RotV and W to work and read them back
  * ------------------------------------------------------------------------- */
 int sfnl_cross_gauss_f64(const double *v, const int *jj, const double *ww, const double *dw, const double *rr,
                          const int *list_mode, const double *omega, double *out, int np_nodes, int me, int n_w,
@@ -205,7 +206,9 @@ int sfnl_smb_curlh_cross_b_gauss(const double *V_in, const double *W_in, const i
  * program analysed once).
  *   v     (np_nodes, 6, nmod) nodal velocity;  c (np_nodes, 2, nmod) nodal scalar
  *   heat  (me) per-element factor of grad c and c, or NULL (factor 1)
- *   work  16*l_G*me*nmod doubles (12 when conservative == 0) or NULL. */
+ *   work  16*l_G*me*nmod doubles (12 when conservative == 0) or NULL.  For nmod <= 96 the
+ *         operands are built inside the product kernel and work holds node-major copies of
+ *         v and c (8*np_nodes*nmod doubles) instead, when they fit in it. */
 int sfnl_ugradc_gauss_f64(const double *v, const double *c, const double *heat, int conservative, const int *jj,
                           const double *ww, const double *dw, const double *rr, const int *list_mode, double *out,
                           int np_nodes, int me, int n_w, int l_G, int nmod, int m_max_pad, double *work,
