@@ -319,18 +319,20 @@ def main():
         configs = _extra_configs(args, sf, torch, dev, world, rank, dist, local, stream)
 
     if args.workload == "mhd_bundle":
-        kname = {"fp64": "fast_bundle_tf_kernel<64>" if m == 64 else "fast_kernel<EK_CROSS>",
+        kname = {"fp64": "fast_bundle_r3_kernel" if m == 64 else "fast_kernel<EK_CROSS>",
                  "split3": "split_kernel<PR_BUNDLE>", "split2": "split_kernel<PR_BUNDLE>", "grid": "grid_kernel<OP_BUNDLE>"}[best]
     else:
         kname = {"fp64": "fast_kernel<EK_CROSS>", "split3": "split_kernel<PR_CROSS>", "split2": "split_kernel<PR_CROSS>",
                  "grid": "grid_kernel<OP_CROSS>"}[best]
-    # The FAST FP64 kernels are bound by the FP64 pipe, not HBM: the third-fold bundle at m = 64 issues
-    # 3,600 mma.sync.m8n8k4.f64 (512 flops each) per 8-point tile (5 operands x 12 warps x 12 k-steps x 3
-    # fields, 10 outputs x 144 k-steps); DMMA and DFMA share about 36.6 TFLOP/s on B200 (a throughput probe).
+    # FP64 tensor work of the FAST bundle at m = 64 (fast_bundle_r3_kernel, the grid split into its three
+    # residue classes): 1,800 mma.sync.m8n8k4.f64 (512 flops each) per 8-point tile (5 operands x 12 warps x
+    # 6 k-steps x 3 fields, and 10 outputs x 3 residues x 24 k-steps), half of what one 192-angle transform
+    # needs; the residue twiddles add about 2 % in FP64 FMAs.  DMMA and DFMA share about 36.6 TFLOP/s on B200
+    # (a throughput probe).
     fp64_pipe = None
     if single and best == "fp64" and args.workload == "mhd_bundle" and m == 64:
-        flops = 3600.0 * 512.0 * ((npts + 7) // 8)
-        fp64_pipe = {"kernel": "fast_bundle_tf_kernel<64>", "flops_per_launch": flops,
+        flops = 1800.0 * 512.0 * ((npts + 7) // 8)
+        fp64_pipe = {"kernel": "fast_bundle_r3_kernel", "flops_per_launch": flops,
                      "achieved_tflops": flops / (dom_ms / 1e3) / 1e12, "peak_tflops": FP64_PIPE_TFLOPS,
                      "peak_source": "sfnl_probe_fp64_tflops (python -m sfemans_b200.profile_case --program fp64peak: "
                                     "DMMA 37.1, DFMA 34.1 TFLOP/s); not in MEASURED_PEAKS.json",
@@ -623,8 +625,8 @@ def _extra_configs(args, sf, torch, dev, world, rank, dist, local, stream):
     except sf.SfnlError as e:
         cfg["split3"] = {"unavailable": str(e)}
     nb = 8.0 * m * npts * (18 + k * (18 + 12))
-    cfg["roofline"] = {"jvp": roof(nb, ms_j, "large_syn_tf_kernel + large_prod_tf_kernel (per tangent)"),
-                       "vjp": roof(nb, ms_t, "large_syn_tf_kernel + large_prod_tf_kernel (per tangent)")}
+    cfg["roofline"] = {"jvp": roof(nb, ms_j, "large_syn_tf_kernel + large_prod_tf_kernel (tangents batched per launch)"),
+                       "vjp": roof(nb, ms_t, "large_syn_tf_kernel + large_prod_tf_kernel (tangents batched per launch)")}
     if cpu_on:
         n_s, kt = 500, 2
         hU, hW, hB = (np.asfortranarray(H(x[:n_s])) for x in (U, W, B))

@@ -399,6 +399,14 @@ int sfnl_finalize(void);
  * alone with CUDA events (long register-only chains, every SM busy, best of
  * five launches): the compute roofline of the all-FP64 forms. */
 int sfnl_probe_fp64_tflops(double *dmma_tflops, double *dfma_tflops);
+/* Kernel of the FAST MHD bundle at m_max = 64 (sfnl_bundle_mhd_f64 and the
+ * host entry), process-wide: SFNL_BUNDLE_RESIDUE (default) splits the
+ * 192-angle grid into its three residue classes (64-angle grids, half the
+ * FP64 tensor-core work); SFNL_BUNDLE_THIRD_FOLD runs the single 192-angle
+ * transform.  Both give the same truncated products (to rounding).  Returns
+ * the previous kind, or SFNL_ERR_ARG for another value. */
+enum { SFNL_BUNDLE_RESIDUE = 0, SFNL_BUNDLE_THIRD_FOLD = 1 };
+int sfnl_set_bundle_kernel(int kind);
 /* Host-side fault injection for tests of the error path: marks the split-form
  * status word as a kernel does when a bounded wait on its tensor-core
  * operations gives up (no GPU work is involved).  The next split-form call

@@ -107,6 +107,7 @@ _SIGS = {
     "sfnl_finalize": [],
     "sfnl_last_host_timing": [_P],
     "sfnl_test_inject_timeout": [],
+    "sfnl_set_bundle_kernel": [_I],
     "sfnl_probe_fp64_tflops": [_P, _P],
     "sfnl_fft_par_pack_modes": [_P, _P] + [_I] * 6,
     "sfnl_fft_par_block": [_I, _P, _P, _P] + [_I] * 4 + [_P],
@@ -434,6 +435,17 @@ def mhd_vjp(u, w, b, cot, m_max_pad=None, out=None, split=None, stream=None):
 
 def set_check_finite(on: bool):
     _check(lib().sfnl_set_check_finite(1 if on else 0))
+
+
+BUNDLE_RESIDUE, BUNDLE_THIRD_FOLD = 0, 1
+
+
+def set_bundle_kernel(kind: int) -> int:
+    """Kernel of the FAST MHD bundle at m = 64 (process-wide): BUNDLE_RESIDUE (default, the grid split into
+    its three residue classes) or BUNDLE_THIRD_FOLD (one 192-angle transform).  Returns the previous kind."""
+    rc = lib().sfnl_set_bundle_kernel(int(kind))
+    _check(min(rc, 0))
+    return rc
 
 
 def finalize():

@@ -17,7 +17,7 @@ SRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libsfemans_nl.so")
 SOURCES = ["sfnl_capi.cu", "sfnl_grid.cu", "sfnl_fast.cu", "sfnl_large.cu", "sfnl_split.cu", "sfnl_synth.cu",
-           "sfnl_gauss.cu", "sfnl_probe.cu"]
+           "sfnl_gauss.cu", "sfnl_probe.cu", "sfnl_r3.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -10,6 +10,7 @@
 //   SPLIT sfnl_split.cu  bf16-sliced tcgen05 contractions, FP64 recombination
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -26,6 +27,7 @@ namespace {
 thread_local std::string g_err = "no error";
 thread_local double g_host_timing[3] = {0, 0, 0};
 int g_check_finite = 0;
+std::atomic<int> g_bundle_kernel{SFNL_BUNDLE_RESIDUE};
 
 struct DevState {
   int sms = 0;
@@ -517,6 +519,8 @@ struct BundleCtx {
 int run_bundle_dev(std::vector<HostBuf> &b, int64_t np_chunk, void *vctx, cudaStream_t st);
 
 }  // namespace
+int bundle_kernel() { return g_bundle_kernel.load(); }
+
 }  // namespace sfnl
 
 using namespace sfnl;
@@ -530,6 +534,11 @@ int sfnl_set_check_finite(int on) {
   return SFNL_OK;
 }
 int sfnl_test_inject_timeout(void) { return split_inject_timeout(); }
+int sfnl_set_bundle_kernel(int kind) {
+  if (kind != SFNL_BUNDLE_RESIDUE && kind != SFNL_BUNDLE_THIRD_FOLD)
+    return set_error(SFNL_ERR_ARG, "bundle kernel: SFNL_BUNDLE_RESIDUE or SFNL_BUNDLE_THIRD_FOLD");
+  return g_bundle_kernel.exchange(kind);
+}
 int sfnl_last_host_timing(double *s3) {
   if (!s3) return set_error(SFNL_ERR_ARG, "null pointer");
   for (int i = 0; i < 3; ++i) s3[i] = g_host_timing[i];

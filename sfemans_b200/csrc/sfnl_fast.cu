@@ -729,93 +729,21 @@ __device__ __forceinline__ void tf_synth(const double *xs, const double *syn, do
   }
 }
 
-// Both exchanges (call with every thread, after a barrier that ends the reads of whatever xc overlays):
-// X1 assembles the even class on the warp's own tile from the two parts (a first-half tile adds its
-// partner's part at the same lane; a second-half tile takes both parts at the mirror lane (lane ^ 3) and
-// parity 1 - e: CE = E0 - E2, SE = S2 - S0); X2 swaps half of the folded sums (A = CE+CO, B = CE-CO against
-// C = SE+SO, D = SO-SE) with the other half, so that half e ends with the four quadrant values
-// v[r][f] of its angles of parity e.  xc holds 2 * NT * NG * 64 doubles.  Returns after the X2 reads.
+// Both exchanges of the CTA's warps (fold_exchange with the CTA barrier; call with every thread, after a
+// barrier that ends the reads of whatever xc overlays).  xc holds 2 * NT * NG * 64 doubles.
 template <int M, int NG>
 __device__ __forceinline__ void tf_fold(const double (&acc_e)[NG][2], const double (&acc_o)[NG][2], double *xc,
                                         double (&v)[4][NG]) {
-  constexpr int NT = TfGeo<M>::NT, NH = TfGeo<M>::NH;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int tau = warp >> 1, half = warp & 1;
-  const bool first = tau < NH;
-  double acc[NG][2][2];  // [f][even, odd class][e]
-  {
-    double *x1 = xc + (size_t)((tau * 2 + half) * NG) * 64 + lane;
-#pragma unroll
-    for (int f = 0; f < NG; ++f) {
-      x1[(f * 2 + 0) * 32] = acc_e[f][0];
-      x1[(f * 2 + 1) * 32] = acc_e[f][1];
-    }
-    __syncthreads();
-    const double *own = xc + (size_t)((tau * 2 + half) * NG) * 64;
-    const double *mate = xc + (size_t)(((NT - 1 - tau) * 2 + half) * NG) * 64;
-#pragma unroll
-    for (int f = 0; f < NG; ++f)
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        double ev;
-        if (first) {
-          ev = acc_e[f][e] + mate[(f * 2 + e) * 32 + lane];
-        } else {
-          const double p0m = mate[(f * 2 + 1 - e) * 32 + (lane ^ 3)];  // E0 / S0 at the mirror angle
-          const double p2m = own[(f * 2 + 1 - e) * 32 + (lane ^ 3)];   // E2 / S2 at the mirror angle
-          ev = half ? p2m - p0m : p0m - p2m;
-        }
-        acc[f][0][e] = ev;
-        acc[f][1][e] = acc_o[f][e];
-      }
-    __syncthreads();  // X1 is read: X2 reuses xc
-  }
-  auto pair_sums = [&](int f, int e, double &X, double &Y) {
-    const double lo = e ? acc[f][0][1] : acc[f][0][0], hi = e ? acc[f][1][1] : acc[f][1][0];
-    X = lo + hi;
-    Y = half ? hi - lo : lo - hi;
-  };
-  double *xw = xc + (size_t)tau * 2 * NG * 64 + lane;  // [writer half][f][X, Y][32]
-#pragma unroll
-  for (int f = 0; f < NG; ++f) {
-    double X, Y;
-    pair_sums(f, 1 - half, X, Y);
-    xw[((half * NG + f) * 2 + 0) * 32] = X;
-    xw[((half * NG + f) * 2 + 1) * 32] = Y;
-  }
-  __syncthreads();
-  const int e = half;
-#pragma unroll
-  for (int f = 0; f < NG; ++f) {
-    double X, Y;
-    pair_sums(f, e, X, Y);
-    const double Xp = xw[(((1 - half) * NG + f) * 2 + 0) * 32], Yp = xw[(((1 - half) * NG + f) * 2 + 1) * 32];
-    const double A = half ? Xp : X, B = half ? Yp : Y, C = half ? X : Xp, D = half ? Y : Yp;
-    v[0][f] = A + C;  // theta
-    v[1][f] = B + D;  // pi - theta
-    v[2][f] = B - D;  // pi + theta
-    v[3][f] = A - C;  // 2 pi - theta
-  }
+  const int warp = threadIdx.x >> 5;
+  fold_exchange<TfGeo<M>::NT, NG>(acc_e, acc_o, xc, warp >> 1, warp & 1, CtaSync{}, v);
 }
 
 // Analysis pre-fold of NO program outputs gq[quadrant][o] at the warp's angles (tile tau, parity half)
 // into ps slots slot0 .. slot0+NO-1 ([slot][class][NT][2][32]).
 template <int M, int NO>
 __device__ __forceinline__ void tf_prefold(const double (&gq)[4][NO], double *ps, int slot0) {
-  constexpr int NT = TfGeo<M>::NT;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int t = warp >> 1, e = warp & 1;
-#pragma unroll
-  for (int o = 0; o < NO; ++o) {
-    const double s14 = gq[0][o] + gq[3][o], d14 = gq[0][o] - gq[3][o];
-    const double s23 = gq[1][o] + gq[2][o], d32 = gq[2][o] - gq[1][o];
-    double *dst = ps + ((size_t)(((slot0 + o) * 4) * NT + t) * 2 + e) * 32 + lane;
-    const size_t cstride = (size_t)NT * 2 * 32;
-    dst[0] = s14 + s23;            // PE
-    dst[cstride] = s14 - s23;      // PO
-    dst[2 * cstride] = d14 + d32;  // QE
-    dst[3 * cstride] = d14 - d32;  // QO
-  }
+  const int warp = threadIdx.x >> 5;
+  prefold_store<TfGeo<M>::NT, NO>(gq, ps, slot0, warp >> 1, warp & 1);
 }
 
 template <int NO>
@@ -1574,7 +1502,8 @@ int launch_fast(const ProgArgs &a, cudaStream_t st) {
   if (a.np == 0) return SFNL_OK;
   const Geo g = make_geo(a.m);
   if (g.N != a.N) return set_error(SFNL_ERR_ARG, "FAST form: unexpected grid length");
-  if (a.op == OP_BUNDLE && a.m == 64 && a.batch == 1 && a.out_ps == 1) return launch_bundle_tf(a, st);
+  if (a.op == OP_BUNDLE && a.m == 64 && a.batch == 1 && a.out_ps == 1)
+    return bundle_kernel() == SFNL_BUNDLE_THIRD_FOLD ? launch_bundle_tf(a, st) : launch_bundle_r3(a, st);
   Tables T;
   int rc = get_tables(g, &T);
   if (rc) return rc;
@@ -1692,6 +1621,7 @@ __global__ void build_tables_kernel(double *syn, double *ana, FastArgs g) {
 }  // namespace
 
 void fast_release_tables() {
+  r3_release_tables();
   std::lock_guard<std::mutex> lk(g_tab_mu);
   int prev = 0;
   cudaGetDevice(&prev);

@@ -120,6 +120,110 @@ __host__ __device__ constexpr int tf_aoff(int m, int gr) {
 // with the analysis weights).  Cached per (device, m).
 int get_tf_tables(const Geo &g, Tables *out);
 
+// Barriers of the exchanges: the whole CTA, or one of three groups of 4 warps on its own named barrier.
+struct CtaSync {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+struct GroupSync {  // groups 0, 1, 2 of 4 warps on barriers 1, 2, 3 (immediate ids: the kernel reserves 4)
+  int group;
+  __device__ __forceinline__ void operator()() const {
+    if (group == 0)
+      asm volatile("bar.sync 1, 128;" ::: "memory");
+    else if (group == 1)
+      asm volatile("bar.sync 2, 128;" ::: "memory");
+    else
+      asm volatile("bar.sync 3, 128;" ::: "memory");
+  }
+};
+
+// Both exchanges of the third fold inside a group of 2*NT warps, warp (tau, half) holding the even part and
+// odd class of half `half` (0 cosine, 1 sine) on angle tile tau (tf_synth).  X1 assembles the even class on
+// the warp's own tile from the two parts (a first-half tile adds its partner's part at the same lane; a
+// second-half tile takes both parts at the mirror lane (lane ^ 3) and parity 1 - e: CE = E0 - E2,
+// SE = S2 - S0); X2 swaps half of the folded sums (A = CE+CO, B = CE-CO against C = SE+SO, D = SO-SE) with
+// the other half, so that half e ends with the four quadrant values v[r][f] of its angles of parity e.
+// xc (the group's own) holds 2 * NT * NG * 64 doubles; call after a barrier of the group that ends the
+// reads of whatever xc overlays.  Returns after the X2 reads.
+template <int NT, int NG, typename Sync>
+__device__ __forceinline__ void fold_exchange(const double (&acc_e)[NG][2], const double (&acc_o)[NG][2], double *xc,
+                                              int tau, int half, Sync sync, double (&v)[4][NG]) {
+  constexpr int NH = NT / 2;
+  const int lane = threadIdx.x & 31;
+  const bool first = tau < NH;
+  double acc[NG][2][2];  // [f][even, odd class][e]
+  {
+    double *x1 = xc + (size_t)((tau * 2 + half) * NG) * 64 + lane;
+#pragma unroll
+    for (int f = 0; f < NG; ++f) {
+      x1[(f * 2 + 0) * 32] = acc_e[f][0];
+      x1[(f * 2 + 1) * 32] = acc_e[f][1];
+    }
+    sync();
+    const double *own = xc + (size_t)((tau * 2 + half) * NG) * 64;
+    const double *mate = xc + (size_t)(((NT - 1 - tau) * 2 + half) * NG) * 64;
+#pragma unroll
+    for (int f = 0; f < NG; ++f)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        double ev;
+        if (first) {
+          ev = acc_e[f][e] + mate[(f * 2 + e) * 32 + lane];
+        } else {
+          const double p0m = mate[(f * 2 + 1 - e) * 32 + (lane ^ 3)];  // E0 / S0 at the mirror angle
+          const double p2m = own[(f * 2 + 1 - e) * 32 + (lane ^ 3)];   // E2 / S2 at the mirror angle
+          ev = half ? p2m - p0m : p0m - p2m;
+        }
+        acc[f][0][e] = ev;
+        acc[f][1][e] = acc_o[f][e];
+      }
+    sync();  // X1 is read: X2 reuses xc
+  }
+  auto pair_sums = [&](int f, int e, double &X, double &Y) {
+    const double lo = e ? acc[f][0][1] : acc[f][0][0], hi = e ? acc[f][1][1] : acc[f][1][0];
+    X = lo + hi;
+    Y = half ? hi - lo : lo - hi;
+  };
+  double *xw = xc + (size_t)tau * 2 * NG * 64 + lane;  // [writer half][f][X, Y][32]
+#pragma unroll
+  for (int f = 0; f < NG; ++f) {
+    double X, Y;
+    pair_sums(f, 1 - half, X, Y);
+    xw[((half * NG + f) * 2 + 0) * 32] = X;
+    xw[((half * NG + f) * 2 + 1) * 32] = Y;
+  }
+  sync();
+  const int e = half;
+#pragma unroll
+  for (int f = 0; f < NG; ++f) {
+    double X, Y;
+    pair_sums(f, e, X, Y);
+    const double Xp = xw[(((1 - half) * NG + f) * 2 + 0) * 32], Yp = xw[(((1 - half) * NG + f) * 2 + 1) * 32];
+    const double A = half ? Xp : X, B = half ? Yp : Y, C = half ? X : Xp, D = half ? Y : Yp;
+    v[0][f] = A + C;  // theta
+    v[1][f] = B + D;  // pi - theta
+    v[2][f] = B - D;  // pi + theta
+    v[3][f] = A - C;  // 2 pi - theta
+  }
+}
+
+// Analysis pre-fold of NO program outputs gq[quadrant][o] at angle tile t, parity e of the lane into ps
+// slots slot0 .. slot0+NO-1 ([slot][class PE, PO, QE, QO][NT][2][32]).
+template <int NT, int NO>
+__device__ __forceinline__ void prefold_store(const double (&gq)[4][NO], double *ps, int slot0, int t, int e) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 0; o < NO; ++o) {
+    const double s14 = gq[0][o] + gq[3][o], d14 = gq[0][o] - gq[3][o];
+    const double s23 = gq[1][o] + gq[2][o], d32 = gq[2][o] - gq[1][o];
+    double *dst = ps + ((size_t)(((slot0 + o) * 4) * NT + t) * 2 + e) * 32 + lane;
+    const size_t cstride = (size_t)NT * 2 * 32;
+    dst[0] = s14 + s23;            // PE
+    dst[cstride] = s14 - s23;      // PO
+    dst[2 * cstride] = d14 + d32;  // QE
+    dst[3 * cstride] = d14 - d32;  // QO
+  }
+}
+
 // Slot of (k-value kq, point p) in a 32-double A-fragment block [4 k][8 points].  A lane (g, q) of
 // m8n8k4 reads (q, g); a 64-bit shared load is served per half-warp, and with the plain order q*8 + g
 // the lanes q and q + 2 of a half-warp hit the same banks (two wavefronts per half-warp).  Flipping

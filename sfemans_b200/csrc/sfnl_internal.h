@@ -22,6 +22,9 @@ int num_sms();
 // Kernel families.
 int launch_grid(const ProgArgs &a, cudaStream_t st);   // sfnl_grid.cu
 int launch_fast(const ProgArgs &a, cudaStream_t st);   // sfnl_fast.cu
+int launch_bundle_r3(const ProgArgs &a, cudaStream_t st);  // sfnl_r3.cu: the MHD bundle at m = 64
+void r3_release_tables();                               // sfnl_r3.cu
+int bundle_kernel();                                    // sfnl_capi.cu: SFNL_BUNDLE_* in use
 bool fast_supported(int op, int m, int N_int);          // sfnl_fast.cu
 int fast_grid_length(int m);                            // sfnl_fast.cu
 void fast_release_tables();                             // sfnl_fast.cu

@@ -55,6 +55,17 @@ def test_product_argument_errors(args, code):
     assert sf.last_error()
 
 
+def test_bundle_kernel_switch():
+    prev = sf.set_bundle_kernel(sf.BUNDLE_THIRD_FOLD)
+    try:
+        assert prev in (sf.BUNDLE_RESIDUE, sf.BUNDLE_THIRD_FOLD)
+        assert sf.set_bundle_kernel(sf.BUNDLE_RESIDUE) == sf.BUNDLE_THIRD_FOLD
+        assert sf.lib().sfnl_set_bundle_kernel(2) == -1 and sf.last_error()
+        assert sf.set_bundle_kernel(sf.BUNDLE_RESIDUE) == sf.BUNDLE_RESIDUE  # unchanged by the refusal
+    finally:
+        sf.set_bundle_kernel(prev)
+
+
 def test_zero_points_is_a_no_op():
     assert sf.lib().sfnl_product_f64(0, NULL, NULL, NULL, 0, 4, 6, 0, 0, NULL) == 0
 

@@ -124,6 +124,27 @@ def test_mhd_bundle(npts, m, algo):
         assert R.rel_l2(host(o), r) <= FP64_TOL
 
 
+@pytest.mark.parametrize("npts", [1, 7, 61, 3001, 100_003])
+def test_bundle_kernels_agree(npts):
+    # the two kernels of the m = 64 bundle (grid split into its residue classes; one 192-angle transform)
+    # against each other, and against the oracle where it is cheap; odd counts take the 8-byte copies
+    m, pad = 64, 96
+    f = [R.synthetic_field(npts, 6, m, 0.1, 700 + i) for i in range(5)]
+    d = [dev(x) for x in f]
+    prev = sf.set_bundle_kernel(sf.BUNDLE_THIRD_FOLD)
+    try:
+        tf = [host(o) for o in sf.bundle_mhd(*d, m_max_pad=pad)]
+        assert sf.set_bundle_kernel(sf.BUNDLE_RESIDUE) == sf.BUNDLE_THIRD_FOLD
+        r3 = [host(o) for o in sf.bundle_mhd(*d, m_max_pad=pad)]
+    finally:
+        sf.set_bundle_kernel(prev)
+    refs = R.mhd_bundle(*f, pad) if npts <= 3001 else None
+    for i in range(4):
+        assert R.rel_l2(r3[i], tf[i]) <= 1e-13
+        if refs is not None:
+            assert R.rel_l2(r3[i], refs[i]) <= FP64_TOL
+
+
 @pytest.mark.parametrize("npts,m", [(90, 10), (3001, 64)])
 def test_host_bundle_entry_point(npts, m):
     import ctypes
