@@ -9,6 +9,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <tuple>
 
 #include "sfnl_fold.cuh"
 #include "sfnl_internal.h"
@@ -63,6 +64,7 @@ struct LargeArgs {
   // third fold (NT even): groups 0 CE0, 1 CE2, 2 CO, 3 SE0, 4 SE2, 5 SO
   int tkoff[7], tks[6], tnuoff[7], tnu[6], taoff[7], tke[3];
   int asteps;  // k-steps of one analysis-table variant
+  int nyq;     // residue pass: the sine row and output of mode 0 carry the residue grid's Nyquist mode
 };
 
 // PT 8-point tiles of one field per CTA: each B fragment of the DFT table (read from L2) feeds PT
@@ -202,7 +204,7 @@ __global__ void __launch_bounds__(kLargeSynMaxWarps * 32, 1) large_syn_tf_kernel
       const int keg = gr % 3 == 0 ? a.tke[0] : gr % 3 == 1 ? a.tke[1] : a.tke[2];
       const int k = r - 4 * kg, n = tf_mode(gr, k);
       double *dst = dst0 + (size_t)ks * 32 + a_frag_slot(r & 3, pc & 7);
-      const bool live = k < keg && !(gr == 3 && k == 0);  // the sine of mode 0 is ignored
+      const bool live = k < keg && (a.nyq || !(gr == 3 && k == 0));  // the sine of mode 0 is ignored
       const double *src = base + (int64_t)n * ldm + (gr >= 3 ? a.in_sin : 0);
       if (live && v16) {
         cp_async16(dst, src);
@@ -421,7 +423,7 @@ __global__ void __launch_bounds__(kLargeProdWarps * 32) large_prod_tf_kernel(con
         const int og = O0 + o;
         double *dst = a.out[og] + (int64_t)b * a.out_bs[og] + p * a.out_ps + (int64_t)n * a.out_ldm[og] +
                       (gr >= 3 ? a.out_sin : 0);
-        *dst = (gr >= 3 && n == 0) ? 0.0 : y[j][o][h];
+        *dst = (gr >= 3 && n == 0 && !a.nyq) ? 0.0 : y[j][o][h];
       }
     }
   }
@@ -514,15 +516,16 @@ __global__ void __launch_bounds__(kLargeProdWarps * 32) large_prod_kernel(const 
   }
 }
 
-// workspace of the grid values, one per (device, stream): calls on different streams do not share it
+// workspaces, one per (device, stream, use): calls on different streams do not share them.  Use 0: the
+// grid values; 1: the residue coefficients and sums of launch_large_r3.
 std::mutex g_lws_mu;
-std::map<std::pair<int, cudaStream_t>, std::pair<double *, size_t>> g_lws;
+std::map<std::tuple<int, cudaStream_t, int>, std::pair<double *, size_t>> g_lws;
 
-int large_workspace(cudaStream_t st, size_t bytes, double **out) {
+int large_workspace(cudaStream_t st, size_t bytes, double **out, int use = 0) {
   int dev = 0;
   cudaGetDevice(&dev);
   std::lock_guard<std::mutex> lk(g_lws_mu);
-  auto &w = g_lws[{dev, st}];
+  auto &w = g_lws[{dev, st, use}];
   if (w.second < bytes) {
     if (w.first) {
       cudaStreamSynchronize(st);  // the previous call on this stream may still read it
@@ -632,32 +635,45 @@ constexpr int64_t kLargeMinChunk = 4096;
 
 }  // namespace
 
+void large_r3_release_tables();
+
 void large_release_workspaces() {
   std::lock_guard<std::mutex> lk(g_lws_mu);
   int prev = 0;
   cudaGetDevice(&prev);
   for (auto &kv : g_lws)
     if (kv.second.first) {
-      cudaSetDevice(kv.first.first);
+      cudaSetDevice(std::get<0>(kv.first));
       cudaFree(kv.second.first);  // waits for the work still reading it
     }
   g_lws.clear();
   cudaSetDevice(prev);
+  large_r3_release_tables();
 }
+
+namespace {
+
+struct LargePlan {
+  int N, NT;                 // grid length and quadrant angle tiles of the pass
+  int mt;                    // modes of its third-fold row and output groups
+  double *syn, *ana;         // its tables
+};
 
 // The two-kernel form: per point chunk, the batch-invariant fields (base state) once, then the batch
 // entries in groups of kb: one synthesis launch for the group's own fields (blockIdx.z = entry) and one
 // launch per group of three outputs (blockIdx.y = entry).  The grid-value workspace holds the shared
 // fields and kb entries' own fields of one point chunk: kb = the whole batch when a chunk of at least
 // kLargeMinChunk points fits the batched workspace bound, else as many entries as such a chunk allows.
-int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStream_t st) {
+// rp: a residue pass (launch_large_r3): the residue grid's geometry and tables, the Nyquist mode in the
+// sine row of mode 0, no analysis weights and no cotangent weights (both applied outside).
+int run_large(const ProgArgs &a, const Geo &g, const Tables &T, const LargePlan *rp, cudaStream_t st) {
   const int ni = op_nin(a.op), no = op_nout(a.op);
   int nshared = 0, nown = 0;  // batch-invariant fields take the first G slots, the batched ones the next
   int64_t gslot[kMaxIn];
   for (int f = 0; f < ni; ++f) gslot[f] = a.in_bs[f] == 0 ? nshared++ : -1;
   for (int f = 0; f < ni; ++f)
     if (gslot[f] < 0) gslot[f] = nshared + nown++;
-  const size_t field_bytes = sizeof(double) * (size_t)g.N;  // one field's grid values per point
+  const size_t field_bytes = sizeof(double) * (size_t)(rp ? rp->N : g.N);  // one field's grid values per point
   size_t cap = kLargeWorkspaceBytes;
   int kb = 1;
   if (a.batch > 1 && nown > 0) {
@@ -682,13 +698,18 @@ int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStre
   double *G = nullptr;
   if (int rc = large_workspace(st, per_point * (size_t)chunk, &G)) return rc;
   // the third fold needs mirror pairs of angle tiles
-  const bool tf = g.NT % 2 == 0;
+  const int NT = rp ? rp->NT : g.NT, mt = rp ? rp->mt : g.m;
+  const bool tf = NT % 2 == 0;
   Tables TT = T;
-  if (tf)
+  if (rp) {
+    TT.syn = rp->syn;
+    TT.ana = rp->ana;
+  } else if (tf) {
     if (int rc = get_tf_tables(g, &TT)) return rc;
-  const bool adj_out = op_adjoint_out(a.op);
+  }
+  const bool adj_out = rp ? true : op_adjoint_out(a.op);
   unsigned adj = 0;
-  for (int f = 0; f < ni; ++f)
+  for (int f = 0; f < ni && !rp; ++f)
     if (op_adjoint_in(a.op, f)) adj |= 1u << f;
   for (int64_t c0 = 0; c0 < a.np; c0 += chunk) {
     LargeArgs la;
@@ -712,7 +733,7 @@ int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStre
       la.out_ldm[o] = a.out_ldm[o];
       la.out_bs[o] = a.out_bs[o];
     }
-    la.NT = g.NT;
+    la.NT = NT;
     la.NU_tot = g.NU_tot;
     la.KS_tot = g.KS_tot;
     for (int c = 0; c < 4; ++c) {
@@ -727,17 +748,20 @@ int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStre
     la.syn = TT.syn;
     la.ana = TT.ana;
     la.G = G;
+    // third-fold row and output groups of mt modes; the analysis k-steps of a group over NT angle tiles
+    la.taoff[0] = 0;
     for (int gr = 0; gr < 7; ++gr) {
-      la.tkoff[gr] = tf_koff(g.m, gr);
-      la.tnuoff[gr] = tf_nuoff(g.m, gr);
-      la.taoff[gr] = tf_aoff(g.m, gr);
+      la.tkoff[gr] = tf_koff(mt, gr);
+      la.tnuoff[gr] = tf_nuoff(mt, gr);
+      if (gr > 0) la.taoff[gr] = la.taoff[gr - 1] + tf_NU(mt, gr - 1) * ((gr - 1) % 3 == 2 ? 2 * NT : NT);
     }
     for (int gr = 0; gr < 6; ++gr) {
-      la.tks[gr] = tf_KS(g.m, gr);
-      la.tnu[gr] = tf_NU(g.m, gr);
+      la.tks[gr] = tf_KS(mt, gr);
+      la.tnu[gr] = tf_NU(mt, gr);
     }
-    for (int gr = 0; gr < 3; ++gr) la.tke[gr] = tf_ke(g.m, gr);
-    la.asteps = tf_aoff(g.m, 6);
+    for (int gr = 0; gr < 3; ++gr) la.tke[gr] = tf_ke(mt, gr);
+    la.asteps = la.taoff[6];
+    la.nyq = rp ? 1 : 0;
     // the batch-invariant fields, once per chunk
     int k = 0;
     for (int f = 0; f < ni; ++f)
@@ -756,6 +780,259 @@ int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStre
     }
   }
   return SFNL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the grid's three residue classes (m = 256, 512)
+// ---------------------------------------------------------------------------
+// On theta_j = pi(2j+1)/N with N = 3m, j = 3i + r gives theta_j = phi_i + d_r, phi_i = pi(2i+1)/m the offset
+// m-angle grid and d_r = 2 pi (r-1)/N.  A field Re sum_n z_n e^{i n theta} (z_n = a_n - i b_n, n < m) is on
+// residue r the series of y_n = z_n e^{i n d_r} on phi, where e^{i m phi_i} = -1 folds the modes k and m - k
+// into alpha_k - i beta_k = y_k - conj(y_{m-k}) (k = 1 .. m/2 - 1), alpha_0 = a_0, and leaves mode m/2 as a
+// sine (cos(m/2 phi_i) = 0): beta_{m/2} = -Im y_{m/2}.  Each residue is a transform of m/2 complex modes on m
+// angles, third-folded like the whole grid: half the DMMAs of the 3m-angle transform.  With C^r_k, S^r_k the
+// residue's cosine and sine sums of a product, sum_j p_j e^{-i n theta_j} = sum_r w^{n(1-r)} P^r_n with
+// w = e^{2 pi i/N}, P^r_k = C^r_k - i S^r_k, P^r_{m-k} = -conj(P^r_k) and P^r_{m/2} = -i S^r_{m/2}.  The
+// residue passes run the two kernels above on the m-angle grid (mode m/2's sine in the sine row of mode 0),
+// between a kernel that forms the residue's coefficients and one that adds its share to the outputs.
+// At m = 128 the extra passes over the coefficients and sums cost more than the DMMAs saved (cross product
+// at 100k points 2.65 -> 2.93 ms, 16 tangents 44.7 -> 52.5 ms); from m = 256 on the residues win (the
+// 16-tangent MHD JVP at 50k points 129 -> 100 ms, the cross product at m = 512 29.0 -> 24.1 ms).
+bool large_r3_supported(int m, int N) { return m >= 256 && m <= 512 && m % 64 == 0 && N == 3 * m; }
+
+struct R3LargeTab {
+  double *base = nullptr;  // syn, ana (two equal variants, no weights), tw [m][2]
+  double *syn = nullptr, *ana = nullptr;
+  const double *tw = nullptr;
+};
+std::mutex g_r3l_mu;
+std::map<std::pair<int, int>, R3LargeTab> g_r3l;  // (device, m) -> tables
+
+__host__ __device__ constexpr int r3l_mode(int gr, int k, int mh) { return (gr == 3 && k == 0) ? mh : tf_mode(gr, k); }
+
+// Third-fold tables of the residue grid (m angles, quadrant tiles NT = m/32, row and output groups of m/2
+// modes with mode m/2 as the sine of group 3's k = 0), laid out like get_tf_tables', and the twiddles
+// cos, sin of 2 pi n / N for n < m.
+int get_large_r3_tables(int m, int N, R3LargeTab *out) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_r3l_mu);
+  auto it = g_r3l.find({dev, m});
+  if (it != g_r3l.end()) {
+    *out = it->second;
+    return SFNL_OK;
+  }
+  const int mh = m / 2, NT = m / 32;
+  const long double pi = acosl(-1.0L);
+  auto phi = [&](int j) { return pi * (long double)(2 * j + 1) / (long double)m; };
+  const int ks_tot = tf_koff(mh, 6);
+  int asteps = 0, aoff[7];
+  for (int gr = 0; gr < 6; ++gr) {
+    aoff[gr] = asteps;
+    asteps += tf_NU(mh, gr) * (gr % 3 == 2 ? 2 * NT : NT);
+  }
+  aoff[6] = asteps;
+  const size_t nsyn = (size_t)ks_tot * NT * 32, nana = (size_t)2 * asteps * 32;
+  std::vector<double> h(nsyn + nana + 2 * (size_t)m, 0.0);
+  for (int gr = 0; gr < 6; ++gr)
+    for (int s = 0; s < tf_KS(mh, gr); ++s)
+      for (int t = 0; t < NT; ++t)
+        for (int l = 0; l < 32; ++l) {
+          const int k = 4 * s + (l & 3);
+          if (k >= tf_ke(mh, gr)) continue;
+          const long double x = (long double)r3l_mode(gr, k, mh) * phi(8 * t + (l >> 2));
+          h[((size_t)(tf_koff(mh, gr) + s) * NT + t) * 32 + l] = (double)(gr < 3 ? cosl(x) : sinl(x));
+        }
+  for (int var = 0; var < 2; ++var)
+    for (int gr = 0; gr < 6; ++gr) {
+      const int TE = gr % 3 == 2 ? 2 * NT : NT;
+      for (int u = 0; u < tf_NU(mh, gr); ++u)
+        for (int te = 0; te < TE; ++te)
+          for (int l = 0; l < 32; ++l) {
+            const int kk = 8 * u + (l >> 2);
+            if (kk >= tf_ke(mh, gr)) continue;
+            const long double x = (long double)r3l_mode(gr, kk, mh) * phi(8 * (te >> 1) + 2 * (l & 3) + (te & 1));
+            h[nsyn + ((size_t)var * asteps + aoff[gr] + u * TE + te) * 32 + l] = (double)(gr < 3 ? cosl(x) : sinl(x));
+          }
+    }
+  for (int n = 0; n < m; ++n) {
+    h[nsyn + nana + 2 * n] = (double)cosl(2.0L * pi * n / (long double)N);
+    h[nsyn + nana + 2 * n + 1] = (double)sinl(2.0L * pi * n / (long double)N);
+  }
+  R3LargeTab T;
+  if (cudaMalloc(&T.base, h.size() * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(SFNL_ERR_ALLOC, "cudaMalloc of the residue-grid tables failed");
+  }
+  if (cudaMemcpy(T.base, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    return set_error(SFNL_ERR_CUDA, "upload of the residue-grid tables failed");
+  T.syn = T.base;
+  T.ana = T.base + nsyn;
+  T.tw = T.base + nsyn + nana;
+  g_r3l[{dev, m}] = T;
+  *out = T;
+  return SFNL_OK;
+}
+
+// The three residues of one input field (batch entry blockIdx.z) at the chunk's points: thread (point, k)
+// forms alpha_k, beta_k of each residue from modes k and m - k (k = 0: alpha_0 and beta_{m/2}) into
+// y + r * ystride, each (npc, 2, m/2): cosine k at 2k npc, sine k at (2k + 1) npc, the sine row 0 holding
+// beta_{m/2}.  Cotangents (adj) take the analysis weights 1/N (n = 0), 2/N first.
+__global__ void large_r3_coef_kernel(const double *x, int64_t ldm, int64_t xsin, int64_t xbs, double *y, int64_t ystride,
+                                     int64_t npc, int m, int adj, double invN, const double *tw) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npc) return;
+  const int k = blockIdx.y, mh = m >> 1;
+  const double *xp = x + (int64_t)blockIdx.z * xbs + p;
+  double *yp = y + (int64_t)blockIdx.z * m * npc + p;
+  auto w = [&](int n) { return adj ? (n == 0 ? invN : 2.0 * invN) : 1.0; };
+  // residue r: twiddle e^{i n (r-1) 2 pi / N} = c_n + i (r-1) s_n
+  if (k == 0) {
+    const double a0 = xp[0] * w(0), am = xp[(int64_t)mh * ldm] * w(mh), bm = xp[(int64_t)mh * ldm + xsin] * w(mh);
+    const double c = __ldg(tw + 2 * mh), s = __ldg(tw + 2 * mh + 1);
+    yp[0] = yp[ystride] = yp[2 * ystride] = a0;
+    yp[npc] = fma(bm, c, am * s);         // r = 0
+    yp[ystride + npc] = bm;               // r = 1
+    yp[2 * ystride + npc] = fma(bm, c, -am * s);  // r = 2
+  } else {
+    const int k2 = m - k;
+    const double a = xp[(int64_t)k * ldm] * w(k), b = xp[(int64_t)k * ldm + xsin] * w(k);
+    const double a2 = xp[(int64_t)k2 * ldm] * w(k2), b2 = xp[(int64_t)k2 * ldm + xsin] * w(k2);
+    const double c = __ldg(tw + 2 * k), s = __ldg(tw + 2 * k + 1), c2 = __ldg(tw + 2 * k2), s2 = __ldg(tw + 2 * k2 + 1);
+    // alpha = (a C + b S) - (a' C' + b' S'), beta = (b C - a S) + (b' C' - a' S') with C = c, S = (r-1) s
+    const double X = fma(a, c, -a2 * c2), Y = fma(b, s, -b2 * s2), Z = fma(b, c, b2 * c2), W = fma(a, s, a2 * s2);
+    const int64_t ic = (int64_t)(2 * k) * npc, is = (int64_t)(2 * k + 1) * npc;
+    yp[ic] = X - Y;
+    yp[is] = Z + W;
+    yp[ystride + ic] = a - a2;
+    yp[ystride + is] = b + b2;
+    yp[2 * ystride + ic] = X + Y;
+    yp[2 * ystride + is] = Z - W;
+  }
+}
+
+// One output (batch entry blockIdx.z) from the three residues' sums R + r * rstride, each (npc, 2, m/2) with
+// the sine row 0 holding S_{m/2}: thread (point, k) writes modes k and m - k (k = 0: modes 0 and m/2).
+// w = 2/N (or 1 without analysis weights), w0 = 1/N (or 1).
+__global__ void large_r3_out_kernel(const double *R, int64_t rstride, double *out, int64_t ldm, int64_t osin, int64_t ops,
+                                    int64_t obs, int64_t npc, int m, double w, double w0, const double *tw) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npc) return;
+  const int k = blockIdx.y, mh = m >> 1;
+  const double *rp = R + (int64_t)blockIdx.z * m * npc + p;
+  double *op = out + (int64_t)blockIdx.z * obs + p * ops;
+  auto put = [&](int n, int sine, double v) { op[(int64_t)n * ldm + (sine ? osin : 0)] = v; };
+  if (k == 0) {
+    const double c = __ldg(tw + 2 * mh), s = __ldg(tw + 2 * mh + 1);
+    const double S0 = rp[npc], S1 = rp[rstride + npc], S2 = rp[2 * rstride + npc];
+    put(0, 0, w0 * (rp[0] + rp[rstride] + rp[2 * rstride]));
+    put(0, 1, 0.0);
+    put(mh, 0, w * (s * (S0 - S2)));
+    put(mh, 1, w * fma(c, S0 + S2, S1));
+  } else {
+    const int k2 = m - k;
+    const int64_t ic = (int64_t)(2 * k) * npc, is = (int64_t)(2 * k + 1) * npc;
+    const double C0 = rp[ic], C1 = rp[rstride + ic], C2 = rp[2 * rstride + ic];
+    const double S0 = rp[is], S1 = rp[rstride + is], S2 = rp[2 * rstride + is];
+    const double c = __ldg(tw + 2 * k), s = __ldg(tw + 2 * k + 1), c2 = __ldg(tw + 2 * k2), s2 = __ldg(tw + 2 * k2 + 1);
+    const double CS = C0 + C2, CD = C0 - C2, SS = S0 + S2, SD = S0 - S2;
+    put(k, 0, w * fma(s, SD, fma(c, CS, C1)));
+    put(k, 1, w * fma(-s, CD, fma(c, SS, S1)));
+    put(k2, 0, w * fma(s2, SD, fma(-c2, CS, -C1)));
+    put(k2, 1, w * fma(s2, CD, fma(c2, SS, S1)));
+  }
+}
+
+// The two-kernel form on the residue grids: per point chunk, the three residues' coefficients of every
+// input field in one pass (m doubles per point, field instance and residue), the residue passes of the
+// program (run_large; sums into m doubles per point, output instance and residue), and the outputs from
+// the three residues' sums in one pass.
+int launch_large_r3(const ProgArgs &a, const Geo &g, cudaStream_t st) {
+  const int m = a.m, mh = m / 2, N = g.N, ni = op_nin(a.op), no = op_nout(a.op);
+  R3LargeTab T;
+  if (int rc = get_large_r3_tables(m, N, &T)) return rc;
+  const LargePlan rp{m, m / 32, mh, T.syn, T.ana};
+  int64_t inst_in = 0;
+  for (int f = 0; f < ni; ++f) inst_in += a.in_bs[f] ? a.batch : 1;
+  const int64_t inst_out = (int64_t)no * a.batch;
+  const size_t per_point = sizeof(double) * (size_t)m * 3 * (size_t)(inst_in + inst_out);
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+    cudaGetLastError();
+    free_b = 0;
+  }
+  size_t cap = free_b / 4;
+  if (cap > (size_t(32) << 30)) cap = size_t(32) << 30;
+  if (cap < (size_t(1) << 30)) cap = size_t(1) << 30;
+  int64_t chunk = (int64_t)(cap / per_point);
+  chunk = (chunk / 32) * 32;
+  if (chunk < 32) chunk = 32;
+  if (chunk > a.np) chunk = ((a.np + 7) / 8) * 8;
+  double *W = nullptr;
+  if (int rc = large_workspace(st, per_point * (size_t)chunk, &W, 1)) return rc;
+  const bool adj_out = op_adjoint_out(a.op);
+  const double invN = 1.0 / N, w = adj_out ? 1.0 : 2.0 * invN, w0 = adj_out ? 1.0 : invN;
+  constexpr int kThreads = 256;
+  for (int64_t c0 = 0; c0 < a.np; c0 += chunk) {
+    const int64_t npc = a.np - c0 < chunk ? a.np - c0 : chunk;
+    const unsigned bx = (unsigned)((npc + kThreads - 1) / kThreads);
+    // residue r's arrays: inputs at W + r * rin, outputs at W + 3 rin + r * rout
+    const int64_t rin = inst_in * m * npc, rout = inst_out * m * npc;
+    ProgArgs ar = a;
+    ar.np = npc;
+    ar.out_ps = 1;
+    int64_t off = 0;
+    for (int f = 0; f < ni; ++f) {
+      const int nb = a.in_bs[f] ? a.batch : 1;
+      large_r3_coef_kernel<<<dim3(bx, (unsigned)mh, (unsigned)nb), kThreads, 0, st>>>(
+          a.in[f] + c0, a.in_ldm[f], a.np, a.in_bs[f], W + off, rin, npc, m, op_adjoint_in(a.op, f) ? 1 : 0, invN, T.tw);
+      ar.in[f] = W + off;
+      ar.in_ldm[f] = 2 * npc;
+      ar.in_bs[f] = a.in_bs[f] ? (int64_t)m * npc : 0;
+      off += (int64_t)nb * m * npc;
+    }
+    if (int rc = check_launch("large-m residue coefficients")) return rc;
+    off = 3 * rin;
+    for (int o = 0; o < no; ++o) {
+      ar.out[o] = W + off;
+      ar.out_ldm[o] = 2 * npc;
+      ar.out_bs[o] = (int64_t)m * npc;
+      off += (int64_t)a.batch * m * npc;
+    }
+    for (int r = 0; r < 3; ++r) {
+      ProgArgs rr = ar;
+      for (int f = 0; f < ni; ++f) rr.in[f] = ar.in[f] + r * rin;
+      for (int o = 0; o < no; ++o) rr.out[o] = ar.out[o] + r * rout;
+      if (int rc = run_large(rr, g, Tables{}, &rp, st)) return rc;
+    }
+    for (int o = 0; o < no; ++o)
+      large_r3_out_kernel<<<dim3(bx, (unsigned)mh, (unsigned)a.batch), kThreads, 0, st>>>(
+          ar.out[o], rout, a.out[o] + c0 * a.out_ps, a.out_ldm[o], a.np * a.out_ps, a.out_ps, a.out_bs[o], npc, m, w, w0,
+          T.tw);
+    if (int rc = check_launch("large-m residue outputs")) return rc;
+  }
+  return SFNL_OK;
+}
+
+}  // namespace
+
+void large_r3_release_tables() {
+  std::lock_guard<std::mutex> lk(g_r3l_mu);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  for (auto &kv : g_r3l) {
+    cudaSetDevice(kv.first.first);
+    cudaFree(kv.second.base);
+  }
+  g_r3l.clear();
+  cudaSetDevice(prev);
+}
+
+// The two-kernel form: on the grid's three residue classes when the grid is 3m angles and m >= 256 (half
+// the DMMAs, launch_large_r3), else on the whole grid.
+int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStream_t st) {
+  if (large_r3_supported(a.m, g.N)) return launch_large_r3(a, g, st);
+  return run_large(a, g, T, nullptr, st);
 }
 
 }  // namespace sfnl

@@ -242,7 +242,9 @@ def test_finite_check_mode():
         sf.set_check_finite(False)
 
 
-LARGE = [(37, 100, 150), (20, 128, 192), (9, 256, 384)]
+# m = 100: the whole grid, odd tile count; 128: the whole grid with the third fold; 256 and 512: the grid's
+# three residue classes
+LARGE = [(37, 100, 150), (20, 128, 192), (9, 256, 384), (5, 512, 768)]
 
 
 @pytest.mark.parametrize("op", [0, 1, 2])
