@@ -446,38 +446,47 @@ def _e2e_bundle(sf, torch, ins, npts, m, pad, form, steps, world, dist):
         dist.all_reduce(dt_t, op=dist.ReduceOp.MAX)
     dt = float(dt_t.item())
     sf.finalize()
-    pcie = _pcie_both_gbs(torch, h_in[0], h_out[0])
-    moved = 8 * npts * m * 50
-    return {"value": world * npts * m / dt, "unit": UNIT, "h2d_bytes_per_step": 8 * npts * m * 30,
-            "d2h_bytes_per_step": 8 * npts * m * 20, "ms_per_step": dt * 1e3,
+    h2d_b, d2h_b = 8 * npts * m * 30, 8 * npts * m * 20
+    rates = _pcie_rates(torch, h_in[0], h_out[0])
+    # the copies cannot end sooner than the slowest of: H2D alone, D2H alone, both directions at once
+    bound_s = max(h2d_b / rates["h2d"], d2h_b / rates["d2h"], (h2d_b + d2h_b) / rates["both"]) / 1e9
+    return {"value": world * npts * m / dt, "unit": UNIT, "h2d_bytes_per_step": h2d_b,
+            "d2h_bytes_per_step": d2h_b, "ms_per_step": dt * 1e3,
             "last_step_device_s": {"copies": t_split[0], "kernels": t_split[1],
                                    "note": "sums over the call's chunks on four streams (overlapping)"},
-            "roofline": {"bound": "pcie", "achieved": moved / dt / 1e9, "peak": pcie, "unit": "GB/s",
-                         "frac": moved / dt / 1e9 / pcie if pcie else None,
-                         "peak_source": "pinned copies measured in this run, both directions at once"},
+            "roofline": {"bound": "pcie", "bound_ms": bound_s * 1e3, "frac": bound_s / dt,
+                         "pinned_copy_gbs": rates,
+                         "peak_source": "pinned copies of 2 GB measured in this run: H2D alone, D2H alone, both at once"},
             "api": "sfnl_bundle_mhd_host (host arrays, pinned)"}
 
 
-def _pcie_both_gbs(torch, h_src, h_dst):
-    """Host<->device bandwidth with both directions at once (pinned buffers of this run, 2 GB each way),
-    the bound of the end-to-end call: GB/s over both directions."""
+def _pcie_rates(torch, h_src, h_dst):
+    """Pinned host<->device copy rates in GB/s (buffers of this run, 2 GB): H2D alone, D2H alone, and both
+    directions at once (bytes of both over the time)."""
     n = min(h_src.numel(), h_dst.numel(), (2 << 30) // 8)
     src, dst = h_src.view(-1)[:n], h_dst.view(-1)[:n]
     d_in = torch.empty(n, dtype=torch.float64, device="cuda")
     d_out = torch.empty(n, dtype=torch.float64, device="cuda")
     s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
-    best = 0.0
-    for _ in range(3):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        with torch.cuda.stream(s1):
-            d_in.copy_(src, non_blocking=True)
-        with torch.cuda.stream(s2):
-            dst.copy_(d_out, non_blocking=True)
-        torch.cuda.synchronize()
-        best = max(best, 2 * 8 * n / (time.perf_counter() - t0) / 1e9)
+
+    def timed(h2d, d2h):
+        best = 0.0
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            if h2d:
+                with torch.cuda.stream(s1):
+                    d_in.copy_(src, non_blocking=True)
+            if d2h:
+                with torch.cuda.stream(s2):
+                    dst.copy_(d_out, non_blocking=True)
+            torch.cuda.synchronize()
+            best = max(best, (h2d + d2h) * 8 * n / (time.perf_counter() - t0) / 1e9)
+        return best
+
+    rates = {"h2d": timed(1, 0), "d2h": timed(0, 1), "both": timed(1, 1)}
     del d_in, d_out
-    return best
+    return rates
 
 
 def _cpu_baseline(args, ins, npts, m, pad):

@@ -618,7 +618,9 @@ int launch_large_syn(const LargeArgs &la, int nfields, int nbz, bool tf, cudaStr
     return check_launch("large-m synthesis");
   };
   if (tf) {
-    if (4 * tile_bytes <= kLargeSynSmem) return go(large_syn_tf_kernel<4>, 4);
+    // two point tiles per CTA: at 118 registers and 2 x 16-32 KB of staged rows, four CTAs share an SM; four
+    // tiles per CTA (each B fragment feeding four DMMAs) left three 4-warp CTAs per SM (168 registers) and
+    // were 10-30 % slower (m = 128 to 512)
     if (2 * tile_bytes <= kLargeSynSmem) return go(large_syn_tf_kernel<2>, 2);
   } else {
     if (4 * tile_bytes <= kLargeSynSmem) return go(large_syn_kernel<4>, 4);
