@@ -596,7 +596,7 @@ def _extra_configs(args, sf, torch, dev, world, rank, dist, local, stream):
     ms_t = tstep(lambda: sf.cross_vjp(u, w, cot, m_max_pad=pad, out=jt), 10)
     cfg["jvp"] = {"ms_per_step": ms_j, "value": world * npts * m / (ms_j / 1e3)}
     cfg["vjp"] = {"ms_per_step": ms_t, "value": world * npts * m / (ms_t / 1e3)}
-    cfg["roofline"] = {"jvp": roof(nbytes, ms_j, "fast_kernel (JVP as two accumulating cross products)"),
+    cfg["roofline"] = {"jvp": roof(nbytes, ms_j, "fast_kernel<EK_CROSS2> (du x w + u x dw in one two-pass launch)"),
                        "vjp": roof(nbytes, ms_t, "fast_kernel (VJP as two cross products)")}
     sf.cross_jvp(u, w, tan, m_max_pad=pad, out=jv)
     sf.cross_vjp(u, w, cot, m_max_pad=pad, out=jt)

@@ -31,9 +31,10 @@
 // products go through shared memory in fragment order, then warp w owns output
 // mode tiles in the analysis.  Elementary programs are cross (6 -> 3), dot
 // (6 -> 1), product (2 -> 1), scalar x vector (4 -> 3, FFT_SCALAR_VECT_DCL
-// pb = 1) and tensor (6 -> 9, FFT_TENSOR_DCL); the bundle and the linearised
-// programs are sequences of elementary launches on one stream (with
-// accumulation).
+// pb = 1), tensor (6 -> 9, FFT_TENSOR_DCL) and the sum of two cross products
+// (12 -> 3, the JVP du x w + u x dw: two synthesis passes, one analysis); the
+// bundle (away from m = 64) and the transposed programs are sequences of
+// elementary launches on one stream.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -195,9 +196,9 @@ namespace {
 // kernel
 // ---------------------------------------------------------------------------
 struct FastArgs {
-  const double *in[6];
+  const double *in[12];
   double *out[9];
-  int64_t in_ldm[6], out_ldm[9], in_bs[6], out_bs[9];
+  int64_t in_ldm[12], out_ldm[9], in_bs[12], out_bs[9];
   int64_t out_ps;   // point stride of the outputs (3 in the tensor layout), sine at out_ps*np
   int64_t np;
   int m, N, NT;
@@ -247,6 +248,11 @@ struct EKDef<EK_ADVECT> {  // [heat grad c 0-2, u 3-5, div u 6, heat c 7] -> gra
   }
 };
 template <>
+struct EKDef<EK_CROSS2> {  // fields [a, b, c, d] -> a x b + c x d, one pair (6 fields) per pass
+  static constexpr int NI = 12, NO = 3;
+  __device__ static void op(const double *x, double *y) { cross3(x, x + 3, y); }
+};
+template <>
 struct EKDef<EK_TENSOR> {
   static constexpr int NI = 6, NO = 9;
   __device__ static void op(const double *x, double *y) {
@@ -256,8 +262,15 @@ struct EKDef<EK_TENSOR> {
       for (int l = 0; l < 3; ++l) y[3 * k + l] = x[k] * x[3 + l];
   }
 };
-__host__ __device__ constexpr int ek_nin(int ek) { return ek == EK_PROD ? 2 : ek == EK_SVECT ? 4 : ek == EK_ADVECT ? 8 : 6; }
-__host__ __device__ constexpr int ek_nout(int ek) { return ek == EK_CROSS || ek == EK_SVECT ? 3 : ek == EK_TENSOR ? 9 : 1; }
+__host__ __device__ constexpr int ek_nin(int ek) {
+  return ek == EK_PROD ? 2 : ek == EK_SVECT ? 4 : ek == EK_ADVECT ? 8 : ek == EK_CROSS2 ? 12 : 6;
+}
+// Synthesis passes of a program: EK_CROSS2 synthesises its two operand pairs one after the other through the
+// accumulators of one pair and adds the second pair's products to the first's pre-folded ones.
+__host__ __device__ constexpr int ek_passes(int ek) { return ek == EK_CROSS2 ? 2 : 1; }
+__host__ __device__ constexpr int ek_nout(int ek) {
+  return ek == EK_CROSS || ek == EK_SVECT || ek == EK_CROSS2 ? 3 : ek == EK_TENSOR ? 9 : 1;
+}
 // Shared memory of one CTA: folded products [NO][4][NT][2][32] and staged coefficients [NI][KT][8].
 // With NT <= 8 angle tiles every warp (pair, with the class split) owns one tile and the products
 // (and the exchange) overlay the coefficients.
@@ -265,11 +278,15 @@ __host__ __device__ constexpr int ek_nout(int ek) { return ek == EK_CROSS || ek 
 // and doubles the warps per SM; it pays for the six-field programs at m >= 64, where the accumulator
 // registers limit residency, and costs shared memory and a barrier elsewhere (measured on B200).
 constexpr bool class_split(int ek, int M) { return (ek == EK_CROSS || ek == EK_DOT) && (M == 64 || M == 0); }
+// With several passes the products overlay only the first pass's coefficients.
+__host__ __device__ constexpr bool fast_overlay(int ek, int NT, int KT) {
+  return NT <= 8 && (ek_passes(ek) == 1 || (size_t)ek_nout(ek) * 4 * NT * 2 * 32 <= (size_t)ek_nin(ek) / ek_passes(ek) * KT * 8);
+}
 inline size_t fast_smem_bytes(int ek, int NT, int KT, bool cs) {
   const int nwt = NT < 8 ? NT : 8;
   const size_t prod = (size_t)ek_nout(ek) * 4 * NT * 2 * 32, coef = (size_t)ek_nin(ek) * KT * 8;
   const size_t xch = cs ? (size_t)nwt * ek_nin(ek) * 128 : 0;
-  return sizeof(double) * (NT <= 8 ? (prod + xch > coef ? prod + xch : coef) : prod + xch + coef);
+  return sizeof(double) * (fast_overlay(ek, NT, KT) ? (prod + xch > coef ? prod + xch : coef) : prod + xch + coef);
 }
 
 
@@ -333,7 +350,9 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS),
   // consecutive threads copy one row (two points each, one 16-byte copy when the row is 16-byte
   // aligned), so a warp instruction moves 8 whole 64-byte rows.
   const int NWT = CS ? NW >> 1 : NW;  // angle tiles per pass (two warps per tile with the class split)
-  const bool overlay = NT <= NWT;
+  constexpr int NPASS = ek_passes(EK), NIP = NI / NPASS;  // synthesis passes, fields per pass
+  static_assert(NPASS == 1 || (!CS && GK < 0), "passes: the four-class kernel on staged fields only");
+  const bool overlay = NT <= NWT && fast_overlay(EK, NT, KT);
   const size_t prod_d = (size_t)NO * 4 * NT * 2 * 32, xch_d = CS ? (size_t)NWT * NI * 128 : 0;
   double *ps = smem, *xc = smem + prod_d;
   double *xs = overlay ? smem : smem + prod_d + xch_d;
@@ -507,15 +526,19 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS),
     // ---- synthesis, fold, program, analysis pre-fold ----
     for (int t0 = 0; t0 < NT; t0 += NW) {  // one pass when the products overlay the coefficients
       const int t = t0 + warp;
-      double acc[NI][4][2];
+      // NPASS > 1: the operand pairs one after the other, fields NIP*pass .. NIP*pass+NIP-1; the products
+      // overlay only pass 0's coefficients, and the later passes add theirs to the pre-folded ones
+#pragma unroll 1
+      for (int pass = 0; pass < NPASS; ++pass) {
+      double acc[NIP][4][2];
 #pragma unroll
-      for (int f = 0; f < NI; ++f)
+      for (int f = 0; f < NIP; ++f)
 #pragma unroll
         for (int c = 0; c < 4; ++c) acc[f][c][0] = acc[f][c][1] = 0.0;
       if (t < NT) {
-      // k-steps outermost, the four classes inside: 4*NI independent accumulator chains per step
+      // k-steps outermost, the four classes inside: 4*NIP independent accumulator chains per step
       const double *syn_t = a.syn + (size_t)t * 32 + lane;
-      const double *xs_l = xs + a_frag_slot(lane & 3, lane >> 2);
+      const double *xs_l = xs + (size_t)pass * NIP * KS_tot * 32 + a_frag_slot(lane & 3, lane >> 2);
 #pragma unroll
       for (int s = 0; s < ks_max; ++s) {
 #pragma unroll
@@ -523,27 +546,27 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS),
           if (s >= KS[c]) continue;
           const double bv = __ldg(syn_t + (size_t)(KOFF[c] + s) * NT * 32);
           const double *xa = xs_l + (size_t)(KOFF[c] + s) * 32;
-          double av[NI];
+          double av[NIP];
 #pragma unroll
-          for (int f = 0; f < NI; ++f) av[f] = xa[(size_t)f * KS_tot * 32];
+          for (int f = 0; f < NIP; ++f) av[f] = xa[(size_t)f * KS_tot * 32];
           if constexpr (ADJ != 0) {
             const double wn = (s == 0 && q == 0 && (c & 1) == 0) ? invN : twoN;  // n == 0 only there
 #pragma unroll
-            for (int f = 0; f < NI; ++f)
+            for (int f = 0; f < NIP; ++f)
               if ((ADJ == 1 && f < 3) || (ADJ == 2 && f >= 3)) av[f] *= wn;
           }
 #pragma unroll
-          for (int f = 0; f < NI; ++f) dmma(acc[f][c], av[f], bv);
+          for (int f = 0; f < NIP; ++f) dmma(acc[f][c], av[f], bv);
         }
       }
       }
-      if (overlay) __syncthreads();  // every warp has read its last coefficient
-      if (t >= NT) continue;
+      if (overlay && pass == 0) __syncthreads();  // every warp has read pass 0's last coefficient
+      if (t < NT) {
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
-        double v[4][NI];
+        double v[4][NIP];
 #pragma unroll
-        for (int f = 0; f < NI; ++f) {
+        for (int f = 0; f < NIP; ++f) {
           const double A = acc[f][0][e] + acc[f][1][e], B = acc[f][0][e] - acc[f][1][e];
           const double C = acc[f][2][e] + acc[f][3][e], D = acc[f][3][e] - acc[f][2][e];
           v[0][f] = A + C;  // theta
@@ -560,11 +583,21 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS),
           const double s23 = gq[1][o] + gq[2][o], d32 = gq[2][o] - gq[1][o];
           double *dst = ps + ((size_t)((o * 4) * NT + t) * 2 + e) * 32 + lane;
           const size_t cstride = (size_t)NT * 2 * 32;
-          dst[0] = s14 + s23;            // PE
-          dst[cstride] = s14 - s23;      // PO
-          dst[2 * cstride] = d14 + d32;  // QE
-          dst[3 * cstride] = d14 - d32;  // QO
+          const double pe = s14 + s23, po = s14 - s23, qe = d14 + d32, qo = d14 - d32;
+          if (pass == 0) {
+            dst[0] = pe;
+            dst[cstride] = po;
+            dst[2 * cstride] = qe;
+            dst[3 * cstride] = qo;
+          } else {  // the same lane wrote these in pass 0
+            dst[0] += pe;
+            dst[cstride] += po;
+            dst[2 * cstride] += qe;
+            dst[3 * cstride] += qo;
+          }
         }
+      }
+      }
       }
     }
     __syncthreads();
@@ -1251,7 +1284,7 @@ int rows_aligned16(const FastArgs &fa, int ni) {
 }
 }  // namespace
 
-int decompose_program(int op, std::vector<Elem> &seq) {
+int decompose_program(int op, std::vector<Elem> &seq, bool fuse_pairs) {
   seq.clear();
   auto add = [&](int ek, std::initializer_list<int> in, std::initializer_list<int> out, unsigned adj, int acc) {
     Elem e{};
@@ -1282,6 +1315,10 @@ int decompose_program(int op, std::vector<Elem> &seq) {
       add(EK_PROD, {6, 7}, {0}, 0, 1);                       // + d c
       break;
     case OP_CROSS_JVP:  // [u, w, du, dw]
+      if (fuse_pairs) {
+        add(EK_CROSS2, {6, 7, 8, 3, 4, 5, 0, 1, 2, 9, 10, 11}, {0, 1, 2}, 0, 0);  // du x w + u x dw
+        break;
+      }
       add(EK_CROSS, {6, 7, 8, 3, 4, 5}, {0, 1, 2}, 0, 0);     // du x w
       add(EK_CROSS, {0, 1, 2, 9, 10, 11}, {0, 1, 2}, 0, 1);   // + u x dw
       break;
@@ -1290,6 +1327,11 @@ int decompose_program(int op, std::vector<Elem> &seq) {
       add(EK_CROSS, {6, 7, 8, 0, 1, 2}, {3, 4, 5}, A0, 0);    // c x u
       break;
     case OP_MHD_JVP:  // [u, w, b, du, dw, db]
+      if (fuse_pairs) {
+        add(EK_CROSS2, {9, 10, 11, 3, 4, 5, 0, 1, 2, 12, 13, 14}, {0, 1, 2}, 0, 0);  // du x w + u x dw
+        add(EK_CROSS2, {9, 10, 11, 6, 7, 8, 0, 1, 2, 15, 16, 17}, {3, 4, 5}, 0, 0);  // du x b + u x db
+        break;
+      }
       add(EK_CROSS, {9, 10, 11, 3, 4, 5}, {0, 1, 2}, 0, 0);   // du x w
       add(EK_CROSS, {0, 1, 2, 12, 13, 14}, {0, 1, 2}, 0, 1);  // + u x dw
       add(EK_CROSS, {9, 10, 11, 6, 7, 8}, {3, 4, 5}, 0, 0);   // du x b
@@ -1509,7 +1551,10 @@ int launch_fast(const ProgArgs &a, cudaStream_t st) {
   if (rc) return rc;
   if (!fast_fused_fits(a.op, a.m)) return launch_fast_large(a, g, T, st);
   std::vector<Elem> seq;
-  rc = decompose_program(a.op, seq);
+  // the linearised cross products as one two-pass program each (the output written once, one analysis):
+  // 1.7x faster than two launches at m = 32 (700k points, one tangent: 3.26 -> 1.92 ms) and 1.25x at
+  // m = 64, where the two launches ran on the third-fold kernel (200k points, 4 tangents: 8.40 -> 6.70 ms)
+  rc = decompose_program(a.op, seq, true);
   if (rc) return rc;
   const bool adj_out = op_adjoint_out(a.op);
   for (const Elem &e : seq) {
@@ -1547,6 +1592,7 @@ int launch_fast(const ProgArgs &a, cudaStream_t st) {
     fa.syn = T.syn;
     fa.ana = T.ana;
     int r = e.ek == EK_CROSS  ? launch_ek<EK_CROSS>(fa, a.batch, st)
+          : e.ek == EK_CROSS2 ? launch_ek<EK_CROSS2>(fa, a.batch, st)
           : e.ek == EK_DOT    ? launch_ek<EK_DOT>(fa, a.batch, st)
           : e.ek == EK_PROD   ? launch_ek<EK_PROD>(fa, a.batch, st)
           : e.ek == EK_SVECT  ? launch_ek<EK_SVECT>(fa, a.batch, st)

@@ -80,15 +80,17 @@ int launch_gauss_general_fused(const GaussArgs &ga, int kind, bool conservative,
 // linearised cross product two or four, accumulating where a term adds to an
 // earlier one).
 enum { EK_CROSS = 0, EK_DOT = 1, EK_PROD = 2, EK_SVECT = 3, EK_TENSOR = 4,
-       EK_ADVECT = 5 };  // g . w + d c (8 -> 1): the fused conservative advection callers only
+       EK_ADVECT = 5,    // g . w + d c (8 -> 1): the fused conservative advection callers only
+       EK_CROSS2 = 6 };  // a x b + c x d (12 -> 3): the linearised cross product, in two passes
 struct Elem {
   int ek;
-  int in[6];     // field indices into ProgArgs.in
+  int in[12];    // field indices into ProgArgs.in
   int out[9];    // indices into ProgArgs.out
   unsigned adj;  // bit f: operand f is a cotangent (synthesised with the analysis weights)
   int acc;       // 1: add to the output instead of overwriting it
 };
-int decompose_program(int op, std::vector<Elem> &seq);   // sfnl_fast.cu
+// fuse_pairs: a x b + c x d as one EK_CROSS2 program (the generic FAST kernel) instead of two launches
+int decompose_program(int op, std::vector<Elem> &seq, bool fuse_pairs = false);  // sfnl_fast.cu
 bool split_supported(int op, int m);                    // sfnl_split.cu
 
 }  // namespace sfnl

@@ -166,7 +166,7 @@ def _batched(npts, nslot, m, k, alpha, seed):
     return x
 
 
-@pytest.mark.parametrize("npts,m,k", [(120, 8, 3), (33, 17, 1), (41, 64, 2)])
+@pytest.mark.parametrize("npts,m,k", [(120, 8, 3), (33, 17, 1), (41, 64, 2), (29, 90, 2), (25, 96, 1)])
 def test_cross_jvp_matches_linearisation(npts, m, k):
     pad = 3 * m // 2
     u = R.synthetic_field(npts, 6, m, 0.2, 1)
@@ -212,7 +212,7 @@ def test_cross_vjp_dot_product_identity(npts, m, k):
         assert R.rel_l2(jtc[..., t], R.cross_vjp(u, w, np.asfortranarray(c[..., t]))) <= FP64_TOL
 
 
-@pytest.mark.parametrize("npts,m,k", [(90, 12, 2), (43, 64, 2)])
+@pytest.mark.parametrize("npts,m,k", [(90, 12, 2), (43, 64, 2), (27, 90, 2)])
 def test_mhd_jvp_vjp(npts, m, k):
     pad = 3 * m // 2
     u, w, b = (R.synthetic_field(npts, 6, m, 0.2, 60 + i) for i in range(3))
