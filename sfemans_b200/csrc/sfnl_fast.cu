@@ -278,9 +278,11 @@ __host__ __device__ constexpr int ek_nout(int ek) {
 // and doubles the warps per SM; it pays for the six-field programs at m >= 64, where the accumulator
 // registers limit residency, and costs shared memory and a barrier elsewhere (measured on B200).
 constexpr bool class_split(int ek, int M) { return (ek == EK_CROSS || ek == EK_DOT) && (M == 64 || M == 0); }
-// With several passes the products overlay only the first pass's coefficients.
+// With several passes the products (written after a barrier that ends pass 0's synthesis, added to in the
+// later passes) may overlay only pass 0's coefficients.
 __host__ __device__ constexpr bool fast_overlay(int ek, int NT, int KT) {
-  return NT <= 8 && (ek_passes(ek) == 1 || (size_t)ek_nout(ek) * 4 * NT * 2 * 32 <= (size_t)ek_nin(ek) / ek_passes(ek) * KT * 8);
+  return NT <= 8 && (ek_passes(ek) == 1 ||
+                     (size_t)ek_nout(ek) * 4 * NT * 2 * 32 <= (size_t)ek_nin(ek) / ek_passes(ek) * KT * 8);
 }
 inline size_t fast_smem_bytes(int ek, int NT, int KT, bool cs) {
   const int nwt = NT < 8 ? NT : 8;
@@ -551,6 +553,7 @@ __global__ void __launch_bounds__(fast_max_threads(M, CS),
           for (int f = 0; f < NIP; ++f) av[f] = xa[(size_t)f * KS_tot * 32];
           if constexpr (ADJ != 0) {
             const double wn = (s == 0 && q == 0 && (c & 1) == 0) ? invN : twoN;  // n == 0 only there
+            // ADJ 1 / 2: the first / second operand (of every pass)
 #pragma unroll
             for (int f = 0; f < NIP; ++f)
               if ((ADJ == 1 && f < 3) || (ADJ == 2 && f >= 3)) av[f] *= wn;
@@ -1261,7 +1264,11 @@ int launch_ek_adj(FastArgs &fa, int batch, cudaStream_t st) {
 
 template <int EK>
 int launch_ek(FastArgs &fa, int batch, cudaStream_t st) {
-  if constexpr (EK == EK_CROSS) {
+  if constexpr (ek_passes(EK) == 2) {  // the cotangents' fields among the 12 staged ones (pass 0: 0-5, pass 1: 6-11)
+    if (fa.adj_in == 0u) return launch_ek_adj<EK, 0>(fa, batch, st);
+    if (fa.adj_in == 0xE38u) return launch_ek_adj<EK, 2>(fa, batch, st);  // second operand of both passes
+    return set_error(SFNL_ERR_ARG, "FAST form: unsupported cotangent operands");
+  } else if constexpr (EK == EK_CROSS) {
     if (fa.adj_in == 0x07u) return launch_ek_adj<EK, 1>(fa, batch, st);
     if (fa.adj_in == 0x38u) return launch_ek_adj<EK, 2>(fa, batch, st);
     if (fa.adj_in != 0u) return set_error(SFNL_ERR_ARG, "FAST form: unsupported cotangent operand");
@@ -1284,7 +1291,7 @@ int rows_aligned16(const FastArgs &fa, int ni) {
 }
 }  // namespace
 
-int decompose_program(int op, std::vector<Elem> &seq, bool fuse_pairs) {
+int decompose_program(int op, std::vector<Elem> &seq, int fuse) {
   seq.clear();
   auto add = [&](int ek, std::initializer_list<int> in, std::initializer_list<int> out, unsigned adj, int acc) {
     Elem e{};
@@ -1315,7 +1322,7 @@ int decompose_program(int op, std::vector<Elem> &seq, bool fuse_pairs) {
       add(EK_PROD, {6, 7}, {0}, 0, 1);                       // + d c
       break;
     case OP_CROSS_JVP:  // [u, w, du, dw]
-      if (fuse_pairs) {
+      if (fuse & kFuseJvp) {
         add(EK_CROSS2, {6, 7, 8, 3, 4, 5, 0, 1, 2, 9, 10, 11}, {0, 1, 2}, 0, 0);  // du x w + u x dw
         break;
       }
@@ -1327,7 +1334,7 @@ int decompose_program(int op, std::vector<Elem> &seq, bool fuse_pairs) {
       add(EK_CROSS, {6, 7, 8, 0, 1, 2}, {3, 4, 5}, A0, 0);    // c x u
       break;
     case OP_MHD_JVP:  // [u, w, b, du, dw, db]
-      if (fuse_pairs) {
+      if (fuse & kFuseJvp) {
         add(EK_CROSS2, {9, 10, 11, 3, 4, 5, 0, 1, 2, 12, 13, 14}, {0, 1, 2}, 0, 0);  // du x w + u x dw
         add(EK_CROSS2, {9, 10, 11, 6, 7, 8, 0, 1, 2, 15, 16, 17}, {3, 4, 5}, 0, 0);  // du x b + u x db
         break;
@@ -1338,8 +1345,12 @@ int decompose_program(int op, std::vector<Elem> &seq, bool fuse_pairs) {
       add(EK_CROSS, {0, 1, 2, 15, 16, 17}, {3, 4, 5}, 0, 1);  // + u x db
       break;
     case OP_MHD_VJP:  // [u, w, b, c1, c2]
-      add(EK_CROSS, {3, 4, 5, 9, 10, 11}, {0, 1, 2}, A1, 0);  // w x c1
-      add(EK_CROSS, {6, 7, 8, 12, 13, 14}, {0, 1, 2}, A1, 1); // + b x c2
+      if (fuse & kFuseVjpSum) {
+        add(EK_CROSS2, {3, 4, 5, 9, 10, 11, 6, 7, 8, 12, 13, 14}, {0, 1, 2}, 0xE38u, 0);  // w x c1 + b x c2
+      } else {
+        add(EK_CROSS, {3, 4, 5, 9, 10, 11}, {0, 1, 2}, A1, 0);  // w x c1
+        add(EK_CROSS, {6, 7, 8, 12, 13, 14}, {0, 1, 2}, A1, 1); // + b x c2
+      }
       add(EK_CROSS, {9, 10, 11, 0, 1, 2}, {3, 4, 5}, A0, 0);  // c1 x u
       add(EK_CROSS, {12, 13, 14, 0, 1, 2}, {6, 7, 8}, A0, 0); // c2 x u
       break;
@@ -1553,8 +1564,14 @@ int launch_fast(const ProgArgs &a, cudaStream_t st) {
   std::vector<Elem> seq;
   // the linearised cross products as one two-pass program each (the output written once, one analysis):
   // 1.7x faster than two launches at m = 32 (700k points, one tangent: 3.26 -> 1.92 ms) and 1.25x at
-  // m = 64, where the two launches ran on the third-fold kernel (200k points, 4 tangents: 8.40 -> 6.70 ms)
-  rc = decompose_program(a.op, seq, true);
+  // m = 64, where the two launches ran on the third-fold kernel (200k points, 4 tangents: 8.40 -> 6.70 ms);
+  // where their products cannot overlay their coefficients (more than 8 angle tiles, m > 85) the two
+  // launches stay.  The MHD VJP's w x c1 + b x c2 likewise (m = 32, 200k points, 4 tangents: 6.51 -> 5.09 ms)
+  // but at m = 64, where its two launches on the third-fold kernel are a little faster (7.74 against
+  // 7.98 ms); the other transposed products (two cross products into different outputs) gained nothing from
+  // one launch of two passes (m = 32: 2.41 -> 2.69 ms).
+  const bool fuse_ok = fast_overlay(EK_CROSS2, g.NT, 4 * g.KS_tot);
+  rc = decompose_program(a.op, seq, fuse_ok ? kFuseJvp | (a.m != 64 ? kFuseVjpSum : 0) : 0);
   if (rc) return rc;
   const bool adj_out = op_adjoint_out(a.op);
   for (const Elem &e : seq) {

@@ -89,8 +89,10 @@ struct Elem {
   unsigned adj;  // bit f: operand f is a cotangent (synthesised with the analysis weights)
   int acc;       // 1: add to the output instead of overwriting it
 };
-// fuse_pairs: a x b + c x d as one EK_CROSS2 program (the generic FAST kernel) instead of two launches
-int decompose_program(int op, std::vector<Elem> &seq, bool fuse_pairs = false);  // sfnl_fast.cu
+// fuse: which sums of two cross products a x b + c x d run as one EK_CROSS2 program of the generic FAST kernel
+// instead of two launches (kFuseJvp: the JVPs; kFuseVjpSum: w x c1 + b x c2 of the MHD VJP)
+enum { kFuseJvp = 1, kFuseVjpSum = 2 };
+int decompose_program(int op, std::vector<Elem> &seq, int fuse = 0);  // sfnl_fast.cu
 bool split_supported(int op, int m);                    // sfnl_split.cu
 
 }  // namespace sfnl
