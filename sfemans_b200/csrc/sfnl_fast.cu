@@ -60,6 +60,26 @@ std::map<std::pair<int, int>, Tables> g_tabs;  // (device, m) -> tables
 
 }  // namespace
 
+// Device copies of a synthesis and an analysis table (none kept on failure).
+static int upload_tables(const std::vector<double> &syn, const std::vector<double> &ana, Tables *T) {
+  T->syn = T->ana = nullptr;
+  if (cudaMalloc(&T->syn, syn.size() * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&T->ana, ana.size() * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(T->syn);
+    T->syn = nullptr;
+    return set_error(SFNL_ERR_ALLOC, "cudaMalloc of the DFT tables failed");
+  }
+  if (cudaMemcpy(T->syn, syn.data(), syn.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(T->ana, ana.data(), ana.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(T->syn);
+    cudaFree(T->ana);
+    T->syn = T->ana = nullptr;
+    return set_error(SFNL_ERR_CUDA, "upload of the DFT tables failed");
+  }
+  return SFNL_OK;
+}
+
 int get_tables(const Geo &g, Tables *out) {
   int dev = 0;
   cudaGetDevice(&dev);
@@ -104,14 +124,7 @@ int get_tables(const Geo &g, Tables *out) {
               ana[((((size_t)var * g.NU_tot + g.nu_off[c] + u) * g.NT + t) * 2 + e) * 32 + l] = v;
             }
   Tables T;
-  if (cudaMalloc(&T.syn, syn.size() * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&T.ana, ana.size() * sizeof(double)) != cudaSuccess) {
-    cudaGetLastError();
-    return set_error(SFNL_ERR_ALLOC, "cudaMalloc of the DFT tables failed");
-  }
-  if (cudaMemcpy(T.syn, syn.data(), syn.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(T.ana, ana.data(), ana.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
-    return set_error(SFNL_ERR_CUDA, "upload of the DFT tables failed");
+  if (int rc = upload_tables(syn, ana, &T)) return rc;
   g_tabs[{dev, g.m}] = T;
   *out = T;
   return SFNL_OK;
@@ -177,14 +190,7 @@ int get_tf_tables(const Geo &g, Tables *out) {
             ana[(((size_t)var * asteps + tf_aoff(g.m, gr) + u * tf_TE(g.m, gr) + te) * 32) + l] = v;
           }
   Tables T;
-  if (cudaMalloc(&T.syn, syn.size() * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&T.ana, ana.size() * sizeof(double)) != cudaSuccess) {
-    cudaGetLastError();
-    return set_error(SFNL_ERR_ALLOC, "cudaMalloc of the DFT tables failed");
-  }
-  if (cudaMemcpy(T.syn, syn.data(), syn.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(T.ana, ana.data(), ana.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
-    return set_error(SFNL_ERR_CUDA, "upload of the DFT tables failed");
+  if (int rc = upload_tables(syn, ana, &T)) return rc;
   g_tftabs[{dev, g.m}] = T;
   *out = T;
   return SFNL_OK;

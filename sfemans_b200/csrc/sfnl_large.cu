@@ -866,8 +866,10 @@ int get_large_r3_tables(int m, int N, R3LargeTab *out) {
     cudaGetLastError();
     return set_error(SFNL_ERR_ALLOC, "cudaMalloc of the residue-grid tables failed");
   }
-  if (cudaMemcpy(T.base, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+  if (cudaMemcpy(T.base, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(T.base);
     return set_error(SFNL_ERR_CUDA, "upload of the residue-grid tables failed");
+  }
   T.syn = T.base;
   T.ana = T.base + nsyn;
   T.tw = T.base + nsyn + nana;

@@ -131,8 +131,10 @@ int get_r3_tables(R3Tables *out) {
     cudaGetLastError();
     return set_error(SFNL_ERR_ALLOC, "cudaMalloc of the residue-split DFT tables failed");
   }
-  if (cudaMemcpy(T.base, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+  if (cudaMemcpy(T.base, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(T.base);
     return set_error(SFNL_ERR_CUDA, "upload of the residue-split DFT tables failed");
+  }
   g_r3_tabs[dev] = T;
   *out = T;
   return SFNL_OK;
