@@ -30,6 +30,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "sfnl_fold.cuh"
@@ -146,22 +147,28 @@ struct R3Fields {  // three fields: cos of mode n, point p at p[f][p + n*ldm[f]]
 };
 
 // Stages the three fields of the 8-point tile at p0 into xr [3][128 rows: cos 0..63, sin 0..63][8 points]
-// with cp.async and commits one group (the sine of mode 0 is not read: zero).
+// with cp.async and commits one group (the sine of mode 0 is not read: zero).  384 threads: thread t copies
+// 16 bytes (points pc, pc + 1) of rows rb, rb + 32 (cosines) and 64 + rb, 96 + rb (sines) of field t / 128,
+// rb = (t % 128) / 4, so that four consecutive threads move one whole 64-byte row and every address derives
+// from two bases by constant offsets.
 __device__ __forceinline__ void r3_stage(double *xr, const R3Fields &fs, int64_t p0, int64_t np, bool vec16) {
-  const bool v16 = vec16 && p0 + 8 <= np;
-  for (int c = threadIdx.x; c < 3 * 128 * 4; c += blockDim.x) {
-    const int pc = 2 * (c & 3), row = (c >> 2) & 127, f = c >> 9;
-    const int n = row & 63;
-    const bool sn = row >= 64, live = !(sn && n == 0);
-    const double *base = f == 0 ? fs.p[0] : f == 1 ? fs.p[1] : fs.p[2];
-    const int64_t ldm = f == 0 ? fs.ldm[0] : f == 1 ? fs.ldm[1] : fs.ldm[2];
-    const double *src = base + (sn ? np : 0) + p0 + pc + (int64_t)n * ldm;
-    double *dst = xr + ((size_t)f * 128 + (row & 64) + r3_xrow(n)) * 8 + pc;
+  const int t = threadIdx.x, f = t >> 7, pc = 2 * (t & 3), rb = (t & 127) >> 2;
+  const double *base = f == 0 ? fs.p[0] : f == 1 ? fs.p[1] : fs.p[2];
+  const int64_t ldm = f == 0 ? fs.ldm[0] : f == 1 ? fs.ldm[1] : fs.ldm[2];
+  const double *src = base + p0 + pc + (int64_t)rb * ldm;        // cosine row rb; rb + 32 at 32 ldm, sines np on
+  double *dst = xr + ((size_t)f * 128 + r3_xrow(rb)) * 8 + pc;  // r3_xrow(rb + 32) = r3_xrow(rb) + 32
+  const bool v16 = vec16 && p0 + 8 <= np, pv0 = p0 + pc < np, pv1 = p0 + pc + 1 < np;
+  // a rolled loop: the four copies' addresses at once would cost registers the synthesis needs
+#pragma unroll 1
+  for (int i = 0; i < 4; ++i) {
+    const double *s_i = src + ((i & 1) ? 32 * ldm : 0) + ((i & 2) ? np : 0);
+    double *d_i = dst + (i & 1) * 256 + (i & 2) * 256;
+    const bool live = !(i == 2 && rb == 0);  // the sine of mode 0
     if (live && v16) {
-      cp_async16(dst, src);
+      cp_async16(d_i, s_i);
     } else {
-      if (live && p0 + pc < np) cp_async8(dst, src); else dst[0] = 0.0;
-      if (live && p0 + pc + 1 < np) cp_async8(dst + 1, src + 1); else dst[1] = 0.0;
+      if (live && pv0) cp_async8(d_i, s_i); else d_i[0] = 0.0;
+      if (live && pv1) cp_async8(d_i + 1, s_i + 1); else d_i[1] = 0.0;
     }
   }
   cp_async_commit();
@@ -408,14 +415,16 @@ __global__ void __launch_bounds__(384, 2) fast_bundle_r3_kernel(const R3BundleAr
     }
     return os;
   };
-  // one operand: wait for its copies, form the residues' coefficients, issue the copies of the operand at
-  // (next_first, next_p0) (none if next_first < 0), synthesise the group's residue, fold
-  auto operand = [&](int next_first, int64_t next_p0, double (&v)[4][3]) {
+  // one operand: wait for its copies, form the residues' coefficients, issue the copies of the operand whose
+  // fields start at a.in[NEXT] (a compile-time index, so that the kernel parameters are read at fixed offsets)
+  // at point next_p0 when stage_next, synthesise the group's residue, fold
+  auto operand = [&](auto next_tag, bool stage_next, int64_t next_p0, double (&v)[4][3]) {
+    constexpr int NEXT = decltype(next_tag)::value;
     cp_async_wait_0();
     __syncthreads();  // the copies have landed; the previous round's sums are read
     r3_precombine(xr, xs, tws);
     __syncthreads();  // xs complete, xr read
-    if (next_first >= 0) r3_stage(xr, fields(next_first), next_p0, a.np, a.vec16 != 0);
+    if (stage_next) r3_stage(xr, fields(NEXT), next_p0, a.np, a.vec16 != 0);
     double acc_e[3][2], acc_o[3][2];
     r3_synth(xs_r, a.syn, tau, half, acc_e, acc_o);
     gsync();  // the group has read its A fragments: the exchanges overlay them
@@ -428,15 +437,15 @@ __global__ void __launch_bounds__(384, 2) fast_bundle_r3_kernel(const R3BundleAr
     const int64_t p0 = tile * 8;
     const bool more = tile + gridDim.x < ntiles;
     double vu[4][3], vb[4][3], vx[4][3];
-    operand(3, p0, vu);   // u; next w
-    operand(12, p0, vx);  // w; next gradT
+    operand(std::integral_constant<int, 3>{}, true, p0, vu);    // u; next w
+    operand(std::integral_constant<int, 12>{}, true, p0, vx);   // w; next gradT
     {
       double gq[4][3];
 #pragma unroll
       for (int q = 0; q < 4; ++q) cross3(vu[q], vx[q], gq[q]);
       prefold_store<kR3NT, 3>(gq, ps_r, 0, tau, half);
     }
-    operand(6, p0, vx);  // gradT; next b
+    operand(std::integral_constant<int, 6>{}, true, p0, vx);  // gradT; next b
     {
       double gq[4][1];
 #pragma unroll
@@ -448,7 +457,7 @@ __global__ void __launch_bounds__(384, 2) fast_bundle_r3_kernel(const R3BundleAr
       r3_combine<3>(xs, kR3RS, tws, outs(0, 3), p0, a.np, v16o);  // u x w
       r3_combine<1>(ps, kR3PS, tws, outs(9, 1), p0, a.np, v16o);  // u . gradT
     }
-    operand(9, p0, vb);  // b; next j
+    operand(std::integral_constant<int, 9>{}, true, p0, vb);  // b; next j
     {
       double gq[4][3];
 #pragma unroll
@@ -459,7 +468,7 @@ __global__ void __launch_bounds__(384, 2) fast_bundle_r3_kernel(const R3BundleAr
       __syncthreads();
       r3_combine<3>(xs, kR3RS, tws, outs(3, 3), p0, a.np, v16o);  // u x b
     }
-    operand(more ? 0 : -1, p0 + 8 * (int64_t)gridDim.x, vx);  // j; next the u of the CTA's next tile
+    operand(std::integral_constant<int, 0>{}, more, p0 + 8 * (int64_t)gridDim.x, vx);  // j; next the next tile's u
     {
       double gq[4][3];
 #pragma unroll
