@@ -412,6 +412,10 @@ int sfnl_set_bundle_kernel(int kind);
  * operations gives up (no GPU work is involved).  The next split-form call
  * returns SFNL_ERR_TIMEOUT and clears the word, as after a real timeout. */
 int sfnl_test_inject_timeout(void);
+/* Test hook: bounds the two workspaces of the large-m FAST form (grid values; the residues' coefficients and
+ * sums) to `bytes` so that small calls run many point chunks and batch groups, the path very large calls
+ * take; 0 restores the production bounds.  Process-wide.  bytes < 0: SFNL_ERR_ARG. */
+int sfnl_test_large_workspace_cap(int64_t bytes);
 /* Device-timed seconds of the last host-array call of this thread (the *_host,
  * sfnl_fft_* and sfnl_smb_* entries): [0] host<->device copies, [1] kernels,
  * [2] 0 (nothing is repacked).  Each is a sum over the call's point chunks; the

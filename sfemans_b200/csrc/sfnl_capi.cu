@@ -534,6 +534,11 @@ int sfnl_set_check_finite(int on) {
   return SFNL_OK;
 }
 int sfnl_test_inject_timeout(void) { return split_inject_timeout(); }
+int sfnl_test_large_workspace_cap(int64_t bytes) {
+  if (bytes < 0) return set_error(SFNL_ERR_ARG, "workspace bound must be >= 0");
+  large_test_workspace_cap((size_t)bytes);
+  return SFNL_OK;
+}
 int sfnl_set_bundle_kernel(int kind) {
   if (kind != SFNL_BUNDLE_RESIDUE && kind != SFNL_BUNDLE_THIRD_FOLD)
     return set_error(SFNL_ERR_ARG, "bundle kernel: SFNL_BUNDLE_RESIDUE or SFNL_BUNDLE_THIRD_FOLD");

@@ -8,6 +8,7 @@
 
 #include <cstring>
 #include <map>
+#include <atomic>
 #include <mutex>
 #include <tuple>
 
@@ -630,6 +631,9 @@ int launch_large_syn(const LargeArgs &la, int nfields, int nbz, bool tf, cudaStr
 }
 
 constexpr size_t kLargeWorkspaceBytes = size_t(1) << 30;  // grid values of one point chunk
+// Tests only (sfnl_test_large_workspace_cap): a bound on both workspaces far below the production ones, so
+// that small calls run many point chunks and batch groups; 0: none.
+std::atomic<size_t> g_test_cap{0};
 // Batched programs (tangents): the workspace may grow to this, or to a quarter of the free device memory,
 // so that one launch serves every batch entry of a point chunk of at least kLargeMinChunk points.
 constexpr size_t kLargeBatchWorkspaceBytes = size_t(8) << 30;
@@ -691,6 +695,13 @@ int run_large(const ProgArgs &a, const Geo &g, const Tables &T, const LargePlan 
     const int64_t fit = bcap > shared_b ? (int64_t)((bcap - shared_b) / per_entry) : 0;
     kb = (int)(fit < 1 ? 1 : fit > a.batch ? a.batch : fit);
     cap = bcap;
+  }
+  if (const size_t tc = g_test_cap.load()) {
+    cap = tc;
+    if (a.batch > 1 && nown > 0) {
+      const int64_t fit = (int64_t)(tc / (field_bytes * (size_t)(nshared + nown) * 32));
+      kb = (int)(fit < 1 ? 1 : fit > a.batch ? a.batch : fit);
+    }
   }
   const size_t per_point = field_bytes * (size_t)(nshared + (int64_t)kb * nown);
   int64_t chunk = (int64_t)(cap / per_point);
@@ -968,6 +979,7 @@ int launch_large_r3(const ProgArgs &a, const Geo &g, cudaStream_t st) {
   size_t cap = free_b / 4;
   if (cap > (size_t(32) << 30)) cap = size_t(32) << 30;
   if (cap < (size_t(1) << 30)) cap = size_t(1) << 30;
+  if (const size_t tc = g_test_cap.load()) cap = tc;
   int64_t chunk = (int64_t)(cap / per_point);
   chunk = (chunk / 32) * 32;
   if (chunk < 32) chunk = 32;
@@ -1019,6 +1031,8 @@ int launch_large_r3(const ProgArgs &a, const Geo &g, cudaStream_t st) {
 }
 
 }  // namespace
+
+void large_test_workspace_cap(size_t bytes) { g_test_cap.store(bytes); }
 
 void large_r3_release_tables() {
   std::lock_guard<std::mutex> lk(g_r3l_mu);

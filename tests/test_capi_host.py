@@ -66,6 +66,11 @@ def test_bundle_kernel_switch():
         sf.set_bundle_kernel(prev)
 
 
+def test_large_workspace_bound_hook_checks_its_argument():
+    assert sf.lib().sfnl_test_large_workspace_cap(-1) == -1 and sf.last_error()
+    assert sf.lib().sfnl_test_large_workspace_cap(0) == 0
+
+
 def test_zero_points_is_a_no_op():
     assert sf.lib().sfnl_product_f64(0, NULL, NULL, NULL, 0, 4, 6, 0, 0, NULL) == 0
 

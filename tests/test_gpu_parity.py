@@ -329,6 +329,25 @@ def test_large_m_linearised_point_chunks():
         assert R.rel_l2(jv[:, 6:, :, t], R.cross_jvp(u, b, du, db, pad, engine=eng)) <= FP64_TOL
 
 
+@pytest.mark.parametrize("m,pad", [(128, 192), (256, 384)])
+def test_large_m_small_workspace_bound(m, pad):
+    # a test-only workspace bound (2 MB) makes the large-m form run many point chunks (and, for the tangents,
+    # batch groups of one entry): at m = 256 the residues' coefficients and sums, at m = 128 the grid values
+    npts, k = 1201, 3
+    u, w = (R.synthetic_field(npts, 6, m, 0.05, 600 + i) for i in range(2))
+    tan = _batched(npts, 12, m, k, 0.05, 610)
+    ref_cross = R.fft_par("cross", u, w, pad, workers=8)
+    ref_jvp = host(sf.cross_jvp(dev(u), dev(w), dev(tan), m_max_pad=pad))  # production bounds: one chunk
+    assert sf.lib().sfnl_test_large_workspace_cap(2 << 20) == 0
+    try:
+        out = host(sf.product(0, dev(u), dev(w), m_max_pad=pad, algo=sf.ALGO_FAST))
+        jvp = host(sf.cross_jvp(dev(u), dev(w), dev(tan), m_max_pad=pad))
+    finally:
+        assert sf.lib().sfnl_test_large_workspace_cap(0) == 0
+    assert R.rel_l2(out, ref_cross) <= FP64_TOL
+    assert R.rel_l2(jvp, ref_jvp) <= 1e-13
+
+
 def test_large_m_point_chunks():
     # more points than one workspace chunk of grid values holds (about 29k points at m = 256)
     npts, m, pad = 70_001, 256, 384
