@@ -19,8 +19,8 @@
 // minus its imaginary part, the grid being alias-free for the product of two fields of 64 modes
 // (fft_parallel.F90:147-328 on its own grid gives the same truncated product).
 //
-// CTA: one 8-point tile, 12 warps = 3 residue groups of 4 warps (tile tau of the 16-angle quadrant,
-// half 0 cosine / 1 sine classes).  A group's synthesis, exchanges, products and analysis touch only its
+// CTA: 8-point tiles one after the other (kR3TilesPerCta of them), 12 warps = 3 residue groups of 4 warps
+// (tile tau of the 16-angle quadrant, half 0 cosine / 1 sine classes).  A group's synthesis, exchanges, products and analysis touch only its
 // own shared memory and synchronise on its own named barrier; the CTA meets only where the twiddles mix
 // the residues (after the coefficients arrive, and before the outputs are combined).  The DFT tables
 // of a residue transform are 14 KB (L1-resident) instead of the 86 KB that streamed from L2.
