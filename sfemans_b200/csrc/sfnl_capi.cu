@@ -166,6 +166,8 @@ ProgArgs make_args(int op, int64_t np, int m, int N, int batch) {
   return a;
 }
 
+int timeout_error();
+
 int run_fp64(ProgArgs a, int algo, int N_caller, cudaStream_t st) {
   const bool alias_free = dealiased(a.m, N_caller);
   if (algo == SFNL_ALGO_AUTO)
@@ -181,18 +183,21 @@ int run_fp64(ProgArgs a, int algo, int N_caller, cudaStream_t st) {
     if (!alias_free) return set_error(SFNL_ERR_ALIAS, "FAST form needs a dealiasing pad (2*m_max_pad-1 >= 3*m_max-2)");
     a.N = fast_grid_length(a.m);
     if (!fast_supported(a.op, a.m, a.N)) return set_error(SFNL_ERR_UNSUPPORTED, "FAST form not built for this size");
+    // the MHD bundle's bounded waits report through the same word as the split kernels' (see run_split)
+    if (a.op == OP_BUNDLE && split_take_status()) return timeout_error();
     rc = launch_fast(a, st);
   } else {
     return set_error(SFNL_ERR_ARG, "unknown algo");
   }
   if (rc == SFNL_OK && g_check_finite) rc = scan_outputs(a, st);
+  if (rc == SFNL_OK && g_check_finite && a.op == OP_BUNDLE && split_take_status()) rc = timeout_error();
   return rc;
 }
 
 int timeout_error() {
   return set_error(SFNL_ERR_TIMEOUT,
-                   "a split-form kernel gave up waiting for its tensor-core operations: the outputs of that call are "
-                   "incomplete");
+                   "a kernel gave up a bounded wait (a split-form kernel on its tensor-core operations, or the FAST "
+                   "MHD bundle on its bulk copies): the outputs of that call are incomplete");
 }
 
 int run_split(ProgArgs a, int split, int N_caller, cudaStream_t st) {

@@ -34,6 +34,7 @@ int launch_split(const ProgArgs &a, int split, cudaStream_t st);  // sfnl_split.
 void split_release_tables();                            // sfnl_split.cu
 int split_take_status();     // 1 if a split kernel gave up a bounded wait since the last call; clears it
 int split_inject_timeout();  // sets that status from the host (tests of the error path)
+int wait_status_word(int **dev);  // that status word's device address (kernels with bounded waits set it)
 // Synthesis only (sfnl_synth.cu): out (N, nslot/2, np); vmax a zeroed device double that receives the
 // maximum of |v|; pmax (np) the maximum of |v| of each point.
 int launch_real(const double *v, double *out, int64_t np, int nslot, int m, int N, cudaStream_t st);

@@ -308,9 +308,12 @@ __global__ void __launch_bounds__(kLargeSynMaxWarps * 32, 1) large_syn_tf_kernel
 
 // Program and analysis with the third fold: chunks of two angle-tile pairs (t, t+1 and their mirrors); the
 // odd output groups contract all four tiles, the even ones P(t) +- P(mirror) over the first-half tiles
-// (signs PE0 +, PE2 -, QE0 -, QE2 +).
+// (signs PE0 +, PE2 -, QE0 -, QE2 +).  With up to two output tiles per warp (m <= 256 on the grid's residue
+// classes, m <= 192 without them) the kernel is held to 64 registers, two CTAs per SM: a spill of about
+// 136 bytes buys twice the resident warps, 4-11 % faster on a B200 from m = 128 to 256; with more tiles per
+// warp the accumulators spill too much and one CTA per SM was as fast or faster (m = 384, 512).
 template <int OP, int O0, int CPW>
-__global__ void __launch_bounds__(kLargeProdWarps * 32) large_prod_tf_kernel(const LargeArgs a) {
+__global__ void __launch_bounds__(kLargeProdWarps * 32, CPW <= 2 ? 2 : 1) large_prod_tf_kernel(const LargeArgs a) {
   constexpr int NI = op_nin(OP), NO = op_nout(OP);
   constexpr int NOG = NO - O0 < kLargeGroup ? NO - O0 : kLargeGroup;
   constexpr int KP = kLargeTfPairs, LT = 2 * KP;  // pairs per chunk, local tiles

@@ -24,6 +24,8 @@
 // own shared memory and synchronise on its own named barrier; the CTA meets only where the twiddles mix
 // the residues (after the coefficients arrive, and before the outputs are combined).  The DFT tables
 // of a residue transform are 14 KB (L1-resident) instead of the 86 KB that streamed from L2.
+#include <cuda.h>  // CUtensorMap (the encoder is reached through the runtime's driver entry point)
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -46,7 +48,8 @@ constexpr int kR3KS = 16;                  // synthesis k-steps of a field (64 c
 constexpr int kR3RS = 3 * kR3KS * 32;      // doubles per residue: 3 fields' A fragments
 constexpr int kR3PS = 4 * 4 * kR3NT * 64;  // doubles per residue: 4 product slots x 4 classes x 16 angles x 8
 constexpr int kR3TilesPerCta = 4;          // tiles walked by one CTA (see fast_bundle_r3_kernel)
-constexpr int kR3Smem = (3 * 128 * 8 + 3 * kR3RS + 3 * kR3PS + 128) * (int)sizeof(double);  // 109 KB
+constexpr int kR3Smem = (3 * 128 * 8 + 3 * kR3RS + 3 * kR3PS + 128 + 2) * (int)sizeof(double);  // 109 KB
+constexpr int kR3StageBytes = 3 * 128 * 8 * (int)sizeof(double);  // one operand's three staged fields
 
 // Row groups of a residue transform: 0 CE0 (cos 4k), 1 CE2 (cos 4k+2), 2 CO (cos 2k+1), 3 SE0 (sin 4k+4,
 // mode 32 included), 4 SE2 (sin 4k+2), 5 SO (sin 2k+1).  The third fold needs the even groups split by
@@ -74,11 +77,15 @@ __device__ __forceinline__ int r3_sin_row(int k) {
   return (k & 1) ? 4 * r3_koff(5) + (k >> 1) : (k & 2) ? 4 * r3_koff(4) + (k >> 2) : 4 * r3_koff(3) + (k >> 2) - 1;
 }
 
-// Shared-memory orders chosen so that every warp access below is conflict-free (a half-warp's 16 8-byte
-// accesses on 16 distinct bank pairs): the staged row of mode n (r3_stage, r3_precombine), and the row and
-// point swizzle of slot s of the analysed sums (cos mode k at slot k, sine mode k at 32 + k % 32;
-// r3_analysis writes them, r3_combine reads them).
-__device__ __forceinline__ int r3_xrow(int n) { return n ^ (((n >> 1) ^ (n >> 2)) & 1); }
+// Shared-memory orders chosen so that every warp access below is conflict-free (each quarter-warp's eight
+// 16-byte accesses, or each half-warp's sixteen 8-byte ones, on distinct banks): the staged row of mode n
+// (r3_stage / the bulk tensor copies, r3_precombine) and the row and point swizzle of slot s of the
+// analysed sums (cos mode k at slot k, sine mode k at 32 + k % 32; r3_analysis writes them, r3_combine
+// reads them).  The staged row moves bit 2 of the mode to the bottom, (n >> 3, n & 3, (n >> 2) & 1), an
+// order a five-dimensional tensor map copies directly (one dimension per group of mode bits), so that the
+// 64-byte rows that one quarter-warp of r3_precombine reads (modes k = 4i and 4i + 4, 4i + 2 and 4i + 6, or
+// odd modes paired with bit 1 of their task flipped) sit on opposite halves of the banks.
+__host__ __device__ __forceinline__ int r3_trow(int n) { return ((n >> 3) << 3) | ((n & 3) << 1) | ((n >> 2) & 1); }
 __device__ __forceinline__ int r3_rpos(int s, int p) { return (s ^ (((s >> 2) ^ (s >> 4)) & 1)) * 8 + (p ^ (((s >> 3) & 1) << 2)); }
 
 struct R3Tables {
@@ -146,17 +153,65 @@ struct R3Fields {  // three fields: cos of mode n, point p at p[f][p + n*ldm[f]]
   int64_t ldm[3];
 };
 
-// Stages the three fields of the 8-point tile at p0 into xr [3][128 rows: cos 0..63, sin 0..63][8 points]
-// with cp.async and commits one group (the sine of mode 0 is not read: zero).  384 threads: thread t copies
-// 16 bytes (points pc, pc + 1) of rows rb, rb + 32 (cosines) and 64 + rb, 96 + rb (sines) of field t / 128,
-// rb = (t % 128) / 4, so that four consecutive threads move one whole 64-byte row and every address derives
-// from two bases by constant offsets.
+// Bulk tensor copies of the staged fields: one tensor map per input field over (point, bit 2 of the mode,
+// mode & 3, mode >> 3, cos/sin) with the box (8, 2, 4, 8, 2) lands an 8-point tile in xr's row order
+// (r3_trow) in one copy; a single thread issues an operand's three copies on the stage barrier, whose
+// transaction count is the 24 KB they write (points past np arrive as zeros).  No multicast: each CTA
+// fetches its own tile.
+__device__ __forceinline__ uint32_t r3_smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void r3_bar_init(uint64_t *bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(r3_smem_addr(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Issued by one thread after a CTA barrier that ends every read of xr.
+__device__ __forceinline__ void r3_bulk_stage(double *xr, const CUtensorMap *const (&maps)[3], int64_t p0,
+                                              uint64_t *bar) {
+  const uint32_t b = r3_smem_addr(bar);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the generic reads of xr before the copies
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(kR3StageBytes) : "memory");
+  const int x = (int)p0;
+#pragma unroll
+  for (int f = 0; f < 3; ++f)
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %3, %3, %3}], [%4];"
+        ::"r"(r3_smem_addr(xr + (size_t)f * 128 * 8)), "l"(reinterpret_cast<uint64_t>(maps[f])), "r"(x), "r"(0), "r"(b)
+        : "memory");
+}
+
+// Bounded wait for phase `parity` of the stage barrier; false if it gave up (the copies never landed).
+__device__ __forceinline__ bool r3_bar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t b = r3_smem_addr(bar);
+  for (int it = 0; it < (1 << 22); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(b), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// Stages the three fields of the 8-point tile at p0 into xr [3][128 rows: cos, then sin, of mode n at row
+// r3_trow(n)][8 points] with cp.async and commits one group (the sine of mode 0 is not read: zero); the
+// form for inputs that the bulk tensor copies cannot take (odd np, unaligned bases or odd mode strides).
+// 384 threads: thread t copies 16 bytes (points pc, pc + 1) of modes rb, rb + 32 (cosines and sines) of
+// field t / 128, so that four consecutive threads move one whole 64-byte row and every address derives
+// from two bases by constant offsets; rb swaps bits 0 and 2 of (t % 128) / 4, so that a quarter-warp's two
+// rows sit on opposite bank halves.
 __device__ __forceinline__ void r3_stage(double *xr, const R3Fields &fs, int64_t p0, int64_t np, bool vec16) {
-  const int t = threadIdx.x, f = t >> 7, pc = 2 * (t & 3), rb = (t & 127) >> 2;
+  const int t = threadIdx.x, f = t >> 7, pc = 2 * (t & 3), j = (t & 127) >> 2;
+  const int rb = (j & ~5) | ((j & 1) << 2) | ((j >> 2) & 1);
   const double *base = f == 0 ? fs.p[0] : f == 1 ? fs.p[1] : fs.p[2];
   const int64_t ldm = f == 0 ? fs.ldm[0] : f == 1 ? fs.ldm[1] : fs.ldm[2];
   const double *src = base + p0 + pc + (int64_t)rb * ldm;        // cosine row rb; rb + 32 at 32 ldm, sines np on
-  double *dst = xr + ((size_t)f * 128 + r3_xrow(rb)) * 8 + pc;  // r3_xrow(rb + 32) = r3_xrow(rb) + 32
+  double *dst = xr + ((size_t)f * 128 + r3_trow(rb)) * 8 + pc;  // r3_trow(rb + 32) = r3_trow(rb) + 32
   const bool v16 = vec16 && p0 + 8 <= np, pv0 = p0 + pc < np, pv1 = p0 + pc + 1 < np;
   // a rolled loop: the four copies' addresses at once would cost registers the synthesis needs
 #pragma unroll 1
@@ -180,11 +235,15 @@ __device__ __forceinline__ void r3_stage(double *xr, const R3Fields &fs, int64_t
 // blocks.  tws: cos, sin of 2 pi n / 192 in shared memory.
 __device__ __forceinline__ void r3_precombine(const double *xr, double *xs, const double *tws) {
   const int t = threadIdx.x;
-  const int p = 2 * (t & 3), rc = (t >> 2) & 31, f = t >> 7;
+  // task rc: even modes (rc < 16) in order, odd ones with bit 1 flipped on odd slots, so that the two tasks
+  // of a quarter-warp differ in the parity of rc (their A-fragment stores) and in bit 2 of their modes
+  // (their staged rows)
+  const int p = 2 * (t & 3), j = (t >> 2) & 31, f = t >> 7;
+  const int rc = j < 16 ? j : 16 + ((j - 16) ^ ((j & 1) << 1));
   const int k = rc < 8 ? 4 * rc : rc < 16 ? 4 * (rc - 8) + 2 : 2 * (rc - 16) + 1;  // cosine mode of row rc
   const double *x = xr + (size_t)f * 128 * 8 + p;
-  auto cosv = [&](int n) { return *reinterpret_cast<const double2 *>(x + r3_xrow(n) * 8); };
-  auto sinv = [&](int n) { return *reinterpret_cast<const double2 *>(x + (64 + r3_xrow(n)) * 8); };
+  auto cosv = [&](int n) { return *reinterpret_cast<const double2 *>(x + r3_trow(n) * 8); };
+  auto sinv = [&](int n) { return *reinterpret_cast<const double2 *>(x + (64 + r3_trow(n)) * 8); };
   double2 al[3], be[3];
   int rs;
   if (k == 0) {
@@ -370,6 +429,7 @@ __device__ __forceinline__ void r3_combine(const double *R, int rstride, const d
 }
 
 struct R3BundleArgs {
+  CUtensorMap tm[15];    // bulk-copy maps of the inputs (the kTma kernel)
   const double *in[15];  // u 0-2, w 3-5, b 6-8, j 9-11, gradT 12-14
   double *out[10];       // u x w 0-2, u x b 3-5, j x b 6-8, u . gradT 9
   int64_t in_ldm[15], out_ldm[10];
@@ -377,6 +437,7 @@ struct R3BundleArgs {
   int vec16;     // inputs: bases 16-byte aligned, even mode strides and np
   int vec16out;  // outputs: the same
   const double *syn, *ana, *tw;
+  int *status;  // the mapped wait-status word (set if a bounded wait on the bulk copies gave up)
 };
 
 // The MHD bundle (u x w, u x b, j x b, u . gradT) on the residue grids, one CTA per 8-point tile (CTAs that
@@ -385,14 +446,23 @@ struct R3BundleArgs {
 // five vector operands are staged and transformed one after the other (u, w, gradT, b, j; each one's
 // copies issued as soon as the previous one's coefficients are combined), u's and b's grid values stay in
 // registers while their partners are transformed, and the products are analysed in three rounds (u x w
-// with u . gradT; u x b; j x b).
-__global__ void __launch_bounds__(384, 2) fast_bundle_r3_kernel(const R3BundleArgs a) {
-  extern __shared__ double smem[];
+// with u . gradT; u x b; j x b).  kTma: the operands arrive by bulk tensor copies (r3_bulk_stage) on the
+// stage barrier, else by every thread's cp.async (r3_stage).
+template <bool kTma>
+__global__ void __launch_bounds__(384, 2) fast_bundle_r3_kernel(const __grid_constant__ R3BundleArgs a) {
+  extern __shared__ __align__(128) double smem[];
   double *xr = smem;                  // staged coefficients of one operand
   double *xs = xr + 3 * 128 * 8;      // per residue: A fragments, then the exchanges, then the analysed sums
   double *ps = xs + 3 * kR3RS;        // per residue: folded products (then the fourth output's sums)
   double *tws = ps + 3 * kR3PS;       // twiddles cos, sin of 2 pi n / 192
+  uint64_t *sbar = reinterpret_cast<uint64_t *>(tws + 128);  // stage barrier (kTma)
   if (threadIdx.x < 128) tws[threadIdx.x] = __ldg(a.tw + threadIdx.x);
+  if constexpr (kTma) {
+    if (threadIdx.x == 0) r3_bar_init(sbar);
+    __syncthreads();
+  }
+  uint32_t phase = 0;     // parity of the stage barrier's next phase
+  bool gave_up = false;   // a bounded wait on the copies ran out
   const int warp = threadIdx.x >> 5, r = warp >> 2, wg = warp & 3, tau = wg >> 1, half = wg & 1;
   double *xs_r = xs + (size_t)r * kR3RS, *ps_r = ps + (size_t)r * kR3PS;
   const GroupSync gsync{r};
@@ -415,16 +485,32 @@ __global__ void __launch_bounds__(384, 2) fast_bundle_r3_kernel(const R3BundleAr
     }
     return os;
   };
+  // the copies of the operand whose fields start at a.in[NEXT] for the tile at p0
+  auto stage = [&](auto tag, int64_t p0) {
+    constexpr int NEXT = decltype(tag)::value;
+    if constexpr (kTma) {
+      if (threadIdx.x == 0) {
+        const CUtensorMap *const mp[3] = {&a.tm[NEXT], &a.tm[NEXT + 1], &a.tm[NEXT + 2]};
+        r3_bulk_stage(xr, mp, p0, sbar);
+      }
+    } else {
+      r3_stage(xr, fields(NEXT), p0, a.np, a.vec16 != 0);
+    }
+  };
   // one operand: wait for its copies, form the residues' coefficients, issue the copies of the operand whose
   // fields start at a.in[NEXT] (a compile-time index, so that the kernel parameters are read at fixed offsets)
   // at point next_p0 when stage_next, synthesise the group's residue, fold
   auto operand = [&](auto next_tag, bool stage_next, int64_t next_p0, double (&v)[4][3]) {
-    constexpr int NEXT = decltype(next_tag)::value;
-    cp_async_wait_0();
+    if constexpr (kTma) {
+      if (!r3_bar_wait(sbar, phase)) gave_up = true;
+      phase ^= 1;
+    } else {
+      cp_async_wait_0();
+    }
     __syncthreads();  // the copies have landed; the previous round's sums are read
     r3_precombine(xr, xs, tws);
     __syncthreads();  // xs complete, xr read
-    if (stage_next) r3_stage(xr, fields(NEXT), next_p0, a.np, a.vec16 != 0);
+    if (stage_next) stage(next_tag, next_p0);
     double acc_e[3][2], acc_o[3][2];
     r3_synth(xs_r, a.syn, tau, half, acc_e, acc_o);
     gsync();  // the group has read its A fragments: the exchanges overlay them
@@ -432,7 +518,7 @@ __global__ void __launch_bounds__(384, 2) fast_bundle_r3_kernel(const R3BundleAr
   };
   const int64_t ntiles = (a.np + 7) / 8;
   int64_t tile = blockIdx.x;
-  if (tile < ntiles) r3_stage(xr, fields(0), tile * 8, a.np, a.vec16 != 0);  // u of the first tile
+  if (tile < ntiles) stage(std::integral_constant<int, 0>{}, tile * 8);  // u of the first tile
   for (; tile < ntiles; tile += gridDim.x) {
     const int64_t p0 = tile * 8;
     const bool more = tile + gridDim.x < ntiles;
@@ -480,9 +566,48 @@ __global__ void __launch_bounds__(384, 2) fast_bundle_r3_kernel(const R3BundleAr
       r3_combine<3>(xs, kR3RS, tws, outs(6, 3), p0, a.np, v16o);  // j x b
     }
   }
+  if (kTma && gave_up) {
+    // the call's outputs are incomplete: say so, and give a copy still in flight one more bounded wait
+    // before the CTA's shared memory is released
+    if (a.status) {
+      *reinterpret_cast<volatile int *>(a.status) = 1;
+      __threadfence_system();
+    }
+    r3_bar_wait(sbar, phase ^ 1);
+  }
 }
 
 }  // namespace
+
+// cuTensorMapEncodeTiled through the runtime (the library links no driver library); null if absent.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+// The bulk-copy map of one input field (cos of mode n, point p at base[p + n ldm], sine np further): dims
+// (point, bit 2 of n, n & 3, n >> 3, cos/sin), box (8, 2, 4, 8, 2).  Needs a 16-byte aligned base and even
+// ldm and np (strides in multiples of 16 bytes), which the caller has checked.
+static bool encode_field_map(PFN_cuTensorMapEncodeTiled_v12000 enc, CUtensorMap *map, const double *base, int64_t ldm,
+                      int64_t np) {
+  const cuuint64_t dims[5] = {(cuuint64_t)np, 2, 4, 8, 2};
+  const cuuint64_t strides[4] = {(cuuint64_t)(4 * ldm * 8), (cuuint64_t)(ldm * 8), (cuuint64_t)(8 * ldm * 8),
+                                 (cuuint64_t)(np * 8)};
+  const cuuint32_t box[5] = {8, 2, 4, 8, 2}, estr[5] = {1, 1, 1, 1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<double *>(base), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 int launch_bundle_r3(const ProgArgs &a, cudaStream_t st) {
   R3BundleArgs ba;
@@ -507,11 +632,18 @@ int launch_bundle_r3(const ProgArgs &a, cudaStream_t st) {
   ba.syn = T.syn();
   ba.ana = T.ana();
   ba.tw = T.tw();
-  if (cudaFuncSetAttribute(fast_bundle_r3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kR3Smem) != cudaSuccess)
+  // bulk tensor copies where every field's strides allow them (tile coordinates are 32-bit)
+  bool tma = v16 && a.np < ((int64_t)1 << 31);
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tma ? tensor_map_encoder() : nullptr;
+  for (int f = 0; f < 15 && tma; ++f) tma = enc && encode_field_map(enc, &ba.tm[f], a.in[f], a.in_ldm[f], a.np);
+  if (tma)
+    if (int rc = wait_status_word(&ba.status)) return rc;
+  auto kern = tma ? fast_bundle_r3_kernel<true> : fast_bundle_r3_kernel<false>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kR3Smem) != cudaSuccess)
     return set_error(SFNL_ERR_CUDA, "cudaFuncSetAttribute failed (residue-split bundle)");
   const int64_t tiles = (a.np + 7) / 8, ctas = (tiles + kR3TilesPerCta - 1) / kR3TilesPerCta;
   if (ctas > 0x7fffffff) return set_error(SFNL_ERR_UNSUPPORTED, "np too large");
-  fast_bundle_r3_kernel<<<(unsigned)ctas, 384, kR3Smem, st>>>(ba);
+  kern<<<(unsigned)ctas, 384, kR3Smem, st>>>(ba);
   return check_launch("fast form (residue-split bundle)");
 }
 

@@ -929,6 +929,8 @@ int split_take_status() {
   return __atomic_exchange_n(reinterpret_cast<volatile int *>(g_status_host), 0, __ATOMIC_SEQ_CST);
 }
 
+int wait_status_word(int **dev) { return status_word(dev); }
+
 int split_inject_timeout() {
   int *d = nullptr;
   if (int rc = status_word(&d)) return rc;

@@ -124,10 +124,11 @@ def test_mhd_bundle(npts, m, algo):
         assert R.rel_l2(host(o), r) <= FP64_TOL
 
 
-@pytest.mark.parametrize("npts", [1, 7, 61, 3001, 100_003])
+@pytest.mark.parametrize("npts", [1, 7, 61, 3001, 100_003, 2, 64, 3002, 100_002])
 def test_bundle_kernels_agree(npts):
     # the two kernels of the m = 64 bundle (grid split into its residue classes; one 192-angle transform)
-    # against each other, and against the oracle where it is cheap; odd counts take the 8-byte copies
+    # against each other, and against the oracle where it is cheap; odd counts take the 8-byte copies,
+    # even ones the residue kernel's bulk tensor copies (2 and 3002: a last tile past np, filled with zeros)
     m, pad = 64, 96
     f = [R.synthetic_field(npts, 6, m, 0.1, 700 + i) for i in range(5)]
     d = [dev(x) for x in f]
@@ -138,7 +139,7 @@ def test_bundle_kernels_agree(npts):
         r3 = [host(o) for o in sf.bundle_mhd(*d, m_max_pad=pad)]
     finally:
         sf.set_bundle_kernel(prev)
-    refs = R.mhd_bundle(*f, pad) if npts <= 3001 else None
+    refs = R.mhd_bundle(*f, pad) if npts <= 3002 else None
     for i in range(4):
         assert R.rel_l2(r3[i], tf[i]) <= 1e-13
         if refs is not None:
