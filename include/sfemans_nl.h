@@ -62,7 +62,9 @@ enum {
   SFNL_ERR_NONFINITE = -6,   /* (check mode) a NaN/Inf was found in the output */
   SFNL_ERR_ALLOC = -7,       /* device or pinned host allocation failed */
   SFNL_ERR_TIMEOUT = -8      /* a split-form kernel gave up a bounded wait on its tensor-core
-                                operations; the outputs of that call are incomplete */
+                                operations, or the FAST MHD bundle on its bulk copies; the outputs of
+                                that call are incomplete (reported by the next call of that form or
+                                at the end of a host-array call) */
 };
 
 /* Algorithm of the all-FP64 forms. */
@@ -416,6 +418,12 @@ int sfnl_test_inject_timeout(void);
  * sums) to `bytes` so that small calls run many point chunks and batch groups, the path very large calls
  * take; 0 restores the production bounds.  Process-wide.  bytes < 0: SFNL_ERR_ARG. */
 int sfnl_test_large_workspace_cap(int64_t bytes);
+/* Test hook: the number of residue classes (3, 6 or 12) into which the large-m FAST form splits its
+ * 3m-angle grid, where the split gives whole quadrant-tile pairs (3m/R a multiple of 64, at most 512), else
+ * the whole grid; 0 restores the automatic choice (from m = 256 the most classes that leave residue grids
+ * of at least 192 angles: 3 at m = 256, 6 at m = 384 and 512; the whole grid below m = 256).  Every choice gives the same products to rounding.  Process-wide.  Other values:
+ * SFNL_ERR_ARG. */
+int sfnl_test_large_residues(int R);
 /* Device-timed seconds of the last host-array call of this thread (the *_host,
  * sfnl_fft_* and sfnl_smb_* entries): [0] host<->device copies, [1] kernels,
  * [2] 0 (nothing is repacked).  Each is a sum over the call's point chunks; the

@@ -109,6 +109,7 @@ _SIGS = {
     "sfnl_test_inject_timeout": [],
     "sfnl_set_bundle_kernel": [_I],
     "sfnl_test_large_workspace_cap": [_L],
+    "sfnl_test_large_residues": [_I],
     "sfnl_probe_fp64_tflops": [_P, _P],
     "sfnl_fft_par_pack_modes": [_P, _P] + [_I] * 6,
     "sfnl_fft_par_block": [_I, _P, _P, _P] + [_I] * 4 + [_P],

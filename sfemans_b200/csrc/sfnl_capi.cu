@@ -544,6 +544,11 @@ int sfnl_test_large_workspace_cap(int64_t bytes) {
   large_test_workspace_cap((size_t)bytes);
   return SFNL_OK;
 }
+int sfnl_test_large_residues(int R) {
+  if (R != 0 && R != 3 && R != 6 && R != 12) return set_error(SFNL_ERR_ARG, "residue classes: 0, 3, 6 or 12");
+  large_test_residues(R);
+  return SFNL_OK;
+}
 int sfnl_set_bundle_kernel(int kind) {
   if (kind != SFNL_BUNDLE_RESIDUE && kind != SFNL_BUNDLE_THIRD_FOLD)
     return set_error(SFNL_ERR_ARG, "bundle kernel: SFNL_BUNDLE_RESIDUE or SFNL_BUNDLE_THIRD_FOLD");

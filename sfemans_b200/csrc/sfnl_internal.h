@@ -30,6 +30,7 @@ int fast_grid_length(int m);                            // sfnl_fast.cu
 void fast_release_tables();                             // sfnl_fast.cu
 void large_release_workspaces();                        // sfnl_large.cu: the grid-value workspaces
 void large_test_workspace_cap(size_t bytes);            // sfnl_large.cu: tests' workspace bound (0: none)
+void large_test_residues(int R);                        // sfnl_large.cu: tests' residue classes (0: automatic)
 int launch_split(const ProgArgs &a, int split, cudaStream_t st);  // sfnl_split.cu
 void split_release_tables();                            // sfnl_split.cu
 int split_take_status();     // 1 if a split kernel gave up a bounded wait since the last call; clears it

@@ -521,7 +521,7 @@ __global__ void __launch_bounds__(kLargeProdWarps * 32) large_prod_kernel(const 
 }
 
 // workspaces, one per (device, stream, use): calls on different streams do not share them.  Use 0: the
-// grid values; 1: the residue coefficients and sums of launch_large_r3.
+// grid values; 1: the residue coefficients and sums of launch_large_res.
 std::mutex g_lws_mu;
 std::map<std::tuple<int, cudaStream_t, int>, std::pair<double *, size_t>> g_lws;
 
@@ -644,7 +644,7 @@ constexpr int64_t kLargeMinChunk = 4096;
 
 }  // namespace
 
-void large_r3_release_tables();
+void large_res_release_tables();
 
 void large_release_workspaces() {
   std::lock_guard<std::mutex> lk(g_lws_mu);
@@ -657,7 +657,7 @@ void large_release_workspaces() {
     }
   g_lws.clear();
   cudaSetDevice(prev);
-  large_r3_release_tables();
+  large_res_release_tables();
 }
 
 namespace {
@@ -673,7 +673,7 @@ struct LargePlan {
 // launch per group of three outputs (blockIdx.y = entry).  The grid-value workspace holds the shared
 // fields and kb entries' own fields of one point chunk: kb = the whole batch when a chunk of at least
 // kLargeMinChunk points fits the batched workspace bound, else as many entries as such a chunk allows.
-// rp: a residue pass (launch_large_r3): the residue grid's geometry and tables, the Nyquist mode in the
+// rp: a residue pass (launch_large_res): the residue grid's geometry and tables, the Nyquist mode in the
 // sine row of mode 0, no analysis weights and no cotangent weights (both applied outside).
 int run_large(const ProgArgs &a, const Geo &g, const Tables &T, const LargePlan *rp, cudaStream_t st) {
   const int ni = op_nin(a.op), no = op_nout(a.op);
@@ -799,48 +799,71 @@ int run_large(const ProgArgs &a, const Geo &g, const Tables &T, const LargePlan 
 }
 
 // ---------------------------------------------------------------------------
-// the grid's three residue classes (m = 256, 512)
+// the grid's residue classes (m >= 256)
 // ---------------------------------------------------------------------------
-// On theta_j = pi(2j+1)/N with N = 3m, j = 3i + r gives theta_j = phi_i + d_r, phi_i = pi(2i+1)/m the offset
-// m-angle grid and d_r = 2 pi (r-1)/N.  A field Re sum_n z_n e^{i n theta} (z_n = a_n - i b_n, n < m) is on
-// residue r the series of y_n = z_n e^{i n d_r} on phi, where e^{i m phi_i} = -1 folds the modes k and m - k
-// into alpha_k - i beta_k = y_k - conj(y_{m-k}) (k = 1 .. m/2 - 1), alpha_0 = a_0, and leaves mode m/2 as a
-// sine (cos(m/2 phi_i) = 0): beta_{m/2} = -Im y_{m/2}.  Each residue is a transform of m/2 complex modes on m
-// angles, third-folded like the whole grid: half the DMMAs of the 3m-angle transform.  With C^r_k, S^r_k the
-// residue's cosine and sine sums of a product, sum_j p_j e^{-i n theta_j} = sum_r w^{n(1-r)} P^r_n with
-// w = e^{2 pi i/N}, P^r_k = C^r_k - i S^r_k, P^r_{m-k} = -conj(P^r_k) and P^r_{m/2} = -i S^r_{m/2}.  The
-// residue passes run the two kernels above on the m-angle grid (mode m/2's sine in the sine row of mode 0),
-// between a kernel that forms the residue's coefficients and one that adds its share to the outputs.
-// At m = 128 the extra passes over the coefficients and sums cost more than the DMMAs saved (cross product
-// at 100k points 2.65 -> 2.93 ms, 16 tangents 44.7 -> 52.5 ms); from m = 256 on the residues win (the
-// 16-tangent MHD JVP at 50k points 129 -> 100 ms, the cross product at m = 512 29.0 -> 24.1 ms).
-bool large_r3_supported(int m, int N) { return m >= 256 && m <= 512 && m % 64 == 0 && N == 3 * m; }
+// On theta_j = pi(2j+1)/N with N = 3m, j = R i + r (r < R, R dividing N) gives theta_j = phi_i + d_r with
+// phi_i = pi(2i+1)/M the offset grid of M = N/R angles and d_r = pi(2r + 1 - R)/N.  A field
+// Re sum_n z_n e^{i n theta} (z_n = a_n - i b_n, n < m) is on residue r the series of y_n = z_n e^{i n d_r}
+// on phi, where e^{i M phi_i} = -1: mode n = qM + k (k < M) is mode k with the sign (-1)^q, so that
+// Y_k = sum_q (-1)^q y_{qM+k}, and the modes k and M - k fold into alpha_k - i beta_k = Y_k - conj(Y_{M-k})
+// (k = 1 .. M/2 - 1), alpha_0 = Re Y_0, with mode M/2 alone as a sine (cos(M/2 phi_i) = 0):
+// beta_{M/2} = -Im Y_{M/2}.  Each residue is a transform of M real coefficients to M angles, third-folded
+// like the whole grid: 1/R of the DMMAs of each of R transforms instead of one on N angles, i.e. 3/R of
+// the work at the same m.  With C^r_k, S^r_k the residue's cosine and sine sums of a product,
+// sum_j p_j e^{-i n theta_j} = sum_r e^{-i n d_r} P^r_n with P^r_k = C^r_k - i S^r_k (k <= M/2),
+// P^r_{M-k} = -conj(P^r_k), P^r_{qM+k} = (-1)^q P^r_k and P^r_{M/2} = -i S^r_{M/2}.  The residue passes run
+// the two kernels above on the M-angle grid (mode M/2's sine in the sine row of mode 0), between a kernel
+// that forms the residues' coefficients and one that adds their shares to the outputs.  Both move N doubles
+// per field and point whatever R is, so more residues cost only their twiddles (R complex products per
+// mode).  At m = 128 the passes over the coefficients and sums cost more than the DMMAs saved (cross
+// product at 100k points 2.65 -> 2.93 ms with R = 3); from m = 256 on the residues win.
+constexpr int kMaxResidues = 12;
+std::atomic<int> g_test_residues{0};  // tests: force R (0: the choice below)
 
-struct R3LargeTab {
-  double *base = nullptr;  // syn, ana (two equal variants, no weights), tw [m][2]
+bool residues_fit(int m, int N, int R) {
+  if (N != 3 * m || R < 3 || R > kMaxResidues || N % R) return false;
+  const int M = N / R;
+  return M >= 64 && M % 64 == 0 && M <= 512;  // an even number of quadrant tiles (third fold), kernels' range
+}
+
+// Residue classes of the two-kernel form for m modes on the N-angle grid; 0: the whole grid.  The most
+// classes that leave residue grids of at least 192 angles: on a B200, R = 6 against 3 took m = 384 from
+// 11.9 to 9.5 ms (cross product, 100k points) and m = 512 from 10.3 to 8.3 ms (60k points), while at
+// m = 256 grids of 128 angles gained nothing (the grid values' round trip through HBM bounds the calls
+// there; 16-tangent MHD JVP at 50k points 91 ms with R = 3, 98 with 6, 112 with 12).
+int large_residues(int m, int N) {
+  if (const int R = g_test_residues.load()) return residues_fit(m, N, R) ? R : 0;
+  if (m < 256 || m > 512) return 0;
+  for (int R : {12, 6, 3})
+    if (residues_fit(m, N, R) && N / R >= 192) return R;
+  return 0;
+}
+
+struct ResTab {
+  double *base = nullptr;  // syn, ana (two equal variants, no weights), tw [R][m][2]
   double *syn = nullptr, *ana = nullptr;
   const double *tw = nullptr;
 };
-std::mutex g_r3l_mu;
-std::map<std::pair<int, int>, R3LargeTab> g_r3l;  // (device, m) -> tables
+std::mutex g_res_mu;
+std::map<std::tuple<int, int, int>, ResTab> g_res;  // (device, m, R) -> tables
 
-__host__ __device__ constexpr int r3l_mode(int gr, int k, int mh) { return (gr == 3 && k == 0) ? mh : tf_mode(gr, k); }
+__host__ __device__ constexpr int res_mode(int gr, int k, int mh) { return (gr == 3 && k == 0) ? mh : tf_mode(gr, k); }
 
-// Third-fold tables of the residue grid (m angles, quadrant tiles NT = m/32, row and output groups of m/2
-// modes with mode m/2 as the sine of group 3's k = 0), laid out like get_tf_tables', and the twiddles
-// cos, sin of 2 pi n / N for n < m.
-int get_large_r3_tables(int m, int N, R3LargeTab *out) {
+// Third-fold tables of the residue grid (M angles, quadrant tiles NT = M/32, row and output groups of M/2
+// modes with mode M/2 as the sine of group 3's k = 0), laid out like get_tf_tables', and the twiddles
+// cos, sin of n d_r for n < m, r < R.
+int get_residue_tables(int m, int N, int R, ResTab *out) {
   int dev = 0;
   cudaGetDevice(&dev);
-  std::lock_guard<std::mutex> lk(g_r3l_mu);
-  auto it = g_r3l.find({dev, m});
-  if (it != g_r3l.end()) {
+  std::lock_guard<std::mutex> lk(g_res_mu);
+  auto it = g_res.find({dev, m, R});
+  if (it != g_res.end()) {
     *out = it->second;
     return SFNL_OK;
   }
-  const int mh = m / 2, NT = m / 32;
+  const int M = N / R, mh = M / 2, NT = M / 32;
   const long double pi = acosl(-1.0L);
-  auto phi = [&](int j) { return pi * (long double)(2 * j + 1) / (long double)m; };
+  auto phi = [&](int j) { return pi * (long double)(2 * j + 1) / (long double)M; };
   const int ks_tot = tf_koff(mh, 6);
   int asteps = 0, aoff[7];
   for (int gr = 0; gr < 6; ++gr) {
@@ -849,14 +872,14 @@ int get_large_r3_tables(int m, int N, R3LargeTab *out) {
   }
   aoff[6] = asteps;
   const size_t nsyn = (size_t)ks_tot * NT * 32, nana = (size_t)2 * asteps * 32;
-  std::vector<double> h(nsyn + nana + 2 * (size_t)m, 0.0);
+  std::vector<double> h(nsyn + nana + 2 * (size_t)R * m, 0.0);
   for (int gr = 0; gr < 6; ++gr)
     for (int s = 0; s < tf_KS(mh, gr); ++s)
       for (int t = 0; t < NT; ++t)
         for (int l = 0; l < 32; ++l) {
           const int k = 4 * s + (l & 3);
           if (k >= tf_ke(mh, gr)) continue;
-          const long double x = (long double)r3l_mode(gr, k, mh) * phi(8 * t + (l >> 2));
+          const long double x = (long double)res_mode(gr, k, mh) * phi(8 * t + (l >> 2));
           h[((size_t)(tf_koff(mh, gr) + s) * NT + t) * 32 + l] = (double)(gr < 3 ? cosl(x) : sinl(x));
         }
   for (int var = 0; var < 2; ++var)
@@ -867,15 +890,17 @@ int get_large_r3_tables(int m, int N, R3LargeTab *out) {
           for (int l = 0; l < 32; ++l) {
             const int kk = 8 * u + (l >> 2);
             if (kk >= tf_ke(mh, gr)) continue;
-            const long double x = (long double)r3l_mode(gr, kk, mh) * phi(8 * (te >> 1) + 2 * (l & 3) + (te & 1));
+            const long double x = (long double)res_mode(gr, kk, mh) * phi(8 * (te >> 1) + 2 * (l & 3) + (te & 1));
             h[nsyn + ((size_t)var * asteps + aoff[gr] + u * TE + te) * 32 + l] = (double)(gr < 3 ? cosl(x) : sinl(x));
           }
     }
-  for (int n = 0; n < m; ++n) {
-    h[nsyn + nana + 2 * n] = (double)cosl(2.0L * pi * n / (long double)N);
-    h[nsyn + nana + 2 * n + 1] = (double)sinl(2.0L * pi * n / (long double)N);
-  }
-  R3LargeTab T;
+  for (int r = 0; r < R; ++r)
+    for (int n = 0; n < m; ++n) {
+      const long double x = pi * (long double)n * (long double)(2 * r + 1 - R) / (long double)N;
+      h[nsyn + nana + 2 * ((size_t)r * m + n)] = (double)cosl(x);
+      h[nsyn + nana + 2 * ((size_t)r * m + n) + 1] = (double)sinl(x);
+    }
+  ResTab T;
   if (cudaMalloc(&T.base, h.size() * sizeof(double)) != cudaSuccess) {
     cudaGetLastError();
     return set_error(SFNL_ERR_ALLOC, "cudaMalloc of the residue-grid tables failed");
@@ -887,93 +912,143 @@ int get_large_r3_tables(int m, int N, R3LargeTab *out) {
   T.syn = T.base;
   T.ana = T.base + nsyn;
   T.tw = T.base + nsyn + nana;
-  g_r3l[{dev, m}] = T;
+  g_res[{dev, m, R}] = T;
   *out = T;
   return SFNL_OK;
 }
 
-// The three residues of one input field (batch entry blockIdx.z) at the chunk's points: thread (point, k)
-// forms alpha_k, beta_k of each residue from modes k and m - k (k = 0: alpha_0 and beta_{m/2}) into
-// y + r * ystride, each (npc, 2, m/2): cosine k at 2k npc, sine k at (2k + 1) npc, the sine row 0 holding
-// beta_{m/2}.  Cotangents (adj) take the analysis weights 1/N (n = 0), 2/N first.
-__global__ void large_r3_coef_kernel(const double *x, int64_t ldm, int64_t xsin, int64_t xbs, double *y, int64_t ystride,
-                                     int64_t npc, int m, int adj, double invN, const double *tw) {
+// The R residues of one input field (batch entry blockIdx.z) at the chunk's points: thread (point, k),
+// k < M/2, gathers Y_k and Y_{M-k} of each residue from the modes qM + k and qM + M - k (k = 0: Y_0 and
+// Y_{M/2} from qM and qM + M/2) and writes alpha_k, beta_k (k = 0: alpha_0 and beta_{M/2}) into
+// y + r * ystride, each (npc, 2, M/2): cosine k at 2k npc, sine k at (2k + 1) npc, the sine row 0 holding
+// beta_{M/2}.  Cotangents (adj) take the analysis weights 1/N (n = 0), 2/N first.
+template <int R>
+__global__ void large_res_coef_kernel(const double *x, int64_t ldm, int64_t xsin, int64_t xbs, double *y,
+                                      int64_t ystride, int64_t npc, int m, int adj, double invN, const double *tw) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npc) return;
-  const int k = blockIdx.y, mh = m >> 1;
+  const int k = blockIdx.y, M = 3 * m / R, mh = M >> 1;
   const double *xp = x + (int64_t)blockIdx.z * xbs + p;
-  double *yp = y + (int64_t)blockIdx.z * m * npc + p;
-  auto w = [&](int n) { return adj ? (n == 0 ? invN : 2.0 * invN) : 1.0; };
-  // residue r: twiddle e^{i n (r-1) 2 pi / N} = c_n + i (r-1) s_n
-  if (k == 0) {
-    const double a0 = xp[0] * w(0), am = xp[(int64_t)mh * ldm] * w(mh), bm = xp[(int64_t)mh * ldm + xsin] * w(mh);
-    const double c = __ldg(tw + 2 * mh), s = __ldg(tw + 2 * mh + 1);
-    yp[0] = yp[ystride] = yp[2 * ystride] = a0;
-    yp[npc] = fma(bm, c, am * s);         // r = 0
-    yp[ystride + npc] = bm;               // r = 1
-    yp[2 * ystride + npc] = fma(bm, c, -am * s);  // r = 2
-  } else {
-    const int k2 = m - k;
-    const double a = xp[(int64_t)k * ldm] * w(k), b = xp[(int64_t)k * ldm + xsin] * w(k);
-    const double a2 = xp[(int64_t)k2 * ldm] * w(k2), b2 = xp[(int64_t)k2 * ldm + xsin] * w(k2);
-    const double c = __ldg(tw + 2 * k), s = __ldg(tw + 2 * k + 1), c2 = __ldg(tw + 2 * k2), s2 = __ldg(tw + 2 * k2 + 1);
-    // alpha = (a C + b S) - (a' C' + b' S'), beta = (b C - a S) + (b' C' - a' S') with C = c, S = (r-1) s
-    const double X = fma(a, c, -a2 * c2), Y = fma(b, s, -b2 * s2), Z = fma(b, c, b2 * c2), W = fma(a, s, a2 * s2);
-    const int64_t ic = (int64_t)(2 * k) * npc, is = (int64_t)(2 * k + 1) * npc;
-    yp[ic] = X - Y;
-    yp[is] = Z + W;
-    yp[ystride + ic] = a - a2;
-    yp[ystride + is] = b + b2;
-    yp[2 * ystride + ic] = X + Y;
-    yp[2 * ystride + is] = Z - W;
+  double *yp = y + (int64_t)blockIdx.z * M * npc + p;
+  double ylr[R], yli[R], yhr[R], yhi[R];  // Y_k (lo) and Y_{M-k} (k = 0: Y_{M/2}) of each residue
+#pragma unroll
+  for (int r = 0; r < R; ++r) ylr[r] = yli[r] = yhr[r] = yhi[r] = 0.0;
+  const int klo = k, khi = k == 0 ? mh : M - k;
+  for (int q = 0; q * M < m; ++q) {
+    const double sg = (q & 1) ? -1.0 : 1.0;
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const int n = q * M + (side ? khi : klo);
+      if (n >= m) continue;
+      const double wn = (adj ? (n == 0 ? invN : 2.0 * invN) : 1.0) * sg;
+      const double a = xp[(int64_t)n * ldm] * wn, b = xp[(int64_t)n * ldm + xsin] * wn;
+      // y_n = (a - i b)(c + i s) = (a c + b s) + i (a s - b c)
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const double c = __ldg(tw + 2 * ((size_t)r * m + n)), s = __ldg(tw + 2 * ((size_t)r * m + n) + 1);
+        const double re = fma(a, c, b * s), im = fma(a, s, -b * c);
+        if (side) {
+          yhr[r] += re;
+          yhi[r] += im;
+        } else {
+          ylr[r] += re;
+          yli[r] += im;
+        }
+      }
+    }
+  }
+  const int64_t ic = (int64_t)(2 * k) * npc, is = (int64_t)(2 * k + 1) * npc;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    double *yr = yp + (int64_t)r * ystride;
+    if (k == 0) {
+      yr[ic] = ylr[r];    // alpha_0 = Re Y_0
+      yr[is] = -yhi[r];   // beta_{M/2} = -Im Y_{M/2}
+    } else {
+      yr[ic] = ylr[r] - yhr[r];     // Re (Y_k - conj Y_{M-k})
+      yr[is] = -(yli[r] + yhi[r]);  // -Im (Y_k - conj Y_{M-k})
+    }
   }
 }
 
-// One output (batch entry blockIdx.z) from the three residues' sums R + r * rstride, each (npc, 2, m/2) with
-// the sine row 0 holding S_{m/2}: thread (point, k) writes modes k and m - k (k = 0: modes 0 and m/2).
-// w = 2/N (or 1 without analysis weights), w0 = 1/N (or 1).
-__global__ void large_r3_out_kernel(const double *R, int64_t rstride, double *out, int64_t ldm, int64_t osin, int64_t ops,
-                                    int64_t obs, int64_t npc, int m, double w, double w0, const double *tw) {
+// One output (batch entry blockIdx.z) from the R residues' sums S + r * rstride, each (npc, 2, M/2) with
+// the sine row 0 holding S_{M/2}: thread (point, k), k < M/2, writes the modes qM + k and qM + M - k
+// (k = 0: qM and qM + M/2) below m.  w = 2/N (or 1 without analysis weights), w0 = 1/N (or 1).
+template <int R>
+__global__ void large_res_out_kernel(const double *S, int64_t rstride, double *out, int64_t ldm, int64_t osin,
+                                     int64_t ops, int64_t obs, int64_t npc, int m, double w, double w0,
+                                     const double *tw) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npc) return;
-  const int k = blockIdx.y, mh = m >> 1;
-  const double *rp = R + (int64_t)blockIdx.z * m * npc + p;
+  const int k = blockIdx.y, M = 3 * m / R, mh = M >> 1;
+  const double *sp = S + (int64_t)blockIdx.z * M * npc + p;
   double *op = out + (int64_t)blockIdx.z * obs + p * ops;
-  auto put = [&](int n, int sine, double v) { op[(int64_t)n * ldm + (sine ? osin : 0)] = v; };
-  if (k == 0) {
-    const double c = __ldg(tw + 2 * mh), s = __ldg(tw + 2 * mh + 1);
-    const double S0 = rp[npc], S1 = rp[rstride + npc], S2 = rp[2 * rstride + npc];
-    put(0, 0, w0 * (rp[0] + rp[rstride] + rp[2 * rstride]));
-    put(0, 1, 0.0);
-    put(mh, 0, w * (s * (S0 - S2)));
-    put(mh, 1, w * fma(c, S0 + S2, S1));
-  } else {
-    const int k2 = m - k;
-    const int64_t ic = (int64_t)(2 * k) * npc, is = (int64_t)(2 * k + 1) * npc;
-    const double C0 = rp[ic], C1 = rp[rstride + ic], C2 = rp[2 * rstride + ic];
-    const double S0 = rp[is], S1 = rp[rstride + is], S2 = rp[2 * rstride + is];
-    const double c = __ldg(tw + 2 * k), s = __ldg(tw + 2 * k + 1), c2 = __ldg(tw + 2 * k2), s2 = __ldg(tw + 2 * k2 + 1);
-    const double CS = C0 + C2, CD = C0 - C2, SS = S0 + S2, SD = S0 - S2;
-    put(k, 0, w * fma(s, SD, fma(c, CS, C1)));
-    put(k, 1, w * fma(-s, CD, fma(c, SS, S1)));
-    put(k2, 0, w * fma(s2, SD, fma(-c2, CS, -C1)));
-    put(k2, 1, w * fma(s2, CD, fma(c2, SS, S1)));
+  const int64_t ic = (int64_t)(2 * k) * npc, is = (int64_t)(2 * k + 1) * npc;
+  // P^r_k (lo) and the mirror P^r_{M-k} = -conj(P^r_k) (k = 0: P^r_0 = C^r_0 and P^r_{M/2} = -i S^r_{M/2})
+  double plr[R], pli[R], phr[R], phi_[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const double C = sp[(int64_t)r * rstride + ic], Sv = sp[(int64_t)r * rstride + is];
+    if (k == 0) {
+      plr[r] = C;
+      pli[r] = 0.0;
+      phr[r] = 0.0;
+      phi_[r] = -Sv;
+    } else {
+      plr[r] = C;
+      pli[r] = -Sv;
+      phr[r] = -C;
+      phi_[r] = -Sv;
+    }
+  }
+  const int klo = k, khi = k == 0 ? mh : M - k;
+  for (int q = 0; q * M < m; ++q) {
+    const double sg = (q & 1) ? -1.0 : 1.0;
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const int n = q * M + (side ? khi : klo);
+      if (n >= m) continue;
+      // c_n = sum_r e^{-i n d_r} P^r_n: (c - i s)(x + i y) = (c x + s y) + i (c y - s x)
+      double re = 0.0, im = 0.0;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const double c = __ldg(tw + 2 * ((size_t)r * m + n)), s = __ldg(tw + 2 * ((size_t)r * m + n) + 1);
+        const double xr = side ? phr[r] : plr[r], yi = side ? phi_[r] : pli[r];
+        re += fma(c, xr, s * yi);
+        im += fma(c, yi, -s * xr);
+      }
+      const double wn = (n == 0 ? w0 : w) * sg;
+      op[(int64_t)n * ldm] = wn * re;
+      op[(int64_t)n * ldm + osin] = n == 0 ? 0.0 : -wn * im;
+    }
   }
 }
 
-// The two-kernel form on the residue grids: per point chunk, the three residues' coefficients of every
-// input field in one pass (m doubles per point, field instance and residue), the residue passes of the
-// program (run_large; sums into m doubles per point, output instance and residue), and the outputs from
-// the three residues' sums in one pass.
-int launch_large_r3(const ProgArgs &a, const Geo &g, cudaStream_t st) {
-  const int m = a.m, mh = m / 2, N = g.N, ni = op_nin(a.op), no = op_nout(a.op);
-  R3LargeTab T;
-  if (int rc = get_large_r3_tables(m, N, &T)) return rc;
-  const LargePlan rp{m, m / 32, mh, T.syn, T.ana};
+template <int R>
+void launch_res_coef(dim3 grid, int threads, cudaStream_t st, const double *x, int64_t ldm, int64_t xsin,
+                     int64_t xbs, double *y, int64_t ystride, int64_t npc, int m, int adj, double invN,
+                     const double *tw) {
+  large_res_coef_kernel<R><<<grid, threads, 0, st>>>(x, ldm, xsin, xbs, y, ystride, npc, m, adj, invN, tw);
+}
+template <int R>
+void launch_res_out(dim3 grid, int threads, cudaStream_t st, const double *S, int64_t rstride, double *out, int64_t ldm,
+                    int64_t osin, int64_t ops, int64_t obs, int64_t npc, int m, double w, double w0, const double *tw) {
+  large_res_out_kernel<R><<<grid, threads, 0, st>>>(S, rstride, out, ldm, osin, ops, obs, npc, m, w, w0, tw);
+}
+
+// The two-kernel form on the residue grids: per point chunk, the R residues' coefficients of every input
+// field in one pass (N/R doubles per point, field instance and residue), the residue passes of the program
+// (run_large; sums into N/R doubles per point, output instance and residue), and the outputs from the R
+// residues' sums in one pass.
+int launch_large_res(const ProgArgs &a, const Geo &g, int R, cudaStream_t st) {
+  const int m = a.m, N = g.N, M = N / R, mh = M / 2, ni = op_nin(a.op), no = op_nout(a.op);
+  ResTab T;
+  if (int rc = get_residue_tables(m, N, R, &T)) return rc;
+  const LargePlan rp{M, M / 32, mh, T.syn, T.ana};
   int64_t inst_in = 0;
   for (int f = 0; f < ni; ++f) inst_in += a.in_bs[f] ? a.batch : 1;
   const int64_t inst_out = (int64_t)no * a.batch;
-  const size_t per_point = sizeof(double) * (size_t)m * 3 * (size_t)(inst_in + inst_out);
+  const size_t per_point = sizeof(double) * (size_t)N * (size_t)(inst_in + inst_out);
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
     cudaGetLastError();
@@ -992,42 +1067,43 @@ int launch_large_r3(const ProgArgs &a, const Geo &g, cudaStream_t st) {
   const bool adj_out = op_adjoint_out(a.op);
   const double invN = 1.0 / N, w = adj_out ? 1.0 : 2.0 * invN, w0 = adj_out ? 1.0 : invN;
   constexpr int kThreads = 256;
+  auto coef = R == 3 ? launch_res_coef<3> : R == 6 ? launch_res_coef<6> : launch_res_coef<12>;
+  auto outk = R == 3 ? launch_res_out<3> : R == 6 ? launch_res_out<6> : launch_res_out<12>;
   for (int64_t c0 = 0; c0 < a.np; c0 += chunk) {
     const int64_t npc = a.np - c0 < chunk ? a.np - c0 : chunk;
     const unsigned bx = (unsigned)((npc + kThreads - 1) / kThreads);
-    // residue r's arrays: inputs at W + r * rin, outputs at W + 3 rin + r * rout
-    const int64_t rin = inst_in * m * npc, rout = inst_out * m * npc;
+    // residue r's arrays: inputs at W + r * rin, outputs at W + R rin + r * rout
+    const int64_t rin = inst_in * M * npc, rout = inst_out * M * npc;
     ProgArgs ar = a;
     ar.np = npc;
     ar.out_ps = 1;
     int64_t off = 0;
     for (int f = 0; f < ni; ++f) {
       const int nb = a.in_bs[f] ? a.batch : 1;
-      large_r3_coef_kernel<<<dim3(bx, (unsigned)mh, (unsigned)nb), kThreads, 0, st>>>(
-          a.in[f] + c0, a.in_ldm[f], a.np, a.in_bs[f], W + off, rin, npc, m, op_adjoint_in(a.op, f) ? 1 : 0, invN, T.tw);
+      coef(dim3(bx, (unsigned)mh, (unsigned)nb), kThreads, st, a.in[f] + c0, a.in_ldm[f], a.np, a.in_bs[f], W + off, rin,
+           npc, m, op_adjoint_in(a.op, f) ? 1 : 0, invN, T.tw);
       ar.in[f] = W + off;
       ar.in_ldm[f] = 2 * npc;
-      ar.in_bs[f] = a.in_bs[f] ? (int64_t)m * npc : 0;
-      off += (int64_t)nb * m * npc;
+      ar.in_bs[f] = a.in_bs[f] ? (int64_t)M * npc : 0;
+      off += (int64_t)nb * M * npc;
     }
     if (int rc = check_launch("large-m residue coefficients")) return rc;
-    off = 3 * rin;
+    off = R * rin;
     for (int o = 0; o < no; ++o) {
       ar.out[o] = W + off;
       ar.out_ldm[o] = 2 * npc;
-      ar.out_bs[o] = (int64_t)m * npc;
-      off += (int64_t)a.batch * m * npc;
+      ar.out_bs[o] = (int64_t)M * npc;
+      off += (int64_t)a.batch * M * npc;
     }
-    for (int r = 0; r < 3; ++r) {
+    for (int r = 0; r < R; ++r) {
       ProgArgs rr = ar;
       for (int f = 0; f < ni; ++f) rr.in[f] = ar.in[f] + r * rin;
       for (int o = 0; o < no; ++o) rr.out[o] = ar.out[o] + r * rout;
       if (int rc = run_large(rr, g, Tables{}, &rp, st)) return rc;
     }
     for (int o = 0; o < no; ++o)
-      large_r3_out_kernel<<<dim3(bx, (unsigned)mh, (unsigned)a.batch), kThreads, 0, st>>>(
-          ar.out[o], rout, a.out[o] + c0 * a.out_ps, a.out_ldm[o], a.np * a.out_ps, a.out_ps, a.out_bs[o], npc, m, w, w0,
-          T.tw);
+      outk(dim3(bx, (unsigned)mh, (unsigned)a.batch), kThreads, st, ar.out[o], rout, a.out[o] + c0 * a.out_ps,
+           a.out_ldm[o], a.np * a.out_ps, a.out_ps, a.out_bs[o], npc, m, w, w0, T.tw);
     if (int rc = check_launch("large-m residue outputs")) return rc;
   }
   return SFNL_OK;
@@ -1037,22 +1113,24 @@ int launch_large_r3(const ProgArgs &a, const Geo &g, cudaStream_t st) {
 
 void large_test_workspace_cap(size_t bytes) { g_test_cap.store(bytes); }
 
-void large_r3_release_tables() {
-  std::lock_guard<std::mutex> lk(g_r3l_mu);
+void large_test_residues(int R) { g_test_residues.store(R); }
+
+void large_res_release_tables() {
+  std::lock_guard<std::mutex> lk(g_res_mu);
   int prev = 0;
   cudaGetDevice(&prev);
-  for (auto &kv : g_r3l) {
-    cudaSetDevice(kv.first.first);
+  for (auto &kv : g_res) {
+    cudaSetDevice(std::get<0>(kv.first));
     cudaFree(kv.second.base);
   }
-  g_r3l.clear();
+  g_res.clear();
   cudaSetDevice(prev);
 }
 
-// The two-kernel form: on the grid's three residue classes when the grid is 3m angles and m >= 256 (half
-// the DMMAs, launch_large_r3), else on the whole grid.
+// The two-kernel form: on the grid's residue classes when the grid is 3m angles and m >= 256 (R of them:
+// 3/R of the DMMAs of the whole grid, launch_large_res), else on the whole grid.
 int launch_fast_large(const ProgArgs &a, const Geo &g, const Tables &T, cudaStream_t st) {
-  if (large_r3_supported(a.m, g.N)) return launch_large_r3(a, g, st);
+  if (const int R = large_residues(a.m, g.N)) return launch_large_res(a, g, R, st);
   return run_large(a, g, T, nullptr, st);
 }
 

@@ -66,9 +66,12 @@ def test_bundle_kernel_switch():
         sf.set_bundle_kernel(prev)
 
 
-def test_large_workspace_bound_hook_checks_its_argument():
+def test_large_m_test_hooks_check_their_arguments():
     assert sf.lib().sfnl_test_large_workspace_cap(-1) == -1 and sf.last_error()
     assert sf.lib().sfnl_test_large_workspace_cap(0) == 0
+    for bad in (-1, 1, 4, 24):
+        assert sf.lib().sfnl_test_large_residues(bad) == -1 and sf.last_error()
+    assert sf.lib().sfnl_test_large_residues(6) == 0 and sf.lib().sfnl_test_large_residues(0) == 0
 
 
 def test_zero_points_is_a_no_op():

@@ -146,6 +146,22 @@ def test_bundle_kernels_agree(npts):
             assert R.rel_l2(r3[i], refs[i]) <= FP64_TOL
 
 
+def test_bundle_reports_a_wait_that_gave_up():
+    # Host-side injection: the wait-status word is marked as the m = 64 bundle kernel marks it when a bounded
+    # wait on its bulk copies gives up; no device wait is made to run out.  The next bundle call reports
+    # it and clears it.
+    npts, m, pad = 64, 64, 96
+    f = [R.synthetic_field(npts, 6, m, 0.1, 710 + i) for i in range(5)]
+    d = [dev(x) for x in f]
+    assert sf.lib().sfnl_test_inject_timeout() == 0
+    with pytest.raises(sf.SfnlError) as e:
+        sf.bundle_mhd(*d, m_max_pad=pad)
+    assert e.value.code == -8 and "bulk copies" in str(e.value)
+    outs = [host(o) for o in sf.bundle_mhd(*d, m_max_pad=pad)]  # cleared
+    for o, r in zip(outs, R.mhd_bundle(*f, pad)):
+        assert R.rel_l2(o, r) <= FP64_TOL
+
+
 @pytest.mark.parametrize("npts,m", [(90, 10), (3001, 64)])
 def test_host_bundle_entry_point(npts, m):
     import ctypes
@@ -347,6 +363,27 @@ def test_large_m_small_workspace_bound(m, pad):
         assert sf.lib().sfnl_test_large_workspace_cap(0) == 0
     assert R.rel_l2(out, ref_cross) <= FP64_TOL
     assert R.rel_l2(jvp, ref_jvp) <= 1e-13
+
+
+@pytest.mark.parametrize("m,pad,splits", [(256, 384, (3, 6, 12)), (512, 768, (3, 6, 12)), (128, 192, (0, 3, 6))])
+def test_large_m_residue_classes(m, pad, splits):
+    # the large-m form on the grid split into R residue classes (a test hook forces R; 0: the whole grid):
+    # every split against the oracle, and the cross JVP of every split against the first one
+    npts, k = 203, 2
+    u, w = (R.synthetic_field(npts, 6, m, 0.05, 620 + i) for i in range(2))
+    tan = _batched(npts, 12, m, k, 0.05, 630)
+    ref = R.fft_par("cross", u, w, pad, workers=8)
+    jvps = []
+    try:
+        for split in splits:
+            assert sf.lib().sfnl_test_large_residues(split) == 0
+            out = host(sf.product(0, dev(u), dev(w), m_max_pad=pad, algo=sf.ALGO_FAST))
+            assert R.rel_l2(out, ref) <= FP64_TOL, split
+            jvps.append(host(sf.cross_jvp(dev(u), dev(w), dev(tan), m_max_pad=pad)))
+    finally:
+        assert sf.lib().sfnl_test_large_residues(0) == 0
+    for jv in jvps[1:]:
+        assert R.rel_l2(jv, jvps[0]) <= 1e-13
 
 
 def test_large_m_point_chunks():
