@@ -420,8 +420,8 @@ int sfnl_test_inject_timeout(void);
 int sfnl_test_large_workspace_cap(int64_t bytes);
 /* Test hook: the number of residue classes (3, 6 or 12) into which the large-m FAST form splits its
  * 3m-angle grid, where the split gives whole quadrant-tile pairs (3m/R a multiple of 64, at most 512), else
- * the whole grid; 0 restores the automatic choice (from m = 256 the most classes that leave residue grids
- * of at least 192 angles: 3 at m = 256, 6 at m = 384 and 512; the whole grid below m = 256).  Every choice gives the same products to rounding.  Process-wide.  Other values:
+ * the whole grid; 0 restores the automatic choice (from m = 256: 6 where it fits, else 3; the whole grid
+ * below m = 256).  Every choice gives the same products to rounding.  Process-wide.  Other values:
  * SFNL_ERR_ARG. */
 int sfnl_test_large_residues(int R);
 /* Device-timed seconds of the last host-array call of this thread (the *_host,

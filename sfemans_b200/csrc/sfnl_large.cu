@@ -826,17 +826,15 @@ bool residues_fit(int m, int N, int R) {
   return M >= 64 && M % 64 == 0 && M <= 512;  // an even number of quadrant tiles (third fold), kernels' range
 }
 
-// Residue classes of the two-kernel form for m modes on the N-angle grid; 0: the whole grid.  The most
-// classes that leave residue grids of at least 192 angles: on a B200, R = 6 against 3 took m = 384 from
-// 11.9 to 9.5 ms (cross product, 100k points) and m = 512 from 10.3 to 8.3 ms (60k points), while at
-// m = 256 grids of 128 angles gained nothing (the grid values' round trip through HBM bounds the calls
-// there; 16-tangent MHD JVP at 50k points 91 ms with R = 3, 98 with 6, 112 with 12).
+// Residue classes of the two-kernel form for m modes on the N-angle grid; 0: the whole grid.  Six where
+// they fit, else three: on a B200, R = 6 against 3 took the cross product at m = 256 (350k points) from
+// 19.8 to 18.5 ms, at m = 384 (100k points) from 12.3 to 8.9 ms and at m = 512 (60k points) from 10.3 to
+// 7.2 ms, the 16-tangent MHD JVP at m = 256 (50k points) from 90.8 to 85.7 ms; residue grids of 64 angles
+// (R = 12 at m = 256) were slower than both.
 int large_residues(int m, int N) {
   if (const int R = g_test_residues.load()) return residues_fit(m, N, R) ? R : 0;
   if (m < 256 || m > 512) return 0;
-  for (int R : {12, 6, 3})
-    if (residues_fit(m, N, R) && N / R >= 192) return R;
-  return 0;
+  return residues_fit(m, N, 6) ? 6 : residues_fit(m, N, 3) ? 3 : 0;
 }
 
 struct ResTab {
@@ -921,101 +919,106 @@ int get_residue_tables(int m, int N, int R, ResTab *out) {
 // k < M/2, gathers Y_k and Y_{M-k} of each residue from the modes qM + k and qM + M - k (k = 0: Y_0 and
 // Y_{M/2} from qM and qM + M/2) and writes alpha_k, beta_k (k = 0: alpha_0 and beta_{M/2}) into
 // y + r * ystride, each (npc, 2, M/2): cosine k at 2k npc, sine k at (2k + 1) npc, the sine row 0 holding
-// beta_{M/2}.  Cotangents (adj) take the analysis weights 1/N (n = 0), 2/N first.
+// beta_{M/2}.  Cotangents (adj) take the analysis weights 1/N (n = 0), 2/N first.  The residues pair as
+// d_{R-1-r} = -d_r (and d = 0 for the middle one of an odd R), so one twiddle serves two residues.
 template <int R>
 __global__ void large_res_coef_kernel(const double *x, int64_t ldm, int64_t xsin, int64_t xbs, double *y,
                                       int64_t ystride, int64_t npc, int m, int adj, double invN, const double *tw) {
+  constexpr int RP = R / 2;  // residue pairs
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npc) return;
   const int k = blockIdx.y, M = 3 * m / R, mh = M >> 1;
   const double *xp = x + (int64_t)blockIdx.z * xbs + p;
   double *yp = y + (int64_t)blockIdx.z * M * npc + p;
-  double ylr[R], yli[R], yhr[R], yhi[R];  // Y_k (lo) and Y_{M-k} (k = 0: Y_{M/2}) of each residue
+  double yr[2][R], yi[2][R];  // Y_k (side 0) and Y_{M-k} (side 1; k = 0: Y_{M/2}) of each residue
 #pragma unroll
-  for (int r = 0; r < R; ++r) ylr[r] = yli[r] = yhr[r] = yhi[r] = 0.0;
-  const int klo = k, khi = k == 0 ? mh : M - k;
-  for (int q = 0; q * M < m; ++q) {
+  for (int side = 0; side < 2; ++side)
+#pragma unroll
+    for (int r = 0; r < R; ++r) yr[side][r] = yi[side][r] = 0.0;
+  const int khi = k == 0 ? mh : M - k;
+#pragma unroll
+  for (int q = 0; q < R / 3; ++q) {  // m = (R/3) M: every qM + k and qM + M - k is a mode
     const double sg = (q & 1) ? -1.0 : 1.0;
 #pragma unroll
     for (int side = 0; side < 2; ++side) {
-      const int n = q * M + (side ? khi : klo);
-      if (n >= m) continue;
+      const int n = q * M + (side ? khi : k);
       const double wn = (adj ? (n == 0 ? invN : 2.0 * invN) : 1.0) * sg;
       const double a = xp[(int64_t)n * ldm] * wn, b = xp[(int64_t)n * ldm + xsin] * wn;
-      // y_n = (a - i b)(c + i s) = (a c + b s) + i (a s - b c)
+      // y_n = (a - i b)(c +- i s): residue r (+s) and R-1-r (-s)
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const double c = __ldg(tw + 2 * ((size_t)r * m + n)), s = __ldg(tw + 2 * ((size_t)r * m + n) + 1);
-        const double re = fma(a, c, b * s), im = fma(a, s, -b * c);
-        if (side) {
-          yhr[r] += re;
-          yhi[r] += im;
-        } else {
-          ylr[r] += re;
-          yli[r] += im;
-        }
+      for (int r = 0; r < RP; ++r) {
+        const double2 cs = __ldg(reinterpret_cast<const double2 *>(tw) + (size_t)r * m + n);
+        const double ac = a * cs.x, bs = b * cs.y, as = a * cs.y, bc = b * cs.x;
+        yr[side][r] += ac + bs;
+        yi[side][r] += as - bc;
+        yr[side][R - 1 - r] += ac - bs;
+        yi[side][R - 1 - r] -= as + bc;
+      }
+      if (R & 1) {
+        yr[side][RP] += a;
+        yi[side][RP] -= b;
       }
     }
   }
   const int64_t ic = (int64_t)(2 * k) * npc, is = (int64_t)(2 * k + 1) * npc;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    double *yr = yp + (int64_t)r * ystride;
+    double *yo = yp + (int64_t)r * ystride;
     if (k == 0) {
-      yr[ic] = ylr[r];    // alpha_0 = Re Y_0
-      yr[is] = -yhi[r];   // beta_{M/2} = -Im Y_{M/2}
+      yo[ic] = yr[0][r];   // alpha_0 = Re Y_0
+      yo[is] = -yi[1][r];  // beta_{M/2} = -Im Y_{M/2}
     } else {
-      yr[ic] = ylr[r] - yhr[r];     // Re (Y_k - conj Y_{M-k})
-      yr[is] = -(yli[r] + yhi[r]);  // -Im (Y_k - conj Y_{M-k})
+      yo[ic] = yr[0][r] - yr[1][r];     // Re (Y_k - conj Y_{M-k})
+      yo[is] = -(yi[0][r] + yi[1][r]);  // -Im (Y_k - conj Y_{M-k})
     }
   }
 }
 
 // One output (batch entry blockIdx.z) from the R residues' sums S + r * rstride, each (npc, 2, M/2) with
 // the sine row 0 holding S_{M/2}: thread (point, k), k < M/2, writes the modes qM + k and qM + M - k
-// (k = 0: qM and qM + M/2) below m.  w = 2/N (or 1 without analysis weights), w0 = 1/N (or 1).
+// (k = 0: qM and qM + M/2) below m.  w = 2/N (or 1 without analysis weights), w0 = 1/N (or 1).  Paired
+// residues share their twiddle as in large_res_coef_kernel.
 template <int R>
 __global__ void large_res_out_kernel(const double *S, int64_t rstride, double *out, int64_t ldm, int64_t osin,
                                      int64_t ops, int64_t obs, int64_t npc, int m, double w, double w0,
                                      const double *tw) {
+  constexpr int RP = R / 2;
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npc) return;
   const int k = blockIdx.y, M = 3 * m / R, mh = M >> 1;
   const double *sp = S + (int64_t)blockIdx.z * M * npc + p;
   double *op = out + (int64_t)blockIdx.z * obs + p * ops;
   const int64_t ic = (int64_t)(2 * k) * npc, is = (int64_t)(2 * k + 1) * npc;
-  // P^r_k (lo) and the mirror P^r_{M-k} = -conj(P^r_k) (k = 0: P^r_0 = C^r_0 and P^r_{M/2} = -i S^r_{M/2})
-  double plr[R], pli[R], phr[R], phi_[R];
+  // P^r_k = C - i S; the mirror P^r_{M-k} = -conj(P^r_k) = -C - i S; k = 0: P^r_0 = C, P^r_{M/2} = -i S
+  double C[R], Sv[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    const double C = sp[(int64_t)r * rstride + ic], Sv = sp[(int64_t)r * rstride + is];
-    if (k == 0) {
-      plr[r] = C;
-      pli[r] = 0.0;
-      phr[r] = 0.0;
-      phi_[r] = -Sv;
-    } else {
-      plr[r] = C;
-      pli[r] = -Sv;
-      phr[r] = -C;
-      phi_[r] = -Sv;
-    }
+    C[r] = sp[(int64_t)r * rstride + ic];
+    Sv[r] = sp[(int64_t)r * rstride + is];
   }
-  const int klo = k, khi = k == 0 ? mh : M - k;
-  for (int q = 0; q * M < m; ++q) {
+  const int khi = k == 0 ? mh : M - k;
+#pragma unroll
+  for (int q = 0; q < R / 3; ++q) {
     const double sg = (q & 1) ? -1.0 : 1.0;
 #pragma unroll
     for (int side = 0; side < 2; ++side) {
-      const int n = q * M + (side ? khi : klo);
-      if (n >= m) continue;
-      // c_n = sum_r e^{-i n d_r} P^r_n: (c - i s)(x + i y) = (c x + s y) + i (c y - s x)
+      const int n = q * M + (side ? khi : k);
+      // P^r_n = x_r + i y_r
+      auto px = [&](int r) { return k == 0 ? (side ? 0.0 : C[r]) : (side ? -C[r] : C[r]); };
+      auto py = [&](int r) { return k == 0 ? (side ? -Sv[r] : 0.0) : -Sv[r]; };
+      // c_n = sum_r e^{-i n d_r} P^r_n; a pair (r, R-1-r) with e^{-i n d} = c -+ i s gives
+      // c (x + x') + s (y - y') + i (c (y + y') - s (x - x'))
       double re = 0.0, im = 0.0;
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const double c = __ldg(tw + 2 * ((size_t)r * m + n)), s = __ldg(tw + 2 * ((size_t)r * m + n) + 1);
-        const double xr = side ? phr[r] : plr[r], yi = side ? phi_[r] : pli[r];
-        re += fma(c, xr, s * yi);
-        im += fma(c, yi, -s * xr);
+      for (int r = 0; r < RP; ++r) {
+        const double2 cs = __ldg(reinterpret_cast<const double2 *>(tw) + (size_t)r * m + n);
+        const double x0 = px(r), y0 = py(r), x1 = px(R - 1 - r), y1 = py(R - 1 - r);
+        re += fma(cs.x, x0 + x1, cs.y * (y0 - y1));
+        im += fma(cs.x, y0 + y1, -cs.y * (x0 - x1));
+      }
+      if (R & 1) {
+        re += px(RP);
+        im += py(RP);
       }
       const double wn = (n == 0 ? w0 : w) * sg;
       op[(int64_t)n * ldm] = wn * re;
