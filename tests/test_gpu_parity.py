@@ -555,6 +555,52 @@ def test_linearised_700k_points_full_size():
     assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
 
 
+def test_mhd_linearised_k16_m256_at_call_size():
+    # the 16-tangent linearised pair (u x w, u x b) at m = 256 with the point count of one call of its
+    # configuration (350k points in ten calls of 35k; production workspace bounds): central differences of
+    # the FP64 cross products at h = 1e-6 for every tangent and the adjoint identity, over every point
+    import torch
+
+    npts, m, k, h = 35_000, 256, 16, 1e-6
+    pad = 3 * m // 2
+    decay = None
+
+    def field(nslot, seed, kk=None):
+        nonlocal decay
+        g = torch.Generator(device="cuda")
+        g.manual_seed(seed)
+        shape = (m, nslot, npts) if kk is None else (kk, m, nslot, npts)
+        t = torch.randn(shape, generator=g, device="cuda", dtype=torch.float64)
+        if decay is None:
+            decay = torch.exp(-0.2 * torch.arange(m, device="cuda", dtype=torch.float64))
+        t *= decay[:, None, None]
+        return t.permute(*reversed(range(t.dim())))
+
+    u, w, b = field(6, 11), field(6, 12), field(6, 13)
+    tan, cot = field(18, 14, k), field(12, 15, k)
+    jv = sf.mhd_jvp(u, w, b, tan, m_max_pad=pad)
+    jt = sf.mhd_vjp(u, w, b, cot, m_max_pad=pad)
+
+    def fortran(t):
+        o = sf.fortran_empty(*t.shape)
+        o.copy_(t)
+        return o
+
+    def cross(x, y):
+        return sf.product(sf.OP_CROSS, fortran(x), fortran(y), m_max_pad=pad)
+
+    for t in range(k):
+        du, dw, db = tan[:, 0:6, :, t], tan[:, 6:12, :, t], tan[:, 12:18, :, t]
+        for c, (base, dbase, out) in enumerate(((w, dw, jv[:, 0:6, :, t]), (b, db, jv[:, 6:12, :, t]))):
+            fd = (cross(u + h * du, base + h * dbase) - cross(u - h * du, base - h * dbase)) / (2 * h)
+            assert float(torch.linalg.vector_norm(fd - out) / torch.linalg.vector_norm(out)) <= 1e-8, (t, c)
+            del fd
+    lhs, rhs = float(torch.sum(jv * cot)), float(torch.sum(tan * jt))
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+    del u, w, b, tan, cot, jv, jt
+    torch.cuda.empty_cache()
+
+
 def test_bundle_full_size_matches_the_elementary_products():
     # the MHD bundle at its configuration's size (1.4 M points, m = 64): the one-launch kernel against the
     # elementary cross and dot products (other kernels, each pinned to the oracle above) over every point
