@@ -63,8 +63,9 @@ enum {
   SFNL_ERR_ALLOC = -7,       /* device or pinned host allocation failed */
   SFNL_ERR_TIMEOUT = -8      /* a split-form kernel gave up a bounded wait on its tensor-core
                                 operations, or the FAST MHD bundle on its bulk copies; the outputs of
-                                that call are incomplete (reported by the next call of that form or
-                                at the end of a host-array call) */
+                                that call are incomplete (reported by the next split-form or FAST
+                                MHD bundle call, which share one status word, or at the end of a
+                                host-array call) */
 };
 
 /* Algorithm of the all-FP64 forms. */
