@@ -146,6 +146,26 @@ def test_bundle_kernels_agree(npts):
             assert R.rel_l2(r3[i], refs[i]) <= FP64_TOL
 
 
+def test_bundle_unaligned_inputs_take_the_copy_path():
+    # inputs 8 bytes off a 16-byte boundary cannot feed the bulk tensor copies: with an even point count the
+    # residue kernel stages them with 8-byte cp.async copies instead, to the same results
+    import torch
+
+    npts, m, pad = 64, 64, 96
+    f = [R.synthetic_field(npts, 6, m, 0.1, 720 + i) for i in range(5)]
+    d = []
+    for x in f:
+        t = dev(x)
+        buf = torch.empty(t.numel() + 1, dtype=torch.float64, device="cuda")
+        v = buf[1:].view(m, 6, npts).permute(2, 1, 0)  # Fortran strides, base 8 bytes past the allocation
+        v.copy_(t)
+        assert v.data_ptr() % 16 == 8
+        d.append(v)
+    outs = [host(o) for o in sf.bundle_mhd(*d, m_max_pad=pad)]
+    for o, r in zip(outs, R.mhd_bundle(*f, pad)):
+        assert R.rel_l2(o, r) <= FP64_TOL
+
+
 def test_bundle_reports_a_wait_that_gave_up():
     # Host-side injection: the wait-status word is marked as the m = 64 bundle kernel marks it when a bounded
     # wait on its bulk copies gives up; no device wait is made to run out.  The next bundle call reports
