@@ -95,7 +95,11 @@ def main(argv=None):
     ap.add_argument("--alpha", type=float, default=0.1)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--k", type=int, default=1, help="tangents (cotangents) of a linearised program")
+    ap.add_argument("--residues", type=int, default=0,
+                    help="residue classes of the large-m FAST form (3, 6 or 12; 0: the library's choice)")
     a = ap.parse_args(argv)
+    if a.residues:
+        sf._check(sf.lib().sfnl_test_large_residues(a.residues))
     kw = {"fast": dict(algo=sf.ALGO_FAST), "grid": dict(algo=sf.ALGO_GRID), "split3": dict(split=sf.SPLIT_BF16X3),
           "split2": dict(split=sf.SPLIT_BF16X2)}[a.form]
     pad = 3 * a.m // 2 if a.m > 1 else 1
