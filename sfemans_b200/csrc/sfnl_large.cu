@@ -828,8 +828,8 @@ bool residues_fit(int m, int N, int R) {
 
 // Residue classes of the two-kernel form for m modes on the N-angle grid; 0: the whole grid.  Six where
 // they fit, else three: on a B200, R = 6 against 3 took the cross product at m = 256 (350k points) from
-// 19.8 to 18.5 ms, at m = 384 (100k points) from 12.3 to 8.9 ms and at m = 512 (60k points) from 10.3 to
-// 7.2 ms, the 16-tangent MHD JVP at m = 256 (50k points) from 90.8 to 85.7 ms; residue grids of 64 angles
+// 18.7 to 16.9 ms, at m = 384 (100k points) from 11.4 to 7.9 ms and at m = 512 (60k points) from 10.1 to
+// 6.8 ms, the 16-tangent MHD JVP at m = 256 (50k points) from 87.0 to 80.3 ms; residue grids of 64 angles
 // (R = 12 at m = 256) were slower than both.
 int large_residues(int m, int N) {
   if (const int R = g_test_residues.load()) return residues_fit(m, N, R) ? R : 0;
