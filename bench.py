@@ -661,8 +661,9 @@ def _extra_configs(args, sf, torch, dev, world, rank, dist, local, stream):
     except sf.SfnlError as e:
         cfg["split3"] = {"unavailable": str(e)}
     nb = 8.0 * m * npts * (18 + k * (18 + 12))
-    cfg["roofline"] = {"jvp": roof(nb, ms_j, "large_syn_tf_kernel + large_prod_tf_kernel (tangents batched per launch)"),
-                       "vjp": roof(nb, ms_t, "large_syn_tf_kernel + large_prod_tf_kernel (tangents batched per launch)")}
+    kname5 = ("large_res_coef_kernel<6> + large_syn_tf_kernel + large_prod_tf_kernel + large_res_out_kernel<6> "
+              "(six residue grids, tangents batched per launch)")
+    cfg["roofline"] = {"jvp": roof(nb, ms_j, kname5), "vjp": roof(nb, ms_t, kname5)}
     if cpu_on:
         n_s, kt = 500, 2
         hU, hW, hB = (np.asfortranarray(H(x[:n_s])) for x in (U, W, B))
